@@ -1,0 +1,223 @@
+"""ctypes binding of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads oracle/liboracle.so (the restatement) and, when it has been built,
+oracle/_ref/libsexref.so (the reference's own background/filter code).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+NISO = 8
+
+
+class OrcConfig(C.Structure):
+    _fields_ = [
+        ("back_size", C.c_int), ("back_filtersize", C.c_int), ("back_filtthresh", C.c_double),
+        ("back_type", C.c_int), ("back_value", C.c_double),
+        ("thresh_type", C.c_int), ("detect_thresh", C.c_double), ("analysis_thresh", C.c_double),
+        ("filter_flag", C.c_int), ("conv_w", C.c_int), ("conv_h", C.c_int),
+        ("conv", C.POINTER(C.c_float)),
+        ("detect_minarea", C.c_int), ("deblend_nthresh", C.c_int), ("deblend_mincont", C.c_double),
+        ("clean_flag", C.c_int), ("clean_param", C.c_double),
+        ("satur_level", C.c_double), ("gain", C.c_double), ("mag_zeropoint", C.c_double),
+        ("phot_aperture", C.c_double), ("phot_autoparams", C.c_double * 2), ("mask_type", C.c_int),
+        ("weight_type", C.c_int), ("numbering", C.c_int),
+    ]
+
+
+OBJECT_FIELDS = [
+    ("number", "i4"), ("root", "i4"), ("level", "i4"), ("fdnpix", "i4"), ("dnpix", "i4"),
+    ("npix", "i4"), ("xmin", "i4"), ("xmax", "i4"), ("ymin", "i4"), ("ymax", "i4"),
+    ("peakx", "i4"), ("peaky", "i4"), ("flags", "i4"), ("iso", "i4", (NISO,)),
+    ("fdflux", "f4"), ("dflux", "f4"), ("flux", "f4"), ("fluxerr", "f4"), ("fdpeak", "f4"),
+    ("dpeak", "f4"), ("peak", "f4"),
+    ("mx", "f8"), ("my", "f8"), ("mx2", "f8"), ("my2", "f8"), ("mxy", "f8"),
+    ("a", "f4"), ("b", "f4"), ("theta", "f4"), ("abcor", "f4"), ("cxx", "f4"), ("cyy", "f4"),
+    ("cxy", "f4"),
+    ("poserr_mx2", "f8"), ("poserr_my2", "f8"), ("poserr_mxy", "f8"),
+    ("bkg", "f4"), ("thresh", "f4"), ("dthresh", "f4"), ("mthresh", "f4"), ("fwhm", "f4"),
+    ("flux_iso", "f4"), ("fluxerr_iso", "f4"), ("mag_iso", "f4"), ("magerr_iso", "f4"),
+    ("flux_isocor", "f4"), ("fluxerr_isocor", "f4"),
+    ("flux_aper", "f4"), ("fluxerr_aper", "f4"), ("mag_aper", "f4"), ("magerr_aper", "f4"),
+    ("kronfactor", "f4"), ("flux_auto", "f4"), ("fluxerr_auto", "f4"), ("mag_auto", "f4"),
+    ("magerr_auto", "f4"), ("elong", "f4"), ("ellip", "f4"), ("polar", "f4"),
+]
+OBJECT_DTYPE = np.dtype(OBJECT_FIELDS, align=True)
+
+
+class OrcSummary(C.Structure):
+    _fields_ = [
+        ("nbackx", C.c_int), ("nbacky", C.c_int), ("backmean", C.c_float), ("backsig", C.c_float),
+        ("dthresh", C.c_float), ("thresh", C.c_float), ("npix_above", C.c_int64),
+        ("nraw", C.c_int32), ("nraw_pix", C.c_int64), ("ndetected", C.c_int32), ("nobj", C.c_int32),
+    ]
+
+
+_lib = None
+_ref = None
+
+
+def build(ref=True):
+    subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
+    if ref and os.path.isdir(os.environ.get("REFSRC", "/root/reference/src")):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build(ref=False)
+        _lib = C.CDLL(path)
+        _lib.orc_extract.restype = C.c_int
+        _lib.orc_background.restype = C.c_int
+        _lib.orc_hmedian.restype = C.c_float
+        _lib.orc_median_walk.restype = C.c_int
+        _lib.orc_median_mergepath.restype = C.c_int
+        _lib.orc_xsum_floats.restype = C.c_double
+    return _lib
+
+
+def ref():
+    """The reference's own background/filter code, or None if not built."""
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libsexref.so")
+        if not os.path.exists(path):
+            return None
+        _ref = C.CDLL(path)
+    return _ref
+
+
+def _f(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def make_config(**kw):
+    d = default_config()
+    d.update(kw)
+    cfg = OrcConfig()
+    mask = np.ascontiguousarray(d.pop("conv"), dtype=np.float32)
+    cfg._mask = mask  # keep alive
+    for k, v in d.items():
+        if k == "phot_autoparams":
+            cfg.phot_autoparams[0], cfg.phot_autoparams[1] = v
+        else:
+            setattr(cfg, k, v)
+    cfg.conv = _f(mask)
+    cfg.conv_h, cfg.conv_w = mask.shape
+    return cfg
+
+
+DEFAULT_CONV = np.array([[1, 2, 1], [2, 4, 2], [1, 2, 1]], np.float32) / np.float32(16.0)
+
+
+def default_config():
+    return dict(back_size=64, back_filtersize=3, back_filtthresh=0.0, back_type=0, back_value=0.0,
+                thresh_type=0, detect_thresh=1.5, analysis_thresh=1.5, filter_flag=1,
+                conv=DEFAULT_CONV, detect_minarea=5, deblend_nthresh=32, deblend_mincont=0.005,
+                clean_flag=1, clean_param=1.0, satur_level=50000.0, gain=0.0, mag_zeropoint=0.0,
+                phot_aperture=5.0, phot_autoparams=(2.5, 3.5), mask_type=2, weight_type=0,
+                numbering=0)
+
+
+def background(img, **kw):
+    """Background-subtract a copy of img; returns (sub, back, sigma, summary)."""
+    cfg = make_config(**kw)
+    sub = np.ascontiguousarray(img, dtype=np.float32).copy()
+    h, w = sub.shape
+    bw, bh = min(cfg.back_size, w), min(cfg.back_size, h)
+    nb = ((w - 1) // bw + 1) * ((h - 1) // bh + 1)
+    back = np.zeros(nb, np.float32)
+    sig = np.zeros(nb, np.float32)
+    s = OrcSummary()
+    lib().orc_background(_f(sub), w, h, C.byref(cfg), _f(back), _f(sig), None, None, C.byref(s))
+    return sub, back, sig, s
+
+
+def filter_image(sub, mask):
+    sub = np.ascontiguousarray(sub, np.float32)
+    mask = np.ascontiguousarray(mask, np.float32)
+    h, w = sub.shape
+    cd = np.zeros_like(sub)
+    lib().orc_filter(_f(sub), w, h, _f(mask), mask.shape[1], mask.shape[0], _f(cd))
+    return cd
+
+
+def extract(img, max_objects=None, want_maps=False, **kw):
+    """Full extraction; returns (objects structured array, segmap, summary[, sub, cd])."""
+    cfg = make_config(**kw)
+    img = np.ascontiguousarray(img, np.float32)
+    h, w = img.shape
+    if max_objects is None:
+        max_objects = w * h // max(1, cfg.detect_minarea) // 2 + 16
+    objs = np.zeros(max_objects, OBJECT_DTYPE)
+    seg = np.zeros((h, w), np.int32)
+    s = OrcSummary()
+    sub = np.zeros_like(img) if want_maps else None
+    cd = np.zeros_like(img) if want_maps else None
+    n = lib().orc_extract(_f(img), None, w, h, C.byref(cfg), objs.ctypes.data_as(C.c_void_p),
+                          max_objects, seg.ctypes.data_as(C.c_void_p),
+                          _f(sub) if want_maps else None, _f(cd) if want_maps else None,
+                          C.byref(s))
+    if n < 0:
+        raise RuntimeError("oracle extraction failed: %d" % n)
+    if want_maps:
+        return objs[:n], seg, s, sub, cd
+    return objs[:n], seg, s
+
+
+def getconv(path):
+    mask = np.zeros(1024, np.float32)
+    mw, mh = C.c_int(), C.c_int()
+    n = lib().orc_getconv(path.encode(), _f(mask), 1024, C.byref(mw), C.byref(mh))
+    if n < 0:
+        raise ValueError("bad convolution file %s (%d)" % (path, n))
+    return mask[:n].reshape(mh.value, mw.value).copy()
+
+
+def ref_background(img, back_size=64, back_filtersize=3, back_filtthresh=0.0, back_type=0,
+                   back_value=0.0, detect_thresh=1.5, analysis_thresh=1.5):
+    r = ref()
+    if r is None:
+        return None
+    sub = np.ascontiguousarray(img, dtype=np.float32).copy()
+    h, w = sub.shape
+    bw, bh = min(back_size, w), min(back_size, h)
+    nb = ((w - 1) // bw + 1) * ((h - 1) // bh + 1)
+    back = np.zeros(nb, np.float32)
+    sig = np.zeros(nb, np.float32)
+    st = np.zeros(4, np.float32)
+    r.ref_background(_f(sub), w, h, back_size, back_filtersize, C.c_double(back_filtthresh),
+                     back_type, C.c_double(back_value), C.c_double(detect_thresh),
+                     C.c_double(analysis_thresh), _f(back), _f(sig), _f(st))
+    return sub, back, sig, st
+
+
+def ref_getconv(path):
+    r = ref()
+    if r is None:
+        return None
+    mask = np.zeros(1024, np.float32)
+    mw, mh = C.c_int(), C.c_int()
+    n = r.ref_getconv(path.encode(), _f(mask), 1024, C.byref(mw), C.byref(mh))
+    if n < 0:
+        raise ValueError(path)
+    return mask[:n].reshape(mh.value, mw.value).copy()
+
+
+def ref_convolve(sub, mask):
+    r = ref()
+    if r is None:
+        return None
+    sub = np.ascontiguousarray(sub, np.float32).copy()
+    mask = np.ascontiguousarray(mask, np.float32)
+    h, w = sub.shape
+    cd = np.zeros_like(sub)
+    r.ref_convolve(_f(sub), w, h, _f(mask), mask.shape[1], mask.shape[0], _f(cd))
+    return cd
