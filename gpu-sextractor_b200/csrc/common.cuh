@@ -1,0 +1,294 @@
+// common.cuh -- shared device helpers for libsexgpu (sm_100a).
+//
+// Compiled with -fmad=false: every floating-point expression below evaluates
+// with separately rounded IEEE operations in the order written, the same
+// arithmetic the reference's host C code performs.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define SX_BIG 1e+30
+#define SX_PI 3.1415926535898
+#define SX_EPS (1e-4)
+#define SX_BACK_MINGOODFRAC 0.5
+#define SX_QUANTIF_NSIGMA 5
+#define SX_QUANTIF_NMAXLEVELS 4096
+#define SX_QUANTIF_AMIN 4
+#define SX_MAXDEBAREA 3
+#define SX_CLEAN_ZONE 10.0
+#define SX_APER_OVERSAMP 5
+#define SX_KRON_NSIG (3 * 2.0)
+#define SX_CROWD_THRESHOLD 0.1
+#define SX_MAXCONV 31
+#define SX_NISO_ 8
+
+// object flags, src/cuda/cudatypes.h:30-37
+#define SX_OBJ_CROWDED 0x0001
+#define SX_OBJ_MERGED 0x0002
+#define SX_OBJ_SATUR 0x0004
+#define SX_OBJ_TRUNC 0x0008
+#define SX_OBJ_APERT_PB 0x0010
+
+// device status word bits
+#define SX_ST_RANGE 1
+#define SX_ST_LOOP 2
+#define SX_ST_CAPACITY 4
+
+#define SX_ALLOC_OTHER 0x7fffffff
+
+// ---------------------------------------------------------------------------
+// Exact, order-free sums of float terms.
+//
+// The value v * 2^(e-23) is exact; e is the smallest binary exponent of the
+// non-zero terms seen so far.  Adding a smaller-exponent term shifts v left
+// (exactly).  Any order of adds and merges gives the same exact value, which
+// is rounded once when read; denormal terms count as zero; a sum whose
+// dynamic range would exceed 125 bits raises ovf.
+// ---------------------------------------------------------------------------
+#define XS_EMPTY 1000
+
+struct XSum {
+    __int128 v;
+    int e;
+    int ovf;
+};
+
+__device__ __forceinline__ void xs_init(XSum &s) {
+    s.v = 0;
+    s.e = XS_EMPTY;
+    s.ovf = 0;
+}
+
+__device__ __forceinline__ int xs_bits(__int128 v) {
+    unsigned __int128 m = v < 0 ? (unsigned __int128)(-v) : (unsigned __int128)v;
+    unsigned long long hi = (unsigned long long)(m >> 64), lo = (unsigned long long)m;
+    if (hi) return 128 - __clzll(hi);
+    if (lo) return 64 - __clzll(lo);
+    return 0;
+}
+
+__device__ __forceinline__ void xs_rescale(XSum &s, int e) {
+    if (e >= s.e) return;
+    if (s.v != 0) {
+        int sh = s.e - e;
+        if (sh > 125 || xs_bits(s.v) + sh > 125) {
+            s.ovf = 1;
+            s.v = 0;
+        } else {
+            s.v = (__int128)((unsigned __int128)s.v << sh);
+        }
+    }
+    s.e = e;
+}
+
+__device__ __forceinline__ void xs_add(XSum &s, float f) {
+    unsigned int u = __float_as_uint(f);
+    int ef = (int)((u >> 23) & 0xff);
+    if (ef == 0) return;
+    ef -= 127;
+    if (ef < s.e) xs_rescale(s, ef);
+    int sh = ef - s.e;
+    if (sh > 100) {
+        s.ovf = 1;
+        return;
+    }
+    unsigned int m = (u & 0x7fffffu) | 0x800000u;
+    __int128 t = (__int128)((unsigned __int128)m << sh);
+    if (u >> 31)
+        s.v -= t;
+    else
+        s.v += t;
+}
+
+__device__ __forceinline__ void xs_merge(XSum &s, XSum b) {
+    if (b.ovf) s.ovf = 1;
+    if (b.e == XS_EMPTY) return;
+    if (s.e == XS_EMPTY) {
+        s.v = b.v;
+        s.e = b.e;
+        return;
+    }
+    if (b.e < s.e)
+        xs_rescale(s, b.e);
+    else if (s.e < b.e)
+        xs_rescale(b, s.e);
+    if (b.ovf) s.ovf = 1;
+    s.v += b.v;
+}
+
+// exact value -> nearest double (ties to even)
+__device__ __forceinline__ double xs_double(const XSum &s) {
+    if (s.v == 0 || s.e == XS_EMPTY) return 0.0;
+    bool neg = s.v < 0;
+    unsigned __int128 mag = neg ? (unsigned __int128)(-s.v) : (unsigned __int128)s.v;
+    unsigned long long hi = (unsigned long long)(mag >> 64), lo = (unsigned long long)mag;
+    double d;
+    int sc;
+    if (!hi) {
+        d = __ull2double_rn(lo);
+        sc = 0;
+    } else {
+        int k = 127 - __clzll(hi);  // msb position
+        int drop = k - 63;
+        unsigned long long top = (unsigned long long)(mag >> drop);
+        unsigned __int128 rem = mag & ((((unsigned __int128)1) << drop) - 1);
+        if (rem) top |= 1ull;
+        d = __ull2double_rn(top);
+        sc = drop;
+    }
+    d = scalbn(d, sc + s.e - 23);
+    return neg ? -d : d;
+}
+
+__device__ __forceinline__ float xs_float(const XSum &s) { return (float)xs_double(s); }
+
+__device__ __forceinline__ XSum xs_shfl_down(const XSum &s, int off) {
+    XSum r;
+    unsigned long long lo = (unsigned long long)s.v, hi = (unsigned long long)(s.v >> 64);
+    lo = __shfl_down_sync(0xffffffffu, lo, off);
+    hi = __shfl_down_sync(0xffffffffu, hi, off);
+    r.v = (__int128)(((unsigned __int128)hi << 64) | lo);
+    r.e = __shfl_down_sync(0xffffffffu, s.e, off);
+    r.ovf = __shfl_down_sync(0xffffffffu, s.ovf, off);
+    return r;
+}
+
+// full-warp reduction; the result is valid in lane 0
+__device__ __forceinline__ XSum xs_warp_reduce(XSum s) {
+    for (int off = 16; off > 0; off >>= 1) xs_merge(s, xs_shfl_down(s, off));
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// Fixed-scale exact accumulators usable with atomics: value =
+// sum_k (int64)w[k] * 2^(32k) in units of 2^(e0-23).  A float term of
+// exponent e >= e0 is split into 32-bit limbs; each limb word stays exact for
+// up to 2^31 terms.
+// ---------------------------------------------------------------------------
+struct Limbs4 {
+    unsigned long long w[4];
+};
+
+__device__ __forceinline__ void limbs_term(float f, int e0, unsigned int lim[4], bool &neg, int &bad) {
+    unsigned int u = __float_as_uint(f);
+    int ef = (int)((u >> 23) & 0xff);
+    lim[0] = lim[1] = lim[2] = lim[3] = 0;
+    neg = (u >> 31) != 0;
+    if (ef == 0) return;
+    int sh = ef - 127 - e0;
+    if (sh < 0 || sh > 100) {
+        bad = 1;
+        return;
+    }
+    unsigned __int128 t = ((unsigned __int128)((u & 0x7fffffu) | 0x800000u)) << sh;
+    lim[0] = (unsigned int)t;
+    lim[1] = (unsigned int)(t >> 32);
+    lim[2] = (unsigned int)(t >> 64);
+    lim[3] = (unsigned int)(t >> 96);
+}
+
+__device__ __forceinline__ void limbs_atomic_add_term(unsigned long long *acc, float f, int e0, int *status) {
+    unsigned int lim[4];
+    bool neg;
+    int bad = 0;
+    limbs_term(f, e0, lim, neg, bad);
+    if (bad) {
+        atomicOr(status, SX_ST_RANGE);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (lim[k]) atomicAdd(acc + k, neg ? (unsigned long long)(-(long long)lim[k]) : (unsigned long long)lim[k]);
+}
+
+__device__ __forceinline__ XSum limbs_to_xsum(const unsigned long long *w, int e0) {
+    XSum s;
+    __int128 v = 0;
+#pragma unroll
+    for (int k = 3; k >= 0; k--) v = (v << 32) + (__int128)(long long)w[k];
+    s.v = v;
+    s.e = e0;
+    s.ovf = 0;
+    return s;
+}
+
+// orderable integer image of a float (monotone for all finite floats)
+__device__ __forceinline__ unsigned int f2ord(float f) {
+    unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(unsigned int o) {
+    unsigned int u = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
+    return __uint_as_float(u);
+}
+
+__device__ __forceinline__ int fexpo(float v) { return (int)((__float_as_uint(v) >> 23) & 0xff) - 127; }
+
+// bilinear background at (x, y), src/back.c:685-731
+__device__ __forceinline__ float back_at(const float *b, int nx, int ny, int backw, int backh, int x, int y) {
+    int xl, yl, pos;
+    double dx, dy, cdx;
+    float b0, b1, b2, b3;
+    dx = (double)x / backw - 0.5;
+    dy = (double)y / backh - 0.5;
+    dx -= (xl = (int)dx);
+    dy -= (yl = (int)dy);
+    if (xl < 0) {
+        xl = 0;
+        dx -= 1.0;
+    } else if (xl >= nx - 1) {
+        xl = nx < 2 ? 0 : nx - 2;
+        dx += 1.0;
+    }
+    if (yl < 0) {
+        yl = 0;
+        dy -= 1.0;
+    } else if (yl >= ny - 1) {
+        yl = ny < 2 ? 0 : ny - 2;
+        dy += 1.0;
+    }
+    pos = yl * nx + xl;
+    cdx = 1 - dx;
+    b += pos;
+    b0 = *b;
+    b1 = nx < 2 ? b0 : *(++b);
+    b2 = ny < 2 ? *b : *(b += nx);
+    b3 = nx < 2 ? *b : *(--b);
+    return (float)((1 - dy) * (cdx * b0 + dx * b1) + dy * (dx * b2 + cdx * b3));
+}
+
+// ---------------------------------------------------------------------------
+// Device-side parameters of one extraction
+// ---------------------------------------------------------------------------
+struct FrameParams {
+    int w, h;
+    int bw, bh, nbx, nby;           // meshes
+    int nfx, nfy;                   // mesh filter window
+    float fthresh;                  // BACK_FILTTHRESH
+    int back_type;
+    float back_value;
+    int thresh_type;
+    double detect_thresh, analysis_thresh;
+    int conv_w, conv_h, filter_flag;
+    int minarea, debminarea, nthresh;
+    double mincont;
+    int clean_flag;
+    double clean_param;
+    double satur_level, gain, mag_zeropoint, aperture;
+    double autoparam0, autoparam1;
+    int mask_type, numbering;
+};
+
+// scalars computed on the device during one extraction
+struct FrameScalars {
+    float backmean, backsig, dthresh, thresh;
+    int e0cd;                       // exponent of dthresh (all object cd >= dthresh)
+    int status;                     // SX_ST_* bits
+    int npix_above;
+    int nroots;
+    int nrootpix;
+    int nobj;                       // objects after deblending
+    int nsurv;                      // after CLEAN
+    int e0sub;                      // smallest exponent of a non-zero |sub|
+};

@@ -1,0 +1,448 @@
+// k_back.cu -- background estimation (reference: src/back.c makeback,
+// backstat, backhisto, backguess, filterback, makebackspline, subbackline and
+// the CUDA driver src/cuda/cudaback.cu:1212).
+//
+// Results are bit-identical to the reference's CPU functions:
+//  * the per-mesh mean/sigma are the reference's sequential double sums, run
+//    one thread per mesh in the same pixel order;
+//  * histogram sums are exact integers, so they are reduced in parallel;
+//  * the two-pointer median walk of backguess is replaced by a binary search
+//    on the merge path of the two cumulative sums, which lands on the same
+//    split;
+//  * spline and interpolation arithmetic is float, in the reference's order.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace sx {
+
+// src/back.c:214-279 for one mesh per thread
+__global__ void k_mesh_stat(const float *__restrict__ img, int w, int h, int bw, int bh, int nbx, int nby,
+                            MeshStat *__restrict__ ms) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nbx * nby) return;
+    int mx = m % nbx, my = m / nbx;
+    int x0 = mx * bw, y0 = my * bh;
+    int mw = (mx == nbx - 1 && w % bw) ? w % bw : bw;
+    int mh = (my == nby - 1 && h % bh) ? h % bh : bh;
+    double pix, sig, mean = 0.0, sigma = 0.0;
+    double step = sqrt(2 / SX_PI) * SX_QUANTIF_NSIGMA / SX_QUANTIF_AMIN;
+    int npix = 0;
+    MeshStat o;
+    o.mean = o.sigma = o.lcut = o.hcut = o.qzero = o.qscale = 0.f;
+    o.nlevels = o.npix = 0;
+    for (int y = 0; y < mh; y++) {
+        const float *row = img + (size_t)(y0 + y) * w + x0;
+        for (int x = 0; x < mw; x++)
+            if ((pix = __ldg(row + x)) > -SX_BIG) {
+                mean += pix;
+                sigma += pix * pix;
+                npix++;
+            }
+    }
+    if ((float)npix < (float)(mw * mh * SX_BACK_MINGOODFRAC)) {
+        o.mean = o.sigma = -SX_BIG;
+        ms[m] = o;
+        return;
+    }
+    mean /= (double)npix;
+    sigma = (sig = sigma / npix - mean * mean) > 0.0 ? sqrt(sig) : 0.0;
+    float lcut = o.lcut = (float)(mean - 2.0 * sigma);
+    float hcut = o.hcut = (float)(mean + 2.0 * sigma);
+    mean = sigma = 0.0;
+    npix = 0;
+    for (int y = 0; y < mh; y++) {
+        const float *row = img + (size_t)(y0 + y) * w + x0;
+        for (int x = 0; x < mw; x++) {
+            pix = __ldg(row + x);
+            if (pix <= hcut && pix >= lcut) {
+                mean += pix;
+                sigma += pix * pix;
+                npix++;
+            }
+        }
+    }
+    o.npix = npix;
+    mean /= (double)npix;
+    sig = sigma / npix - mean * mean;
+    sigma = sig > 0.0 ? sqrt(sig) : 0.0;
+    o.mean = mean;
+    o.sigma = sigma;
+    if ((o.nlevels = (int)(step * npix + 1)) > SX_QUANTIF_NMAXLEVELS) o.nlevels = SX_QUANTIF_NMAXLEVELS;
+    o.qscale = sigma > 0.0 ? 2 * SX_QUANTIF_NSIGMA * sigma / o.nlevels : 1.0;
+    o.qzero = mean - SX_QUANTIF_NSIGMA * sigma;
+    ms[m] = o;
+}
+
+constexpr int GUESS_THREADS = 256;
+
+// src/back.c:297-339 (backhisto) + :347-432 (backguess), one CTA per mesh
+__global__ void __launch_bounds__(GUESS_THREADS) k_mesh_guess(const float *__restrict__ img, int w, int h, int bw,
+                                                                int bh, int nbx, int nby,
+                                                                const MeshStat *__restrict__ ms,
+                                                                float *__restrict__ back, float *__restrict__ sig) {
+    __shared__ int hist[SX_QUANTIF_NMAXLEVELS + 2];
+    __shared__ int pfx[SX_QUANTIF_NMAXLEVELS + 2];   // pfx[i] = sum_{k<i} hist[k]
+    __shared__ long long red[3][GUESS_THREADS / 32];
+    __shared__ int sh_lcut, sh_hcut, sh_go;
+    int m = blockIdx.x;
+    int mx = m % nbx, my = m / nbx;
+    MeshStat bm = ms[m];
+    if (bm.mean <= -SX_BIG) {
+        if (threadIdx.x == 0) back[m] = sig[m] = -SX_BIG;
+        return;
+    }
+    int x0 = mx * bw, y0 = my * bh;
+    int mw = (mx == nbx - 1 && w % bw) ? w % bw : bw;
+    int mh = (my == nby - 1 && h % bh) ? h % bh : bh;
+    for (int i = threadIdx.x; i < SX_QUANTIF_NMAXLEVELS + 2; i += GUESS_THREADS) hist[i] = 0;
+    __syncthreads();
+    int nlevels = bm.nlevels;
+    float qscale = bm.qscale;
+    float cste = 0.499999 - bm.qzero / qscale;
+    int np = mw * mh;
+    for (int i = threadIdx.x; i < np; i += GUESS_THREADS) {
+        float p = __ldg(img + (size_t)(y0 + i / mw) * w + x0 + i % mw);
+        float b = p / qscale + cste;
+        if (b != b) continue;  // NaN: the host conversion yields INT_MIN
+        int bin = (int)b;
+        if (bin >= 0 && bin < nlevels) atomicAdd(&hist[bin], 1);
+    }
+    __syncthreads();
+    // prefix of the histogram (one warp per 1/8 of the bins, then fix-up)
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int i = 0; i <= SX_QUANTIF_NMAXLEVELS + 1; i++) {
+            pfx[i] = s;
+            s += hist[i];
+        }
+    }
+    __syncthreads();
+
+    int nlevelsm1 = nlevels - 1;
+    double sig_ = 10.0 * nlevelsm1, sig1 = 1.0, mea = bm.mean, med = bm.mean;
+    if (threadIdx.x == 0) {
+        sh_lcut = 0;
+        sh_hcut = nlevelsm1;
+    }
+    for (int n = 100;;) {
+        if (threadIdx.x == 0) sh_go = (n-- && (sig_ >= 0.1) && (fabs(sig_ / sig1 - 1.0) > SX_EPS));
+        __syncthreads();
+        if (!sh_go) break;
+        int lcut = sh_lcut, hcut = sh_hcut;
+        // exact integer sums over [lcut, hcut]
+        long long s0 = 0, s1 = 0, s2 = 0;
+        for (int i = lcut + threadIdx.x; i <= hcut; i += GUESS_THREADS) {
+            long long pv = hist[i];
+            s0 += pv;
+            s1 += pv * i;
+            s2 += pv * i * (long long)i;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            s0 += __shfl_down_sync(0xffffffffu, s0, o);
+            s1 += __shfl_down_sync(0xffffffffu, s1, o);
+            s2 += __shfl_down_sync(0xffffffffu, s2, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            red[0][threadIdx.x >> 5] = s0;
+            red[1][threadIdx.x >> 5] = s1;
+            red[2][threadIdx.x >> 5] = s2;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long sum = 0, t1 = 0, t2 = 0;
+            for (int k = 0; k < GUESS_THREADS / 32; k++) {
+                sum += red[0][k];
+                t1 += red[1][k];
+                t2 += red[2][k];
+            }
+            // split of the two-pointer walk: smallest a with NOT(A(a) < B(nn-1-a))
+            int nn = hcut - lcut + 1, lo = 0, hi = nn;
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                int A = pfx[lcut + mid] - pfx[lcut];
+                int B = pfx[hcut + 1] - pfx[hcut + 1 - (nn - 1 - mid)];
+                if (A < B)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            int il = lcut + lo, ih = il - 1;
+            unsigned long lowsum = (unsigned long)(pfx[il] - pfx[lcut]);
+            unsigned long highsum = (unsigned long)(pfx[hcut + 1] - pfx[il]);
+            double ftemp;
+            sig1 = sig_;
+            sig_ = (double)t2;
+            mea = (double)t1;
+            long hl = hist[il], hh = ih >= 0 ? hist[ih] : 0;
+            med = ih >= 0 ? ((double)ih + 0.5 + ((double)highsum - lowsum) / (2.0 * (hl > hh ? hl : hh))) : 0.0;
+            if (sum) {
+                mea /= (double)sum;
+                sig_ = sig_ / sum - mea * mea;
+            }
+            sig_ = sig_ > 0.0 ? sqrt(sig_) : 0.0;
+            sh_lcut = (ftemp = med - 3.0 * sig_) > 0.0 ? (int)(ftemp > 0.0 ? ftemp + 0.5 : ftemp - 0.5) : 0;
+            sh_hcut = (ftemp = med + 3.0 * sig_) < nlevelsm1 ? (int)(ftemp > 0.0 ? ftemp + 0.5 : ftemp - 0.5)
+                                                               : nlevelsm1;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        float mean;
+        // src/back.c:408: the C library abs(int) applied to the double sig
+        if (abs((int)sig_) > 0.0) {
+            if (fabs((mea - med) / sig_) < 0.3)
+                mean = bm.qzero + (2.5 * med - 1.5 * mea) * bm.qscale;
+            else
+                mean = bm.qzero + med * bm.qscale;
+        } else
+            mean = bm.qzero + mea * bm.qscale;
+        back[m] = mean;
+        sig[m] = sig_ * bm.qscale;
+    }
+}
+
+// src/back.c:455-480: bad meshes take the mean of the nearest valid meshes.
+// Writes back2 (all meshes) and fixes sigma in place for bad meshes.
+__global__ void k_mesh_badfill(const float *__restrict__ back, float *__restrict__ sigma, float *__restrict__ back2,
+                               int nx, int ny) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx * ny) return;
+    float b = back[i];
+    back2[i] = b;
+    if (b > -SX_BIG) return;
+    int px = i % nx, py = i / nx;
+    float d2min = SX_BIG, val = 0.f, sval = 0.f, d2;
+    int nmin = 0;
+    for (int j = 0, y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++, j++)
+            if (back[j] > -SX_BIG) {
+                d2 = (float)(x - px) * (x - px) + (y - py) * (y - py);
+                if (d2 < d2min) {
+                    val = back[j];
+                    sval = sigma[j];
+                    nmin = 1;
+                    d2min = d2;
+                } else if (d2 == d2min) {
+                    val += back[j];
+                    sval += sigma[j];
+                    nmin++;
+                }
+            }
+    back2[i] = nmin ? val / nmin : 0.0;
+    sigma[i] = nmin ? sval / nmin : 1.0;
+}
+
+__device__ __forceinline__ float median_small(float *v, int n) {
+    for (int i = 1; i < n; i++) {
+        float t = v[i];
+        int j = i - 1;
+        while (j >= 0 && v[j] > t) {
+            v[j + 1] = v[j];
+            j--;
+        }
+        v[j + 1] = t;
+    }
+    return n & 1 ? v[n / 2] : (float)((v[n / 2 - 1] + v[n / 2]) / 2.0);
+}
+
+// src/back.c:482-533: median filter of the mesh maps (window shrunk at edges)
+__global__ void k_mesh_median(const float *__restrict__ back, const float *__restrict__ sigma,
+                              float *__restrict__ back3, float *__restrict__ sigma3, int nx, int ny, int npx,
+                              int npy, float fthresh) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx * ny) return;
+    int px = i % nx, py = i / nx;
+    int npx2 = nx - px - 1, npy2 = ny - py - 1;
+    if (npx2 > npx) npx2 = npx;
+    if (npx2 > px) npx2 = px;
+    if (npy2 > npy) npy2 = npy;
+    if (npy2 > py) npy2 = py;
+    float bm[121], sm[121];
+    int n = 0;
+    for (int dy = -npy2; dy <= npy2; dy++)
+        for (int dx = -npx2; dx <= npx2; dx++) {
+            int j = (py + dy) * nx + px + dx;
+            bm[n] = back[j];
+            sm[n++] = sigma[j];
+        }
+    float med = median_small(bm, n);
+    if (fabs(med - back[i]) >= fthresh) {
+        back3[i] = med;
+        sigma3[i] = median_small(sm, n);
+    } else {
+        back3[i] = back[i];
+        sigma3[i] = sigma[i];
+    }
+}
+
+// k-th smallest (0-based) of n floats (orderable keys), single CTA radix select
+__device__ unsigned select_kth(const float *v, int n, int k, unsigned lowkey, unsigned *hist) {
+    unsigned prefix = 0, mask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            unsigned key = f2ord(v[i]);
+            if (key < lowkey) continue;
+            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255], 1u);
+        }
+        __syncthreads();
+        __shared__ unsigned s_digit, s_k;
+        if (threadIdx.x == 0) {
+            unsigned c = 0, d = 0;
+            for (d = 0; d < 256; d++) {
+                if (c + hist[d] > (unsigned)k) break;
+                c += hist[d];
+            }
+            s_digit = d;
+            s_k = k - c;
+        }
+        __syncthreads();
+        prefix |= s_digit << shift;
+        mask |= 255u << shift;
+        k = s_k;
+        __syncthreads();
+    }
+    return prefix;
+}
+
+// global medians of the filtered maps (src/back.c:536-557), one CTA
+__global__ void k_back_medians(const float *__restrict__ back3, const float *__restrict__ sigma3, int nb,
+                               FrameScalars *sc, int back_type, float back_value, int thresh_type,
+                               double dthr, double athr) {
+    __shared__ unsigned hist[256];
+    __shared__ unsigned s_npos;
+    float med[2];
+    for (int q = 0; q < 2; q++) {
+        const float *v = q ? sigma3 : back3;
+        if (nb & 1) {
+            med[q] = ord2f(select_kth(v, nb, nb / 2, 0u, hist));
+        } else {
+            float a = ord2f(select_kth(v, nb, nb / 2 - 1, 0u, hist));
+            float b = ord2f(select_kth(v, nb, nb / 2, 0u, hist));
+            med[q] = (float)((a + b) / 2.0);
+        }
+    }
+    float backsig = med[1];
+    if (backsig <= 0.0) {
+        // median of the strictly positive sigmas, else 1.0
+        if (threadIdx.x == 0) s_npos = 0;
+        __syncthreads();
+        unsigned c = 0;
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) c += sigma3[i] > 0.0f;
+        atomicAdd(&s_npos, c);
+        __syncthreads();
+        int npos = (int)s_npos;
+        unsigned low = f2ord(__uint_as_float(1u));  // smallest positive float
+        if (npos > 0 && npos < nb) {
+            if (npos & 1)
+                backsig = ord2f(select_kth(sigma3, nb, npos / 2, low, hist));
+            else {
+                float a = ord2f(select_kth(sigma3, nb, npos / 2 - 1, low, hist));
+                float b = ord2f(select_kth(sigma3, nb, npos / 2, low, hist));
+                backsig = (float)((a + b) / 2.0);
+            }
+        } else
+            backsig = 1.0;
+    }
+    if (threadIdx.x == 0) {
+        sc->backmean = back_type == 1 ? back_value : med[0];
+        sc->backsig = backsig;
+        if (thresh_type == 1) {
+            sc->dthresh = (float)dthr;
+            sc->thresh = (float)athr;
+        } else {
+            sc->dthresh = (float)(dthr * backsig);
+            sc->thresh = (float)(athr * backsig);
+        }
+        sc->e0cd = fexpo(sc->dthresh);
+    }
+}
+
+// src/back.c:739-773 (makebackspline), one thread per mesh column
+__global__ void k_back_spline(const float *__restrict__ map, float *__restrict__ dmap, float *__restrict__ u,
+                              int nbx, int nby) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= nbx) return;
+    float temp;
+    if (nby > 1) {
+        float *ux = u + (size_t)x * nby;
+        dmap[x] = ux[0] = 0.0;
+        for (int y = 1; y < nby - 1; y++) {
+            temp = -1 / (dmap[(size_t)(y - 1) * nbx + x] + 4);
+            dmap[(size_t)y * nbx + x] = temp;
+            temp *= ux[y - 1] - 6 * (map[(size_t)(y + 1) * nbx + x] + map[(size_t)(y - 1) * nbx + x]
+                                     - 2 * map[(size_t)y * nbx + x]);
+            ux[y] = temp;
+        }
+        dmap[(size_t)(nby - 1) * nbx + x] = 0.0;
+        for (int y = nby - 2; y >= 1; y--)
+            dmap[(size_t)y * nbx + x] = (dmap[(size_t)y * nbx + x] * dmap[(size_t)(y + 1) * nbx + x] + ux[y]) / 6.0;
+    } else
+        dmap[x] = 0.0;
+}
+
+// src/back.c:790-862: y-interpolated nodes of every image row and their
+// x-direction second derivatives (one thread per row)
+__global__ void k_row_nodes(const float *__restrict__ back, const float *__restrict__ dback, int nbx, int nby,
+                            int backh, int h, float *__restrict__ node, float *__restrict__ dnode,
+                            float *__restrict__ u) {
+    int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= h) return;
+    float *nd = node + (size_t)y * nbx, *dnd = dnode + (size_t)y * nbx, *uu = u + (size_t)y * nbx;
+    if (nby > 1) {
+        int yl;
+        float dy, dy3, cdy, cdy3, temp;
+        dy = (float)y / backh - 0.5;
+        dy -= (yl = (int)dy);
+        if (yl < 0) {
+            yl = 0;
+            dy -= 1.0;
+        } else if (yl >= nby - 1) {
+            yl = nby < 2 ? 0 : nby - 2;
+            dy += 1.0;
+        }
+        cdy = 1 - dy;
+        dy3 = (dy * dy * dy - dy);
+        cdy3 = (cdy * cdy * cdy - cdy);
+        const float *blo = back + (size_t)nbx * yl, *bhi = blo + nbx;
+        const float *dblo = dback + (size_t)nbx * yl, *dbhi = dblo + nbx;
+        for (int x = 0; x < nbx; x++) nd[x] = cdy * blo[x] + dy * bhi[x] + cdy3 * dblo[x] + dy3 * dbhi[x];
+        if (nbx > 1) {
+            dnd[0] = uu[0] = 0.0;
+            for (int x = 1; x < nbx - 1; x++) {
+                temp = -1 / (dnd[x - 1] + 4);
+                dnd[x] = temp;
+                temp *= uu[x - 1] - 6 * (nd[x + 1] + nd[x - 1] - 2 * nd[x]);
+                uu[x] = temp;
+            }
+            dnd[nbx - 1] = 0.0;
+            for (int x = nbx - 2; x >= 1; x--) dnd[x] = (dnd[x] * dnd[x + 1] + uu[x]) / 6.0;
+        } else
+            dnd[0] = 0.0;
+    } else {
+        for (int x = 0; x < nbx; x++) {
+            nd[x] = back[x];
+            dnd[x] = dback[x];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+void launch_background(BackBufs &B, const float *img, const FrameParams &P, FrameScalars *d_sc,
+                       cudaStream_t st, int &launches) {
+    int nb = P.nbx * P.nby;
+    k_mesh_stat<<<(nb + 127) / 128, 128, 0, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, B.ms);
+    k_mesh_guess<<<nb, GUESS_THREADS, 0, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, B.ms, B.back, B.sigma);
+    k_mesh_badfill<<<(nb + 127) / 128, 128, 0, st>>>(B.back, B.sigma, B.back2, P.nbx, P.nby);
+    k_mesh_median<<<(nb + 127) / 128, 128, 0, st>>>(B.back2, B.sigma, B.back3, B.sigma3, P.nbx, P.nby, P.nfx / 2,
+                                                   P.nfy / 2, P.fthresh);
+    k_back_medians<<<1, 1024, 0, st>>>(B.back3, B.sigma3, nb, d_sc, P.back_type, P.back_value, P.thresh_type,
+                                       P.detect_thresh, P.analysis_thresh);
+    k_back_spline<<<(P.nbx + 127) / 128, 128, 0, st>>>(B.back3, B.dback, B.u, P.nbx, P.nby);
+    k_row_nodes<<<(P.h + 127) / 128, 128, 0, st>>>(B.back3, B.dback, P.nbx, P.nby, P.bh, P.h, B.rownode,
+                                                  B.rowdnode, B.rowu);
+    launches += 7;
+}
+
+}  // namespace sx

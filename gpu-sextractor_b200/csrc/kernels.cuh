@@ -1,0 +1,86 @@
+// kernels.cuh -- buffers and launchers shared by the stages of libsexgpu.
+#pragma once
+#include "common.cuh"
+
+namespace sx {
+
+struct MeshStat {
+    float mean, sigma, lcut, hcut, qzero, qscale;
+    int nlevels, npix;
+};
+
+struct BackBufs {
+    MeshStat *ms;
+    float *back, *sigma, *back2, *back3, *sigma3, *dback, *u;
+    float *rownode, *rowdnode, *rowu;   // h x nbx each
+    int *colk;                          // w
+    float *coldx;                       // w
+};
+
+// per-root data (index = root id, first-pixel order)
+struct RootBufs {
+    int *size, *off, *first;            // pixels, offset in the root pixel list, first pixel
+    int *ymax, *lastx;                  // completion-order keys
+    float *fdpeak, *fdflux;
+    int *nkept, *objbase;
+};
+
+// per-element scratch of the deblending (index = position in the root pixel list)
+struct DebBufs {
+    int *par, *lev, *sz, *order, *rl0, *rl1, *nid0, *nid1;
+    unsigned long long *acc;            // 4 limbs per element
+    int *nd_root0, *nd_root1, *nd_flag0, *nd_flag1, *nd_nson0, *nd_nson1, *nd_okc0, *nd_okc1;
+    int *nd_oka0, *nd_oka1;
+    unsigned long long *kept;           // packed (level << 32) | element, per root at its offset
+    int *own, *kl, *kidx;
+    // per-kept-object accumulators (index = root offset + kept index)
+    unsigned long long *pacc;           // 7 sums x 4 limbs
+    int *pint;                          // xmin, xmax, ymin, ymax, peak(ord), cpeak(ord), dnpix, area2
+};
+
+// per-object data (index = object id: root order, then (level, label))
+struct ObjBufs {
+    int *root, *level, *n, *off;
+    int *xmin, *xmax, *ymin, *ymax, *dnpix, *flags, *singu;
+    float *fdflux, *dflux, *fdpeak, *dpeak, *node_dthresh;
+    double *mx, *my, *mx2, *my2, *mxy;
+    float *a, *b, *theta, *abcor, *cxx, *cyy, *cxy;
+    int *npix, *peakx, *peaky, *iso;    // iso: 8 per object
+    float *flux, *fluxerr, *peak, *bkg, *mthresh, *fwhm;
+    double *pmx2, *pmy2, *pmxy;
+    int *master, *fmaster, *number;
+    float *flux_isocor, *fluxerr_isocor, *flux_aper, *fluxerr_aper, *mag_aper, *magerr_aper;
+    float *kron, *flux_auto, *fluxerr_auto, *mag_auto, *magerr_auto;
+    float *mag_iso, *magerr_iso, *fluxerr_iso;
+    int *fdnpix;
+    unsigned long long *sortkey;
+};
+
+void launch_background(BackBufs &B, const float *img, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st,
+                       int &launches);
+
+void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const BackBufs &B,
+                       const FrameParams &P, FrameScalars *d_sc, const float *d_var, cudaStream_t st,
+                       int &launches);
+void set_conv_mask(const float *mask, int mw, int mh, cudaStream_t st);
+
+void launch_ccl(int *lab, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st, int &launches);
+
+struct DebArgs {
+    const float *cd, *sub;
+    const int *pos2idx;
+    const unsigned *rpix;       // root pixel lists (raster order per root)
+    RootBufs R;
+    DebBufs D;
+    ObjBufs O;
+    FrameScalars *sc;
+    int *alloc;                 // W*H object id map (-1 elsewhere)
+    unsigned *objkey;           // object id per root-list element
+    int w, h, N, debminarea;
+    double mincont;
+};
+
+void launch_deblend_sweep(const DebArgs &A, int nroots, cudaStream_t st);
+void launch_deblend_assign(const DebArgs &A, int nroots, cudaStream_t st);
+
+}  // namespace sx

@@ -1,0 +1,1005 @@
+// sexgpu.cu -- libsexgpu: context, extraction pipeline and the C ABI of
+// include/sexgpu.h.  Built as one translation unit with the stage files.
+//
+// The pipeline is the reference's scanimage() sequence (src/scan.c:65-163):
+// background (makeback), filter + threshold, connected components, deblending
+// (init_deblend/parcel_out), analysis (analyse_gpu), CLEAN (run_clean),
+// photometry/FLAGS (endobject_gpu), catalogue.  All stages run on one CUDA
+// stream; the host reads back four counts per frame to size launches.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "sexgpu.h"
+#include "common.cuh"
+#include "kernels.cuh"
+#include "prim.cuh"
+
+#include "prim.cu"
+#include "k_back.cu"
+#include "k_detect.cu"
+#include "k_roots.cu"
+#include "k_deblend.cu"
+#include "k_analyse.cu"
+#include "k_post.cu"
+
+using namespace sx;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+struct StageRec {
+    const char *name;
+    int launches;
+    cudaEvent_t ev;
+};
+
+}  // namespace
+
+struct sexgpu_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<DevBuf *> bufs;
+    std::string err;
+    // frame-size buffers
+    DevBuf img, sub, cd, lab, cnt, flag, pos, alloc, seg, pos2idx, var;
+    // scan / sort scratch
+    DevBuf scan_tmp, keys, vals, kalt, valt;
+    // background
+    DevBuf ms, back, sigma, back2, back3, sigma3, dback, bu, rownode, rowdnode, rowu, colk, coldx;
+    // roots
+    DevBuf rsize, roff, rfirst, rymax, rlastx, rfdpeak, rfdflux, rnkept, robjbase;
+    // deblend scratch
+    DevBuf dpar, dlev, dsz, dorder, drl0, drl1, dnid0, dnid1, dacc, nr0, nr1, nf0, nf1, ns0, ns1, nc0, nc1, na0, na1,
+        dkept, down, dkl, dkidx, dpacc, dpint, objkey, rpix;
+    // objects
+    DevBuf o_i[20], o_f[30], o_d[10], o_iso, o_sortkey, amp, alpha, cellhead, cellnext, vkey, vval, vkalt, vvalt,
+        skeys, svals, skalt, svalt, rows;
+    DevBuf sc;
+    FrameScalars hsc;
+    ObjBufs O;
+    std::vector<int> colk_h;
+    std::vector<float> coldx_h;
+    int last_w = 0, last_h = 0, last_nobj = 0, last_ns = 0;
+    std::vector<StageRec> stages;
+    cudaEvent_t ev0 = nullptr;
+    std::vector<float> stage_ms;
+    std::vector<std::string> stage_names;
+    std::vector<int> stage_launches;
+};
+
+namespace {
+
+int set_err(sexgpu_ctx *c, cudaError_t e, const char *what) {
+    c->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return SEXGPU_ERR_CUDA;
+}
+
+#define CK(call)                                               \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return set_err(ctx, _e, #call); \
+    } while (0)
+
+int ensure(sexgpu_ctx *ctx, DevBuf &b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.bytes >= bytes) return SEXGPU_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    size_t want = bytes + bytes / 8;
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ctx->err = "device allocation failed";
+        return SEXGPU_ERR_NOMEM;
+    }
+    b.bytes = want;
+    return SEXGPU_OK;
+}
+
+#define EN(buf, bytes)                                 \
+    do {                                               \
+        int _r = ensure(ctx, ctx->buf, (size_t)(bytes)); \
+        if (_r) return _r;                             \
+    } while (0)
+
+template <class T> T *P(DevBuf &b) { return (T *)b.p; }
+
+void stage_begin(sexgpu_ctx *ctx) {
+    ctx->stage_names.clear();
+    ctx->stage_launches.clear();
+    for (auto &s : ctx->stages) cudaEventDestroy(s.ev);
+    ctx->stages.clear();
+    if (!ctx->ev0) cudaEventCreate(&ctx->ev0);
+    cudaEventRecord(ctx->ev0, ctx->stream);
+}
+
+void stage_mark(sexgpu_ctx *ctx, const char *name, int launches) {
+    StageRec s;
+    s.name = name;
+    s.launches = launches;
+    cudaEventCreate(&s.ev);
+    cudaEventRecord(s.ev, ctx->stream);
+    ctx->stages.push_back(s);
+}
+
+void stage_collect(sexgpu_ctx *ctx) {
+    ctx->stage_ms.clear();
+    ctx->stage_names.clear();
+    ctx->stage_launches.clear();
+    cudaEvent_t prev = ctx->ev0;
+    for (auto &s : ctx->stages) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, prev, s.ev);
+        ctx->stage_ms.push_back(ms);
+        ctx->stage_names.push_back(s.name);
+        ctx->stage_launches.push_back(s.launches);
+        prev = s.ev;
+    }
+}
+
+// x-interpolation table of src/back.c:863-899 (segment index and dx of
+// every column), the same float arithmetic as the reference's loop
+void column_table(int width, int nbx, int backw, std::vector<int> &colk, std::vector<float> &coldx) {
+    colk.assign(width, 0);
+    coldx.assign(width, 0.f);
+    if (nbx <= 1) return;
+    int nx = backw, changepoint = nx / 2, x = 0, i = 0, k = 0;
+    float xstep = 1.0 / nx;
+    float dx = (xstep - 1) / 2;
+    float dx0 = ((nx + 1) % 2) * xstep / 2;
+    for (int j = 0; j < width; j++, i++, dx += xstep) {
+        if (i == changepoint && x > 0 && x < nbx - 1) {
+            k++;
+            dx = dx0;
+        }
+        colk[j] = k;
+        coldx[j] = dx;
+        if (i == nx) {
+            x++;
+            i = 0;
+        }
+    }
+}
+
+int check_config(const sexgpu_config *cfg, int w, int h) {
+    if (!cfg || w <= 0 || h <= 0) return SEXGPU_ERR_ARG;
+    if ((long long)w * h >= (1ll << 31)) return SEXGPU_ERR_ARG;
+    if (cfg->back_size < 1 || cfg->back_filtersize < 1 || cfg->back_filtersize > 11) return SEXGPU_ERR_ARG;
+    if (cfg->filter_flag && (!cfg->conv || cfg->conv_w < 1 || cfg->conv_h < 1 || cfg->conv_w > SX_MAXCONV ||
+                             cfg->conv_h > SX_MAXCONV))
+        return SEXGPU_ERR_ARG;
+    if (cfg->detect_minarea < 1 || cfg->deblend_nthresh < 1 || cfg->deblend_nthresh > 64) return SEXGPU_ERR_ARG;
+    if (cfg->weight_type != 0) return SEXGPU_ERR_ARG;
+    return SEXGPU_OK;
+}
+
+void make_params(const sexgpu_config *cfg, int w, int h, FrameParams &P) {
+    memset(&P, 0, sizeof(P));
+    P.w = w;
+    P.h = h;
+    P.bw = cfg->back_size < w ? cfg->back_size : w;
+    P.bh = cfg->back_size < h ? cfg->back_size : h;
+    P.nbx = (w - 1) / P.bw + 1;
+    P.nby = (h - 1) / P.bh + 1;
+    P.nfx = P.nbx > 1 ? cfg->back_filtersize : 1;
+    P.nfy = P.nby > 1 ? cfg->back_filtersize : 1;
+    P.fthresh = (float)cfg->back_filtthresh;
+    P.back_type = cfg->back_type;
+    P.back_value = (float)cfg->back_value;
+    P.thresh_type = cfg->thresh_type;
+    P.detect_thresh = cfg->detect_thresh;
+    P.analysis_thresh = cfg->analysis_thresh;
+    P.filter_flag = cfg->filter_flag;
+    P.conv_w = cfg->conv_w;
+    P.conv_h = cfg->conv_h;
+    P.minarea = cfg->detect_minarea;
+    P.debminarea = cfg->detect_minarea < SX_MAXDEBAREA ? cfg->detect_minarea : SX_MAXDEBAREA;
+    P.nthresh = cfg->deblend_nthresh;
+    P.mincont = cfg->deblend_mincont;
+    P.clean_flag = cfg->clean_flag;
+    P.clean_param = cfg->clean_param;
+    P.satur_level = cfg->satur_level;
+    P.gain = cfg->gain;
+    P.mag_zeropoint = cfg->mag_zeropoint;
+    P.aperture = cfg->phot_aperture;
+    P.autoparam0 = cfg->phot_autoparams[0];
+    P.autoparam1 = cfg->phot_autoparams[1];
+    P.mask_type = cfg->mask_type;
+    P.numbering = cfg->numbering;
+}
+
+__global__ void k_init_scalars(FrameScalars *sc) {
+    FrameScalars z;
+    memset(&z, 0, sizeof(z));
+    z.e0sub = 1000;
+    *sc = z;
+}
+
+__global__ void k_alloc_init(const int *lab, int *alloc, long long n) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) alloc[p] = lab[p] >= 0 ? SX_ALLOC_OTHER : -1;
+}
+
+int read_scalars(sexgpu_ctx *ctx) {
+    CK(cudaMemcpyAsync(&ctx->hsc, ctx->sc.p, sizeof(FrameScalars), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->hsc.status & SX_ST_LOOP) {
+        ctx->err = "device loop iteration cap reached";
+        return SEXGPU_ERR_LOOP;
+    }
+    if (ctx->hsc.status & SX_ST_RANGE) {
+        ctx->err = "exact sum out of range";
+        return SEXGPU_ERR_RANGE;
+    }
+    return SEXGPU_OK;
+}
+
+int alloc_objects(sexgpu_ctx *ctx, int nobj) {
+    size_t n = (size_t)nobj + 1;
+    int *ip[20];
+    float *fp[30];
+    double *dp[10];
+    for (int i = 0; i < 20; i++) {
+        EN(o_i[i], n * sizeof(int));
+        ip[i] = P<int>(ctx->o_i[i]);
+    }
+    for (int i = 0; i < 30; i++) {
+        EN(o_f[i], n * sizeof(float));
+        fp[i] = P<float>(ctx->o_f[i]);
+    }
+    for (int i = 0; i < 10; i++) {
+        EN(o_d[i], n * sizeof(double));
+        dp[i] = P<double>(ctx->o_d[i]);
+    }
+    EN(o_iso, n * SX_NISO_ * sizeof(int));
+    ObjBufs &O = ctx->O;
+    O.root = ip[0];
+    O.level = ip[1];
+    O.n = ip[2];
+    O.off = ip[3];
+    O.xmin = ip[4];
+    O.xmax = ip[5];
+    O.ymin = ip[6];
+    O.ymax = ip[7];
+    O.dnpix = ip[8];
+    O.flags = ip[9];
+    O.singu = ip[10];
+    O.npix = ip[11];
+    O.peakx = ip[12];
+    O.peaky = ip[13];
+    O.master = ip[14];
+    O.fmaster = ip[15];
+    O.number = ip[16];
+    O.fdnpix = ip[17];
+    O.fdflux = fp[0];
+    O.dflux = fp[1];
+    O.fdpeak = fp[2];
+    O.dpeak = fp[3];
+    O.node_dthresh = fp[4];
+    O.a = fp[5];
+    O.b = fp[6];
+    O.theta = fp[7];
+    O.abcor = fp[8];
+    O.cxx = fp[9];
+    O.cyy = fp[10];
+    O.cxy = fp[11];
+    O.flux = fp[12];
+    O.fluxerr = fp[13];
+    O.peak = fp[14];
+    O.bkg = fp[15];
+    O.mthresh = fp[16];
+    O.fwhm = fp[17];
+    O.flux_isocor = fp[18];
+    O.fluxerr_isocor = fp[19];
+    O.flux_aper = fp[20];
+    O.fluxerr_aper = fp[21];
+    O.mag_aper = fp[22];
+    O.magerr_aper = fp[23];
+    O.kron = fp[24];
+    O.flux_auto = fp[25];
+    O.fluxerr_auto = fp[26];
+    O.mag_auto = fp[27];
+    O.magerr_auto = fp[28];
+    O.mag_iso = fp[29];
+    O.mx = dp[0];
+    O.my = dp[1];
+    O.mx2 = dp[2];
+    O.my2 = dp[3];
+    O.mxy = dp[4];
+    O.pmx2 = dp[5];
+    O.pmy2 = dp[6];
+    O.pmxy = dp[7];
+    O.iso = P<int>(ctx->o_iso);
+    EN(o_d[8], n * sizeof(float));   // magerr_iso
+    EN(o_d[9], n * sizeof(float));   // fluxerr_iso
+    O.magerr_iso = P<float>(ctx->o_d[8]);
+    O.fluxerr_iso = P<float>(ctx->o_d[9]);
+    return SEXGPU_OK;
+}
+
+unsigned grid1(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// the whole pipeline on a device-resident frame
+int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu_config *cfg) {
+    int rc = check_config(cfg, w, h);
+    if (rc) {
+        ctx->err = "invalid configuration or frame size";
+        return rc;
+    }
+    cudaStream_t st = ctx->stream;
+    FrameParams Pm;
+    make_params(cfg, w, h, Pm);
+    const long long N = (long long)w * h;
+    const int nb = Pm.nbx * Pm.nby;
+    // ---- buffers sized by the frame
+    EN(sub, N * 4);
+    EN(cd, N * 4);
+    EN(lab, N * 4);
+    EN(cnt, N * 4);
+    EN(flag, N * 4);
+    EN(pos, N * 4);
+    EN(alloc, N * 4);
+    EN(pos2idx, N * 4);
+    EN(keys, N * 4);
+    EN(vals, N * 4);
+    EN(kalt, N * 4);
+    EN(valt, N * 4);
+    EN(rpix, N * 4);
+    EN(objkey, N * 4);
+    EN(scan_tmp, (std::max(scan_temp_ints(N), radix_temp_ints(N)) + 64) * 4);
+    EN(ms, nb * sizeof(MeshStat));
+    EN(back, nb * 4);
+    EN(sigma, nb * 4);
+    EN(back2, nb * 4);
+    EN(back3, nb * 4);
+    EN(sigma3, nb * 4);
+    EN(dback, nb * 4);
+    EN(bu, (size_t)nb * 4 + 64);
+    EN(rownode, (size_t)h * Pm.nbx * 4);
+    EN(rowdnode, (size_t)h * Pm.nbx * 4);
+    EN(rowu, (size_t)h * Pm.nbx * 4);
+    EN(colk, w * 4);
+    EN(coldx, w * 4);
+    EN(sc, sizeof(FrameScalars));
+    BackBufs B;
+    B.ms = P<MeshStat>(ctx->ms);
+    B.back = P<float>(ctx->back);
+    B.sigma = P<float>(ctx->sigma);
+    B.back2 = P<float>(ctx->back2);
+    B.back3 = P<float>(ctx->back3);
+    B.sigma3 = P<float>(ctx->sigma3);
+    B.dback = P<float>(ctx->dback);
+    B.u = P<float>(ctx->bu);
+    B.rownode = P<float>(ctx->rownode);
+    B.rowdnode = P<float>(ctx->rowdnode);
+    B.rowu = P<float>(ctx->rowu);
+    B.colk = P<int>(ctx->colk);
+    B.coldx = P<float>(ctx->coldx);
+    FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
+    int *tmp = P<int>(ctx->scan_tmp);
+
+    column_table(w, Pm.nbx, Pm.bw, ctx->colk_h, ctx->coldx_h);
+    CK(cudaMemcpyAsync(B.colk, ctx->colk_h.data(), w * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(B.coldx, ctx->coldx_h.data(), w * 4, cudaMemcpyHostToDevice, st));
+    static const float one = 1.0f;
+    if (cfg->filter_flag)
+        set_conv_mask(cfg->conv, cfg->conv_w, cfg->conv_h, st);
+    else
+        set_conv_mask(&one, 1, 1, st);
+
+    stage_begin(ctx);
+    int nl = 0;
+    k_init_scalars<<<1, 1, 0, st>>>(d_sc);
+    launch_background(B, d_img, Pm, d_sc, st, nl);
+    stage_mark(ctx, "background", nl + 1);
+
+    nl = 0;
+    launch_sub_filter(d_img, P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm, d_sc, nullptr, st, nl);
+    stage_mark(ctx, "sub_filter", nl);
+
+    nl = 0;
+    launch_ccl(P<int>(ctx->lab), Pm, d_sc, st, nl);
+    stage_mark(ctx, "ccl", nl);
+
+    // ---- raw objects
+    int *lab = P<int>(ctx->lab), *cnt = P<int>(ctx->cnt), *flag = P<int>(ctx->flag), *pos = P<int>(ctx->pos);
+    CK(cudaMemsetAsync(cnt, 0, N * 4, st));
+    k_count_labels<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, N);
+    k_root_flags<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, flag, N, Pm.minarea);
+    int *d_tot = &d_sc->nroots;
+    exclusive_scan(flag, flag, N, d_tot, tmp, st);  // flag -> root id
+    rc = read_scalars(ctx);
+    if (rc) return rc;
+    if (ctx->hsc.dthresh <= 0.0f || ctx->hsc.thresh <= 0.0f) {
+        ctx->err = "zero or negative threshold";
+        return SEXGPU_ERR_THRESH;
+    }
+    const int nroots = ctx->hsc.nroots;
+    EN(rsize, (nroots + 1) * 4);
+    EN(roff, (nroots + 1) * 4);
+    EN(rfirst, (nroots + 1) * 4);
+    EN(rymax, (nroots + 1) * 4);
+    EN(rlastx, (nroots + 1) * 4);
+    EN(rfdpeak, (nroots + 1) * 4);
+    EN(rfdflux, (nroots + 1) * 4);
+    EN(rnkept, (nroots + 1) * 4);
+    EN(robjbase, (nroots + 1) * 4);
+    RootBufs R;
+    R.size = P<int>(ctx->rsize);
+    R.off = P<int>(ctx->roff);
+    R.first = P<int>(ctx->rfirst);
+    R.ymax = P<int>(ctx->rymax);
+    R.lastx = P<int>(ctx->rlastx);
+    R.fdpeak = P<float>(ctx->rfdpeak);
+    R.fdflux = P<float>(ctx->rfdflux);
+    R.nkept = P<int>(ctx->rnkept);
+    R.objbase = P<int>(ctx->robjbase);
+    k_root_setup<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, flag, R.size, R.first, N, Pm.minarea);
+    exclusive_scan(R.size, R.off, nroots, &d_sc->nrootpix, tmp, st);
+    k_pix_flags<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, pos, N, Pm.minarea);
+    exclusive_scan(pos, pos, N, nullptr, tmp, st);
+    unsigned *keys = P<unsigned>(ctx->keys), *vals = P<unsigned>(ctx->vals);
+    k_pix_compact<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, flag, pos, keys, vals, N, Pm.minarea);
+    rc = read_scalars(ctx);
+    if (rc) return rc;
+    const int nrootpix = ctx->hsc.nrootpix;
+    radix_sort_pairs(keys, vals, P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), nrootpix, bits_for(nroots), tmp, st);
+    unsigned *rpix = P<unsigned>(ctx->rpix);
+    CK(cudaMemcpyAsync(rpix, vals, (size_t)nrootpix * 4, cudaMemcpyDeviceToDevice, st));
+    int *pos2idx = P<int>(ctx->pos2idx);
+    CK(cudaMemsetAsync(pos2idx, 0xff, N * 4, st));
+    k_pos2idx<<<grid1(nrootpix, 256), 256, 0, st>>>(rpix, pos2idx, nrootpix);
+    k_alloc_init<<<grid1(N, 256), 256, 0, st>>>(lab, P<int>(ctx->alloc), N);
+    stage_mark(ctx, "roots", 8 + 3 * scan_launches(N) + scan_launches(nroots) + radix_launches(bits_for(nroots), nrootpix));
+
+    // ---- deblending
+    size_t M = (size_t)nrootpix + 1;
+    EN(dpar, M * 4);
+    EN(dlev, M * 4);
+    EN(dsz, M * 4);
+    EN(dorder, M * 4);
+    EN(drl0, M * 4);
+    EN(drl1, M * 4);
+    EN(dnid0, M * 4);
+    EN(dnid1, M * 4);
+    EN(dacc, M * 32);
+    EN(nr0, M * 4);
+    EN(nr1, M * 4);
+    EN(nf0, M * 4);
+    EN(nf1, M * 4);
+    EN(ns0, M * 4);
+    EN(ns1, M * 4);
+    EN(nc0, M * 4);
+    EN(nc1, M * 4);
+    EN(na0, M * 4);
+    EN(na1, M * 4);
+    EN(dkept, M * 8);
+    EN(down, M * 4);
+    EN(dkl, M * 4);
+    EN(dkidx, M * 4);
+    EN(dpacc, M * 28 * 8);
+    EN(dpint, M * 8 * 4);
+    DebArgs A;
+    A.cd = P<float>(ctx->cd);
+    A.sub = P<float>(ctx->sub);
+    A.pos2idx = pos2idx;
+    A.rpix = rpix;
+    A.R = R;
+    DebBufs &D = A.D;
+    D.par = P<int>(ctx->dpar);
+    D.lev = P<int>(ctx->dlev);
+    D.sz = P<int>(ctx->dsz);
+    D.order = P<int>(ctx->dorder);
+    D.rl0 = P<int>(ctx->drl0);
+    D.rl1 = P<int>(ctx->drl1);
+    D.nid0 = P<int>(ctx->dnid0);
+    D.nid1 = P<int>(ctx->dnid1);
+    D.acc = P<unsigned long long>(ctx->dacc);
+    D.nd_root0 = P<int>(ctx->nr0);
+    D.nd_root1 = P<int>(ctx->nr1);
+    D.nd_flag0 = P<int>(ctx->nf0);
+    D.nd_flag1 = P<int>(ctx->nf1);
+    D.nd_nson0 = P<int>(ctx->ns0);
+    D.nd_nson1 = P<int>(ctx->ns1);
+    D.nd_okc0 = P<int>(ctx->nc0);
+    D.nd_okc1 = P<int>(ctx->nc1);
+    D.nd_oka0 = P<int>(ctx->na0);
+    D.nd_oka1 = P<int>(ctx->na1);
+    D.kept = P<unsigned long long>(ctx->dkept);
+    D.own = P<int>(ctx->down);
+    D.kl = P<int>(ctx->dkl);
+    D.kidx = P<int>(ctx->dkidx);
+    D.pacc = P<unsigned long long>(ctx->dpacc);
+    D.pint = P<int>(ctx->dpint);
+    A.sc = d_sc;
+    A.alloc = P<int>(ctx->alloc);
+    A.objkey = P<unsigned>(ctx->objkey);
+    A.w = w;
+    A.h = h;
+    A.N = Pm.nthresh;
+    A.debminarea = Pm.debminarea;
+    A.mincont = Pm.mincont;
+    launch_deblend_sweep(A, nroots, st);
+    exclusive_scan(R.nkept, R.objbase, nroots, &d_sc->nobj, tmp, st);
+    rc = read_scalars(ctx);
+    if (rc) return rc;
+    const int nobj = ctx->hsc.nobj;
+    rc = alloc_objects(ctx, nobj);
+    if (rc) return rc;
+    A.O = ctx->O;
+    launch_deblend_assign(A, nroots, st);
+    stage_mark(ctx, "deblend", 2 + scan_launches(nroots));
+
+    // ---- object pixel lists (stable by object id: raster order inside)
+    ObjBufs &O = ctx->O;
+    CK(cudaMemcpyAsync(keys, A.objkey, (size_t)nrootpix * 4, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(vals, rpix, (size_t)nrootpix * 4, cudaMemcpyDeviceToDevice, st));
+    radix_sort_pairs(keys, vals, P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), nrootpix, bits_for(nobj), tmp, st);
+    exclusive_scan(O.n, O.off, nobj, nullptr, tmp, st);
+    AnaArgs AA;
+    AA.cd = A.cd;
+    AA.sub = A.sub;
+    AA.back = B.back3;
+    AA.opix = vals;
+    AA.O = O;
+    AA.sc = d_sc;
+    AA.w = w;
+    AA.h = h;
+    AA.nbx = Pm.nbx;
+    AA.nby = Pm.nby;
+    AA.bw = Pm.bw;
+    AA.bh = Pm.bh;
+    AA.nobj = nobj;
+    AA.minarea = Pm.minarea;
+    AA.clean_flag = Pm.clean_flag;
+    AA.gain = Pm.gain;
+    AA.satur = Pm.satur_level;
+    launch_analyse(AA, st);
+    stage_mark(ctx, "analyse", 1 + radix_launches(bits_for(nobj), nrootpix) + scan_launches(nobj));
+
+    // ---- CLEAN
+    int nv = 0;
+    int cl_launch = 0;
+    if (Pm.clean_flag && nobj > 0) {
+        int gx = (int)(w / CL_CELL) + 2, gy = (int)(h / CL_CELL) + 2;
+        EN(amp, (size_t)(nobj + 1) * 8);
+        EN(alpha, (size_t)(nobj + 1) * 8);
+        EN(cellhead, (size_t)gx * gy * 4);
+        EN(cellnext, (size_t)(nobj + 1) * 4);
+        EN(vkey, (size_t)(nobj + 1) * 4);
+        EN(vval, (size_t)(nobj + 1) * 4);
+        EN(vkalt, (size_t)(nobj + 1) * 4);
+        EN(vvalt, (size_t)(nobj + 1) * 4);
+        CK(cudaMemsetAsync(ctx->cellhead.p, 0xff, (size_t)gx * gy * 4, st));
+        k_clean_prep<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, ctx->hsc.dthresh, Pm.clean_param, P<double>(ctx->amp),
+                                                       P<double>(ctx->alpha), P<int>(ctx->cellhead),
+                                                       P<int>(ctx->cellnext), gx, gy);
+        k_clean_pairs<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, Pm.clean_param, P<double>(ctx->amp),
+                                                        P<double>(ctx->alpha), P<int>(ctx->cellhead),
+                                                        P<int>(ctx->cellnext), gx, gy);
+        CK(cudaMemsetAsync(&d_sc->nsurv, 0, 4, st));
+        k_clean_chain<<<grid1(nobj, 256), 256, 0, st>>>(O, nobj, P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval),
+                                                        &d_sc->nsurv);
+        rc = read_scalars(ctx);
+        if (rc) return rc;
+        nv = ctx->hsc.nsurv;
+        radix_sort_pairs(P<unsigned>(ctx->vval), P<unsigned>(ctx->vkey), P<unsigned>(ctx->vkalt),
+                         P<unsigned>(ctx->vvalt), nv, bits_for(nobj), tmp, st);  // victims by index
+        radix_sort_pairs(P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval), P<unsigned>(ctx->vkalt),
+                         P<unsigned>(ctx->vvalt), nv, bits_for(nobj), tmp, st);  // then by master
+        if (nv > 0) {
+            k_clean_merge<<<grid1(nv, 128), 128, 0, st>>>(O, P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval), nv);
+            k_alloc_victims<<<nobj, 128, 0, st>>>(O, vals, A.alloc, nobj);
+        }
+        cl_launch = 5 + 2 * radix_launches(bits_for(nobj), nv);
+    } else if (nobj > 0) {
+        CK(cudaMemsetAsync(O.fmaster, 0xff, (size_t)nobj * 4, st));
+    }
+    stage_mark(ctx, "clean", cl_launch);
+
+    // ---- photometry / FLAGS
+    EndArgs E;
+    E.sub = A.sub;
+    E.alloc = A.alloc;
+    E.O = O;
+    E.sc = d_sc;
+    E.w = w;
+    E.h = h;
+    E.n = nobj;
+    E.mask_type = Pm.mask_type;
+    E.aperture = Pm.aperture;
+    E.autoparam0 = Pm.autoparam0;
+    E.autoparam1 = Pm.autoparam1;
+    E.gain = Pm.gain;
+    E.zp = Pm.mag_zeropoint;
+    E.satur = Pm.satur_level;
+    if (nobj > 0) k_endobject<<<grid1(nobj, 4), 128, 0, st>>>(E);
+    stage_mark(ctx, "endobject", nobj > 0);
+
+    // ---- catalogue order
+    EN(skeys, (size_t)(nobj + 1) * 4);
+    EN(svals, (size_t)(nobj + 1) * 4);
+    EN(skalt, (size_t)(nobj + 1) * 4);
+    EN(svalt, (size_t)(nobj + 1) * 4);
+    int *sflag = P<int>(ctx->cnt);  // free now
+    CK(cudaMemsetAsync(O.number, 0, (size_t)(nobj + 1) * 4, st));
+    k_surv_flags<<<grid1(nobj + 1, 256), 256, 0, st>>>(O, nobj, sflag);
+    exclusive_scan(sflag, sflag, nobj, &d_sc->nsurv, tmp, st);
+    rc = read_scalars(ctx);
+    if (rc) return rc;
+    const int ns = ctx->hsc.nsurv;
+    k_surv_compact<<<grid1(nobj + 1, 256), 256, 0, st>>>(O, R.ymax, R.lastx, sflag, nobj, w, Pm.numbering,
+                                                         P<unsigned>(ctx->skeys), P<unsigned>(ctx->svals));
+    radix_sort_pairs(P<unsigned>(ctx->skeys), P<unsigned>(ctx->svals), P<unsigned>(ctx->skalt),
+                     P<unsigned>(ctx->svalt), ns, bits_for((long long)w * h), tmp, st);
+    k_number<<<grid1(ns + 1, 256), 256, 0, st>>>(O, P<unsigned>(ctx->svals), ns);
+    EN(rows, (size_t)(ns + 1) * sizeof(sexgpu_object));
+    k_write_rows<<<grid1(ns + 1, 128), 128, 0, st>>>(O, P<unsigned>(ctx->svals), ns, ctx->hsc.dthresh,
+                                                     ctx->hsc.thresh, P<sexgpu_object>(ctx->rows));
+    stage_mark(ctx, "catalog", 5 + scan_launches(nobj) + radix_launches(bits_for((long long)w * h), ns));
+    CK(cudaGetLastError());
+    rc = read_scalars(ctx);
+    if (rc) return rc;
+    stage_collect(ctx);
+    ctx->last_w = w;
+    ctx->last_h = h;
+    ctx->last_nobj = nobj;
+    ctx->last_ns = ns;
+    return SEXGPU_OK;
+}
+
+void fill_summary(sexgpu_ctx *ctx, const FrameParams &P, sexgpu_summary *s) {
+    if (!s) return;
+    memset(s, 0, sizeof(*s));
+    s->nbackx = P.nbx;
+    s->nbacky = P.nby;
+    s->backmean = ctx->hsc.backmean;
+    s->backsig = ctx->hsc.backsig;
+    s->dthresh = ctx->hsc.dthresh;
+    s->thresh = ctx->hsc.thresh;
+    s->npix_above = ctx->hsc.npix_above;
+    s->nraw = ctx->hsc.nroots;
+    s->nraw_pix = ctx->hsc.nrootpix;
+    s->ndetected = ctx->last_nobj;
+    s->nobj = ctx->last_ns;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int sexgpu_create(sexgpu_ctx **out, int device) {
+    if (!out) return SEXGPU_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0 || device < 0 || device >= n) {
+        cudaGetLastError();
+        return SEXGPU_ERR_NODEVICE;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return SEXGPU_ERR_NODEVICE;
+    sexgpu_ctx *ctx = new sexgpu_ctx();
+    ctx->device = device;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return SEXGPU_ERR_CUDA;
+    }
+    ctx->own_stream = true;
+    *out = ctx;
+    return SEXGPU_OK;
+}
+
+static void free_buf(DevBuf &b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+int sexgpu_destroy(sexgpu_ctx *ctx) {
+    if (!ctx) return SEXGPU_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    DevBuf *all[] = {&ctx->img, &ctx->sub, &ctx->cd, &ctx->lab, &ctx->cnt, &ctx->flag, &ctx->pos, &ctx->alloc,
+                     &ctx->seg, &ctx->pos2idx, &ctx->var, &ctx->scan_tmp, &ctx->keys, &ctx->vals, &ctx->kalt,
+                     &ctx->valt, &ctx->ms, &ctx->back, &ctx->sigma, &ctx->back2, &ctx->back3, &ctx->sigma3,
+                     &ctx->dback, &ctx->bu, &ctx->rownode, &ctx->rowdnode, &ctx->rowu, &ctx->colk, &ctx->coldx,
+                     &ctx->rsize, &ctx->roff, &ctx->rfirst, &ctx->rymax, &ctx->rlastx, &ctx->rfdpeak,
+                     &ctx->rfdflux, &ctx->rnkept, &ctx->robjbase, &ctx->dpar, &ctx->dlev, &ctx->dsz, &ctx->dorder,
+                     &ctx->drl0, &ctx->drl1, &ctx->dnid0, &ctx->dnid1, &ctx->dacc, &ctx->nr0, &ctx->nr1,
+                     &ctx->nf0, &ctx->nf1, &ctx->ns0, &ctx->ns1, &ctx->nc0, &ctx->nc1, &ctx->na0, &ctx->na1,
+                     &ctx->dkept, &ctx->down, &ctx->dkl, &ctx->dkidx, &ctx->dpacc, &ctx->dpint, &ctx->objkey,
+                     &ctx->rpix, &ctx->o_iso, &ctx->o_sortkey, &ctx->amp, &ctx->alpha, &ctx->cellhead,
+                     &ctx->cellnext, &ctx->vkey, &ctx->vval, &ctx->vkalt, &ctx->vvalt, &ctx->skeys, &ctx->svals,
+                     &ctx->skalt, &ctx->svalt, &ctx->rows, &ctx->sc};
+    for (DevBuf *b : all) free_buf(*b);
+    for (auto &b : ctx->o_i) free_buf(b);
+    for (auto &b : ctx->o_f) free_buf(b);
+    for (auto &b : ctx->o_d) free_buf(b);
+    for (auto &s : ctx->stages) cudaEventDestroy(s.ev);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return SEXGPU_OK;
+}
+
+int sexgpu_set_stream(sexgpu_ctx *ctx, void *stream) {
+    if (!ctx) return SEXGPU_ERR_ARG;
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (stream) {
+        ctx->stream = (cudaStream_t)stream;
+        ctx->own_stream = false;
+    } else {
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+        ctx->own_stream = true;
+    }
+    return SEXGPU_OK;
+}
+
+void sexgpu_default_config(sexgpu_config *c) {
+    static const float pyramid[9] = {1 / 16.f, 2 / 16.f, 1 / 16.f, 2 / 16.f, 4 / 16.f, 2 / 16.f, 1 / 16.f, 2 / 16.f, 1 / 16.f};
+    memset(c, 0, sizeof(*c));
+    c->back_size = 64;
+    c->back_filtersize = 3;
+    c->back_filtthresh = 0.0;
+    c->back_type = 0;
+    c->thresh_type = 0;
+    c->detect_thresh = 1.5;
+    c->analysis_thresh = 1.5;
+    c->filter_flag = 1;
+    c->conv_w = c->conv_h = 3;
+    c->conv = pyramid;
+    c->detect_minarea = 5;
+    c->deblend_nthresh = 32;
+    c->deblend_mincont = 0.005;
+    c->clean_flag = 1;
+    c->clean_param = 1.0;
+    c->satur_level = 50000.0;
+    c->gain = 0.0;
+    c->mag_zeropoint = 0.0;
+    c->phot_aperture = 5.0;
+    c->phot_autoparams[0] = 2.5;
+    c->phot_autoparams[1] = 3.5;
+    c->mask_type = 2;
+    c->weight_type = 0;
+    c->numbering = 0;
+}
+
+const char *sexgpu_last_error(sexgpu_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int sexgpu_extract_device(sexgpu_ctx *ctx, const float *d_img, const float *d_var, int w, int h,
+                          const sexgpu_config *cfg, sexgpu_summary *sum) {
+    if (!ctx || !d_img) return SEXGPU_ERR_ARG;
+    if (d_var) return SEXGPU_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    ctx->err.clear();
+    int rc = run_pipeline(ctx, d_img, w, h, cfg);
+    if (rc == SEXGPU_OK && sum) {
+        FrameParams Pm;
+        make_params(cfg, w, h, Pm);
+        fill_summary(ctx, Pm, sum);
+    }
+    return rc;
+}
+
+int sexgpu_copy_results(sexgpu_ctx *ctx, sexgpu_object *objs, int max_objects, int *nobj, int32_t *segmap,
+                        float *sub, float *cd) {
+    if (!ctx) return SEXGPU_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    long long N = (long long)ctx->last_w * ctx->last_h;
+    int ns = ctx->last_ns, rc = SEXGPU_OK;
+    if (nobj) *nobj = ns;
+    if (objs) {
+        int n = ns < max_objects ? ns : max_objects;
+        if (ns > max_objects) rc = SEXGPU_ERR_CAPACITY;
+        if (n > 0) CK(cudaMemcpyAsync(objs, ctx->rows.p, (size_t)n * sizeof(sexgpu_object), cudaMemcpyDeviceToHost, st));
+    }
+    if (segmap && N > 0) {
+        EN(seg, N * 4);
+        k_segmap<<<grid1(N, 256), 256, 0, st>>>(P<int>(ctx->alloc), ctx->O.number, P<int>(ctx->seg), N);
+        CK(cudaMemcpyAsync(segmap, ctx->seg.p, N * 4, cudaMemcpyDeviceToHost, st));
+    }
+    if (sub && N > 0) CK(cudaMemcpyAsync(sub, ctx->sub.p, N * 4, cudaMemcpyDeviceToHost, st));
+    if (cd && N > 0) CK(cudaMemcpyAsync(cd, ctx->cd.p, N * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return rc;
+}
+
+int sexgpu_extract(sexgpu_ctx *ctx, const float *img, const float *var, int w, int h, const sexgpu_config *cfg,
+                   sexgpu_object *objs, int max_objects, int *nobj, int32_t *segmap, float *sub, float *cd,
+                   sexgpu_summary *sum) {
+    if (!ctx || !img || w <= 0 || h <= 0) return SEXGPU_ERR_ARG;
+    if (var) return SEXGPU_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    long long N = (long long)w * h;
+    EN(img, N * 4);
+    CK(cudaMemcpyAsync(ctx->img.p, img, N * 4, cudaMemcpyHostToDevice, ctx->stream));
+    int rc = sexgpu_extract_device(ctx, P<float>(ctx->img), nullptr, w, h, cfg, sum);
+    if (rc) return rc;
+    return sexgpu_copy_results(ctx, objs, max_objects, nobj, segmap, sub, cd);
+}
+
+int sexgpu_background(sexgpu_ctx *ctx, float *img, int w, int h, const sexgpu_config *cfg, float *back,
+                      float *sigma, sexgpu_summary *sum) {
+    if (!ctx || !img || !cfg) return SEXGPU_ERR_ARG;
+    int rc = check_config(cfg, w, h);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    FrameParams Pm;
+    make_params(cfg, w, h, Pm);
+    Pm.filter_flag = 0;
+    long long N = (long long)w * h;
+    int nb = Pm.nbx * Pm.nby;
+    EN(img, N * 4);
+    EN(sub, N * 4);
+    EN(cd, N * 4);
+    EN(lab, N * 4);
+    EN(ms, nb * sizeof(MeshStat));
+    EN(back, nb * 4);
+    EN(sigma, nb * 4);
+    EN(back2, nb * 4);
+    EN(back3, nb * 4);
+    EN(sigma3, nb * 4);
+    EN(dback, nb * 4);
+    EN(bu, (size_t)nb * 4 + 64);
+    EN(rownode, (size_t)h * Pm.nbx * 4);
+    EN(rowdnode, (size_t)h * Pm.nbx * 4);
+    EN(rowu, (size_t)h * Pm.nbx * 4);
+    EN(colk, w * 4);
+    EN(coldx, w * 4);
+    EN(sc, sizeof(FrameScalars));
+    BackBufs B;
+    B.ms = P<MeshStat>(ctx->ms);
+    B.back = P<float>(ctx->back);
+    B.sigma = P<float>(ctx->sigma);
+    B.back2 = P<float>(ctx->back2);
+    B.back3 = P<float>(ctx->back3);
+    B.sigma3 = P<float>(ctx->sigma3);
+    B.dback = P<float>(ctx->dback);
+    B.u = P<float>(ctx->bu);
+    B.rownode = P<float>(ctx->rownode);
+    B.rowdnode = P<float>(ctx->rowdnode);
+    B.rowu = P<float>(ctx->rowu);
+    B.colk = P<int>(ctx->colk);
+    B.coldx = P<float>(ctx->coldx);
+    column_table(w, Pm.nbx, Pm.bw, ctx->colk_h, ctx->coldx_h);
+    CK(cudaMemcpyAsync(B.colk, ctx->colk_h.data(), w * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(B.coldx, ctx->coldx_h.data(), w * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->img.p, img, N * 4, cudaMemcpyHostToDevice, st));
+    static const float one = 1.0f;
+    set_conv_mask(&one, 1, 1, st);
+    FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
+    int nl = 0;
+    k_init_scalars<<<1, 1, 0, st>>>(d_sc);
+    launch_background(B, P<float>(ctx->img), Pm, d_sc, st, nl);
+    launch_sub_filter(P<float>(ctx->img), P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm, d_sc,
+                      nullptr, st, nl);
+    CK(cudaMemcpyAsync(img, ctx->sub.p, N * 4, cudaMemcpyDeviceToHost, st));
+    if (back) CK(cudaMemcpyAsync(back, B.back3, nb * 4, cudaMemcpyDeviceToHost, st));
+    if (sigma) CK(cudaMemcpyAsync(sigma, B.sigma3, nb * 4, cudaMemcpyDeviceToHost, st));
+    rc = read_scalars(ctx);
+    if (rc) return rc;
+    if (sum) {
+        ctx->last_nobj = ctx->last_ns = 0;
+        fill_summary(ctx, Pm, sum);
+    }
+    return SEXGPU_OK;
+}
+
+int sexgpu_filter(sexgpu_ctx *ctx, const float *sub, int w, int h, const float *mask, int mw, int mh, float *cd) {
+    if (!ctx || !sub || !mask || !cd || w <= 0 || h <= 0 || mw < 1 || mh < 1 || mw > SX_MAXCONV || mh > SX_MAXCONV)
+        return SEXGPU_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    long long N = (long long)w * h;
+    EN(img, N * 4);
+    EN(sub, N * 4);
+    EN(cd, N * 4);
+    EN(lab, N * 4);
+    EN(sc, sizeof(FrameScalars));
+    EN(rownode, 16);
+    EN(colk, 16);
+    EN(coldx, 16);
+    CK(cudaMemcpyAsync(ctx->img.p, sub, N * 4, cudaMemcpyHostToDevice, st));
+    set_conv_mask(mask, mw, mh, st);
+    FrameScalars z;
+    memset(&z, 0, sizeof(z));
+    z.backmean = 0.0f;
+    z.dthresh = 1e30f;
+    z.e0sub = 1000;
+    CK(cudaMemcpyAsync(ctx->sc.p, &z, sizeof(z), cudaMemcpyHostToDevice, st));
+    BackBufs B;
+    memset(&B, 0, sizeof(B));
+    B.rownode = P<float>(ctx->rownode);
+    B.colk = P<int>(ctx->colk);
+    B.coldx = P<float>(ctx->coldx);
+    FrameParams Pm;
+    memset(&Pm, 0, sizeof(Pm));
+    Pm.w = w;
+    Pm.h = h;
+    Pm.nbx = 1;
+    Pm.back_type = 1;
+    Pm.filter_flag = 1;
+    Pm.conv_w = mw;
+    Pm.conv_h = mh;
+    int nl = 0;
+    launch_sub_filter(P<float>(ctx->img), P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm,
+                      P<FrameScalars>(ctx->sc), nullptr, st, nl);
+    CK(cudaMemcpyAsync(cd, ctx->cd.p, N * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    return SEXGPU_OK;
+}
+
+// src/filter.c:101-185, restated: header line CONV [NORM|NONORM], rows of
+// numbers ('#' starts a comment line), L1 normalisation (variance
+// normalisation for zero-sum masks)
+int sexgpu_getconv(const char *path, float *mask, int maxn, int *mw, int *mh) {
+    if (!path || !mask || !mw || !mh) return SEXGPU_ERR_ARG;
+    FILE *f = fopen(path, "r");
+    if (!f) return SEXGPU_ERR_ARG;
+    char line[512];
+    if (!fgets(line, sizeof(line), f) || strncmp(line, "CONV", 4)) {
+        fclose(f);
+        return SEXGPU_ERR_ARG;
+    }
+    int normflag = strstr(line, "NORM") ? (strstr(line, "NONORM") ? 0 : 1) : 1;
+    int n = 0, width = 0;
+    while (fgets(line, sizeof(line), f)) {
+        int j = 0;
+        char *save = nullptr;
+        char *tok = strtok_r(line, " \t\n", &save);
+        if (!tok || tok[0] == '#') continue;
+        do {
+            if (n >= maxn) {
+                fclose(f);
+                return SEXGPU_ERR_CAPACITY;
+            }
+            mask[n++] = (float)atof(tok);
+            j++;
+        } while ((tok = strtok_r(nullptr, " \t\n", &save)));
+        if (j > width) width = j;
+    }
+    fclose(f);
+    if (width < 1 || n % width) return SEXGPU_ERR_ARG;
+    *mw = width;
+    *mh = n / width;
+    double sum = 0.0, var = 0.0;
+    for (int j = 0; j < n; j++) {
+        double pix = mask[j];
+        sum += fabs(pix);
+        var += pix * pix;
+    }
+    var = sqrt(var);
+    if (normflag) {
+        if (sum == 0.0) sum = var;
+        for (int j = 0; j < n; j++) mask[j] /= sum;
+    }
+    return n;
+}
+
+int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max) {
+    if (!ctx) return SEXGPU_ERR_ARG;
+    int n = (int)ctx->stage_ms.size();
+    for (int i = 0; i < n && i < max; i++) {
+        memset(&stages[i], 0, sizeof(stages[i]));
+        strncpy(stages[i].name, ctx->stage_names[i].c_str(), sizeof(stages[i].name) - 1);
+        stages[i].launches = ctx->stage_launches[i];
+        stages[i].ms = ctx->stage_ms[i];
+    }
+    return n;
+}
+
+}  // extern "C"

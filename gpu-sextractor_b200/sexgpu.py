@@ -1,0 +1,242 @@
+"""Python binding of libsexgpu (include/sexgpu.h) through ctypes.
+
+The library is the product: every call goes through its C ABI, there is no
+Python or CPU fallback.  If libsexgpu.so is missing or no CUDA device is
+present, the calls raise.
+
+Mirrors the reference's entry points (baoxuezhao/GPU-SExtractor):
+  background()  <- makeback()   src/back.c:43
+  filter()      <- cudaFilter() src/cuda/cudafilter.h:11
+  extract()     <- scanimage()  src/scan.c:65
+  getconv()     <- getconv()    src/filter.c:101
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libsexgpu.so")
+NISO = 8
+
+OK = 0
+ERRORS = {-1: "bad argument", -2: "CUDA error", -3: "out of device memory",
+          -4: "exact sum out of range", -5: "buffer too small", -6: "no CUDA device",
+          -7: "zero or negative threshold", -8: "device loop cap reached"}
+
+
+class Config(C.Structure):
+    """sexgpu_config; field names follow the .sex keywords."""
+    _fields_ = [
+        ("back_size", C.c_int), ("back_filtersize", C.c_int), ("back_filtthresh", C.c_double),
+        ("back_type", C.c_int), ("back_value", C.c_double),
+        ("thresh_type", C.c_int), ("detect_thresh", C.c_double), ("analysis_thresh", C.c_double),
+        ("filter_flag", C.c_int), ("conv_w", C.c_int), ("conv_h", C.c_int),
+        ("conv", C.POINTER(C.c_float)),
+        ("detect_minarea", C.c_int), ("deblend_nthresh", C.c_int), ("deblend_mincont", C.c_double),
+        ("clean_flag", C.c_int), ("clean_param", C.c_double),
+        ("satur_level", C.c_double), ("gain", C.c_double), ("mag_zeropoint", C.c_double),
+        ("phot_aperture", C.c_double), ("phot_autoparams", C.c_double * 2), ("mask_type", C.c_int),
+        ("weight_type", C.c_int), ("numbering", C.c_int),
+    ]
+
+
+OBJECT_FIELDS = [
+    ("number", "i4"), ("root", "i4"), ("level", "i4"), ("fdnpix", "i4"), ("dnpix", "i4"),
+    ("npix", "i4"), ("xmin", "i4"), ("xmax", "i4"), ("ymin", "i4"), ("ymax", "i4"),
+    ("peakx", "i4"), ("peaky", "i4"), ("flags", "i4"), ("iso", "i4", (NISO,)),
+    ("fdflux", "f4"), ("dflux", "f4"), ("flux", "f4"), ("fluxerr", "f4"), ("fdpeak", "f4"),
+    ("dpeak", "f4"), ("peak", "f4"),
+    ("mx", "f8"), ("my", "f8"), ("mx2", "f8"), ("my2", "f8"), ("mxy", "f8"),
+    ("a", "f4"), ("b", "f4"), ("theta", "f4"), ("abcor", "f4"), ("cxx", "f4"), ("cyy", "f4"),
+    ("cxy", "f4"),
+    ("poserr_mx2", "f8"), ("poserr_my2", "f8"), ("poserr_mxy", "f8"),
+    ("bkg", "f4"), ("thresh", "f4"), ("dthresh", "f4"), ("mthresh", "f4"), ("fwhm", "f4"),
+    ("flux_iso", "f4"), ("fluxerr_iso", "f4"), ("mag_iso", "f4"), ("magerr_iso", "f4"),
+    ("flux_isocor", "f4"), ("fluxerr_isocor", "f4"),
+    ("flux_aper", "f4"), ("fluxerr_aper", "f4"), ("mag_aper", "f4"), ("magerr_aper", "f4"),
+    ("kronfactor", "f4"), ("flux_auto", "f4"), ("fluxerr_auto", "f4"), ("mag_auto", "f4"),
+    ("magerr_auto", "f4"), ("elong", "f4"), ("ellip", "f4"), ("polar", "f4"),
+]
+OBJECT_DTYPE = np.dtype(OBJECT_FIELDS, align=True)
+
+
+class Summary(C.Structure):
+    _fields_ = [
+        ("nbackx", C.c_int), ("nbacky", C.c_int), ("backmean", C.c_float), ("backsig", C.c_float),
+        ("dthresh", C.c_float), ("thresh", C.c_float), ("npix_above", C.c_int64),
+        ("nraw", C.c_int32), ("nraw_pix", C.c_int64), ("ndetected", C.c_int32), ("nobj", C.c_int32),
+    ]
+
+
+class Stage(C.Structure):
+    _fields_ = [("name", C.c_char * 24), ("launches", C.c_int32), ("ms", C.c_float)]
+
+
+EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extract",
+           "sexgpu_extract_device", "sexgpu_copy_results", "sexgpu_background", "sexgpu_filter",
+           "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times"]
+
+_lib = None
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise RuntimeError("libsexgpu.so is not built (run make in %s)" % HERE)
+        _lib = C.CDLL(LIB)
+        _lib.sexgpu_last_error.restype = C.c_char_p
+        for name in EXPORTS:
+            getattr(_lib, name)
+    return _lib
+
+
+def _f(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _check(rc, ctx=None, what="sexgpu"):
+    if rc != OK:
+        msg = ERRORS.get(rc, str(rc))
+        if ctx is not None:
+            detail = lib().sexgpu_last_error(ctx)
+            if detail:
+                msg += " (%s)" % detail.decode()
+        raise RuntimeError("%s failed: %s" % (what, msg))
+
+
+DEFAULT_CONV = np.array([[1, 2, 1], [2, 4, 2], [1, 2, 1]], np.float32) / np.float32(16.0)
+
+
+def default_config():
+    return dict(back_size=64, back_filtersize=3, back_filtthresh=0.0, back_type=0, back_value=0.0,
+                thresh_type=0, detect_thresh=1.5, analysis_thresh=1.5, filter_flag=1,
+                conv=DEFAULT_CONV, detect_minarea=5, deblend_nthresh=32, deblend_mincont=0.005,
+                clean_flag=1, clean_param=1.0, satur_level=50000.0, gain=0.0, mag_zeropoint=0.0,
+                phot_aperture=5.0, phot_autoparams=(2.5, 3.5), mask_type=2, weight_type=0,
+                numbering=0)
+
+
+def make_config(**kw):
+    d = default_config()
+    d.update(kw)
+    cfg = Config()
+    mask = np.ascontiguousarray(d.pop("conv"), dtype=np.float32)
+    cfg._mask = mask
+    for k, v in d.items():
+        if k == "phot_autoparams":
+            cfg.phot_autoparams[0], cfg.phot_autoparams[1] = v
+        else:
+            setattr(cfg, k, v)
+    cfg.conv = _f(mask)
+    cfg.conv_h, cfg.conv_w = mask.shape
+    return cfg
+
+
+class Context:
+    """One libsexgpu context (device buffers are kept between calls)."""
+
+    def __init__(self, device=0):
+        self.h = C.c_void_p()
+        _check(lib().sexgpu_create(C.byref(self.h), device), None, "sexgpu_create")
+
+    def close(self):
+        if self.h:
+            lib().sexgpu_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        _check(lib().sexgpu_set_stream(self.h, C.c_void_p(stream_ptr)), self.h, "sexgpu_set_stream")
+
+    def background(self, img, **kw):
+        cfg = make_config(**kw)
+        sub = np.ascontiguousarray(img, np.float32).copy()
+        h, w = sub.shape
+        bw, bh = min(cfg.back_size, w), min(cfg.back_size, h)
+        nb = ((w - 1) // bw + 1) * ((h - 1) // bh + 1)
+        back = np.zeros(nb, np.float32)
+        sig = np.zeros(nb, np.float32)
+        s = Summary()
+        _check(lib().sexgpu_background(self.h, _f(sub), w, h, C.byref(cfg), _f(back), _f(sig), C.byref(s)),
+               self.h, "sexgpu_background")
+        return sub, back, sig, s
+
+    def filter(self, sub, mask):
+        sub = np.ascontiguousarray(sub, np.float32)
+        mask = np.ascontiguousarray(mask, np.float32)
+        h, w = sub.shape
+        cd = np.zeros_like(sub)
+        _check(lib().sexgpu_filter(self.h, _f(sub), w, h, _f(mask), mask.shape[1], mask.shape[0], _f(cd)),
+               self.h, "sexgpu_filter")
+        return cd
+
+    def extract(self, img, max_objects=None, want_maps=False, **kw):
+        """Host frame in, catalogue (+ segmentation map) out."""
+        cfg = make_config(**kw)
+        img = np.ascontiguousarray(img, np.float32)
+        h, w = img.shape
+        if max_objects is None:
+            max_objects = w * h // max(1, cfg.detect_minarea) // 2 + 16
+        objs = np.zeros(max_objects, OBJECT_DTYPE)
+        seg = np.zeros((h, w), np.int32)
+        n = C.c_int()
+        s = Summary()
+        sub = np.zeros_like(img) if want_maps else None
+        cd = np.zeros_like(img) if want_maps else None
+        rc = lib().sexgpu_extract(self.h, _f(img), None, w, h, C.byref(cfg),
+                                  objs.ctypes.data_as(C.c_void_p), max_objects, C.byref(n),
+                                  seg.ctypes.data_as(C.c_void_p), _f(sub) if want_maps else None,
+                                  _f(cd) if want_maps else None, C.byref(s))
+        _check(rc, self.h, "sexgpu_extract")
+        if want_maps:
+            return objs[:n.value], seg, s, sub, cd
+        return objs[:n.value], seg, s
+
+    def extract_device(self, dev_ptr, w, h, **kw):
+        """Frame already in device memory (e.g. torch tensor .data_ptr())."""
+        cfg = make_config(**kw)
+        s = Summary()
+        _check(lib().sexgpu_extract_device(self.h, C.c_void_p(dev_ptr), None, w, h, C.byref(cfg), C.byref(s)),
+               self.h, "sexgpu_extract_device")
+        return s
+
+    def copy_results(self, max_objects, segmap=False, shape=None):
+        objs = np.zeros(max_objects, OBJECT_DTYPE)
+        n = C.c_int()
+        seg = np.zeros(shape, np.int32) if segmap else None
+        rc = lib().sexgpu_copy_results(self.h, objs.ctypes.data_as(C.c_void_p), max_objects, C.byref(n),
+                                       seg.ctypes.data_as(C.c_void_p) if segmap else None, None, None)
+        _check(rc, self.h, "sexgpu_copy_results")
+        return (objs[:n.value], seg) if segmap else objs[:n.value]
+
+    def stage_times(self):
+        st = (Stage * 32)()
+        n = lib().sexgpu_stage_times(self.h, st, 32)
+        return [(st[i].name.decode(), st[i].launches, st[i].ms) for i in range(max(n, 0))]
+
+
+def getconv(path):
+    mask = np.zeros(1024, np.float32)
+    mw, mh = C.c_int(), C.c_int()
+    n = lib().sexgpu_getconv(path.encode(), _f(mask), 1024, C.byref(mw), C.byref(mh))
+    if n < 0:
+        raise ValueError("bad convolution file %s" % path)
+    return mask[:n].reshape(mh.value, mw.value).copy()

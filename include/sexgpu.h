@@ -1,0 +1,172 @@
+/*
+ * sexgpu.h -- C ABI of libsexgpu, the B200 (sm_100a) implementation of
+ * SExtractor's per-field extraction path (background -> detection filter ->
+ * thresholding/CCL -> multi-threshold deblending -> CLEAN -> isophotal
+ * analysis, photometry and FLAGS -> catalogue).
+ *
+ * Every entry point returns an int status (SEXGPU_OK or a negative code) and
+ * never exits the process.  All arguments are plain pointers and sizes.
+ *
+ * Reference interfaces replaced (baoxuezhao/GPU-SExtractor):
+ *   sexgpu_background   <- makeback()            src/back.c:43, with
+ *                          back_estimate()       src/cuda/cudaback.h:5
+ *   sexgpu_filter       <- cudaFilter()          src/cuda/cudafilter.h:11
+ *   sexgpu_extract      <- scanimage()           src/scan.c:65, i.e. the call
+ *                          sequence init_device  src/cuda/cudainit.h:11,
+ *                          run_detection         src/cuda/cudadetection.h:15,
+ *                          init_deblend/parcel_out src/cuda/cudadeblend.h:11,16,
+ *                          analyse_gpu           src/cuda/cudaanalyse.h:13,
+ *                          run_clean             src/cuda/cudaclean.h:4,
+ *                          endobject_gpu         src/cuda/cudaanalyse.h:39,
+ *                          clear_device          src/cuda/cudainit.h:12
+ *   sexgpu_getconv      <- getconv()             src/filter.c:101
+ */
+#ifndef SEXGPU_H
+#define SEXGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SEXGPU_OK              0
+#define SEXGPU_ERR_ARG        -1   /* bad argument (sizes, config values) */
+#define SEXGPU_ERR_CUDA       -2   /* CUDA runtime error */
+#define SEXGPU_ERR_NOMEM      -3   /* device allocation failed */
+#define SEXGPU_ERR_RANGE      -4   /* an exact sum exceeded its dynamic range */
+#define SEXGPU_ERR_CAPACITY   -5   /* caller buffer too small (count returned) */
+#define SEXGPU_ERR_NODEVICE   -6   /* no usable CUDA device */
+#define SEXGPU_ERR_THRESH     -7   /* zero or negative threshold (src/back.c:196) */
+#define SEXGPU_ERR_LOOP       -8   /* a bounded device loop hit its iteration cap */
+
+#define SEXGPU_NISO 8
+
+/* Extraction settings; names follow the .sex keywords (src/preflist.h). */
+typedef struct {
+    int     back_size;          /* BACK_SIZE (square meshes) */
+    int     back_filtersize;    /* BACK_FILTERSIZE (square window) */
+    double  back_filtthresh;    /* BACK_FILTTHRESH */
+    int     back_type;          /* BACK_TYPE: 0 AUTO, 1 MANUAL */
+    double  back_value;         /* BACK_VALUE */
+    int     thresh_type;        /* THRESH_TYPE: 0 RELATIVE, 1 ABSOLUTE */
+    double  detect_thresh;      /* DETECT_THRESH */
+    double  analysis_thresh;    /* ANALYSIS_THRESH */
+    int     filter_flag;        /* FILTER */
+    int     conv_w, conv_h;     /* normalised mask size (<= 31 x 31) */
+    const float *conv;          /* normalised mask, row-major (host memory) */
+    int     detect_minarea;     /* DETECT_MINAREA */
+    int     deblend_nthresh;    /* DEBLEND_NTHRESH (1..64) */
+    double  deblend_mincont;    /* DEBLEND_MINCONT */
+    int     clean_flag;         /* CLEAN */
+    double  clean_param;        /* CLEAN_PARAM */
+    double  satur_level;        /* SATUR_LEVEL */
+    double  gain;               /* GAIN */
+    double  mag_zeropoint;      /* MAG_ZEROPOINT */
+    double  phot_aperture;      /* PHOT_APERTURES (one diameter) */
+    double  phot_autoparams[2]; /* PHOT_AUTOPARAMS */
+    int     mask_type;          /* MASK_TYPE: 0 NONE, 1 BLANK, 2 CORRECT */
+    int     weight_type;        /* WEIGHT_TYPE: 0 NONE, 1 MAP_VAR */
+    int     numbering;          /* 0 completion order, 1 first-pixel order */
+} sexgpu_config;
+
+/* One catalogue row (0-based pixel coordinates unless stated). */
+typedef struct {
+    int32_t number;             /* NUMBER, 1-based */
+    int32_t root;               /* raw (pre-deblending) object, first-pixel order */
+    int32_t level;              /* deblending level of the branch */
+    int32_t fdnpix, dnpix;
+    int32_t npix;               /* ISOAREA_IMAGE */
+    int32_t xmin, xmax, ymin, ymax;
+    int32_t peakx, peaky;       /* 1-based */
+    int32_t flags;              /* FLAGS */
+    int32_t iso[SEXGPU_NISO];   /* ISO0..ISO7 */
+    float   fdflux, dflux, flux, fluxerr, fdpeak, dpeak, peak;
+    double  mx, my, mx2, my2, mxy;
+    float   a, b, theta, abcor, cxx, cyy, cxy;
+    double  poserr_mx2, poserr_my2, poserr_mxy;
+    float   bkg, thresh, dthresh, mthresh, fwhm;
+    float   flux_iso, fluxerr_iso, mag_iso, magerr_iso;
+    float   flux_isocor, fluxerr_isocor;
+    float   flux_aper, fluxerr_aper, mag_aper, magerr_aper;
+    float   kronfactor, flux_auto, fluxerr_auto, mag_auto, magerr_auto;
+    float   elong, ellip, polar;
+} sexgpu_object;
+
+typedef struct {
+    int     nbackx, nbacky;
+    float   backmean, backsig;  /* global background median and rms */
+    float   dthresh, thresh;    /* detection / analysis thresholds in ADU */
+    int64_t npix_above;         /* pixels with filtered value >= dthresh */
+    int32_t nraw;               /* connected components >= DETECT_MINAREA */
+    int64_t nraw_pix;           /* pixels in those components */
+    int32_t ndetected;          /* objects after deblending */
+    int32_t nobj;               /* catalogue rows after CLEAN */
+} sexgpu_summary;
+
+typedef struct sexgpu_ctx sexgpu_ctx;
+
+/* Context on CUDA device `device`.  Device buffers grow on demand and are
+ * kept for later calls. */
+int sexgpu_create(sexgpu_ctx **ctx, int device);
+int sexgpu_destroy(sexgpu_ctx *ctx);
+/* Run later work on this cudaStream_t (NULL: the context's own stream). */
+int sexgpu_set_stream(sexgpu_ctx *ctx, void *stream);
+
+/* Whole extraction of one host frame (w*h float32, row-major).  var (w*h,
+ * may be NULL) is the variance map for weight_type MAP_VAR.  Writes up to
+ * max_objects catalogue rows to objs (host) and their count to *nobj; if the
+ * catalogue is longer, *nobj holds its length and SEXGPU_ERR_CAPACITY is
+ * returned.  segmap (w*h int32 host, may be NULL) receives NUMBER per pixel,
+ * 0 for sky.  sub/cd (w*h float host, may be NULL) receive the background-
+ * subtracted and the filtered frame. */
+int sexgpu_extract(sexgpu_ctx *ctx, const float *img, const float *var, int w, int h,
+                   const sexgpu_config *cfg, sexgpu_object *objs, int max_objects,
+                   int *nobj, int32_t *segmap, float *sub, float *cd, sexgpu_summary *sum);
+
+/* Same, for a frame already in device memory (d_img, d_var are device
+ * pointers; d_img is not modified).  Results stay on the device; read them
+ * with sexgpu_copy_results. */
+int sexgpu_extract_device(sexgpu_ctx *ctx, const float *d_img, const float *d_var, int w, int h,
+                          const sexgpu_config *cfg, sexgpu_summary *sum);
+
+/* Copy the results of the last extraction to host memory (any pointer may
+ * be NULL). */
+int sexgpu_copy_results(sexgpu_ctx *ctx, sexgpu_object *objs, int max_objects, int *nobj,
+                        int32_t *segmap, float *sub, float *cd);
+
+/* Background only (makeback + subbackline): img (host, w*h) is replaced by
+ * the background-subtracted frame; back/sigma (host, nbackx*nbacky, may be
+ * NULL) receive the filtered mesh maps. */
+int sexgpu_background(sexgpu_ctx *ctx, float *img, int w, int h, const sexgpu_config *cfg,
+                      float *back, float *sigma, sexgpu_summary *sum);
+
+/* Detection filter only: cd = mask (x) sub with a zero-padded frame. */
+int sexgpu_filter(sexgpu_ctx *ctx, const float *sub, int w, int h, const float *mask,
+                  int mw, int mh, float *cd);
+
+/* Read and normalise a .conv file (src/filter.c:101).  Returns the number
+ * of elements (mw*mh) or a negative status. */
+int sexgpu_getconv(const char *path, float *mask, int maxn, int *mw, int *mh);
+
+/* Fill cfg with the defaults of the reference's default.sex. */
+void sexgpu_default_config(sexgpu_config *cfg);
+
+/* Last CUDA error string of this context (empty if none). */
+const char *sexgpu_last_error(sexgpu_ctx *ctx);
+
+/* Timed kernel launches of the last extraction, per stage: number of
+ * launches of this library's kernels and event-timed milliseconds.  stages
+ * is filled with up to max entries; returns the number of stages. */
+typedef struct {
+    char    name[24];
+    int32_t launches;
+    float   ms;
+} sexgpu_stage;
+int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,57 @@
+"""The C ABI library loads and exports every entry point of include/sexgpu.h;
+the ctypes layouts match the C structs (CPU only: no compute calls)."""
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+import sexgpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "sexgpu.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void|const char \*)\s*\**\s*(sexgpu_\w+)\s*\(", src, re.M)))
+
+
+def test_library_exports_header_symbols():
+    lib = sexgpu.lib()
+    names = header_functions()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(sexgpu.EXPORTS)
+
+
+def test_struct_layouts_match_header():
+    prog = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "sexgpu.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(sexgpu_config), sizeof(sexgpu_object),
+         offsetof(sexgpu_object, mx), offsetof(sexgpu_object, poserr_mx2),
+         offsetof(sexgpu_object, polar), sizeof(sexgpu_summary), sizeof(sexgpu_stage));
+  return 0;
+}'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(prog)
+        exe = os.path.join(d, "t")
+        subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe])
+        vals = [int(v) for v in subprocess.check_output([exe]).split()]
+    import ctypes as C
+    dt = sexgpu.OBJECT_DTYPE
+    assert vals == [C.sizeof(sexgpu.Config), dt.itemsize, dt.fields["mx"][1], dt.fields["poserr_mx2"][1],
+                    dt.fields["polar"][1], C.sizeof(sexgpu.Summary), C.sizeof(sexgpu.Stage)]
+
+
+def test_config_rejected_without_device_work():
+    """Argument errors are reported as status codes (no GPU needed)."""
+    import ctypes as C
+    lib = sexgpu.lib()
+    assert lib.sexgpu_create(None, 0) == -1
+    assert lib.sexgpu_destroy(None) == -1
