@@ -62,6 +62,11 @@ class ClockSampler:
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        if vis:
+            ids = [v.strip() for v in vis.split(",") if v.strip()]
+            if index < len(ids):
+                index = ids[index]
         self.index = index
         self.proc = None
         self.lines = []
@@ -220,7 +225,9 @@ def run_gpu(args):
                 "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": None, "algorithmic_bytes": algo,
                 "stage_ms": {s[0]: round(s[2], 4) for s in stages}}
-    frame_bytes = 24 * N + 8 * 16 * summ.nraw_pix + 64 * summ.nobj
+    # algorithmic bytes of a frame (24N pixel stages + 8 B per pixel and
+    # deblending level + 16 B per object pixel + 64 B per catalogue row)
+    frame_bytes = 24 * N + 8 * int(summ.level_pix) + 16 * int(summ.nraw_pix) + 64 * int(summ.nobj)
     line = {
         "metric": METRIC, "value": round(frames_dev, 3), "unit": "frames/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_dev, 4),
@@ -228,6 +235,7 @@ def run_gpu(args):
         "data": "synthetic (seeded; stands in for the paper's unpublished 4096^2 frames)",
         "config": {"workload": WORKLOAD, "frame": [h, w], "objects": int(summ.nobj),
                    "raw_objects": int(summ.nraw), "pixels_above_threshold": int(summ.npix_above),
+                   "raw_object_pixels": int(summ.nraw_pix), "pixel_levels": int(summ.level_pix),
                    "l2": "flushed between steps (256 MB write outside the timed window)",
                    "parallelism": "frame-sharded replicas" if world > 1 else "single GPU"},
         "mobj_per_s": round(frames_dev * summ.nobj / 1e6, 4),
@@ -261,14 +269,19 @@ def algorithmic_bytes(stage, N, s):
     if stage == "roots":
         return 24 * N
     if stage == "deblend":
-        return 8 * 16 * int(s.nraw_pix)    # index + cd per pixel and level (~N/2 levels)
+        return 8 * int(s.level_pix)        # index + cd per pixel and level
     return 4 * N
+
+
+_FRAMES = {}
 
 
 def _oracle_worker(args):
     seed, n = args
     from oracle import oracle as O
-    frame = make_frame(seed)
+    if seed not in _FRAMES:
+        _FRAMES[seed] = make_frame(seed)
+    frame = _FRAMES[seed]
     cfg = workload_config()
     t = time.perf_counter()
     for _ in range(n):

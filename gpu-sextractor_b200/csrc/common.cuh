@@ -291,4 +291,5 @@ struct FrameScalars {
     int nobj;                       // objects after deblending
     int nsurv;                      // after CLEAN
     int e0sub;                      // smallest exponent of a non-zero |sub|
+    unsigned long long levpix;      // sum of the deblending level of every raw-object pixel
 };

@@ -108,13 +108,20 @@ __global__ void __launch_bounds__(GUESS_THREADS) k_mesh_guess(const float *__res
         if (bin >= 0 && bin < nlevels) atomicAdd(&hist[bin], 1);
     }
     __syncthreads();
-    // prefix of the histogram (one warp per 1/8 of the bins, then fix-up)
-    if (threadIdx.x == 0) {
-        int s = 0;
-        for (int i = 0; i <= SX_QUANTIF_NMAXLEVELS + 1; i++) {
-            pfx[i] = s;
-            s += hist[i];
-        }
+    // exclusive prefix of the histogram: 17 consecutive bins per thread
+    {
+        constexpr int PER = (SX_QUANTIF_NMAXLEVELS + 2 + GUESS_THREADS - 1) / GUESS_THREADS;
+        __shared__ int wsum[32];
+        int base = threadIdx.x * PER, loc = 0;
+        for (int k = 0; k < PER; k++)
+            if (base + k < SX_QUANTIF_NMAXLEVELS + 2) loc += hist[base + k];
+        int tot;
+        int run = block_exclusive_scan(loc, wsum, tot);
+        for (int k = 0; k < PER; k++)
+            if (base + k < SX_QUANTIF_NMAXLEVELS + 2) {
+                pfx[base + k] = run;
+                run += hist[base + k];
+            }
     }
     __syncthreads();
 

@@ -175,10 +175,13 @@ __global__ void __launch_bounds__(DB_THREADS) k_deblend_sweep(DebArgs A) {
     __syncthreads();
     if (threadIdx.x == 0) {
         int s = 0;
+        unsigned long long lp = 0;
         for (int L = A.N - 1; L >= 0; L--) {
             lvstart[L] = s;
             s += lvcnt[L];
+            lp += (unsigned long long)L * lvcnt[L];
         }
+        atomicAdd(&A.sc->levpix, lp);
     }
     __syncthreads();
     for (int k = threadIdx.x; k < P; k += blockDim.x) {

@@ -672,6 +672,7 @@ void fill_summary(sexgpu_ctx *ctx, const FrameParams &P, sexgpu_summary *s) {
     s->nraw_pix = ctx->hsc.nrootpix;
     s->ndetected = ctx->last_nobj;
     s->nobj = ctx->last_ns;
+    s->level_pix = (int64_t)ctx->hsc.levpix;
 }
 
 }  // namespace

@@ -1,0 +1,478 @@
+/*
+ * sex.c -- command-line front end of libsexgpu with the reference's usage:
+ *
+ *     sex image.fits [-c file.sex] [-KEYWORD value ...]
+ *
+ * Reference: src/main.c:40 (argument loop :65-121), src/prefs.c:66 (readprefs,
+ * `KEY value` lines, '#' comments), src/makeit.c:58 (per-image flow), and the
+ * catalogue row of src/scan.c:331-406 (printobj).  The extraction itself is
+ * the C ABI call sexgpu_extract() (include/sexgpu.h), which replaces
+ * makeback() + scanimage().
+ *
+ * Supported keywords (the extraction settings of src/preflist.h):
+ *   CATALOG_NAME CATALOG_TYPE (ASCII, ASCII_HEAD) PARAMETERS_NAME
+ *   DETECT_MINAREA DETECT_THRESH ANALYSIS_THRESH THRESH_TYPE FILTER FILTER_NAME
+ *   DEBLEND_NTHRESH DEBLEND_MINCONT CLEAN CLEAN_PARAM MASK_TYPE
+ *   PHOT_APERTURES PHOT_AUTOPARAMS SATUR_LEVEL MAG_ZEROPOINT GAIN
+ *   BACK_SIZE BACK_FILTERSIZE BACK_FILTTHRESH BACK_TYPE BACK_VALUE
+ *   CHECKIMAGE_TYPE (NONE, SEGMENTATION, BACKGROUND, -BACKGROUND, FILTERED)
+ *   CHECKIMAGE_NAME VERBOSE_TYPE
+ * Other keywords of the reference are accepted and ignored.
+ */
+#include <ctype.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <strings.h>
+#include <time.h>
+
+#include "sexgpu.h"
+
+#define MAXLINE 4096
+
+typedef struct {
+    char catalog_name[1024], catalog_type[64], parameters_name[1024], filter_name[1024];
+    char check_type[64], check_name[1024], verbose[32];
+    sexgpu_config cfg;
+    float mask[1024];
+} prefs_t;
+
+static void die(const char *msg, const char *arg)
+{
+    fprintf(stderr, "sex: %s%s\n", msg, arg ? arg : "");
+    exit(EXIT_FAILURE);
+}
+
+static char *trim(char *s)
+{
+    char *e;
+    while (*s && isspace((unsigned char)*s)) s++;
+    e = s + strlen(s);
+    while (e > s && isspace((unsigned char)e[-1])) *--e = 0;
+    return s;
+}
+
+static int yes(const char *v) { return v[0] == 'Y' || v[0] == 'y' || v[0] == 'T' || v[0] == 't' || v[0] == '1'; }
+
+/* one KEY value pair (src/prefs.c:66-305 semantics for the keys we use) */
+static void setpref(prefs_t *p, const char *key, char *val)
+{
+    sexgpu_config *c = &p->cfg;
+    char *comma;
+    if ((comma = strchr(val, '#'))) *comma = 0;
+    val = trim(val);
+    if (!strcasecmp(key, "CATALOG_NAME")) snprintf(p->catalog_name, sizeof p->catalog_name, "%s", val);
+    else if (!strcasecmp(key, "CATALOG_TYPE")) snprintf(p->catalog_type, sizeof p->catalog_type, "%s", val);
+    else if (!strcasecmp(key, "PARAMETERS_NAME")) snprintf(p->parameters_name, sizeof p->parameters_name, "%s", val);
+    else if (!strcasecmp(key, "FILTER_NAME")) snprintf(p->filter_name, sizeof p->filter_name, "%s", val);
+    else if (!strcasecmp(key, "CHECKIMAGE_TYPE")) snprintf(p->check_type, sizeof p->check_type, "%s", val);
+    else if (!strcasecmp(key, "CHECKIMAGE_NAME")) snprintf(p->check_name, sizeof p->check_name, "%s", val);
+    else if (!strcasecmp(key, "VERBOSE_TYPE")) snprintf(p->verbose, sizeof p->verbose, "%s", val);
+    else if (!strcasecmp(key, "DETECT_MINAREA")) c->detect_minarea = atoi(val);
+    else if (!strcasecmp(key, "DETECT_THRESH")) c->detect_thresh = atof(val);
+    else if (!strcasecmp(key, "ANALYSIS_THRESH")) c->analysis_thresh = atof(val);
+    else if (!strcasecmp(key, "THRESH_TYPE")) c->thresh_type = !strncasecmp(val, "ABSOLUTE", 8);
+    else if (!strcasecmp(key, "FILTER")) c->filter_flag = yes(val);
+    else if (!strcasecmp(key, "DEBLEND_NTHRESH")) c->deblend_nthresh = atoi(val);
+    else if (!strcasecmp(key, "DEBLEND_MINCONT")) c->deblend_mincont = atof(val);
+    else if (!strcasecmp(key, "CLEAN")) c->clean_flag = yes(val);
+    else if (!strcasecmp(key, "CLEAN_PARAM")) c->clean_param = atof(val);
+    else if (!strcasecmp(key, "MASK_TYPE"))
+        c->mask_type = !strncasecmp(val, "NONE", 4) ? 0 : !strncasecmp(val, "BLANK", 5) ? 1 : 2;
+    else if (!strcasecmp(key, "PHOT_APERTURES")) c->phot_aperture = atof(val);
+    else if (!strcasecmp(key, "PHOT_AUTOPARAMS")) {
+        c->phot_autoparams[0] = atof(val);
+        if ((comma = strchr(val, ','))) c->phot_autoparams[1] = atof(comma + 1);
+    } else if (!strcasecmp(key, "SATUR_LEVEL")) c->satur_level = atof(val);
+    else if (!strcasecmp(key, "MAG_ZEROPOINT")) c->mag_zeropoint = atof(val);
+    else if (!strcasecmp(key, "GAIN")) c->gain = atof(val);
+    else if (!strcasecmp(key, "BACK_SIZE")) c->back_size = atoi(val);
+    else if (!strcasecmp(key, "BACK_FILTERSIZE")) c->back_filtersize = atoi(val);
+    else if (!strcasecmp(key, "BACK_FILTTHRESH")) c->back_filtthresh = atof(val);
+    else if (!strcasecmp(key, "BACK_TYPE")) c->back_type = !strncasecmp(val, "MANUAL", 6);
+    else if (!strcasecmp(key, "BACK_VALUE")) c->back_value = atof(val);
+}
+
+static void readprefs(prefs_t *p, const char *path)
+{
+    char line[MAXLINE], *key, *val;
+    FILE *f = fopen(path, "r");
+    if (!f) die("cannot open configuration file ", path);
+    while (fgets(line, sizeof line, f)) {
+        key = trim(line);
+        if (!*key || *key == '#') continue;
+        val = key;
+        while (*val && !isspace((unsigned char)*val)) val++;
+        if (*val) *val++ = 0;
+        setpref(p, key, val);
+    }
+    fclose(f);
+}
+
+/* ---------------------------------------------------------------- FITS --- */
+static double card_num(const char *hdr, int ncards, const char *key, double def, int *found)
+{
+    char k[9];
+    int i;
+    snprintf(k, sizeof k, "%-8s", key);
+    for (i = 0; i < ncards; i++)
+        if (!strncmp(hdr + 80 * i, k, 8) && hdr[80 * i + 8] == '=') {
+            if (found) *found = 1;
+            return atof(hdr + 80 * i + 10);
+        }
+    if (found) *found = 0;
+    return def;
+}
+
+/* primary image of a FITS file as float (src/fits/fitsbody.c:195 read_body:
+ * BITPIX 8/16/32/-32/-64, BSCALE/BZERO) */
+static float *read_fits(const char *path, int *w, int *h)
+{
+    FILE *f = fopen(path, "rb");
+    char *hdr = NULL;
+    int ncards = 0, end = 0, bitpix, naxis, i, found;
+    size_t n, bytes;
+    double bscale, bzero;
+    unsigned char *raw;
+    float *img;
+    if (!f) die("cannot open image ", path);
+    while (!end) {
+        hdr = (char *)realloc(hdr, (size_t)(ncards + 36) * 80);
+        if (fread(hdr + (size_t)ncards * 80, 80, 36, f) != 36) die("truncated FITS header in ", path);
+        for (i = 0; i < 36; i++)
+            if (!strncmp(hdr + (size_t)(ncards + i) * 80, "END     ", 8)) end = 1;
+        ncards += 36;
+    }
+    bitpix = (int)card_num(hdr, ncards, "BITPIX", 0, &found);
+    naxis = (int)card_num(hdr, ncards, "NAXIS", 0, &found);
+    *w = (int)card_num(hdr, ncards, "NAXIS1", 0, &found);
+    *h = (int)card_num(hdr, ncards, "NAXIS2", 0, &found);
+    bscale = card_num(hdr, ncards, "BSCALE", 1.0, &found);
+    bzero = card_num(hdr, ncards, "BZERO", 0.0, &found);
+    free(hdr);
+    if (naxis < 2 || *w <= 0 || *h <= 0) die("not a 2-D image: ", path);
+    n = (size_t)*w * *h;
+    bytes = n * (size_t)(abs(bitpix) / 8);
+    raw = (unsigned char *)malloc(bytes);
+    if (fread(raw, 1, bytes, f) != bytes) die("truncated FITS data in ", path);
+    fclose(f);
+    img = (float *)malloc(n * sizeof(float));
+    for (size_t k = 0; k < n; k++) {
+        const unsigned char *q = raw + k * (size_t)(abs(bitpix) / 8);
+        double v;
+        switch (bitpix) {
+        case 8: v = q[0]; break;
+        case 16: v = (int16_t)((q[0] << 8) | q[1]); break;
+        case 32: v = (int32_t)(((uint32_t)q[0] << 24) | ((uint32_t)q[1] << 16) | ((uint32_t)q[2] << 8) | q[3]); break;
+        case -32: {
+            uint32_t u = ((uint32_t)q[0] << 24) | ((uint32_t)q[1] << 16) | ((uint32_t)q[2] << 8) | q[3];
+            float fv;
+            memcpy(&fv, &u, 4);
+            v = fv;
+            break;
+        }
+        case -64: {
+            uint64_t u = 0;
+            double dv;
+            for (int b = 0; b < 8; b++) u = (u << 8) | q[b];
+            memcpy(&dv, &u, 8);
+            v = dv;
+            break;
+        }
+        default: die("unsupported BITPIX in ", path); v = 0;
+        }
+        img[k] = (float)(bscale * v + bzero);
+        if (img[k] != img[k]) img[k] = -1e30f;   /* NaN: unusable pixel */
+    }
+    free(raw);
+    return img;
+}
+
+static void write_card(FILE *f, const char *card)
+{
+    char buf[81];
+    memset(buf, ' ', 80);
+    buf[80] = 0;
+    memcpy(buf, card, strlen(card) < 80 ? strlen(card) : 80);
+    fwrite(buf, 1, 80, f);
+}
+
+/* check image: BITPIX 32 (segmentation) or -32 (maps) */
+static void write_fits(const char *path, const void *data, int w, int h, int bitpix)
+{
+    FILE *f = fopen(path, "wb");
+    char card[81];
+    size_t n = (size_t)w * h, k;
+    int ncard = 0;
+    if (!f) die("cannot write ", path);
+    write_card(f, "SIMPLE  =                    T"); ncard++;
+    snprintf(card, sizeof card, "BITPIX  = %20d", bitpix); write_card(f, card); ncard++;
+    write_card(f, "NAXIS   =                    2"); ncard++;
+    snprintf(card, sizeof card, "NAXIS1  = %20d", w); write_card(f, card); ncard++;
+    snprintf(card, sizeof card, "NAXIS2  = %20d", h); write_card(f, card); ncard++;
+    write_card(f, "END"); ncard++;
+    for (; ncard % 36; ncard++) write_card(f, "");
+    for (k = 0; k < n; k++) {
+        uint32_t u;
+        unsigned char b[4];
+        memcpy(&u, (const char *)data + 4 * k, 4);
+        b[0] = u >> 24; b[1] = u >> 16; b[2] = u >> 8; b[3] = u;
+        fwrite(b, 1, 4, f);
+    }
+    for (k = (n * 4) % 2880; k && k < 2880; k++) fputc(0, f);
+    fclose(f);
+}
+
+/* ------------------------------------------------------------ catalogue --- */
+typedef struct {
+    const char *name, *fmt, *unit, *comment;
+} col_t;
+
+static const col_t COLS[] = {
+    {"NUMBER", "%10d", "", "Running object number"},
+    {"X_IMAGE", "%11.4f", "pixel", "Object position along x"},
+    {"Y_IMAGE", "%11.4f", "pixel", "Object position along y"},
+    {"XMIN_IMAGE", "%10d", "pixel", "Minimum x-coordinate among detected pixels"},
+    {"YMIN_IMAGE", "%10d", "pixel", "Minimum y-coordinate among detected pixels"},
+    {"XMAX_IMAGE", "%10d", "pixel", "Maximum x-coordinate among detected pixels"},
+    {"YMAX_IMAGE", "%10d", "pixel", "Maximum y-coordinate among detected pixels"},
+    {"ISOAREA_IMAGE", "%9d", "pixel**2", "Isophotal area above Analysis threshold"},
+    {"FLUX_ISO", "%12.7g", "count", "Isophotal flux"},
+    {"FLUXERR_ISO", "%12.7g", "count", "RMS error for isophotal flux"},
+    {"MAG_ISO", "%8.4f", "mag", "Isophotal magnitude"},
+    {"MAGERR_ISO", "%8.4f", "mag", "RMS error for isophotal magnitude"},
+    {"FLUX_ISOCOR", "%12.7g", "count", "Corrected isophotal flux"},
+    {"FLUXERR_ISOCOR", "%12.7g", "count", "RMS error for corrected isophotal flux"},
+    {"FLUX_APER", "%12.7g", "count", "Flux vector within fixed circular aperture(s)"},
+    {"FLUXERR_APER", "%12.7g", "count", "RMS error vector for aperture flux(es)"},
+    {"MAG_APER", "%8.4f", "mag", "Fixed aperture magnitude vector"},
+    {"MAGERR_APER", "%8.4f", "mag", "RMS error vector for fixed aperture mag."},
+    {"FLUX_AUTO", "%12.7g", "count", "Flux within a Kron-like elliptical aperture"},
+    {"FLUXERR_AUTO", "%12.7g", "count", "RMS error for AUTO flux"},
+    {"MAG_AUTO", "%8.4f", "mag", "Kron-like elliptical aperture magnitude"},
+    {"MAGERR_AUTO", "%8.4f", "mag", "RMS error for AUTO magnitude"},
+    {"KRON_RADIUS", "%5.2f", "", "Kron apertures in units of A or B"},
+    {"BACKGROUND", "%12.7g", "count", "Background at centroid position"},
+    {"THRESHOLD", "%12.7g", "count", "Detection threshold above background"},
+    {"FLUX_MAX", "%12.7g", "count", "Peak flux above background"},
+    {"X2_IMAGE", "%15.10e", "pixel**2", "Variance along x"},
+    {"Y2_IMAGE", "%15.10e", "pixel**2", "Variance along y"},
+    {"XY_IMAGE", "%15.10e", "pixel**2", "Covariance between x and y"},
+    {"ERRX2_IMAGE", "%15.10e", "pixel**2", "Variance of position along x"},
+    {"ERRY2_IMAGE", "%15.10e", "pixel**2", "Variance of position along y"},
+    {"ERRXY_IMAGE", "%15.10e", "pixel**2", "Covariance of position between x and y"},
+    {"CXX_IMAGE", "%12.7g", "pixel**(-2)", "Cxx object ellipse parameter"},
+    {"CYY_IMAGE", "%12.7g", "pixel**(-2)", "Cyy object ellipse parameter"},
+    {"CXY_IMAGE", "%12.7g", "pixel**(-2)", "Cxy object ellipse parameter"},
+    {"A_IMAGE", "%9.3f", "pixel", "Profile RMS along major axis"},
+    {"B_IMAGE", "%9.3f", "pixel", "Profile RMS along minor axis"},
+    {"THETA_IMAGE", "%5.1f", "deg", "Position angle (CCW/x)"},
+    {"ELONGATION", "%8.3f", "", "A_IMAGE/B_IMAGE"},
+    {"ELLIPTICITY", "%8.3f", "", "1 - B_IMAGE/A_IMAGE"},
+    {"FWHM_IMAGE", "%8.2f", "pixel", "FWHM assuming a gaussian core"},
+    {"FLAGS", "%3d", "", "Extraction flags"},
+    {"XPEAK_IMAGE", "%10d", "pixel", "x-coordinate of the brightest pixel"},
+    {"YPEAK_IMAGE", "%10d", "pixel", "y-coordinate of the brightest pixel"},
+    {NULL, NULL, NULL, NULL}};
+
+static void print_col(FILE *f, int c, const sexgpu_object *o)
+{
+    const char *fmt = COLS[c].fmt;
+    switch (c) {
+    case 0: fprintf(f, fmt, o->number); break;
+    case 1: fprintf(f, fmt, o->mx + 1.0); break;
+    case 2: fprintf(f, fmt, o->my + 1.0); break;
+    case 3: fprintf(f, fmt, o->xmin + 1); break;
+    case 4: fprintf(f, fmt, o->ymin + 1); break;
+    case 5: fprintf(f, fmt, o->xmax + 1); break;
+    case 6: fprintf(f, fmt, o->ymax + 1); break;
+    case 7: fprintf(f, fmt, o->npix); break;
+    case 8: fprintf(f, fmt, o->flux_iso); break;
+    case 9: fprintf(f, fmt, o->fluxerr_iso); break;
+    case 10: fprintf(f, fmt, o->mag_iso); break;
+    case 11: fprintf(f, fmt, o->magerr_iso); break;
+    case 12: fprintf(f, fmt, o->flux_isocor); break;
+    case 13: fprintf(f, fmt, o->fluxerr_isocor); break;
+    case 14: fprintf(f, fmt, o->flux_aper); break;
+    case 15: fprintf(f, fmt, o->fluxerr_aper); break;
+    case 16: fprintf(f, fmt, o->mag_aper); break;
+    case 17: fprintf(f, fmt, o->magerr_aper); break;
+    case 18: fprintf(f, fmt, o->flux_auto); break;
+    case 19: fprintf(f, fmt, o->fluxerr_auto); break;
+    case 20: fprintf(f, fmt, o->mag_auto); break;
+    case 21: fprintf(f, fmt, o->magerr_auto); break;
+    case 22: fprintf(f, fmt, o->kronfactor); break;
+    case 23: fprintf(f, fmt, o->bkg); break;
+    case 24: fprintf(f, fmt, o->thresh); break;
+    case 25: fprintf(f, fmt, o->peak); break;
+    case 26: fprintf(f, fmt, o->mx2); break;
+    case 27: fprintf(f, fmt, o->my2); break;
+    case 28: fprintf(f, fmt, o->mxy); break;
+    case 29: fprintf(f, fmt, o->poserr_mx2); break;
+    case 30: fprintf(f, fmt, o->poserr_my2); break;
+    case 31: fprintf(f, fmt, o->poserr_mxy); break;
+    case 32: fprintf(f, fmt, o->cxx); break;
+    case 33: fprintf(f, fmt, o->cyy); break;
+    case 34: fprintf(f, fmt, o->cxy); break;
+    case 35: fprintf(f, fmt, o->a); break;
+    case 36: fprintf(f, fmt, o->b); break;
+    case 37: fprintf(f, fmt, o->theta); break;
+    case 38: fprintf(f, fmt, o->elong); break;
+    case 39: fprintf(f, fmt, o->ellip); break;
+    case 40: fprintf(f, fmt, o->fwhm); break;
+    case 41: fprintf(f, fmt, o->flags); break;
+    case 42: fprintf(f, fmt, o->peakx); break;
+    case 43: fprintf(f, fmt, o->peaky); break;
+    }
+}
+
+/* the 31 columns of src/scan.c:331-406 (printobj); world coordinates and
+ * CLASS_STAR are written as 0, as the reference does for ALPHA/DELTA */
+static void printobj(FILE *f, const sexgpu_object *o)
+{
+    fprintf(f, "%10d %11.7f %+11.7f %10.3f %10.3f %12.7g %12.7g %8.4f %8.4f %12.7g %12.7g %12.7g %12.7g "
+               "%8.4f %8.4f %12.7g %12.7g %8.4f %8.4f %5.1f %15.10e %15.10e %15.10e %3d %8.3f %8.3f %5.2f "
+               "%12.7g %5.2f %12.7g %8.2f\n",
+            o->number, 0.0, 0.0, (float)(o->mx + 1.0), (float)(o->my + 1.0), o->flux_iso, o->fluxerr_iso,
+            o->mag_iso, o->magerr_iso, o->flux_isocor, o->fluxerr_isocor, o->flux_aper, o->fluxerr_aper,
+            o->mag_aper, o->magerr_aper, o->flux_auto, o->fluxerr_auto, o->mag_auto, o->magerr_auto, o->theta,
+            o->poserr_mx2, o->poserr_my2, o->poserr_mxy, o->flags, o->elong, o->ellip, 0.0f, o->peak,
+            o->kronfactor, o->bkg, o->fwhm);
+}
+
+static int read_params(const char *path, int *sel, int maxsel)
+{
+    char line[MAXLINE];
+    int n = 0;
+    FILE *f = fopen(path, "r");
+    if (!f) return 0;
+    while (fgets(line, sizeof line, f) && n < maxsel) {
+        char *s = trim(line), *par;
+        if (!*s || *s == '#') continue;
+        if ((par = strchr(s, '('))) *par = 0;
+        for (int c = 0; COLS[c].name; c++)
+            if (!strcasecmp(COLS[c].name, s)) {
+                sel[n++] = c;
+                break;
+            }
+    }
+    fclose(f);
+    return n;
+}
+
+int main(int argc, char **argv)
+{
+    prefs_t p;
+    const char *image = NULL, *conf = "default.sex";
+    int i, w, h, n = 0, rc, mw, mh;
+    float *img;
+    sexgpu_object *objs;
+    int32_t *seg = NULL;
+    float *sub = NULL, *cd = NULL;
+    sexgpu_summary s;
+    sexgpu_ctx *ctx;
+    clock_t t0 = clock();
+
+    memset(&p, 0, sizeof p);
+    sexgpu_default_config(&p.cfg);
+    strcpy(p.catalog_name, "test.cat");
+    strcpy(p.catalog_type, "ASCII_HEAD");
+    strcpy(p.parameters_name, "default.param");
+    strcpy(p.filter_name, "default.conv");
+    strcpy(p.check_type, "NONE");
+    strcpy(p.check_name, "check.fits");
+    /* src/main.c:65-121: configuration file first, then -KEY value overrides */
+    for (i = 1; i < argc; i++)
+        if (!strcmp(argv[i], "-c") && i + 1 < argc) conf = argv[++i];
+        else if (argv[i][0] == '-' && i + 1 < argc) i++;
+        else if (!image) image = argv[i];
+    if (!image) {
+        fprintf(stderr, "usage: sex image.fits [-c file.sex] [-KEYWORD value ...]\n");
+        return EXIT_FAILURE;
+    }
+    {
+        FILE *f = fopen(conf, "r");
+        if (f) {
+            fclose(f);
+            readprefs(&p, conf);
+        } else if (strcmp(conf, "default.sex"))
+            die("cannot open configuration file ", conf);
+    }
+    for (i = 1; i < argc; i++)
+        if (!strcmp(argv[i], "-c")) i++;
+        else if (argv[i][0] == '-' && i + 1 < argc) {
+            char val[MAXLINE];
+            snprintf(val, sizeof val, "%s", argv[i + 1]);
+            setpref(&p, argv[i] + 1, val);
+            i++;
+        }
+    if (p.cfg.filter_flag) {
+        if (sexgpu_getconv(p.filter_name, p.mask, 1024, &mw, &mh) < 0) die("cannot read filter ", p.filter_name);
+        p.cfg.conv = p.mask;
+        p.cfg.conv_w = mw;
+        p.cfg.conv_h = mh;
+    }
+    img = read_fits(image, &w, &h);
+    if ((rc = sexgpu_create(&ctx, 0)) != SEXGPU_OK) die("no usable CUDA device", NULL);
+    objs = (sexgpu_object *)malloc(sizeof(sexgpu_object) * 1024);
+    if (strcasecmp(p.check_type, "NONE")) {
+        seg = (int32_t *)malloc(sizeof(int32_t) * (size_t)w * h);
+        sub = (float *)malloc(sizeof(float) * (size_t)w * h);
+        cd = (float *)malloc(sizeof(float) * (size_t)w * h);
+    }
+    rc = sexgpu_extract(ctx, img, NULL, w, h, &p.cfg, objs, 1024, &n, seg, sub, cd, &s);
+    if (rc == SEXGPU_ERR_CAPACITY) {
+        objs = (sexgpu_object *)realloc(objs, sizeof(sexgpu_object) * (size_t)(n + 1));
+        rc = sexgpu_copy_results(ctx, objs, n, &n, NULL, NULL, NULL);
+    }
+    if (rc != SEXGPU_OK) {
+        fprintf(stderr, "sex: extraction failed (%d): %s\n", rc, sexgpu_last_error(ctx));
+        return EXIT_FAILURE;
+    }
+    if (strcasecmp(p.catalog_type, "NONE")) {
+        FILE *cat = !strcmp(p.catalog_name, "STDOUT") ? stdout : fopen(p.catalog_name, "w");
+        if (!cat) die("cannot write ", p.catalog_name);
+        if (!strcasecmp(p.catalog_type, "ASCII_HEAD") || !strcasecmp(p.catalog_type, "ASCII")) {
+            int sel[64], ns = read_params(p.parameters_name, sel, 64), k;
+            if (ns == 0) {
+                for (i = 0; i < n; i++) printobj(cat, &objs[i]);
+            } else {
+                if (!strcasecmp(p.catalog_type, "ASCII_HEAD"))
+                    for (k = 0; k < ns; k++)
+                        fprintf(cat, "#%4d %-22s %-58s [%s]\n", k + 1, COLS[sel[k]].name, COLS[sel[k]].comment,
+                                COLS[sel[k]].unit);
+                for (i = 0; i < n; i++) {
+                    for (k = 0; k < ns; k++) {
+                        if (k) fputc(' ', cat);
+                        print_col(cat, sel[k], &objs[i]);
+                    }
+                    fputc('\n', cat);
+                }
+            }
+        } else
+            for (i = 0; i < n; i++) printobj(cat, &objs[i]);
+        if (cat != stdout) fclose(cat);
+    }
+    if (seg) {
+        if (!strcasecmp(p.check_type, "SEGMENTATION")) write_fits(p.check_name, seg, w, h, 32);
+        else if (!strcasecmp(p.check_type, "-BACKGROUND")) write_fits(p.check_name, sub, w, h, -32);
+        else if (!strcasecmp(p.check_type, "FILTERED")) write_fits(p.check_name, cd, w, h, -32);
+        else if (!strcasecmp(p.check_type, "BACKGROUND")) {
+            for (size_t k = 0; k < (size_t)w * h; k++) sub[k] = img[k] - sub[k];
+            write_fits(p.check_name, sub, w, h, -32);
+        }
+    }
+    if (strcasecmp(p.verbose, "QUIET"))
+        fprintf(stderr, "Background: %g RMS: %g / Threshold: %g\nObjects: detected %d / sextracted %d\n"
+                        "> All done (in %.2f s)\n",
+                s.backmean, s.backsig, s.dthresh, s.ndetected, n, (double)(clock() - t0) / CLOCKS_PER_SEC);
+    sexgpu_destroy(ctx);
+    free(img);
+    free(objs);
+    free(seg);
+    free(sub);
+    free(cd);
+    return EXIT_SUCCESS;
+}

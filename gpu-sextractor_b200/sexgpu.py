@@ -67,6 +67,7 @@ class Summary(C.Structure):
         ("nbackx", C.c_int), ("nbacky", C.c_int), ("backmean", C.c_float), ("backsig", C.c_float),
         ("dthresh", C.c_float), ("thresh", C.c_float), ("npix_above", C.c_int64),
         ("nraw", C.c_int32), ("nraw_pix", C.c_int64), ("ndetected", C.c_int32), ("nobj", C.c_int32),
+        ("level_pix", C.c_int64),
     ]
 
 

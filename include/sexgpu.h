@@ -103,6 +103,8 @@ typedef struct {
     int64_t nraw_pix;           /* pixels in those components */
     int32_t ndetected;          /* objects after deblending */
     int32_t nobj;               /* catalogue rows after CLEAN */
+    int64_t level_pix;          /* sum over raw-object pixels of the highest
+                                   deblending level each pixel reaches */
 } sexgpu_summary;
 
 typedef struct sexgpu_ctx sexgpu_ctx;

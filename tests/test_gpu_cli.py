@@ -1,0 +1,63 @@
+"""The `sex` front end (gpu-sextractor_b200/host/sex.c) on a FITS frame:
+configuration file + -KEY overrides, catalogue rows and the segmentation check
+image, compared with the oracle."""
+import os
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SEX = os.path.join(ROOT, "gpu-sextractor_b200", "sex")
+
+
+def write_fits(path, img, bitpix=-32, bscale=1.0, bzero=0.0):
+    cards = ["SIMPLE  =                    T", "BITPIX  = %20d" % bitpix, "NAXIS   =                    2",
+             "NAXIS1  = %20d" % img.shape[1], "NAXIS2  = %20d" % img.shape[0]]
+    if bitpix == 16:
+        cards += ["BSCALE  = %20.10f" % bscale, "BZERO   = %20.10f" % bzero]
+    cards.append("END")
+    hdr = "".join(c.ljust(80) for c in cards)
+    hdr = hdr.ljust((len(hdr) + 2879) // 2880 * 2880)
+    if bitpix == -32:
+        data = img.astype(">f4").tobytes()
+    else:
+        data = np.round((img - bzero) / bscale).astype(">i2").tobytes()
+    data += b"\0" * ((2880 - len(data) % 2880) % 2880)
+    with open(path, "wb") as f:
+        f.write(hdr.encode() + data)
+
+
+def read_fits_i32(path, w, h):
+    with open(path, "rb") as f:
+        raw = f.read()
+    return np.frombuffer(raw[2880:2880 + 4 * w * h], ">i4").reshape(h, w)
+
+
+def test_cli_catalog_and_segmentation(tmp_path, masks):
+    if not os.path.exists(SEX):
+        subprocess.check_call(["make", "-s", "-C", os.path.dirname(SEX)])
+    img = synth.frame_c0(seed=3, w=400, h=300, nsrc=300)
+    fits = tmp_path / "img.fits"
+    write_fits(str(fits), img)
+    conv = tmp_path / "g.conv"
+    m = masks["gauss_2.5_5x5"]
+    conv.write_text("CONV NONORM\n" + "\n".join(" ".join("%.9g" % v for v in row) for row in m) + "\n")
+    cfgf = tmp_path / "t.sex"
+    cfgf.write_text("CATALOG_TYPE ASCII\nFILTER_NAME %s\nDETECT_THRESH 1.5\nBACK_SIZE 64\n" % conv)
+    cat = tmp_path / "t.cat"
+    seg = tmp_path / "seg.fits"
+    subprocess.check_call([SEX, str(fits), "-c", str(cfgf), "-CATALOG_NAME", str(cat), "-CHECKIMAGE_TYPE",
+                           "SEGMENTATION", "-CHECKIMAGE_NAME", str(seg), "-VERBOSE_TYPE", "QUIET"],
+                          cwd=str(tmp_path))
+    rows = [l.split() for l in cat.read_text().splitlines() if l.strip()]
+    o, oseg, s = O.extract(img, conv=m)
+    assert len(rows) == len(o)
+    assert [int(r[0]) for r in rows] == list(o["number"])
+    assert [int(r[23]) for r in rows] == list(o["flags"])
+    assert np.array_equal(read_fits_i32(str(seg), 400, 300), oseg)
