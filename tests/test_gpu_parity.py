@@ -70,3 +70,67 @@ def test_extract_c0(gpu_ctx, masks, seed):
     assert gs.ndetected == os_.ndetected
     assert np.array_equal(gseg, oseg)
     compare_catalogs(g, o)
+
+
+def run_both(gpu_ctx, img, **kw):
+    g, gseg, gs = gpu_ctx.extract(img, **kw)
+    o, oseg, os_ = O.extract(img, **kw)
+    assert (gs.nraw, gs.nraw_pix, gs.ndetected, gs.nobj) == (os_.nraw, os_.nraw_pix, os_.ndetected, os_.nobj)
+    assert (gs.backmean, gs.backsig, gs.dthresh, gs.thresh) == (os_.backmean, os_.backsig, os_.dthresh, os_.thresh)
+    assert gs.npix_above == os_.npix_above
+    assert np.array_equal(gseg, oseg)
+    compare_catalogs(g, o)
+    return g
+
+
+@pytest.mark.parametrize("w,h", [(7, 5), (64, 64), (333, 257), (1000, 37), (37, 700)])
+def test_shapes(gpu_ctx, w, h):
+    img = synth.frame_c0(seed=w * 7 + h, w=w, h=h, nsrc=max(1, w * h // 400))
+    run_both(gpu_ctx, img)
+
+
+def test_constant_frame_has_no_objects(gpu_ctx):
+    img = np.full((200, 300), 1000.0, np.float32)
+    g = run_both(gpu_ctx, img)
+    assert len(g) == 0
+
+
+def test_bad_pixels_and_nan(gpu_ctx):
+    img = synth.frame_c0(seed=21, w=400, h=300, nsrc=300)
+    img[:70, :130] = -1e30          # whole meshes unusable: nearest-mesh fill
+    img[200:203, 50:60] = np.nan
+    run_both(gpu_ctx, img)
+
+
+@pytest.mark.parametrize("opts", [
+    dict(deblend_nthresh=1), dict(clean_flag=0), dict(filter_flag=0),
+    dict(back_type=1, back_value=1000.0), dict(thresh_type=1, detect_thresh=40.0, analysis_thresh=40.0),
+    dict(numbering=1), dict(detect_minarea=1), dict(detect_minarea=3), dict(detect_minarea=12),
+    dict(deblend_mincont=0.0), dict(deblend_mincont=1.0), dict(deblend_nthresh=64, deblend_mincont=0.0005),
+    dict(clean_param=2.0), dict(gain=4.0), dict(mask_type=0), dict(back_filtersize=1),
+    dict(back_filtersize=5, back_filtthresh=3.0), dict(satur_level=2000.0), dict(phot_aperture=12.0),
+])
+def test_options(gpu_ctx, masks, opts):
+    img = synth.frame_c0(seed=3, w=512, h=400, nsrc=700)
+    run_both(gpu_ctx, img, **opts)
+
+
+@pytest.mark.parametrize("mask", ["gauss_2.5_5x5", "mexhat_2.5_7x7", "gauss_4.0_7x7", "tophat_5.0_5x5"])
+def test_masks_crowded(gpu_ctx, masks, mask):
+    img = synth.frame_c1(seed=77, w=600, h=500, nsrc=3000)
+    run_both(gpu_ctx, img, conv=masks[mask])
+
+
+def test_repeatable(gpu_ctx, masks):
+    img = synth.frame_c1(seed=78, w=700, h=600, nsrc=4000)
+    a, sa, _ = gpu_ctx.extract(img, conv=masks["gauss_2.5_5x5"])
+    b, sb, _ = gpu_ctx.extract(img, conv=masks["gauss_2.5_5x5"])
+    assert a.tobytes() == b.tobytes() and np.array_equal(sa, sb)
+
+
+def test_full_size_c1(gpu_ctx, masks):
+    """The 4096^2 paper-scale frame: the whole catalogue and segmentation map
+    against the oracle (about 10 s of CPU for the oracle)."""
+    img = synth.frame_c1(seed=1000)
+    g = run_both(gpu_ctx, img, conv=masks["gauss_2.5_5x5"])
+    assert len(g) > 50000
