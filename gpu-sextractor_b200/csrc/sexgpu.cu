@@ -1004,3 +1004,6 @@ int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max) {
 }
 
 }  // extern "C"
+
+// background estimation without device allocation (fixed scratch array)
+#include "noalloc.cu"

@@ -23,7 +23,8 @@ NISO = 8
 OK = 0
 ERRORS = {-1: "bad argument", -2: "CUDA error", -3: "out of device memory",
           -4: "exact sum out of range", -5: "buffer too small", -6: "no CUDA device",
-          -7: "zero or negative threshold", -8: "device loop cap reached"}
+          -7: "zero or negative threshold", -8: "device loop cap reached",
+          -9: "frame beyond the fixed scratch of the no-allocation entry point"}
 
 
 class Config(C.Structure):
@@ -77,7 +78,8 @@ class Stage(C.Structure):
 
 EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extract",
            "sexgpu_extract_device", "sexgpu_copy_results", "sexgpu_background", "sexgpu_filter",
-           "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times"]
+           "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times",
+           "sexgpu_background_noalloc"]
 
 _lib = None
 
@@ -232,6 +234,19 @@ class Context:
         st = (Stage * 32)()
         n = lib().sexgpu_stage_times(self.h, st, 32)
         return [(st[i].name.decode(), st[i].launches, st[i].ms) for i in range(max(n, 0))]
+
+
+def background_noalloc(d_img, d_sub, w, h, d_back, d_sigma, stream=0, **kw):
+    """sexgpu_background_noalloc on caller-owned device buffers (device
+    pointers as ints).  For callers that cannot allocate device memory: the
+    library works in a fixed device array; see include/sexgpu.h for limits."""
+    cfg = make_config(**kw)
+    s = Summary()
+    rc = lib().sexgpu_background_noalloc(C.c_void_p(d_img), C.c_void_p(d_sub), w, h, C.byref(cfg),
+                                         C.c_void_p(d_back), C.c_void_p(d_sigma), C.byref(s),
+                                         C.c_void_p(stream))
+    _check(rc, None, "sexgpu_background_noalloc")
+    return s
 
 
 def getconv(path):

@@ -40,6 +40,7 @@ extern "C" {
 #define SEXGPU_ERR_NODEVICE   -6   /* no usable CUDA device */
 #define SEXGPU_ERR_THRESH     -7   /* zero or negative threshold (src/back.c:196) */
 #define SEXGPU_ERR_LOOP       -8   /* a bounded device loop hit its iteration cap */
+#define SEXGPU_ERR_NOALLOC_LIMIT -9 /* frame beyond the fixed scratch of sexgpu_background_noalloc */
 
 #define SEXGPU_NISO 8
 
@@ -154,6 +155,31 @@ int sexgpu_getconv(const char *path, float *mask, int maxn, int *mw, int *mh);
 
 /* Fill cfg with the defaults of the reference's default.sex. */
 void sexgpu_default_config(sexgpu_config *cfg);
+
+/* Background estimation and subtraction that allocates no device memory.
+ *
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc or
+ * cudaFree (a pipeline living inside another framework's memory pool, a
+ * process with a device-memory budget fixed at start-up, a real-time loop that
+ * must not allocate or trigger the synchronisation an allocation can cause):
+ * the caller owns all buffers, the library's working memory is a fixed device
+ * array of about 13.2 MB that every GPU loading this library holds until the
+ * process exits.
+ *
+ * d_img (w*h floats) is the frame and d_sub (w*h) receives the background-
+ * subtracted frame; d_back and d_sigma (nbackx*nbacky floats) receive the
+ * filtered mesh maps; all four are device pointers.  stream is a
+ * cudaStream_t (NULL: the default stream).  sum (host, may be NULL) receives
+ * the global background, its rms and the thresholds, after which the call has
+ * synchronised the stream.  Results equal those of sexgpu_background.
+ *
+ * Limits: w, h <= 16384, nbackx*nbacky <= 16384, h*nbackx <= 1048576;
+ * larger frames return SEXGPU_ERR_NOALLOC_LIMIT.  The first call on a device
+ * looks up the array's device address (make that first call before any
+ * stream capture).  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
+int sexgpu_background_noalloc(const float *d_img, float *d_sub, int w, int h, const sexgpu_config *cfg,
+                              float *d_back, float *d_sigma, sexgpu_summary *sum, void *stream);
 
 /* Last CUDA error string of this context (empty if none). */
 const char *sexgpu_last_error(sexgpu_ctx *ctx);
