@@ -200,10 +200,8 @@ def run_gpu(args):
     clk = clocks.stop()
 
     # max over ranks
-    if dist:
-        t = torch.tensor([t_dev, t_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_dev, t_e2e = float(t[0]), float(t[1])
+    import multiframe
+    t_dev, t_e2e = multiframe.max_over_ranks([t_dev, t_e2e], dist, dev)
     ms_dev = t_dev / args.steps
     ms_e2e = t_e2e / args.steps
     frames_dev = world * args.steps / (t_dev / 1e3)

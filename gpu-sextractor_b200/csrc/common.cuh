@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #define SX_BIG 1e+30
+// blank (NaN) input pixels read as -BIG, like the FITS reader's blank value
+__device__ __forceinline__ float sx_unblank(float v) { return v != v ? -1e+30f : v; }
 #define SX_PI 3.1415926535898
 #define SX_EPS (1e-4)
 #define SX_BACK_MINGOODFRAC 0.5
@@ -154,11 +156,57 @@ __device__ __forceinline__ XSum xs_shfl_down(const XSum &s, int off) {
     return r;
 }
 
-// full-warp reduction; the result is valid in lane 0
-__device__ __forceinline__ XSum xs_warp_reduce(XSum s) {
+// full-warp reduction by a merge tree; the result is valid in lane 0
+__device__ __noinline__ XSum xs_warp_reduce_tree(XSum s) {
     for (int off = 16; off > 0; off >>= 1) xs_merge(s, xs_shfl_down(s, off));
     return s;
 }
+
+// Full-warp exact sum, valid in every lane.  Every lane's value is brought to
+// the warp's smallest exponent; when each then fits in 122 bits the 32 of them
+// add in an int128 without overflow (a butterfly of plain integer adds).
+// Otherwise the merge tree above decides, with its range check.  The exact
+// value, and so every rounding of it, is the same either way.
+__device__ __forceinline__ XSum xs_warp_sum(XSum s) {
+    int emin = s.e;
+    for (int o = 16; o > 0; o >>= 1) emin = min(emin, __shfl_xor_sync(0xffffffffu, emin, o));
+    int ovf = __any_sync(0xffffffffu, s.ovf);
+    XSum r;
+    r.e = emin;
+    r.ovf = ovf;
+    r.v = 0;
+    if (emin == XS_EMPTY) return r;
+    bool fits = true;
+    __int128 v = 0;
+    if (s.e != XS_EMPTY && s.v != 0) {
+        int sh = s.e - emin;
+        if (sh > 122 || xs_bits(s.v) + sh > 122)
+            fits = false;
+        else
+            v = (__int128)((unsigned __int128)s.v << sh);
+    }
+    if (__all_sync(0xffffffffu, fits)) {
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long lo = (unsigned long long)v, hi = (unsigned long long)(v >> 64);
+            lo = __shfl_xor_sync(0xffffffffu, lo, o);
+            hi = __shfl_xor_sync(0xffffffffu, hi, o);
+            v += (__int128)(((unsigned __int128)hi << 64) | lo);
+        }
+        r.v = v;
+        return r;
+    }
+    s = xs_warp_reduce_tree(s);
+    unsigned long long lo = (unsigned long long)s.v, hi = (unsigned long long)(s.v >> 64);
+    lo = __shfl_sync(0xffffffffu, lo, 0);
+    hi = __shfl_sync(0xffffffffu, hi, 0);
+    r.v = (__int128)(((unsigned __int128)hi << 64) | lo);
+    r.e = __shfl_sync(0xffffffffu, s.e, 0);
+    r.ovf = __shfl_sync(0xffffffffu, s.ovf, 0);
+    return r;
+}
+
+// the same, for callers that read the result in lane 0 only
+__device__ __forceinline__ XSum xs_warp_reduce(XSum s) { return xs_warp_sum(s); }
 
 // ---------------------------------------------------------------------------
 // Fixed-scale exact accumulators usable with atomics: value =
@@ -221,6 +269,29 @@ __device__ __forceinline__ unsigned int f2ord(float f) {
 __device__ __forceinline__ float ord2f(unsigned int o) {
     unsigned int u = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
     return __uint_as_float(u);
+}
+
+// Division of a pixel index by the frame width without the integer divide:
+// q = floor(p * m / 2^64) with m = ceil(2^64 / d) is exact whenever
+// p * d < 2^64, which holds for any 32-bit p and d.  d == 1 is m == 0.
+struct FastDiv {
+    unsigned long long m;
+    unsigned d;
+};
+inline FastDiv make_fastdiv(unsigned d) {
+    FastDiv f;
+    f.d = d;
+    f.m = d > 1 ? (~0ull) / d + 1 : 0ull;
+    return f;
+}
+__device__ __forceinline__ FastDiv make_fastdiv_dev(unsigned d) {
+    FastDiv f;
+    f.d = d;
+    f.m = d > 1 ? (~0ull) / d + 1 : 0ull;
+    return f;
+}
+__device__ __forceinline__ unsigned fdiv(unsigned p, const FastDiv &f) {
+    return f.m ? (unsigned)__umul64hi((unsigned long long)p, f.m) : p;
 }
 
 __device__ __forceinline__ int fexpo(float v) { return (int)((__float_as_uint(v) >> 23) & 0xff) - 127; }

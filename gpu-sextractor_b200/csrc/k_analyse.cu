@@ -3,7 +3,8 @@
 // (src/cuda/cudaanalyse.cu:1906-2124) and examineiso (:2176-2581).
 //
 // One warp per object walks the object's pixel list (contiguous, raster
-// order).  Sums that feed decisions or integer outputs are exact (XSum);
+// order), in two kernels: the robust preanalysis, whose moments examineiso
+// reads, then examineiso itself.  Sums that feed decisions or integer outputs are exact (XSum);
 // the double sums of the position errors and of the FWHM fit are reduced in
 // a fixed lane order.
 #include "common.cuh"
@@ -38,40 +39,49 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
-__device__ __forceinline__ XSum xs_warp_all(XSum s) {
-    s = xs_warp_reduce(s);
-    unsigned long long lo = (unsigned long long)s.v, hi = (unsigned long long)(s.v >> 64);
-    lo = __shfl_sync(0xffffffffu, lo, 0);
-    hi = __shfl_sync(0xffffffffu, hi, 0);
-    s.v = (__int128)(((unsigned __int128)hi << 64) | lo);
-    s.e = __shfl_sync(0xffffffffu, s.e, 0);
-    s.ovf = __shfl_sync(0xffffffffu, s.ovf, 0);
-    return s;
-}
+__device__ __forceinline__ XSum xs_warp_all(XSum s) { return xs_warp_sum(s); }
 
-// k-th smallest (0-based) of n positive floats given as bits; warp-wide
+// k-th smallest (0-based) of the cd values of n pixels, as float bits; the
+// values are positive (object pixels lie above the detection threshold), so
+// their bit patterns sort like the values.  Four 8-bit radix passes; in each
+// pass the digit that holds rank k is found by a warp scan over 256 bins
+// (lane l owns bins 8l..8l+7).
 __device__ unsigned warp_select(const unsigned *opix, int n, const float *cd, int k, unsigned *hist) {
-    int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
     unsigned prefix = 0, mask = 0;
     for (int shift = 24; shift >= 0; shift -= 8) {
         for (int i = lane; i < 256; i += 32) hist[i] = 0;
         __syncwarp();
         for (int i = lane; i < n; i += 32) {
-            unsigned key = __float_as_uint(cd[opix[i]]);
+            unsigned key = __float_as_uint(__ldg(cd + __ldg(opix + i)));
             if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255], 1u);
         }
         __syncwarp();
-        unsigned digit = 0, below = 0;
-        if (lane == 0) {
-            unsigned c = 0;
-            for (digit = 0; digit < 255; digit++) {
-                if (c + hist[digit] > (unsigned)k) break;
-                c += hist[digit];
-            }
-            below = c;
+        const uint4 h0 = reinterpret_cast<const uint4 *>(hist)[lane * 2];
+        const uint4 h1 = reinterpret_cast<const uint4 *>(hist)[lane * 2 + 1];
+        const unsigned c[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+        unsigned tot = c[0] + c[1] + c[2] + c[3] + c[4] + c[5] + c[6] + c[7];
+        unsigned incl = tot;
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
         }
-        digit = __shfl_sync(0xffffffffu, digit, 0);
-        below = __shfl_sync(0xffffffffu, below, 0);
+        unsigned excl = incl - tot;
+        unsigned sel = __ballot_sync(0xffffffffu, incl > (unsigned)k);
+        int owner = __ffs(sel) - 1;  // k < n, so some lane holds rank k
+        unsigned digit = 0, below = excl;
+        if (lane == owner) {
+            int j = 0;
+#pragma unroll
+            for (int t = 0; t < 7; t++)
+                if (j == t && below + c[t] <= (unsigned)k) {
+                    below += c[t];
+                    j = t + 1;
+                }
+            digit = lane * 8 + j;
+        }
+        digit = __shfl_sync(0xffffffffu, digit, owner);
+        below = __shfl_sync(0xffffffffu, below, owner);
         prefix |= digit << shift;
         mask |= 255u << shift;
         k -= (int)below;
@@ -86,149 +96,155 @@ struct AnaArgs {
     ObjBufs O;
     FrameScalars *sc;
     int w, h, nbx, nby, bw, bh, nobj, minarea, clean_flag;
+    FastDiv wdiv;
     double gain, satur;
 };
 
-__global__ void __launch_bounds__(AN_WARPS * 32) k_analyse(AnaArgs A) {
-    __shared__ unsigned hist[AN_WARPS][256];
+// Robust preanalysis of a deblended object over its final pixels
+// (src/cuda/cudaanalyse.cu:1906-2124); objects of level 0 kept the values of
+// the first preanalysis.
+__global__ void __launch_bounds__(AN_WARPS * 32) k_analyse_robust(AnaArgs A) {
+    const int lane = threadIdx.x & 31;
+    const int o = blockIdx.x * AN_WARPS + (threadIdx.x >> 5);
+    if (o >= A.nobj || A.O.level[o] == 0) return;
+    const int n = A.O.n[o], off = A.O.off[o], w = A.w, h = A.h;
+    const unsigned *pix = A.opix + off;
+    const float dthresh = A.sc->dthresh;
+    int flags = A.O.flags[o];
+
+    XSum srv;
+    xs_init(srv);
+    unsigned pk = 0u, cpk = 0u;
+    int xmin = 0x7fffffff, xmax = -1, ymin = 0x7fffffff, ymax = -1;
+    for (int i = lane; i < n; i += 32) {
+        unsigned p = __ldg(pix + i);
+        int y = (int)fdiv(p, A.wdiv), x = (int)p - y * w;
+        pk = max(pk, f2ord(__ldg(A.sub + p)));
+        float c = __ldg(A.cd + p);
+        cpk = max(cpk, f2ord(c));
+        xs_add(srv, c);
+        xmin = min(xmin, x);
+        xmax = max(xmax, x);
+        ymin = min(ymin, y);
+        ymax = max(ymax, y);
+    }
+    srv = xs_warp_sum(srv);
+    float peak = ord2f(warp_max_u(pk)), cpeak = ord2f(warp_max_u(cpk));
+    xmin = warp_min_i(xmin);
+    xmax = warp_max_i(xmax);
+    ymin = warp_min_i(ymin);
+    ymax = warp_max_i(ymax);
+    if (xmin == 0 || xmax == w - 1 || ymin == 0 || ymax == h - 1) flags |= SX_OBJ_TRUNC;
+    float rv = xs_float(srv);
+    double dth = dthresh, dthresh2 = (dth + peak) / 2.0;
+    XSum stv, smx, smy, smx2, smy2, smxy;
+    xs_init(stv);
+    xs_init(smx);
+    xs_init(smy);
+    xs_init(smx2);
+    xs_init(smy2);
+    xs_init(smxy);
+    int dnpix = 0, area2 = 0;
+    for (int i = lane; i < n; i += 32) {
+        unsigned p = __ldg(pix + i);
+        int yy = (int)fdiv(p, A.wdiv), x = (int)p - yy * w - xmin, y = yy - ymin;
+        float cval = __ldg(A.cd + p), val = __ldg(A.sub + p);
+        xs_add(stv, val);
+        dnpix += val > dth;
+        area2 += val > dthresh2;
+        xs_add(smx, cval * x);
+        xs_add(smy, cval * y);
+        xs_add(smx2, cval * x * x);
+        xs_add(smy2, cval * y * y);
+        xs_add(smxy, cval * x * y);
+    }
+    stv = xs_warp_sum(stv);
+    smx = xs_warp_sum(smx);
+    smy = xs_warp_sum(smy);
+    smx2 = xs_warp_sum(smx2);
+    smy2 = xs_warp_sum(smy2);
+    smxy = xs_warp_sum(smxy);
+    dnpix = warp_sum_i(dnpix);
+    area2 = warp_sum_i(area2);
+    if (lane != 0) return;
+    if (srv.ovf | stv.ovf | smx.ovf | smy.ovf | smx2.ovf | smy2.ovf | smxy.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
+    double mxo = A.O.mx[o], myo = A.O.my[o];
+    double rvd = rv, mx = xs_double(smx), my = xs_double(smy);
+    double mx2 = xs_double(smx2), my2 = xs_double(smy2), mxy = xs_double(smxy);
+    double xm = mx / rvd, ym = my / rvd, xm2, ym2, xym;
+    if (flags & SX_OBJ_MERGED) {
+        double xn = mxo - xmin, yn = myo - ymin;
+        xm2 = mx2 / rvd + xn * xn - 2 * xm * xn;
+        ym2 = my2 / rvd + yn * yn - 2 * ym * yn;
+        xym = mxy / rvd + xn * yn - xm * yn - xn * ym;
+        xm = xn;
+        ym = yn;
+    } else {
+        xm2 = mx2 / rvd - xm * xm;
+        ym2 = my2 / rvd - ym * ym;
+        xym = mxy / rvd - xm * ym;
+    }
+    double temp, temp2, theta, pmx2, pmy2, darea, t1t2;
+    int singu = 0;
+    if ((temp2 = xm2 * ym2 - xym * xym) < 0.00694) {
+        xm2 += 0.0833333;
+        ym2 += 0.0833333;
+        temp2 = xm2 * ym2 - xym * xym;
+        singu = 1;
+    }
+    if ((fabs(temp = xm2 - ym2)) > 0.0)
+        theta = atan2(2.0 * xym, temp) / 2.0;
+    else
+        theta = SX_PI / 4.0;
+    temp = sqrt(0.25 * temp * temp + xym * xym);
+    pmy2 = pmx2 = 0.5 * (xm2 + ym2);
+    pmx2 += temp;
+    pmy2 -= temp;
+    float a = (float)sqrt(pmx2), b = (float)sqrt(pmy2);
+    float abcor;
+    darea = (double)area2 - dnpix;
+    t1t2 = dth / dthresh2;
+    if (t1t2 > 0.0) {
+        abcor = (darea < 0.0 ? darea : -1.0) / (2 * SX_PI * log(t1t2 < 1.0 ? t1t2 : 0.99) * a * b);
+        if (abcor > 1.0) abcor = 1.0;
+    } else
+        abcor = 1.0;
+    A.O.flags[o] = flags;
+    A.O.singu[o] = singu;
+    A.O.xmin[o] = xmin;
+    A.O.xmax[o] = xmax;
+    A.O.ymin[o] = ymin;
+    A.O.ymax[o] = ymax;
+    A.O.fdflux[o] = rv;
+    A.O.fdpeak[o] = cpeak;
+    A.O.dpeak[o] = peak;
+    A.O.dnpix[o] = dnpix;
+    A.O.dflux[o] = xs_float(stv);
+    A.O.mx[o] = xm + xmin;
+    A.O.my[o] = ym + ymin;
+    A.O.mx2[o] = xm2;
+    A.O.my2[o] = ym2;
+    A.O.mxy[o] = xym;
+    A.O.a[o] = a;
+    A.O.b[o] = b;
+    A.O.theta[o] = theta * 180.0 / SX_PI;
+    A.O.cxx[o] = (float)(ym2 / temp2);
+    A.O.cyy[o] = (float)(xm2 / temp2);
+    A.O.cxy[o] = (float)(-2 * xym / temp2);
+    A.O.abcor[o] = abcor;
+}
+
+// examineiso (src/cuda/cudaanalyse.cu:2176-2581) and the CLEAN threshold
+// mthresh of every object.
+__global__ void __launch_bounds__(AN_WARPS * 32) k_examineiso(AnaArgs A) {
+    __shared__ __align__(16) unsigned hist[AN_WARPS][256];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int o = blockIdx.x * AN_WARPS + wid;
     if (o >= A.nobj) return;
-    const int n = A.O.n[o], off = A.O.off[o], w = A.w, h = A.h;
+    const int n = A.O.n[o], off = A.O.off[o], w = A.w;
     const unsigned *pix = A.opix + off;
     const float dthresh = A.sc->dthresh, thresh = A.sc->thresh, backsig = A.sc->backsig;
-    int flags = A.O.flags[o];
-    int singu = A.O.singu[o];
-    double mxo = A.O.mx[o], myo = A.O.my[o];
-    float a = A.O.a[o], b = A.O.b[o], fdflux = A.O.fdflux[o];
-
-    // ---------------- robust preanalysis (deblended objects only)
-    if (A.O.level[o] > 0) {
-        XSum srv;
-        xs_init(srv);
-        unsigned pk = 0u, cpk = 0u;
-        int xmin = 0x7fffffff, xmax = -1, ymin = 0x7fffffff, ymax = -1;
-        for (int i = lane; i < n; i += 32) {
-            int p = (int)pix[i], x = p % w, y = p / w;
-            pk = max(pk, f2ord(A.sub[p]));
-            float c = A.cd[p];
-            cpk = max(cpk, f2ord(c));
-            xs_add(srv, c);
-            xmin = min(xmin, x);
-            xmax = max(xmax, x);
-            ymin = min(ymin, y);
-            ymax = max(ymax, y);
-        }
-        srv = xs_warp_all(srv);
-        float peak = ord2f(warp_max_u(pk)), cpeak = ord2f(warp_max_u(cpk));
-        xmin = warp_min_i(xmin);
-        xmax = warp_max_i(xmax);
-        ymin = warp_min_i(ymin);
-        ymax = warp_max_i(ymax);
-        if (xmin == 0 || xmax == w - 1 || ymin == 0 || ymax == h - 1) flags |= SX_OBJ_TRUNC;
-        float rv = xs_float(srv);
-        double dth = dthresh, dthresh2 = (dth + peak) / 2.0;
-        XSum stv, smx, smy, smx2, smy2, smxy;
-        xs_init(stv);
-        xs_init(smx);
-        xs_init(smy);
-        xs_init(smx2);
-        xs_init(smy2);
-        xs_init(smxy);
-        int dnpix = 0, area2 = 0;
-        for (int i = lane; i < n; i += 32) {
-            int p = (int)pix[i], x = p % w - xmin, y = p / w - ymin;
-            float cval = A.cd[p], val = A.sub[p];
-            xs_add(stv, val);
-            dnpix += val > dth;
-            area2 += val > dthresh2;
-            xs_add(smx, cval * x);
-            xs_add(smy, cval * y);
-            xs_add(smx2, cval * x * x);
-            xs_add(smy2, cval * y * y);
-            xs_add(smxy, cval * x * y);
-        }
-        stv = xs_warp_all(stv);
-        smx = xs_warp_all(smx);
-        smy = xs_warp_all(smy);
-        smx2 = xs_warp_all(smx2);
-        smy2 = xs_warp_all(smy2);
-        smxy = xs_warp_all(smxy);
-        dnpix = warp_sum_i(dnpix);
-        area2 = warp_sum_i(area2);
-        if (srv.ovf | stv.ovf | smx.ovf | smy.ovf | smx2.ovf | smy2.ovf | smxy.ovf)
-            if (lane == 0) atomicOr(&A.sc->status, SX_ST_RANGE);
-        double rvd = rv, mx = xs_double(smx), my = xs_double(smy);
-        double mx2 = xs_double(smx2), my2 = xs_double(smy2), mxy = xs_double(smxy);
-        double xm = mx / rvd, ym = my / rvd, xm2, ym2, xym;
-        if (flags & SX_OBJ_MERGED) {
-            double xn = mxo - xmin, yn = myo - ymin;
-            xm2 = mx2 / rvd + xn * xn - 2 * xm * xn;
-            ym2 = my2 / rvd + yn * yn - 2 * ym * yn;
-            xym = mxy / rvd + xn * yn - xm * yn - xn * ym;
-            xm = xn;
-            ym = yn;
-        } else {
-            xm2 = mx2 / rvd - xm * xm;
-            ym2 = my2 / rvd - ym * ym;
-            xym = mxy / rvd - xm * ym;
-        }
-        double temp, temp2, theta, pmx2, pmy2, darea, t1t2;
-        singu = 0;
-        if ((temp2 = xm2 * ym2 - xym * xym) < 0.00694) {
-            xm2 += 0.0833333;
-            ym2 += 0.0833333;
-            temp2 = xm2 * ym2 - xym * xym;
-            singu = 1;
-        }
-        if ((fabs(temp = xm2 - ym2)) > 0.0)
-            theta = atan2(2.0 * xym, temp) / 2.0;
-        else
-            theta = SX_PI / 4.0;
-        temp = sqrt(0.25 * temp * temp + xym * xym);
-        pmy2 = pmx2 = 0.5 * (xm2 + ym2);
-        pmx2 += temp;
-        pmy2 -= temp;
-        a = (float)sqrt(pmx2);
-        b = (float)sqrt(pmy2);
-        float abcor;
-        darea = (double)area2 - dnpix;
-        t1t2 = dth / dthresh2;
-        if (t1t2 > 0.0) {
-            abcor = (darea < 0.0 ? darea : -1.0) / (2 * SX_PI * log(t1t2 < 1.0 ? t1t2 : 0.99) * a * b);
-            if (abcor > 1.0) abcor = 1.0;
-        } else
-            abcor = 1.0;
-        mxo = xm + xmin;
-        myo = ym + ymin;
-        fdflux = rv;
-        if (lane == 0) {
-            A.O.xmin[o] = xmin;
-            A.O.xmax[o] = xmax;
-            A.O.ymin[o] = ymin;
-            A.O.ymax[o] = ymax;
-            A.O.fdflux[o] = rv;
-            A.O.fdpeak[o] = cpeak;
-            A.O.dpeak[o] = peak;
-            A.O.dnpix[o] = dnpix;
-            A.O.dflux[o] = xs_float(stv);
-            A.O.mx[o] = mxo;
-            A.O.my[o] = myo;
-            A.O.mx2[o] = xm2;
-            A.O.my2[o] = ym2;
-            A.O.mxy[o] = xym;
-            A.O.a[o] = a;
-            A.O.b[o] = b;
-            A.O.theta[o] = theta * 180.0 / SX_PI;
-            A.O.cxx[o] = (float)(ym2 / temp2);
-            A.O.cyy[o] = (float)(xm2 / temp2);
-            A.O.cxy[o] = (float)(-2 * xym / temp2);
-            A.O.abcor[o] = abcor;
-        }
-    }
-
-    // ---------------- examineiso (cudaanalyse.cu:2176-2581)
-    float bkg = back_at(A.back, A.nbx, A.nby, A.bw, A.bh, (int)(mxo + 0.5), (int)(myo + 0.5));
+    const double mxo = A.O.mx[o], myo = A.O.my[o];
     double dbacknoise2 = backsig * backsig, var = backsig * backsig;
     unsigned pk = 0u;
     unsigned long long best = 0ull;
@@ -237,11 +253,12 @@ __global__ void __launch_bounds__(AN_WARPS * 32) k_analyse(AnaArgs A) {
     xs_init(stv);
     double esum = 0, emx2 = 0, emy2 = 0, emxy = 0;
     for (int i = lane; i < n; i += 32) {
-        int p = (int)pix[i], ix = p % w, iy = p / w;
-        float pv = A.sub[p], cdpix = A.cd[p];
+        unsigned p = __ldg(pix + i);
+        int iy = (int)fdiv(p, A.wdiv), ix = (int)p - iy * w;
+        float pv = __ldg(A.sub + p), cdpix = __ldg(A.cd + p);
         pk = max(pk, f2ord(pv));
         // first maximum of cd in raster order: max cd, then smallest index
-        unsigned long long key = ((unsigned long long)f2ord(cdpix) << 32) | (unsigned)(0xffffffffu - (unsigned)p);
+        unsigned long long key = ((unsigned long long)f2ord(cdpix) << 32) | (unsigned)(0xffffffffu - p);
         best = max(best, key);
         area += pv > thresh;
         xs_add(stv, pv);
@@ -256,17 +273,67 @@ __global__ void __launch_bounds__(AN_WARPS * 32) k_analyse(AnaArgs A) {
     float peak = ord2f(warp_max_u(pk));
     best = warp_max_ull(best);
     area = warp_sum_i(area);
-    stv = xs_warp_all(stv);
+    stv = xs_warp_sum(stv);
     esum = warp_sum_d(esum);
     emx2 = warp_sum_d(emx2);
     emy2 = warp_sum_d(emy2);
     emxy = warp_sum_d(emxy);
-    int peakpix = (int)(0xffffffffu - (unsigned)(best & 0xffffffffu));
     float mthresh = 0.0f;
     if (A.clean_flag && n >= A.minarea) {
         unsigned kbits = warp_select(pix, n, A.cd, n - A.minarea, hist[wid]);
         mthresh = __uint_as_float(kbits) - dthresh;
     }
+    // isophotal thresholds: lane k < 8 evaluates threshold k, every lane reads all
+    float othresh = thresh - 0.0f;
+    float opeak = peak - 0.0f;
+    float tk = 0.0f;
+    if (opeak > 0.0 && othresh > 0.0 && lane < SX_NISO_)
+        tk = othresh * pow((double)opeak / othresh, (double)lane / SX_NISO_);
+    float threshs[SX_NISO_];
+#pragma unroll
+    for (int k = 0; k < SX_NISO_; k++) threshs[k] = __shfl_sync(0xffffffffu, tk, k);
+    int iso[SX_NISO_];
+#pragma unroll
+    for (int k = 0; k < SX_NISO_; k++) iso[k] = 0;
+    float thresh0 = opeak / 5.0;
+    if (thresh0 < othresh) thresh0 = othresh;
+    double s = 0, sx = 0, sy = 0, sxx = 0, sxy = 0;
+    double sat = (double)(A.satur - 0.0);
+    for (int i = lane; i < n; i += 32) {
+        unsigned p = __ldg(pix + i);
+        float v = __ldg(A.sub + p);
+        bool go = true;
+#pragma unroll
+        for (int k = 0; k < SX_NISO_; k++) {
+            go = go && v > threshs[k];
+            iso[k] += go;
+        }
+        double pv = v - 0.0;
+        if (thresh0 > 0.0 && pv > thresh0 && pv < sat) {
+            int iy = (int)fdiv(p, A.wdiv), ix = (int)p - iy * w;
+            double dx = ix - mxo, dy = iy - myo;
+            double lpix = log(pv);
+            double inverr2 = pv * pv;
+            s += inverr2;
+            double d2 = dx * dx + dy * dy;
+            sx += d2 * inverr2;
+            sxx += d2 * d2 * inverr2;
+            sy += lpix * inverr2;
+            sxy += lpix * d2 * inverr2;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < SX_NISO_; k++) iso[k] = warp_sum_i(iso[k]);
+    s = warp_sum_d(s);
+    sx = warp_sum_d(sx);
+    sy = warp_sum_d(sy);
+    sxx = warp_sum_d(sxx);
+    sxy = warp_sum_d(sxy);
+    if (lane != 0) return;
+    const int singu = A.O.singu[o];
+    const float fdflux = A.O.fdflux[o], a = A.O.a[o], b = A.O.b[o];
+    float bkg = back_at(A.back, A.nbx, A.nby, A.bw, A.bh, (int)(mxo + 0.5), (int)(myo + 0.5));
+    int peakpix = (int)(0xffffffffu - (unsigned)(best & 0xffffffffu));
     {
         double flux2 = fdflux * fdflux;
         emx2 /= flux2;
@@ -281,42 +348,6 @@ __global__ void __launch_bounds__(AN_WARPS * 32) k_analyse(AnaArgs A) {
     double tvd = xs_double(stv);
     double sigtv = (double)n * var;
     if (A.gain > 0.0 && tvd > 0.0) sigtv += tvd / A.gain;
-    float othresh = thresh - 0.0f;
-    float opeak = peak - 0.0f;
-    float threshs[SX_NISO_];
-    if (opeak > 0.0 && othresh > 0.0)
-        for (int i = 0; i < SX_NISO_; i++) threshs[i] = othresh * pow((double)opeak / othresh, (double)i / SX_NISO_);
-    else
-        for (int i = 0; i < SX_NISO_; i++) threshs[i] = 0.0;
-    int iso[SX_NISO_];
-    for (int i = 0; i < SX_NISO_; i++) iso[i] = 0;
-    float thresh0 = opeak / 5.0;
-    if (thresh0 < othresh) thresh0 = othresh;
-    double s = 0, sx = 0, sy = 0, sxx = 0, sxy = 0;
-    double sat = (double)(A.satur - 0.0);
-    for (int i = lane; i < n; i += 32) {
-        int p = (int)pix[i];
-        float v = A.sub[p];
-        for (int k = 0; k < SX_NISO_ && v > threshs[k]; k++) iso[k]++;
-        double pv = v - 0.0;
-        if (thresh0 > 0.0 && pv > thresh0 && pv < sat) {
-            double dx = p % w - mxo, dy = p / w - myo;
-            double lpix = log(pv);
-            double inverr2 = pv * pv;
-            s += inverr2;
-            double d2 = dx * dx + dy * dy;
-            sx += d2 * inverr2;
-            sxx += d2 * d2 * inverr2;
-            sy += lpix * inverr2;
-            sxy += lpix * d2 * inverr2;
-        }
-    }
-    for (int k = 0; k < SX_NISO_; k++) iso[k] = warp_sum_i(iso[k]);
-    s = warp_sum_d(s);
-    sx = warp_sum_d(sx);
-    sy = warp_sum_d(sy);
-    sxx = warp_sum_d(sxx);
-    sxy = warp_sum_d(sxy);
     float fwhm = 0.0f;
     if (thresh0 > 0.0) {
         double d = s * sxx - sx * sx;
@@ -327,29 +358,30 @@ __global__ void __launch_bounds__(AN_WARPS * 32) k_analyse(AnaArgs A) {
             if (fwhm > 0.0) fwhm -= 1 / (4 * fwhm);
         }
     }
-    if (lane == 0) {
-        A.O.flags[o] = flags;
-        A.O.singu[o] = singu;
-        A.O.bkg[o] = bkg;
-        A.O.peak[o] = opeak;
-        A.O.peakx[o] = peakpix % w + 1;
-        A.O.peaky[o] = peakpix / w + 1;
-        A.O.npix[o] = area;
-        A.O.flux[o] = tvd;
-        A.O.fluxerr[o] = sigtv;
-        A.O.mthresh[o] = mthresh;
-        A.O.pmx2[o] = emx2;
-        A.O.pmy2[o] = emy2;
-        A.O.pmxy[o] = emxy;
-        A.O.fwhm[o] = fwhm;
-        A.O.fdnpix[o] = n;
-        for (int k = 0; k < SX_NISO_; k++) A.O.iso[(size_t)o * SX_NISO_ + k] = iso[k];
-        if (stv.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
-    }
+    int py = (int)fdiv((unsigned)peakpix, A.wdiv);
+    A.O.bkg[o] = bkg;
+    A.O.peak[o] = opeak;
+    A.O.peakx[o] = peakpix - py * w + 1;
+    A.O.peaky[o] = py + 1;
+    A.O.npix[o] = area;
+    A.O.flux[o] = tvd;
+    A.O.fluxerr[o] = sigtv;
+    A.O.mthresh[o] = mthresh;
+    A.O.pmx2[o] = emx2;
+    A.O.pmy2[o] = emy2;
+    A.O.pmxy[o] = emxy;
+    A.O.fwhm[o] = fwhm;
+    A.O.fdnpix[o] = n;
+#pragma unroll
+    for (int k = 0; k < SX_NISO_; k++) A.O.iso[(size_t)o * SX_NISO_ + k] = iso[k];
+    if (stv.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
 }
 
 void launch_analyse(const AnaArgs &A, cudaStream_t st) {
-    if (A.nobj > 0) k_analyse<<<(A.nobj + AN_WARPS - 1) / AN_WARPS, AN_WARPS * 32, 0, st>>>(A);
+    if (A.nobj <= 0) return;
+    const unsigned grid = (A.nobj + AN_WARPS - 1) / AN_WARPS;
+    k_analyse_robust<<<grid, AN_WARPS * 32, 0, st>>>(A);
+    k_examineiso<<<grid, AN_WARPS * 32, 0, st>>>(A);
 }
 
 }  // namespace sx

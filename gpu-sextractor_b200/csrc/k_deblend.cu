@@ -91,14 +91,15 @@ __device__ __forceinline__ void activate_and_union(const DebArgs &A, int off, in
 }
 
 // first sweep: branch tree, MINCONT pruning, kept branches
-__global__ void __launch_bounds__(DB_THREADS) k_deblend_sweep(DebArgs A) {
+__global__ void __launch_bounds__(DB_THREADS) k_deblend_sweep(DebArgs A, const int *roots, const int *nroots) {
+    if ((int)blockIdx.x >= *nroots) return;
     __shared__ float thr[DB_MAXLEV];
     __shared__ int lvcnt[DB_MAXLEV + 1], lvstart[DB_MAXLEV + 1], lvcur[DB_MAXLEV];
     __shared__ int s_nrl[2], s_nn[2], s_nkept;
     __shared__ unsigned s_peak;
     __shared__ XSum s_part[DB_THREADS / 32];
     __shared__ float s_fdflux;
-    const int r = blockIdx.x, off = A.R.off[r], P = A.R.size[r];
+    const int r = roots[blockIdx.x], off = A.R.off[r], P = A.R.size[r];
     const unsigned *pix = A.rpix + off;
     int *par = A.D.par + off, *lev = A.D.lev + off, *sz = A.D.sz + off, *order = A.D.order + off;
     unsigned long long *acc = A.D.acc + (size_t)off * 4;
@@ -146,7 +147,7 @@ __global__ void __launch_bounds__(DB_THREADS) k_deblend_sweep(DebArgs A) {
     __syncthreads();
     if (threadIdx.x == 0) {
         XSum t = s_part[0];
-        for (int k = 1; k < DB_THREADS / 32; k++) xs_merge(t, s_part[k]);
+        for (int k = 1; k < (int)(blockDim.x >> 5); k++) xs_merge(t, s_part[k]);
         if (t.ovf) atomicOr(status, SX_ST_RANGE);
         s_fdflux = xs_float(t);
         A.R.fdflux[r] = s_fdflux;
@@ -303,18 +304,17 @@ __device__ __forceinline__ void lacc_add(unsigned long long *a, float f, int e0,
     limbs_atomic_add_term(a, f, e0, status);
 }
 
-__global__ void __launch_bounds__(DB_THREADS) k_deblend_assign(DebArgs A) {
+__global__ void __launch_bounds__(DB_THREADS) k_deblend_assign(DebArgs A, const int *roots, const int *nroots) {
+    if ((int)blockIdx.x >= *nroots) return;
     __shared__ float thr[DB_MAXLEV];
     __shared__ int lvcnt[DB_MAXLEV + 1], lvstart[DB_MAXLEV + 1], lvkept[DB_MAXLEV];
-    const int r = blockIdx.x, off = A.R.off[r], P = A.R.size[r], K = A.R.nkept[r], ob = A.R.objbase[r];
+    const int r = roots[blockIdx.x], off = A.R.off[r], P = A.R.size[r], K = A.R.nkept[r], ob = A.R.objbase[r];
     const unsigned *pix = A.rpix + off;
     int *par = A.D.par + off, *lev = A.D.lev + off, *order = A.D.order + off;
     int *own = A.D.own + off, *kl = A.D.kl + off, *kidx = A.D.kidx + off;
     unsigned long long *kept = A.D.kept + off;
     unsigned long long *kept2 = A.D.acc + (size_t)off * 4;  // this root's acc is free now: sorted kept list
-    unsigned long long *pacc = A.D.pacc + (size_t)off * 28;
     int *pint = A.D.pint + (size_t)off * 8;
-    const int e0 = A.sc->e0cd, e0s = A.sc->e0sub;
     int *status = &A.sc->status;
     const float fdpeak = A.R.fdpeak[r];
     block_thresholds(A, fdpeak, thr);
@@ -342,13 +342,6 @@ __global__ void __launch_bounds__(DB_THREADS) k_deblend_assign(DebArgs A) {
         kl[c] = L;
         kidx[c] = i;
         atomicAdd(&lvkept[L], 1);
-        unsigned long long *pa = pacc + (size_t)i * 28;
-        for (int q = 0; q < 28; q++) pa[q] = 0ull;
-        int *pi = pint + (size_t)i * 8;
-        pi[PI_XMIN] = pi[PI_YMIN] = 0x7fffffff;
-        pi[PI_XMAX] = pi[PI_YMAX] = -1;
-        pi[PI_PEAK] = pi[PI_CPEAK] = 0;
-        pi[PI_DNPIX] = pi[PI_AREA2] = 0;
     }
     if (threadIdx.x == 0) {
         int s = 0;
@@ -371,64 +364,97 @@ __global__ void __launch_bounds__(DB_THREADS) k_deblend_assign(DebArgs A) {
             __syncthreads();
         }
     }
-    // preanalysis of each kept branch over its own pixels (cudaanalyse.cu:1686-1903)
-    for (int e = threadIdx.x; e < P; e += blockDim.x) {
-        int k = own[e];
-        if (k < 0) continue;
-        int p = (int)pix[e], x = p % A.w, y = p / A.w;
-        int *pi = pint + (size_t)k * 8;
-        atomicMin(&pi[PI_XMIN], x);
-        atomicMax(&pi[PI_XMAX], x);
-        atomicMin(&pi[PI_YMIN], y);
-        atomicMax(&pi[PI_YMAX], y);
-        atomicMax((unsigned *)&pi[PI_PEAK], f2ord(A.sub[p]));
-        float c = A.cd[p];
-        atomicMax((unsigned *)&pi[PI_CPEAK], f2ord(c));
-        lacc_add(pacc + (size_t)k * 28 + PA_RV * 4, c, e0, status);
+    // preanalysis of each kept branch over its own pixels
+    // (cudaanalyse.cu:1686-1903).  The owned pixels are grouped by branch with
+    // a counting sort, then one warp reduces each branch with exact sums.
+    int *bcnt = pint, *bstart = pint + K, *bcur = pint + 2 * K, *blist = pint + 3 * K;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) bcnt[k] = bcur[k] = 0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < P; e += blockDim.x)
+        if (own[e] >= 0) atomicAdd(&bcnt[own[e]], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int k = 0; k < K; k++) {
+            bstart[k] = s;
+            s += bcnt[k];
+        }
     }
     __syncthreads();
     for (int e = threadIdx.x; e < P; e += blockDim.x) {
         int k = own[e];
-        if (k < 0) continue;
-        int L = (int)(kept2[k] >> 32);
-        int *pi = pint + (size_t)k * 8;
-        int p = (int)pix[e];
-        int x = p % A.w - pi[PI_XMIN], y = p / A.w - pi[PI_YMIN];
-        float cval = A.cd[p], val = A.sub[p];
-        double dthresh = thr[L];
-        float peak = ord2f((unsigned)pi[PI_PEAK]);
-        double dthresh2 = (dthresh + peak) / 2.0;
-        if (val > dthresh) atomicAdd(&pi[PI_DNPIX], 1);
-        if (val > dthresh2) atomicAdd(&pi[PI_AREA2], 1);
-        unsigned long long *pa = pacc + (size_t)k * 28;
-        lacc_add(pa + PA_MX * 4, cval * x, e0, status);
-        lacc_add(pa + PA_MY * 4, cval * y, e0, status);
-        lacc_add(pa + PA_MX2 * 4, cval * x * x, e0, status);
-        lacc_add(pa + PA_MY2 * 4, cval * y * y, e0, status);
-        lacc_add(pa + PA_MXY * 4, cval * x * y, e0, status);
-        lacc_add(pa + PA_TV * 4, val, e0s, status);
+        if (k >= 0) blist[bstart[k] + atomicAdd(&bcur[k], 1)] = e;
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < K; k += blockDim.x) {
-        int o = ob + k;
-        int L = (int)(kept2[k] >> 32);
-        int *pi = pint + (size_t)k * 8;
-        unsigned long long *pa = pacc + (size_t)k * 28;
-        int xmin = pi[PI_XMIN], xmax = pi[PI_XMAX], ymin = pi[PI_YMIN], ymax = pi[PI_YMAX];
+    const int lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    for (int k = threadIdx.x >> 5; k < K; k += nwarp) {
+        const int o = ob + k, L = (int)(kept2[k] >> 32), nb = bcnt[k], b0 = bstart[k];
+        int xmin = 0x7fffffff, xmax = -1, ymin = 0x7fffffff, ymax = -1;
+        unsigned pk = 0u, cpk = 0u;
+        XSum srv;
+        xs_init(srv);
+        for (int i = lane; i < nb; i += 32) {
+            int p = (int)pix[blist[b0 + i]], x = p % A.w, y = p / A.w;
+            xmin = min(xmin, x);
+            xmax = max(xmax, x);
+            ymin = min(ymin, y);
+            ymax = max(ymax, y);
+            pk = max(pk, f2ord(A.sub[p]));
+            float c = A.cd[p];
+            cpk = max(cpk, f2ord(c));
+            xs_add(srv, c);
+        }
+        for (int d = 16; d > 0; d >>= 1) {
+            xmin = min(xmin, __shfl_xor_sync(0xffffffffu, xmin, d));
+            xmax = max(xmax, __shfl_xor_sync(0xffffffffu, xmax, d));
+            ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, d));
+            ymax = max(ymax, __shfl_xor_sync(0xffffffffu, ymax, d));
+            pk = max(pk, __shfl_xor_sync(0xffffffffu, pk, d));
+            cpk = max(cpk, __shfl_xor_sync(0xffffffffu, cpk, d));
+        }
+        srv = xs_warp_reduce(srv);
+        const float peak = ord2f(pk);
+        const double dthresh = thr[L], dthresh2 = (dthresh + peak) / 2.0;
+        XSum smx, smy, smx2, smy2, smxy, stv;
+        xs_init(smx);
+        xs_init(smy);
+        xs_init(smx2);
+        xs_init(smy2);
+        xs_init(smxy);
+        xs_init(stv);
+        int dnpix = 0, area2 = 0;
+        for (int i = lane; i < nb; i += 32) {
+            int p = (int)pix[blist[b0 + i]];
+            int x = p % A.w - xmin, y = p / A.w - ymin;
+            float cval = A.cd[p], val = A.sub[p];
+            dnpix += val > dthresh;
+            area2 += val > dthresh2;
+            xs_add(smx, cval * x);
+            xs_add(smy, cval * y);
+            xs_add(smx2, cval * x * x);
+            xs_add(smy2, cval * y * y);
+            xs_add(smxy, cval * x * y);
+            xs_add(stv, val);
+        }
+        for (int d = 16; d > 0; d >>= 1) {
+            dnpix += __shfl_xor_sync(0xffffffffu, dnpix, d);
+            area2 += __shfl_xor_sync(0xffffffffu, area2, d);
+        }
+        smx = xs_warp_reduce(smx);
+        smy = xs_warp_reduce(smy);
+        smx2 = xs_warp_reduce(smx2);
+        smy2 = xs_warp_reduce(smy2);
+        smxy = xs_warp_reduce(smxy);
+        stv = xs_warp_reduce(stv);
+        if (lane != 0) continue;
+        if (srv.ovf | smx.ovf | smy.ovf | smx2.ovf | smy2.ovf | smxy.ovf | stv.ovf) atomicOr(status, SX_ST_RANGE);
         int flag = 0;
         if (L > 0) flag |= SX_OBJ_MERGED;
         if (xmin == 0 || xmax == A.w - 1 || ymin == 0 || ymax == A.h - 1) flag |= SX_OBJ_TRUNC;
-        float rv = xs_float(limbs_to_xsum(pa + PA_RV * 4, e0));
+        float rv = xs_float(srv);
         double rvd = rv;
-        double mx = xs_double(limbs_to_xsum(pa + PA_MX * 4, e0));
-        double my = xs_double(limbs_to_xsum(pa + PA_MY * 4, e0));
-        double mx2 = xs_double(limbs_to_xsum(pa + PA_MX2 * 4, e0));
-        double my2 = xs_double(limbs_to_xsum(pa + PA_MY2 * 4, e0));
-        double mxy = xs_double(limbs_to_xsum(pa + PA_MXY * 4, e0));
-        double dthresh = thr[L];
-        float peak = ord2f((unsigned)pi[PI_PEAK]);
-        double dthresh2 = (dthresh + peak) / 2.0;
-        int dnpix = pi[PI_DNPIX], area2 = pi[PI_AREA2];
+        double mx = xs_double(smx), my = xs_double(smy);
+        double mx2 = xs_double(smx2), my2 = xs_double(smy2), mxy = xs_double(smxy);
         double xm = mx / rvd, ym = my / rvd;
         double xm2 = mx2 / rvd - xm * xm, ym2 = my2 / rvd - ym * ym, xym = mxy / rvd - xm * ym;
         double temp, temp2, theta, pmx2, pmy2, darea, t1t2;
@@ -447,11 +473,11 @@ __global__ void __launch_bounds__(DB_THREADS) k_deblend_assign(DebArgs A) {
         pmy2 = pmx2 = 0.5 * (xm2 + ym2);
         pmx2 += temp;
         pmy2 -= temp;
-        float a = (float)sqrt(pmx2), b = (float)sqrt(pmy2), abcor;
+        float fa = (float)sqrt(pmx2), fb = (float)sqrt(pmy2), abcor;
         darea = (double)area2 - dnpix;
         t1t2 = dthresh / dthresh2;
         if (t1t2 > 0.0) {
-            abcor = (darea < 0.0 ? darea : -1.0) / (2 * SX_PI * log(t1t2 < 1.0 ? t1t2 : 0.99) * a * b);
+            abcor = (darea < 0.0 ? darea : -1.0) / (2 * SX_PI * log(t1t2 < 1.0 ? t1t2 : 0.99) * fa * fb);
             if (abcor > 1.0) abcor = 1.0;
         } else
             abcor = 1.0;
@@ -466,16 +492,16 @@ __global__ void __launch_bounds__(DB_THREADS) k_deblend_assign(DebArgs A) {
         A.O.singu[o] = singu;
         A.O.dnpix[o] = dnpix;
         A.O.fdflux[o] = rv;
-        A.O.dflux[o] = xs_float(limbs_to_xsum(pa + PA_TV * 4, e0s));
-        A.O.fdpeak[o] = ord2f((unsigned)pi[PI_CPEAK]);
+        A.O.dflux[o] = xs_float(stv);
+        A.O.fdpeak[o] = ord2f(cpk);
         A.O.dpeak[o] = peak;
         A.O.mx[o] = xm + xmin;
         A.O.my[o] = ym + ymin;
         A.O.mx2[o] = xm2;
         A.O.my2[o] = ym2;
         A.O.mxy[o] = xym;
-        A.O.a[o] = a;
-        A.O.b[o] = b;
+        A.O.a[o] = fa;
+        A.O.b[o] = fb;
         A.O.theta[o] = theta * 180.0 / SX_PI;
         A.O.cxx[o] = (float)(ym2 / temp2);
         A.O.cyy[o] = (float)(xm2 / temp2);
@@ -510,11 +536,35 @@ __global__ void __launch_bounds__(DB_THREADS) k_deblend_assign(DebArgs A) {
     }
 }
 
-void launch_deblend_sweep(const DebArgs &A, int nroots, cudaStream_t st) {
-    if (nroots > 0) k_deblend_sweep<<<nroots, DB_THREADS, 0, st>>>(A);
+// raw objects of at most DB_SMALL pixels run with one-warp CTAs (their
+// per-level barriers are then warp-wide), the others with 256 threads
+constexpr int DB_SMALL = 256;
+
+__global__ void k_split_roots(const int *size, int n, int *small, int *large, int *counts) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    if (size[r] <= DB_SMALL)
+        small[atomicAdd(&counts[0], 1)] = r;
+    else
+        large[atomicAdd(&counts[1], 1)] = r;
 }
-void launch_deblend_assign(const DebArgs &A, int nroots, cudaStream_t st) {
-    if (nroots > 0) k_deblend_assign<<<nroots, DB_THREADS, 0, st>>>(A);
+
+// lists[0..nroots) small roots, lists[nroots..2*nroots) large roots; the
+// counts are on the device, grids are sized for the worst case and surplus
+// CTAs return at once
+void launch_deblend_split(const int *size, int nroots, int *lists, int *counts, cudaStream_t st) {
+    cudaMemsetAsync(counts, 0, 2 * sizeof(int), st);
+    if (nroots > 0) k_split_roots<<<(nroots + 255) / 256, 256, 0, st>>>(size, nroots, lists, lists + nroots, counts);
+}
+void launch_deblend_sweep(const DebArgs &A, const int *lists, const int *counts, int nroots, cudaStream_t st) {
+    if (nroots <= 0) return;
+    k_deblend_sweep<<<nroots, DB_THREADS, 0, st>>>(A, lists + nroots, counts + 1);
+    k_deblend_sweep<<<nroots, 32, 0, st>>>(A, lists, counts);
+}
+void launch_deblend_assign(const DebArgs &A, const int *lists, const int *counts, int nroots, cudaStream_t st) {
+    if (nroots <= 0) return;
+    k_deblend_assign<<<nroots, DB_THREADS, 0, st>>>(A, lists + nroots, counts + 1);
+    k_deblend_assign<<<nroots, 32, 0, st>>>(A, lists, counts);
 }
 
 }  // namespace sx

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(SF_TX *SF_TY) k_sub_filter(const float *__rest
         int gx = x0 - rx + tx, gy = y0 - ry + ty;
         float s = 0.0f;
         if (gx >= 0 && gx < w && gy >= 0 && gy < h) {
-            float raw = __ldg(img + (size_t)gy * w + gx);
+            float raw = sx_unblank(__ldg(img + (size_t)gy * w + gx));
             s = raw - bkg_at(gx, gy, B, nbx, back_type, backmean);
             if (tx >= rx && tx < rx + SF_TW && ty >= ry && ty < ry + SF_TH) {
                 sub[(size_t)gy * w + gx] = s;

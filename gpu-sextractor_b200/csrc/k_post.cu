@@ -16,66 +16,100 @@ namespace sx {
 // ---------------------------------------------------------------------------
 constexpr float CL_CELL = 32.0f;
 
-__global__ void k_clean_prep(ObjBufs O, int n, float dthresh, double beta, double *amp, double *alpha,
-                             int *cellhead, int *cellnext, int gx, int gy) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double unitarea = SX_PI * O.a[i] * O.b[i];
-    double am = O.fdflux[i] / (2 * unitarea * O.abcor[i]);
-    double q = am / dthresh;
-    amp[i] = am;
-    alpha[i] = ((beta == 1.0 ? q : pow(q, 1.0 / beta)) - 1) * unitarea / O.fdnpix[i];
-    O.master[i] = 0x7fffffff;
-    int cx = (int)floor(O.mx[i] / CL_CELL), cy = (int)floor(O.my[i] / CL_CELL);
+// per-object CLEAN record, stored in cell order so that a cell's objects are
+// contiguous (src/clean.c:105-107 for amp and alpha)
+struct CleanObj {
+    double mx, my, amp, alpha;
+    float a, fdflux, cxx, cyy, cxy, mthresh;
+    int idx, pad;
+};
+
+__device__ __forceinline__ int clean_cell(double mx, double my, int gx, int gy) {
+    int cx = (int)floor(mx / CL_CELL), cy = (int)floor(my / CL_CELL);
     cx = min(max(cx, 0), gx - 1);
     cy = min(max(cy, 0), gy - 1);
-    cellnext[i] = atomicExch(&cellhead[cy * gx + cx], i);
+    return cy * gx + cx;
 }
 
-__device__ __forceinline__ void clean_pair(const ObjBufs &O, const double *amp, const double *alpha, double beta,
-                                           int i, int j) {
+__global__ void k_clean_count(ObjBufs O, int n, int *cellcnt, int gx, int gy) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    O.master[i] = 0x7fffffff;
+    atomicAdd(&cellcnt[clean_cell(O.mx[i], O.my[i], gx, gy)], 1);
+}
+
+__global__ void k_clean_pack(ObjBufs O, int n, float dthresh, double beta, const int *cellstart, int *cellcur,
+                             CleanObj *packed, int gx, int gy) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    CleanObj c;
+    double unitarea = SX_PI * O.a[i] * O.b[i];
+    c.amp = O.fdflux[i] / (2 * unitarea * O.abcor[i]);
+    double q = c.amp / dthresh;
+    c.alpha = ((beta == 1.0 ? q : pow(q, 1.0 / beta)) - 1) * unitarea / O.fdnpix[i];
+    c.mx = O.mx[i];
+    c.my = O.my[i];
+    c.a = O.a[i];
+    c.fdflux = O.fdflux[i];
+    c.cxx = O.cxx[i];
+    c.cyy = O.cyy[i];
+    c.cxy = O.cxy[i];
+    c.mthresh = O.mthresh[i];
+    c.idx = i;
+    c.pad = 0;
+    int cell = clean_cell(c.mx, c.my, gx, gy);
+    packed[cellstart[cell] + atomicAdd(&cellcur[cell], 1)] = c;
+}
+
+// src/clean.c:108-132 on the pair (p, q) with p.idx < q.idx (the kernel's
+// orientation, src/cuda/cudaclean.cu:140-170)
+__device__ __forceinline__ void clean_test(const CleanObj &p, const CleanObj &q, double beta, int *master) {
     float dx, dy, rlim;
     double val;
-    dx = O.mx[i] - O.mx[j];
-    dy = O.my[i] - O.my[j];
-    rlim = O.a[i] + O.a[j];
+    dx = p.mx - q.mx;
+    dy = p.my - q.my;
+    rlim = p.a + q.a;
     rlim *= rlim;
     if (!(dx * dx + dy * dy < rlim * SX_CLEAN_ZONE * SX_CLEAN_ZONE)) return;
-    if (O.fdflux[i] < O.fdflux[j]) {
-        val = 1 + alpha[j] * (O.cxx[j] * dx * dx + O.cyy[j] * dy * dy + O.cxy[j] * dx * dy);
-        if (val > 1.0 && ((float)(val < 1e10 ? amp[j] * (beta == 1.0 ? 1.0 / val : pow(val, -beta)) : 0.0)
-                          > O.mthresh[i]))
-            atomicMin(&O.master[i], j);
+    if (p.fdflux < q.fdflux) {
+        val = 1 + q.alpha * (q.cxx * dx * dx + q.cyy * dy * dy + q.cxy * dx * dy);
+        if (val > 1.0 && ((float)(val < 1e10 ? q.amp * (beta == 1.0 ? 1.0 / val : pow(val, -beta)) : 0.0)
+                          > p.mthresh))
+            atomicMin(&master[p.idx], q.idx);
     } else {
-        val = 1 + alpha[i] * (O.cxx[i] * dx * dx + O.cyy[i] * dy * dy + O.cxy[i] * dx * dy);
-        if (val > 1.0 && ((float)(val < 1e10 ? amp[i] * (beta == 1.0 ? 1.0 / val : pow(val, -beta)) : 0.0)
-                          > O.mthresh[j]))
-            atomicMin(&O.master[j], i);
+        val = 1 + p.alpha * (p.cxx * dx * dx + p.cyy * dy * dy + p.cxy * dx * dy);
+        if (val > 1.0 && ((float)(val < 1e10 ? p.amp * (beta == 1.0 ? 1.0 / val : pow(val, -beta)) : 0.0)
+                          > q.mthresh))
+            atomicMin(&master[q.idx], p.idx);
     }
 }
 
 // every pair closer than CLEAN_ZONE*(a_i+a_j) is tested once, by the object
-// of larger a (lower index on ties), which searches 20*a around itself
-__global__ void k_clean_pairs(ObjBufs O, int n, double beta, const double *amp, const double *alpha,
-                              const int *cellhead, const int *cellnext, int gx, int gy) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float ai = O.a[i];
-    double rad = 20.0 * ai * 1.001 + 2.0;
-    int x0 = max((int)floor((O.mx[i] - rad) / CL_CELL), 0), x1 = min((int)floor((O.mx[i] + rad) / CL_CELL), gx - 1);
-    int y0 = max((int)floor((O.my[i] - rad) / CL_CELL), 0), y1 = min((int)floor((O.my[i] + rad) / CL_CELL), gy - 1);
-    for (int cy = y0; cy <= y1; cy++)
-        for (int cx = x0; cx <= x1; cx++)
-            for (int j = cellhead[cy * gx + cx]; j >= 0; j = cellnext[j]) {
-                if (j == i) continue;
-                float aj = O.a[j];
-                if (aj < ai || (aj == ai && j > i)) {
-                    if (i < j)
-                        clean_pair(O, amp, alpha, beta, i, j);
-                    else
-                        clean_pair(O, amp, alpha, beta, j, i);
-                }
+// of larger a (lower index on ties), which searches 20*a around itself; one
+// warp per object, lanes over the cells of the search box
+__global__ void k_clean_pairs(const CleanObj *__restrict__ packed, int n, double beta,
+                              const int *__restrict__ cellstart, int *master, int gx, int gy) {
+    const int lane = threadIdx.x & 31;
+    const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (k >= n) return;
+    const CleanObj me = packed[k];
+    const double rad = 20.0 * me.a * 1.001 + 2.0;
+    int x0 = max((int)floor((me.mx - rad) / CL_CELL), 0), x1 = min((int)floor((me.mx + rad) / CL_CELL), gx - 1);
+    int y0 = max((int)floor((me.my - rad) / CL_CELL), 0), y1 = min((int)floor((me.my + rad) / CL_CELL), gy - 1);
+    int bw = x1 - x0 + 1, nc = bw * (y1 - y0 + 1);
+    for (int c = lane; c < nc; c += 32) {
+        int cell = (y0 + c / bw) * gx + x0 + c % bw;
+        for (int t = cellstart[cell]; t < cellstart[cell + 1]; t++) {
+            const CleanObj o = packed[t];
+            if (o.idx == me.idx) continue;
+            if (o.a < me.a || (o.a == me.a && o.idx > me.idx)) {
+                if (me.idx < o.idx)
+                    clean_test(me, o, beta, master);
+                else
+                    clean_test(o, me, beta, master);
             }
+        }
+    }
 }
 
 // end of the master chain; victims with a master get sort keys for merging
@@ -145,30 +179,27 @@ struct EndArgs {
     double aperture, autoparam0, autoparam1, gain, zp, satur;
 };
 
-// src/cuda/cudaanalyse.cu:104-287, one thread (sequential, as the reference)
-__device__ void aper_one(const EndArgs &A, int o, int &flags) {
-    float r2, raper, raper2, rintlim, rintlim2, rextlim2, dx, dx1, dy, dy2, offsetx, offsety, scalex, scaley, scale2,
-        locarea;
-    double tv, sigtv, area, pix, var;
-    int x, y, x2, y2, xmin, xmax, ymin, ymax, sx, sy, t, w = A.w, h = A.h;
-    int corrflag = (A.mask_type == 2);
-    double mx = A.O.mx[o], my = A.O.my[o];
-    float backsig = A.sc->backsig;
-    var = backsig * backsig;
-    raper = A.aperture / 2.0;
-    raper2 = raper * raper;
-    rintlim = raper - 0.75;
-    rintlim2 = (rintlim > 0.0) ? rintlim * rintlim : 0.0;
-    rextlim2 = (raper + 0.75) * (raper + 0.75);
-    tv = sigtv = area = 0.0;
-    scaley = scalex = 1.0 / SX_APER_OVERSAMP;
-    scale2 = scalex * scaley;
-    offsetx = 0.5 * (scalex - 1.0);
-    offsety = 0.5 * (scaley - 1.0);
-    xmin = (int)(mx - raper + 0.499999);
-    xmax = (int)(mx + raper + 1.499999);
-    ymin = (int)(my - raper + 0.499999);
-    ymax = (int)(my + raper + 1.499999);
+// src/cuda/cudaanalyse.cu:104-287 (computeaperflux, one aperture).  The
+// lanes of the warp evaluate 32 aperture pixels at a time (sub-pixel area,
+// masked value); the three double sums then take the terms one by one in the
+// raster order of the sequential loop, so the rounding is that loop's.
+__device__ void aper_warp(const EndArgs &A, int o, double mx, double my, int &flags) {
+    const int lane = threadIdx.x & 31, w = A.w, h = A.h;
+    const int corrflag = (A.mask_type == 2);
+    const float backsig = A.sc->backsig;
+    const double var = backsig * backsig;
+    const float raper = A.aperture / 2.0;
+    const float raper2 = raper * raper;
+    const float rintlim = raper - 0.75;
+    const float rintlim2 = (rintlim > 0.0) ? rintlim * rintlim : 0.0;
+    const float rextlim2 = (raper + 0.75) * (raper + 0.75);
+    const float scalex = 1.0 / SX_APER_OVERSAMP, scaley = scalex;
+    const float scale2 = scalex * scaley;
+    const float offsetx = 0.5 * (scalex - 1.0), offsety = 0.5 * (scaley - 1.0);
+    int xmin = (int)(mx - raper + 0.499999);
+    int xmax = (int)(mx + raper + 1.499999);
+    int ymin = (int)(my - raper + 0.499999);
+    int ymax = (int)(my + raper + 1.499999);
     if (xmin < 0) {
         xmin = 0;
         flags |= SX_OBJ_APERT_PB;
@@ -185,38 +216,50 @@ __device__ void aper_one(const EndArgs &A, int o, int &flags) {
         ymax = h;
         flags |= SX_OBJ_APERT_PB;
     }
-    for (y = ymin; y < ymax; y++)
-        for (x = xmin; x < xmax; x++) {
-            dx = x - mx;
-            dy = y - my;
+    double tv = 0.0, sigtv = 0.0, area = 0.0;
+    const int bw = xmax - xmin, nn = bw * (ymax - ymin);
+    for (int base = 0; base < nn; base += 32) {
+        const int i = base + lane;
+        bool in = false;
+        float locarea = 0.0f;
+        double pix = 0.0;
+        if (i < nn) {
+            const int yo = i / bw, x = xmin + (i - yo * bw), y = ymin + yo;
+            float dx = x - mx, dy = y - my, r2;
             if ((r2 = dx * dx + dy * dy) < rextlim2) {
+                in = true;
                 if (r2 > rintlim2) {
                     dx += offsetx;
                     dy += offsety;
-                    locarea = 0.0;
-                    for (sy = SX_APER_OVERSAMP; sy--; dy += scaley) {
-                        dx1 = dx;
-                        dy2 = dy * dy;
-                        for (sx = SX_APER_OVERSAMP; sx--; dx1 += scalex)
+                    for (int sy = SX_APER_OVERSAMP; sy--; dy += scaley) {
+                        float dx1 = dx, dy2 = dy * dy;
+                        for (int sx = SX_APER_OVERSAMP; sx--; dx1 += scalex)
                             if (dx1 * dx1 + dy2 < raper2) locarea += scale2;
                     }
                 } else
                     locarea = 1.0;
-                area += locarea;
                 pix = A.sub[(size_t)y * w + x];
-                t = A.alloc[(size_t)y * w + x];
-                if (t >= 0 && t != o) {
+                int t = A.alloc[(size_t)y * w + x], x2, y2;
+                if ((t >= 0 && t != o) || pix <= -SX_BIG) {
                     if (corrflag && (x2 = (int)(2 * mx + 0.49999 - x)) >= 0 && x2 < w &&
                         (y2 = (int)(2 * my + 0.49999 - y)) >= 0 && y2 < h &&
-                        ((t = A.alloc[(size_t)y2 * w + x2]) == o || t == -1))
+                        ((t = A.alloc[(size_t)y2 * w + x2]) == o || t == -1) &&
+                        A.sub[(size_t)y2 * w + x2] > -SX_BIG)
                         pix = A.sub[(size_t)y2 * w + x2];
                     else
                         pix = 0.0;
                 }
-                sigtv += var * locarea;
-                tv += locarea * pix;
             }
         }
+        const double tsig = var * locarea, ttv = locarea * pix;
+        for (unsigned m = __ballot_sync(0xffffffffu, in); m; m &= m - 1) {
+            const int q = __ffs(m) - 1;
+            area += __shfl_sync(0xffffffffu, locarea, q);
+            sigtv += __shfl_sync(0xffffffffu, tsig, q);
+            tv += __shfl_sync(0xffffffffu, ttv, q);
+        }
+    }
+    if (lane != 0) return;
     tv -= area * 0.0;
     if (A.gain > 0.0 && tv > 0.0) sigtv += tv / A.gain;
     A.O.flux_aper[o] = tv;
@@ -254,8 +297,7 @@ __global__ void k_endobject(EndArgs A) {
     double mx = A.O.mx[o], my = A.O.my[o];
     float flux = A.O.flux[o], fluxerr = A.O.fluxerr[o], dthresh = A.sc->dthresh, backsig = A.sc->backsig;
     int fdnpix = A.O.fdnpix[o];
-    if (lane == 0) aper_one(A, o, flags);
-    flags = __shfl_sync(0xffffffffu, flags, 0);
+    aper_warp(A, o, mx, my, flags);
     // AUTO / Kron, src/cuda/cudaanalyse.cu:293-592
     double var = backsig * backsig;
     int corrflag = (A.mask_type == 2);
@@ -300,8 +342,9 @@ __global__ void k_endobject(EndArgs A) {
     area = areab = 0;
     {
         int bw = xmax - xmin, nn = bw * (ymax - ymin);
+        const FastDiv bd = make_fastdiv_dev((unsigned)bw);
         for (int i = lane; i < nn; i += 32) {
-            int x = xmin + i % bw, y = ymin + i / bw;
+            int yo = (int)fdiv((unsigned)i, bd), x = xmin + (i - yo * bw), y = ymin + yo;
             dx = x - mx;
             dy = y - my;
             if ((r2 = cx2 * dx * dx + cy2 * dy * dy + cxy * dx * dy) <= klim2) {
@@ -366,20 +409,22 @@ __global__ void k_endobject(EndArgs A) {
         XSum stv;
         xs_init(stv);
         int bw = xmax - xmin, nn = bw * (ymax - ymin);
+        const FastDiv bd = make_fastdiv_dev((unsigned)bw);
         for (int i = lane; i < nn; i += 32) {
-            int x = xmin + i % bw, y = ymin + i / bw;
+            int yo = (int)fdiv((unsigned)i, bd), x = xmin + (i - yo * bw), y = ymin + yo;
             dx = x - mx;
             dy = y - my;
             if ((cx2 * dx * dx + cy2 * dy * dy + cxy * dx * dy) <= klim2) {
                 area++;
                 pix = A.sub[(size_t)y * w + x];
                 int t = A.alloc[(size_t)y * w + x];
-                if (t >= 0 && t != o) {
+                if ((t >= 0 && t != o) || pix <= -SX_BIG) {
                     areab++;
                     int x2, y2;
                     if (corrflag && (x2 = (int)(2 * mx + 0.49999 - x)) >= 0 && x2 < w &&
                         (y2 = (int)(2 * my + 0.49999 - y)) >= 0 && y2 < h &&
-                        ((t = A.alloc[(size_t)y2 * w + x2]) == -1 || t == o))
+                        ((t = A.alloc[(size_t)y2 * w + x2]) == -1 || t == o) &&
+                        A.sub[(size_t)y2 * w + x2] > -SX_BIG)
                         pix = A.sub[(size_t)y2 * w + x2];
                     else
                         pix = 0.0;

@@ -80,7 +80,8 @@ struct DebArgs {
     double mincont;
 };
 
-void launch_deblend_sweep(const DebArgs &A, int nroots, cudaStream_t st);
-void launch_deblend_assign(const DebArgs &A, int nroots, cudaStream_t st);
+void launch_deblend_split(const int *size, int nroots, int *lists, int *counts, cudaStream_t st);
+void launch_deblend_sweep(const DebArgs &A, const int *lists, const int *counts, int nroots, cudaStream_t st);
+void launch_deblend_assign(const DebArgs &A, const int *lists, const int *counts, int nroots, cudaStream_t st);
 
 }  // namespace sx

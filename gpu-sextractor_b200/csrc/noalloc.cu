@@ -118,7 +118,7 @@ __global__ void k_sub_only(const float *__restrict__ img, float *__restrict__ su
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= (long long)w * h) return;
     int x = (int)(p % w), y = (int)(p / w);
-    sub[p] = img[p] - sx::bkg_at(x, y, B, nbx, back_type, sc->backmean);
+    sub[p] = sx_unblank(img[p]) - sx::bkg_at(x, y, B, nbx, back_type, sc->backmean);
 }
 
 __global__ void k_init(FrameScalars *sc) {

@@ -56,7 +56,7 @@ struct sexgpu_ctx {
     // background
     DevBuf ms, back, sigma, back2, back3, sigma3, dback, bu, rownode, rowdnode, rowu, colk, coldx;
     // roots
-    DevBuf rsize, roff, rfirst, rymax, rlastx, rfdpeak, rfdflux, rnkept, robjbase;
+    DevBuf rsize, roff, rfirst, rymax, rlastx, rfdpeak, rfdflux, rnkept, robjbase, rlists, rcounts;
     // deblend scratch
     DevBuf dpar, dlev, dsz, dorder, drl0, drl1, dnid0, dnid1, dacc, nr0, nr1, nf0, nf1, ns0, ns1, nc0, nc1, na0, na1,
         dkept, down, dkl, dkidx, dpacc, dpint, objkey, rpix;
@@ -327,7 +327,7 @@ int alloc_objects(sexgpu_ctx *ctx, int nobj) {
     return SEXGPU_OK;
 }
 
-unsigned grid1(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+unsigned grid1(long long n, int t) { return n > 0 ? (unsigned)((n + t - 1) / t) : 1u; }
 
 // the whole pipeline on a device-resident frame
 int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu_config *cfg) {
@@ -529,7 +529,10 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     A.N = Pm.nthresh;
     A.debminarea = Pm.debminarea;
     A.mincont = Pm.mincont;
-    launch_deblend_sweep(A, nroots, st);
+    EN(rlists, (size_t)(2 * nroots + 2) * 4);
+    EN(rcounts, 16);
+    launch_deblend_split(R.size, nroots, P<int>(ctx->rlists), P<int>(ctx->rcounts), st);
+    launch_deblend_sweep(A, P<int>(ctx->rlists), P<int>(ctx->rcounts), nroots, st);
     exclusive_scan(R.nkept, R.objbase, nroots, &d_sc->nobj, tmp, st);
     rc = read_scalars(ctx);
     if (rc) return rc;
@@ -537,8 +540,8 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     rc = alloc_objects(ctx, nobj);
     if (rc) return rc;
     A.O = ctx->O;
-    launch_deblend_assign(A, nroots, st);
-    stage_mark(ctx, "deblend", 2 + scan_launches(nroots));
+    launch_deblend_assign(A, P<int>(ctx->rlists), P<int>(ctx->rcounts), nroots, st);
+    stage_mark(ctx, "deblend", 5 + scan_launches(nroots));
 
     // ---- object pixel lists (stable by object id: raster order inside)
     ObjBufs &O = ctx->O;
@@ -564,29 +567,31 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     AA.clean_flag = Pm.clean_flag;
     AA.gain = Pm.gain;
     AA.satur = Pm.satur_level;
+    AA.wdiv = make_fastdiv((unsigned)w);
     launch_analyse(AA, st);
-    stage_mark(ctx, "analyse", 1 + radix_launches(bits_for(nobj), nrootpix) + scan_launches(nobj));
+    stage_mark(ctx, "analyse", 2 + radix_launches(bits_for(nobj), nrootpix) + scan_launches(nobj));
 
     // ---- CLEAN
     int nv = 0;
     int cl_launch = 0;
     if (Pm.clean_flag && nobj > 0) {
-        int gx = (int)(w / CL_CELL) + 2, gy = (int)(h / CL_CELL) + 2;
-        EN(amp, (size_t)(nobj + 1) * 8);
-        EN(alpha, (size_t)(nobj + 1) * 8);
-        EN(cellhead, (size_t)gx * gy * 4);
-        EN(cellnext, (size_t)(nobj + 1) * 4);
+        int gx = (int)(w / CL_CELL) + 2, gy = (int)(h / CL_CELL) + 2, ncell = gx * gy;
+        EN(cellhead, (size_t)(ncell + 1) * 4);   // cell counts, then starts
+        EN(cellnext, (size_t)(ncell + 1) * 4);   // fill cursors
+        EN(amp, (size_t)(nobj + 1) * sizeof(CleanObj));
         EN(vkey, (size_t)(nobj + 1) * 4);
         EN(vval, (size_t)(nobj + 1) * 4);
         EN(vkalt, (size_t)(nobj + 1) * 4);
         EN(vvalt, (size_t)(nobj + 1) * 4);
-        CK(cudaMemsetAsync(ctx->cellhead.p, 0xff, (size_t)gx * gy * 4, st));
-        k_clean_prep<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, ctx->hsc.dthresh, Pm.clean_param, P<double>(ctx->amp),
-                                                       P<double>(ctx->alpha), P<int>(ctx->cellhead),
-                                                       P<int>(ctx->cellnext), gx, gy);
-        k_clean_pairs<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, Pm.clean_param, P<double>(ctx->amp),
-                                                        P<double>(ctx->alpha), P<int>(ctx->cellhead),
-                                                        P<int>(ctx->cellnext), gx, gy);
+        int *cellcnt = P<int>(ctx->cellhead), *cellcur = P<int>(ctx->cellnext);
+        CK(cudaMemsetAsync(cellcnt, 0, (size_t)(ncell + 1) * 4, st));
+        CK(cudaMemsetAsync(cellcur, 0, (size_t)(ncell + 1) * 4, st));
+        k_clean_count<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, cellcnt, gx, gy);
+        exclusive_scan(cellcnt, cellcnt, ncell + 1, nullptr, tmp, st);
+        k_clean_pack<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, ctx->hsc.dthresh, Pm.clean_param, cellcnt, cellcur,
+                                                       P<CleanObj>(ctx->amp), gx, gy);
+        k_clean_pairs<<<grid1(nobj, 4), 128, 0, st>>>(P<CleanObj>(ctx->amp), nobj, Pm.clean_param, cellcnt, O.master,
+                                                      gx, gy);
         CK(cudaMemsetAsync(&d_sc->nsurv, 0, 4, st));
         k_clean_chain<<<grid1(nobj, 256), 256, 0, st>>>(O, nobj, P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval),
                                                         &d_sc->nsurv);
@@ -601,7 +606,7 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
             k_clean_merge<<<grid1(nv, 128), 128, 0, st>>>(O, P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval), nv);
             k_alloc_victims<<<nobj, 128, 0, st>>>(O, vals, A.alloc, nobj);
         }
-        cl_launch = 5 + 2 * radix_launches(bits_for(nobj), nv);
+        cl_launch = 6 + scan_launches(ncell + 1) + 2 * radix_launches(bits_for(nobj), nv);
     } else if (nobj > 0) {
         CK(cudaMemsetAsync(O.fmaster, 0xff, (size_t)nobj * 4, st));
     }
@@ -717,7 +722,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
                      &ctx->valt, &ctx->ms, &ctx->back, &ctx->sigma, &ctx->back2, &ctx->back3, &ctx->sigma3,
                      &ctx->dback, &ctx->bu, &ctx->rownode, &ctx->rowdnode, &ctx->rowu, &ctx->colk, &ctx->coldx,
                      &ctx->rsize, &ctx->roff, &ctx->rfirst, &ctx->rymax, &ctx->rlastx, &ctx->rfdpeak,
-                     &ctx->rfdflux, &ctx->rnkept, &ctx->robjbase, &ctx->dpar, &ctx->dlev, &ctx->dsz, &ctx->dorder,
+                     &ctx->rfdflux, &ctx->rnkept, &ctx->robjbase, &ctx->rlists, &ctx->rcounts, &ctx->dpar, &ctx->dlev, &ctx->dsz, &ctx->dorder,
                      &ctx->drl0, &ctx->drl1, &ctx->dnid0, &ctx->dnid1, &ctx->dacc, &ctx->nr0, &ctx->nr1,
                      &ctx->nf0, &ctx->nf1, &ctx->ns0, &ctx->ns1, &ctx->nc0, &ctx->nc1, &ctx->na0, &ctx->na1,
                      &ctx->dkept, &ctx->down, &ctx->dkl, &ctx->dkidx, &ctx->dpacc, &ctx->dpint, &ctx->objkey,

@@ -522,6 +522,11 @@ int orc_background(float *img, int w, int h, const orc_config *cfg,
     back_spline(sigma, dsigma, nx, ny);
     if (cfg->back_type == 1)
         backmean = (float)cfg->back_value;
+    /* blank (NaN) pixels read as -BIG, as the FITS reader does
+     * (src/fits/fitsbody.c:328); the mesh statistics above skip both alike */
+    for (size_t p = 0; p < (size_t)w * h; p++)
+        if (img[p] != img[p])
+            img[p] = -ORC_BIGF;
     for (y = 0; y < h; y++)
         sub_back_line(back, dback, nx, ny, bw, bh, cfg->back_type, backmean, y,
                       img + (size_t)y * w, w);

@@ -759,7 +759,10 @@ static void run_clean(const frame_t *F, obj_t *o, int n)
 /* ------------------------------------------------------------------------ */
 #define ALLOC_OTHER 0x7fffffff
 
-/* src/cuda/cudaanalyse.cu:104-287 (computeaperflux, one aperture, CCD). */
+/* src/cuda/cudaanalyse.cu:104-287 (computeaperflux, one aperture, CCD).
+ * Pixels at or below -BIG (blank or NaN input pixels) are replaced like
+ * pixels of other objects, as the CPU computeaperflux does (src/photom.c:128-
+ * 145): the GPU kernel drops that test and would sum the -BIG sentinel. */
 static void aperflux(const frame_t *F, const int *alloc, obj_t *o, int self)
 {
     const orc_config *cfg = F->cfg;
@@ -808,10 +811,11 @@ static void aperflux(const frame_t *F, const int *alloc, obj_t *o, int self)
                 area += locarea;
                 pix = F->sub[(size_t)y * w + x];
                 t = alloc[(size_t)y * w + x];
-                if (t >= 0 && t != self) {
+                if ((t >= 0 && t != self) || pix <= -ORC_BIG) {
                     if (corrflag && (x2 = (int)(2 * o->mx + 0.49999 - x)) >= 0 && x2 < w
                         && (y2 = (int)(2 * o->my + 0.49999 - y)) >= 0 && y2 < h
-                        && ((t = alloc[(size_t)y2 * w + x2]) == self || t == -1))
+                        && ((t = alloc[(size_t)y2 * w + x2]) == self || t == -1)
+                        && F->sub[(size_t)y2 * w + x2] > -ORC_BIG)
                         pix = F->sub[(size_t)y2 * w + x2];
                     else
                         pix = 0.0;
@@ -833,7 +837,8 @@ static void aperflux(const frame_t *F, const int *alloc, obj_t *o, int self)
 
 /* src/cuda/cudaanalyse.cu:293-592 (computeautoflux, CCD, no weights).  The
  * sums r1, v1 and tv are exact order-free sums of the float terms the kernel
- * accumulates. */
+ * accumulates.  In the flux pass, pixels at or below -BIG count as bad and are
+ * replaced as in the CPU computeautoflux (src/photom.c:640-657). */
 static void autoflux(const frame_t *F, const int *alloc, obj_t *o, int self)
 {
     const orc_config *cfg = F->cfg;
@@ -924,11 +929,12 @@ static void autoflux(const frame_t *F, const int *alloc, obj_t *o, int self)
                     area++;
                     pix = F->sub[(size_t)y * w + x];
                     t = alloc[(size_t)y * w + x];
-                    if (t >= 0 && t != self) {
+                    if ((t >= 0 && t != self) || pix <= -ORC_BIG) {
                         areab++;
                         if (corrflag && (x2 = (int)(2 * o->mx + 0.49999 - x)) >= 0 && x2 < w
                             && (y2 = (int)(2 * o->my + 0.49999 - y)) >= 0 && y2 < h
-                            && ((t = alloc[(size_t)y2 * w + x2]) == -1 || t == self))
+                            && ((t = alloc[(size_t)y2 * w + x2]) == -1 || t == self)
+                            && F->sub[(size_t)y2 * w + x2] > -ORC_BIG)
                             pix = F->sub[(size_t)y2 * w + x2];
                         else
                             pix = 0.0;

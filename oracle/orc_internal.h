@@ -8,6 +8,7 @@
 #include <stdint.h>
 
 #define ORC_BIG                 1e+30
+#define ORC_BIGF                1e+30f
 #define ORC_PI                  3.1415926535898
 #define ORC_EPS                 (1e-4)
 #define ORC_BACK_MINGOODFRAC    0.5
