@@ -91,15 +91,14 @@ __device__ __forceinline__ void activate_and_union(const DebArgs &A, int off, in
 }
 
 // first sweep: branch tree, MINCONT pruning, kept branches
-__global__ void __launch_bounds__(DB_THREADS) k_deblend_sweep(DebArgs A, const int *roots, const int *nroots) {
-    if ((int)blockIdx.x >= *nroots) return;
+__device__ __forceinline__ void deblend_sweep_root(const DebArgs &A, const int r) {
     __shared__ float thr[DB_MAXLEV];
     __shared__ int lvcnt[DB_MAXLEV + 1], lvstart[DB_MAXLEV + 1], lvcur[DB_MAXLEV];
     __shared__ int s_nrl[2], s_nn[2], s_nkept;
     __shared__ unsigned s_peak;
     __shared__ XSum s_part[DB_THREADS / 32];
     __shared__ float s_fdflux;
-    const int r = roots[blockIdx.x], off = A.R.off[r], P = A.R.size[r];
+    const int off = A.R.off[r], P = A.R.size[r];
     const unsigned *pix = A.rpix + off;
     int *par = A.D.par + off, *lev = A.D.lev + off, *sz = A.D.sz + off, *order = A.D.order + off;
     unsigned long long *acc = A.D.acc + (size_t)off * 4;
@@ -304,11 +303,10 @@ __device__ __forceinline__ void lacc_add(unsigned long long *a, float f, int e0,
     limbs_atomic_add_term(a, f, e0, status);
 }
 
-__global__ void __launch_bounds__(DB_THREADS) k_deblend_assign(DebArgs A, const int *roots, const int *nroots) {
-    if ((int)blockIdx.x >= *nroots) return;
+__device__ __forceinline__ void deblend_assign_root(const DebArgs &A, const int r) {
     __shared__ float thr[DB_MAXLEV];
     __shared__ int lvcnt[DB_MAXLEV + 1], lvstart[DB_MAXLEV + 1], lvkept[DB_MAXLEV];
-    const int r = roots[blockIdx.x], off = A.R.off[r], P = A.R.size[r], K = A.R.nkept[r], ob = A.R.objbase[r];
+    const int off = A.R.off[r], P = A.R.size[r], K = A.R.nkept[r], ob = A.R.objbase[r];
     const unsigned *pix = A.rpix + off;
     int *par = A.D.par + off, *lev = A.D.lev + off, *order = A.D.order + off;
     int *own = A.D.own + off, *kl = A.D.kl + off, *kidx = A.D.kidx + off;
@@ -536,35 +534,34 @@ __global__ void __launch_bounds__(DB_THREADS) k_deblend_assign(DebArgs A, const 
     }
 }
 
-// raw objects of at most DB_SMALL pixels run with one-warp CTAs (their
-// per-level barriers are then warp-wide), the others with 256 threads
-constexpr int DB_SMALL = 256;
-
-__global__ void k_split_roots(const int *size, int n, int *small, int *large, int *counts) {
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    if (size[r] <= DB_SMALL)
-        small[atomicAdd(&counts[0], 1)] = r;
-    else
-        large[atomicAdd(&counts[1], 1)] = r;
+// persistent CTAs over a device-side list of raw objects (see
+// k_deblend_local.cu); these take the objects too large for shared memory
+__global__ void __launch_bounds__(DB_THREADS) k_deblend_sweep(const __grid_constant__ DebArgs A, const int *roots,
+                                                              const int *nroots, int *cursor) {
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(cursor, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= *nroots) break;
+        deblend_sweep_root(A, roots[item]);
+        __syncthreads();
+    }
 }
 
-// lists[0..nroots) small roots, lists[nroots..2*nroots) large roots; the
-// counts are on the device, grids are sized for the worst case and surplus
-// CTAs return at once
-void launch_deblend_split(const int *size, int nroots, int *lists, int *counts, cudaStream_t st) {
-    cudaMemsetAsync(counts, 0, 2 * sizeof(int), st);
-    if (nroots > 0) k_split_roots<<<(nroots + 255) / 256, 256, 0, st>>>(size, nroots, lists, lists + nroots, counts);
-}
-void launch_deblend_sweep(const DebArgs &A, const int *lists, const int *counts, int nroots, cudaStream_t st) {
-    if (nroots <= 0) return;
-    k_deblend_sweep<<<nroots, DB_THREADS, 0, st>>>(A, lists + nroots, counts + 1);
-    k_deblend_sweep<<<nroots, 32, 0, st>>>(A, lists, counts);
-}
-void launch_deblend_assign(const DebArgs &A, const int *lists, const int *counts, int nroots, cudaStream_t st) {
-    if (nroots <= 0) return;
-    k_deblend_assign<<<nroots, DB_THREADS, 0, st>>>(A, lists + nroots, counts + 1);
-    k_deblend_assign<<<nroots, 32, 0, st>>>(A, lists, counts);
+__global__ void __launch_bounds__(DB_THREADS) k_deblend_assign(const __grid_constant__ DebArgs A, const int *roots,
+                                                               const int *nroots, int *cursor) {
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(cursor, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= *nroots) break;
+        deblend_assign_root(A, roots[item]);
+        __syncthreads();
+    }
 }
 
 }  // namespace sx

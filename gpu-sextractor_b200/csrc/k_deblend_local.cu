@@ -1,0 +1,769 @@
+// k_deblend_local.cu -- deblending of raw objects of at most 32767 pixels
+// with a compact per-object state: in shared memory for objects of at most
+// 256 pixels (one warp each), in a global arena of 48 B per pixel otherwise.
+//
+// Same algorithm and results as k_deblend_sweep / k_deblend_assign (one CTA
+// per raw object, incremental union-find sweep from the top threshold down,
+// MINCONT cut evaluated two levels at a time, replay sweep for ownership,
+// preanalysis of the kept branches, gatherup), with three changes that only
+// affect speed:
+//
+//  * the union-find forest, the component sizes, the branch fluxes, the
+//    branch nodes of two consecutive levels and the level order of the pixels
+//    are packed (16-bit element indices; about 45 B per pixel in the sweep,
+//    34 B in the assignment); grids are persistent, sized to the resident
+//    capacity, and take objects from a device-side cursor;
+//  * a branch flux is one 64-bit fixed-scale integer (units of 2^(e0-23),
+//    e0 the exponent of the detection threshold, every cd of the object being
+//    at least that threshold).  The object's range is checked first: when
+//    (exponent of its peak - e0) + 24 + bits(pixels) exceeds 63 the object is
+//    handed to the global kernels (128-bit limbs) instead;
+//  * levels at which no pixel of the object first passes the threshold are
+//    skipped.  At such a level the components do not change, every branch has
+//    one child (itself one level up), no branch is cut there and the ok-after
+//    state carries over; the only thing that changes is the flag of each
+//    branch, which depends on the threshold, so when the next populated level
+//    L is reached the branches of the list are re-flagged at threshold L+1
+//    before they act as L's children.
+//
+// Reference for the algorithm: src/cuda/cudadeblend.cu:199-217, :579-727,
+// :1262-1360, :1425-1776; src/cuda/cudaanalyse.cu:1686-1903.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace sx {
+
+#ifndef SX_DL_MID
+#define SX_DL_MID 2048
+#endif
+#ifndef SX_DL_ARENA_MAX
+#define SX_DL_ARENA_MAX 32767
+#endif
+constexpr int DL_CAP0 = 256;                   // shared-memory tier (one warp per object)
+constexpr int DL_MID = SX_DL_MID;              // arena tier with 64-thread CTAs up to here, 256 above
+constexpr int DL_ARENA_MAX = SX_DL_ARENA_MAX;  // at most 32767: element indices are 16-bit
+constexpr int DL_SWEEP_BYTES = 45;   // shared bytes per pixel, sweep
+constexpr int DL_ASSIGN_BYTES = 34;  // shared bytes per pixel, assignment
+constexpr int DL_ARENA_BYTES = 48;   // global arena bytes per pixel (either pass)
+
+// ---- shared-memory union-find over the element indices of one object
+// Path halving: a node's pointer is replaced by its grandparent.  Every
+// pointer goes to a smaller element index and only roots are linked, so a
+// halving store that races with a link of the same node can only drop that
+// link to an ancestor; the linking thread then continues with the old parent,
+// so no connection is lost.
+// Plain (cached) loads: a stale pointer read is an older pointer to an
+// ancestor, so a walk still ends at a root of the same tree, and a union that
+// acted on a stale root sees it in the value atomicMin returns and retries.
+__device__ __forceinline__ int sfind(int *par, int a, int cap, int *status) {
+    for (int n = 0; n <= cap; n++) {
+        int p = par[a];
+        if (p == a) return a;
+        int g = par[p];
+        if (g != p) par[a] = g;
+        a = g;
+    }
+    atomicOr(status, SX_ST_LOOP);
+    return a;
+}
+
+// find with path compression; only used while no union is in flight, so every
+// pointer written is the final root of the tree
+__device__ __forceinline__ int sfind_c(int *par, int a, int cap, int *status) {
+    int rt = sfind(par, a, cap, status);
+    for (int n = 0; n <= cap; n++) {
+        int p = par[a];
+        if (p == rt || p == a) break;
+        par[a] = rt;
+        a = p;
+    }
+    return rt;
+}
+
+__device__ __forceinline__ void sunion(int *par, int a, int b, int cap, int *status) {
+    for (int it = 0; it <= 2 * cap + 2; it++) {
+        a = sfind(par, a, cap, status);
+        b = sfind(par, b, cap, status);
+        if (a == b) return;
+        if (a < b) {
+            int t = a;
+            a = b;
+            b = t;
+        }
+        int old = atomicMin(&par[a], b);
+        if (old == a) return;
+        a = old;
+    }
+    atomicOr(status, SX_ST_LOOP);
+}
+
+// the 64-bit fixed-scale flux is usable for this object
+__device__ __forceinline__ bool dl_range_ok(float fdpeak, int e0, int P) {
+    return fexpo(fdpeak) - e0 + 24 + (32 - __clz(P)) <= 63;
+}
+
+// flux of a branch: the exact fixed-scale sum rounded to double, then to
+// float, as the 128-bit path rounds it
+__device__ __forceinline__ float dl_flux(unsigned long long acc, int e0) {
+    return (float)scalbn(__ull2double_rn(acc), e0 - 23);
+}
+
+__device__ __forceinline__ unsigned long long dl_term(float c, int e0) {
+    unsigned u = __float_as_uint(c);
+    int sh = (int)((u >> 23) & 0xff) - 127 - e0;
+    return (unsigned long long)((u & 0x7fffffu) | 0x800000u) << sh;
+}
+
+// pixels first active at level L: activate, then join to active neighbours
+template <int NT>
+__device__ __forceinline__ void dl_activate_union(const DebArgs &A, int off, int P, int L, int b0, int b1,
+                                                  const unsigned short *order, int *par, const unsigned char *lev,
+                                                  int *status) {
+    for (int i = b0 + (int)threadIdx.x; i < b1; i += NT) par[order[i]] = order[i];
+    __syncthreads();
+    for (int i = b0 + (int)threadIdx.x; i < b1; i += NT) {
+        const int e = order[i];
+        const int p = (int)A.rpix[off + e];
+        const int y = (int)fdiv((unsigned)p, A.wdiv), x = p - y * A.w;
+        // the eight neighbour lookups are independent: issue them together
+        int nb[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int ddx[8] = {-1, 0, 1, -1, 1, -1, 0, 1}, ddy[8] = {-1, -1, -1, 0, 0, 1, 1, 1};
+            const int nx = x + ddx[q], ny = y + ddy[q];
+            nb[q] = (nx < 0 || ny < 0 || nx >= A.w || ny >= A.h) ? -1 : __ldg(A.pos2idx + (size_t)ny * A.w + nx);
+        }
+        bool act[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) act[q] = nb[q] >= 0 && lev[nb[q] - off] >= L;
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+            if (act[q]) sunion(par, e, nb[q] - off, P, status);
+    }
+    __syncthreads();
+}
+
+// levels, level counts, level order (highest level first)
+template <int NT>
+__device__ __forceinline__ void dl_levels(const DebArgs &A, int P, const unsigned *pix, const float *thr,
+                                          unsigned char *lev, unsigned short *order, int *lvcnt, int *lvstart,
+                                          int *lvcur, bool count_levpix) {
+    for (int i = threadIdx.x; i <= A.N; i += NT) {
+        lvcnt[i] = 0;
+        if (i < DB_MAXLEV) lvcur[i] = 0;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < P; k += NT) {
+        float c = A.cd[pix[k]];
+        int lo = 0, hi = A.N - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (c >= thr[mid])
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        lev[k] = (unsigned char)lo;
+        atomicAdd(&lvcnt[lo], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0;
+        unsigned long long lp = 0;
+        for (int L = A.N - 1; L >= 0; L--) {
+            lvstart[L] = s;
+            s += lvcnt[L];
+            lp += (unsigned long long)L * lvcnt[L];
+        }
+        if (count_levpix) atomicAdd(&A.sc->levpix, lp);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < P; k += NT) {
+        int L = lev[k];
+        order[lvstart[L] + atomicAdd(&lvcur[L], 1)] = (unsigned short)k;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// sweep: branch tree, MINCONT cut, kept branches
+// ---------------------------------------------------------------------------
+template <int NT>
+__device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, unsigned char *base, int cap,
+                                              int *glist, int *gcount) {
+    __shared__ float thr[DB_MAXLEV];
+    __shared__ int lvcnt[DB_MAXLEV + 1], lvstart[DB_MAXLEV + 1], lvcur[DB_MAXLEV];
+    __shared__ int s_nrl[2], s_nn[2], s_nkept;
+    __shared__ unsigned s_peak;
+    __shared__ XSum s_part[NT / 32];
+    __shared__ float s_fdflux;
+    const int tid = threadIdx.x;
+    const int off = A.R.off[r], P = A.R.size[r];
+    const unsigned *pix = A.rpix + off;
+    if (!base) {  // global-memory arena: 48 B per element at the root's offset
+        base = A.D.arena + (size_t)off * DL_ARENA_BYTES;
+        cap = P;
+    }
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(base);
+    int *par = reinterpret_cast<int *>(acc + cap);
+    int *sz = par + cap;
+    // two-level arrays: level slot s of X is X0 + s * cap (arithmetic, so
+    // that no pointer table lands in local memory)
+    int *const nds0 = sz + cap;
+    unsigned *const nfl0 = reinterpret_cast<unsigned *>(sz + 3 * cap);
+    unsigned short *const order = reinterpret_cast<unsigned short *>(sz + 5 * cap);
+    unsigned short *const rl0 = order + cap;
+    unsigned short *const nid = order + 3 * cap;
+    unsigned short *const ndr0 = order + 4 * cap;
+    unsigned char *const lev = reinterpret_cast<unsigned char *>(order + 6 * cap);
+#define NDS(s) (nds0 + (s) * cap)
+#define NFL(s) (nfl0 + (s) * cap)
+#define RL(s) (rl0 + (s) * cap)
+#define NDR(s) (ndr0 + (s) * cap)
+    unsigned long long *kept = A.D.kept + off;
+    const int e0 = A.sc->e0cd;
+    int *status = &A.sc->status;
+
+    // fdpeak, exact fdflux, completion keys (as k_deblend_sweep)
+    if (tid == 0) {
+        s_peak = 0u;
+        s_nkept = 0;
+        s_nrl[0] = s_nrl[1] = s_nn[0] = s_nn[1] = 0;
+    }
+    __syncthreads();
+    XSum xs;
+    xs_init(xs);
+    unsigned pk = 0u;
+    for (int k = tid; k < P; k += NT) {
+        float c = A.cd[pix[k]];
+        xs_add(xs, c);
+        pk = max(pk, f2ord(c));
+    }
+    xs = xs_warp_sum(xs);
+    if ((tid & 31) == 0) s_part[tid >> 5] = xs;
+    atomicMax(&s_peak, pk);
+    {
+        const int ymax = (int)fdiv(pix[P - 1], A.wdiv);
+        for (int k = tid; k < P; k += NT) {
+            const int y = (int)fdiv(pix[k], A.wdiv);
+            if (y == ymax && (k == 0 || (int)fdiv(pix[k - 1], A.wdiv) < ymax)) {
+                A.R.ymax[r] = ymax;
+                A.R.lastx[r] = (int)pix[k] - ymax * A.w;
+            }
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        XSum t = s_part[0];
+        for (int k = 1; k < NT / 32; k++) xs_merge(t, s_part[k]);
+        if (t.ovf) atomicOr(status, SX_ST_RANGE);
+        s_fdflux = xs_float(t);
+        A.R.fdflux[r] = s_fdflux;
+        A.R.fdpeak[r] = ord2f(s_peak);
+        A.R.first[r] = (int)pix[0];
+    }
+    __syncthreads();
+    const float fdpeak = ord2f(s_peak);
+    if (!dl_range_ok(fdpeak, e0, P)) {
+        if (tid == 0) glist[atomicAdd(gcount, 1)] = r;
+        return;
+    }
+    const double value0 = (double)s_fdflux * A.mincont;
+    block_thresholds(A, fdpeak, thr);
+    __syncthreads();
+    dl_levels<NT>(A, P, pix, thr, lev, order, lvcnt, lvstart, lvcur, true);
+
+    int cur = 0, lastL = -1;
+    for (int L = A.N - 1; L >= 0; L--) {
+        const int cnt = lvcnt[L];
+        if (cnt == 0) continue;
+        const int prv = cur ^ 1, cl = L + 1;
+        const int b0 = lvstart[L], b1 = b0 + cnt;
+        const int nold = lastL >= 0 ? s_nrl[prv] : 0;
+        const int nprev = lastL >= 0 ? s_nn[prv] : 0;
+        // (a) sizes and fluxes of the new pixels; the children re-flagged at
+        // level L+1 when the levels since the last populated one were empty
+        for (int i = b0 + tid; i < b1; i += NT) {
+            const int e = order[i];
+            sz[e] = 1;
+            acc[e] = dl_term(A.cd[pix[e]], e0);
+        }
+        if (lastL > cl)
+            for (int i = tid; i < nprev; i += NT) {
+                const int c = NDR(prv)[i];
+                const float lhs = dl_flux(acc[c], e0) - thr[cl] * (float)(unsigned)sz[c];
+                NFL(prv)[i] = (NFL(prv)[i] & ~1u) | (lhs > value0 ? 1u : 0u);
+            }
+        // (b) activation and unions
+        dl_activate_union<NT>(A, off, P, L, b0, b1, order, par, lev, status);
+        // (c) roots that joined another component hand over size and flux
+        for (int i = tid; i < nold + cnt; i += NT) {
+            const int c = i < nold ? RL(prv)[i] : order[b0 + i - nold];
+            if (par[c] != c) {
+                const int rt = sfind_c(par, c, P, status);
+                atomicAdd(&sz[rt], sz[c]);
+                atomicAdd(&acc[rt], acc[c]);
+            } else {
+                RL(cur)[atomicAdd(&s_nrl[cur], 1)] = (unsigned short)c;
+            }
+        }
+        __syncthreads();
+        // (d) this level's branches
+        const int nr = s_nrl[cur];
+        for (int i = tid; i < nr; i += NT) {
+            const int c = RL(cur)[i], s = sz[c];
+            if (s >= A.debminarea) {
+                const int k = atomicAdd(&s_nn[cur], 1);
+                NDR(cur)[k] = (unsigned short)c;
+                nid[c] = (unsigned short)k;
+                const float lhs = dl_flux(acc[c], e0) - thr[L] * (float)(unsigned)s;
+                NFL(cur)[k] = (lhs > value0 ? 1u : 0u) | 2u;
+                NDS(cur)[k] = 0;
+            }
+        }
+        __syncthreads();
+        // (e) children report to their parent
+        for (int i = tid; i < nprev; i += NT) {
+            const int p = nid[sfind_c(par, NDR(prv)[i], P, status)];
+            const unsigned f = NFL(prv)[i];
+            NDS(prv)[i] = p;
+            if (f & 1u) atomicAdd(&NDS(cur)[p], 1);
+            if (!(f & 4u)) atomicAnd(&NFL(cur)[p], ~2u);
+        }
+        __syncthreads();
+        // (f) cut decisions for the children; (g) ok-after for this level
+        for (int i = tid; i < nprev; i += NT) {
+            const unsigned f = NFL(prv)[i];
+            if ((f & 5u) == 5u && NDS(cur)[NDS(prv)[i]] > 1) {
+                const int k = atomicAdd(&s_nkept, 1);
+                kept[k] = ((unsigned long long)cl << 32) | NDR(prv)[i];
+            }
+        }
+        const int ncur = s_nn[cur];
+        for (int i = tid; i < ncur; i += NT) {
+            const unsigned f = NFL(cur)[i];
+            if ((f & 2u) && NDS(cur)[i] <= 1) NFL(cur)[i] = f | 4u;
+        }
+        if (tid == 0) {
+            s_nrl[prv] = 0;
+            s_nn[prv] = 0;
+        }
+        __syncthreads();
+        lastL = L;
+        cur = prv;
+    }
+    // level 0: the whole object is one branch
+    const int fin = cur ^ 1;
+    if (tid == 0) {
+        int nk = s_nkept;
+        for (int i = 0; i < s_nn[fin]; i++)
+            if (NFL(fin)[i] & 4u) kept[nk++] = (unsigned long long)NDR(fin)[i];
+        A.R.nkept[r] = nk;
+    }
+#undef NDS
+#undef NFL
+#undef RL
+#undef NDR
+}
+
+// ---------------------------------------------------------------------------
+// assignment: ownership of the kept branches, their preanalysis, gatherup
+// ---------------------------------------------------------------------------
+template <int NT>
+__device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, unsigned char *base, int cap) {
+    __shared__ float thr[DB_MAXLEV];
+    __shared__ int lvcnt[DB_MAXLEV + 1], lvstart[DB_MAXLEV + 1], lvcur[DB_MAXLEV], lvkept[DB_MAXLEV];
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int off = A.R.off[r], P = A.R.size[r];
+    const float fdpeak = A.R.fdpeak[r];
+    const int e0 = A.sc->e0cd;
+    if (!dl_range_ok(fdpeak, e0, P)) return;  // done by the global kernels
+    const int K = A.R.nkept[r], ob = A.R.objbase[r];
+    const unsigned *pix = A.rpix + off;
+    const unsigned long long *kept = A.D.kept + off;
+    if (!base) {
+        base = A.D.arena + (size_t)off * DL_ARENA_BYTES;
+        cap = P;
+    }
+    unsigned long long *kept2 = reinterpret_cast<unsigned long long *>(base);
+    int *par = reinterpret_cast<int *>(kept2 + cap);
+    int *bcnt = par + cap, *bstart = bcnt + cap, *bcur = bstart + cap;
+    unsigned short *order = reinterpret_cast<unsigned short *>(bcur + cap);
+    unsigned short *blist = order + cap;
+    short *own = reinterpret_cast<short *>(blist + cap);
+    unsigned short *kidx = reinterpret_cast<unsigned short *>(own + cap);
+    unsigned char *lev = reinterpret_cast<unsigned char *>(kidx + cap);
+    unsigned char *kl = lev + cap;
+    int *status = &A.sc->status;
+
+    block_thresholds(A, fdpeak, thr);
+    for (int i = tid; i < DB_MAXLEV; i += NT) lvkept[i] = 0;
+    for (int k = tid; k < P; k += NT) {
+        own[k] = -1;
+        kl[k] = 0xff;
+    }
+    for (int k = tid; k < K; k += NT) bcnt[k] = bcur[k] = 0;
+    __syncthreads();
+    dl_levels<NT>(A, P, pix, thr, lev, order, lvcnt, lvstart, lvcur, false);
+    // kept list in (level, element) order
+    for (int i = tid; i < K; i += NT) {
+        const unsigned long long key = kept[i];
+        int rank = 0;
+        for (int j = 0; j < K; j++) rank += kept[j] < key;
+        kept2[rank] = key;
+    }
+    __syncthreads();
+    for (int i = tid; i < K; i += NT) {
+        const unsigned long long key = kept2[i];
+        const int L = (int)(key >> 32), c = (int)(key & 0xffffffffu);
+        kl[c] = (unsigned char)L;
+        kidx[c] = (unsigned short)i;
+        atomicAdd(&lvkept[L], 1);
+    }
+    __syncthreads();
+    // replay of the sweep; at levels with kept branches label their pixels
+    for (int L = A.N - 1; L >= 0; L--) {
+        const int b0 = lvstart[L], b1 = b0 + lvcnt[L];
+        if (lvcnt[L]) dl_activate_union<NT>(A, off, P, L, b0, b1, order, par, lev, status);
+        if (lvkept[L]) {
+            for (int i = tid; i < b1; i += NT) {
+                const int e = order[i];
+                const int rt = sfind_c(par, e, P, status);
+                if (kl[rt] == L) own[e] = (short)kidx[rt];
+            }
+            __syncthreads();
+        }
+    }
+    // owned pixels grouped by branch (counting sort)
+    for (int e = tid; e < P; e += NT)
+        if (own[e] >= 0) atomicAdd(&bcnt[own[e]], 1);
+    __syncthreads();
+    if (tid == 0) {
+        int s = 0;
+        for (int k = 0; k < K; k++) {
+            bstart[k] = s;
+            s += bcnt[k];
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < P; e += NT) {
+        const int k = own[e];
+        if (k >= 0) blist[bstart[k] + atomicAdd(&bcur[k], 1)] = (unsigned short)e;
+    }
+    __syncthreads();
+    // preanalysis of each kept branch over its own pixels, one warp per branch
+    for (int k = tid >> 5; k < K; k += NT / 32) {
+        const int o = ob + k, L = (int)(kept2[k] >> 32), nb = bcnt[k], bb = bstart[k];
+        int xmin = 0x7fffffff, xmax = -1, ymin = 0x7fffffff, ymax = -1;
+        unsigned pk = 0u, cpk = 0u;
+        XSum srv;
+        xs_init(srv);
+        for (int i = lane; i < nb; i += 32) {
+            const unsigned p = pix[blist[bb + i]];
+            const int y = (int)fdiv(p, A.wdiv), x = (int)p - y * A.w;
+            xmin = min(xmin, x);
+            xmax = max(xmax, x);
+            ymin = min(ymin, y);
+            ymax = max(ymax, y);
+            pk = max(pk, f2ord(A.sub[p]));
+            const float c = A.cd[p];
+            cpk = max(cpk, f2ord(c));
+            xs_add(srv, c);
+        }
+        for (int d = 16; d > 0; d >>= 1) {
+            xmin = min(xmin, __shfl_xor_sync(0xffffffffu, xmin, d));
+            xmax = max(xmax, __shfl_xor_sync(0xffffffffu, xmax, d));
+            ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, d));
+            ymax = max(ymax, __shfl_xor_sync(0xffffffffu, ymax, d));
+            pk = max(pk, __shfl_xor_sync(0xffffffffu, pk, d));
+            cpk = max(cpk, __shfl_xor_sync(0xffffffffu, cpk, d));
+        }
+        srv = xs_warp_sum(srv);
+        const float peak = ord2f(pk);
+        const double dthresh = thr[L], dthresh2 = (dthresh + peak) / 2.0;
+        XSum smx, smy, smx2, smy2, smxy, stv;
+        xs_init(smx);
+        xs_init(smy);
+        xs_init(smx2);
+        xs_init(smy2);
+        xs_init(smxy);
+        xs_init(stv);
+        int dnpix = 0, area2 = 0;
+        for (int i = lane; i < nb; i += 32) {
+            const unsigned p = pix[blist[bb + i]];
+            const int yy = (int)fdiv(p, A.wdiv), x = (int)p - yy * A.w - xmin, y = yy - ymin;
+            const float cval = A.cd[p], val = A.sub[p];
+            dnpix += val > dthresh;
+            area2 += val > dthresh2;
+            xs_add(smx, cval * x);
+            xs_add(smy, cval * y);
+            xs_add(smx2, cval * x * x);
+            xs_add(smy2, cval * y * y);
+            xs_add(smxy, cval * x * y);
+            xs_add(stv, val);
+        }
+        for (int d = 16; d > 0; d >>= 1) {
+            dnpix += __shfl_xor_sync(0xffffffffu, dnpix, d);
+            area2 += __shfl_xor_sync(0xffffffffu, area2, d);
+        }
+        smx = xs_warp_sum(smx);
+        smy = xs_warp_sum(smy);
+        smx2 = xs_warp_sum(smx2);
+        smy2 = xs_warp_sum(smy2);
+        smxy = xs_warp_sum(smxy);
+        stv = xs_warp_sum(stv);
+        if (lane != 0) continue;
+        if (srv.ovf | smx.ovf | smy.ovf | smx2.ovf | smy2.ovf | smxy.ovf | stv.ovf) atomicOr(status, SX_ST_RANGE);
+        int flag = 0;
+        if (L > 0) flag |= SX_OBJ_MERGED;
+        if (xmin == 0 || xmax == A.w - 1 || ymin == 0 || ymax == A.h - 1) flag |= SX_OBJ_TRUNC;
+        const float rv = xs_float(srv);
+        const double rvd = rv;
+        const double mx = xs_double(smx), my = xs_double(smy);
+        const double mx2 = xs_double(smx2), my2 = xs_double(smy2), mxy = xs_double(smxy);
+        const double xm = mx / rvd, ym = my / rvd;
+        double xm2 = mx2 / rvd - xm * xm, ym2 = my2 / rvd - ym * ym, xym = mxy / rvd - xm * ym;
+        double temp, temp2, theta, pmx2, pmy2, darea, t1t2;
+        int singu = 0;
+        if ((temp2 = xm2 * ym2 - xym * xym) < 0.00694) {
+            xm2 += 0.0833333;
+            ym2 += 0.0833333;
+            temp2 = xm2 * ym2 - xym * xym;
+            singu = 1;
+        }
+        if ((fabs(temp = xm2 - ym2)) > 0.0)
+            theta = atan2(2.0 * xym, temp) / 2.0;
+        else
+            theta = SX_PI / 4.0;
+        temp = sqrt(0.25 * temp * temp + xym * xym);
+        pmy2 = pmx2 = 0.5 * (xm2 + ym2);
+        pmx2 += temp;
+        pmy2 -= temp;
+        const float fa = (float)sqrt(pmx2), fb = (float)sqrt(pmy2);
+        float abcor;
+        darea = (double)area2 - dnpix;
+        t1t2 = dthresh / dthresh2;
+        if (t1t2 > 0.0) {
+            abcor = (darea < 0.0 ? darea : -1.0) / (2 * SX_PI * log(t1t2 < 1.0 ? t1t2 : 0.99) * fa * fb);
+            if (abcor > 1.0) abcor = 1.0;
+        } else
+            abcor = 1.0;
+        A.O.root[o] = r;
+        A.O.level[o] = L;
+        A.O.node_dthresh[o] = thr[L];
+        A.O.xmin[o] = xmin;
+        A.O.xmax[o] = xmax;
+        A.O.ymin[o] = ymin;
+        A.O.ymax[o] = ymax;
+        A.O.flags[o] = flag;
+        A.O.singu[o] = singu;
+        A.O.dnpix[o] = dnpix;
+        A.O.fdflux[o] = rv;
+        A.O.dflux[o] = xs_float(stv);
+        A.O.fdpeak[o] = ord2f(cpk);
+        A.O.dpeak[o] = peak;
+        A.O.mx[o] = xm + xmin;
+        A.O.my[o] = ym + ymin;
+        A.O.mx2[o] = xm2;
+        A.O.my2[o] = ym2;
+        A.O.mxy[o] = xym;
+        A.O.a[o] = fa;
+        A.O.b[o] = fb;
+        A.O.theta[o] = theta * 180.0 / SX_PI;
+        A.O.cxx[o] = (float)(ym2 / temp2);
+        A.O.cyy[o] = (float)(xm2 / temp2);
+        A.O.cxy[o] = (float)(-2 * xym / temp2);
+        A.O.abcor[o] = abcor;
+        A.O.n[o] = bcnt[k];
+    }
+    __syncthreads();
+    // gatherup (cudadeblend.cu:1262-1360): the nearest kept branch in the
+    // elliptical metric, first in order on ties
+    for (int e = tid; e < P; e += NT) {
+        int k = own[e];
+        const unsigned p = pix[e];
+        if (k < 0) {
+            const int y = (int)fdiv(p, A.wdiv), x = (int)p - y * A.w;
+            int iclst = 0;
+            float distmin = 1e+31f, dx, dy, dist;
+            for (int i = 0; i < K; i++) {
+                const int o = ob + i;
+                dx = x - A.O.mx[o];
+                dy = y - A.O.my[o];
+                dist = 0.5 * (A.O.cxx[o] * dx * dx + A.O.cyy[o] * dy * dy + A.O.cxy[o] * dx * dy) / A.O.abcor[o];
+                if (dist < distmin) {
+                    distmin = dist;
+                    iclst = i;
+                }
+            }
+            k = iclst;
+            atomicAdd(&A.O.n[ob + k], 1);
+        }
+        A.alloc[p] = ob + k;
+        A.objkey[off + e] = (unsigned)(ob + k);
+    }
+}
+
+// Persistent CTAs: each takes the next root of its list from a device
+// cursor until the list is exhausted, so the grid is sized to the resident
+// capacity rather than to the (device-side) length of the list.
+// cap > 0: per-object state in dynamic shared memory of cap elements;
+// cap == 0: in the global arena
+// Up to three lists of objects taken in order through one device cursor
+// (the larger size classes first, so the longest objects start earliest).
+struct RootLists {
+    const int *list[3];
+    const int *count[3];
+};
+
+__device__ __forceinline__ int rl_item(const RootLists &L, int c) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        if (!L.list[k]) return -1;
+        const int n = *L.count[k];
+        if (c < n) return L.list[k][c];
+        c -= n;
+    }
+    return -1;
+}
+
+// cap > 0: per-object state in dynamic shared memory of cap elements;
+// cap == 0: in the global arena
+template <int NT>
+__global__ void __launch_bounds__(NT) k_dl_sweep(const __grid_constant__ DebArgs A, const RootLists L, int *cursor,
+                                                 int cap, int *glist, int *gcount) {
+    extern __shared__ __align__(16) unsigned char dl_smem[];
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = rl_item(L, atomicAdd(cursor, 1));
+        __syncthreads();
+        const int r = s_item;
+        __syncthreads();
+        if (r < 0) break;
+        dl_sweep_root<NT>(A, r, cap ? dl_smem : nullptr, cap, glist, gcount);
+        __syncthreads();
+    }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_dl_assign(const __grid_constant__ DebArgs A, const RootLists L, int *cursor,
+                                                  int cap) {
+    extern __shared__ __align__(16) unsigned char dl_smem[];
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = rl_item(L, atomicAdd(cursor, 1));
+        __syncthreads();
+        const int r = s_item;
+        __syncthreads();
+        if (r < 0) break;
+        dl_assign_root<NT>(A, r, cap ? dl_smem : nullptr, cap);
+        __syncthreads();
+    }
+}
+
+// Size classes (list k at lists + k * nroots, its length in counts[k]):
+//   0  <= 256 pixels             shared memory, one warp
+//   1  (1024, 2048]   2 (256, 1024]       arena, 64 threads
+//   3  > 8192   4 (4096, 8192]   5 (2048, 4096]   arena, 256 threads
+//   6  > 32767 pixels            128-bit global kernels
+//   7  objects the compact sweeps hand over (flux range beyond 64 bits)
+// counts[8..15] are the sweep cursors, counts[16..23] the assignment cursors.
+constexpr int DL_NLISTS = 8;
+
+__global__ void k_split_roots(const int *size, int n, int *lists, int *counts) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int s = size[r];
+    int t;
+    if (s <= DL_CAP0)
+        t = 0;
+    else if (s <= DL_MID)
+        t = s > DL_MID / 2 ? 1 : 2;
+    else if (s <= DL_ARENA_MAX)
+        t = s > 4 * DL_MID ? 3 : s > 2 * DL_MID ? 4 : 5;
+    else
+        t = 6;
+    lists[(size_t)t * n + atomicAdd(&counts[t], 1)] = r;
+}
+
+// resident CTAs of a kernel on this device (cached per kernel and device)
+template <typename K>
+static int dl_grid(K kernel, int nt, size_t smem, int *cache) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cache[dev]) {
+        int nsm = 0, per = 0;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, nt, smem);
+        cache[dev] = max(1, nsm) * max(1, per);
+    }
+    return cache[dev];
+}
+
+static RootLists dl_lists(const int *lists, int *counts, size_t n, int a, int b = -1, int c = -1) {
+    RootLists L;
+    const int k[3] = {a, b, c};
+    for (int i = 0; i < 3; i++) {
+        L.list[i] = k[i] >= 0 ? lists + (size_t)k[i] * n : nullptr;
+        L.count[i] = k[i] >= 0 ? counts + k[i] : nullptr;
+    }
+    return L;
+}
+
+void launch_deblend_split(const int *size, int nroots, int *lists, int *counts, cudaStream_t st) {
+    cudaMemsetAsync(counts, 0, 3 * DL_NLISTS * sizeof(int), st);
+    if (nroots > 0) k_split_roots<<<(nroots + 255) / 256, 256, 0, st>>>(size, nroots, lists, counts);
+}
+
+// The large size classes go first, on two side streams, so that their long
+// per-object latency overlaps the many small objects on the main stream; the
+// objects handed over by the compact sweeps are swept last, after the join.
+void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S) {
+    if (nroots <= 0) return;
+    static int g0[64], g1[64], g2[64], g3[64];
+    const size_t n = (size_t)nroots;
+    int *glist = const_cast<int *>(lists) + 7 * n;
+    const size_t m0 = DL_CAP0 * DL_SWEEP_BYTES;
+    cudaEventRecord(S.fork, S.main);
+    cudaStreamWaitEvent(S.side[0], S.fork, 0);
+    cudaStreamWaitEvent(S.side[1], S.fork, 0);
+    const int grid3 = min(nroots, dl_grid(k_deblend_sweep, DB_THREADS, 0, g3));
+    k_deblend_sweep<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 6 * n, counts + 6, counts + 14);
+    k_dl_sweep<256><<<min(nroots, dl_grid(k_dl_sweep<256>, 256, 0, g2)), 256, 0, S.side[1]>>>(
+        A, dl_lists(lists, counts, n, 3, 4, 5), counts + 10, 0, glist, counts + 7);
+    k_dl_sweep<64><<<min(nroots, dl_grid(k_dl_sweep<64>, 64, 0, g1)), 64, 0, S.main>>>(
+        A, dl_lists(lists, counts, n, 1, 2), counts + 9, 0, glist, counts + 7);
+    k_dl_sweep<32><<<min(nroots, dl_grid(k_dl_sweep<32>, 32, m0, g0)), 32, m0, S.main>>>(
+        A, dl_lists(lists, counts, n, 0), counts + 8, DL_CAP0, glist, counts + 7);
+    cudaEventRecord(S.join[0], S.side[0]);
+    cudaEventRecord(S.join[1], S.side[1]);
+    cudaStreamWaitEvent(S.main, S.join[0], 0);
+    cudaStreamWaitEvent(S.main, S.join[1], 0);
+    k_deblend_sweep<<<grid3, DB_THREADS, 0, S.main>>>(A, glist, counts + 7, counts + 15);
+}
+
+void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S) {
+    if (nroots <= 0) return;
+    static int g0[64], g1[64], g2[64], g3[64];
+    const size_t n = (size_t)nroots;
+    const size_t m0 = DL_CAP0 * DL_ASSIGN_BYTES;
+    cudaEventRecord(S.fork, S.main);
+    cudaStreamWaitEvent(S.side[0], S.fork, 0);
+    cudaStreamWaitEvent(S.side[1], S.fork, 0);
+    const int grid3 = min(nroots, dl_grid(k_deblend_assign, DB_THREADS, 0, g3));
+    k_deblend_assign<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 6 * n, counts + 6, counts + 22);
+    k_deblend_assign<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 7 * n, counts + 7, counts + 23);
+    k_dl_assign<256><<<min(nroots, dl_grid(k_dl_assign<256>, 256, 0, g2)), 256, 0, S.side[1]>>>(
+        A, dl_lists(lists, counts, n, 3, 4, 5), counts + 18, 0);
+    k_dl_assign<64><<<min(nroots, dl_grid(k_dl_assign<64>, 64, 0, g1)), 64, 0, S.main>>>(
+        A, dl_lists(lists, counts, n, 1, 2), counts + 17, 0);
+    k_dl_assign<32><<<min(nroots, dl_grid(k_dl_assign<32>, 32, m0, g0)), 32, m0, S.main>>>(
+        A, dl_lists(lists, counts, n, 0), counts + 16, DL_CAP0);
+    cudaEventRecord(S.join[0], S.side[0]);
+    cudaEventRecord(S.join[1], S.side[1]);
+    cudaStreamWaitEvent(S.main, S.join[0], 0);
+    cudaStreamWaitEvent(S.main, S.join[1], 0);
+}
+
+}  // namespace sx

@@ -33,9 +33,8 @@ struct DebBufs {
     int *nd_oka0, *nd_oka1;
     unsigned long long *kept;           // packed (level << 32) | element, per root at its offset
     int *own, *kl, *kidx;
-    // per-kept-object accumulators (index = root offset + kept index)
-    unsigned long long *pacc;           // 7 sums x 4 limbs
     int *pint;                          // xmin, xmax, ymin, ymax, peak(ord), cpeak(ord), dnpix, area2
+    unsigned char *arena;               // 48 B per element: the compact per-object state of k_dl_*
 };
 
 // per-object data (index = object id: root order, then (level, label))
@@ -77,11 +76,18 @@ struct DebArgs {
     int *alloc;                 // W*H object id map (-1 elsewhere)
     unsigned *objkey;           // object id per root-list element
     int w, h, N, debminarea;
+    FastDiv wdiv;
     double mincont;
 };
 
+// the main stream, two side streams and the events that fork and join them
+struct DebStreams {
+    cudaStream_t main, side[2];
+    cudaEvent_t fork, join[2];
+};
+
 void launch_deblend_split(const int *size, int nroots, int *lists, int *counts, cudaStream_t st);
-void launch_deblend_sweep(const DebArgs &A, const int *lists, const int *counts, int nroots, cudaStream_t st);
-void launch_deblend_assign(const DebArgs &A, const int *lists, const int *counts, int nroots, cudaStream_t st);
+void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S);
+void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S);
 
 }  // namespace sx

@@ -23,6 +23,7 @@
 #include "k_detect.cu"
 #include "k_roots.cu"
 #include "k_deblend.cu"
+#include "k_deblend_local.cu"
 #include "k_analyse.cu"
 #include "k_post.cu"
 
@@ -43,9 +44,25 @@ struct StageRec {
 
 }  // namespace
 
+namespace {
+struct PipeState {
+    FrameParams Pm;
+    int w = 0, h = 0;
+    const float *d_img = nullptr;
+    int nroots = 0, nrootpix = 0, nobj = 0, ns = 0;
+    int stage = 0;  // last completed: 1 background ... 6 catalogue
+    BackBufs B;
+    RootBufs R;
+    DebArgs A;
+};
+}  // namespace
+
 struct sexgpu_ctx {
     int device = 0;
+    PipeState ps;
     cudaStream_t stream = nullptr;
+    cudaStream_t side[2] = {nullptr, nullptr};  // fork/join helpers of the deblending
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     bool own_stream = false;
     std::vector<DevBuf *> bufs;
     std::string err;
@@ -59,7 +76,7 @@ struct sexgpu_ctx {
     DevBuf rsize, roff, rfirst, rymax, rlastx, rfdpeak, rfdflux, rnkept, robjbase, rlists, rcounts;
     // deblend scratch
     DevBuf dpar, dlev, dsz, dorder, drl0, drl1, dnid0, dnid1, dacc, nr0, nr1, nf0, nf1, ns0, ns1, nc0, nc1, na0, na1,
-        dkept, down, dkl, dkidx, dpacc, dpint, objkey, rpix;
+        dkept, down, dkl, dkidx, dpint, objkey, rpix, darena;
     // objects
     DevBuf o_i[20], o_f[30], o_d[10], o_iso, o_sortkey, amp, alpha, cellhead, cellnext, vkey, vval, vkalt, vvalt,
         skeys, svals, skalt, svalt, rows;
@@ -329,16 +346,27 @@ int alloc_objects(sexgpu_ctx *ctx, int nobj) {
 
 unsigned grid1(long long n, int t) { return n > 0 ? (unsigned)((n + t - 1) / t) : 1u; }
 
-// the whole pipeline on a device-resident frame
-int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu_config *cfg) {
+// ---------------------------------------------------------------------------
+// The pipeline in resumable stages: pipe_begin (buffers, background),
+// pipe_detect (subtraction, filter, threshold, components, raw objects),
+// pipe_deblend, pipe_analyse, pipe_clean, pipe_end (photometry, catalogue).
+// State that crosses stages lives in ctx->ps; parameters a later stage reads
+// (ps.Pm) may be changed between stages.
+// ---------------------------------------------------------------------------
+int pipe_begin(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu_config *cfg) {
     int rc = check_config(cfg, w, h);
     if (rc) {
         ctx->err = "invalid configuration or frame size";
         return rc;
     }
     cudaStream_t st = ctx->stream;
-    FrameParams Pm;
+    PipeState &ps = ctx->ps;
+    ps.stage = 0;
+    FrameParams &Pm = ps.Pm;
     make_params(cfg, w, h, Pm);
+    ps.w = w;
+    ps.h = h;
+    ps.d_img = d_img;
     const long long N = (long long)w * h;
     const int nb = Pm.nbx * Pm.nby;
     // ---- buffers sized by the frame
@@ -371,7 +399,7 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     EN(colk, w * 4);
     EN(coldx, w * 4);
     EN(sc, sizeof(FrameScalars));
-    BackBufs B;
+    BackBufs &B = ps.B;
     B.ms = P<MeshStat>(ctx->ms);
     B.back = P<float>(ctx->back);
     B.sigma = P<float>(ctx->sigma);
@@ -402,8 +430,22 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     k_init_scalars<<<1, 1, 0, st>>>(d_sc);
     launch_background(B, d_img, Pm, d_sc, st, nl);
     stage_mark(ctx, "background", nl + 1);
+    ps.stage = 1;
+    return SEXGPU_OK;
+}
 
-    nl = 0;
+int pipe_detect(sexgpu_ctx *ctx) {
+    PipeState &ps = ctx->ps;
+    if (ps.stage != 1) return SEXGPU_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    const FrameParams &Pm = ps.Pm;
+    const int w = ps.w, h = ps.h;
+    const long long N = (long long)w * h;
+    const float *d_img = ps.d_img;
+    BackBufs &B = ps.B;
+    FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
+    int *tmp = P<int>(ctx->scan_tmp);
+    int rc = SEXGPU_OK, nl = 0;
     launch_sub_filter(d_img, P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm, d_sc, nullptr, st, nl);
     stage_mark(ctx, "sub_filter", nl);
 
@@ -424,7 +466,7 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
         ctx->err = "zero or negative threshold";
         return SEXGPU_ERR_THRESH;
     }
-    const int nroots = ctx->hsc.nroots;
+    const int nroots = ps.nroots = ctx->hsc.nroots;
     EN(rsize, (nroots + 1) * 4);
     EN(roff, (nroots + 1) * 4);
     EN(rfirst, (nroots + 1) * 4);
@@ -434,7 +476,7 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     EN(rfdflux, (nroots + 1) * 4);
     EN(rnkept, (nroots + 1) * 4);
     EN(robjbase, (nroots + 1) * 4);
-    RootBufs R;
+    RootBufs &R = ps.R;
     R.size = P<int>(ctx->rsize);
     R.off = P<int>(ctx->roff);
     R.first = P<int>(ctx->rfirst);
@@ -452,7 +494,7 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     k_pix_compact<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, flag, pos, keys, vals, N, Pm.minarea);
     rc = read_scalars(ctx);
     if (rc) return rc;
-    const int nrootpix = ctx->hsc.nrootpix;
+    const int nrootpix = ps.nrootpix = ctx->hsc.nrootpix;
     radix_sort_pairs(keys, vals, P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), nrootpix, bits_for(nroots), tmp, st);
     unsigned *rpix = P<unsigned>(ctx->rpix);
     CK(cudaMemcpyAsync(rpix, vals, (size_t)nrootpix * 4, cudaMemcpyDeviceToDevice, st));
@@ -461,7 +503,22 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     k_pos2idx<<<grid1(nrootpix, 256), 256, 0, st>>>(rpix, pos2idx, nrootpix);
     k_alloc_init<<<grid1(N, 256), 256, 0, st>>>(lab, P<int>(ctx->alloc), N);
     stage_mark(ctx, "roots", 8 + 3 * scan_launches(N) + scan_launches(nroots) + radix_launches(bits_for(nroots), nrootpix));
+    ps.stage = 2;
+    return SEXGPU_OK;
+}
 
+int pipe_deblend(sexgpu_ctx *ctx) {
+    PipeState &ps = ctx->ps;
+    if (ps.stage != 2) return SEXGPU_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    const FrameParams &Pm = ps.Pm;
+    const int w = ps.w, h = ps.h, nroots = ps.nroots, nrootpix = ps.nrootpix;
+    RootBufs &R = ps.R;
+    FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
+    int *tmp = P<int>(ctx->scan_tmp);
+    int *pos2idx = P<int>(ctx->pos2idx);
+    unsigned *rpix = P<unsigned>(ctx->rpix);
+    int rc = SEXGPU_OK;
     // ---- deblending
     size_t M = (size_t)nrootpix + 1;
     EN(dpar, M * 4);
@@ -487,9 +544,9 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     EN(down, M * 4);
     EN(dkl, M * 4);
     EN(dkidx, M * 4);
-    EN(dpacc, M * 28 * 8);
     EN(dpint, M * 8 * 4);
-    DebArgs A;
+    EN(darena, M * DL_ARENA_BYTES);
+    DebArgs &A = ps.A;
     A.cd = P<float>(ctx->cd);
     A.sub = P<float>(ctx->sub);
     A.pos2idx = pos2idx;
@@ -519,8 +576,8 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     D.own = P<int>(ctx->down);
     D.kl = P<int>(ctx->dkl);
     D.kidx = P<int>(ctx->dkidx);
-    D.pacc = P<unsigned long long>(ctx->dpacc);
     D.pint = P<int>(ctx->dpint);
+    D.arena = P<unsigned char>(ctx->darena);
     A.sc = d_sc;
     A.alloc = P<int>(ctx->alloc);
     A.objkey = P<unsigned>(ctx->objkey);
@@ -529,20 +586,43 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     A.N = Pm.nthresh;
     A.debminarea = Pm.debminarea;
     A.mincont = Pm.mincont;
-    EN(rlists, (size_t)(2 * nroots + 2) * 4);
-    EN(rcounts, 16);
+    A.wdiv = make_fastdiv((unsigned)w);
+    EN(rlists, (size_t)(DL_NLISTS * (nroots + 1)) * 4);
+    EN(rcounts, 3 * DL_NLISTS * 4);
+    DebStreams S;
+    S.main = st;
+    S.side[0] = ctx->side[0];
+    S.side[1] = ctx->side[1];
+    S.fork = ctx->ev_fork;
+    S.join[0] = ctx->ev_join[0];
+    S.join[1] = ctx->ev_join[1];
     launch_deblend_split(R.size, nroots, P<int>(ctx->rlists), P<int>(ctx->rcounts), st);
-    launch_deblend_sweep(A, P<int>(ctx->rlists), P<int>(ctx->rcounts), nroots, st);
+    launch_deblend_sweep(A, P<int>(ctx->rlists), P<int>(ctx->rcounts), nroots, S);
     exclusive_scan(R.nkept, R.objbase, nroots, &d_sc->nobj, tmp, st);
     rc = read_scalars(ctx);
     if (rc) return rc;
-    const int nobj = ctx->hsc.nobj;
+    const int nobj = ps.nobj = ctx->hsc.nobj;
     rc = alloc_objects(ctx, nobj);
     if (rc) return rc;
     A.O = ctx->O;
-    launch_deblend_assign(A, P<int>(ctx->rlists), P<int>(ctx->rcounts), nroots, st);
-    stage_mark(ctx, "deblend", 5 + scan_launches(nroots));
+    launch_deblend_assign(A, P<int>(ctx->rlists), P<int>(ctx->rcounts), nroots, S);
+    stage_mark(ctx, "deblend", 11 + scan_launches(nroots));
+    ps.stage = 3;
+    return SEXGPU_OK;
+}
 
+int pipe_analyse(sexgpu_ctx *ctx) {
+    PipeState &ps = ctx->ps;
+    if (ps.stage != 3) return SEXGPU_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    const FrameParams &Pm = ps.Pm;
+    const int w = ps.w, h = ps.h, nobj = ps.nobj, nrootpix = ps.nrootpix;
+    const DebArgs &A = ps.A;
+    const BackBufs &B = ps.B;
+    FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
+    int *tmp = P<int>(ctx->scan_tmp);
+    unsigned *keys = P<unsigned>(ctx->keys), *vals = P<unsigned>(ctx->vals);
+    unsigned *rpix = P<unsigned>(ctx->rpix);
     // ---- object pixel lists (stable by object id: raster order inside)
     ObjBufs &O = ctx->O;
     CK(cudaMemcpyAsync(keys, A.objkey, (size_t)nrootpix * 4, cudaMemcpyDeviceToDevice, st));
@@ -570,7 +650,22 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     AA.wdiv = make_fastdiv((unsigned)w);
     launch_analyse(AA, st);
     stage_mark(ctx, "analyse", 2 + radix_launches(bits_for(nobj), nrootpix) + scan_launches(nobj));
+    ps.stage = 4;
+    return SEXGPU_OK;
+}
 
+int pipe_clean(sexgpu_ctx *ctx) {
+    PipeState &ps = ctx->ps;
+    if (ps.stage != 4) return SEXGPU_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    const FrameParams &Pm = ps.Pm;
+    const int w = ps.w, h = ps.h, nobj = ps.nobj;
+    const DebArgs &A = ps.A;
+    ObjBufs &O = ctx->O;
+    FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
+    int *tmp = P<int>(ctx->scan_tmp);
+    unsigned *vals = P<unsigned>(ctx->vals);
+    int rc = SEXGPU_OK;
     // ---- CLEAN
     int nv = 0;
     int cl_launch = 0;
@@ -611,7 +706,22 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
         CK(cudaMemsetAsync(O.fmaster, 0xff, (size_t)nobj * 4, st));
     }
     stage_mark(ctx, "clean", cl_launch);
+    ps.stage = 5;
+    return SEXGPU_OK;
+}
 
+int pipe_end(sexgpu_ctx *ctx) {
+    PipeState &ps = ctx->ps;
+    if (ps.stage != 5) return SEXGPU_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    const FrameParams &Pm = ps.Pm;
+    const int w = ps.w, h = ps.h, nobj = ps.nobj;
+    const DebArgs &A = ps.A;
+    const RootBufs &R = ps.R;
+    ObjBufs &O = ctx->O;
+    FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
+    int *tmp = P<int>(ctx->scan_tmp);
+    int rc = SEXGPU_OK;
     // ---- photometry / FLAGS
     EndArgs E;
     E.sub = A.sub;
@@ -660,8 +770,22 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu
     ctx->last_h = h;
     ctx->last_nobj = nobj;
     ctx->last_ns = ns;
+    ps.ns = ns;
+    ps.stage = 6;
     return SEXGPU_OK;
 }
+
+// the whole pipeline on a device-resident frame
+int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu_config *cfg) {
+    int rc = pipe_begin(ctx, d_img, w, h, cfg);
+    if (!rc) rc = pipe_detect(ctx);
+    if (!rc) rc = pipe_deblend(ctx);
+    if (!rc) rc = pipe_analyse(ctx);
+    if (!rc) rc = pipe_clean(ctx);
+    if (!rc) rc = pipe_end(ctx);
+    return rc;
+}
+
 
 void fill_summary(sexgpu_ctx *ctx, const FrameParams &P, sexgpu_summary *s) {
     if (!s) return;
@@ -703,6 +827,14 @@ int sexgpu_create(sexgpu_ctx **out, int device) {
         return SEXGPU_ERR_CUDA;
     }
     ctx->own_stream = true;
+    if (cudaStreamCreateWithFlags(&ctx->side[0], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->side[1], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_join[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_join[1], cudaEventDisableTiming) != cudaSuccess) {
+        sexgpu_destroy(ctx);
+        return SEXGPU_ERR_CUDA;
+    }
     *out = ctx;
     return SEXGPU_OK;
 }
@@ -725,8 +857,8 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
                      &ctx->rfdflux, &ctx->rnkept, &ctx->robjbase, &ctx->rlists, &ctx->rcounts, &ctx->dpar, &ctx->dlev, &ctx->dsz, &ctx->dorder,
                      &ctx->drl0, &ctx->drl1, &ctx->dnid0, &ctx->dnid1, &ctx->dacc, &ctx->nr0, &ctx->nr1,
                      &ctx->nf0, &ctx->nf1, &ctx->ns0, &ctx->ns1, &ctx->nc0, &ctx->nc1, &ctx->na0, &ctx->na1,
-                     &ctx->dkept, &ctx->down, &ctx->dkl, &ctx->dkidx, &ctx->dpacc, &ctx->dpint, &ctx->objkey,
-                     &ctx->rpix, &ctx->o_iso, &ctx->o_sortkey, &ctx->amp, &ctx->alpha, &ctx->cellhead,
+                     &ctx->dkept, &ctx->down, &ctx->dkl, &ctx->dkidx, &ctx->dpint, &ctx->objkey,
+                     &ctx->rpix, &ctx->darena, &ctx->o_iso, &ctx->o_sortkey, &ctx->amp, &ctx->alpha, &ctx->cellhead,
                      &ctx->cellnext, &ctx->vkey, &ctx->vval, &ctx->vkalt, &ctx->vvalt, &ctx->skeys, &ctx->svals,
                      &ctx->skalt, &ctx->svalt, &ctx->rows, &ctx->sc};
     for (DevBuf *b : all) free_buf(*b);
@@ -735,6 +867,11 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     for (auto &b : ctx->o_d) free_buf(b);
     for (auto &s : ctx->stages) cudaEventDestroy(s.ev);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    for (int i = 0; i < 2; i++) {
+        if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
+        if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SEXGPU_OK;

@@ -55,3 +55,46 @@ def test_config_rejected_without_device_work():
     lib = sexgpu.lib()
     assert lib.sexgpu_create(None, 0) == -1
     assert lib.sexgpu_destroy(None) == -1
+
+
+COMPAT_NAMES = ["init_device", "clear_device", "back_estimate", "cudaFilter", "init_detection", "run_detection",
+                "clear_detection", "init_deblend", "parcel_out", "clear_deblend", "analyse_gpu", "run_clean",
+                "endobject_gpu", "sexgpu_compat_configure", "sexgpu_compat_set_device",
+                "sexgpu_compat_set_error_handler"]
+
+
+def test_compat_library_exports_reference_names():
+    """libsexgpu_compat.so exports the thirteen entry points of the reference's
+    src/cuda/*.h (and libsexgpu.so none of them)."""
+    import ctypes as C
+    path = os.path.join(ROOT, "gpu-sextractor_b200", "libsexgpu_compat.so")
+    lib = C.CDLL(path)
+    for n in COMPAT_NAMES:
+        assert hasattr(lib, n), n
+    src = open(os.path.join(ROOT, "include", "sexgpu_compat.h")).read()
+    declared = set(re.findall(r"^(?:int|void)\s+(\w+)\s*\(", src, re.M))
+    assert declared == set(COMPAT_NAMES)
+    main = sexgpu.lib()
+    assert not hasattr(main, "init_device") and not hasattr(main, "parcel_out")
+
+
+def test_compat_record_layout():
+    """sexgpu_outobj has the member offsets of the reference's outobjstruct
+    (src/types.h:417-455 with NAPER = 1, 16-byte aligned)."""
+    prog = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "sexgpu_compat.h"
+#define O(m) (int)offsetof(sexgpu_outobj, m)
+int main(void) {
+  printf("%d %d %d %d %d %d %d %d %d %d %d %d\n", (int)sizeof(sexgpu_outobj), O(alpha2000), O(sposx),
+         O(flux_aper), O(magerr_aper), O(theta), O(poserr_mx2), O(poserr_mxy), O(flag), O(elong), O(sprob), O(fwhm));
+  return 0;
+}'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(prog)
+        exe = os.path.join(d, "t")
+        subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe])
+        vals = [int(v) for v in subprocess.check_output([exe]).split()]
+    assert vals == [160, 8, 24, 56, 68, 88, 96, 112, 120, 124, 132, 148]

@@ -1,0 +1,78 @@
+"""The reference's own call sequence (makeback + scanimage, through the
+thirteen entry points of libsexgpu_compat.so) gives the catalogue of
+sexgpu_extract: the same surviving objects, in object index order, with the
+record fields scanimage() prints, and the same background-subtracted frame.
+
+tests/compat/scan_like.c is the driver; it is compiled here with gcc."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import sexgpu
+import synth
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "gpu-sextractor_b200")
+
+OUTOBJ = np.dtype({
+    "names": ["number", "alpha2000", "delta2000", "sposx", "sposy", "flux_iso", "fluxerr_iso", "mag_iso",
+              "magerr_iso", "flux_isocor", "fluxerr_isocor", "flux_aper", "fluxerr_aper", "mag_aper",
+              "magerr_aper", "flux_auto", "fluxerr_auto", "mag_auto", "magerr_auto", "theta", "poserr_mx2",
+              "poserr_my2", "poserr_mxy", "flag", "elong", "ellip", "sprob", "peak", "kronfactor", "bkg", "fwhm"],
+    "formats": ["i4", "f8", "f8"] + ["f4"] * 17 + ["f8"] * 3 + ["i2"] + ["f4"] * 7,
+    "offsets": [0, 8, 16, 24, 28, 32, 36, 40, 44, 48, 52, 56, 60, 64, 68, 72, 76, 80, 84, 88, 96, 104, 112, 120,
+                124, 128, 132, 136, 140, 144, 148],
+    "itemsize": 160})
+
+
+@pytest.fixture(scope="module")
+def harness(tmp_path_factory):
+    d = tmp_path_factory.mktemp("compat")
+    exe = str(d / "scan_like")
+    subprocess.check_call(["gcc", "-O2", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "compat", "scan_like.c"), "-o", exe, "-L", PKG,
+                           "-lsexgpu_compat", "-Wl,-rpath," + PKG])
+    return exe, d
+
+
+@pytest.mark.parametrize("case", ["c0", "crowded"])
+def test_reference_call_sequence(gpu_ctx, masks, harness, case):
+    exe, d = harness
+    if case == "c0":
+        img = synth.frame_c0(seed=31, w=640, h=480, nsrc=600)
+        mask = masks["default"]
+        opts = dict(back_size=64, back_filtersize=3, clean_flag=1, clean_param=1.0, gain=0.0, satur_level=50000.0)
+    else:
+        img = synth.frame_c1(seed=32, w=700, h=600, nsrc=4000)
+        mask = masks["gauss_2.5_5x5"]
+        opts = dict(back_size=48, back_filtersize=5, clean_flag=1, clean_param=1.5, gain=2.0, satur_level=4e4)
+    h, w = img.shape
+    fimg, fmask = d / ("%s_img.f32" % case), d / ("%s_mask.f32" % case)
+    frows, fsub = d / ("%s_rows.bin" % case), d / ("%s_sub.f32" % case)
+    img.astype(np.float32).tofile(fimg)
+    mask.astype(np.float32).tofile(fmask)
+    args = [exe, str(fimg), str(w), str(h), str(fmask), str(mask.shape[0]), str(frows), str(fsub),
+            str(opts["back_size"]), str(opts["back_filtersize"]), "0.0", "1.5", "1.5", "5", "32", "0.005",
+            str(opts["clean_flag"]), repr(opts["clean_param"]), repr(opts["gain"]), repr(opts["satur_level"])]
+    out = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    rows = np.fromfile(frows, OUTOBJ)
+    sub_c = np.fromfile(fsub, np.float32).reshape(h, w)
+
+    g, seg, s, sub_g, cd_g = gpu_ctx.extract(img, conv=mask, numbering=1, want_maps=True, **opts)
+    assert np.array_equal(sub_c, sub_g)
+    assert len(rows) == len(g) == s.nobj
+    assert np.array_equal(rows["number"], np.arange(len(g)))
+    assert np.array_equal(rows["sposx"], (g["mx"] + 1.0).astype(np.float32))
+    assert np.array_equal(rows["sposy"], (g["my"] + 1.0).astype(np.float32))
+    for name in ["flux_iso", "fluxerr_iso", "mag_iso", "magerr_iso", "flux_isocor", "fluxerr_isocor", "flux_aper",
+                 "fluxerr_aper", "mag_aper", "magerr_aper", "flux_auto", "fluxerr_auto", "mag_auto", "magerr_auto",
+                 "theta", "poserr_mx2", "poserr_my2", "poserr_mxy", "elong", "ellip", "peak", "bkg", "fwhm"]:
+        assert np.array_equal(rows[name], g[name].astype(rows[name].dtype)), name
+    assert np.array_equal(rows["kronfactor"], g["kronfactor"])
+    assert np.array_equal(rows["flag"].astype(np.int32), g["flags"])
+    assert not rows["alpha2000"].any() and not rows["sprob"].any()

@@ -89,6 +89,29 @@ def test_shapes(gpu_ctx, w, h):
     run_both(gpu_ctx, img)
 
 
+def _blob(img, xc, yc, sigma, flux):
+    h, w = img.shape
+    y, x = np.mgrid[0:h, 0:w]
+    img += (flux / (2 * np.pi * sigma ** 2) * np.exp(-((x - xc) ** 2 + (y - yc) ** 2) / (2 * sigma ** 2))).astype(np.float32)
+
+
+def test_object_size_tiers_and_flux_range(gpu_ctx):
+    """Raw objects of every size class (a few pixels, hundreds, ~2000,
+    >4096) and point sources so bright (peak 2^29 and 2^32 x the detection
+    threshold) that their branch fluxes come close to, or need more than,
+    64 bits of fixed-scale sum."""
+    img = synth.frame_c0(seed=91, w=700, h=600, nsrc=500)
+    _blob(img, 150.0, 150.0, 25.0, 4e8)       # 34,000 pixels above threshold
+    _blob(img, 160.0, 175.0, 4.0, 2e6)        # a knot inside it: deblended
+    _blob(img, 450.0, 150.0, 7.0, 3e6)        # ~2000 pixels
+    _blob(img, 465.0, 160.0, 3.0, 1e6)
+    _blob(img, 300.0, 450.0, 0.7, 6e10)       # 178 pixels, peak 2^29 x threshold
+    _blob(img, 560.0, 470.0, 1.2, 8e11)       # 367 pixels, peak 2^32 x threshold
+    _blob(img, 566.0, 474.0, 1.2, 5e11)
+    g = run_both(gpu_ctx, img)
+    assert len(g) > 100
+
+
 def test_constant_frame_has_no_objects(gpu_ctx):
     img = np.full((200, 300), 1000.0, np.float32)
     g = run_both(gpu_ctx, img)
