@@ -246,6 +246,10 @@ def run_gpu(args):
                            "frac": round(frame_bytes / (peak * 1e9) / (ms_dev / 1e3), 4)},
         "clocks": clk,
     }
+    if rank == 0:
+        line["catalog_err_fp64"] = catalog_err(ctx, frame, cfg)
+    if world == 1 and not args.no_batch:
+        line["batch"] = run_batch(ctx, c3_frames())
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(frame, cfg)
     if rank == 0:
@@ -254,6 +258,78 @@ def run_gpu(args):
         dist.barrier()
         dist.destroy_process_group()
     ctx.close()
+
+
+def catalog_err(ctx, frame, cfg, tol=1e-5):
+    """Per-column error of the catalogue against a float64 recomputation
+    from the same segmentation (fp64check).  CLEAN is off for this one
+    extraction so that every row is the measurement of its own segmentation
+    pixels (a CLEAN merge adds fluxes but keeps the master's moments)."""
+    import fp64check
+    kw = dict(cfg)
+    kw["clean_flag"] = 0
+    cat, seg, s, sub, cd = ctx.extract(frame, max_objects=400000, want_maps=True, **kw)
+    rep = fp64check.catalog_error(cat, seg, sub, cd, s.thresh, s.dthresh, s.backsig, gain=kw.get("gain", 0.0))
+    worst = fp64check.worst(rep)
+    return {"settings": "workload frame with CLEAN off; float64 recomputation from the GPU's segmentation, "
+                        "subtracted and filtered frames; mag_iso and theta_deg are absolute errors",
+            "tolerance_rel": tol, "worst_rel": worst, "within": worst is not None and worst <= tol,
+            "columns": {k: {kk: (round(vv, 12) if isinstance(vv, float) else vv) for kk, vv in v.items()}
+                        for k, v in rep.items()}}
+
+
+def _c3_base(job):
+    seed, dens = job
+    sys.path.insert(0, os.path.join(ROOT, "gpu-sextractor_b200"))
+    import synth
+    return synth.frame_c1(seed=seed, density=dens)
+
+
+def c3_frames():
+    """The 64-frame mixed batch (c3 shapes, per-frame BACK_SIZE and mask),
+    cut from four seeded 4096^2 base fields generated in parallel."""
+    import multiprocessing as mp
+    import synth
+    dens = synth.c3_base_densities(4)
+    with mp.get_context("spawn").Pool(4) as pool:
+        bases = pool.map(_c3_base, [(3100 + i, d) for i, d in enumerate(dens)])
+    return [(f, dict(back_size=bs, conv=load_mask(m))) for f, bs, m in synth.batch_c3_from_bases(bases)]
+
+
+def run_batch(ctx, frames, reps=2, workers=4, maxobj=400000):
+    """Plain path (sexgpu_extract, one frame after the other) against the
+    batched form (sexgpu_extract_batch) on the same frames: host frames in,
+    host catalogues out, wall clock around the whole batch; catalogues
+    compared frame by frame."""
+    def plain():
+        return [ctx.extract(f, max_objects=maxobj, segmap=False, **kw)[0] for f, kw in frames]
+
+    def batched():
+        return [c for c, _ in ctx.extract_batch(frames, workers=workers, max_objects=maxobj)]
+
+    ref, got = plain(), batched()  # warm-up (first use allocates the workers' buffers)
+    identical = len(ref) == len(got) and all(a.tobytes() == b.tobytes() for a, b in zip(ref, got))
+    nobj = sum(len(c) for c in ref)
+    t_plain = t_batch = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        plain()
+        t_plain = min(t_plain, time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        batched()
+        t_batch = min(t_batch, time.perf_counter() - t0)
+    npx = sum(f.size for f, _ in frames)
+    return {"workload": "c3: 64 frames (16x 4096x2048, 24x 1024^2, 16x 512^2, 8x 4096^2) cut from four "
+                        "seeded 4096^2 fields of density 2e-4..1e-2 px^-2; BACK_SIZE 32/64/128 and "
+                        "gauss_2.0_3x3/gauss_3.0_7x7/mexhat_2.5_7x7 per frame",
+            "frames": len(frames), "pixels": int(npx), "objects": int(nobj), "workers": workers,
+            "timing": "host wall clock around the whole batch, host frames in and host catalogues out "
+                      "in both forms, best of %d" % reps,
+            "plain": {"frames_per_s": round(len(frames) / t_plain, 2), "mobj_per_s": round(nobj / t_plain / 1e6, 4),
+                      "s": round(t_plain, 4)},
+            "batched": {"frames_per_s": round(len(frames) / t_batch, 2),
+                        "mobj_per_s": round(nobj / t_batch / 1e6, 4), "s": round(t_batch, 4)},
+            "objects_ratio": round(t_plain / t_batch, 3), "identical_catalogues": bool(identical)}
 
 
 def algorithmic_bytes(stage, N, s):
@@ -335,6 +411,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sexgpu")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

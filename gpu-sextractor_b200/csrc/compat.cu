@@ -194,18 +194,20 @@ void run_detection(float dthresh, float thresh, int minarea, size_t *numValidObj
     FrameParams &Pm = ctx->ps.Pm;
     Pm.minarea = minarea;
     Pm.debminarea = minarea < SX_MAXDEBAREA ? minarea : SX_MAXDEBAREA;
-    static const float one = 1.0f;
     if (s.mask_w > 0) {
         Pm.filter_flag = 1;
         Pm.conv_w = Pm.conv_h = s.mask_w;
-        set_conv_mask(s.mask.data(), s.mask_w, s.mask_w, ctx->stream);
     } else {
         Pm.filter_flag = 0;
         Pm.conv_w = Pm.conv_h = 1;
-        set_conv_mask(&one, 1, 1, ctx->stream);
+    }
+    int rc = load_mask(ctx, s.mask_w > 0 ? s.mask.data() : nullptr, s.mask_w, s.mask_w);
+    if (rc) {
+        compat_fail("run_detection", rc);
+        return;
     }
     k_compat_thresholds<<<1, 1, 0, ctx->stream>>>(P<FrameScalars>(ctx->sc), dthresh, thresh);
-    int rc = pipe_detect(ctx);
+    rc = pipe_detect(ctx);
     if (rc) {
         compat_fail("run_detection", rc);
         return;

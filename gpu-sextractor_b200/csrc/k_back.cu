@@ -15,25 +15,22 @@
 
 namespace sx {
 
-// src/back.c:214-279 for one mesh per thread
-__global__ void k_mesh_stat(const float *__restrict__ img, int w, int h, int bw, int bh, int nbx, int nby,
-                            MeshStat *__restrict__ ms) {
-    int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= nbx * nby) return;
-    int mx = m % nbx, my = m / nbx;
-    int x0 = mx * bw, y0 = my * bh;
-    int mw = (mx == nbx - 1 && w % bw) ? w % bw : bw;
-    int mh = (my == nby - 1 && h % bh) ? h % bh : bh;
+// src/back.c:214-279 for one mesh: the reference's two sequential double
+// passes, in its pixel order.  `row0` points at the mesh's first pixel, rows
+// `stride` floats apart.
+__device__ __forceinline__ void mesh_stat_seq(const float *row0, int stride, int mw, int mh, MeshStat &o) {
     double pix, sig, mean = 0.0, sigma = 0.0;
-    double step = sqrt(2 / SX_PI) * SX_QUANTIF_NSIGMA / SX_QUANTIF_AMIN;
+    const double step = sqrt(2 / SX_PI) * SX_QUANTIF_NSIGMA / SX_QUANTIF_AMIN;
     int npix = 0;
-    MeshStat o;
     o.mean = o.sigma = o.lcut = o.hcut = o.qzero = o.qscale = 0.f;
     o.nlevels = o.npix = 0;
     for (int y = 0; y < mh; y++) {
-        const float *row = img + (size_t)(y0 + y) * w + x0;
+        const float *row = row0 + (size_t)y * stride;
+        // unrolled so that loads and conversions run ahead of the two
+        // accumulation chains; the additions stay in pixel order
+#pragma unroll 8
         for (int x = 0; x < mw; x++)
-            if ((pix = __ldg(row + x)) > -SX_BIG) {
+            if ((pix = row[x]) > -SX_BIG) {
                 mean += pix;
                 sigma += pix * pix;
                 npix++;
@@ -41,19 +38,19 @@ __global__ void k_mesh_stat(const float *__restrict__ img, int w, int h, int bw,
     }
     if ((float)npix < (float)(mw * mh * SX_BACK_MINGOODFRAC)) {
         o.mean = o.sigma = -SX_BIG;
-        ms[m] = o;
         return;
     }
     mean /= (double)npix;
     sigma = (sig = sigma / npix - mean * mean) > 0.0 ? sqrt(sig) : 0.0;
-    float lcut = o.lcut = (float)(mean - 2.0 * sigma);
-    float hcut = o.hcut = (float)(mean + 2.0 * sigma);
+    const float lcut = o.lcut = (float)(mean - 2.0 * sigma);
+    const float hcut = o.hcut = (float)(mean + 2.0 * sigma);
     mean = sigma = 0.0;
     npix = 0;
     for (int y = 0; y < mh; y++) {
-        const float *row = img + (size_t)(y0 + y) * w + x0;
+        const float *row = row0 + (size_t)y * stride;
+#pragma unroll 8
         for (int x = 0; x < mw; x++) {
-            pix = __ldg(row + x);
+            pix = row[x];
             if (pix <= hcut && pix >= lcut) {
                 mean += pix;
                 sigma += pix * pix;
@@ -70,7 +67,135 @@ __global__ void k_mesh_stat(const float *__restrict__ img, int w, int h, int bw,
     if ((o.nlevels = (int)(step * npix + 1)) > SX_QUANTIF_NMAXLEVELS) o.nlevels = SX_QUANTIF_NMAXLEVELS;
     o.qscale = sigma > 0.0 ? 2 * SX_QUANTIF_NSIGMA * sigma / o.nlevels : 1.0;
     o.qzero = mean - SX_QUANTIF_NSIGMA * sigma;
+}
+
+__device__ __forceinline__ void mesh_geometry(int m, int w, int h, int bw, int bh, int nbx, int nby, int &x0, int &y0,
+                                              int &mw, int &mh) {
+    const int mx = m % nbx, my = m / nbx;
+    x0 = mx * bw;
+    y0 = my * bh;
+    mw = (mx == nbx - 1 && w % bw) ? w % bw : bw;
+    mh = (my == nby - 1 && h % bh) ? h % bh : bh;
+}
+
+// one thread per mesh, straight from the frame (meshes too large to stage)
+__global__ void k_mesh_stat(const float *__restrict__ img, int w, int h, int bw, int bh, int nbx, int nby,
+                            MeshStat *__restrict__ ms) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nbx * nby) return;
+    int x0, y0, mw, mh;
+    mesh_geometry(m, w, h, bw, bh, nbx, nby, x0, y0, mw, mh);
+    MeshStat o;
+    mesh_stat_seq(img + (size_t)y0 * w + x0, w, mw, mh, o);
     ms[m] = o;
+}
+
+// One warp per row band of 32 meshes, one lane per mesh.  The band's pixel
+// rows are staged in shared memory one at a time (double buffered with
+// cp.async, coalesced across the band); every lane then adds its mesh's part
+// of the row to its own sums, so each lane performs the reference's sequential
+// double sums in the reference's pixel order.  Mesh j of the band sits at
+// j * stride in the row buffer; an odd stride keeps the lanes' reads on
+// distinct banks.
+__device__ __forceinline__ void band_row_async(float *dst, const float *img, int w, int gy, int x0, int bw, int mw_last,
+                                               int nmesh, int stride) {
+    const int lane = threadIdx.x & 31;
+    const float *src = img + (size_t)gy * w + x0;
+    for (int j = 0; j < nmesh; j++) {
+        const int mw = j == nmesh - 1 ? mw_last : bw;
+        for (int x = lane; x < mw; x += 32) {
+            const unsigned d = (unsigned)__cvta_generic_to_shared(dst + j * stride + x);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src + (size_t)j * bw + x)
+                         : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(32) k_mesh_stat_band(const float *__restrict__ img, int w, int h, int bw, int bh,
+                                                       int nbx, int nby, int stride, MeshStat *__restrict__ ms) {
+    extern __shared__ float band_smem[];
+    const int lane = threadIdx.x;
+    const int mx0 = blockIdx.x * 32, my = blockIdx.y;
+    const int nmesh = min(32, nbx - mx0);
+    const int x0 = mx0 * bw, y0 = my * bh;
+    const int mh = (my == nby - 1 && h % bh) ? h % bh : bh;
+    const int mw_last = (mx0 + nmesh == nbx && w % bw) ? w % bw : bw;
+    const bool active = lane < nmesh;
+    const int mw = lane == nmesh - 1 ? mw_last : bw;
+    float *buf[2] = {band_smem, band_smem + 32 * stride};
+    double pix, sig, mean = 0.0, sigma = 0.0;
+    const double step = sqrt(2 / SX_PI) * SX_QUANTIF_NSIGMA / SX_QUANTIF_AMIN;
+    int npix = 0;
+    float lcut = 0.0f, hcut = 0.0f;
+    bool bad = false;
+    for (int pass = 0; pass < 2; pass++) {
+        band_row_async(buf[0], img, w, y0, x0, bw, mw_last, nmesh, stride);
+        for (int y = 0; y < mh; y++) {
+            if (y + 1 < mh)
+                band_row_async(buf[(y + 1) & 1], img, w, y0 + y + 1, x0, bw, mw_last, nmesh, stride);
+            else
+                asm volatile("cp.async.commit_group;" ::: "memory");
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+            __syncwarp();
+            if (active) {
+                const float *row = buf[y & 1] + lane * stride;
+                if (pass == 0) {
+#pragma unroll 8
+                    for (int x = 0; x < mw; x++)
+                        if ((pix = row[x]) > -SX_BIG) {
+                            mean += pix;
+                            sigma += pix * pix;
+                            npix++;
+                        }
+                } else {
+#pragma unroll 8
+                    for (int x = 0; x < mw; x++) {
+                        pix = row[x];
+                        if (pix <= hcut && pix >= lcut) {
+                            mean += pix;
+                            sigma += pix * pix;
+                            npix++;
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncwarp();
+        if (pass == 0) {
+            // src/back.c:249: too few valid pixels: a bad mesh
+            if ((float)npix < (float)(mw * mh * SX_BACK_MINGOODFRAC)) bad = true;
+            mean /= (double)npix;
+            sigma = (sig = sigma / npix - mean * mean) > 0.0 ? sqrt(sig) : 0.0;
+            lcut = (float)(mean - 2.0 * sigma);
+            hcut = (float)(mean + 2.0 * sigma);
+            mean = sigma = 0.0;
+            npix = 0;
+            if (__all_sync(0xffffffffu, bad || !active)) break;
+        }
+    }
+    if (!active) return;
+    MeshStat o;
+    o.mean = o.sigma = o.lcut = o.hcut = o.qzero = o.qscale = 0.f;
+    o.nlevels = o.npix = 0;
+    if (bad) {
+        o.mean = o.sigma = -SX_BIG;
+    } else {
+        o.lcut = lcut;
+        o.hcut = hcut;
+        o.npix = npix;
+        mean /= (double)npix;
+        sig = sigma / npix - mean * mean;
+        sigma = sig > 0.0 ? sqrt(sig) : 0.0;
+        o.mean = mean;
+        o.sigma = sigma;
+        if ((o.nlevels = (int)(step * npix + 1)) > SX_QUANTIF_NMAXLEVELS) o.nlevels = SX_QUANTIF_NMAXLEVELS;
+        o.qscale = sigma > 0.0 ? 2 * SX_QUANTIF_NSIGMA * sigma / o.nlevels : 1.0;
+        o.qzero = mean - SX_QUANTIF_NSIGMA * sigma;
+    }
+    ms[my * nbx + mx0 + lane] = o;
 }
 
 constexpr int GUESS_THREADS = 256;
@@ -439,7 +564,22 @@ __global__ void k_row_nodes(const float *__restrict__ back, const float *__restr
 void launch_background(BackBufs &B, const float *img, const FrameParams &P, FrameScalars *d_sc,
                        cudaStream_t st, int &launches) {
     int nb = P.nbx * P.nby;
-    k_mesh_stat<<<(nb + 127) / 128, 128, 0, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, B.ms);
+    // row-band kernel when two rows of 32 meshes fit in 96 KB of shared memory
+    const int stride = P.bw + ((P.bw & 1) ? 2 : 1);
+    const size_t band_bytes = 2 * 32 * (size_t)stride * sizeof(float);
+    if (band_bytes <= 96 * 1024) {
+        static bool attr_set[64];
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+            cudaFuncSetAttribute(k_mesh_stat_band, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+            attr_set[dev] = true;
+        }
+        dim3 grid((P.nbx + 31) / 32, P.nby);
+        k_mesh_stat_band<<<grid, 32, band_bytes, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, stride, B.ms);
+    } else {
+        k_mesh_stat<<<(nb + 127) / 128, 128, 0, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, B.ms);
+    }
     k_mesh_guess<<<nb, GUESS_THREADS, 0, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, B.ms, B.back, B.sigma);
     k_mesh_badfill<<<(nb + 127) / 128, 128, 0, st>>>(B.back, B.sigma, B.back2, P.nbx, P.nby);
     k_mesh_median<<<(nb + 127) / 128, 128, 0, st>>>(B.back2, B.sigma, B.back3, B.sigma3, P.nbx, P.nby, P.nfx / 2,

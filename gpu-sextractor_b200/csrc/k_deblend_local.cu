@@ -397,60 +397,72 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
     int *status = &A.sc->status;
 
     block_thresholds(A, fdpeak, thr);
-    for (int i = tid; i < DB_MAXLEV; i += NT) lvkept[i] = 0;
-    for (int k = tid; k < P; k += NT) {
-        own[k] = -1;
-        kl[k] = 0xff;
-    }
-    for (int k = tid; k < K; k += NT) bcnt[k] = bcur[k] = 0;
-    __syncthreads();
-    dl_levels<NT>(A, P, pix, thr, lev, order, lvcnt, lvstart, lvcur, false);
-    // kept list in (level, element) order
-    for (int i = tid; i < K; i += NT) {
-        const unsigned long long key = kept[i];
-        int rank = 0;
-        for (int j = 0; j < K; j++) rank += kept[j] < key;
-        kept2[rank] = key;
-    }
-    __syncthreads();
-    for (int i = tid; i < K; i += NT) {
-        const unsigned long long key = kept2[i];
-        const int L = (int)(key >> 32), c = (int)(key & 0xffffffffu);
-        kl[c] = (unsigned char)L;
-        kidx[c] = (unsigned short)i;
-        atomicAdd(&lvkept[L], 1);
-    }
-    __syncthreads();
-    // replay of the sweep; at levels with kept branches label their pixels
-    for (int L = A.N - 1; L >= 0; L--) {
-        const int b0 = lvstart[L], b1 = b0 + lvcnt[L];
-        if (lvcnt[L]) dl_activate_union<NT>(A, off, P, L, b0, b1, order, par, lev, status);
-        if (lvkept[L]) {
-            for (int i = tid; i < b1; i += NT) {
-                const int e = order[i];
-                const int rt = sfind_c(par, e, P, status);
-                if (kl[rt] == L) own[e] = (short)kidx[rt];
+    // one kept branch that is the whole object at level 0 (nothing split
+    // off): every pixel is its own, in list order; no replay is needed
+    const bool whole = K == 1 && (kept[0] >> 32) == 0;
+    if (whole) {
+        if (tid == 0) {
+            kept2[0] = kept[0];
+            bcnt[0] = P;
+            bstart[0] = 0;
+        }
+        __syncthreads();
+    } else {
+        for (int i = tid; i < DB_MAXLEV; i += NT) lvkept[i] = 0;
+        for (int k = tid; k < P; k += NT) {
+            own[k] = -1;
+            kl[k] = 0xff;
+        }
+        for (int k = tid; k < K; k += NT) bcnt[k] = bcur[k] = 0;
+        __syncthreads();
+        dl_levels<NT>(A, P, pix, thr, lev, order, lvcnt, lvstart, lvcur, false);
+        // kept list in (level, element) order
+        for (int i = tid; i < K; i += NT) {
+            const unsigned long long key = kept[i];
+            int rank = 0;
+            for (int j = 0; j < K; j++) rank += kept[j] < key;
+            kept2[rank] = key;
+        }
+        __syncthreads();
+        for (int i = tid; i < K; i += NT) {
+            const unsigned long long key = kept2[i];
+            const int L = (int)(key >> 32), c = (int)(key & 0xffffffffu);
+            kl[c] = (unsigned char)L;
+            kidx[c] = (unsigned short)i;
+            atomicAdd(&lvkept[L], 1);
+        }
+        __syncthreads();
+        // replay of the sweep; at levels with kept branches label their pixels
+        for (int L = A.N - 1; L >= 0; L--) {
+            const int b0 = lvstart[L], b1 = b0 + lvcnt[L];
+            if (lvcnt[L]) dl_activate_union<NT>(A, off, P, L, b0, b1, order, par, lev, status);
+            if (lvkept[L]) {
+                for (int i = tid; i < b1; i += NT) {
+                    const int e = order[i];
+                    const int rt = sfind_c(par, e, P, status);
+                    if (kl[rt] == L) own[e] = (short)kidx[rt];
+                }
+                __syncthreads();
             }
-            __syncthreads();
         }
-    }
-    // owned pixels grouped by branch (counting sort)
-    for (int e = tid; e < P; e += NT)
-        if (own[e] >= 0) atomicAdd(&bcnt[own[e]], 1);
-    __syncthreads();
-    if (tid == 0) {
-        int s = 0;
-        for (int k = 0; k < K; k++) {
-            bstart[k] = s;
-            s += bcnt[k];
+        // owned pixels grouped by branch (counting sort)
+        for (int e = tid; e < P; e += NT)
+            if (own[e] >= 0) atomicAdd(&bcnt[own[e]], 1);
+        __syncthreads();
+        if (tid == 0) {
+            int s = 0;
+            for (int k = 0; k < K; k++) {
+                bstart[k] = s;
+                s += bcnt[k];
+            }
         }
+        __syncthreads();
+        for (int e = tid; e < P; e += NT) {
+            const int k = own[e];
+            if (k >= 0) blist[bstart[k] + atomicAdd(&bcur[k], 1)] = (unsigned short)e;
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    for (int e = tid; e < P; e += NT) {
-        const int k = own[e];
-        if (k >= 0) blist[bstart[k] + atomicAdd(&bcur[k], 1)] = (unsigned short)e;
-    }
-    __syncthreads();
     // preanalysis of each kept branch over its own pixels, one warp per branch
     for (int k = tid >> 5; k < K; k += NT / 32) {
         const int o = ob + k, L = (int)(kept2[k] >> 32), nb = bcnt[k], bb = bstart[k];
@@ -459,7 +471,7 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
         XSum srv;
         xs_init(srv);
         for (int i = lane; i < nb; i += 32) {
-            const unsigned p = pix[blist[bb + i]];
+            const unsigned p = pix[whole ? i : blist[bb + i]];
             const int y = (int)fdiv(p, A.wdiv), x = (int)p - y * A.w;
             xmin = min(xmin, x);
             xmax = max(xmax, x);
@@ -490,7 +502,7 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
         xs_init(stv);
         int dnpix = 0, area2 = 0;
         for (int i = lane; i < nb; i += 32) {
-            const unsigned p = pix[blist[bb + i]];
+            const unsigned p = pix[whole ? i : blist[bb + i]];
             const int yy = (int)fdiv(p, A.wdiv), x = (int)p - yy * A.w - xmin, y = yy - ymin;
             const float cval = A.cd[p], val = A.sub[p];
             dnpix += val > dthresh;
@@ -580,7 +592,7 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
     // gatherup (cudadeblend.cu:1262-1360): the nearest kept branch in the
     // elliptical metric, first in order on ties
     for (int e = tid; e < P; e += NT) {
-        int k = own[e];
+        int k = whole ? 0 : own[e];
         const unsigned p = pix[e];
         if (k < 0) {
             const int y = (int)fdiv(p, A.wdiv), x = (int)p - y * A.w;

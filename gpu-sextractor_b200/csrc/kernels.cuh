@@ -58,10 +58,18 @@ struct ObjBufs {
 void launch_background(BackBufs &B, const float *img, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st,
                        int &launches);
 
+// The detection mask of one extraction: row-major mw x mh values on the
+// device and on the host (per context, so that contexts extracting at the
+// same time with different masks do not share it).
+struct ConvMask {
+    const float *dev;
+    const float *host;
+    int mw, mh;
+};
+
 void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const BackBufs &B,
-                       const FrameParams &P, FrameScalars *d_sc, const float *d_var, cudaStream_t st,
-                       int &launches);
-void set_conv_mask(const float *mask, int mw, int mh, cudaStream_t st);
+                       const FrameParams &P, FrameScalars *d_sc, const float *d_var, const ConvMask &M,
+                       cudaStream_t st, int &launches);
 
 void launch_ccl(int *lab, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st, int &launches);
 

@@ -10,7 +10,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <cmath>
+#include <algorithm>
+#include <atomic>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "sexgpu.h"
@@ -91,6 +94,10 @@ struct sexgpu_ctx {
     std::vector<float> stage_ms;
     std::vector<std::string> stage_names;
     std::vector<int> stage_launches;
+    std::vector<sexgpu_ctx *> workers;  // contexts of sexgpu_extract_batch
+    DevBuf dmask;                       // detection mask of the current extraction
+    std::vector<float> hmask;
+    ConvMask cmask{nullptr, nullptr, 1, 1};
 };
 
 namespace {
@@ -261,6 +268,23 @@ int read_scalars(sexgpu_ctx *ctx) {
     return SEXGPU_OK;
 }
 
+// the detection mask of this context's next extraction (host and device copy)
+int load_mask(sexgpu_ctx *ctx, const float *mask, int mw, int mh) {
+    static const float one = 1.0f;
+    if (!mask) {
+        mask = &one;
+        mw = mh = 1;
+    }
+    ctx->hmask.assign(mask, mask + (size_t)mw * mh);
+    EN(dmask, sizeof(float) * SX_MAXCONV * SX_MAXCONV);
+    CK(cudaMemcpyAsync(ctx->dmask.p, ctx->hmask.data(), sizeof(float) * mw * mh, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->cmask.dev = P<float>(ctx->dmask);
+    ctx->cmask.host = ctx->hmask.data();
+    ctx->cmask.mw = mw;
+    ctx->cmask.mh = mh;
+    return SEXGPU_OK;
+}
+
 int alloc_objects(sexgpu_ctx *ctx, int nobj) {
     size_t n = (size_t)nobj + 1;
     int *ip[20];
@@ -419,11 +443,8 @@ int pipe_begin(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu_c
     column_table(w, Pm.nbx, Pm.bw, ctx->colk_h, ctx->coldx_h);
     CK(cudaMemcpyAsync(B.colk, ctx->colk_h.data(), w * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(B.coldx, ctx->coldx_h.data(), w * 4, cudaMemcpyHostToDevice, st));
-    static const float one = 1.0f;
-    if (cfg->filter_flag)
-        set_conv_mask(cfg->conv, cfg->conv_w, cfg->conv_h, st);
-    else
-        set_conv_mask(&one, 1, 1, st);
+    rc = load_mask(ctx, cfg->filter_flag ? cfg->conv : nullptr, cfg->conv_w, cfg->conv_h);
+    if (rc) return rc;
 
     stage_begin(ctx);
     int nl = 0;
@@ -446,7 +467,8 @@ int pipe_detect(sexgpu_ctx *ctx) {
     FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
     int *tmp = P<int>(ctx->scan_tmp);
     int rc = SEXGPU_OK, nl = 0;
-    launch_sub_filter(d_img, P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm, d_sc, nullptr, st, nl);
+    launch_sub_filter(d_img, P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm, d_sc, nullptr,
+                      ctx->cmask, st, nl);
     stage_mark(ctx, "sub_filter", nl);
 
     nl = 0;
@@ -872,6 +894,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
         if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
     }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    for (sexgpu_ctx *w : ctx->workers) sexgpu_destroy(w);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SEXGPU_OK;
@@ -1021,14 +1044,14 @@ int sexgpu_background(sexgpu_ctx *ctx, float *img, int w, int h, const sexgpu_co
     CK(cudaMemcpyAsync(B.colk, ctx->colk_h.data(), w * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(B.coldx, ctx->coldx_h.data(), w * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->img.p, img, N * 4, cudaMemcpyHostToDevice, st));
-    static const float one = 1.0f;
-    set_conv_mask(&one, 1, 1, st);
+    rc = load_mask(ctx, nullptr, 1, 1);
+    if (rc) return rc;
     FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
     int nl = 0;
     k_init_scalars<<<1, 1, 0, st>>>(d_sc);
     launch_background(B, P<float>(ctx->img), Pm, d_sc, st, nl);
     launch_sub_filter(P<float>(ctx->img), P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm, d_sc,
-                      nullptr, st, nl);
+                      nullptr, ctx->cmask, st, nl);
     CK(cudaMemcpyAsync(img, ctx->sub.p, N * 4, cudaMemcpyDeviceToHost, st));
     if (back) CK(cudaMemcpyAsync(back, B.back3, nb * 4, cudaMemcpyDeviceToHost, st));
     if (sigma) CK(cudaMemcpyAsync(sigma, B.sigma3, nb * 4, cudaMemcpyDeviceToHost, st));
@@ -1056,7 +1079,8 @@ int sexgpu_filter(sexgpu_ctx *ctx, const float *sub, int w, int h, const float *
     EN(colk, 16);
     EN(coldx, 16);
     CK(cudaMemcpyAsync(ctx->img.p, sub, N * 4, cudaMemcpyHostToDevice, st));
-    set_conv_mask(mask, mw, mh, st);
+    int rc = load_mask(ctx, mask, mw, mh);
+    if (rc) return rc;
     FrameScalars z;
     memset(&z, 0, sizeof(z));
     z.backmean = 0.0f;
@@ -1079,7 +1103,7 @@ int sexgpu_filter(sexgpu_ctx *ctx, const float *sub, int w, int h, const float *
     Pm.conv_h = mh;
     int nl = 0;
     launch_sub_filter(P<float>(ctx->img), P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm,
-                      P<FrameScalars>(ctx->sc), nullptr, st, nl);
+                      P<FrameScalars>(ctx->sc), nullptr, ctx->cmask, st, nl);
     CK(cudaMemcpyAsync(cd, ctx->cd.p, N * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
@@ -1131,6 +1155,49 @@ int sexgpu_getconv(const char *path, float *mask, int maxn, int *mw, int *mh) {
         for (int j = 0; j < n; j++) mask[j] /= sum;
     }
     return n;
+}
+
+int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframes, int workers) {
+    if (!ctx || nframes < 0 || (nframes > 0 && !frames) || workers < 0) return SEXGPU_ERR_ARG;
+    if (nframes == 0) return SEXGPU_OK;
+    if (workers == 0) workers = 4;
+    workers = std::min(workers, nframes);
+    while ((int)ctx->workers.size() < workers) {
+        sexgpu_ctx *w = nullptr;
+        int rc = sexgpu_create(&w, ctx->device);
+        if (rc) {
+            ctx->err = "cannot create a batch worker context";
+            return rc;
+        }
+        ctx->workers.push_back(w);
+    }
+    // largest frames first, so that the last frames to start are short
+    std::vector<int> order(nframes);
+    for (int i = 0; i < nframes; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (long long)frames[a].w * frames[a].h > (long long)frames[b].w * frames[b].h;
+    });
+    std::atomic<int> next(0);
+    auto run = [&](sexgpu_ctx *wc) {
+        cudaSetDevice(wc->device);
+        for (int k; (k = next.fetch_add(1)) < nframes;) {
+            sexgpu_batch_frame &f = frames[order[k]];
+            f.nobj = 0;
+            f.status = f.img && f.cfg ? sexgpu_extract(wc, f.img, nullptr, f.w, f.h, f.cfg, f.objs, f.max_objects,
+                                                       &f.nobj, nullptr, nullptr, nullptr, &f.summary)
+                                      : SEXGPU_ERR_ARG;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int i = 1; i < workers; i++) pool.emplace_back(run, ctx->workers[i]);
+    run(ctx->workers[0]);
+    for (auto &t : pool) t.join();
+    for (int i = 0; i < nframes; i++)
+        if (frames[i].status != SEXGPU_OK) {
+            ctx->err = "frame " + std::to_string(i) + " failed";
+            return frames[i].status;
+        }
+    return SEXGPU_OK;
 }
 
 int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max) {

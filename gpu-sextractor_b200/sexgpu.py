@@ -72,6 +72,13 @@ class Summary(C.Structure):
     ]
 
 
+class BatchFrame(C.Structure):
+    """sexgpu_batch_frame."""
+    _fields_ = [("img", C.POINTER(C.c_float)), ("w", C.c_int32), ("h", C.c_int32),
+                ("cfg", C.POINTER(Config)), ("objs", C.c_void_p), ("max_objects", C.c_int32),
+                ("nobj", C.c_int32), ("status", C.c_int32), ("pad", C.c_int32), ("summary", Summary)]
+
+
 class Stage(C.Structure):
     _fields_ = [("name", C.c_char * 24), ("launches", C.c_int32), ("ms", C.c_float)]
 
@@ -79,7 +86,7 @@ class Stage(C.Structure):
 EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extract",
            "sexgpu_extract_device", "sexgpu_copy_results", "sexgpu_background", "sexgpu_filter",
            "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times",
-           "sexgpu_background_noalloc"]
+           "sexgpu_background_noalloc", "sexgpu_extract_batch"]
 
 _lib = None
 
@@ -191,7 +198,7 @@ class Context:
                self.h, "sexgpu_filter")
         return cd
 
-    def extract(self, img, max_objects=None, want_maps=False, **kw):
+    def extract(self, img, max_objects=None, want_maps=False, segmap=True, **kw):
         """Host frame in, catalogue (+ segmentation map) out."""
         cfg = make_config(**kw)
         img = np.ascontiguousarray(img, np.float32)
@@ -199,14 +206,15 @@ class Context:
         if max_objects is None:
             max_objects = w * h // max(1, cfg.detect_minarea) // 2 + 16
         objs = np.zeros(max_objects, OBJECT_DTYPE)
-        seg = np.zeros((h, w), np.int32)
+        seg = np.zeros((h, w), np.int32) if segmap else None
         n = C.c_int()
         s = Summary()
         sub = np.zeros_like(img) if want_maps else None
         cd = np.zeros_like(img) if want_maps else None
         rc = lib().sexgpu_extract(self.h, _f(img), None, w, h, C.byref(cfg),
                                   objs.ctypes.data_as(C.c_void_p), max_objects, C.byref(n),
-                                  seg.ctypes.data_as(C.c_void_p), _f(sub) if want_maps else None,
+                                  seg.ctypes.data_as(C.c_void_p) if segmap else None,
+                                  _f(sub) if want_maps else None,
                                   _f(cd) if want_maps else None, C.byref(s))
         _check(rc, self.h, "sexgpu_extract")
         if want_maps:
@@ -229,6 +237,25 @@ class Context:
                                        seg.ctypes.data_as(C.c_void_p) if segmap else None, None, None)
         _check(rc, self.h, "sexgpu_copy_results")
         return (objs[:n.value], seg) if segmap else objs[:n.value]
+
+    def extract_batch(self, frames, workers=0, max_objects=None):
+        """frames: list of (img, settings dict).  All frames go to the library
+        in one sexgpu_extract_batch call; returns [(catalogue, summary)]."""
+        n = len(frames)
+        arr = (BatchFrame * max(n, 1))()
+        keep = []
+        for i, (img, kw) in enumerate(frames):
+            img = np.ascontiguousarray(img, np.float32)
+            cfg = make_config(**kw)
+            h, w = img.shape
+            cap = max_objects or (w * h // max(1, cfg.detect_minarea) // 2 + 16)
+            objs = np.zeros(cap, OBJECT_DTYPE)
+            keep.append((img, cfg, objs))
+            f = arr[i]
+            f.img, f.w, f.h, f.cfg = _f(img), w, h, C.pointer(cfg)
+            f.objs, f.max_objects = objs.ctypes.data_as(C.c_void_p), cap
+        _check(lib().sexgpu_extract_batch(self.h, arr, n, workers), self.h, "sexgpu_extract_batch")
+        return [(keep[i][2][:arr[i].nobj], arr[i].summary) for i in range(n)]
 
     def stage_times(self):
         st = (Stage * 32)()

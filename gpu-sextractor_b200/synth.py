@@ -230,3 +230,31 @@ def batch_c3(seed=3000, scale=1):
         f = frame_c1(seed=seed + 1 + i, w=ww, h=hh, density=dens)
         out.append((f, bs, masks[i % 3]))
     return out
+
+
+C3_SHAPES = [(4096, 2048)] * 16 + [(1024, 1024)] * 24 + [(512, 512)] * 16 + [(4096, 4096)] * 8
+C3_MASKS = ["gauss_2.0_3x3", "gauss_3.0_7x7", "mexhat_2.5_7x7"]
+
+
+def c3_base_densities(nbase=4, lo=2e-4, hi=1e-2):
+    """Source densities of the 4096^2 base fields the c3 frames are cut from,
+    spread over the workload's range."""
+    return [float(v) for v in np.linspace(lo, hi, nbase)]
+
+
+def batch_c3_from_bases(bases, seed=3000):
+    """Workload c3 from a few 4096^2 base fields (frame_c1 at the densities of
+    c3_base_densities): the 64 frames of batch_c3's shapes, each cut from a
+    base field at a seeded offset, with batch_c3's per-frame BACK_SIZE and
+    mask.  Returns a list of (frame, back_size, mask_name); the frames are
+    contiguous copies."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i, (hh, ww) in enumerate(C3_SHAPES):
+        base = bases[int(rng.integers(len(bases)))]
+        H, W = base.shape
+        y = int(rng.integers(0, H - hh + 1))
+        x = int(rng.integers(0, W - ww + 1))
+        bs = int(rng.choice([32, 64, 128]))
+        out.append((np.ascontiguousarray(base[y:y + hh, x:x + ww]), bs, C3_MASKS[i % 3]))
+    return out

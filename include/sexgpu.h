@@ -181,6 +181,30 @@ void sexgpu_default_config(sexgpu_config *cfg);
 int sexgpu_background_noalloc(const float *d_img, float *d_sub, int w, int h, const sexgpu_config *cfg,
                               float *d_back, float *d_sigma, sexgpu_summary *sum, void *stream);
 
+/* One frame of a batch: inputs, the caller's catalogue buffer, and outputs. */
+typedef struct {
+    const float *img;            /* host frame, w*h float32, row-major */
+    int32_t w, h;
+    const sexgpu_config *cfg;    /* this frame's settings */
+    sexgpu_object *objs;         /* host catalogue buffer (may be NULL) */
+    int32_t max_objects;
+    int32_t nobj;                /* out: catalogue length */
+    int32_t status;              /* out: SEXGPU_OK or this frame's error */
+    int32_t pad;
+    sexgpu_summary summary;      /* out */
+} sexgpu_batch_frame;
+
+/* Extraction of many frames of any sizes and settings (the batched form of
+ * scanimage(); no counterpart in the reference, which handles one frame per
+ * process).  The frames are taken largest first by `workers` device streams
+ * of this context's device (0: 4), each with its own buffers, so that the
+ * stages of different frames overlap on the GPU.  Every frame's results are
+ * exactly those of sexgpu_extract on that frame.  Returns SEXGPU_OK if every
+ * frame succeeded, else the status of the first failed frame (each frame's
+ * own status is in frames[i].status).  Not for use on the same context from
+ * two threads at once. */
+int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframes, int workers);
+
 /* Last CUDA error string of this context (empty if none). */
 const char *sexgpu_last_error(sexgpu_ctx *ctx);
 

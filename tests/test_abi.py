@@ -98,3 +98,24 @@ int main(void) {
         subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe])
         vals = [int(v) for v in subprocess.check_output([exe]).split()]
     assert vals == [160, 8, 24, 56, 68, 88, 96, 112, 120, 124, 132, 148]
+
+
+def test_batch_frame_layout():
+    prog = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "sexgpu.h"
+int main(void) {
+  printf("%zu %zu %zu %zu\n", sizeof(sexgpu_batch_frame), offsetof(sexgpu_batch_frame, objs),
+         offsetof(sexgpu_batch_frame, status), offsetof(sexgpu_batch_frame, summary));
+  return 0;
+}'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(prog)
+        exe = os.path.join(d, "t")
+        subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe])
+        vals = [int(v) for v in subprocess.check_output([exe]).split()]
+    import ctypes as C
+    B = sexgpu.BatchFrame
+    assert vals == [C.sizeof(B), B.objs.offset, B.status.offset, B.summary.offset]

@@ -1,0 +1,32 @@
+"""sexgpu_extract_batch: frames of different sizes and settings extracted
+concurrently give, frame by frame, exactly the catalogue of sexgpu_extract."""
+import numpy as np
+import pytest
+
+import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def test_batch_equals_plain(gpu_ctx, masks):
+    frames = [
+        (synth.frame_c1(seed=41, w=1024, h=512, density=6e-3), dict(back_size=32, conv=masks["gauss_2.0_3x3"])),
+        (synth.frame_c0(seed=42, w=700, h=500, nsrc=600), dict(back_size=64, conv=masks["gauss_3.0_7x7"])),
+        (synth.frame_c1(seed=43, w=512, h=512, density=2e-3), dict(back_size=128, conv=masks["mexhat_2.5_7x7"])),
+        (synth.frame_c1(seed=44, w=256, h=384, density=1e-2), dict(back_size=64, conv=masks["gauss_2.0_3x3"])),
+        (synth.frame_c0(seed=45, w=64, h=64, nsrc=4), dict()),
+        (synth.frame_c1(seed=46, w=900, h=333, density=4e-3), dict(back_size=32, conv=masks["gauss_3.0_7x7"],
+                                                                     clean_flag=0)),
+    ]
+    got = gpu_ctx.extract_batch(frames, workers=3)
+    assert len(got) == len(frames)
+    for (img, kw), (cat, summ) in zip(frames, got):
+        ref, _, s = gpu_ctx.extract(img, **kw)
+        assert cat.tobytes() == ref.tobytes()
+        assert (summ.nobj, summ.nraw, summ.backsig) == (s.nobj, s.nraw, s.backsig)
+
+
+def test_batch_reports_bad_frame(gpu_ctx):
+    img = synth.frame_c0(seed=47, w=300, h=200, nsrc=50)
+    with pytest.raises(RuntimeError):
+        gpu_ctx.extract_batch([(img, dict()), (img, dict(deblend_nthresh=0))], workers=2)
