@@ -221,6 +221,10 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
 #define RL(s) (rl0 + (s) * cap)
 #define NDR(s) (ndr0 + (s) * cap)
     unsigned long long *kept = A.D.kept + off;
+    // merge record of every element: (activation level << 24) |
+    // (level at which it stopped being a root, 0xff if never << 16) | the root
+    // that absorbed it; the assignment walks these instead of replaying
+    int *rec = A.D.rec + off;
     const int e0 = A.sc->e0cd;
     int *status = &A.sc->status;
 
@@ -287,6 +291,7 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
             const int e = order[i];
             sz[e] = 1;
             acc[e] = dl_term(A.cd[pix[e]], e0);
+            rec[e] = (L << 24) | 0x00ffffff;  // active from level L, not absorbed yet
         }
         if (lastL > cl)
             for (int i = tid; i < nprev; i += NT) {
@@ -303,6 +308,7 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
                 const int rt = sfind_c(par, c, P, status);
                 atomicAdd(&sz[rt], sz[c]);
                 atomicAdd(&acc[rt], acc[c]);
+                rec[c] = (lev[c] << 24) | (L << 16) | rt;  // absorbed at level L by rt
             } else {
                 RL(cur)[atomicAdd(&s_nrl[cur], 1)] = (unsigned short)c;
             }
@@ -372,7 +378,6 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
 template <int NT>
 __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, unsigned char *base, int cap) {
     __shared__ float thr[DB_MAXLEV];
-    __shared__ int lvcnt[DB_MAXLEV + 1], lvstart[DB_MAXLEV + 1], lvcur[DB_MAXLEV], lvkept[DB_MAXLEV];
     const int tid = threadIdx.x, lane = tid & 31;
     const int off = A.R.off[r], P = A.R.size[r];
     const float fdpeak = A.R.fdpeak[r];
@@ -381,24 +386,22 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
     const int K = A.R.nkept[r], ob = A.R.objbase[r];
     const unsigned *pix = A.rpix + off;
     const unsigned long long *kept = A.D.kept + off;
+    const int *rec = A.D.rec + off;
     if (!base) {
         base = A.D.arena + (size_t)off * DL_ARENA_BYTES;
         cap = P;
     }
     unsigned long long *kept2 = reinterpret_cast<unsigned long long *>(base);
-    int *par = reinterpret_cast<int *>(kept2 + cap);
-    int *bcnt = par + cap, *bstart = bcnt + cap, *bcur = bstart + cap;
-    unsigned short *order = reinterpret_cast<unsigned short *>(bcur + cap);
-    unsigned short *blist = order + cap;
+    int *bcnt = reinterpret_cast<int *>(kept2 + cap), *bstart = bcnt + cap, *bcur = bstart + cap;
+    unsigned short *blist = reinterpret_cast<unsigned short *>(bcur + cap);
     short *own = reinterpret_cast<short *>(blist + cap);
     unsigned short *kidx = reinterpret_cast<unsigned short *>(own + cap);
-    unsigned char *lev = reinterpret_cast<unsigned char *>(kidx + cap);
-    unsigned char *kl = lev + cap;
+    unsigned char *kl = reinterpret_cast<unsigned char *>(kidx + cap);
     int *status = &A.sc->status;
 
     block_thresholds(A, fdpeak, thr);
     // one kept branch that is the whole object at level 0 (nothing split
-    // off): every pixel is its own, in list order; no replay is needed
+    // off): every pixel is its own, in list order
     const bool whole = K == 1 && (kept[0] >> 32) == 0;
     if (whole) {
         if (tid == 0) {
@@ -408,14 +411,9 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
         }
         __syncthreads();
     } else {
-        for (int i = tid; i < DB_MAXLEV; i += NT) lvkept[i] = 0;
-        for (int k = tid; k < P; k += NT) {
-            own[k] = -1;
-            kl[k] = 0xff;
-        }
+        for (int k = tid; k < P; k += NT) kl[k] = 0xff;
         for (int k = tid; k < K; k += NT) bcnt[k] = bcur[k] = 0;
         __syncthreads();
-        dl_levels<NT>(A, P, pix, thr, lev, order, lvcnt, lvstart, lvcur, false);
         // kept list in (level, element) order
         for (int i = tid; i < K; i += NT) {
             const unsigned long long key = kept[i];
@@ -426,28 +424,33 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
         __syncthreads();
         for (int i = tid; i < K; i += NT) {
             const unsigned long long key = kept2[i];
-            const int L = (int)(key >> 32), c = (int)(key & 0xffffffffu);
-            kl[c] = (unsigned char)L;
-            kidx[c] = (unsigned short)i;
-            atomicAdd(&lvkept[L], 1);
+            kl[(int)(key & 0xffffffffu)] = (unsigned char)(key >> 32);
+            kidx[(int)(key & 0xffffffffu)] = (unsigned short)i;
         }
         __syncthreads();
-        // replay of the sweep; at levels with kept branches label their pixels
-        for (int L = A.N - 1; L >= 0; L--) {
-            const int b0 = lvstart[L], b1 = b0 + lvcnt[L];
-            if (lvcnt[L]) dl_activate_union<NT>(A, off, P, L, b0, b1, order, par, lev, status);
-            if (lvkept[L]) {
-                for (int i = tid; i < b1; i += NT) {
-                    const int e = order[i];
-                    const int rt = sfind_c(par, e, P, status);
-                    if (kl[rt] == L) own[e] = (short)kidx[rt];
+        // Owner of each pixel: its component at level L is the node of its
+        // merge chain e -> up(e) -> ... that covers L (node x covers the levels
+        // above the one at which it was absorbed, down from where the previous
+        // node was absorbed); a kept branch (L, c) owns the pixel when c covers
+        // L on the chain.  Absorption levels fall strictly along a chain.
+        for (int e = tid; e < P; e += NT) {
+            int x = e, hi = rec[e] >> 24, o = -1;
+            for (int step = 0; step <= DB_MAXLEV + 1; step++) {
+                const int rx = rec[x], m = (rx >> 16) & 0xff;
+                const int lo = m == 0xff ? -1 : m;
+                const int kx = kl[x];
+                if (kx != 0xff && kx > lo && kx <= hi) {
+                    o = kidx[x];
+                    break;
                 }
-                __syncthreads();
+                if (m == 0xff) break;
+                if (step == DB_MAXLEV + 1) atomicOr(status, SX_ST_LOOP);
+                hi = lo;
+                x = rx & 0xffff;
             }
+            own[e] = (short)o;
+            if (o >= 0) atomicAdd(&bcnt[o], 1);
         }
-        // owned pixels grouped by branch (counting sort)
-        for (int e = tid; e < P; e += NT)
-            if (own[e] >= 0) atomicAdd(&bcnt[own[e]], 1);
         __syncthreads();
         if (tid == 0) {
             int s = 0;

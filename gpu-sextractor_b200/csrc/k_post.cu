@@ -504,6 +504,7 @@ __global__ void k_write_rows(ObjBufs O, const unsigned *vals, int ns, float dthr
     if (k >= ns) return;
     int o = (int)vals[k];
     sexgpu_object q;
+    memset(&q, 0, sizeof(q));  // padding bytes too: rows are byte-for-byte reproducible
     q.number = k + 1;
     q.root = O.root[o];
     q.level = O.level[o];

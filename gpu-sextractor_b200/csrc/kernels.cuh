@@ -35,6 +35,7 @@ struct DebBufs {
     int *own, *kl, *kidx;
     int *pint;                          // xmin, xmax, ymin, ymax, peak(ord), cpeak(ord), dnpix, area2
     unsigned char *arena;               // 48 B per element: the compact per-object state of k_dl_*
+    int *rec;                           // merge record per element (k_dl_sweep -> k_dl_assign)
 };
 
 // per-object data (index = object id: root order, then (level, label))

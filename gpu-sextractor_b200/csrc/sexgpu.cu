@@ -79,7 +79,7 @@ struct sexgpu_ctx {
     DevBuf rsize, roff, rfirst, rymax, rlastx, rfdpeak, rfdflux, rnkept, robjbase, rlists, rcounts;
     // deblend scratch
     DevBuf dpar, dlev, dsz, dorder, drl0, drl1, dnid0, dnid1, dacc, nr0, nr1, nf0, nf1, ns0, ns1, nc0, nc1, na0, na1,
-        dkept, down, dkl, dkidx, dpint, objkey, rpix, darena;
+        dkept, down, dkl, dkidx, dpint, objkey, rpix, darena, drec;
     // objects
     DevBuf o_i[20], o_f[30], o_d[10], o_iso, o_sortkey, amp, alpha, cellhead, cellnext, vkey, vval, vkalt, vvalt,
         skeys, svals, skalt, svalt, rows;
@@ -95,6 +95,8 @@ struct sexgpu_ctx {
     std::vector<std::string> stage_names;
     std::vector<int> stage_launches;
     std::vector<sexgpu_ctx *> workers;  // contexts of sexgpu_extract_batch
+    void *stage_host = nullptr;         // pinned staging of a batch worker's frames
+    size_t stage_bytes = 0;
     DevBuf dmask;                       // detection mask of the current extraction
     std::vector<float> hmask;
     ConvMask cmask{nullptr, nullptr, 1, 1};
@@ -568,6 +570,7 @@ int pipe_deblend(sexgpu_ctx *ctx) {
     EN(dkidx, M * 4);
     EN(dpint, M * 8 * 4);
     EN(darena, M * DL_ARENA_BYTES);
+    EN(drec, M * 4);
     DebArgs &A = ps.A;
     A.cd = P<float>(ctx->cd);
     A.sub = P<float>(ctx->sub);
@@ -600,6 +603,7 @@ int pipe_deblend(sexgpu_ctx *ctx) {
     D.kidx = P<int>(ctx->dkidx);
     D.pint = P<int>(ctx->dpint);
     D.arena = P<unsigned char>(ctx->darena);
+    D.rec = P<int>(ctx->drec);
     A.sc = d_sc;
     A.alloc = P<int>(ctx->alloc);
     A.objkey = P<unsigned>(ctx->objkey);
@@ -880,7 +884,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
                      &ctx->drl0, &ctx->drl1, &ctx->dnid0, &ctx->dnid1, &ctx->dacc, &ctx->nr0, &ctx->nr1,
                      &ctx->nf0, &ctx->nf1, &ctx->ns0, &ctx->ns1, &ctx->nc0, &ctx->nc1, &ctx->na0, &ctx->na1,
                      &ctx->dkept, &ctx->down, &ctx->dkl, &ctx->dkidx, &ctx->dpint, &ctx->objkey,
-                     &ctx->rpix, &ctx->darena, &ctx->o_iso, &ctx->o_sortkey, &ctx->amp, &ctx->alpha, &ctx->cellhead,
+                     &ctx->rpix, &ctx->darena, &ctx->drec, &ctx->o_iso, &ctx->o_sortkey, &ctx->amp, &ctx->alpha, &ctx->cellhead,
                      &ctx->cellnext, &ctx->vkey, &ctx->vval, &ctx->vkalt, &ctx->vvalt, &ctx->skeys, &ctx->svals,
                      &ctx->skalt, &ctx->svalt, &ctx->rows, &ctx->sc};
     for (DevBuf *b : all) free_buf(*b);
@@ -895,6 +899,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     for (sexgpu_ctx *w : ctx->workers) sexgpu_destroy(w);
+    if (ctx->stage_host) cudaFreeHost(ctx->stage_host);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SEXGPU_OK;
@@ -1178,14 +1183,35 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
         return (long long)frames[a].w * frames[a].h > (long long)frames[b].w * frames[b].h;
     });
     std::atomic<int> next(0);
+    // Each worker copies its frame into its own pinned buffer first, so that
+    // the host->device transfers of different workers are DMA transfers that
+    // proceed in parallel instead of queueing on pageable staging.
     auto run = [&](sexgpu_ctx *wc) {
         cudaSetDevice(wc->device);
         for (int k; (k = next.fetch_add(1)) < nframes;) {
             sexgpu_batch_frame &f = frames[order[k]];
             f.nobj = 0;
-            f.status = f.img && f.cfg ? sexgpu_extract(wc, f.img, nullptr, f.w, f.h, f.cfg, f.objs, f.max_objects,
-                                                       &f.nobj, nullptr, nullptr, nullptr, &f.summary)
-                                      : SEXGPU_ERR_ARG;
+            if (!f.img || !f.cfg || f.w <= 0 || f.h <= 0) {
+                f.status = SEXGPU_ERR_ARG;
+                continue;
+            }
+            const size_t bytes = (size_t)f.w * f.h * sizeof(float);
+            if (wc->stage_bytes < bytes) {
+                if (wc->stage_host) cudaFreeHost(wc->stage_host);
+                wc->stage_host = nullptr;
+                wc->stage_bytes = 0;
+                if (cudaHostAlloc(&wc->stage_host, bytes, cudaHostAllocPortable) == cudaSuccess)
+                    wc->stage_bytes = bytes;
+                else
+                    cudaGetLastError();
+            }
+            const float *src = f.img;
+            if (wc->stage_bytes >= bytes) {
+                memcpy(wc->stage_host, f.img, bytes);
+                src = (const float *)wc->stage_host;
+            }
+            f.status = sexgpu_extract(wc, src, nullptr, f.w, f.h, f.cfg, f.objs, f.max_objects, &f.nobj, nullptr,
+                                      nullptr, nullptr, &f.summary);
         }
     };
     std::vector<std::thread> pool;

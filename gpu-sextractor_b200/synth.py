@@ -196,11 +196,12 @@ def frame_c1(seed=1000, w=4096, h=4096, nsrc=200000, density=None, var=False, fm
     return img, vm
 
 
-def frame_c2(seed=2000, w=4096, h=4096, nsrc=400000):
-    """Workload c2: crowded King-profile field."""
+def frame_c2(seed=2000, w=4096, h=4096, nsrc=400000, rc=300.0, rt=2000.0):
+    """Workload c2: crowded King-profile field (core radius rc, tidal radius
+    rt, centred)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     src = np.zeros(w * h)
-    r = _king_radius(rng, nsrc)
+    r = _king_radius(rng, nsrc, rc=rc, rt=rt)
     th = rng.uniform(0, 2 * np.pi, nsrc)
     xc = w / 2 + r * np.cos(th)
     yc = h / 2 + r * np.sin(th)

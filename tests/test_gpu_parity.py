@@ -112,6 +112,14 @@ def test_object_size_tiers_and_flux_range(gpu_ctx):
     assert len(g) > 100
 
 
+def test_crowded_king_field_precision_settings(gpu_ctx, masks):
+    """The crowded-field precision form (DEBLEND_NTHRESH 64, DEBLEND_MINCONT
+    0.0005, King-profile density) at a quarter of its size."""
+    img = synth.frame_c2(seed=2001, w=1024, h=1024, nsrc=25000, rc=75.0, rt=500.0)
+    g = run_both(gpu_ctx, img, conv=masks["gauss_2.5_5x5"], deblend_nthresh=64, deblend_mincont=0.0005)
+    assert len(g) > 1000
+
+
 def test_constant_frame_has_no_objects(gpu_ctx):
     img = np.full((200, 300), 1000.0, np.float32)
     g = run_both(gpu_ctx, img)
