@@ -349,11 +349,14 @@ struct FrameParams {
     double satur_level, gain, mag_zeropoint, aperture;
     double autoparam0, autoparam1;
     int mask_type, numbering;
+    int wtype;                      // weight map: 0 none, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT
+    int wthr;                       // thresholds follow the local rms (weight map, relative thresholds)
 };
 
 // scalars computed on the device during one extraction
 struct FrameScalars {
     float backmean, backsig, dthresh, thresh;
+    float sigfac;                   // weight-map scale factor (1 without a map)
     int e0cd;                       // exponent of dthresh (all object cd >= dthresh)
     int status;                     // SX_ST_* bits
     int npix_above;
@@ -364,3 +367,38 @@ struct FrameScalars {
     int e0sub;                      // smallest exponent of a non-zero |sub|
     unsigned long long levpix;      // sum of the deblending level of every raw-object pixel
 };
+
+// ---------------------------------------------------------------------------
+// Weight maps (restated after the SExtractor manual and src/weight.c:91-125;
+// the reference has no weighted path).  Relative variance of a weight value:
+// MAP_VAR v, MAP_RMS v^2, MAP_WEIGHT 1/v; calibrated variance: MAP_VAR
+// v*sigfac^2, MAP_RMS v^2, MAP_WEIGHT sigfac^2/v.  NaN, a variance or rms at
+// or above BIG and a weight at or below 0 are unusable (BIG).
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ float sx_rel_var(float v, int wtype) {
+    float r;
+    if (wtype == 1)
+        r = v;
+    else if (wtype == 2)
+        r = v < 1e30f ? v * v : 1e30f;
+    else
+        r = v > 0.0f ? 1.0f / v : 1e30f;
+    return r < 1e30f ? r : 1e30f;
+}
+
+__host__ __device__ __forceinline__ float sx_calib_var(float v, int wtype, float sigfac2) {
+    float r;
+    if (wtype == 1)
+        r = v < 1e30f ? v * sigfac2 : 1e30f;
+    else if (wtype == 2)
+        r = v < 1e30f ? v * v : 1e30f;
+    else
+        r = v > 0.0f ? sigfac2 / v : 1e30f;
+    return r < 1e30f ? r : 1e30f;
+}
+
+// detection / analysis threshold at a pixel of calibrated variance var
+__device__ __forceinline__ float sx_pix_thr(bool wthr, double fac, float var, float global) {
+    return wthr ? (float)(fac * sqrt((double)var)) : global;
+}
+

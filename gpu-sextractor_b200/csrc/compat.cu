@@ -161,7 +161,7 @@ void back_estimate(int back_size, float backfthresh, float *backmean, float *bac
     s.cfg.conv = nullptr;
     s.cfg.conv_w = s.cfg.conv_h = 0;
     sexgpu_ctx *ctx = s.ctx;
-    int rc = pipe_begin(ctx, P<float>(ctx->img), s.w, s.h, &s.cfg);
+    int rc = pipe_begin(ctx, P<float>(ctx->img), nullptr, s.w, s.h, &s.cfg);
     if (!rc) rc = read_scalars(ctx);
     if (rc) {
         compat_fail("back_estimate", rc);

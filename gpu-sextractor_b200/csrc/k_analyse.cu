@@ -98,6 +98,9 @@ struct AnaArgs {
     int w, h, nbx, nby, bw, bh, nobj, minarea, clean_flag;
     FastDiv wdiv;
     double gain, satur;
+    const float *wvar;  // calibrated variance map, or null
+    int wthr;           // analysis threshold follows the local rms
+    double afac;        // ANALYSIS_THRESH
 };
 
 // Robust preanalysis of a deblended object over its final pixels
@@ -109,7 +112,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32) k_analyse_robust(AnaArgs A) {
     if (o >= A.nobj || A.O.level[o] == 0) return;
     const int n = A.O.n[o], off = A.O.off[o], w = A.w, h = A.h;
     const unsigned *pix = A.opix + off;
-    const float dthresh = A.sc->dthresh;
+    const float dthresh = A.O.dthr[o];
     int flags = A.O.flags[o];
 
     XSum srv;
@@ -243,14 +246,15 @@ __global__ void __launch_bounds__(AN_WARPS * 32) k_examineiso(AnaArgs A) {
     if (o >= A.nobj) return;
     const int n = A.O.n[o], off = A.O.off[o], w = A.w;
     const unsigned *pix = A.opix + off;
-    const float dthresh = A.sc->dthresh, thresh = A.sc->thresh, backsig = A.sc->backsig;
+    const float dthresh = A.O.dthr[o], thresh = A.O.athr[o], gthresh = A.sc->thresh, backsig = A.sc->backsig;
     const double mxo = A.O.mx[o], myo = A.O.my[o];
     double dbacknoise2 = backsig * backsig, var = backsig * backsig;
     unsigned pk = 0u;
     unsigned long long best = 0ull;
     int area = 0;
-    XSum stv;
+    XSum stv, svar;
     xs_init(stv);
+    xs_init(svar);
     double esum = 0, emx2 = 0, emy2 = 0, emxy = 0;
     for (int i = lane; i < n; i += 32) {
         unsigned p = __ldg(pix + i);
@@ -260,9 +264,12 @@ __global__ void __launch_bounds__(AN_WARPS * 32) k_examineiso(AnaArgs A) {
         // first maximum of cd in raster order: max cd, then smallest index
         unsigned long long key = ((unsigned long long)f2ord(cdpix) << 32) | (unsigned)(0xffffffffu - p);
         best = max(best, key);
-        area += pv > thresh;
+        // with a weight map: the pixel's own analysis threshold and variance
+        const float pvar = A.wvar ? __ldg(A.wvar + p) : 0.0f;
+        area += pv > sx_pix_thr(A.wthr, A.afac, pvar, gthresh);
         xs_add(stv, pv);
-        double err = dbacknoise2;
+        if (A.wvar) xs_add(svar, pvar);
+        double err = A.wvar ? (double)pvar : dbacknoise2;
         if (A.gain > 0.0 && cdpix > 0.0) err += cdpix / A.gain;
         double x = ix - mxo, y = iy - myo;
         esum += err;
@@ -274,6 +281,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32) k_examineiso(AnaArgs A) {
     best = warp_max_ull(best);
     area = warp_sum_i(area);
     stv = xs_warp_sum(stv);
+    if (A.wvar) svar = xs_warp_sum(svar);
     esum = warp_sum_d(esum);
     emx2 = warp_sum_d(emx2);
     emy2 = warp_sum_d(emy2);
@@ -346,7 +354,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32) k_examineiso(AnaArgs A) {
         }
     }
     double tvd = xs_double(stv);
-    double sigtv = (double)n * var;
+    double sigtv = A.wvar ? xs_double(svar) : (double)n * var;
     if (A.gain > 0.0 && tvd > 0.0) sigtv += tvd / A.gain;
     float fwhm = 0.0f;
     if (thresh0 > 0.0) {
@@ -374,7 +382,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32) k_examineiso(AnaArgs A) {
     A.O.fdnpix[o] = n;
 #pragma unroll
     for (int k = 0; k < SX_NISO_; k++) A.O.iso[(size_t)o * SX_NISO_ + k] = iso[k];
-    if (stv.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
+    if (stv.ovf | svar.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
 }
 
 void launch_analyse(const AnaArgs &A, cudaStream_t st) {

@@ -561,6 +561,98 @@ __global__ void k_row_nodes(const float *__restrict__ back, const float *__restr
 }
 
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// weight maps: blank the unusable pixels, then (after the background) the
+// scale factor sigfac and the calibrated variance map
+// ---------------------------------------------------------------------------
+__global__ void k_weight_mask(const float *__restrict__ img, const float *__restrict__ wmap, int wtype,
+                              float *__restrict__ imgm, long long n) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) imgm[p] = sx_rel_var(__ldg(wmap + p), wtype) < 1e30f ? __ldg(img + p) : -1e30f;
+}
+
+// one warp per mesh: exact mean of the relative variance over its usable
+// pixels; ratio = mesh rms / sqrt(mean) for a usable mesh, -1 otherwise
+__global__ void k_weight_ratio(const float *__restrict__ wmap, int wtype, int w, int h, int bw, int bh, int nbx,
+                               int nby, const float *__restrict__ sigma, float *__restrict__ ratio) {
+    const int lane = threadIdx.x & 31;
+    const int m = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (m >= nbx * nby) return;
+    int x0, y0, mw, mh;
+    mesh_geometry(m, w, h, bw, bh, nbx, nby, x0, y0, mw, mh);
+    XSum sv;
+    xs_init(sv);
+    int n = 0;
+    for (int y = 0; y < mh; y++) {
+        const float *row = wmap + (size_t)(y0 + y) * w + x0;
+        for (int x = lane; x < mw; x += 32) {
+            const float r = sx_rel_var(__ldg(row + x), wtype);
+            if (r < 1e30f) {
+                xs_add(sv, r);
+                n++;
+            }
+        }
+    }
+    sv = xs_warp_sum(sv);
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    if (lane) return;
+    float rt = -1.0f;
+    if (!((float)n < (float)(mw * mh * SX_BACK_MINGOODFRAC))) {
+        const double vmean = xs_double(sv) / n;
+        const float sm = sigma[m];
+        if (vmean > 0.0 && sm > 0.0f) rt = (float)(sm / sqrt(vmean));
+    }
+    ratio[m] = rt;
+}
+
+// sigfac: median of the usable meshes' ratios (hmedian, src/misc.c:30), 1 if none
+__global__ void k_weight_sigfac(const float *__restrict__ ratio, int nb, FrameScalars *sc) {
+    __shared__ unsigned hist[256];
+    __shared__ unsigned s_npos;
+    if (threadIdx.x == 0) s_npos = 0;
+    __syncthreads();
+    unsigned c = 0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) c += ratio[i] > 0.0f;
+    atomicAdd(&s_npos, c);
+    __syncthreads();
+    const int npos = (int)s_npos;
+    const unsigned low = f2ord(__uint_as_float(1u));  // smallest positive float
+    float f = 1.0f;
+    if (npos & 1) {
+        f = ord2f(select_kth(ratio, nb, npos / 2, low, hist));
+    } else if (npos) {
+        const float a = ord2f(select_kth(ratio, nb, npos / 2 - 1, low, hist));
+        const float b = ord2f(select_kth(ratio, nb, npos / 2, low, hist));
+        f = (float)((a + b) / 2.0);
+    }
+    if (threadIdx.x == 0) sc->sigfac = f;
+}
+
+__global__ void k_weight_var(const float *__restrict__ wmap, int wtype, const FrameScalars *sc,
+                             float *__restrict__ wvar, long long n) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const float sigfac = sc->sigfac, sigfac2 = sigfac * sigfac;
+    if (p < n) wvar[p] = sx_calib_var(__ldg(wmap + p), wtype, sigfac2);
+}
+
+void launch_weight_mask(const float *img, const float *wmap, int wtype, float *imgm, long long n, cudaStream_t st) {
+    if (n > 0) k_weight_mask<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(img, wmap, wtype, imgm, n);
+}
+
+// after launch_background: sigfac from the filtered mesh rms map, then the
+// calibrated variance of every pixel
+void launch_weight_var(const BackBufs &B, const float *wmap, const FrameParams &P, float *ratio, float *wvar,
+                       FrameScalars *d_sc, cudaStream_t st) {
+    const int nb = P.nbx * P.nby;
+    const long long n = (long long)P.w * P.h;
+    if (P.wtype != 2) {
+        k_weight_ratio<<<(nb + 3) / 4, 128, 0, st>>>(wmap, P.wtype, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, B.sigma3,
+                                                     ratio);
+        k_weight_sigfac<<<1, 1024, 0, st>>>(ratio, nb, d_sc);
+    }
+    k_weight_var<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(wmap, P.wtype, d_sc, wvar, n);
+}
+
 void launch_background(BackBufs &B, const float *img, const FrameParams &P, FrameScalars *d_sc,
                        cudaStream_t st, int &launches) {
     int nb = P.nbx * P.nby;

@@ -52,8 +52,9 @@ __device__ __forceinline__ void lunion(int *par, int a, int b, int *status) {
 
 
 
-__device__ __forceinline__ void block_thresholds(const DebArgs &A, float fdpeak, float *thr) {
-    float d0 = A.sc->dthresh;
+// the raw object's detection threshold d0 (its pixels' smallest) and the
+// N-1 thresholds above it (src/cuda/cudadeblend.cu:199-217)
+__device__ __forceinline__ void block_thresholds(const DebArgs &A, float d0, float fdpeak, float *thr) {
     for (int i = threadIdx.x; i < A.N; i += blockDim.x) {
         if (i == 0)
             thr[0] = d0;
@@ -156,7 +157,7 @@ __device__ __forceinline__ void deblend_sweep_root(const DebArgs &A, const int r
     __syncthreads();
     const float fdpeak = ord2f(s_peak);
     const double value0 = (double)s_fdflux * A.mincont;
-    block_thresholds(A, fdpeak, thr);
+    block_thresholds(A, A.R.dthresh[r], fdpeak, thr);
     __syncthreads();
     // level of every pixel: largest i with cd >= thr[i]
     for (int k = threadIdx.x; k < P; k += blockDim.x) {
@@ -315,7 +316,7 @@ __device__ __forceinline__ void deblend_assign_root(const DebArgs &A, const int 
     int *pint = A.D.pint + (size_t)off * 8;
     int *status = &A.sc->status;
     const float fdpeak = A.R.fdpeak[r];
-    block_thresholds(A, fdpeak, thr);
+    block_thresholds(A, A.R.dthresh[r], fdpeak, thr);
     for (int i = threadIdx.x; i <= A.N; i += blockDim.x) {
         lvcnt[i] = 0;
         if (i < DB_MAXLEV) lvkept[i] = 0;
@@ -482,6 +483,8 @@ __device__ __forceinline__ void deblend_assign_root(const DebArgs &A, const int 
         A.O.root[o] = r;
         A.O.level[o] = L;
         A.O.node_dthresh[o] = thr[L];
+        A.O.dthr[o] = A.R.dthresh[r];
+        A.O.athr[o] = A.R.thresh[r];
         A.O.xmin[o] = xmin;
         A.O.xmax[o] = xmax;
         A.O.ymin[o] = ymin;

@@ -273,7 +273,7 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
         return;
     }
     const double value0 = (double)s_fdflux * A.mincont;
-    block_thresholds(A, fdpeak, thr);
+    block_thresholds(A, A.R.dthresh[r], fdpeak, thr);
     __syncthreads();
     dl_levels<NT>(A, P, pix, thr, lev, order, lvcnt, lvstart, lvcur, true);
 
@@ -399,7 +399,7 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
     unsigned char *kl = reinterpret_cast<unsigned char *>(kidx + cap);
     int *status = &A.sc->status;
 
-    block_thresholds(A, fdpeak, thr);
+    block_thresholds(A, A.R.dthresh[r], fdpeak, thr);
     // one kept branch that is the whole object at level 0 (nothing split
     // off): every pixel is its own, in list order
     const bool whole = K == 1 && (kept[0] >> 32) == 0;
@@ -566,6 +566,8 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
         A.O.root[o] = r;
         A.O.level[o] = L;
         A.O.node_dthresh[o] = thr[L];
+        A.O.dthr[o] = A.R.dthresh[r];
+        A.O.athr[o] = A.R.thresh[r];
         A.O.xmin[o] = xmin;
         A.O.xmax[o] = xmax;
         A.O.ymin[o] = ymin;

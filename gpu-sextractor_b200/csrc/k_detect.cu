@@ -41,6 +41,7 @@ __global__ void __launch_bounds__(SF_TX *SF_TY) k_sub_filter(const float *__rest
                                                               float *__restrict__ cd, int *__restrict__ lab,
                                                               BackBufs B, int w, int h, int nbx, int back_type,
                                                               const float *__restrict__ mask, int mw, int mh,
+                                                              const float *__restrict__ wvar, int wthr, double dfac,
                                                               FrameScalars *sc) {
     extern __shared__ float tile[];
     const int rx = mw / 2, ry = mh / 2;
@@ -79,7 +80,8 @@ __global__ void __launch_bounds__(SF_TX *SF_TY) k_sub_filter(const float *__rest
             }
             size_t p = (size_t)gy * w + gx;
             cd[p] = acc;
-            bool fg = acc >= dthresh;
+            const float v = wvar ? __ldg(wvar + p) : 0.0f;
+            bool fg = !(wvar && !(v < 1e30f)) && acc >= sx_pix_thr(wthr, dfac, v, dthresh);
             lab[p] = fg ? (int)p : -1;
             nabove += fg;
         }
@@ -157,7 +159,8 @@ __global__ void __launch_bounds__(ST_THREADS) k_sub_filter_tma(const __grid_cons
                                                                int nbx, int back_type,
                                                                const __grid_constant__ ConvTaps taps,
                                                                const float *__restrict__ mask, int mw, int mh,
-                                                               int rxa, FrameScalars *sc) {
+                                                               int rxa, const float *__restrict__ wvar, int wthr,
+                                                               double dfac, FrameScalars *sc) {
     __shared__ __align__(128) float tile[ST_MAXBH * ST_MAXBW];
     __shared__ int s_colk[ST_MAXBW];
     __shared__ float s_coldx[ST_MAXBW];
@@ -270,7 +273,9 @@ __global__ void __launch_bounds__(ST_THREADS) k_sub_filter_tma(const __grid_cons
         if (gx < w && gy < h) {
             const size_t p = (size_t)gy * w + gx;
             cd[p] = acc[k];
-            const bool fg = acc[k] >= dthresh;
+            // with a weight map: unusable pixels never, others against the local rms
+            const float v = wvar ? __ldg(wvar + p) : 0.0f;
+            const bool fg = !(wvar && !(v < 1e30f)) && acc[k] >= sx_pix_thr(wthr, dfac, v, dthresh);
             lab[p] = fg ? (int)p : -1;
             nabove += fg;
         }
@@ -311,7 +316,6 @@ static bool make_frame_tmap(CUtensorMap *m, const float *img, int w, int h, int 
 
 void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const BackBufs &B, const FrameParams &P,
                        FrameScalars *d_sc, const float *d_var, const ConvMask &M, cudaStream_t st, int &launches) {
-    (void)d_var;
     const int mw = M.mw, mh = M.mh;
     const int rxa = ((mw / 2) + 3) & ~3;  // halo width rounded up to 16 bytes
     CUtensorMap tmap;
@@ -322,7 +326,8 @@ void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const 
         if (mw * mh <= 121) memcpy(taps.m, M.host, sizeof(float) * mw * mh);
 #define SF_LAUNCH(a, b)                                                                                      \
     k_sub_filter_tma<a, b><<<tgrid, ST_THREADS, 0, st>>>(tmap, sub, cd, lab, B, P.w, P.h, P.nbx, P.back_type, \
-                                                         taps, M.dev, mw, mh, rxa, d_sc)
+                                                         taps, M.dev, mw, mh, rxa, d_var, P.wthr,           \
+                                                         P.detect_thresh, d_sc)
         if (mw == mh && mw == 1)
             SF_LAUNCH(1, 1);
         else if (mw == mh && mw == 3)
@@ -344,7 +349,8 @@ void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const 
     dim3 grid((P.w + SF_TW - 1) / SF_TW, (P.h + SF_TH - 1) / SF_TH);
     dim3 block(SF_TX, SF_TY);
     size_t smem = sizeof(float) * (SF_TW + mw - 1) * (SF_TH + mh - 1);
-    k_sub_filter<<<grid, block, smem, st>>>(img, sub, cd, lab, B, P.w, P.h, P.nbx, P.back_type, M.dev, mw, mh, d_sc);
+    k_sub_filter<<<grid, block, smem, st>>>(img, sub, cd, lab, B, P.w, P.h, P.nbx, P.back_type, M.dev, mw, mh, d_var,
+                                            P.wthr, P.detect_thresh, d_sc);
     launches += 1;
 }
 

@@ -38,14 +38,14 @@ __global__ void k_clean_count(ObjBufs O, int n, int *cellcnt, int gx, int gy) {
     atomicAdd(&cellcnt[clean_cell(O.mx[i], O.my[i], gx, gy)], 1);
 }
 
-__global__ void k_clean_pack(ObjBufs O, int n, float dthresh, double beta, const int *cellstart, int *cellcur,
-                             CleanObj *packed, int gx, int gy) {
+__global__ void k_clean_pack(ObjBufs O, int n, double beta, const int *cellstart, int *cellcur, CleanObj *packed,
+                             int gx, int gy) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     CleanObj c;
     double unitarea = SX_PI * O.a[i] * O.b[i];
     c.amp = O.fdflux[i] / (2 * unitarea * O.abcor[i]);
-    double q = c.amp / dthresh;
+    double q = c.amp / O.dthr[i];
     c.alpha = ((beta == 1.0 ? q : pow(q, 1.0 / beta)) - 1) * unitarea / O.fdnpix[i];
     c.mx = O.mx[i];
     c.my = O.my[i];
@@ -177,6 +177,7 @@ struct EndArgs {
     FrameScalars *sc;
     int w, h, n, mask_type;
     double aperture, autoparam0, autoparam1, gain, zp, satur;
+    const float *wvar;  // calibrated variance map, or null
 };
 
 // src/cuda/cudaanalyse.cu:104-287 (computeaperflux, one aperture).  The
@@ -222,7 +223,7 @@ __device__ void aper_warp(const EndArgs &A, int o, double mx, double my, int &fl
         const int i = base + lane;
         bool in = false;
         float locarea = 0.0f;
-        double pix = 0.0;
+        double pix = 0.0, pvar = var;
         if (i < nn) {
             const int yo = i / bw, x = xmin + (i - yo * bw), y = ymin + yo;
             float dx = x - mx, dy = y - my, r2;
@@ -240,18 +241,24 @@ __device__ void aper_warp(const EndArgs &A, int o, double mx, double my, int &fl
                     locarea = 1.0;
                 pix = A.sub[(size_t)y * w + x];
                 int t = A.alloc[(size_t)y * w + x], x2, y2;
+                // with a weight map: the variance of the pixel actually used,
+                // 0 for a pixel replaced by 0 (src/photom.c:128-145)
+                if (A.wvar) pvar = A.wvar[(size_t)y * w + x];
                 if ((t >= 0 && t != o) || pix <= -SX_BIG) {
                     if (corrflag && (x2 = (int)(2 * mx + 0.49999 - x)) >= 0 && x2 < w &&
                         (y2 = (int)(2 * my + 0.49999 - y)) >= 0 && y2 < h &&
                         ((t = A.alloc[(size_t)y2 * w + x2]) == o || t == -1) &&
-                        A.sub[(size_t)y2 * w + x2] > -SX_BIG)
+                        A.sub[(size_t)y2 * w + x2] > -SX_BIG) {
                         pix = A.sub[(size_t)y2 * w + x2];
-                    else
+                        if (A.wvar) pvar = A.wvar[(size_t)y2 * w + x2];
+                    } else {
                         pix = 0.0;
+                        if (A.wvar) pvar = 0.0;
+                    }
                 }
             }
         }
-        const double tsig = var * locarea, ttv = locarea * pix;
+        const double tsig = pvar * locarea, ttv = locarea * pix;
         for (unsigned m = __ballot_sync(0xffffffffu, in); m; m &= m - 1) {
             const int q = __ffs(m) - 1;
             area += __shfl_sync(0xffffffffu, locarea, q);
@@ -295,7 +302,7 @@ __global__ void k_endobject(EndArgs A) {
     int flags = A.O.flags[o];
     float a = A.O.a[o], b = A.O.b[o];
     double mx = A.O.mx[o], my = A.O.my[o];
-    float flux = A.O.flux[o], fluxerr = A.O.fluxerr[o], dthresh = A.sc->dthresh, backsig = A.sc->backsig;
+    float flux = A.O.flux[o], fluxerr = A.O.fluxerr[o], dthresh = A.O.dthr[o], backsig = A.sc->backsig;
     int fdnpix = A.O.fdnpix[o];
     aper_warp(A, o, mx, my, flags);
     // AUTO / Kron, src/cuda/cudaanalyse.cu:293-592
@@ -406,8 +413,9 @@ __global__ void k_endobject(EndArgs A) {
             flags |= SX_OBJ_APERT_PB;
         }
         area = areab = 0;
-        XSum stv;
+        XSum stv, svar;
         xs_init(stv);
+        xs_init(svar);
         int bw = xmax - xmin, nn = bw * (ymax - ymin);
         const FastDiv bd = make_fastdiv_dev((unsigned)bw);
         for (int i = lane; i < nn; i += 32) {
@@ -418,29 +426,35 @@ __global__ void k_endobject(EndArgs A) {
                 area++;
                 pix = A.sub[(size_t)y * w + x];
                 int t = A.alloc[(size_t)y * w + x];
+                float pvar = A.wvar ? A.wvar[(size_t)y * w + x] : 0.0f;
                 if ((t >= 0 && t != o) || pix <= -SX_BIG) {
                     areab++;
                     int x2, y2;
                     if (corrflag && (x2 = (int)(2 * mx + 0.49999 - x)) >= 0 && x2 < w &&
                         (y2 = (int)(2 * my + 0.49999 - y)) >= 0 && y2 < h &&
                         ((t = A.alloc[(size_t)y2 * w + x2]) == -1 || t == o) &&
-                        A.sub[(size_t)y2 * w + x2] > -SX_BIG)
+                        A.sub[(size_t)y2 * w + x2] > -SX_BIG) {
                         pix = A.sub[(size_t)y2 * w + x2];
-                    else
+                        if (A.wvar) pvar = A.wvar[(size_t)y2 * w + x2];
+                    } else {
                         pix = 0.0;
+                        pvar = 0.0f;
+                    }
                 }
                 xs_add(stv, pix);
+                if (A.wvar) xs_add(svar, pvar);
             }
         }
         stv = xs_warp_all2(stv);
+        if (A.wvar) svar = xs_warp_all2(svar);
         area = wsum(area);
         areab = wsum(areab);
         if ((float)areab > SX_CROWD_THRESHOLD * area) flags |= SX_OBJ_CROWDED;
         tv = xs_double(stv);
-        sigtv = (double)area * var;
+        sigtv = A.wvar ? xs_double(svar) : (double)area * var;
         tv -= area * (double)0.0f;
         if (A.gain > 0.0 && tv > 0.0) sigtv += tv / A.gain;
-        if (stv.ovf && lane == 0) atomicOr(&A.sc->status, SX_ST_RANGE);
+        if ((stv.ovf | svar.ovf) && lane == 0) atomicOr(&A.sc->status, SX_ST_RANGE);
     } else
         tv = sigtv = 0.0;
     if ((sr1.ovf | sv1.ovf) && lane == 0) atomicOr(&A.sc->status, SX_ST_RANGE);
@@ -542,8 +556,8 @@ __global__ void k_write_rows(ObjBufs O, const unsigned *vals, int ns, float dthr
     q.poserr_my2 = O.pmy2[o];
     q.poserr_mxy = O.pmxy[o];
     q.bkg = O.bkg[o];
-    q.thresh = thresh;
-    q.dthresh = dthresh;
+    q.thresh = O.athr[o];
+    q.dthresh = O.dthr[o];
     q.mthresh = O.mthresh[o];
     q.fwhm = O.fwhm[o];
     q.flux_iso = O.flux[o];

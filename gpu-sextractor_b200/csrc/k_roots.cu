@@ -66,6 +66,35 @@ __global__ void k_pos2idx(const unsigned *__restrict__ vals, int *__restrict__ p
     if (j < m) pos2idx[vals[j]] = j;
 }
 
+// Each raw object's thresholds: the smallest detection and analysis threshold
+// of its pixels (the global ones without a weight map); rdthr/rathr start at a
+// large positive float and are lowered through their bit patterns (positive
+// floats order like their bits).  The fixed-point scale of the exact branch
+// sums, sc->e0cd, becomes the exponent of the smallest of them.
+__global__ void k_root_thresholds(const int *__restrict__ lab, const int *__restrict__ cnt,
+                                  const int *__restrict__ rid, long long n, int minarea, const float *__restrict__ wvar,
+                                  int wthr, double dfac, double afac, FrameScalars *sc, int *rdthr, int *rathr) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int l = lab[p];
+    if (l < 0 || cnt[l] < minarea) return;
+    const int r = rid[l];
+    const float v = wvar ? __ldg(wvar + p) : 0.0f;
+    const float dt = sx_pix_thr(wthr, dfac, v, sc->dthresh), at = sx_pix_thr(wthr, afac, v, sc->thresh);
+    atomicMin(rdthr + r, __float_as_int(dt));
+    atomicMin(rathr + r, __float_as_int(at));
+    atomicMin(&sc->e0cd, fexpo(dt));
+}
+
+// without a weight map every raw object has the global thresholds
+__global__ void k_root_thresholds_global(int nroots, const FrameScalars *sc, float *rdthr, float *rathr) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nroots) {
+        rdthr[r] = sc->dthresh;
+        rathr[r] = sc->thresh;
+    }
+}
+
 int bits_for(long long v) {
     int b = 1;
     while ((1ll << b) <= v) b++;

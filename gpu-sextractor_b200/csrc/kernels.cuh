@@ -23,6 +23,7 @@ struct RootBufs {
     int *ymax, *lastx;                  // completion-order keys
     float *fdpeak, *fdflux;
     int *nkept, *objbase;
+    float *dthresh, *thresh;            // smallest detection / analysis threshold of its pixels
 };
 
 // per-element scratch of the deblending (index = position in the root pixel list)
@@ -53,11 +54,15 @@ struct ObjBufs {
     float *kron, *flux_auto, *fluxerr_auto, *mag_auto, *magerr_auto;
     float *mag_iso, *magerr_iso, *fluxerr_iso;
     int *fdnpix;
+    float *dthr, *athr;                 // the raw object's detection / analysis thresholds
     unsigned long long *sortkey;
 };
 
 void launch_background(BackBufs &B, const float *img, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st,
                        int &launches);
+void launch_weight_mask(const float *img, const float *wmap, int wtype, float *imgm, long long n, cudaStream_t st);
+void launch_weight_var(const BackBufs &B, const float *wmap, const FrameParams &P, float *ratio, float *wvar,
+                       FrameScalars *d_sc, cudaStream_t st);
 
 // The detection mask of one extraction: row-major mw x mh values on the
 // device and on the host (per context, so that contexts extracting at the

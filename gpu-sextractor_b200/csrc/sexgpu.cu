@@ -52,6 +52,7 @@ struct PipeState {
     FrameParams Pm;
     int w = 0, h = 0;
     const float *d_img = nullptr;
+    const float *wvar = nullptr;  // calibrated variance map (weight map given), else null
     int nroots = 0, nrootpix = 0, nobj = 0, ns = 0;
     int stage = 0;  // last completed: 1 background ... 6 catalogue
     BackBufs B;
@@ -70,18 +71,18 @@ struct sexgpu_ctx {
     std::vector<DevBuf *> bufs;
     std::string err;
     // frame-size buffers
-    DevBuf img, sub, cd, lab, cnt, flag, pos, alloc, seg, pos2idx, var;
+    DevBuf img, sub, cd, lab, cnt, flag, pos, alloc, seg, pos2idx, var, imgm, wvar, wratio;
     // scan / sort scratch
     DevBuf scan_tmp, keys, vals, kalt, valt;
     // background
     DevBuf ms, back, sigma, back2, back3, sigma3, dback, bu, rownode, rowdnode, rowu, colk, coldx;
     // roots
-    DevBuf rsize, roff, rfirst, rymax, rlastx, rfdpeak, rfdflux, rnkept, robjbase, rlists, rcounts;
+    DevBuf rsize, roff, rfirst, rymax, rlastx, rfdpeak, rfdflux, rnkept, robjbase, rdthr, rathr, rlists, rcounts;
     // deblend scratch
     DevBuf dpar, dlev, dsz, dorder, drl0, drl1, dnid0, dnid1, dacc, nr0, nr1, nf0, nf1, ns0, ns1, nc0, nc1, na0, na1,
         dkept, down, dkl, dkidx, dpint, objkey, rpix, darena, drec;
     // objects
-    DevBuf o_i[20], o_f[30], o_d[10], o_iso, o_sortkey, amp, alpha, cellhead, cellnext, vkey, vval, vkalt, vvalt,
+    DevBuf o_i[20], o_f[32], o_d[10], o_iso, o_sortkey, amp, alpha, cellhead, cellnext, vkey, vval, vkalt, vvalt,
         skeys, svals, skalt, svalt, rows;
     DevBuf sc;
     FrameScalars hsc;
@@ -205,7 +206,7 @@ int check_config(const sexgpu_config *cfg, int w, int h) {
                              cfg->conv_h > SX_MAXCONV))
         return SEXGPU_ERR_ARG;
     if (cfg->detect_minarea < 1 || cfg->deblend_nthresh < 1 || cfg->deblend_nthresh > 64) return SEXGPU_ERR_ARG;
-    if (cfg->weight_type != 0) return SEXGPU_ERR_ARG;
+    if (cfg->weight_type < 0 || cfg->weight_type > 3) return SEXGPU_ERR_ARG;
     return SEXGPU_OK;
 }
 
@@ -242,12 +243,15 @@ void make_params(const sexgpu_config *cfg, int w, int h, FrameParams &P) {
     P.autoparam1 = cfg->phot_autoparams[1];
     P.mask_type = cfg->mask_type;
     P.numbering = cfg->numbering;
+    P.wtype = cfg->weight_type;
+    P.wthr = cfg->weight_type != 0 && cfg->thresh_type != 1;
 }
 
 __global__ void k_init_scalars(FrameScalars *sc) {
     FrameScalars z;
     memset(&z, 0, sizeof(z));
     z.e0sub = 1000;
+    z.sigfac = 1.0f;
     *sc = z;
 }
 
@@ -290,13 +294,13 @@ int load_mask(sexgpu_ctx *ctx, const float *mask, int mw, int mh) {
 int alloc_objects(sexgpu_ctx *ctx, int nobj) {
     size_t n = (size_t)nobj + 1;
     int *ip[20];
-    float *fp[30];
+    float *fp[32];
     double *dp[10];
     for (int i = 0; i < 20; i++) {
         EN(o_i[i], n * sizeof(int));
         ip[i] = P<int>(ctx->o_i[i]);
     }
-    for (int i = 0; i < 30; i++) {
+    for (int i = 0; i < 32; i++) {
         EN(o_f[i], n * sizeof(float));
         fp[i] = P<float>(ctx->o_f[i]);
     }
@@ -354,6 +358,8 @@ int alloc_objects(sexgpu_ctx *ctx, int nobj) {
     O.mag_auto = fp[27];
     O.magerr_auto = fp[28];
     O.mag_iso = fp[29];
+    O.dthr = fp[30];
+    O.athr = fp[31];
     O.mx = dp[0];
     O.my = dp[1];
     O.mx2 = dp[2];
@@ -379,8 +385,9 @@ unsigned grid1(long long n, int t) { return n > 0 ? (unsigned)((n + t - 1) / t) 
 // State that crosses stages lives in ctx->ps; parameters a later stage reads
 // (ps.Pm) may be changed between stages.
 // ---------------------------------------------------------------------------
-int pipe_begin(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu_config *cfg) {
+int pipe_begin(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, int h, const sexgpu_config *cfg) {
     int rc = check_config(cfg, w, h);
+    if (!rc && (cfg->weight_type != 0) != (d_wmap != nullptr)) rc = SEXGPU_ERR_ARG;
     if (rc) {
         ctx->err = "invalid configuration or frame size";
         return rc;
@@ -451,7 +458,22 @@ int pipe_begin(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu_c
     stage_begin(ctx);
     int nl = 0;
     k_init_scalars<<<1, 1, 0, st>>>(d_sc);
+    ps.wvar = nullptr;
+    if (d_wmap) {
+        // pixels of unusable weight are blank for the background and the detection
+        EN(imgm, N * 4);
+        EN(wvar, N * 4);
+        EN(wratio, (size_t)nb * 4);
+        launch_weight_mask(d_img, d_wmap, Pm.wtype, P<float>(ctx->imgm), N, st);
+        d_img = ps.d_img = P<float>(ctx->imgm);
+        nl += 1;
+    }
     launch_background(B, d_img, Pm, d_sc, st, nl);
+    if (d_wmap) {
+        launch_weight_var(B, d_wmap, Pm, P<float>(ctx->wratio), P<float>(ctx->wvar), d_sc, st);
+        ps.wvar = P<float>(ctx->wvar);
+        nl += Pm.wtype != 2 ? 3 : 1;
+    }
     stage_mark(ctx, "background", nl + 1);
     ps.stage = 1;
     return SEXGPU_OK;
@@ -469,7 +491,7 @@ int pipe_detect(sexgpu_ctx *ctx) {
     FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
     int *tmp = P<int>(ctx->scan_tmp);
     int rc = SEXGPU_OK, nl = 0;
-    launch_sub_filter(d_img, P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm, d_sc, nullptr,
+    launch_sub_filter(d_img, P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm, d_sc, ps.wvar,
                       ctx->cmask, st, nl);
     stage_mark(ctx, "sub_filter", nl);
 
@@ -500,6 +522,8 @@ int pipe_detect(sexgpu_ctx *ctx) {
     EN(rfdflux, (nroots + 1) * 4);
     EN(rnkept, (nroots + 1) * 4);
     EN(robjbase, (nroots + 1) * 4);
+    EN(rdthr, (nroots + 1) * 4);
+    EN(rathr, (nroots + 1) * 4);
     RootBufs &R = ps.R;
     R.size = P<int>(ctx->rsize);
     R.off = P<int>(ctx->roff);
@@ -510,12 +534,23 @@ int pipe_detect(sexgpu_ctx *ctx) {
     R.fdflux = P<float>(ctx->rfdflux);
     R.nkept = P<int>(ctx->rnkept);
     R.objbase = P<int>(ctx->robjbase);
+    R.dthresh = P<float>(ctx->rdthr);
+    R.thresh = P<float>(ctx->rathr);
     k_root_setup<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, flag, R.size, R.first, N, Pm.minarea);
     exclusive_scan(R.size, R.off, nroots, &d_sc->nrootpix, tmp, st);
     k_pix_flags<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, pos, N, Pm.minarea);
     exclusive_scan(pos, pos, N, nullptr, tmp, st);
     unsigned *keys = P<unsigned>(ctx->keys), *vals = P<unsigned>(ctx->vals);
     k_pix_compact<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, flag, pos, keys, vals, N, Pm.minarea);
+    if (ps.wvar) {
+        CK(cudaMemsetAsync(R.dthresh, 0x7f, (size_t)(nroots + 1) * 4, st));
+        CK(cudaMemsetAsync(R.thresh, 0x7f, (size_t)(nroots + 1) * 4, st));
+        k_root_thresholds<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, flag, N, Pm.minarea, ps.wvar, Pm.wthr,
+                                                         Pm.detect_thresh, Pm.analysis_thresh, d_sc,
+                                                         (int *)R.dthresh, (int *)R.thresh);
+    } else {
+        k_root_thresholds_global<<<grid1(nroots, 256), 256, 0, st>>>(nroots, d_sc, R.dthresh, R.thresh);
+    }
     rc = read_scalars(ctx);
     if (rc) return rc;
     const int nrootpix = ps.nrootpix = ctx->hsc.nrootpix;
@@ -526,7 +561,7 @@ int pipe_detect(sexgpu_ctx *ctx) {
     CK(cudaMemsetAsync(pos2idx, 0xff, N * 4, st));
     k_pos2idx<<<grid1(nrootpix, 256), 256, 0, st>>>(rpix, pos2idx, nrootpix);
     k_alloc_init<<<grid1(N, 256), 256, 0, st>>>(lab, P<int>(ctx->alloc), N);
-    stage_mark(ctx, "roots", 8 + 3 * scan_launches(N) + scan_launches(nroots) + radix_launches(bits_for(nroots), nrootpix));
+    stage_mark(ctx, "roots", 9 + 3 * scan_launches(N) + scan_launches(nroots) + radix_launches(bits_for(nroots), nrootpix));
     ps.stage = 2;
     return SEXGPU_OK;
 }
@@ -674,6 +709,9 @@ int pipe_analyse(sexgpu_ctx *ctx) {
     AA.gain = Pm.gain;
     AA.satur = Pm.satur_level;
     AA.wdiv = make_fastdiv((unsigned)w);
+    AA.wvar = ps.wvar;
+    AA.wthr = Pm.wthr;
+    AA.afac = Pm.analysis_thresh;
     launch_analyse(AA, st);
     stage_mark(ctx, "analyse", 2 + radix_launches(bits_for(nobj), nrootpix) + scan_launches(nobj));
     ps.stage = 4;
@@ -709,7 +747,7 @@ int pipe_clean(sexgpu_ctx *ctx) {
         CK(cudaMemsetAsync(cellcur, 0, (size_t)(ncell + 1) * 4, st));
         k_clean_count<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, cellcnt, gx, gy);
         exclusive_scan(cellcnt, cellcnt, ncell + 1, nullptr, tmp, st);
-        k_clean_pack<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, ctx->hsc.dthresh, Pm.clean_param, cellcnt, cellcur,
+        k_clean_pack<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, Pm.clean_param, cellcnt, cellcur,
                                                        P<CleanObj>(ctx->amp), gx, gy);
         k_clean_pairs<<<grid1(nobj, 4), 128, 0, st>>>(P<CleanObj>(ctx->amp), nobj, Pm.clean_param, cellcnt, O.master,
                                                       gx, gy);
@@ -764,6 +802,7 @@ int pipe_end(sexgpu_ctx *ctx) {
     E.gain = Pm.gain;
     E.zp = Pm.mag_zeropoint;
     E.satur = Pm.satur_level;
+    E.wvar = ps.wvar;
     if (nobj > 0) k_endobject<<<grid1(nobj, 4), 128, 0, st>>>(E);
     stage_mark(ctx, "endobject", nobj > 0);
 
@@ -802,8 +841,8 @@ int pipe_end(sexgpu_ctx *ctx) {
 }
 
 // the whole pipeline on a device-resident frame
-int run_pipeline(sexgpu_ctx *ctx, const float *d_img, int w, int h, const sexgpu_config *cfg) {
-    int rc = pipe_begin(ctx, d_img, w, h, cfg);
+int run_pipeline(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, int h, const sexgpu_config *cfg) {
+    int rc = pipe_begin(ctx, d_img, d_wmap, w, h, cfg);
     if (!rc) rc = pipe_detect(ctx);
     if (!rc) rc = pipe_deblend(ctx);
     if (!rc) rc = pipe_analyse(ctx);
@@ -828,6 +867,7 @@ void fill_summary(sexgpu_ctx *ctx, const FrameParams &P, sexgpu_summary *s) {
     s->ndetected = ctx->last_nobj;
     s->nobj = ctx->last_ns;
     s->level_pix = (int64_t)ctx->hsc.levpix;
+    s->sigfac = ctx->hsc.sigfac;
 }
 
 }  // namespace
@@ -880,7 +920,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
                      &ctx->valt, &ctx->ms, &ctx->back, &ctx->sigma, &ctx->back2, &ctx->back3, &ctx->sigma3,
                      &ctx->dback, &ctx->bu, &ctx->rownode, &ctx->rowdnode, &ctx->rowu, &ctx->colk, &ctx->coldx,
                      &ctx->rsize, &ctx->roff, &ctx->rfirst, &ctx->rymax, &ctx->rlastx, &ctx->rfdpeak,
-                     &ctx->rfdflux, &ctx->rnkept, &ctx->robjbase, &ctx->rlists, &ctx->rcounts, &ctx->dpar, &ctx->dlev, &ctx->dsz, &ctx->dorder,
+                     &ctx->rfdflux, &ctx->rnkept, &ctx->robjbase, &ctx->rdthr, &ctx->rathr, &ctx->imgm, &ctx->wvar, &ctx->wratio, &ctx->rlists, &ctx->rcounts, &ctx->dpar, &ctx->dlev, &ctx->dsz, &ctx->dorder,
                      &ctx->drl0, &ctx->drl1, &ctx->dnid0, &ctx->dnid1, &ctx->dacc, &ctx->nr0, &ctx->nr1,
                      &ctx->nf0, &ctx->nf1, &ctx->ns0, &ctx->ns1, &ctx->nc0, &ctx->nc1, &ctx->na0, &ctx->na1,
                      &ctx->dkept, &ctx->down, &ctx->dkl, &ctx->dkidx, &ctx->dpint, &ctx->objkey,
@@ -952,10 +992,9 @@ const char *sexgpu_last_error(sexgpu_ctx *ctx) { return ctx ? ctx->err.c_str() :
 int sexgpu_extract_device(sexgpu_ctx *ctx, const float *d_img, const float *d_var, int w, int h,
                           const sexgpu_config *cfg, sexgpu_summary *sum) {
     if (!ctx || !d_img) return SEXGPU_ERR_ARG;
-    if (d_var) return SEXGPU_ERR_ARG;
     cudaSetDevice(ctx->device);
     ctx->err.clear();
-    int rc = run_pipeline(ctx, d_img, w, h, cfg);
+    int rc = run_pipeline(ctx, d_img, d_var, w, h, cfg);
     if (rc == SEXGPU_OK && sum) {
         FrameParams Pm;
         make_params(cfg, w, h, Pm);
@@ -991,12 +1030,15 @@ int sexgpu_extract(sexgpu_ctx *ctx, const float *img, const float *var, int w, i
                    sexgpu_object *objs, int max_objects, int *nobj, int32_t *segmap, float *sub, float *cd,
                    sexgpu_summary *sum) {
     if (!ctx || !img || w <= 0 || h <= 0) return SEXGPU_ERR_ARG;
-    if (var) return SEXGPU_ERR_ARG;
     cudaSetDevice(ctx->device);
     long long N = (long long)w * h;
     EN(img, N * 4);
     CK(cudaMemcpyAsync(ctx->img.p, img, N * 4, cudaMemcpyHostToDevice, ctx->stream));
-    int rc = sexgpu_extract_device(ctx, P<float>(ctx->img), nullptr, w, h, cfg, sum);
+    if (var) {
+        EN(var, N * 4);
+        CK(cudaMemcpyAsync(ctx->var.p, var, N * 4, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    int rc = sexgpu_extract_device(ctx, P<float>(ctx->img), var ? P<float>(ctx->var) : nullptr, w, h, cfg, sum);
     if (rc) return rc;
     return sexgpu_copy_results(ctx, objs, max_objects, nobj, segmap, sub, cd);
 }
@@ -1210,7 +1252,7 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
                 memcpy(wc->stage_host, f.img, bytes);
                 src = (const float *)wc->stage_host;
             }
-            f.status = sexgpu_extract(wc, src, nullptr, f.w, f.h, f.cfg, f.objs, f.max_objects, &f.nobj, nullptr,
+            f.status = sexgpu_extract(wc, src, f.wmap, f.w, f.h, f.cfg, f.objs, f.max_objects, &f.nobj, nullptr,
                                       nullptr, nullptr, &f.summary);
         }
     };

@@ -68,13 +68,13 @@ class Summary(C.Structure):
         ("nbackx", C.c_int), ("nbacky", C.c_int), ("backmean", C.c_float), ("backsig", C.c_float),
         ("dthresh", C.c_float), ("thresh", C.c_float), ("npix_above", C.c_int64),
         ("nraw", C.c_int32), ("nraw_pix", C.c_int64), ("ndetected", C.c_int32), ("nobj", C.c_int32),
-        ("level_pix", C.c_int64),
+        ("level_pix", C.c_int64), ("sigfac", C.c_float), ("pad", C.c_int32),
     ]
 
 
 class BatchFrame(C.Structure):
     """sexgpu_batch_frame."""
-    _fields_ = [("img", C.POINTER(C.c_float)), ("w", C.c_int32), ("h", C.c_int32),
+    _fields_ = [("img", C.POINTER(C.c_float)), ("wmap", C.POINTER(C.c_float)), ("w", C.c_int32), ("h", C.c_int32),
                 ("cfg", C.POINTER(Config)), ("objs", C.c_void_p), ("max_objects", C.c_int32),
                 ("nobj", C.c_int32), ("status", C.c_int32), ("pad", C.c_int32), ("summary", Summary)]
 
@@ -198,10 +198,12 @@ class Context:
                self.h, "sexgpu_filter")
         return cd
 
-    def extract(self, img, max_objects=None, want_maps=False, segmap=True, **kw):
-        """Host frame in, catalogue (+ segmentation map) out."""
+    def extract(self, img, max_objects=None, want_maps=False, segmap=True, weight=None, **kw):
+        """Host frame in, catalogue (+ segmentation map) out.  weight: the
+        weight map of weight_type (1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT)."""
         cfg = make_config(**kw)
         img = np.ascontiguousarray(img, np.float32)
+        wmap = np.ascontiguousarray(weight, np.float32) if weight is not None else None
         h, w = img.shape
         if max_objects is None:
             max_objects = w * h // max(1, cfg.detect_minarea) // 2 + 16
@@ -211,7 +213,7 @@ class Context:
         s = Summary()
         sub = np.zeros_like(img) if want_maps else None
         cd = np.zeros_like(img) if want_maps else None
-        rc = lib().sexgpu_extract(self.h, _f(img), None, w, h, C.byref(cfg),
+        rc = lib().sexgpu_extract(self.h, _f(img), _f(wmap) if wmap is not None else None, w, h, C.byref(cfg),
                                   objs.ctypes.data_as(C.c_void_p), max_objects, C.byref(n),
                                   seg.ctypes.data_as(C.c_void_p) if segmap else None,
                                   _f(sub) if want_maps else None,
@@ -221,11 +223,13 @@ class Context:
             return objs[:n.value], seg, s, sub, cd
         return objs[:n.value], seg, s
 
-    def extract_device(self, dev_ptr, w, h, **kw):
-        """Frame already in device memory (e.g. torch tensor .data_ptr())."""
+    def extract_device(self, dev_ptr, w, h, wmap_ptr=None, **kw):
+        """Frame (and weight map) already in device memory (e.g. torch tensor
+        .data_ptr())."""
         cfg = make_config(**kw)
         s = Summary()
-        _check(lib().sexgpu_extract_device(self.h, C.c_void_p(dev_ptr), None, w, h, C.byref(cfg), C.byref(s)),
+        _check(lib().sexgpu_extract_device(self.h, C.c_void_p(dev_ptr), C.c_void_p(wmap_ptr) if wmap_ptr else None,
+                                           w, h, C.byref(cfg), C.byref(s)),
                self.h, "sexgpu_extract_device")
         return s
 
@@ -239,20 +243,24 @@ class Context:
         return (objs[:n.value], seg) if segmap else objs[:n.value]
 
     def extract_batch(self, frames, workers=0, max_objects=None):
-        """frames: list of (img, settings dict).  All frames go to the library
+        """frames: list of (img, settings dict[, weight map]).  All frames go to the library
         in one sexgpu_extract_batch call; returns [(catalogue, summary)]."""
         n = len(frames)
         arr = (BatchFrame * max(n, 1))()
         keep = []
-        for i, (img, kw) in enumerate(frames):
+        for i, fr in enumerate(frames):
+            img, kw = fr[0], fr[1]
+            wmap = np.ascontiguousarray(fr[2], np.float32) if len(fr) > 2 and fr[2] is not None else None
             img = np.ascontiguousarray(img, np.float32)
             cfg = make_config(**kw)
             h, w = img.shape
             cap = max_objects or (w * h // max(1, cfg.detect_minarea) // 2 + 16)
             objs = np.zeros(cap, OBJECT_DTYPE)
-            keep.append((img, cfg, objs))
+            keep.append((img, cfg, objs, wmap))
             f = arr[i]
             f.img, f.w, f.h, f.cfg = _f(img), w, h, C.pointer(cfg)
+            if wmap is not None:
+                f.wmap = _f(wmap)
             f.objs, f.max_objects = objs.ctypes.data_as(C.c_void_p), cap
         _check(lib().sexgpu_extract_batch(self.h, arr, n, workers), self.h, "sexgpu_extract_batch")
         return [(keep[i][2][:arr[i].nobj], arr[i].summary) for i in range(n)]

@@ -68,7 +68,7 @@ typedef struct {
     double  phot_aperture;      /* PHOT_APERTURES (one diameter) */
     double  phot_autoparams[2]; /* PHOT_AUTOPARAMS */
     int     mask_type;          /* MASK_TYPE: 0 NONE, 1 BLANK, 2 CORRECT */
-    int     weight_type;        /* WEIGHT_TYPE: 0 NONE, 1 MAP_VAR */
+    int     weight_type;        /* WEIGHT_TYPE: 0 NONE, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT */
     int     numbering;          /* 0 completion order, 1 first-pixel order */
 } sexgpu_config;
 
@@ -106,6 +106,8 @@ typedef struct {
     int32_t nobj;               /* catalogue rows after CLEAN */
     int64_t level_pix;          /* sum over raw-object pixels of the highest
                                    deblending level each pixel reaches */
+    float   sigfac;             /* weight-map scale factor (1 without a map) */
+    int32_t pad;
 } sexgpu_summary;
 
 typedef struct sexgpu_ctx sexgpu_ctx;
@@ -117,8 +119,15 @@ int sexgpu_destroy(sexgpu_ctx *ctx);
 /* Run later work on this cudaStream_t (NULL: the context's own stream). */
 int sexgpu_set_stream(sexgpu_ctx *ctx, void *stream);
 
-/* Whole extraction of one host frame (w*h float32, row-major).  var (w*h,
- * may be NULL) is the variance map for weight_type MAP_VAR.  Writes up to
+/* Whole extraction of one host frame (w*h float32, row-major).  var (w*h)
+ * is the weight map of cfg->weight_type (variance, rms or weight values) and
+ * must be NULL exactly when weight_type is NONE.  With a weight map, pixels of
+ * unusable weight (variance or rms >= 1e30, weight <= 0, NaN) are blank, the
+ * map is calibrated to the frame's noise (MAP_VAR, MAP_WEIGHT: scale factor
+ * summary.sigfac, the median over the meshes of rms / sqrt(mean relative
+ * variance)), relative thresholds are taken against the local rms, each
+ * object's thresholds are its pixels' smallest, and the flux errors add the
+ * pixels' variances.  Writes up to
  * max_objects catalogue rows to objs (host) and their count to *nobj; if the
  * catalogue is longer, *nobj holds its length and SEXGPU_ERR_CAPACITY is
  * returned.  segmap (w*h int32 host, may be NULL) receives NUMBER per pixel,
@@ -184,6 +193,7 @@ int sexgpu_background_noalloc(const float *d_img, float *d_sub, int w, int h, co
 /* One frame of a batch: inputs, the caller's catalogue buffer, and outputs. */
 typedef struct {
     const float *img;            /* host frame, w*h float32, row-major */
+    const float *wmap;           /* host weight map of cfg->weight_type, or NULL */
     int32_t w, h;
     const sexgpu_config *cfg;    /* this frame's settings */
     sexgpu_object *objs;         /* host catalogue buffer (may be NULL) */

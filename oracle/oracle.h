@@ -73,7 +73,7 @@ typedef struct {
     double  phot_autoparams[2]; /* PHOT_AUTOPARAMS */
     int     mask_type;          /* 0 NONE, 1 BLANK, 2 CORRECT */
     /* weighting */
-    int     weight_type;        /* 0 NONE, 1 MAP_VAR */
+    int     weight_type;        /* 0 NONE, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT */
     /* catalog order: 0 completion order, 1 first-pixel order */
     int     numbering;
 } orc_config;
@@ -111,6 +111,7 @@ typedef struct {
     int64_t nraw_pix;           /* pixels in raw objects */
     int32_t ndetected;          /* objects after deblending */
     int32_t nobj;               /* objects after CLEAN (catalog rows) */
+    float   sigfac;             /* weight-map scale (1 without a weight map) */
 } orc_summary;
 
 /* Background only.  img is modified in place (background subtracted).
@@ -125,7 +126,8 @@ void orc_filter(const float *sub, int w, int h, const float *mask, int mw, int m
                 float *cd);
 
 /* Full extraction.  img (w*h) is the raw frame and is left unchanged; var
- * (w*h, may be NULL) is the variance map for weight_type MAP_VAR.
+ * (w*h, may be NULL) is the weight map of weight_type (variance, rms or
+ * weight values).
  * out_objects receives up to max_objects rows; segmap (w*h int32, may be NULL)
  * receives NUMBER per pixel (0 = sky).  Returns the number of rows or <0. */
 int orc_extract(const float *img, const float *var, int w, int h, const orc_config *cfg,

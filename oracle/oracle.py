@@ -54,6 +54,7 @@ class OrcSummary(C.Structure):
         ("nbackx", C.c_int), ("nbacky", C.c_int), ("backmean", C.c_float), ("backsig", C.c_float),
         ("dthresh", C.c_float), ("thresh", C.c_float), ("npix_above", C.c_int64),
         ("nraw", C.c_int32), ("nraw_pix", C.c_int64), ("ndetected", C.c_int32), ("nobj", C.c_int32),
+        ("sigfac", C.c_float),
     ]
 
 
@@ -149,10 +150,12 @@ def filter_image(sub, mask):
     return cd
 
 
-def extract(img, max_objects=None, want_maps=False, **kw):
-    """Full extraction; returns (objects structured array, segmap, summary[, sub, cd])."""
+def extract(img, max_objects=None, want_maps=False, weight=None, **kw):
+    """Full extraction; returns (objects structured array, segmap, summary[, sub, cd]).
+    weight: the weight map of weight_type (1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT)."""
     cfg = make_config(**kw)
     img = np.ascontiguousarray(img, np.float32)
+    wmap = np.ascontiguousarray(weight, np.float32) if weight is not None else None
     h, w = img.shape
     if max_objects is None:
         max_objects = w * h // max(1, cfg.detect_minarea) // 2 + 16
@@ -161,7 +164,8 @@ def extract(img, max_objects=None, want_maps=False, **kw):
     s = OrcSummary()
     sub = np.zeros_like(img) if want_maps else None
     cd = np.zeros_like(img) if want_maps else None
-    n = lib().orc_extract(_f(img), None, w, h, C.byref(cfg), objs.ctypes.data_as(C.c_void_p),
+    n = lib().orc_extract(_f(img), _f(wmap) if wmap is not None else None, w, h, C.byref(cfg),
+                          objs.ctypes.data_as(C.c_void_p),
                           max_objects, seg.ctypes.data_as(C.c_void_p),
                           _f(sub) if want_maps else None, _f(cd) if want_maps else None,
                           C.byref(s))

@@ -75,6 +75,7 @@ typedef struct {
     xsum_t fdflux;
     int firstpix;   /* smallest index */
     int lastrow_x;  /* x of the first pixel on row ymax */
+    float dthresh, thresh;  /* smallest detection / analysis threshold of its pixels */
 } root_t;
 
 typedef struct {
@@ -88,6 +89,7 @@ typedef struct {
 typedef struct {
     int root, level;
     float node_dthresh;
+    float dthr, athr;      /* the raw object's detection / analysis thresholds */
     int nnode;             /* pixels of the branch at its own level */
     int *nodepix;
     int n;                 /* final pixels (raster order) */
@@ -118,7 +120,24 @@ typedef struct {
     const float *back;
     int nbx, nby, bw, bh;
     int minarea, debminarea;
+    /* weight map: calibrated variance per pixel (ORC_BIGF where unusable),
+     * NULL without one; wthr: thresholds follow the local rms */
+    const float *var;
+    int wthr;
 } frame_t;
+
+/* Pixel thresholds with a weight map (SExtractor manual, weight maps: a
+ * relative threshold is taken against the local rms): DETECT_THRESH (or
+ * ANALYSIS_THRESH) x sqrt(variance); the global value otherwise. */
+static inline int pix_bad(const frame_t *F, size_t p) { return F->var && !(F->var[p] < ORC_BIGF); }
+static inline float pix_dthr(const frame_t *F, size_t p)
+{
+    return F->wthr ? (float)(F->cfg->detect_thresh * sqrt((double)F->var[p])) : F->dthresh;
+}
+static inline float pix_athr(const frame_t *F, size_t p)
+{
+    return F->wthr ? (float)(F->cfg->analysis_thresh * sqrt((double)F->var[p])) : F->thresh;
+}
 
 /* ------------------------------------------------------------------------ */
 /* Branch CCL inside one root at threshold t: labels lab[k] (index into the
@@ -307,9 +326,9 @@ static int deblend_root(const frame_t *F, int r, root_t *R, obj_t **objs, int *n
 
     /* multi-thresholds, cudadeblend.cu:199-217 */
     thr = (float *)malloc(sizeof(float) * (N + 1));
-    thr[0] = F->dthresh;
+    thr[0] = R->dthresh;
     for (i = 1; i < N; i++) {
-        double d0 = F->dthresh, dp = R->fdpeak;
+        double d0 = R->dthresh, dp = R->fdpeak;
         thr[i] = d0 * pow(dp / d0, (double)i / N);
     }
 
@@ -320,7 +339,7 @@ static int deblend_root(const frame_t *F, int r, root_t *R, obj_t **objs, int *n
     nodes[0].label = 0;
     nodes[0].npix = R->n;
     nodes[0].fdflux = fdflux0;
-    nodes[0].dthresh = F->dthresh;
+    nodes[0].dthresh = R->dthresh;
     nodes[0].parent = -1;
     nnodes = 1;
     lvstart[0] = 0;
@@ -424,6 +443,8 @@ static int deblend_root(const frame_t *F, int r, root_t *R, obj_t **objs, int *n
             o->root = r;
             o->level = L;
             o->node_dthresh = nodes[k].dthresh;
+            o->dthr = R->dthresh;
+            o->athr = R->thresh;
             o->nodepix = (int *)malloc(sizeof(int) * nodes[k].npix);
             for (j = 0; j < R->n; j++)
                 if (lab[j] == nodes[k].label) {
@@ -498,7 +519,7 @@ static void examineiso(const frame_t *F, obj_t *o)
     float peak = -ORC_BIG, cdpeak = -ORC_BIG, pix, cdpix;
     float threshs[ORC_NISO];
     float *heap = NULL;
-    xsum_t stv;
+    xsum_t stv, svar;
 
     o->bkg = orc_back_at(F->back, F->nbx, F->nby, F->bw, F->bh, (int)(o->mx + 0.5), (int)(o->my + 0.5));
     dbacknoise2 = F->backsig * F->backsig;
@@ -514,6 +535,7 @@ static void examineiso(const frame_t *F, obj_t *o)
     } else
         o->mthresh = 0.0;
     xs_init(&stv);
+    xs_init(&svar);
     o->peakx = o->peaky = 0;
     for (k = 0; k < o->n; k++) {
         int p = o->pix[k], ix = p % w, iy = p / w;
@@ -526,11 +548,13 @@ static void examineiso(const frame_t *F, obj_t *o)
             o->peakx = ix + 1;
             o->peaky = iy + 1;
         }
-        if (pix > F->thresh)
+        if (pix > pix_athr(F, p))
             area++;
         xs_add(&stv, pix);
+        if (F->var)
+            xs_add(&svar, F->var[p]);
         if (errflag) {
-            err = dbacknoise2;
+            err = F->var ? (double)F->var[p] : dbacknoise2;
             if (cfg->gain > 0.0 && cdpix > 0.0)
                 err += cdpix / cfg->gain;
             x = ix - xm;
@@ -541,7 +565,7 @@ static void examineiso(const frame_t *F, obj_t *o)
             emxy += err * x * y;
         }
         if (cleanflag)
-            heap[k] = cdpix - F->dthresh;
+            heap[k] = cdpix - o->dthr;
     }
     /* mthresh: the minarea-th largest (cd - dthresh), the value the reference
      * heap of src/cuda/cudaanalyse.cu:2331-2365 intends to select */
@@ -564,15 +588,16 @@ static void examineiso(const frame_t *F, obj_t *o)
         o->poserr_my2 = emy2;
         o->poserr_mxy = emxy;
     }
-    /* sigtv accumulates the constant var once per pixel (exact n*var) */
-    sigtv = (double)o->n * var;
+    /* sigtv accumulates the constant var once per pixel (exact n*var); with a
+     * weight map, the pixels' variances (an exact sum) */
+    sigtv = F->var ? xs_double(&svar) : (double)o->n * var;
     tvd = xs_double(&stv);
     if (cfg->gain > 0.0 && tvd > 0.0)
         sigtv += tvd / cfg->gain;
     o->npix = area;
     o->flux = tvd;
     o->fluxerr = sigtv;
-    o->thresh = F->thresh - 0.0f;
+    o->thresh = o->athr - 0.0f;
     o->peak = peak - 0.0f;
     if (o->peak > 0.0 && o->thresh > 0.0)
         for (i = 0; i < ORC_NISO; i++)
@@ -697,7 +722,7 @@ static void run_clean(const frame_t *F, obj_t *o, int n)
     for (i = 0; i < n; i++) {
         double unitarea = ORC_PI * o[i].a * o[i].b, q;
         amp[i] = o[i].fdflux / (2 * unitarea * o[i].abcor);
-        q = amp[i] / F->dthresh;
+        q = amp[i] / o[i].dthr;
         alpha[i] = ((beta == 1.0 ? q : pow(q, 1.0 / beta)) - 1) * unitarea / o[i].fdnpix;
         master[i] = -1;
     }
@@ -767,7 +792,7 @@ static void aperflux(const frame_t *F, const int *alloc, obj_t *o, int self)
 {
     const orc_config *cfg = F->cfg;
     float r2, raper, raper2, rintlim, rintlim2, rextlim2, dx, dx1, dy, dy2, offsetx, offsety, scalex, scaley, scale2, locarea;
-    double tv, sigtv, area, pix, var;
+    double tv, sigtv, area, pix, var, pvar;
     int x, y, x2, y2, xmin, xmax, ymin, ymax, sx, sy, corrflag, w = F->w, h = F->h, t;
 
     corrflag = (cfg->mask_type == 2);
@@ -811,16 +836,24 @@ static void aperflux(const frame_t *F, const int *alloc, obj_t *o, int self)
                 area += locarea;
                 pix = F->sub[(size_t)y * w + x];
                 t = alloc[(size_t)y * w + x];
+                /* with a weight map the variance of the pixel actually used,
+                 * 0 for a pixel replaced by 0 (src/photom.c:128-145) */
+                pvar = F->var ? (double)F->var[(size_t)y * w + x] : var;
                 if ((t >= 0 && t != self) || pix <= -ORC_BIG) {
                     if (corrflag && (x2 = (int)(2 * o->mx + 0.49999 - x)) >= 0 && x2 < w
                         && (y2 = (int)(2 * o->my + 0.49999 - y)) >= 0 && y2 < h
                         && ((t = alloc[(size_t)y2 * w + x2]) == self || t == -1)
-                        && F->sub[(size_t)y2 * w + x2] > -ORC_BIG)
+                        && F->sub[(size_t)y2 * w + x2] > -ORC_BIG) {
                         pix = F->sub[(size_t)y2 * w + x2];
-                    else
+                        if (F->var)
+                            pvar = F->var[(size_t)y2 * w + x2];
+                    } else {
                         pix = 0.0;
+                        if (F->var)
+                            pvar = 0.0;
+                    }
                 }
-                sigtv += var * locarea;
+                sigtv += pvar * locarea;
                 tv += locarea * pix;
             }
         }
@@ -845,7 +878,7 @@ static void autoflux(const frame_t *F, const int *alloc, obj_t *o, int self)
     double sigtv, tv, r1, v1, var;
     float dx, dy, cx2, cy2, cxy, r2, klim2, dxlim, dylim, pix;
     int area, areab, x, y, x2, y2, xmin, xmax, ymin, ymax, corrflag, t, w = F->w, h = F->h;
-    xsum_t sr1, sv1, stv;
+    xsum_t sr1, sv1, stv, svar;
     const double autoaper0 = 0.0, autoaper1 = 0.0;
 
     var = F->backsig * F->backsig;
@@ -921,31 +954,40 @@ static void autoflux(const frame_t *F, const int *alloc, obj_t *o, int self)
         if ((ymax = RINT(o->my + dylim) + 1) > h) { ymax = h; o->flags |= ORC_OBJ_APERT_PB; }
         area = areab = 0;
         xs_init(&stv);
+        xs_init(&svar);
         for (y = ymin; y < ymax; y++)
             for (x = xmin; x < xmax; x++) {
                 dx = x - o->mx;
                 dy = y - o->my;
                 if ((cx2 * dx * dx + cy2 * dy * dy + cxy * dx * dy) <= klim2) {
+                    float pvar;
                     area++;
                     pix = F->sub[(size_t)y * w + x];
                     t = alloc[(size_t)y * w + x];
+                    pvar = F->var ? F->var[(size_t)y * w + x] : 0.0f;
                     if ((t >= 0 && t != self) || pix <= -ORC_BIG) {
                         areab++;
                         if (corrflag && (x2 = (int)(2 * o->mx + 0.49999 - x)) >= 0 && x2 < w
                             && (y2 = (int)(2 * o->my + 0.49999 - y)) >= 0 && y2 < h
                             && ((t = alloc[(size_t)y2 * w + x2]) == -1 || t == self)
-                            && F->sub[(size_t)y2 * w + x2] > -ORC_BIG)
+                            && F->sub[(size_t)y2 * w + x2] > -ORC_BIG) {
                             pix = F->sub[(size_t)y2 * w + x2];
-                        else
+                            if (F->var)
+                                pvar = F->var[(size_t)y2 * w + x2];
+                        } else {
                             pix = 0.0;
+                            pvar = 0.0f;
+                        }
                     }
                     xs_add(&stv, pix);
+                    if (F->var)
+                        xs_add(&svar, pvar);
                 }
             }
         if ((float)areab > ORC_CROWD_THRESHOLD * area)
             o->flags |= ORC_OBJ_CROWDED;
         tv = xs_double(&stv);
-        sigtv = (double)area * var;
+        sigtv = F->var ? xs_double(&svar) : (double)area * var;
         tv -= area * (double)0.0f;
         if (cfg->gain > 0.0 && tv > 0.0)
             sigtv += tv / cfg->gain;
@@ -969,7 +1011,7 @@ static void endobject(const frame_t *F, const int *alloc, obj_t *o, int self)
     o->polar = (o->a * o->a - o->b * o->b) / (o->a * o->a + o->b * o->b);
     o->fluxerr_iso = sqrt(o->fluxerr);
     /* computeisocorflux, :62-98 */
-    ati = (o->flux > 0.0) ? (o->fdnpix * F->dthresh / o->flux) : 0.0;
+    ati = (o->flux > 0.0) ? (o->fdnpix * o->dthr / o->flux) : 0.0;
     if (ati > 1.0)
         ati = 1.0;
     else if (ati < 0.0)
@@ -1004,6 +1046,77 @@ static int cmp_okey(const void *a, const void *b)
     return (p->idx > q->idx) - (p->idx < q->idx);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Weight maps.  The reference keeps weight_to_var (src/weight.c:91-125) but
+ * no weighted background, threshold or measurement; this restates them after
+ * the SExtractor manual (weight maps): unusable pixels (variance or rms at or
+ * above BIG, weight at or below 0, NaN) are blank for the background and the
+ * detection; the relative map is scaled by sigfac^2 (MAP_VAR, MAP_WEIGHT) with
+ * sigfac the median over usable meshes of (mesh rms of the frame) /
+ * sqrt(mesh mean of the relative variance), or used as it is (MAP_RMS). */
+static float rel_var(float v, int wtype)
+{
+    float r;
+    if (wtype == 1)
+        r = v;
+    else if (wtype == 2)
+        r = v < ORC_BIGF ? v * v : ORC_BIGF;
+    else
+        r = v > 0.0f ? 1.0f / v : ORC_BIGF;
+    return r < ORC_BIGF ? r : ORC_BIGF;  /* NaN and overflow too */
+}
+
+/* src/weight.c:104-118 with the scale factor */
+static float calib_var(float v, int wtype, float sigfac2)
+{
+    float r;
+    if (wtype == 1)
+        r = v < ORC_BIGF ? v * sigfac2 : ORC_BIGF;
+    else if (wtype == 2)
+        r = v < ORC_BIGF ? v * v : ORC_BIGF;
+    else
+        r = v > 0.0f ? sigfac2 / v : ORC_BIGF;
+    return r < ORC_BIGF ? r : ORC_BIGF;
+}
+
+/* sigfac from the frame's filtered mesh rms map `sigma` */
+static float weight_sigfac(const float *wmap, int wtype, int w, int h, int bw, int bh, int nx, int ny,
+                           const float *sigma)
+{
+    float *ratio = (float *)malloc(sizeof(float) * nx * ny), f;
+    int nr = 0, mx, my, x, y;
+    if (wtype == 2) {
+        free(ratio);
+        return 1.0f;
+    }
+    for (my = 0; my < ny; my++) {
+        int mh = (my == ny - 1 && h % bh) ? h % bh : bh;
+        for (mx = 0; mx < nx; mx++) {
+            int mw = (mx == nx - 1 && w % bw) ? w % bw : bw, n = 0;
+            xsum_t sv;
+            double vmean;
+            float sm = sigma[my * nx + mx];
+            xs_init(&sv);
+            for (y = 0; y < mh; y++)
+                for (x = 0; x < mw; x++) {
+                    float r = rel_var(wmap[(size_t)(my * bh + y) * w + mx * bw + x], wtype);
+                    if (r < ORC_BIGF) {
+                        xs_add(&sv, r);
+                        n++;
+                    }
+                }
+            if ((float)n < (float)(mw * mh * ORC_BACK_MINGOODFRAC))
+                continue;
+            vmean = xs_double(&sv) / n;
+            if (vmean > 0.0 && sm > 0.0f)
+                ratio[nr++] = (float)(sm / sqrt(vmean));
+        }
+    }
+    f = nr ? orc_hmedian(ratio, nr) : 1.0f;
+    free(ratio);
+    return f;
+}
+
 int orc_extract(const float *img, const float *var, int w, int h, const orc_config *cfg,
                 orc_object *out, int max_objects, int32_t *segmap,
                 float *sub_out, float *cd_out, orc_summary *sum)
@@ -1014,20 +1127,40 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
     int *lab, *alloc;
     size_t N = (size_t)w * h, p;
     int nroots = 0, r, i, k, nobj = 0, cap = 1024, nout = 0;
+    float *wvar;
     root_t *roots;
     int *rootid;
     obj_t *objs;
     (void)var;
 
     memset(&S, 0, sizeof(S));
+    S.sigfac = 1.0f;
     sub = (float *)malloc(sizeof(float) * N);
     cd = (float *)malloc(sizeof(float) * N);
     memcpy(sub, img, sizeof(float) * N);
+    wvar = NULL;
+    if (var && cfg->weight_type >= 1 && cfg->weight_type <= 3) {
+        /* unusable weight: a blank pixel */
+        for (p = 0; p < N; p++)
+            if (!(rel_var(var[p], cfg->weight_type) < ORC_BIGF))
+                sub[p] = -ORC_BIGF;
+    } else
+        var = NULL;
     {
         int bw = cfg->back_size < w ? cfg->back_size : w, bh = cfg->back_size < h ? cfg->back_size : h;
         int nbx = (w - 1) / bw + 1, nby = (h - 1) / bh + 1;
+        float *sig = (float *)malloc(sizeof(float) * nbx * nby);
         back = (float *)malloc(sizeof(float) * nbx * nby);
-        orc_background(sub, w, h, cfg, back, NULL, NULL, NULL, &S);
+        orc_background(sub, w, h, cfg, back, sig, NULL, NULL, &S);
+        if (var) {
+            float sigfac2;
+            S.sigfac = weight_sigfac(var, cfg->weight_type, w, h, bw, bh, nbx, nby, sig);
+            sigfac2 = S.sigfac * S.sigfac;
+            wvar = (float *)malloc(sizeof(float) * N);
+            for (p = 0; p < N; p++)
+                wvar[p] = calib_var(var[p], cfg->weight_type, sigfac2);
+        }
+        free(sig);
         F.nbx = nbx;
         F.nby = nby;
         F.bw = bw;
@@ -1048,11 +1181,13 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
     F.back = back;
     F.minarea = cfg->detect_minarea;
     F.debminarea = cfg->detect_minarea < ORC_MAXDEBAREA ? cfg->detect_minarea : ORC_MAXDEBAREA;
+    F.var = wvar;
+    F.wthr = wvar != NULL && cfg->thresh_type != 1;
 
     /* thresholding + 8-connected components, src/cuda/cudadetection.cu:36-276 */
     lab = (int *)malloc(sizeof(int) * N);
     for (p = 0; p < N; p++)
-        lab[p] = (cd[p] >= F.dthresh) ? (int)p : -1;
+        lab[p] = (!pix_bad(&F, p) && cd[p] >= pix_dthr(&F, p)) ? (int)p : -1;
     for (p = 0; p < N; p++) {
         int x = p % w, y = p / w;
         if (lab[p] < 0)
@@ -1090,6 +1225,7 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
                 R->ymin = h;
                 R->xmax = R->ymax = -1;
                 R->fdpeak = -ORC_BIG;
+                R->dthresh = R->thresh = ORC_BIGF;
                 xs_init(&R->fdflux);
             }
         for (p = 0; p < N; p++)
@@ -1103,6 +1239,8 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
                 if (y > R->ymax) { R->ymax = y; R->lastrow_x = x; }
                 if (cd[p] > R->fdpeak) R->fdpeak = cd[p];
                 xs_add(&R->fdflux, cd[p]);
+                if (pix_dthr(&F, p) < R->dthresh) R->dthresh = pix_dthr(&F, p);
+                if (pix_athr(&F, p) < R->thresh) R->thresh = pix_athr(&F, p);
             }
         for (p = 0; p < N; p++)
             rootid[p] = (lab[p] >= 0) ? rootid[lab[p]] : -1;
@@ -1122,7 +1260,7 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
     for (i = 0; i < nobj; i++) {
         obj_t *o = &objs[i];
         if (o->level > 0)
-            preanalyse(&F, o, o->pix, o->n, F.dthresh, 1);
+            preanalyse(&F, o, o->pix, o->n, o->dthr, 1);
         o->fdnpix = o->n;
         o->master = o->final_master = -1;
         examineiso(&F, o);
@@ -1134,7 +1272,7 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
      * threshold pixels outside every object, -1 elsewhere */
     alloc = (int *)malloc(sizeof(int) * N);
     for (p = 0; p < N; p++)
-        alloc[p] = (cd[p] >= F.dthresh) ? ALLOC_OTHER : -1;
+        alloc[p] = (!pix_bad(&F, p) && cd[p] >= pix_dthr(&F, p)) ? ALLOC_OTHER : -1;
     for (i = 0; i < nobj; i++) {
         int m = objs[i].final_master >= 0 ? objs[i].final_master : i;
         for (k = 0; k < objs[i].n; k++)
@@ -1181,7 +1319,7 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
             q->a = o->a; q->b = o->b; q->theta = o->theta; q->abcor = o->abcor;
             q->cxx = o->cxx; q->cyy = o->cyy; q->cxy = o->cxy;
             q->poserr_mx2 = o->poserr_mx2; q->poserr_my2 = o->poserr_my2; q->poserr_mxy = o->poserr_mxy;
-            q->bkg = o->bkg; q->thresh = o->thresh; q->dthresh = F.dthresh; q->mthresh = o->mthresh;
+            q->bkg = o->bkg; q->thresh = o->thresh; q->dthresh = o->dthr; q->mthresh = o->mthresh;
             q->fwhm = o->fwhm;
             q->flux_iso = o->flux; q->fluxerr_iso = o->fluxerr_iso; q->mag_iso = o->mag_iso; q->magerr_iso = o->magerr_iso;
             q->flux_isocor = o->flux_isocor; q->fluxerr_isocor = o->fluxerr_isocor;
@@ -1213,7 +1351,7 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
     }
     for (r = 0; r < nroots; r++)
         free(roots[r].pix);
-    free(objs); free(roots); free(rootid); free(lab); free(alloc); free(sub); free(cd); free(back);
+    free(objs); free(roots); free(rootid); free(lab); free(alloc); free(sub); free(cd); free(back); free(wvar);
     return nout;
 }
 

@@ -30,3 +30,11 @@ def test_batch_reports_bad_frame(gpu_ctx):
     img = synth.frame_c0(seed=47, w=300, h=200, nsrc=50)
     with pytest.raises(RuntimeError):
         gpu_ctx.extract_batch([(img, dict()), (img, dict(deblend_nthresh=0))], workers=2)
+
+
+def test_batch_with_weight_map(gpu_ctx, masks):
+    img, vm = synth.frame_c1(seed=48, w=640, h=480, density=8e-3, var=True)
+    kw = dict(weight_type=1, back_size=64, conv=masks["gauss_2.5_5x5"])
+    (cat, summ), = gpu_ctx.extract_batch([(img, kw, vm)], workers=1)
+    ref, _, s = gpu_ctx.extract(img, weight=vm, **kw)
+    assert cat.tobytes() == ref.tobytes() and summ.sigfac == s.sigfac

@@ -165,3 +165,30 @@ def test_full_size_c1(gpu_ctx, masks):
     img = synth.frame_c1(seed=1000)
     g = run_both(gpu_ctx, img, conv=masks["gauss_2.5_5x5"])
     assert len(g) > 50000
+
+
+@pytest.mark.parametrize("wtype", [1, 2, 3])
+def test_weight_maps(gpu_ctx, masks, wtype):
+    """WEIGHT_TYPE MAP_VAR / MAP_RMS / MAP_WEIGHT: variance 1.0 +- 20% (x64),
+    2% of the pixels unusable in 8x8 blocks; per-pixel thresholds against the
+    local rms, per-object thresholds, variance-weighted errors."""
+    img, vm = synth.frame_c1(seed=4001, w=768, h=640, density=9e-3, var=True)
+    wmap = {1: vm, 2: np.sqrt(vm), 3: np.where(vm < 1e29, 1.0 / vm, 0.0).astype(np.float32)}[wtype]
+    kw = dict(conv=masks["gauss_4.0_7x7"], back_size=128, weight_type=wtype)
+    g, gseg, gs = gpu_ctx.extract(img, weight=wmap, **kw)
+    o, oseg, os_ = O.extract(img, weight=wmap, **kw)
+    assert gs.sigfac == os_.sigfac
+    assert (gs.nraw, gs.nraw_pix, gs.ndetected, gs.nobj) == (os_.nraw, os_.nraw_pix, os_.ndetected, os_.nobj)
+    assert gs.npix_above == os_.npix_above
+    assert np.array_equal(gseg, oseg)
+    compare_catalogs(g, o)
+    assert len(g) > 100 and g["dthresh"].min() < g["dthresh"].max()
+
+
+def test_weight_map_absolute_thresholds(gpu_ctx, masks):
+    img, vm = synth.frame_c1(seed=4002, w=512, h=512, density=8e-3, var=True)
+    kw = dict(conv=masks["gauss_2.5_5x5"], weight_type=1, thresh_type=1, detect_thresh=30.0, analysis_thresh=30.0)
+    g, gseg, gs = gpu_ctx.extract(img, weight=vm, **kw)
+    o, oseg, os_ = O.extract(img, weight=vm, **kw)
+    assert np.array_equal(gseg, oseg)
+    compare_catalogs(g, o)
