@@ -365,6 +365,7 @@ struct FrameScalars {
     int nobj;                       // objects after deblending
     int nsurv;                      // after CLEAN
     int e0sub;                      // smallest exponent of a non-zero |sub|
+    int kitems[2], kchunks[2];      // queued Kron boxes and their work items (pass 1, 2)
     unsigned long long levpix;      // sum of the deblending level of every raw-object pixel
 };
 

@@ -178,6 +178,7 @@ struct EndArgs {
     int w, h, n, mask_type;
     double aperture, autoparam0, autoparam1, gain, zp, satur;
     const float *wvar;  // calibrated variance map, or null
+    KronBufs K;         // queued Kron boxes
 };
 
 // src/cuda/cudaanalyse.cu:104-287 (computeaperflux, one aperture).  The
@@ -292,173 +293,214 @@ __device__ __forceinline__ int wsum(int v) {
     return v;
 }
 
-// one warp per surviving object
-__global__ void k_endobject(EndArgs A) {
-    const int lane = threadIdx.x & 31;
-    const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (o >= A.n) return;
-    if (A.O.fmaster[o] >= 0) return;
-    const int w = A.w, h = A.h;
-    int flags = A.O.flags[o];
-    float a = A.O.a[o], b = A.O.b[o];
-    double mx = A.O.mx[o], my = A.O.my[o];
-    float flux = A.O.flux[o], fluxerr = A.O.fluxerr[o], dthresh = A.O.dthr[o], backsig = A.sc->backsig;
-    int fdnpix = A.O.fdnpix[o];
-    aper_warp(A, o, mx, my, flags);
-    // AUTO / Kron, src/cuda/cudaanalyse.cu:293-592
-    double var = backsig * backsig;
-    int corrflag = (A.mask_type == 2);
-    float dx, dy, cx2, cy2, cxy, r2, klim2, dxlim, dylim, pix, kron = 0.0f;
-    int xmin, xmax, ymin, ymax, area, areab;
-    const double autoaper0 = 0.0, autoaper1 = 0.0;
-    float cxx = A.O.cxx[o], cyy = A.O.cyy[o], cxyo = A.O.cxy[o];
+// ---------------------------------------------------------------------------
+// AUTO / Kron photometry, src/cuda/cudaanalyse.cu:293-592.  Pass 1 sums
+// r*pix and pix over the 6-sigma ellipse (kron radius), pass 2 the flux inside
+// kron*ellipse.  Both sums are exact, so a box may be split freely: a warp
+// takes the boxes of up to KronBufs::warp_max pixels; larger ones (a kron
+// radius that grew over a faint, elongated object can span the frame) are
+// queued and cut into KR_CHUNK-pixel work items for whole CTAs, whose
+// partial sums a warp per object merges afterwards.
+// ---------------------------------------------------------------------------
+struct KronAcc {
+    XSum s0, s1;  // pass 1: r*pix, pix;  pass 2: pix, variance
+    int area, areab;
+};
+
+__device__ __forceinline__ void kacc_init(KronAcc &c) {
+    xs_init(c.s0);
+    xs_init(c.s1);
+    c.area = c.areab = 0;
+}
+
+__device__ __forceinline__ void kacc_merge(KronAcc &c, const KronAcc &b) {
+    xs_merge(c.s0, b.s0);
+    xs_merge(c.s1, b.s1);
+    c.area += b.area;
+    c.areab += b.areab;
+}
+
+__device__ __forceinline__ void kacc_warp(KronAcc &c) {
+    c.s0 = xs_warp_all2(c.s0);
+    c.s1 = xs_warp_all2(c.s1);
+    c.area = wsum(c.area);
+    c.areab = wsum(c.areab);
+}
+
+__device__ __forceinline__ void kron_box(const EndArgs &A, double mx, double my, float dxlim, float dylim, KronGeo &g,
+                                         int &flags) {
+    if ((g.xmin = SX_RINT(mx - dxlim)) < 0) {
+        g.xmin = 0;
+        flags |= SX_OBJ_APERT_PB;
+    }
+    if ((g.xmax = SX_RINT(mx + dxlim) + 1) > A.w) {
+        g.xmax = A.w;
+        flags |= SX_OBJ_APERT_PB;
+    }
+    if ((g.ymin = SX_RINT(my - dylim)) < 0) {
+        g.ymin = 0;
+        flags |= SX_OBJ_APERT_PB;
+    }
+    if ((g.ymax = SX_RINT(my + dylim) + 1) > A.h) {
+        g.ymax = A.h;
+        flags |= SX_OBJ_APERT_PB;
+    }
+}
+
+// pass-1 ellipse and box (cudaanalyse.cu:318-357)
+__device__ __forceinline__ void kron_geo1(const EndArgs &A, int o, double mx, double my, KronGeo &g, int &flags) {
+    const double autoaper0 = 0.0;
+    const float a = A.O.a[o], b = A.O.b[o];
+    float dxlim, dylim;
     if (SX_KRON_NSIG * sqrtf(a * b) > autoaper0 / 2.0) {
-        cx2 = cxx;
-        cy2 = cyy;
-        cxy = cxyo;
-        dxlim = cx2 - cxy * cxy / (4.0 * cy2);
+        g.cx2 = A.O.cxx[o];
+        g.cy2 = A.O.cyy[o];
+        g.cxy = A.O.cxy[o];
+        dxlim = g.cx2 - g.cxy * g.cxy / (4.0 * g.cy2);
         dxlim = dxlim > 0.0 ? SX_KRON_NSIG / sqrtf(dxlim) : 0.0;
-        dylim = cy2 - cxy * cxy / (4.0 * cx2);
+        dylim = g.cy2 - g.cxy * g.cxy / (4.0 * g.cx2);
         dylim = dylim > 0.0 ? SX_KRON_NSIG / sqrtf(dylim) : 0.0;
-        klim2 = SX_KRON_NSIG * SX_KRON_NSIG;
+        g.klim2 = SX_KRON_NSIG * SX_KRON_NSIG;
     } else {
-        cx2 = cy2 = 1.0;
-        cxy = 0.0;
+        g.cx2 = g.cy2 = 1.0;
+        g.cxy = 0.0;
         dxlim = dylim = autoaper0 / 2.0;
-        klim2 = dxlim * dxlim;
+        g.klim2 = dxlim * dxlim;
     }
-    if ((xmin = SX_RINT(mx - dxlim)) < 0) {
-        xmin = 0;
-        flags |= SX_OBJ_APERT_PB;
+    kron_box(A, mx, my, dxlim, dylim, g, flags);
+}
+
+// kron radius from pass 1 and the pass-2 ellipse and box (cudaanalyse.cu:
+// 385-440); false when pass 1 found no pixel (no AUTO flux)
+__device__ __forceinline__ bool kron_geo2(const EndArgs &A, int o, double mx, double my, const KronAcc &p, float &kron,
+                                          KronGeo &g, int &flags) {
+    const double autoaper1 = 0.0;
+    const int areab = p.areab, area = p.area + p.areab;
+    if (!area) return false;
+    const double r1 = xs_double(p.s0), v1 = xs_double(p.s1);
+    if (r1 > 0.0 && v1 > 0.0) {
+        kron = A.autoparam0 * r1 / v1;
+        if (kron < A.autoparam1) kron = A.autoparam1;
+    } else
+        kron = A.autoparam1;
+    if ((float)areab / area > SX_CROWD_THRESHOLD) flags |= SX_OBJ_CROWDED;
+    const float a = A.O.a[o], b = A.O.b[o];
+    float dxlim, dylim;
+    if (kron * sqrtf(a * b) > autoaper1 / 2.0) {
+        g.cx2 = A.O.cxx[o];
+        g.cy2 = A.O.cyy[o];
+        g.cxy = A.O.cxy[o];
+        dxlim = g.cx2 - g.cxy * g.cxy / (4.0 * g.cy2);
+        dxlim = dxlim > 0.0 ? kron / sqrtf(dxlim) : 0.0;
+        dylim = g.cy2 - g.cxy * g.cxy / (4.0 * g.cx2);
+        dylim = dylim > 0.0 ? kron / sqrtf(dylim) : 0.0;
+        g.klim2 = kron * kron;
+    } else {
+        g.cx2 = g.cy2 = 1.0;
+        g.cxy = 0.0;
+        dxlim = dylim = autoaper1 / 2.0;
+        g.klim2 = dxlim * dxlim;
+        kron = 0.0;
     }
-    if ((xmax = SX_RINT(mx + dxlim) + 1) > w) {
-        xmax = w;
-        flags |= SX_OBJ_APERT_PB;
-    }
-    if ((ymin = SX_RINT(my - dylim)) < 0) {
-        ymin = 0;
-        flags |= SX_OBJ_APERT_PB;
-    }
-    if ((ymax = SX_RINT(my + dylim) + 1) > h) {
-        ymax = h;
-        flags |= SX_OBJ_APERT_PB;
-    }
-    XSum sr1, sv1;
-    xs_init(sr1);
-    xs_init(sv1);
-    area = areab = 0;
-    {
-        int bw = xmax - xmin, nn = bw * (ymax - ymin);
-        const FastDiv bd = make_fastdiv_dev((unsigned)bw);
-        for (int i = lane; i < nn; i += 32) {
-            int yo = (int)fdiv((unsigned)i, bd), x = xmin + (i - yo * bw), y = ymin + yo;
-            dx = x - mx;
-            dy = y - my;
-            if ((r2 = cx2 * dx * dx + cy2 * dy * dy + cxy * dx * dy) <= klim2) {
-                pix = A.sub[(size_t)y * w + x];
-                int t = A.alloc[(size_t)y * w + x];
+    kron_box(A, mx, my, dxlim, dylim, g, flags);
+    return true;
+}
+
+__device__ __forceinline__ int kron_npix(const KronGeo &g) { return (g.xmax - g.xmin) * (g.ymax - g.ymin); }
+
+// box pixels i0, i0+step, ... below i1 (raster index inside the box)
+template <int PASS>
+__device__ __forceinline__ void kron_range(const EndArgs &A, int o, double mx, double my, const KronGeo &g, int i0,
+                                           int i1, int step, KronAcc &c) {
+    const int w = A.w, h = A.h, bw = g.xmax - g.xmin;
+    const FastDiv bd = make_fastdiv_dev((unsigned)bw);
+    const int corrflag = (A.mask_type == 2);
+    for (int i = i0; i < i1; i += step) {
+        const int yo = (int)fdiv((unsigned)i, bd), x = g.xmin + (i - yo * bw), y = g.ymin + yo;
+        const float dx = x - mx, dy = y - my;
+        if (PASS == 1) {
+            float r2;
+            if ((r2 = g.cx2 * dx * dx + g.cy2 * dy * dy + g.cxy * dx * dy) <= g.klim2) {
+                const float pix = A.sub[(size_t)y * w + x];
+                const int t = A.alloc[(size_t)y * w + x];
                 if ((t == o || t == -1) & (pix > -SX_BIG)) {
-                    area++;
-                    xs_add(sr1, sqrtf(r2) * pix);
-                    xs_add(sv1, pix);
+                    c.area++;
+                    xs_add(c.s0, sqrtf(r2) * pix);
+                    xs_add(c.s1, pix);
                 } else
-                    areab++;
+                    c.areab++;
             }
+        } else if ((g.cx2 * dx * dx + g.cy2 * dy * dy + g.cxy * dx * dy) <= g.klim2) {
+            c.area++;
+            float pix = A.sub[(size_t)y * w + x];
+            int t = A.alloc[(size_t)y * w + x];
+            float pvar = A.wvar ? A.wvar[(size_t)y * w + x] : 0.0f;
+            if ((t >= 0 && t != o) || pix <= -SX_BIG) {
+                c.areab++;
+                int x2, y2;
+                if (corrflag && (x2 = (int)(2 * mx + 0.49999 - x)) >= 0 && x2 < w &&
+                    (y2 = (int)(2 * my + 0.49999 - y)) >= 0 && y2 < h &&
+                    ((t = A.alloc[(size_t)y2 * w + x2]) == -1 || t == o) && A.sub[(size_t)y2 * w + x2] > -SX_BIG) {
+                    pix = A.sub[(size_t)y2 * w + x2];
+                    if (A.wvar) pvar = A.wvar[(size_t)y2 * w + x2];
+                } else {
+                    pix = 0.0;
+                    pvar = 0.0f;
+                }
+            }
+            xs_add(c.s0, pix);
+            if (A.wvar) xs_add(c.s1, pvar);
         }
     }
-    sr1 = xs_warp_all2(sr1);
-    sv1 = xs_warp_all2(sv1);
-    area = wsum(area);
-    areab = wsum(areab);
-    area += areab;
+}
+
+// Queue object o's pass-`pass` box (warp-collective).  False when the queue is
+// full; the warp then sums the box itself.
+__device__ bool kron_defer(const EndArgs &A, int pass, int o, int flags, float kron, const KronGeo &g, int nn) {
+    const int lane = threadIdx.x & 31;
+    const int nch = (nn + KR_CHUNK - 1) / KR_CHUNK;
+    int k = 0, c0 = 0;
+    if (lane == 0) {
+        k = atomicAdd(&A.sc->kitems[pass], 1);
+        c0 = atomicAdd(&A.sc->kchunks[pass], nch);
+    }
+    k = __shfl_sync(0xffffffffu, k, 0);
+    c0 = __shfl_sync(0xffffffffu, c0, 0);
+    const bool ok = k < A.K.icap && c0 <= A.K.ccap - nch;
+    // this warp's chunk range: item index, or -1 where the item did not fit
+    const int cend = min(c0 + nch, A.K.ccap);
+    for (int c = c0 + lane; c < cend; c += 32) A.K.chunk[pass][c] = ok ? k : -1;
+    if (lane == 0 && k < A.K.icap) {
+        KronItem it;
+        it.o = o;
+        it.flags = flags;
+        it.c0 = c0;
+        it.nch = ok ? nch : -1;
+        it.kron = kron;
+        it.g = g;
+        A.K.item[pass][k] = it;
+    }
+    return ok;
+}
+
+// catalogue columns of a survivor (lane 0 writes); p2 = pass-2 sums if any
+__device__ void end_finish(const EndArgs &A, int o, int flags, float kron, bool have2, const KronAcc &p2) {
+    if ((threadIdx.x & 31) != 0) return;
+    const float backsig = A.sc->backsig;
+    const double var = backsig * backsig;
     double tv, sigtv;
-    double r1 = xs_double(sr1), v1 = xs_double(sv1);
-    if (area) {
-        if (r1 > 0.0 && v1 > 0.0) {
-            kron = A.autoparam0 * r1 / v1;
-            if (kron < A.autoparam1) kron = A.autoparam1;
-        } else
-            kron = A.autoparam1;
-        if ((float)areab / area > SX_CROWD_THRESHOLD) flags |= SX_OBJ_CROWDED;
-        if (kron * sqrtf(a * b) > autoaper1 / 2.0) {
-            cx2 = cxx;
-            cy2 = cyy;
-            cxy = cxyo;
-            dxlim = cx2 - cxy * cxy / (4.0 * cy2);
-            dxlim = dxlim > 0.0 ? kron / sqrtf(dxlim) : 0.0;
-            dylim = cy2 - cxy * cxy / (4.0 * cx2);
-            dylim = dylim > 0.0 ? kron / sqrtf(dylim) : 0.0;
-            klim2 = kron * kron;
-        } else {
-            cx2 = cy2 = 1.0;
-            cxy = 0.0;
-            dxlim = dylim = autoaper1 / 2.0;
-            klim2 = dxlim * dxlim;
-            kron = 0.0;
-        }
-        if ((xmin = SX_RINT(mx - dxlim)) < 0) {
-            xmin = 0;
-            flags |= SX_OBJ_APERT_PB;
-        }
-        if ((xmax = SX_RINT(mx + dxlim) + 1) > w) {
-            xmax = w;
-            flags |= SX_OBJ_APERT_PB;
-        }
-        if ((ymin = SX_RINT(my - dylim)) < 0) {
-            ymin = 0;
-            flags |= SX_OBJ_APERT_PB;
-        }
-        if ((ymax = SX_RINT(my + dylim) + 1) > h) {
-            ymax = h;
-            flags |= SX_OBJ_APERT_PB;
-        }
-        area = areab = 0;
-        XSum stv, svar;
-        xs_init(stv);
-        xs_init(svar);
-        int bw = xmax - xmin, nn = bw * (ymax - ymin);
-        const FastDiv bd = make_fastdiv_dev((unsigned)bw);
-        for (int i = lane; i < nn; i += 32) {
-            int yo = (int)fdiv((unsigned)i, bd), x = xmin + (i - yo * bw), y = ymin + yo;
-            dx = x - mx;
-            dy = y - my;
-            if ((cx2 * dx * dx + cy2 * dy * dy + cxy * dx * dy) <= klim2) {
-                area++;
-                pix = A.sub[(size_t)y * w + x];
-                int t = A.alloc[(size_t)y * w + x];
-                float pvar = A.wvar ? A.wvar[(size_t)y * w + x] : 0.0f;
-                if ((t >= 0 && t != o) || pix <= -SX_BIG) {
-                    areab++;
-                    int x2, y2;
-                    if (corrflag && (x2 = (int)(2 * mx + 0.49999 - x)) >= 0 && x2 < w &&
-                        (y2 = (int)(2 * my + 0.49999 - y)) >= 0 && y2 < h &&
-                        ((t = A.alloc[(size_t)y2 * w + x2]) == -1 || t == o) &&
-                        A.sub[(size_t)y2 * w + x2] > -SX_BIG) {
-                        pix = A.sub[(size_t)y2 * w + x2];
-                        if (A.wvar) pvar = A.wvar[(size_t)y2 * w + x2];
-                    } else {
-                        pix = 0.0;
-                        pvar = 0.0f;
-                    }
-                }
-                xs_add(stv, pix);
-                if (A.wvar) xs_add(svar, pvar);
-            }
-        }
-        stv = xs_warp_all2(stv);
-        if (A.wvar) svar = xs_warp_all2(svar);
-        area = wsum(area);
-        areab = wsum(areab);
+    if (have2) {
+        const int area = p2.area, areab = p2.areab;
         if ((float)areab > SX_CROWD_THRESHOLD * area) flags |= SX_OBJ_CROWDED;
-        tv = xs_double(stv);
-        sigtv = A.wvar ? xs_double(svar) : (double)area * var;
+        tv = xs_double(p2.s0);
+        sigtv = A.wvar ? xs_double(p2.s1) : (double)area * var;
         tv -= area * (double)0.0f;
         if (A.gain > 0.0 && tv > 0.0) sigtv += tv / A.gain;
-        if ((stv.ovf | svar.ovf) && lane == 0) atomicOr(&A.sc->status, SX_ST_RANGE);
+        if (p2.s0.ovf | p2.s1.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
     } else
         tv = sigtv = 0.0;
-    if ((sr1.ovf | sv1.ovf) && lane == 0) atomicOr(&A.sc->status, SX_ST_RANGE);
-    if (lane != 0) return;
+    const float flux = A.O.flux[o], fluxerr = A.O.fluxerr[o], dthresh = A.O.dthr[o];
+    const int fdnpix = A.O.fdnpix[o];
     float flux_auto = tv, fluxerr_auto = sqrt(sigtv);
     if (tv <= 0.0) kron = 0.0;
     A.O.kron[o] = kron;
@@ -487,6 +529,102 @@ __global__ void k_endobject(EndArgs A) {
     A.O.magerr_iso[o] = flux > 0.0 ? 1.086 * fluxerr_iso / flux : 99.0;
     if (A.O.peak[o] + A.O.bkg[o] >= A.satur) flags |= SX_OBJ_SATUR;
     A.O.flags[o] = flags;
+}
+
+// after pass 1 (every lane holds its sums): pass 2 in this warp or queued
+__device__ void kron_after1(const EndArgs &A, int o, double mx, double my, int flags, const KronAcc &p1) {
+    if ((p1.s0.ovf | p1.s1.ovf) && (threadIdx.x & 31) == 0) atomicOr(&A.sc->status, SX_ST_RANGE);
+    float kron = 0.0f;
+    KronGeo g;
+    KronAcc p2;
+    kacc_init(p2);
+    if (!kron_geo2(A, o, mx, my, p1, kron, g, flags)) {
+        end_finish(A, o, flags, kron, false, p2);
+        return;
+    }
+    const int nn = kron_npix(g);
+    if (nn > A.K.warp_max && kron_defer(A, 1, o, flags, kron, g, nn)) return;
+    kron_range<2>(A, o, mx, my, g, threadIdx.x & 31, nn, 32, p2);
+    kacc_warp(p2);
+    end_finish(A, o, flags, kron, true, p2);
+}
+
+// one warp per surviving object
+__global__ void k_endobject(EndArgs A) {
+    const int lane = threadIdx.x & 31;
+    const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (o >= A.n) return;
+    if (A.O.fmaster[o] >= 0) return;
+    int flags = A.O.flags[o];
+    const double mx = A.O.mx[o], my = A.O.my[o];
+    aper_warp(A, o, mx, my, flags);
+    KronGeo g;
+    kron_geo1(A, o, mx, my, g, flags);
+    const int nn = kron_npix(g);
+    if (nn > A.K.warp_max && kron_defer(A, 0, o, flags, 0.0f, g, nn)) return;
+    KronAcc p1;
+    kacc_init(p1);
+    kron_range<1>(A, o, mx, my, g, lane, nn, 32, p1);
+    kacc_warp(p1);
+    kron_after1(A, o, mx, my, flags, p1);
+}
+
+// queued boxes: one CTA per KR_CHUNK-pixel work item, partial sums per item
+template <int PASS>
+__global__ void __launch_bounds__(KR_THREADS) k_kron_chunks(EndArgs A) {
+    __shared__ KronAcc red[KR_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nc = min(A.sc->kchunks[PASS - 1], A.K.ccap);
+    for (int c = blockIdx.x; c < nc; c += gridDim.x) {
+        const int k = A.K.chunk[PASS - 1][c];
+        if (k < 0) continue;
+        const KronItem it = A.K.item[PASS - 1][k];
+        const int i0 = (c - it.c0) * KR_CHUNK, i1 = min(kron_npix(it.g), i0 + KR_CHUNK);
+        KronAcc acc;
+        kacc_init(acc);
+        kron_range<PASS>(A, it.o, A.O.mx[it.o], A.O.my[it.o], it.g, i0 + threadIdx.x, i1, KR_THREADS, acc);
+        kacc_warp(acc);
+        if (lane == 0) red[wid] = acc;
+        __syncthreads();
+        if (wid == 0) {
+            KronAcc r;
+            kacc_init(r);
+            if (lane < KR_THREADS / 32) r = red[lane];
+            kacc_warp(r);
+            if (lane == 0) A.K.part[PASS - 1][c] = r;
+        }
+        __syncthreads();
+    }
+}
+
+// queued boxes: one warp per object merges its items' sums and continues
+template <int PASS>
+__global__ void k_kron_merge(EndArgs A) {
+    const int lane = threadIdx.x & 31;
+    const int n = min(A.sc->kitems[PASS - 1], A.K.icap);
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < n; k += nw) {
+        const KronItem it = A.K.item[PASS - 1][k];
+        if (it.nch < 0) continue;
+        KronAcc acc;
+        kacc_init(acc);
+        for (int j = lane; j < it.nch; j += 32) kacc_merge(acc, A.K.part[PASS - 1][it.c0 + j]);
+        kacc_warp(acc);
+        if (PASS == 1)
+            kron_after1(A, it.o, A.O.mx[it.o], A.O.my[it.o], it.flags, acc);
+        else
+            end_finish(A, it.o, it.flags, it.kron, true, acc);
+    }
+}
+
+void launch_endobject(const EndArgs &E, int nobj, cudaStream_t st, int &launches) {
+    if (nobj <= 0) return;
+    k_endobject<<<(unsigned)((nobj + 3) / 4), 128, 0, st>>>(E);
+    k_kron_chunks<1><<<KR_GRID, KR_THREADS, 0, st>>>(E);
+    k_kron_merge<1><<<KR_GRID / 2, 128, 0, st>>>(E);
+    k_kron_chunks<2><<<KR_GRID, KR_THREADS, 0, st>>>(E);
+    k_kron_merge<2><<<KR_GRID / 2, 128, 0, st>>>(E);
+    launches += 5;
 }
 
 // ---------------------------------------------------------------------------

@@ -39,6 +39,31 @@ struct DebBufs {
     int *rec;                           // merge record per element (k_dl_sweep -> k_dl_assign)
 };
 
+// Kron boxes too large for one warp, summed by whole CTAs (k_post.cu)
+constexpr int KR_CHUNK = 8192;     // box pixels per CTA work item
+constexpr int KR_THREADS = 256;
+constexpr int KR_GRID = 2 * 148;
+constexpr int KR_ITEMS = 8192;     // queued boxes per pass
+constexpr int KR_CHUNKS = 65536;   // work items per pass (2^29 box pixels)
+constexpr int KR_WARP_MAX = 32768; // default: larger boxes are queued
+
+struct KronGeo {
+    float cx2, cy2, cxy, klim2;
+    int xmin, xmax, ymin, ymax;
+};
+struct KronItem {
+    int o, flags, c0, nch;  // object, FLAGS so far, first work item, items (-1: summed by its warp)
+    float kron;
+    KronGeo g;
+};
+struct KronAcc;
+struct KronBufs {
+    KronItem *item[2];
+    int *chunk[2];    // work item -> queued box
+    KronAcc *part[2]; // work item -> partial sums
+    int icap, ccap, warp_max;
+};
+
 // per-object data (index = object id: root order, then (level, label))
 struct ObjBufs {
     int *root, *level, *n, *off;

@@ -84,6 +84,8 @@ struct sexgpu_ctx {
     // objects
     DevBuf o_i[20], o_f[32], o_d[10], o_iso, o_sortkey, amp, alpha, cellhead, cellnext, vkey, vval, vkalt, vvalt,
         skeys, svals, skalt, svalt, rows;
+    DevBuf kitem[2], kchunk[2], kpart[2];  // queued Kron boxes
+    int kron_warp_max = KR_WARP_MAX;
     DevBuf sc;
     FrameScalars hsc;
     ObjBufs O;
@@ -98,6 +100,8 @@ struct sexgpu_ctx {
     std::vector<sexgpu_ctx *> workers;  // contexts of sexgpu_extract_batch
     void *stage_host = nullptr;         // pinned staging of a batch worker's frames
     size_t stage_bytes = 0;
+    void *rows_host = nullptr;          // pinned staging of a batch worker's catalogue rows
+    size_t rows_bytes = 0;
     DevBuf dmask;                       // detection mask of the current extraction
     std::vector<float> hmask;
     ConvMask cmask{nullptr, nullptr, 1, 1};
@@ -803,8 +807,20 @@ int pipe_end(sexgpu_ctx *ctx) {
     E.zp = Pm.mag_zeropoint;
     E.satur = Pm.satur_level;
     E.wvar = ps.wvar;
-    if (nobj > 0) k_endobject<<<grid1(nobj, 4), 128, 0, st>>>(E);
-    stage_mark(ctx, "endobject", nobj > 0);
+    for (int p = 0; p < 2; p++) {
+        EN(kitem[p], (size_t)KR_ITEMS * sizeof(KronItem));
+        EN(kchunk[p], (size_t)KR_CHUNKS * sizeof(int));
+        EN(kpart[p], (size_t)KR_CHUNKS * sizeof(KronAcc));
+        E.K.item[p] = P<KronItem>(ctx->kitem[p]);
+        E.K.chunk[p] = P<int>(ctx->kchunk[p]);
+        E.K.part[p] = P<KronAcc>(ctx->kpart[p]);
+    }
+    E.K.icap = KR_ITEMS;
+    E.K.ccap = KR_CHUNKS;
+    E.K.warp_max = ctx->kron_warp_max;
+    int nl = 0;
+    launch_endobject(E, nobj, st, nl);
+    stage_mark(ctx, "endobject", nl);
 
     // ---- catalogue order
     EN(skeys, (size_t)(nobj + 1) * 4);
@@ -940,6 +956,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     for (sexgpu_ctx *w : ctx->workers) sexgpu_destroy(w);
     if (ctx->stage_host) cudaFreeHost(ctx->stage_host);
+    if (ctx->rows_host) cudaFreeHost(ctx->rows_host);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SEXGPU_OK;
@@ -1218,6 +1235,7 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
         }
         ctx->workers.push_back(w);
     }
+    for (sexgpu_ctx *w : ctx->workers) w->kron_warp_max = ctx->kron_warp_max;
     // largest frames first, so that the last frames to start are short
     std::vector<int> order(nframes);
     for (int i = 0; i < nframes; i++) order[i] = i;
@@ -1225,35 +1243,66 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
         return (long long)frames[a].w * frames[a].h > (long long)frames[b].w * frames[b].h;
     });
     std::atomic<int> next(0);
-    // Each worker copies its frame into its own pinned buffer first, so that
-    // the host->device transfers of different workers are DMA transfers that
-    // proceed in parallel instead of queueing on pageable staging.
+    // Each worker copies its frame (and weight map) into its own pinned buffer
+    // first and brings the catalogue rows back through another, so that the
+    // transfers of different workers are DMA transfers that proceed in
+    // parallel instead of queueing on the driver's pageable staging.
+    auto grow = [](void *&buf, size_t &have, size_t need) {
+        if (have >= need) return true;
+        if (buf) cudaFreeHost(buf);
+        buf = nullptr;
+        have = 0;
+        if (cudaHostAlloc(&buf, need, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        have = need;
+        return true;
+    };
     auto run = [&](sexgpu_ctx *wc) {
         cudaSetDevice(wc->device);
         for (int k; (k = next.fetch_add(1)) < nframes;) {
             sexgpu_batch_frame &f = frames[order[k]];
             f.nobj = 0;
-            if (!f.img || !f.cfg || f.w <= 0 || f.h <= 0) {
+            if (!f.img || !f.cfg || f.w <= 0 || f.h <= 0 || f.max_objects < 0 || (f.max_objects > 0 && !f.objs)) {
                 f.status = SEXGPU_ERR_ARG;
                 continue;
             }
             const size_t bytes = (size_t)f.w * f.h * sizeof(float);
-            if (wc->stage_bytes < bytes) {
-                if (wc->stage_host) cudaFreeHost(wc->stage_host);
-                wc->stage_host = nullptr;
-                wc->stage_bytes = 0;
-                if (cudaHostAlloc(&wc->stage_host, bytes, cudaHostAllocPortable) == cudaSuccess)
-                    wc->stage_bytes = bytes;
-                else
-                    cudaGetLastError();
-            }
-            const float *src = f.img;
-            if (wc->stage_bytes >= bytes) {
+            const float *src = f.img, *wsrc = f.wmap;
+            if (grow(wc->stage_host, wc->stage_bytes, f.wmap ? 2 * bytes : bytes)) {
                 memcpy(wc->stage_host, f.img, bytes);
                 src = (const float *)wc->stage_host;
+                if (f.wmap) {
+                    memcpy((char *)wc->stage_host + bytes, f.wmap, bytes);
+                    wsrc = (const float *)((char *)wc->stage_host + bytes);
+                }
             }
-            f.status = sexgpu_extract(wc, src, f.wmap, f.w, f.h, f.cfg, f.objs, f.max_objects, &f.nobj, nullptr,
-                                      nullptr, nullptr, &f.summary);
+            const size_t rbytes = (size_t)f.max_objects * sizeof(sexgpu_object);
+            if (!grow(wc->rows_host, wc->rows_bytes, std::min(rbytes, (size_t)1 << 20))) {
+                f.status = sexgpu_extract(wc, src, wsrc, f.w, f.h, f.cfg, f.objs, f.max_objects, &f.nobj, nullptr,
+                                          nullptr, nullptr, &f.summary);
+                continue;
+            }
+            f.status = sexgpu_extract(wc, src, wsrc, f.w, f.h, f.cfg, nullptr, 0, &f.nobj, nullptr, nullptr,
+                                      nullptr, &f.summary);
+            if (f.status) continue;
+            const int n = std::min(f.nobj, f.max_objects);
+            const size_t nb = (size_t)n * sizeof(sexgpu_object);
+            if (n > 0 && !grow(wc->rows_host, wc->rows_bytes, nb)) {
+                f.status = SEXGPU_ERR_NOMEM;
+                continue;
+            }
+            if (n > 0) {
+                cudaError_t e = cudaMemcpyAsync(wc->rows_host, wc->rows.p, nb, cudaMemcpyDeviceToHost, wc->stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(wc->stream);
+                if (e != cudaSuccess) {
+                    f.status = set_err(wc, e, "catalogue copy");
+                    continue;
+                }
+                memcpy(f.objs, wc->rows_host, nb);
+            }
+            if (f.nobj > f.max_objects) f.status = SEXGPU_ERR_CAPACITY;
         }
     };
     std::vector<std::thread> pool;
@@ -1266,6 +1315,17 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
             return frames[i].status;
         }
     return SEXGPU_OK;
+}
+
+int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value) {
+    if (!ctx || !name) return SEXGPU_ERR_ARG;
+    if (!strcmp(name, "kron_warp_max")) {
+        if (value < 1) return SEXGPU_ERR_ARG;
+        ctx->kron_warp_max = value;
+        return SEXGPU_OK;
+    }
+    ctx->err = std::string("unknown parameter ") + name;
+    return SEXGPU_ERR_ARG;
 }
 
 int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max) {

@@ -10,13 +10,14 @@
  * makeback() + scanimage().
  *
  * Supported keywords (the extraction settings of src/preflist.h):
- *   CATALOG_NAME CATALOG_TYPE (ASCII, ASCII_HEAD) PARAMETERS_NAME
+ *   CATALOG_NAME CATALOG_TYPE (ASCII, ASCII_HEAD, FITS_LDAC) PARAMETERS_NAME
  *   DETECT_MINAREA DETECT_THRESH ANALYSIS_THRESH THRESH_TYPE FILTER FILTER_NAME
  *   DEBLEND_NTHRESH DEBLEND_MINCONT CLEAN CLEAN_PARAM MASK_TYPE
  *   PHOT_APERTURES PHOT_AUTOPARAMS SATUR_LEVEL MAG_ZEROPOINT GAIN
  *   BACK_SIZE BACK_FILTERSIZE BACK_FILTTHRESH BACK_TYPE BACK_VALUE
  *   CHECKIMAGE_TYPE (NONE, SEGMENTATION, BACKGROUND, -BACKGROUND, FILTERED)
  *   CHECKIMAGE_NAME VERBOSE_TYPE
+ *   WEIGHT_TYPE (NONE, MAP_VAR, MAP_RMS, MAP_WEIGHT) WEIGHT_IMAGE
  * Other keywords of the reference are accepted and ignored.
  */
 #include <ctype.h>
@@ -34,7 +35,7 @@
 
 typedef struct {
     char catalog_name[1024], catalog_type[64], parameters_name[1024], filter_name[1024];
-    char check_type[64], check_name[1024], verbose[32];
+    char check_type[64], check_name[1024], verbose[32], weight_image[1024];
     sexgpu_config cfg;
     float mask[1024];
 } prefs_t;
@@ -93,6 +94,12 @@ static void setpref(prefs_t *p, const char *key, char *val)
     else if (!strcasecmp(key, "BACK_FILTTHRESH")) c->back_filtthresh = atof(val);
     else if (!strcasecmp(key, "BACK_TYPE")) c->back_type = !strncasecmp(val, "MANUAL", 6);
     else if (!strcasecmp(key, "BACK_VALUE")) c->back_value = atof(val);
+    else if (!strcasecmp(key, "WEIGHT_TYPE"))
+        c->weight_type = !strncasecmp(val, "MAP_VAR", 7)      ? 1
+                         : !strncasecmp(val, "MAP_RMS", 7)    ? 2
+                         : !strncasecmp(val, "MAP_WEIGHT", 10) ? 3
+                                                               : 0;
+    else if (!strcasecmp(key, "WEIGHT_IMAGE")) snprintf(p->weight_image, sizeof p->weight_image, "%s", val);
 }
 
 static void readprefs(prefs_t *p, const char *path)
@@ -342,6 +349,177 @@ static void printobj(FILE *f, const sexgpu_object *o)
             o->kronfactor, o->bkg, o->fwhm);
 }
 
+/* ------------------------------------------------------------ FITS_LDAC --- */
+/* binary type of a column: J int32, D double (second moments), E float */
+static char col_type(int c)
+{
+    const char *fmt = COLS[c].fmt;
+    return fmt[strlen(fmt) - 1] == 'd' ? 'J' : !strcmp(fmt, "%15.10e") ? 'D' : 'E';
+}
+
+static double col_value(int c, const sexgpu_object *o)
+{
+    switch (c) {
+    case 0: return o->number;
+    case 1: return o->mx + 1.0;
+    case 2: return o->my + 1.0;
+    case 3: return o->xmin + 1;
+    case 4: return o->ymin + 1;
+    case 5: return o->xmax + 1;
+    case 6: return o->ymax + 1;
+    case 7: return o->npix;
+    case 8: return o->flux_iso;
+    case 9: return o->fluxerr_iso;
+    case 10: return o->mag_iso;
+    case 11: return o->magerr_iso;
+    case 12: return o->flux_isocor;
+    case 13: return o->fluxerr_isocor;
+    case 14: return o->flux_aper;
+    case 15: return o->fluxerr_aper;
+    case 16: return o->mag_aper;
+    case 17: return o->magerr_aper;
+    case 18: return o->flux_auto;
+    case 19: return o->fluxerr_auto;
+    case 20: return o->mag_auto;
+    case 21: return o->magerr_auto;
+    case 22: return o->kronfactor;
+    case 23: return o->bkg;
+    case 24: return o->thresh;
+    case 25: return o->peak;
+    case 26: return o->mx2;
+    case 27: return o->my2;
+    case 28: return o->mxy;
+    case 29: return o->poserr_mx2;
+    case 30: return o->poserr_my2;
+    case 31: return o->poserr_mxy;
+    case 32: return o->cxx;
+    case 33: return o->cyy;
+    case 34: return o->cxy;
+    case 35: return o->a;
+    case 36: return o->b;
+    case 37: return o->theta;
+    case 38: return o->elong;
+    case 39: return o->ellip;
+    case 40: return o->fwhm;
+    case 41: return o->flags;
+    case 42: return o->peakx;
+    case 43: return o->peaky;
+    }
+    return 0.0;
+}
+
+static void put_be(FILE *f, const void *v, int n)
+{
+    const unsigned char *b = (const unsigned char *)v;
+    for (int i = n - 1; i >= 0; i--) fputc(b[i], f);
+}
+
+static void pad_block(FILE *f, long n, int fill)
+{
+    for (long k = n % 2880; k && k < 2880; k++) fputc(fill, f);
+}
+
+static void card_str(FILE *f, const char *key, const char *val)
+{
+    char card[81];
+    snprintf(card, sizeof card, "%-8s= '%-8s'", key, val);
+    write_card(f, card);
+}
+
+static void card_int(FILE *f, const char *key, long v)
+{
+    char card[81];
+    snprintf(card, sizeof card, "%-8s= %20ld", key, v);
+    write_card(f, card);
+}
+
+/* FITS_LDAC catalogue (the layout of SExtractor's LDAC output): an empty
+ * primary HDU, LDAC_IMHEAD (the image header as one character cell) and
+ * LDAC_OBJECTS (one row per object, the .param columns, big-endian) */
+static void write_ldac(const char *path, const sexgpu_object *objs, int n, const int *sel, int ns, int w, int h)
+{
+    FILE *f = fopen(path, "wb");
+    char card[81], hdr[6 * 80 + 1], form[32];
+    int k, ncard = 0, rowbytes = 0, nhdr = 6;
+    if (!f) die("cannot write ", path);
+    write_card(f, "SIMPLE  =                    T");
+    write_card(f, "BITPIX  =                    8");
+    write_card(f, "NAXIS   =                    0");
+    write_card(f, "EXTEND  =                    T");
+    write_card(f, "END");
+    for (ncard = 5; ncard % 36; ncard++) write_card(f, "");
+    /* LDAC_IMHEAD */
+    memset(hdr, ' ', sizeof hdr - 1);
+    hdr[sizeof hdr - 1] = 0;
+    snprintf(card, sizeof card, "%-8s= %20s", "SIMPLE", "T"); memcpy(hdr, card, strlen(card));
+    snprintf(card, sizeof card, "%-8s= %20d", "BITPIX", -32); memcpy(hdr + 80, card, strlen(card));
+    snprintf(card, sizeof card, "%-8s= %20d", "NAXIS", 2); memcpy(hdr + 160, card, strlen(card));
+    snprintf(card, sizeof card, "%-8s= %20d", "NAXIS1", w); memcpy(hdr + 240, card, strlen(card));
+    snprintf(card, sizeof card, "%-8s= %20d", "NAXIS2", h); memcpy(hdr + 320, card, strlen(card));
+    memcpy(hdr + 400, "END", 3);
+    ncard = 0;
+    card_str(f, "XTENSION", "BINTABLE"); ncard++;
+    card_int(f, "BITPIX", 8); ncard++;
+    card_int(f, "NAXIS", 2); ncard++;
+    card_int(f, "NAXIS1", 80 * nhdr); ncard++;
+    card_int(f, "NAXIS2", 1); ncard++;
+    card_int(f, "PCOUNT", 0); ncard++;
+    card_int(f, "GCOUNT", 1); ncard++;
+    card_int(f, "TFIELDS", 1); ncard++;
+    card_str(f, "TTYPE1", "Field Header Card"); ncard++;
+    snprintf(form, sizeof form, "%dA", 80 * nhdr);
+    card_str(f, "TFORM1", form); ncard++;
+    snprintf(form, sizeof form, "(80, %d)", nhdr);
+    card_str(f, "TDIM1", form); ncard++;
+    card_str(f, "EXTNAME", "LDAC_IMHEAD"); ncard++;
+    write_card(f, "END"); ncard++;
+    for (; ncard % 36; ncard++) write_card(f, "");
+    fwrite(hdr, 1, 80 * nhdr, f);
+    pad_block(f, 80 * nhdr, 0);
+    /* LDAC_OBJECTS */
+    for (k = 0; k < ns; k++) rowbytes += col_type(sel[k]) == 'D' ? 8 : 4;
+    ncard = 0;
+    card_str(f, "XTENSION", "BINTABLE"); ncard++;
+    card_int(f, "BITPIX", 8); ncard++;
+    card_int(f, "NAXIS", 2); ncard++;
+    card_int(f, "NAXIS1", rowbytes); ncard++;
+    card_int(f, "NAXIS2", n); ncard++;
+    card_int(f, "PCOUNT", 0); ncard++;
+    card_int(f, "GCOUNT", 1); ncard++;
+    card_int(f, "TFIELDS", ns); ncard++;
+    for (k = 0; k < ns; k++) {
+        char key[16];
+        snprintf(key, sizeof key, "TTYPE%d", k + 1);
+        card_str(f, key, COLS[sel[k]].name); ncard++;
+        snprintf(key, sizeof key, "TFORM%d", k + 1);
+        snprintf(form, sizeof form, "1%c", col_type(sel[k]));
+        card_str(f, key, form); ncard++;
+        if (*COLS[sel[k]].unit) {
+            snprintf(key, sizeof key, "TUNIT%d", k + 1);
+            card_str(f, key, COLS[sel[k]].unit); ncard++;
+        }
+    }
+    card_str(f, "EXTNAME", "LDAC_OBJECTS"); ncard++;
+    write_card(f, "END"); ncard++;
+    for (; ncard % 36; ncard++) write_card(f, "");
+    for (int i = 0; i < n; i++)
+        for (k = 0; k < ns; k++) {
+            double v = col_value(sel[k], &objs[i]);
+            char t = col_type(sel[k]);
+            if (t == 'J') {
+                int32_t iv = (int32_t)v;
+                put_be(f, &iv, 4);
+            } else if (t == 'D') {
+                put_be(f, &v, 8);
+            } else {
+                float fv = (float)v;
+                put_be(f, &fv, 4);
+            }
+        }
+    pad_block(f, (long)rowbytes * n, 0);
+    fclose(f);
+}
+
 static int read_params(const char *path, int *sel, int maxsel)
 {
     char line[MAXLINE];
@@ -367,7 +545,7 @@ int main(int argc, char **argv)
     prefs_t p;
     const char *image = NULL, *conf = "default.sex";
     int i, w, h, n = 0, rc, mw, mh;
-    float *img;
+    float *img, *wmap = NULL;
     sexgpu_object *objs;
     int32_t *seg = NULL;
     float *sub = NULL, *cd = NULL;
@@ -415,6 +593,15 @@ int main(int argc, char **argv)
         p.cfg.conv_h = mh;
     }
     img = read_fits(image, &w, &h);
+    if (p.cfg.weight_type) {
+        int ww, wh;
+        if (!*p.weight_image) die("WEIGHT_IMAGE missing", NULL);
+        wmap = read_fits(p.weight_image, &ww, &wh);
+        if (ww != w || wh != h) die("measured frame and weight map have different sizes: ", p.weight_image);
+        /* read_fits marks NaN as -1e30; for a weight map that is unusable */
+        for (size_t k = 0; k < (size_t)w * h; k++)
+            if (wmap[k] <= -1e30f) wmap[k] = p.cfg.weight_type == 3 ? 0.0f : 1e30f;
+    }
     if ((rc = sexgpu_create(&ctx, 0)) != SEXGPU_OK) die("no usable CUDA device", NULL);
     objs = (sexgpu_object *)malloc(sizeof(sexgpu_object) * 1024);
     if (strcasecmp(p.check_type, "NONE")) {
@@ -422,7 +609,7 @@ int main(int argc, char **argv)
         sub = (float *)malloc(sizeof(float) * (size_t)w * h);
         cd = (float *)malloc(sizeof(float) * (size_t)w * h);
     }
-    rc = sexgpu_extract(ctx, img, NULL, w, h, &p.cfg, objs, 1024, &n, seg, sub, cd, &s);
+    rc = sexgpu_extract(ctx, img, wmap, w, h, &p.cfg, objs, 1024, &n, seg, sub, cd, &s);
     if (rc == SEXGPU_ERR_CAPACITY) {
         objs = (sexgpu_object *)realloc(objs, sizeof(sexgpu_object) * (size_t)(n + 1));
         rc = sexgpu_copy_results(ctx, objs, n, &n, NULL, NULL, NULL);
@@ -451,6 +638,13 @@ int main(int argc, char **argv)
                     fputc('\n', cat);
                 }
             }
+        } else if (!strcasecmp(p.catalog_type, "FITS_LDAC")) {
+            int sel[64], ns = read_params(p.parameters_name, sel, 64);
+            if (cat != stdout) fclose(cat);
+            cat = stdout;
+            if (ns == 0)
+                for (ns = 0; COLS[ns].name; ns++) sel[ns] = ns;
+            write_ldac(p.catalog_name, objs, n, sel, ns, w, h);
         } else
             for (i = 0; i < n; i++) printobj(cat, &objs[i]);
         if (cat != stdout) fclose(cat);
@@ -470,6 +664,7 @@ int main(int argc, char **argv)
                 s.backmean, s.backsig, s.dthresh, s.ndetected, n, (double)(clock() - t0) / CLOCKS_PER_SEC);
     sexgpu_destroy(ctx);
     free(img);
+    free(wmap);
     free(objs);
     free(seg);
     free(sub);

@@ -85,7 +85,7 @@ class Stage(C.Structure):
 
 EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extract",
            "sexgpu_extract_device", "sexgpu_copy_results", "sexgpu_background", "sexgpu_filter",
-           "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times",
+           "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times", "sexgpu_set_param",
            "sexgpu_background_noalloc", "sexgpu_extract_batch"]
 
 _lib = None
@@ -264,6 +264,10 @@ class Context:
             f.objs, f.max_objects = objs.ctypes.data_as(C.c_void_p), cap
         _check(lib().sexgpu_extract_batch(self.h, arr, n, workers), self.h, "sexgpu_extract_batch")
         return [(keep[i][2][:arr[i].nobj], arr[i].summary) for i in range(n)]
+
+    def set_param(self, name, value):
+        """Execution parameter (results do not depend on it), e.g. kron_warp_max."""
+        _check(lib().sexgpu_set_param(self.h, name.encode(), int(value)), self.h, "sexgpu_set_param")
 
     def stage_times(self):
         st = (Stage * 32)()

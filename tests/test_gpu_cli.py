@@ -61,3 +61,68 @@ def test_cli_catalog_and_segmentation(tmp_path, masks):
     assert [int(r[0]) for r in rows] == list(o["number"])
     assert [int(r[23]) for r in rows] == list(o["flags"])
     assert np.array_equal(read_fits_i32(str(seg), 400, 300), oseg)
+
+
+def read_ldac_objects(path):
+    """LDAC_OBJECTS table of a FITS_LDAC catalogue as a numpy record array."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    pos = 0
+    while pos < len(raw):
+        cards = {}
+        while True:
+            block = raw[pos:pos + 2880].decode("ascii")
+            pos += 2880
+            end = False
+            for k in range(36):
+                c = block[80 * k:80 * k + 80]
+                if c.startswith("END"):
+                    end = True
+                    break
+                if c[8:10] == "= ":
+                    cards[c[:8].strip()] = c[10:].strip().strip("'").strip()
+            if end:
+                break
+        nbytes = int(cards.get("NAXIS1", 0)) * int(cards.get("NAXIS2", 0)) if cards.get("NAXIS") == "2" else 0
+        if cards.get("EXTNAME") == "LDAC_OBJECTS":
+            code = {"J": ">i4", "E": ">f4", "D": ">f8"}
+            dt = np.dtype([(cards["TTYPE%d" % (k + 1)], code[cards["TFORM%d" % (k + 1)][-1]])
+                           for k in range(int(cards["TFIELDS"]))])
+            assert dt.itemsize == int(cards["NAXIS1"])
+            return np.frombuffer(raw[pos:pos + nbytes], dt)
+        pos += (nbytes + 2879) // 2880 * 2880
+    raise AssertionError("no LDAC_OBJECTS table")
+
+
+def test_cli_fits_ldac_with_weight_map(tmp_path, masks):
+    if not os.path.exists(SEX):
+        subprocess.check_call(["make", "-s", "-C", os.path.dirname(SEX)])
+    img, vm = synth.frame_c1(seed=5, w=256, h=192, nsrc=150, var=True)
+    fits = tmp_path / "img.fits"
+    wfits = tmp_path / "var.fits"
+    write_fits(str(fits), img)
+    write_fits(str(wfits), vm)
+    conv = tmp_path / "g.conv"
+    m = masks["gauss_2.5_5x5"]
+    conv.write_text("CONV NONORM\n" + "\n".join(" ".join("%.9g" % v for v in row) for row in m) + "\n")
+    par = tmp_path / "t.param"
+    par.write_text("NUMBER\nX_IMAGE\nY_IMAGE\nFLUX_ISO\nFLUXERR_ISO\nX2_IMAGE\nFLAGS\nFLUX_APER(1)\n")
+    cfgf = tmp_path / "t.sex"
+    cfgf.write_text("CATALOG_TYPE FITS_LDAC\nFILTER_NAME %s\nPARAMETERS_NAME %s\nWEIGHT_TYPE MAP_VAR\n"
+                    "WEIGHT_IMAGE %s\nBACK_SIZE 64\n" % (conv, par, wfits))
+    cat = tmp_path / "t.ldac"
+    subprocess.check_call([SEX, str(fits), "-c", str(cfgf), "-CATALOG_NAME", str(cat), "-VERBOSE_TYPE", "QUIET"],
+                          cwd=str(tmp_path))
+    t = read_ldac_objects(str(cat))
+    o, _, _ = O.extract(img, conv=m, weight_type=1, weight=vm)
+    assert len(t) == len(o) > 0
+    assert list(t.dtype.names) == ["NUMBER", "X_IMAGE", "Y_IMAGE", "FLUX_ISO", "FLUXERR_ISO", "X2_IMAGE", "FLAGS",
+                                   "FLUX_APER"]
+    assert t.dtype["X2_IMAGE"] == np.dtype(">f8") and t.dtype["NUMBER"] == np.dtype(">i4")
+    assert np.array_equal(t["NUMBER"], o["number"])
+    assert np.array_equal(t["FLAGS"], o["flags"])
+    assert np.array_equal(t["X_IMAGE"], (o["mx"] + 1.0).astype(np.float32))
+    assert np.array_equal(t["FLUX_ISO"], o["flux_iso"])
+    assert np.array_equal(t["FLUXERR_ISO"], o["fluxerr_iso"])
+    assert np.array_equal(t["X2_IMAGE"], o["mx2"])
+    assert np.array_equal(t["FLUX_APER"], o["flux_aper"])

@@ -192,3 +192,31 @@ def test_weight_map_absolute_thresholds(gpu_ctx, masks):
     o, oseg, os_ = O.extract(img, weight=vm, **kw)
     assert np.array_equal(gseg, oseg)
     compare_catalogs(g, o)
+
+
+@pytest.mark.parametrize("warp_max,mask,weighted", [(1, "mexhat_2.5_7x7", False), (300, "gauss_2.5_5x5", False),
+                                                    (1, "gauss_4.0_7x7", True)])
+def test_kron_boxes_summed_by_blocks(masks, warp_max, mask, weighted):
+    """AUTO photometry with the Kron boxes queued for whole thread blocks
+    (kron_warp_max 1: every box; with more than 8192 survivors the queue
+    overflows and the remaining boxes are summed by their warps; 300: a mix).
+    The catalogue must not change."""
+    import sexgpu
+    with sexgpu.Context(0) as ctx:
+        ctx.set_param("kron_warp_max", warp_max)
+        kw = dict(conv=masks[mask])
+        if weighted:
+            img, vm = synth.frame_c1(seed=4003, w=768, h=640, density=9e-3, var=True)
+            kw.update(weight=vm, weight_type=1, back_size=128)
+        else:
+            img = synth.frame_c1(seed=79, w=1700, h=1600, density=9e-3)
+        g = run_both(ctx, img, **kw)
+        assert len(g) > (100 if weighted else 8192)
+
+
+def test_kron_param_rejects_bad_values(gpu_ctx):
+    import sexgpu
+    with pytest.raises(RuntimeError):
+        gpu_ctx.set_param("kron_warp_max", 0)
+    with pytest.raises(RuntimeError):
+        gpu_ctx.set_param("no_such_parameter", 1)
