@@ -250,6 +250,8 @@ def run_gpu(args):
         line["catalog_err_fp64"] = catalog_err(ctx, frame, cfg)
     if world == 1 and not args.no_batch:
         line["batch"] = run_batch(ctx, c3_frames())
+    if world == 1 and not args.no_c4:
+        line["c4"] = run_c4(ctx, torch, dev, stream, peak)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(frame, cfg)
     if rank == 0:
@@ -347,6 +349,102 @@ def algorithmic_bytes(stage, N, s):
     return 4 * N
 
 
+C4_WORKLOAD = ("c4: one 16384x16384 float32 frame with 2.5 M injected sources (c1 generator) and a MAP_VAR "
+               "variance map (1.0 +- 20% smooth, 2% masked in 8x8 blocks); BACK_SIZE 128, gauss_4.0_7x7")
+
+
+def stage_bytes(stage, N, s, weighted):
+    """Compulsory bytes of a stage of one extraction: pixel stages from the
+    frame size N, object stages from the counts the extraction reports
+    (raw-object pixels P, pixel-levels of the deblending, catalogue rows)."""
+    P, L, M = int(s.nraw_pix), int(s.level_pix), int(s.nobj)
+    if stage == "background":
+        return 4 * N + (8 * N if weighted else 0)   # frame; weight map read + variance written
+    if stage == "sub_filter":
+        return 16 * N + (4 * N if weighted else 0)  # frame in; sub, cd, labels out; variance in
+    if stage == "ccl":
+        return 8 * N
+    if stage == "roots":
+        return 24 * N
+    if stage == "deblend":
+        return 8 * L
+    if stage in ("analyse", "endobject"):
+        return 16 * P
+    return 64 * M
+
+
+def run_c4(ctx, torch, dev, stream, peak, steps=3):
+    """The c4 frame through the weighted path: device-resident time per
+    frame, stage times and per-stage GB/s, and one end-to-end call with the
+    frame and the variance map in pinned host memory."""
+    import ctypes as C
+    import multiprocessing as mp
+    import synth
+    import sexgpu
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(max(1, min(os.cpu_count() or 1, 32))) as pool:
+        img, vm = synth.frame_c4(seed=4000, pool=pool)
+    gen_s = time.perf_counter() - t0
+    cfg = dict(conv=load_mask("gauss_4.0_7x7"), back_size=128, weight_type=1)
+    h, w = img.shape
+    N = w * h
+    d_img = torch.from_numpy(img).to(dev)
+    d_var = torch.from_numpy(vm).to(dev)
+
+    def step():
+        return ctx.extract_device(d_img.data_ptr(), w, h, wmap_ptr=d_var.data_ptr(), **cfg)
+
+    s = step()
+    step()
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s = step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    stages = ctx.stage_times()
+    per = {}
+    for name, _, t in stages:
+        b = stage_bytes(name, N, s, True)
+        per[name] = {"ms": round(t, 4), "bytes": b, "gb_s": round(b / (t / 1e3) / 1e9, 1) if t > 0 else None,
+                     "frac_of_peak": round(b / (t / 1e3) / 1e9 / peak, 4) if t > 0 else None}
+    h_img = torch.from_numpy(img).pin_memory()
+    h_var = torch.from_numpy(vm).pin_memory()
+    del img, vm
+    maxobj = 2_500_000
+    h_rows = torch.empty(maxobj * sexgpu.OBJECT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    c = sexgpu.make_config(**cfg)
+    n = C.c_int()
+    summ = sexgpu.Summary()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rc = sexgpu.lib().sexgpu_extract(ctx.h, C.c_void_p(h_img.data_ptr()), C.c_void_p(h_var.data_ptr()), w, h,
+                                     C.byref(c), C.c_void_p(h_rows.data_ptr()), maxobj, C.byref(n), None, None,
+                                     None, C.byref(summ))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if rc != 0:
+        raise RuntimeError("sexgpu_extract failed %d" % rc)
+    ms_e2e = e0.elapsed_time(e1)
+    rows = h_rows.numpy().view(sexgpu.OBJECT_DTYPE)[:n.value]
+    same = bool(n.value == s.nobj and np.array_equal(rows["number"], np.arange(1, n.value + 1)))
+    msd = min(ms)
+    return {"workload": C4_WORKLOAD, "frame": [h, w], "objects": int(s.nobj), "raw_objects": int(s.nraw),
+            "raw_object_pixels": int(s.nraw_pix), "pixel_levels": int(s.level_pix), "sigfac": float(s.sigfac),
+            "ms_per_frame": round(msd, 3), "frames_per_s": round(1e3 / msd, 3),
+            "mobj_per_s": round(s.nobj / msd / 1e3, 4), "steps": steps, "generate_s": round(gen_s, 1),
+            "stages": per,
+            "e2e": {"ms": round(ms_e2e, 3), "h2d_bytes": 8 * N,
+                    "d2h_bytes": int(n.value) * sexgpu.OBJECT_DTYPE.itemsize, "same_object_count": same},
+            "note": "inputs (2 GiB) larger than L2; per-stage bytes are the compulsory bytes of the stage"}
+
+
 _FRAMES = {}
 
 
@@ -412,6 +510,7 @@ def main():
     ap.add_argument("--impl", default="sexgpu")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-c4", action="store_true", help="skip the 16384^2 weighted frame (c4)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

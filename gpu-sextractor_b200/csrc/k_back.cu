@@ -17,7 +17,10 @@ namespace sx {
 
 // src/back.c:214-279 for one mesh: the reference's two sequential double
 // passes, in its pixel order.  `row0` points at the mesh's first pixel, rows
-// `stride` floats apart.
+// `stride` floats apart.  A pixel left out adds +0.0 instead of skipping the
+// addition: the sums start at +0.0 and so are never -0.0, hence s + 0.0 == s
+// exactly, and the select stays off the dependent chain of additions (the
+// double-add latency, about 17 cycles on B200, is the cost of these loops).
 __device__ __forceinline__ void mesh_stat_seq(const float *row0, int stride, int mw, int mh, MeshStat &o) {
     double pix, sig, mean = 0.0, sigma = 0.0;
     const double step = sqrt(2 / SX_PI) * SX_QUANTIF_NSIGMA / SX_QUANTIF_AMIN;
@@ -29,12 +32,13 @@ __device__ __forceinline__ void mesh_stat_seq(const float *row0, int stride, int
         // unrolled so that loads and conversions run ahead of the two
         // accumulation chains; the additions stay in pixel order
 #pragma unroll 8
-        for (int x = 0; x < mw; x++)
-            if ((pix = row[x]) > -SX_BIG) {
-                mean += pix;
-                sigma += pix * pix;
-                npix++;
-            }
+        for (int x = 0; x < mw; x++) {
+            pix = row[x];
+            const bool in = pix > -SX_BIG;
+            mean += in ? pix : 0.0;
+            sigma += in ? pix * pix : 0.0;
+            npix += in;
+        }
     }
     if ((float)npix < (float)(mw * mh * SX_BACK_MINGOODFRAC)) {
         o.mean = o.sigma = -SX_BIG;
@@ -51,11 +55,10 @@ __device__ __forceinline__ void mesh_stat_seq(const float *row0, int stride, int
 #pragma unroll 8
         for (int x = 0; x < mw; x++) {
             pix = row[x];
-            if (pix <= hcut && pix >= lcut) {
-                mean += pix;
-                sigma += pix * pix;
-                npix++;
-            }
+            const bool in = pix <= hcut && pix >= lcut;
+            mean += in ? pix : 0.0;
+            sigma += in ? pix * pix : 0.0;
+            npix += in;
         }
     }
     o.npix = npix;
@@ -142,21 +145,21 @@ __global__ void __launch_bounds__(32) k_mesh_stat_band(const float *__restrict__
                 const float *row = buf[y & 1] + lane * stride;
                 if (pass == 0) {
 #pragma unroll 8
-                    for (int x = 0; x < mw; x++)
-                        if ((pix = row[x]) > -SX_BIG) {
-                            mean += pix;
-                            sigma += pix * pix;
-                            npix++;
-                        }
+                    for (int x = 0; x < mw; x++) {
+                        pix = row[x];
+                        const bool in = pix > -SX_BIG;
+                        mean += in ? pix : 0.0;
+                        sigma += in ? pix * pix : 0.0;
+                        npix += in;
+                    }
                 } else {
 #pragma unroll 8
                     for (int x = 0; x < mw; x++) {
                         pix = row[x];
-                        if (pix <= hcut && pix >= lcut) {
-                            mean += pix;
-                            sigma += pix * pix;
-                            npix++;
-                        }
+                        const bool in = pix <= hcut && pix >= lcut;
+                        mean += in ? pix : 0.0;
+                        sigma += in ? pix * pix : 0.0;
+                        npix += in;
                     }
                 }
             }

@@ -259,3 +259,107 @@ def batch_c3_from_bases(bases, seed=3000):
         bs = int(rng.choice([32, 64, 128]))
         out.append((np.ascontiguousarray(base[y:y + hh, x:x + ww]), bs, C3_MASKS[i % 3]))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Workload c4: one 16384^2 frame with ~2.5 M sources and a variance map.  The
+# sources are drawn here, then rendered tile by tile (every tile onto its own
+# canvas with a margin as wide as the largest stamp, so the frame-size
+# histogram of _render is never built); the tiles can go to a process pool.
+# ---------------------------------------------------------------------------
+C4_TILE = 2048
+C4_MARGIN = 24
+
+
+def _c4_tile(job):
+    """Render one tile's sources (job = (x0, y0, tw, th, star params,
+    galaxy params)); returns the canvas of (th + 2m) x (tw + 2m) floats."""
+    x0, y0, tw, th, stars, gals = job
+    m = C4_MARGIN
+    cw, ch = tw + 2 * m, th + 2 * m
+    out = np.zeros(cw * ch)
+    sx, sy, sf = stars
+    alpha = 2.5 / (2.0 * np.sqrt(2.0 ** (1.0 / 3.0) - 1.0))
+    for b in range(0, sx.size, 4096):
+        _render(1, sx[b:b + 4096] - x0 + m, sy[b:b + 4096] - y0 + m, sf[b:b + 4096],
+                np.full(min(4096, sx.size - b), alpha), 12, cw, ch, out)
+    gx, gy, gf, sn, re, q, pa = gals
+    half = np.clip(np.ceil(3.0 * re), 6, 24).astype(np.int64)
+    for hv in np.unique(half):
+        sel = np.nonzero(half == hv)[0]
+        for b in range(0, sel.size, 2048):
+            k = sel[b:b + 2048]
+            _render(2, gx[k] - x0 + m, gy[k] - y0 + m, gf[k], (sn[k], re[k], q[k], pa[k]), int(hv), cw, ch, out)
+    return out.reshape(ch, cw).astype(np.float32)
+
+
+def frame_c4(seed=4000, n=16384, nsrc=2_500_000, pool=None):
+    """Workload c4: n x n float32 frame from the c1 generator (60% Moffat
+    stars, 40% Sersic galaxies, power-law fluxes from 1e3, 5% blended pairs,
+    sky 800 +- 5%, sigma 8 plus Poisson, clipped at 60000, 3 bad columns) and
+    its MAP_VAR variance map (1.0 +- 20% smooth, x64 to the sky noise, 2% of
+    the pixels masked in 8x8 blocks).  pool: optional process pool (map) for
+    the tiles.  Returns (img, var)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = h = n
+    npair = int(0.05 * nsrc) // 2
+    nsing = nsrc - 2 * npair
+    xc = rng.uniform(0, w, nsing)
+    yc = rng.uniform(0, h, nsing)
+    px = rng.uniform(0, w, npair)
+    py = rng.uniform(0, h, npair)
+    sep = rng.uniform(3.0, 10.0, npair)
+    ang = rng.uniform(0.0, 2 * np.pi, npair)
+    xc = np.concatenate([xc, px, px + sep * np.cos(ang)])
+    yc = np.concatenate([yc, py, py + sep * np.sin(ang)])
+    flux = _powerlaw_flux(rng, xc.size, fmin=1e3)
+    is_star = rng.random(xc.size) < 0.6
+    ng = int((~is_star).sum())
+    sn = rng.uniform(0.5, 4.0, ng)
+    re = rng.uniform(1.0, 8.0, ng)
+    q = rng.uniform(0.3, 1.0, ng)
+    pa = rng.uniform(0.0, np.pi, ng)
+    st, gl = np.nonzero(is_star)[0], np.nonzero(~is_star)[0]
+    T = C4_TILE
+    nt = (n + T - 1) // T
+    sk = (np.floor(yc[st] + 0.5).astype(np.int64).clip(0, n - 1) // T) * nt + \
+        np.floor(xc[st] + 0.5).astype(np.int64).clip(0, n - 1) // T
+    gk = (np.floor(yc[gl] + 0.5).astype(np.int64).clip(0, n - 1) // T) * nt + \
+        np.floor(xc[gl] + 0.5).astype(np.int64).clip(0, n - 1) // T
+    jobs = []
+    for t in range(nt * nt):
+        ty, tx = divmod(t, nt)
+        s = st[sk == t]
+        g = np.nonzero(gk == t)[0]
+        gi = gl[g]
+        jobs.append((tx * T, ty * T, min(T, n - tx * T), min(T, n - ty * T), (xc[s], yc[s], flux[s]),
+                     (xc[gi], yc[gi], flux[gi], sn[g], re[g], q[g], pa[g])))
+    tiles = (pool.map if pool is not None else map)(_c4_tile, jobs)
+    m = C4_MARGIN
+    src = np.zeros((h + 2 * m, w + 2 * m), np.float32)
+    for (x0, y0, tw, th, _, _), c in zip(jobs, tiles):
+        src[y0:y0 + th + 2 * m, x0:x0 + tw + 2 * m] += c
+    src = src[m:m + h, m:m + w]
+    c = rng.uniform(-1.0, 1.0, 6)
+    u = (np.arange(w, dtype=np.float32) / (w - 1) * 2 - 1)[None, :]
+    v = (np.arange(h, dtype=np.float32) / (h - 1) * 2 - 1)[:, None]
+    p2 = c[0] + c[1] * u + c[2] * v + c[3] * u * u + c[4] * u * v + c[5] * v * v
+    p2 = p2 / max(float(np.abs(p2).max()), 1e-12)
+    img = (800.0 * (1.0 + 0.05 * p2)).astype(np.float32)
+    img += src
+    noise = rng.standard_normal((h, w), dtype=np.float32)
+    noise *= np.sqrt(64.0 + np.maximum(src, 0.0))
+    img += noise
+    del noise, src
+    np.minimum(img, 60000.0, out=img)
+    img[:, rng.choice(w, 3, replace=False)] = 0.0
+    kx = rng.uniform(1, 4, 2)
+    vm = (1.0 + 0.2 * np.sin(2 * np.pi * kx[0] * u + 1.0) * np.cos(2 * np.pi * kx[1] * v + 2.0))
+    vm = (64.0 * vm).astype(np.float32)
+    nb = int(0.02 * w * h / 64)
+    bx = rng.integers(0, w // 8, nb)
+    by = rng.integers(0, h // 8, nb)
+    for ox in range(8):
+        for oy in range(8):
+            vm[by * 8 + oy, bx * 8 + ox] = np.float32(1e30)
+    return img, vm
