@@ -298,7 +298,20 @@ def c3_frames():
     return [(f, dict(back_size=bs, conv=load_mask(m))) for f, bs, m in synth.batch_c3_from_bases(bases)]
 
 
-def run_batch(ctx, frames, reps=2, workers=4, maxobj=400000):
+def host_state(frames):
+    """Host conditions the batch timing depends on (the workers copy frames
+    through pinned memory on host cores): cores, load, memcpy bandwidth."""
+    big = max((f for f, _ in frames), key=lambda f: f.size)
+    dst = np.empty_like(big)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        np.copyto(dst, big)
+    dt = (time.perf_counter() - t0) / 3
+    return {"nproc": os.cpu_count(), "loadavg_1m": round(os.getloadavg()[0], 2),
+            "memcpy_gb_s": round(2 * big.nbytes / dt / 1e9, 2)}
+
+
+def run_batch(ctx, frames, reps=3, workers=4, maxobj=400000):
     """Plain path (sexgpu_extract, one frame after the other) against the
     batched form (sexgpu_extract_batch) on the same frames: host frames in,
     host catalogues out, wall clock around the whole batch; catalogues
@@ -311,6 +324,12 @@ def run_batch(ctx, frames, reps=2, workers=4, maxobj=400000):
 
     ref, got = plain(), batched()  # warm-up (first use allocates the workers' buffers)
     identical = len(ref) == len(got) and all(a.tobytes() == b.tobytes() for a, b in zip(ref, got))
+    differing = []
+    for i, (a, b) in enumerate(zip(ref, got)):
+        if a.tobytes() != b.tobytes() and len(differing) < 5:
+            cols = [n for n in a.dtype.names if len(a) != len(b) or a[n].tobytes() != b[n].tobytes()]
+            differing.append({"frame": i, "shape": list(frames[i][0].shape), "objects": [len(a), len(b)],
+                              "columns": cols[:8]})
     nobj = sum(len(c) for c in ref)
     t_plain = t_batch = float("inf")
     for _ in range(reps):
@@ -331,7 +350,9 @@ def run_batch(ctx, frames, reps=2, workers=4, maxobj=400000):
                       "s": round(t_plain, 4)},
             "batched": {"frames_per_s": round(len(frames) / t_batch, 2),
                         "mobj_per_s": round(nobj / t_batch / 1e6, 4), "s": round(t_batch, 4)},
-            "objects_ratio": round(t_plain / t_batch, 3), "identical_catalogues": bool(identical)}
+            "objects_ratio": round(t_plain / t_batch, 3), "identical_catalogues": bool(identical),
+            "host": host_state(frames),
+            **({"differing": differing} if differing else {})}
 
 
 def algorithmic_bytes(stage, N, s):

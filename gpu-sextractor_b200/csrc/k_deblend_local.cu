@@ -40,6 +40,7 @@ namespace sx {
 #define SX_DL_ARENA_MAX 32767
 #endif
 constexpr int DL_CAP0 = 256;                   // shared-memory tier (one warp per object)
+constexpr int DL_CAP1 = 64;                    // its small-object half (more warps resident per SM)
 constexpr int DL_MID = SX_DL_MID;              // arena tier with 64-thread CTAs up to here, 256 above
 constexpr int DL_ARENA_MAX = SX_DL_ARENA_MAX;  // at most 32767: element indices are 16-bit
 constexpr int DL_SWEEP_BYTES = 45;   // shared bytes per pixel, sweep
@@ -679,28 +680,51 @@ __global__ void __launch_bounds__(NT) k_dl_assign(const __grid_constant__ DebArg
 }
 
 // Size classes (list k at lists + k * nroots, its length in counts[k]):
-//   0  <= 256 pixels             shared memory, one warp
+//   8  <= 64 pixels              shared memory, one warp
+//   0  (64, 256]                 shared memory, one warp
 //   1  (1024, 2048]   2 (256, 1024]       arena, 64 threads
 //   3  > 8192   4 (4096, 8192]   5 (2048, 4096]   arena, 256 threads
 //   6  > 32767 pixels            128-bit global kernels
 //   7  objects the compact sweeps hand over (flux range beyond 64 bits)
-// counts[8..15] are the sweep cursors, counts[16..23] the assignment cursors.
-constexpr int DL_NLISTS = 8;
+// Every list holds its objects largest first (a stable sort of the roots by
+// size), so that the persistent grids start the longest objects first and
+// end on short ones.  counts[DL_NLISTS + k] and counts[2 * DL_NLISTS + k]
+// are the cursors of the sweep and the assignment kernel that takes list k
+// first; counts[3 * DL_NLISTS ...] hold the class boundaries in sorted order.
+constexpr int DL_NLISTS = 9;
 
-__global__ void k_split_roots(const int *size, int n, int *lists, int *counts) {
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ int dl_class(int s) {
+    if (s <= DL_CAP1) return 8;
+    if (s <= DL_CAP0) return 0;
+    if (s <= DL_MID) return s > DL_MID / 2 ? 1 : 2;
+    if (s <= DL_ARENA_MAX) return s > 4 * DL_MID ? 3 : s > 2 * DL_MID ? 4 : 5;
+    return 6;
+}
+
+// sort keys: larger objects first (sizes above 65535 tie, all in class 6)
+__global__ void k_root_keys(const int *size, int n, unsigned *keys, unsigned *vals) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
-    const int s = size[r];
-    int t;
-    if (s <= DL_CAP0)
-        t = 0;
-    else if (s <= DL_MID)
-        t = s > DL_MID / 2 ? 1 : 2;
-    else if (s <= DL_ARENA_MAX)
-        t = s > 4 * DL_MID ? 3 : s > 2 * DL_MID ? 4 : 5;
-    else
-        t = 6;
-    lists[(size_t)t * n + atomicAdd(&counts[t], 1)] = r;
+    keys[r] = 65535u - (unsigned)min(size[r], 65535);
+    vals[r] = (unsigned)r;
+}
+
+// first and last sorted position of every size class present
+__global__ void k_class_bounds(const int *size, const unsigned *sorted, int n, int *bnd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int t = dl_class(size[sorted[i]]);
+    if (i == 0 || dl_class(size[sorted[i - 1]]) != t) bnd[t] = i;
+    if (i == n - 1 || dl_class(size[sorted[i + 1]]) != t) bnd[DL_NLISTS + t] = i;
+}
+
+__global__ void k_class_fill(const int *size, const unsigned *sorted, int n, const int *bnd, int *lists,
+                             int *counts) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int t = dl_class(size[sorted[i]]);
+    lists[(size_t)t * n + (i - bnd[t])] = (int)sorted[i];
+    if (i == bnd[DL_NLISTS + t]) counts[t] = i - bnd[t] + 1;
 }
 
 // resident CTAs of a kernel on this device (cached per kernel and device)
@@ -728,55 +752,71 @@ static RootLists dl_lists(const int *lists, int *counts, size_t n, int a, int b 
     return L;
 }
 
-void launch_deblend_split(const int *size, int nroots, int *lists, int *counts, cudaStream_t st) {
+// keys, vals, kalt, valt: scratch of nroots elements each; tmp: sort scratch
+void launch_deblend_split(const int *size, int nroots, int *lists, int *counts, unsigned *keys, unsigned *vals,
+                          unsigned *kalt, unsigned *valt, int *tmp, cudaStream_t st) {
     cudaMemsetAsync(counts, 0, 3 * DL_NLISTS * sizeof(int), st);
-    if (nroots > 0) k_split_roots<<<(nroots + 255) / 256, 256, 0, st>>>(size, nroots, lists, counts);
+    if (nroots <= 0) return;
+    const unsigned g = (unsigned)((nroots + 255) / 256);
+    k_root_keys<<<g, 256, 0, st>>>(size, nroots, keys, vals);
+    radix_sort_pairs(keys, vals, kalt, valt, nroots, 16, tmp, st);
+    k_class_bounds<<<g, 256, 0, st>>>(size, vals, nroots, counts + 3 * DL_NLISTS);
+    k_class_fill<<<g, 256, 0, st>>>(size, vals, nroots, counts + 3 * DL_NLISTS, lists, counts);
 }
+
+int deblend_split_launches(int nroots) { return nroots > 0 ? 3 + radix_launches(16, nroots) : 0; }
+
+#define DL_SCUR(k) (counts + DL_NLISTS + (k))
+#define DL_ACUR(k) (counts + 2 * DL_NLISTS + (k))
 
 // The large size classes go first, on two side streams, so that their long
 // per-object latency overlaps the many small objects on the main stream; the
 // objects handed over by the compact sweeps are swept last, after the join.
 void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S) {
     if (nroots <= 0) return;
-    static int g0[64], g1[64], g2[64], g3[64];
+    static int g0[64], g1[64], g2[64], g3[64], g4[64];
     const size_t n = (size_t)nroots;
     int *glist = const_cast<int *>(lists) + 7 * n;
-    const size_t m0 = DL_CAP0 * DL_SWEEP_BYTES;
+    const size_t m0 = DL_CAP0 * DL_SWEEP_BYTES, m1 = DL_CAP1 * DL_SWEEP_BYTES;
     cudaEventRecord(S.fork, S.main);
     cudaStreamWaitEvent(S.side[0], S.fork, 0);
     cudaStreamWaitEvent(S.side[1], S.fork, 0);
     const int grid3 = min(nroots, dl_grid(k_deblend_sweep, DB_THREADS, 0, g3));
-    k_deblend_sweep<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 6 * n, counts + 6, counts + 14);
+    k_deblend_sweep<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 6 * n, counts + 6, DL_SCUR(6));
     k_dl_sweep<256><<<min(nroots, dl_grid(k_dl_sweep<256>, 256, 0, g2)), 256, 0, S.side[1]>>>(
-        A, dl_lists(lists, counts, n, 3, 4, 5), counts + 10, 0, glist, counts + 7);
+        A, dl_lists(lists, counts, n, 3, 4, 5), DL_SCUR(3), 0, glist, counts + 7);
     k_dl_sweep<64><<<min(nroots, dl_grid(k_dl_sweep<64>, 64, 0, g1)), 64, 0, S.main>>>(
-        A, dl_lists(lists, counts, n, 1, 2), counts + 9, 0, glist, counts + 7);
+        A, dl_lists(lists, counts, n, 1, 2), DL_SCUR(1), 0, glist, counts + 7);
     k_dl_sweep<32><<<min(nroots, dl_grid(k_dl_sweep<32>, 32, m0, g0)), 32, m0, S.main>>>(
-        A, dl_lists(lists, counts, n, 0), counts + 8, DL_CAP0, glist, counts + 7);
+        A, dl_lists(lists, counts, n, 0), DL_SCUR(0), DL_CAP0, glist, counts + 7);
+    k_dl_sweep<32><<<min(nroots, dl_grid(k_dl_sweep<32>, 32, m1, g4)), 32, m1, S.main>>>(
+        A, dl_lists(lists, counts, n, 8), DL_SCUR(8), DL_CAP1, glist, counts + 7);
     cudaEventRecord(S.join[0], S.side[0]);
     cudaEventRecord(S.join[1], S.side[1]);
     cudaStreamWaitEvent(S.main, S.join[0], 0);
     cudaStreamWaitEvent(S.main, S.join[1], 0);
-    k_deblend_sweep<<<grid3, DB_THREADS, 0, S.main>>>(A, glist, counts + 7, counts + 15);
+    k_deblend_sweep<<<grid3, DB_THREADS, 0, S.main>>>(A, glist, counts + 7, DL_SCUR(7));
 }
 
 void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S) {
     if (nroots <= 0) return;
-    static int g0[64], g1[64], g2[64], g3[64];
+    static int g0[64], g1[64], g2[64], g3[64], g4[64];
     const size_t n = (size_t)nroots;
-    const size_t m0 = DL_CAP0 * DL_ASSIGN_BYTES;
+    const size_t m0 = DL_CAP0 * DL_ASSIGN_BYTES, m1 = DL_CAP1 * DL_ASSIGN_BYTES;
     cudaEventRecord(S.fork, S.main);
     cudaStreamWaitEvent(S.side[0], S.fork, 0);
     cudaStreamWaitEvent(S.side[1], S.fork, 0);
     const int grid3 = min(nroots, dl_grid(k_deblend_assign, DB_THREADS, 0, g3));
-    k_deblend_assign<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 6 * n, counts + 6, counts + 22);
-    k_deblend_assign<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 7 * n, counts + 7, counts + 23);
+    k_deblend_assign<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 6 * n, counts + 6, DL_ACUR(6));
+    k_deblend_assign<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 7 * n, counts + 7, DL_ACUR(7));
     k_dl_assign<256><<<min(nroots, dl_grid(k_dl_assign<256>, 256, 0, g2)), 256, 0, S.side[1]>>>(
-        A, dl_lists(lists, counts, n, 3, 4, 5), counts + 18, 0);
+        A, dl_lists(lists, counts, n, 3, 4, 5), DL_ACUR(3), 0);
     k_dl_assign<64><<<min(nroots, dl_grid(k_dl_assign<64>, 64, 0, g1)), 64, 0, S.main>>>(
-        A, dl_lists(lists, counts, n, 1, 2), counts + 17, 0);
+        A, dl_lists(lists, counts, n, 1, 2), DL_ACUR(1), 0);
     k_dl_assign<32><<<min(nroots, dl_grid(k_dl_assign<32>, 32, m0, g0)), 32, m0, S.main>>>(
-        A, dl_lists(lists, counts, n, 0), counts + 16, DL_CAP0);
+        A, dl_lists(lists, counts, n, 0), DL_ACUR(0), DL_CAP0);
+    k_dl_assign<32><<<min(nroots, dl_grid(k_dl_assign<32>, 32, m1, g4)), 32, m1, S.main>>>(
+        A, dl_lists(lists, counts, n, 8), DL_ACUR(8), DL_CAP1);
     cudaEventRecord(S.join[0], S.side[0]);
     cudaEventRecord(S.join[1], S.side[1]);
     cudaStreamWaitEvent(S.main, S.join[0], 0);

@@ -45,7 +45,7 @@ constexpr int KR_THREADS = 256;
 constexpr int KR_GRID = 2 * 148;
 constexpr int KR_ITEMS = 8192;     // queued boxes per pass
 constexpr int KR_CHUNKS = 65536;   // work items per pass (2^29 box pixels)
-constexpr int KR_WARP_MAX = 32768; // default: larger boxes are queued
+constexpr int KR_WARP_MAX = 8192;  // default: larger boxes are queued
 
 struct KronGeo {
     float cx2, cy2, cxy, klim2;
@@ -125,7 +125,9 @@ struct DebStreams {
     cudaEvent_t fork, join[2];
 };
 
-void launch_deblend_split(const int *size, int nroots, int *lists, int *counts, cudaStream_t st);
+void launch_deblend_split(const int *size, int nroots, int *lists, int *counts, unsigned *keys, unsigned *vals,
+                          unsigned *kalt, unsigned *valt, int *tmp, cudaStream_t st);
+int deblend_split_launches(int nroots);
 void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S);
 void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S);
 

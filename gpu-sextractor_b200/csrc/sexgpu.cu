@@ -653,7 +653,7 @@ int pipe_deblend(sexgpu_ctx *ctx) {
     A.mincont = Pm.mincont;
     A.wdiv = make_fastdiv((unsigned)w);
     EN(rlists, (size_t)(DL_NLISTS * (nroots + 1)) * 4);
-    EN(rcounts, 3 * DL_NLISTS * 4);
+    EN(rcounts, 5 * DL_NLISTS * 4);
     DebStreams S;
     S.main = st;
     S.side[0] = ctx->side[0];
@@ -661,7 +661,8 @@ int pipe_deblend(sexgpu_ctx *ctx) {
     S.fork = ctx->ev_fork;
     S.join[0] = ctx->ev_join[0];
     S.join[1] = ctx->ev_join[1];
-    launch_deblend_split(R.size, nroots, P<int>(ctx->rlists), P<int>(ctx->rcounts), st);
+    launch_deblend_split(R.size, nroots, P<int>(ctx->rlists), P<int>(ctx->rcounts), P<unsigned>(ctx->keys),
+                         P<unsigned>(ctx->vals), P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), tmp, st);
     launch_deblend_sweep(A, P<int>(ctx->rlists), P<int>(ctx->rcounts), nroots, S);
     exclusive_scan(R.nkept, R.objbase, nroots, &d_sc->nobj, tmp, st);
     rc = read_scalars(ctx);
@@ -671,7 +672,7 @@ int pipe_deblend(sexgpu_ctx *ctx) {
     if (rc) return rc;
     A.O = ctx->O;
     launch_deblend_assign(A, P<int>(ctx->rlists), P<int>(ctx->rcounts), nroots, S);
-    stage_mark(ctx, "deblend", 11 + scan_launches(nroots));
+    stage_mark(ctx, "deblend", 12 + deblend_split_launches(nroots) + scan_launches(nroots));
     ps.stage = 3;
     return SEXGPU_OK;
 }

@@ -231,7 +231,7 @@ int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max);
 /* Execution parameters of this context (and of its batch workers); results
  * do not depend on them.  "kron_warp_max": AUTO-photometry boxes of more
  * pixels than this are summed by whole thread blocks instead of one warp
- * (default 32768, >= 1).  Returns SEXGPU_ERR_ARG for an unknown name or value. */
+ * (default 8192, >= 1).  Returns SEXGPU_ERR_ARG for an unknown name or value. */
 int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value);
 
 #ifdef __cplusplus
