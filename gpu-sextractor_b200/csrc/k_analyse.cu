@@ -13,6 +13,9 @@
 namespace sx {
 
 constexpr int AN_WARPS = 8;
+// four resident CTAs per SM (at most 64 registers): these kernels wait on
+// pixel-list loads, and residency hides that better than registers saved
+constexpr int AN_MINB = 4;
 
 __device__ __forceinline__ unsigned warp_max_u(unsigned v) {
     for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -106,7 +109,7 @@ struct AnaArgs {
 // Robust preanalysis of a deblended object over its final pixels
 // (src/cuda/cudaanalyse.cu:1906-2124); objects of level 0 kept the values of
 // the first preanalysis.
-__global__ void __launch_bounds__(AN_WARPS * 32) k_analyse_robust(AnaArgs A) {
+__global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(AnaArgs A) {
     const int lane = threadIdx.x & 31;
     const int o = blockIdx.x * AN_WARPS + (threadIdx.x >> 5);
     if (o >= A.nobj || A.O.level[o] == 0) return;
@@ -239,7 +242,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32) k_analyse_robust(AnaArgs A) {
 
 // examineiso (src/cuda/cudaanalyse.cu:2176-2581) and the CLEAN threshold
 // mthresh of every object.
-__global__ void __launch_bounds__(AN_WARPS * 32) k_examineiso(AnaArgs A) {
+__global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A) {
     __shared__ __align__(16) unsigned hist[AN_WARPS][256];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int o = blockIdx.x * AN_WARPS + wid;

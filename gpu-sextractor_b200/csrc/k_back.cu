@@ -94,74 +94,107 @@ __global__ void k_mesh_stat(const float *__restrict__ img, int w, int h, int bw,
 }
 
 // One warp per row band of 32 meshes, one lane per mesh.  The band's pixel
-// rows are staged in shared memory one at a time (double buffered with
-// cp.async, coalesced across the band); every lane then adds its mesh's part
-// of the row to its own sums, so each lane performs the reference's sequential
-// double sums in the reference's pixel order.  Mesh j of the band sits at
-// j * stride in the row buffer; an odd stride keeps the lanes' reads on
-// distinct banks.
-__device__ __forceinline__ void band_row_async(float *dst, const float *img, int w, int gy, int x0, int bw, int mw_last,
-                                               int nmesh, int stride) {
+// rows are staged in shared memory by cp.async (coalesced across the band) in
+// a ring of BAND_STAGES rows, so that the loads of the next rows are in
+// flight while the lanes add the current one; every lane then adds its mesh's
+// part of the row to its own sums, so each lane performs the reference's
+// sequential double sums in the reference's pixel order.  Mesh j of the band
+// sits at j * stride in a row buffer.  VEC (frame width and mesh width
+// multiples of 4): 16-byte copies, float4 reads, stride = 4 (mod 8) so that
+// the eight lanes of a float4 read phase hit distinct banks; otherwise 4-byte
+// copies and an odd stride.
+constexpr int BAND_STAGES = 4;
+
+template <bool VEC>
+__device__ __forceinline__ void band_row_async(float *dst, const float *img, int w, int gy, int x0, int bw, int tw,
+                                               int stride) {
     const int lane = threadIdx.x & 31;
     const float *src = img + (size_t)gy * w + x0;
-    for (int j = 0; j < nmesh; j++) {
-        const int mw = j == nmesh - 1 ? mw_last : bw;
-        for (int x = lane; x < mw; x += 32) {
-            const unsigned d = (unsigned)__cvta_generic_to_shared(dst + j * stride + x);
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src + (size_t)j * bw + x)
-                         : "memory");
+    if (VEC) {
+        for (int c = lane; 4 * c < tw; c += 32) {
+            const int j = (4 * c) / bw;
+            const unsigned d = (unsigned)__cvta_generic_to_shared(dst + j * stride + (4 * c - j * bw));
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src + 4 * c) : "memory");
+        }
+    } else {
+        for (int c = lane; c < tw; c += 32) {
+            const int j = c / bw;
+            const unsigned d = (unsigned)__cvta_generic_to_shared(dst + j * stride + (c - j * bw));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src + c) : "memory");
         }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
+// the two accumulation loops of one row (pass 0: valid pixels; pass 1:
+// pixels inside [lcut, hcut])
+template <int PASS>
+__device__ __forceinline__ void band_add(double pix, float lcut, float hcut, double &mean, double &sigma, int &npix) {
+    const bool in = PASS == 0 ? pix > -SX_BIG : (pix <= hcut && pix >= lcut);
+    mean += in ? pix : 0.0;
+    sigma += in ? pix * pix : 0.0;
+    npix += in;
+}
+
+template <int PASS, bool VEC>
+__device__ __forceinline__ void band_row_add(const float *row, int mw, float lcut, float hcut, double &mean,
+                                             double &sigma, int &npix) {
+    if (VEC) {
+        const float4 *r4 = reinterpret_cast<const float4 *>(row);
+#pragma unroll 4
+        for (int q = 0; q < (mw >> 2); q++) {
+            const float4 v = r4[q];
+            band_add<PASS>(v.x, lcut, hcut, mean, sigma, npix);
+            band_add<PASS>(v.y, lcut, hcut, mean, sigma, npix);
+            band_add<PASS>(v.z, lcut, hcut, mean, sigma, npix);
+            band_add<PASS>(v.w, lcut, hcut, mean, sigma, npix);
+        }
+    } else {
+#pragma unroll 8
+        for (int x = 0; x < mw; x++) band_add<PASS>(row[x], lcut, hcut, mean, sigma, npix);
+    }
+}
+
+template <bool VEC>
 __global__ void __launch_bounds__(32) k_mesh_stat_band(const float *__restrict__ img, int w, int h, int bw, int bh,
                                                        int nbx, int nby, int stride, MeshStat *__restrict__ ms) {
-    extern __shared__ float band_smem[];
+    extern __shared__ __align__(16) float band_smem[];
     const int lane = threadIdx.x;
     const int mx0 = blockIdx.x * 32, my = blockIdx.y;
     const int nmesh = min(32, nbx - mx0);
     const int x0 = mx0 * bw, y0 = my * bh;
     const int mh = (my == nby - 1 && h % bh) ? h % bh : bh;
     const int mw_last = (mx0 + nmesh == nbx && w % bw) ? w % bw : bw;
+    const int tw = (nmesh - 1) * bw + mw_last;  // band width in pixels
     const bool active = lane < nmesh;
     const int mw = lane == nmesh - 1 ? mw_last : bw;
-    float *buf[2] = {band_smem, band_smem + 32 * stride};
-    double pix, sig, mean = 0.0, sigma = 0.0;
+    const int rowf = 32 * stride;  // floats per staged row
+    double sig, mean = 0.0, sigma = 0.0;
     const double step = sqrt(2 / SX_PI) * SX_QUANTIF_NSIGMA / SX_QUANTIF_AMIN;
     int npix = 0;
     float lcut = 0.0f, hcut = 0.0f;
     bool bad = false;
     for (int pass = 0; pass < 2; pass++) {
-        band_row_async(buf[0], img, w, y0, x0, bw, mw_last, nmesh, stride);
-        for (int y = 0; y < mh; y++) {
-            if (y + 1 < mh)
-                band_row_async(buf[(y + 1) & 1], img, w, y0 + y + 1, x0, bw, mw_last, nmesh, stride);
+        for (int y = 0; y < BAND_STAGES - 1; y++) {
+            if (y < mh)
+                band_row_async<VEC>(band_smem + y * rowf, img, w, y0 + y, x0, bw, tw, stride);
             else
                 asm volatile("cp.async.commit_group;" ::: "memory");
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        }
+        for (int y = 0; y < mh; y++) {
+            const int ya = y + BAND_STAGES - 1;
+            if (ya < mh)
+                band_row_async<VEC>(band_smem + (ya % BAND_STAGES) * rowf, img, w, y0 + ya, x0, bw, tw, stride);
+            else
+                asm volatile("cp.async.commit_group;" ::: "memory");
+            asm volatile("cp.async.wait_group %0;" ::"n"(BAND_STAGES - 1) : "memory");
             __syncwarp();
             if (active) {
-                const float *row = buf[y & 1] + lane * stride;
-                if (pass == 0) {
-#pragma unroll 8
-                    for (int x = 0; x < mw; x++) {
-                        pix = row[x];
-                        const bool in = pix > -SX_BIG;
-                        mean += in ? pix : 0.0;
-                        sigma += in ? pix * pix : 0.0;
-                        npix += in;
-                    }
-                } else {
-#pragma unroll 8
-                    for (int x = 0; x < mw; x++) {
-                        pix = row[x];
-                        const bool in = pix <= hcut && pix >= lcut;
-                        mean += in ? pix : 0.0;
-                        sigma += in ? pix * pix : 0.0;
-                        npix += in;
-                    }
-                }
+                const float *row = band_smem + (y % BAND_STAGES) * rowf + lane * stride;
+                if (pass == 0)
+                    band_row_add<0, VEC>(row, mw, lcut, hcut, mean, sigma, npix);
+                else
+                    band_row_add<1, VEC>(row, mw, lcut, hcut, mean, sigma, npix);
             }
             __syncwarp();
         }
@@ -227,13 +260,15 @@ __global__ void __launch_bounds__(GUESS_THREADS) k_mesh_guess(const float *__res
     int nlevels = bm.nlevels;
     float qscale = bm.qscale;
     float cste = 0.499999 - bm.qzero / qscale;
-    int np = mw * mh;
-    for (int i = threadIdx.x; i < np; i += GUESS_THREADS) {
-        float p = __ldg(img + (size_t)(y0 + i / mw) * w + x0 + i % mw);
-        float b = p / qscale + cste;
-        if (b != b) continue;  // NaN: the host conversion yields INT_MIN
-        int bin = (int)b;
-        if (bin >= 0 && bin < nlevels) atomicAdd(&hist[bin], 1);
+    // one warp per mesh row, lanes along the row (no index division)
+    for (int r = threadIdx.x >> 5; r < mh; r += GUESS_THREADS / 32) {
+        const float *row = img + (size_t)(y0 + r) * w + x0;
+        for (int x = threadIdx.x & 31; x < mw; x += 32) {
+            float b = __ldg(row + x) / qscale + cste;
+            if (b != b) continue;  // NaN: the host conversion yields INT_MIN
+            int bin = (int)b;
+            if (bin >= 0 && bin < nlevels) atomicAdd(&hist[bin], 1);
+        }
     }
     __syncthreads();
     // exclusive prefix of the histogram: 17 consecutive bins per thread
@@ -659,19 +694,33 @@ void launch_weight_var(const BackBufs &B, const float *wmap, const FrameParams &
 void launch_background(BackBufs &B, const float *img, const FrameParams &P, FrameScalars *d_sc,
                        cudaStream_t st, int &launches) {
     int nb = P.nbx * P.nby;
-    // row-band kernel when two rows of 32 meshes fit in 96 KB of shared memory
-    const int stride = P.bw + ((P.bw & 1) ? 2 : 1);
-    const size_t band_bytes = 2 * 32 * (size_t)stride * sizeof(float);
-    if (band_bytes <= 96 * 1024) {
+    // row-band kernel when BAND_STAGES rows of 32 meshes fit in 200 KB of
+    // shared memory
+    const bool vec = (P.w % 4) == 0 && (P.bw % 4) == 0 && ((uintptr_t)img & 15) == 0;
+    int stride;
+    if (vec) {
+        stride = (P.bw + 3) & ~3;
+        if (((stride >> 2) & 1) == 0) stride += 4;  // stride / 4 odd
+    } else {
+        stride = P.bw | 1;  // odd
+    }
+    const size_t band_bytes = (size_t)BAND_STAGES * 32 * stride * sizeof(float);
+    constexpr int BAND_SMEM_MAX = 200 * 1024;
+    if (band_bytes <= BAND_SMEM_MAX) {
         static bool attr_set[64];
         int dev = 0;
         cudaGetDevice(&dev);
         if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-            cudaFuncSetAttribute(k_mesh_stat_band, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+            cudaFuncSetAttribute(k_mesh_stat_band<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, BAND_SMEM_MAX);
+            cudaFuncSetAttribute(k_mesh_stat_band<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, BAND_SMEM_MAX);
             attr_set[dev] = true;
         }
         dim3 grid((P.nbx + 31) / 32, P.nby);
-        k_mesh_stat_band<<<grid, 32, band_bytes, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, stride, B.ms);
+        if (vec)
+            k_mesh_stat_band<true><<<grid, 32, band_bytes, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, stride, B.ms);
+        else
+            k_mesh_stat_band<false><<<grid, 32, band_bytes, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, stride,
+                                                                   B.ms);
     } else {
         k_mesh_stat<<<(nb + 127) / 128, 128, 0, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, B.ms);
     }

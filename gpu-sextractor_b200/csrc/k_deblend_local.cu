@@ -663,8 +663,11 @@ __global__ void __launch_bounds__(NT) k_dl_sweep(const __grid_constant__ DebArgs
     }
 }
 
+// at most 64 registers (32 one-warp, 16 two-warp or 4 eight-warp CTAs per
+// SM): the assignment waits on its chain walks and gathers, so residency
+// pays more than the registers it costs
 template <int NT>
-__global__ void __launch_bounds__(NT) k_dl_assign(const __grid_constant__ DebArgs A, const RootLists L, int *cursor,
+__global__ void __launch_bounds__(NT, NT == 32 ? 32 : NT == 64 ? 16 : 4) k_dl_assign(const __grid_constant__ DebArgs A, const RootLists L, int *cursor,
                                                   int cap) {
     extern __shared__ __align__(16) unsigned char dl_smem[];
     __shared__ int s_item;

@@ -380,21 +380,42 @@ __device__ __forceinline__ void sunion(int *L, int a, int b) {
     }
 }
 
-// labels within one tile, union in shared memory
+// Labels within one 32 x CC_TH tile, one warp per tile row.  A row's
+// foreground is one ballot; pixels of a horizontal run are connected
+// through the run's first pixel (bit arithmetic, no unions); a run joins the
+// runs of the row above that touch it or its two diagonal ends (8-connected)
+// with one union each, in shared memory.  Every link goes to a smaller tile
+// index, so each tile component ends at its smallest pixel.
+__device__ __forceinline__ int run_start(unsigned starts, int b) {  // start bit of the run holding bit b
+    return 31 - __clz(starts & (0xffffffffu >> (31 - b)));
+}
+__device__ __forceinline__ int run_end(unsigned m, int b) {  // last bit of the run holding bit b
+    return b + __ffsll(~(unsigned long long)(m >> b)) - 2;     // 64-bit: a run may reach bit 31
+}
+
 __global__ void __launch_bounds__(CC_TW *CC_TH) k_ccl_local(int *__restrict__ lab, int w, int h) {
     __shared__ int L[CC_TH * CC_TW];
-    int lx = threadIdx.x, ly = threadIdx.y, t = ly * CC_TW + lx;
-    int gx = blockIdx.x * CC_TW + lx, gy = blockIdx.y * CC_TH + ly;
-    bool in = gx < w && gy < h;
-    bool fg = in && lab[(size_t)gy * w + gx] >= 0;
-    L[t] = fg ? t : -1;
+    __shared__ unsigned rowm[CC_TH];
+    const int lx = threadIdx.x, ly = threadIdx.y, t = ly * CC_TW + lx;
+    const int gx = blockIdx.x * CC_TW + lx, gy = blockIdx.y * CC_TH + ly;
+    const bool in = gx < w && gy < h;
+    const bool fg = in && lab[(size_t)gy * w + gx] >= 0;
+    const unsigned m = __ballot_sync(0xffffffffu, fg);
+    const unsigned starts = m & ~(m << 1);
+    if (lx == 0) rowm[ly] = m;
+    L[t] = fg ? ly * CC_TW + run_start(starts, lx) : -1;
     __syncthreads();
-    if (fg) {
-        if (lx > 0 && L[t - 1] >= 0) sunion(L, t, t - 1);
-        if (ly > 0) {
-            if (lx > 0 && L[t - CC_TW - 1] >= 0) sunion(L, t, t - CC_TW - 1);
-            if (L[t - CC_TW] >= 0) sunion(L, t, t - CC_TW);
-            if (lx < CC_TW - 1 && L[t - CC_TW + 1] >= 0) sunion(L, t, t - CC_TW + 1);
+    if (fg && ly > 0 && ((starts >> lx) & 1u)) {
+        const int e = run_end(m, lx);
+        const int s1 = lx > 0 ? lx - 1 : 0, e1 = e < 31 ? e + 1 : 31;
+        const unsigned dil = (unsigned)((2ull << e1) - 1ull) & ~((1u << s1) - 1u);
+        const unsigned mp = rowm[ly - 1], sp = mp & ~(mp << 1);
+        unsigned ov = mp & dil;
+        while (ov) {
+            const int b = __ffs(ov) - 1;
+            sunion(L, t, (ly - 1) * CC_TW + run_start(sp, b));
+            const int eb = run_end(mp, b);
+            ov = eb >= 31 ? 0u : ov & ~((2u << eb) - 1u);
         }
     }
     __syncthreads();

@@ -549,8 +549,8 @@ __device__ void kron_after1(const EndArgs &A, int o, double mx, double my, int f
     end_finish(A, o, flags, kron, true, p2);
 }
 
-// one warp per surviving object
-__global__ void k_endobject(EndArgs A) {
+// one warp per surviving object (eight CTAs of four warps per SM)
+__global__ void __launch_bounds__(128, 8) k_endobject(EndArgs A) {
     const int lane = threadIdx.x & 31;
     const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (o >= A.n) return;
