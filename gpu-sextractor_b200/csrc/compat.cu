@@ -96,7 +96,7 @@ __global__ void k_compat_rows(ObjBufs O, int n, sexgpu_outobj *rows) {
     q.kronfactor = O.kron[o];
     q.bkg = O.bkg[o];
     q.fwhm = O.fwhm[o];
-    rows[o] = q;
+    memcpy(rows + o, &q, sizeof(q));  // padding bytes too
 }
 
 }  // namespace

@@ -716,7 +716,9 @@ __global__ void k_write_rows(ObjBufs O, const unsigned *vals, int ns, float dthr
     q.elong = q.a / q.b;
     q.ellip = 1 - q.b / q.a;
     q.polar = (q.a * q.a - q.b * q.b) / (q.a * q.a + q.b * q.b);
-    rows[k] = q;
+    // byte copy: an assignment may store the members only and leave the
+    // padding of the destination row as it was
+    memcpy(rows + k, &q, sizeof(q));
 }
 
 // segmentation map: NUMBER of the owning object, 0 elsewhere
