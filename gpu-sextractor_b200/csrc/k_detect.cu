@@ -152,141 +152,219 @@ __device__ __forceinline__ void conv_rows_any(const float *__restrict__ mask, co
     }
 }
 
-template <int MW, int MH>
-__global__ void __launch_bounds__(ST_THREADS) k_sub_filter_tma(const __grid_constant__ CUtensorMap tmap,
-                                                               float *__restrict__ sub, float *__restrict__ cd,
-                                                               int *__restrict__ lab, BackBufs B, int w, int h,
-                                                               int nbx, int back_type,
-                                                               const __grid_constant__ ConvTaps taps,
-                                                               const float *__restrict__ mask, int mw, int mh,
-                                                               int rxa, const float *__restrict__ wvar, int wthr,
-                                                               double dfac, FrameScalars *sc) {
-    __shared__ __align__(128) float tile[ST_MAXBH * ST_MAXBW];
-    __shared__ int s_colk[ST_MAXBW];
-    __shared__ float s_coldx[ST_MAXBW];
-    __shared__ __align__(8) unsigned long long bar;
-    if constexpr (MW > 0) {
-        mw = MW;
-        mh = MH;
-    }
-    const int rx = mw / 2, ry = mh / 2;
-    const int bw = ST_TW + 2 * rxa, bh = ST_TH + 2 * ry;
-    const int x0 = blockIdx.x * ST_TW, y0 = blockIdx.y * ST_TH;
-    const int tid = threadIdx.x, lane = tid & 31;
-    const unsigned bar_a = smem_u32(&bar);
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_a), "r"(1));
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
-    __syncthreads();
-    if (tid == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a),
-                     "r"((unsigned)(bw * bh * 4))
-                     : "memory");
-        asm volatile(
-            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
-                "r"(smem_u32(tile)),
-            "l"(&tmap), "r"(x0 - rxa), "r"(y0 - ry), "r"(bar_a)
-            : "memory");
-    }
-    // column table of the tile while the load is in flight
-    for (int i = tid; i < bw; i += ST_THREADS) {
-        const int gx = x0 - rxa + i;
-        const bool in = gx >= 0 && gx < w;
-        s_colk[i] = in ? B.colk[gx] : 0;
-        s_coldx[i] = in ? B.coldx[gx] : 0.0f;
-    }
+// ---------------------------------------------------------------------------
+// Persistent form: each CTA walks tiles t, t + G, ... with two tile buffers;
+// the TMA load of the next tile is in flight while the current one is
+// subtracted, filtered and thresholded.  Per tile the spline column constants
+// (segment, dx, 1 - dx and the two cubic factors, all the float values the
+// per-pixel formula uses) sit in each lane's registers (a lane keeps its four
+// columns for the whole tile) and the row nodes of the tile's rows are staged
+// in shared memory, so the per-pixel background is shared-memory reads and
+// float arithmetic in the reference's order.
+// ---------------------------------------------------------------------------
+constexpr int SP_NK = 16;  // staged spline nodes per row (segments touching a tile + 1)
+
+struct SpArgs {
+    float *sub, *cd;
+    int *lab;
+    BackBufs B;
+    int w, h, nbx, back_type, mw, mh, rxa, wthr, tilesx, ntiles;
+    double dfac;
+    const float *mask, *wvar;
+    FrameScalars *sc;
+};
+
+__device__ __forceinline__ void sp_issue(const CUtensorMap *tmap, float *buf, unsigned bar, int x, int y,
+                                         unsigned bytes) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(smem_u32(buf)),
+        "l"(tmap), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ bool sp_wait(unsigned bar, unsigned parity) {
     unsigned done = 0;
     for (unsigned it = 0; it < ST_WAIT_LIMIT && !done; it++)
         asm volatile(
             "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
             : "=r"(done)
-            : "r"(bar_a), "r"(0u)
+            : "r"(bar), "r"(parity)
             : "memory");
-    if (!__syncthreads_and(done)) {
-        // the load did not complete in time: report it, give the copy one more
-        // bounded wait so that it is not left writing into a finished CTA's
-        // shared memory, and leave the outputs untouched
-        if (tid == 0) {
-            atomicOr(&sc->status, SX_ST_LOOP);
-            for (unsigned it = 0; it < ST_WAIT_LIMIT && !done; it++)
-                asm volatile(
-                    "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-                    : "=r"(done)
-                    : "r"(bar_a), "r"(0u)
-                    : "memory");
-        }
-        return;
-    }
-    const float backmean = sc->backmean, dthresh = sc->dthresh;
-    // subtract the background in place, one warp per tile row; outside the
-    // frame the value is 0
-    int emin = 1000;
-    for (int ty = tid >> 5; ty < bh; ty += ST_THREADS / 32) {
-        const int gy = y0 - ry + ty;
-        float *trow = tile + ty * bw;
-        if (gy < 0 || gy >= h) {
-            for (int tx = lane; tx < bw; tx += 32) trow[tx] = 0.0f;
-            continue;
-        }
-        const float *nd = B.rownode + (size_t)gy * nbx;
-        const float *dnd = B.rowdnode + (size_t)gy * nbx;
-        const bool inner_row = ty >= ry && ty < ry + ST_TH;
-        for (int tx = lane; tx < bw; tx += 32) {
-            const int gx = x0 - rxa + tx;
-            float s = 0.0f;
-            if (gx >= 0 && gx < w) {
-                float b;
-                if (back_type == 1) {
-                    b = backmean;
-                } else if (nbx <= 1) {
-                    b = __ldg(nd);
-                } else {
-                    const int k = s_colk[tx];
-                    const float dx = s_coldx[tx], cdx = 1 - dx;
-                    b = (float)(cdx * (__ldg(nd + k) + (cdx * cdx - 1) * __ldg(dnd + k)) +
-                                dx * (__ldg(nd + k + 1) + (dx * dx - 1) * __ldg(dnd + k + 1)));
-                }
-                s = sx_unblank(trow[tx]) - b;
-                if (inner_row && tx >= rxa && tx < rxa + ST_TW) {
-                    sub[(size_t)gy * w + gx] = s;
-                    const unsigned ef = (__float_as_uint(s) >> 23) & 0xff;
-                    if (ef) emin = min(emin, (int)ef - 127);
-                }
-            }
-            trow[tx] = s;
-        }
+    return done != 0;
+}
+
+template <int MW, int MH, bool WEIGHTED>
+__global__ void __launch_bounds__(ST_THREADS) k_sub_filter_pipe(const __grid_constant__ CUtensorMap tmap,
+                                                                const __grid_constant__ SpArgs A,
+                                                                const __grid_constant__ ConvTaps taps) {
+    extern __shared__ __align__(128) float sp_smem[];
+    __shared__ __align__(8) unsigned long long bars[2];
+    __shared__ float s_nd[ST_MAXBH][SP_NK], s_dnd[ST_MAXBH][SP_NK];
+    __shared__ int s_kmin, s_nk;
+    const int mw = MW > 0 ? MW : A.mw, mh = MH > 0 ? MH : A.mh;
+    const int rx = mw / 2, ry = mh / 2, rxa = A.rxa;
+    const int bw = ST_TW + 2 * rxa, bh = ST_TH + 2 * ry;
+    const int tsz = (bw * bh + 31) & ~31;  // floats per tile buffer (128-byte multiple)
+    float *const buf0 = sp_smem, *const buf1 = sp_smem + tsz;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int w = A.w, h = A.h;
+    const unsigned bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+    const unsigned tbytes = (unsigned)(bw * bh * 4);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar1), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    // convolution, threshold, label seed
-    int nabove = 0;
-    const int cx = tid & (ST_TW - 1), r0 = (tid / ST_TW) * ST_RPT;
-    float acc[ST_RPT];
-    if constexpr (MW > 0)
-        conv_rows<MW, MH>(taps, tile, bw, cx + rxa - rx, r0, acc);
-    else
-        conv_rows_any(mask, tile, bw, cx + rxa - rx, r0, mw, mh, acc);
-    const int gx = x0 + cx;
-#pragma unroll
-    for (int k = 0; k < ST_RPT; k++) {
-        const int gy = y0 + r0 + k;
-        if (gx < w && gy < h) {
-            const size_t p = (size_t)gy * w + gx;
-            cd[p] = acc[k];
-            // with a weight map: unusable pixels never, others against the local rms
-            const float v = wvar ? __ldg(wvar + p) : 0.0f;
-            const bool fg = !(wvar && !(v < 1e30f)) && acc[k] >= sx_pix_thr(wthr, dfac, v, dthresh);
-            lab[p] = fg ? (int)p : -1;
-            nabove += fg;
+    int t = blockIdx.x;
+    if (tid == 0 && t < A.ntiles)
+        sp_issue(&tmap, buf0, bar0, (t % A.tilesx) * ST_TW - rxa, (t / A.tilesx) * ST_TH - ry, tbytes);
+    const float backmean = A.sc->backmean, dthresh = A.sc->dthresh;
+    int emin = 1000, nabove = 0;
+    bool failed = false;
+    for (int it = 0; t < A.ntiles; it++, t += gridDim.x) {
+        const int cur = it & 1;
+        float *const tile = cur ? buf1 : buf0;
+        const int x0 = (t % A.tilesx) * ST_TW, y0 = (t / A.tilesx) * ST_TH;
+        // next tile into the other buffer (free: the previous iteration ended
+        // with a barrier after its last read)
+        const int tn = t + gridDim.x;
+        if (tid == 0 && tn < A.ntiles)
+            sp_issue(&tmap, cur ? buf0 : buf1, cur ? bar0 : bar1, (tn % A.tilesx) * ST_TW - rxa,
+                     (tn / A.tilesx) * ST_TH - ry, tbytes);
+        // spline row nodes of this tile's rows, while the load is in flight
+        const int gxa = x0 - rxa;
+        const bool spline = A.back_type != 1 && A.nbx > 1;
+        if (spline && tid == 0) {
+            const int ka = A.B.colk[max(gxa, 0)], kb = A.B.colk[min(gxa + bw, w) - 1];
+            s_kmin = ka;
+            s_nk = kb - ka + 2;
         }
+        __syncthreads();
+        const int kmin = spline ? s_kmin : 0, nk = spline ? s_nk : 0;
+        const bool staged = nk <= SP_NK;
+        if (spline && staged)
+            for (int i = tid; i < bh * nk; i += ST_THREADS) {
+                const int ty = i / nk, j = i - ty * nk, gy = y0 - ry + ty;
+                const int k = min(kmin + j, A.nbx - 1);
+                const bool in = gy >= 0 && gy < h;
+                s_nd[ty][j] = in ? A.B.rownode[(size_t)gy * A.nbx + k] : 0.0f;
+                s_dnd[ty][j] = in ? A.B.rowdnode[(size_t)gy * A.nbx + k] : 0.0f;
+            }
+        // this lane's tile columns: 4*lane .. 4*lane+3 (lanes beyond the tile idle)
+        int ck[4];
+        float cdx[4], cb[4], cx[4], cdd[4];
+        bool cin[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int tx = 4 * lane + q, gx = gxa + tx;
+            cin[q] = tx < bw && gx >= 0 && gx < w;
+            const int gxc = min(max(gx, 0), w - 1);
+            const float dx = A.B.coldx[gxc];
+            ck[q] = A.B.colk[gxc] - kmin;
+            cx[q] = dx;
+            cdx[q] = 1 - dx;
+            cb[q] = cdx[q] * cdx[q] - 1;
+            cdd[q] = dx * dx - 1;
+        }
+        // every thread polls; the outcome is made uniform before anyone acts on it
+        if (!__syncthreads_and(sp_wait(cur ? bar1 : bar0, (unsigned)((it >> 1) & 1)))) {
+            failed = true;
+            break;
+        }
+        // subtract the background in place, one warp per tile row, four
+        // columns per lane; outside the frame the value is 0
+        for (int ty = wid; ty < bh; ty += ST_THREADS / 32) {
+            const int gy = y0 - ry + ty;
+            if (4 * lane >= bw) continue;
+            float4 *tp = reinterpret_cast<float4 *>(tile + ty * bw) + lane;
+            float4 v = *tp;
+            float *vv = reinterpret_cast<float *>(&v);
+            const bool rin = gy >= 0 && gy < h;
+            const bool inner = ty >= ry && ty < ry + ST_TH;
+            float *srow = A.sub + (size_t)(rin ? gy : 0) * w;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                float s = 0.0f;
+                if (rin && cin[q]) {
+                    float b;
+                    if (!spline) {
+                        b = A.back_type == 1 ? backmean : __ldg(A.B.rownode + (size_t)gy * A.nbx);
+                    } else if (staged) {
+                        const int k = ck[q];
+                        b = (float)(cdx[q] * (s_nd[ty][k] + cb[q] * s_dnd[ty][k]) +
+                                    cx[q] * (s_nd[ty][k + 1] + cdd[q] * s_dnd[ty][k + 1]));
+                    } else {
+                        const float *nd = A.B.rownode + (size_t)gy * A.nbx, *dnd = A.B.rowdnode + (size_t)gy * A.nbx;
+                        const int k = ck[q] + kmin;
+                        b = (float)(cdx[q] * (__ldg(nd + k) + cb[q] * __ldg(dnd + k)) +
+                                    cx[q] * (__ldg(nd + k + 1) + cdd[q] * __ldg(dnd + k + 1)));
+                    }
+                    s = sx_unblank(vv[q]) - b;
+                    const int tx = 4 * lane + q;
+                    if (inner && tx >= rxa && tx < rxa + ST_TW) {
+                        srow[gxa + tx] = s;
+                        const unsigned ef = (__float_as_uint(s) >> 23) & 0xff;
+                        if (ef) emin = min(emin, (int)ef - 127);
+                    }
+                }
+                vv[q] = s;
+            }
+            *tp = v;
+        }
+        __syncthreads();
+        // convolution, threshold, label seed: one column, ST_RPT rows per thread
+        const int cxo = tid & (ST_TW - 1), r0 = (tid / ST_TW) * ST_RPT;
+        float acc[ST_RPT];
+        if constexpr (MW > 0)
+            conv_rows<MW, MH>(taps, tile, bw, cxo + rxa - rx, r0, acc);
+        else
+            conv_rows_any(A.mask, tile, bw, cxo + rxa - rx, r0, mw, mh, acc);
+        const int gx = x0 + cxo;
+        if (gx < w) {
+#pragma unroll
+            for (int k = 0; k < ST_RPT; k++) {
+                const int gy = y0 + r0 + k;
+                if (gy < h) {
+                    const int p = gy * w + gx;
+                    A.cd[p] = acc[k];
+                    bool fg;
+                    if (WEIGHTED) {
+                        const float v = __ldg(A.wvar + p);
+                        fg = (v < 1e30f) && acc[k] >= sx_pix_thr(A.wthr, A.dfac, v, dthresh);
+                    } else {
+                        fg = acc[k] >= dthresh;
+                    }
+                    A.lab[p] = fg ? p : -1;
+                    nabove += fg;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (failed) {
+        // a load did not complete in time: report it and give the copies
+        // still in flight one more bounded wait, so that none is left writing
+        // into a finished CTA's shared memory
+        if (tid == 0) {
+            atomicOr(&A.sc->status, SX_ST_LOOP);
+            sp_wait(bar0, 0);
+            sp_wait(bar0, 1);
+            sp_wait(bar1, 0);
+            sp_wait(bar1, 1);
+        }
+        return;
     }
     for (int o = 16; o > 0; o >>= 1) {
         nabove += __shfl_down_sync(0xffffffffu, nabove, o);
         emin = min(emin, __shfl_down_sync(0xffffffffu, emin, o));
     }
     if (lane == 0) {
-        if (nabove) atomicAdd(&sc->npix_above, nabove);
-        if (emin < 1000) atomicMin(&sc->e0sub, emin);
+        if (nabove) atomicAdd(&A.sc->npix_above, nabove);
+        if (emin < 1000) atomicMin(&A.sc->e0sub, emin);
     }
 }
 
@@ -320,29 +398,64 @@ void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const 
     const int rxa = ((mw / 2) + 3) & ~3;  // halo width rounded up to 16 bytes
     CUtensorMap tmap;
     if (make_frame_tmap(&tmap, img, P.w, P.h, rxa, mh / 2)) {
-        dim3 tgrid((P.w + ST_TW - 1) / ST_TW, (P.h + ST_TH - 1) / ST_TH);
+        SpArgs A;
+        A.sub = sub;
+        A.cd = cd;
+        A.lab = lab;
+        A.B = B;
+        A.w = P.w;
+        A.h = P.h;
+        A.nbx = P.nbx;
+        A.back_type = P.back_type;
+        A.mw = mw;
+        A.mh = mh;
+        A.rxa = rxa;
+        A.wthr = P.wthr;
+        A.tilesx = (P.w + ST_TW - 1) / ST_TW;
+        A.ntiles = A.tilesx * ((P.h + ST_TH - 1) / ST_TH);
+        A.dfac = P.detect_thresh;
+        A.mask = M.dev;
+        A.wvar = d_var;
+        A.sc = d_sc;
         ConvTaps taps;
         memset(&taps, 0, sizeof(taps));
         if (mw * mh <= 121) memcpy(taps.m, M.host, sizeof(float) * mw * mh);
-#define SF_LAUNCH(a, b)                                                                                      \
-    k_sub_filter_tma<a, b><<<tgrid, ST_THREADS, 0, st>>>(tmap, sub, cd, lab, B, P.w, P.h, P.nbx, P.back_type, \
-                                                         taps, M.dev, mw, mh, rxa, d_var, P.wthr,           \
-                                                         P.detect_thresh, d_sc)
-        if (mw == mh && mw == 1)
-            SF_LAUNCH(1, 1);
-        else if (mw == mh && mw == 3)
-            SF_LAUNCH(3, 3);
-        else if (mw == mh && mw == 5)
-            SF_LAUNCH(5, 5);
-        else if (mw == mh && mw == 7)
-            SF_LAUNCH(7, 7);
-        else if (mw == mh && mw == 9)
-            SF_LAUNCH(9, 9);
-        else if (mw == mh && mw == 11)
-            SF_LAUNCH(11, 11);
-        else
-            SF_LAUNCH(0, 0);
-#undef SF_LAUNCH
+        const int bw = ST_TW + 2 * rxa, bh = ST_TH + 2 * (mh / 2);
+        const size_t smem = 2 * sizeof(float) * (size_t)((bw * bh + 31) & ~31);
+        int dev = 0, nsm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+#define SP_LAUNCH(a, b, wt)                                                                              \
+    do {                                                                                                \
+        auto kern = k_sub_filter_pipe<a, b, wt>;                                                        \
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);             \
+        int per = 1;                                                                                    \
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, ST_THREADS, smem);                    \
+        const int grid = std::max(1, std::min(A.ntiles, nsm * std::max(per, 1)));                      \
+        kern<<<grid, ST_THREADS, smem, st>>>(tmap, A, taps);                                            \
+    } while (0)
+#define SP_MASK(wt)                    \
+    if (mw == mh && mw == 1)           \
+        SP_LAUNCH(1, 1, wt);           \
+    else if (mw == mh && mw == 3)      \
+        SP_LAUNCH(3, 3, wt);           \
+    else if (mw == mh && mw == 5)      \
+        SP_LAUNCH(5, 5, wt);           \
+    else if (mw == mh && mw == 7)      \
+        SP_LAUNCH(7, 7, wt);           \
+    else if (mw == mh && mw == 9)      \
+        SP_LAUNCH(9, 9, wt);           \
+    else if (mw == mh && mw == 11)     \
+        SP_LAUNCH(11, 11, wt);         \
+    else                               \
+        SP_LAUNCH(0, 0, wt)
+        if (d_var) {
+            SP_MASK(true);
+        } else {
+            SP_MASK(false);
+        }
+#undef SP_MASK
+#undef SP_LAUNCH
         launches += 1;
         return;
     }
