@@ -351,6 +351,7 @@ struct FrameParams {
     int mask_type, numbering;
     int wtype;                      // weight map: 0 none, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT
     int wthr;                       // thresholds follow the local rms (weight map, relative thresholds)
+    double seeing, pixscale;        // SEEING_FWHM, PIXEL_SCALE (CLASS_STAR)
 };
 
 // scalars computed on the device during one extraction

@@ -18,6 +18,8 @@ struct CompatState {
     int mask_w = 0;
     int nobj = 0;
     void (*handler)(const char *) = nullptr;
+    bool have_nnw = false;
+    sexgpu_nnw nnw;
 };
 
 CompatState &cs() {
@@ -91,7 +93,7 @@ __global__ void k_compat_rows(ObjBufs O, int n, sexgpu_outobj *rows) {
     q.flag = (short)O.flags[o];
     q.elong = O.a[o] / O.b[o];
     q.ellip = 1 - O.b[o] / O.a[o];
-    q.sprob = 0.0f;
+    q.sprob = O.sprob ? O.sprob[o] : 0.0f;
     q.peak = O.peak[o];
     q.kronfactor = O.kron[o];
     q.bkg = O.bkg[o];
@@ -116,6 +118,17 @@ void sexgpu_compat_configure(double mag_zeropoint, double phot_aperture, double 
 
 void sexgpu_compat_set_device(int device) { cs().device = device; }
 
+void sexgpu_compat_set_nnw(const sexgpu_nnw *net, double seeing_fwhm) {
+    CompatState &s = cs();
+    s.have_nnw = net != nullptr;
+    if (net) s.nnw = *net;
+    if (seeing_fwhm > 0.0) s.cfg.seeing_fwhm = seeing_fwhm;
+    if (s.ctx) {
+        const int rc = sexgpu_set_nnw(s.ctx, s.have_nnw ? &s.nnw : nullptr);
+        if (rc) compat_fail("sexgpu_compat_set_nnw", rc);
+    }
+}
+
 void sexgpu_compat_set_error_handler(void (*handler)(const char *msg)) { cs().handler = handler; }
 
 void init_device(int width, int height, float *img) {
@@ -124,6 +137,10 @@ void init_device(int width, int height, float *img) {
     if (!s.ctx && (rc = sexgpu_create(&s.ctx, s.device)) != SEXGPU_OK) {
         s.ctx = nullptr;
         compat_fail("init_device", rc);
+        return;
+    }
+    if (s.have_nnw && (rc = sexgpu_set_nnw(s.ctx, &s.nnw)) != SEXGPU_OK) {
+        compat_fail("init_device (CLASS_STAR network)", rc);
         return;
     }
     if (!img || width <= 0 || height <= 0) {
@@ -306,7 +323,7 @@ void endobject_gpu(void *prefs, void *brain, void *flagobj2, sexgpu_outobj *outo
                    double gain, int numobj) {
     CompatState &s = cs();
     (void)prefs, (void)brain, (void)flagobj2, (void)wcs, (void)fymin, (void)fymax, (void)backsig, (void)thresh;
-    (void)pixscale, (void)ngamma;
+    (void)ngamma;
     if (!compat_ready("endobject_gpu", 5)) return;
     if (numobj != s.nobj || width != s.w || height != s.h) {
         compat_fail("endobject_gpu (object count or frame size differs)", SEXGPU_ERR_ARG);
@@ -322,6 +339,8 @@ void endobject_gpu(void *prefs, void *brain, void *flagobj2, sexgpu_outobj *outo
     Pm.autoparam1 = s.cfg.phot_autoparams[1];
     Pm.mask_type = s.cfg.mask_type;
     Pm.numbering = 1;
+    Pm.seeing = s.cfg.seeing_fwhm;
+    Pm.pixscale = pixscale > 0.0 ? pixscale : 1.0;
     int rc = pipe_end(ctx);
     if (!rc && numobj > 0) {
         rc = ensure(ctx, ctx->rows, (size_t)numobj * sizeof(sexgpu_outobj));

@@ -179,6 +179,8 @@ struct EndArgs {
     double aperture, autoparam0, autoparam1, gain, zp, satur;
     const float *wvar;  // calibrated variance map, or null
     KronBufs K;         // queued Kron boxes
+    const sexgpu_nnw *nnw;  // CLASS_STAR network (device), or null
+    double seeing, pixscale;
 };
 
 // src/cuda/cudaanalyse.cu:104-287 (computeaperflux, one aperture).  The
@@ -617,6 +619,36 @@ __global__ void k_kron_merge(EndArgs A) {
     }
 }
 
+// CLASS_STAR, src/cuda/cudaanalyse.cu:2901-2920 with the network response of
+// :599-632 (src/neurro.c neurresp): inputs are log10 of the eight isophotal
+// areas in seeing units and of FLUX_MAX over the threshold, plus log10 of the
+// seeing; every layer applies the logistic function; double arithmetic.
+__global__ void k_class_star(ObjBufs O, int n, const sexgpu_nnw *__restrict__ net, double fwhm, double pixscale) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n || O.fmaster[o] >= 0) return;
+    double fac2 = fwhm / pixscale;
+    fac2 *= fac2;
+    const float thresh = O.athr[o], peak = O.peak[o];
+    double in[SEXGPU_NNW_NEURONS], nx[SEXGPU_NNW_NEURONS];
+    const int *iso = O.iso + (size_t)o * SX_NISO_;
+    int j = 0;
+    in[j] = log10(iso[0] ? iso[0] / fac2 : 0.01);
+    in[++j] = thresh > 0.0 ? log10(peak > 0.0 ? peak / thresh : 0.1) : -1.0;
+    for (int i = 1; i < SX_NISO_; i++) in[++j] = log10(iso[i] ? iso[i] / fac2 : 0.01);
+    in[++j] = log10(fwhm);
+    const int last = net->nlayers - 1;
+    for (int i = 0; i < net->nn[0]; i++) in[i] = in[i] * net->inscale[i] + net->inbias[i];
+    for (int l = 0; l < last; l++) {
+        for (int k = 0; k < net->nn[l + 1]; k++) {
+            double sum = net->b[l][k];
+            for (int i = 0; i < net->nn[l]; i++) sum += net->w[l][i][k] * in[i];
+            nx[k] = 1.0 / (1.0 + exp(-sum));
+        }
+        for (int k = 0; k < net->nn[l + 1]; k++) in[k] = nx[k];
+    }
+    O.sprob[o] = (float)((in[0] - net->outbias[0]) / net->outscale[0]);
+}
+
 void launch_endobject(const EndArgs &E, int nobj, cudaStream_t st, int &launches) {
     if (nobj <= 0) return;
     k_endobject<<<(unsigned)((nobj + 3) / 4), 128, 0, st>>>(E);
@@ -625,6 +657,10 @@ void launch_endobject(const EndArgs &E, int nobj, cudaStream_t st, int &launches
     k_kron_chunks<2><<<KR_GRID, KR_THREADS, 0, st>>>(E);
     k_kron_merge<2><<<KR_GRID / 2, 128, 0, st>>>(E);
     launches += 5;
+    if (E.nnw) {
+        k_class_star<<<(unsigned)((nobj + 127) / 128), 128, 0, st>>>(E.O, nobj, E.nnw, E.seeing, E.pixscale);
+        launches += 1;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -690,6 +726,7 @@ __global__ void k_write_rows(ObjBufs O, const unsigned *vals, int ns, float dthr
     q.cxx = O.cxx[o];
     q.cyy = O.cyy[o];
     q.cxy = O.cxy[o];
+    q.class_star = O.sprob ? O.sprob[o] : 0.0f;
     q.poserr_mx2 = O.pmx2[o];
     q.poserr_my2 = O.pmy2[o];
     q.poserr_mxy = O.pmxy[o];

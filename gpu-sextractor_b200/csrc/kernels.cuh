@@ -80,6 +80,7 @@ struct ObjBufs {
     float *mag_iso, *magerr_iso, *fluxerr_iso;
     int *fdnpix;
     float *dthr, *athr;                 // the raw object's detection / analysis thresholds
+    float *sprob;                       // CLASS_STAR
     unsigned long long *sortkey;
 };
 

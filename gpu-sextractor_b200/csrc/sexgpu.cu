@@ -85,6 +85,9 @@ struct sexgpu_ctx {
     DevBuf o_i[20], o_f[32], o_d[10], o_iso, o_sortkey, amp, alpha, cellhead, cellnext, vkey, vval, vkalt, vvalt,
         skeys, svals, skalt, svalt, rows;
     DevBuf kitem[2], kchunk[2], kpart[2];  // queued Kron boxes
+    DevBuf o_sprob;                        // CLASS_STAR per object
+    DevBuf dnnw;                           // this context's copy of the CLASS_STAR network
+    const sexgpu_nnw *nnw_dev = nullptr;   // network used (this context's or, for a batch worker, its owner's)
     int kron_warp_max = KR_WARP_MAX;
     DevBuf sc;
     FrameScalars hsc;
@@ -211,6 +214,7 @@ int check_config(const sexgpu_config *cfg, int w, int h) {
         return SEXGPU_ERR_ARG;
     if (cfg->detect_minarea < 1 || cfg->deblend_nthresh < 1 || cfg->deblend_nthresh > 64) return SEXGPU_ERR_ARG;
     if (cfg->weight_type < 0 || cfg->weight_type > 3) return SEXGPU_ERR_ARG;
+    if (!(cfg->seeing_fwhm > 0.0)) return SEXGPU_ERR_ARG;
     return SEXGPU_OK;
 }
 
@@ -249,6 +253,8 @@ void make_params(const sexgpu_config *cfg, int w, int h, FrameParams &P) {
     P.numbering = cfg->numbering;
     P.wtype = cfg->weight_type;
     P.wthr = cfg->weight_type != 0 && cfg->thresh_type != 1;
+    P.seeing = cfg->seeing_fwhm;
+    P.pixscale = cfg->pixel_scale > 0.0 ? cfg->pixel_scale : 1.0;
 }
 
 __global__ void k_init_scalars(FrameScalars *sc) {
@@ -376,6 +382,8 @@ int alloc_objects(sexgpu_ctx *ctx, int nobj) {
     EN(o_d[8], n * sizeof(float));   // magerr_iso
     EN(o_d[9], n * sizeof(float));   // fluxerr_iso
     O.magerr_iso = P<float>(ctx->o_d[8]);
+    EN(o_sprob, n * sizeof(float));
+    O.sprob = ctx->nnw_dev ? P<float>(ctx->o_sprob) : nullptr;
     O.fluxerr_iso = P<float>(ctx->o_d[9]);
     return SEXGPU_OK;
 }
@@ -819,6 +827,9 @@ int pipe_end(sexgpu_ctx *ctx) {
     E.K.icap = KR_ITEMS;
     E.K.ccap = KR_CHUNKS;
     E.K.warp_max = ctx->kron_warp_max;
+    E.nnw = ctx->nnw_dev;
+    E.seeing = Pm.seeing;
+    E.pixscale = Pm.pixscale;
     int nl = 0;
     launch_endobject(E, nobj, st, nl);
     stage_mark(ctx, "endobject", nl);
@@ -948,6 +959,14 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     for (auto &b : ctx->o_i) free_buf(b);
     for (auto &b : ctx->o_f) free_buf(b);
     for (auto &b : ctx->o_d) free_buf(b);
+    for (int i = 0; i < 2; i++) {
+        free_buf(ctx->kitem[i]);
+        free_buf(ctx->kchunk[i]);
+        free_buf(ctx->kpart[i]);
+    }
+    free_buf(ctx->o_sprob);
+    free_buf(ctx->dnnw);
+    free_buf(ctx->dmask);
     for (auto &s : ctx->stages) cudaEventDestroy(s.ev);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     for (int i = 0; i < 2; i++) {
@@ -1003,6 +1022,8 @@ void sexgpu_default_config(sexgpu_config *c) {
     c->mask_type = 2;
     c->weight_type = 0;
     c->numbering = 0;
+    c->seeing_fwhm = 1.2;
+    c->pixel_scale = 0.0;
 }
 
 const char *sexgpu_last_error(sexgpu_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
@@ -1236,7 +1257,10 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
         }
         ctx->workers.push_back(w);
     }
-    for (sexgpu_ctx *w : ctx->workers) w->kron_warp_max = ctx->kron_warp_max;
+    for (sexgpu_ctx *w : ctx->workers) {
+        w->kron_warp_max = ctx->kron_warp_max;
+        w->nnw_dev = ctx->nnw_dev;
+    }
     // largest frames first, so that the last frames to start are short
     std::vector<int> order(nframes);
     for (int i = 0; i < nframes; i++) order[i] = i;
@@ -1315,6 +1339,81 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
             ctx->err = "frame " + std::to_string(i) + " failed";
             return frames[i].status;
         }
+    return SEXGPU_OK;
+}
+
+int sexgpu_set_nnw(sexgpu_ctx *ctx, const sexgpu_nnw *net) {
+    if (!ctx) return SEXGPU_ERR_ARG;
+    if (!net) {
+        ctx->nnw_dev = nullptr;
+        return SEXGPU_OK;
+    }
+    if (net->nlayers < 2 || net->nlayers > SEXGPU_NNW_LAYERS || net->nn[0] != 10) return SEXGPU_ERR_ARG;
+    for (int l = 0; l < net->nlayers; l++)
+        if (net->nn[l] < 1 || net->nn[l] > SEXGPU_NNW_NEURONS) return SEXGPU_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = ensure(ctx, ctx->dnnw, sizeof(sexgpu_nnw));
+    if (rc) return rc;
+    CK(cudaMemcpy(ctx->dnnw.p, net, sizeof(sexgpu_nnw), cudaMemcpyHostToDevice));
+    ctx->nnw_dev = P<sexgpu_nnw>(ctx->dnnw);
+    return SEXGPU_OK;
+}
+
+// the .nnw format (src/neurro.c getnnw): a first line starting with NNW;
+// then, skipping blank and '#' lines: the layer count and the neurons per
+// layer; the input biases; the input scales; for every layer l and every
+// neuron j of layer l + 1 one line with the nn[l] weights into j and j's
+// bias; the output biases; the output scales
+int sexgpu_read_nnw(const char *path, sexgpu_nnw *net) {
+    if (!path || !net) return SEXGPU_ERR_ARG;
+    FILE *f = fopen(path, "r");
+    if (!f) return SEXGPU_ERR_ARG;
+    memset(net, 0, sizeof(*net));
+    char line[8192];
+    const int rc = SEXGPU_ERR_ARG;
+    if (!fgets(line, sizeof line, f) || strncmp(line, "NNW", 3)) {
+        fclose(f);
+        return rc;
+    }
+    std::vector<std::vector<double>> rows;
+    while (fgets(line, sizeof line, f)) {
+        const char *p = line + strspn(line, " \t");
+        if (*p == '#' || *p == '\n' || *p == '\r' || !*p) continue;
+        std::vector<double> v;
+        char *end;
+        for (;;) {
+            const double d = strtod(p, &end);
+            if (end == p) break;
+            v.push_back(d);
+            p = end;
+        }
+        if (!v.empty()) rows.push_back(v);
+    }
+    fclose(f);
+    if (rows.empty()) return rc;
+    const int nl = (int)rows[0][0];
+    if (nl < 2 || nl > SEXGPU_NNW_LAYERS || (int)rows[0].size() < nl + 1) return rc;
+    net->nlayers = nl;
+    for (int l = 0; l < nl; l++) {
+        net->nn[l] = (int)rows[0][l + 1];
+        if (net->nn[l] < 1 || net->nn[l] > SEXGPU_NNW_NEURONS) return rc;
+    }
+    size_t r = 1;
+    auto take = [&](double *dst, int n) {
+        if (r >= rows.size() || (int)rows[r].size() < n) return false;
+        for (int i = 0; i < n; i++) dst[i] = rows[r][i];
+        r++;
+        return true;
+    };
+    if (!take(net->inbias, net->nn[0]) || !take(net->inscale, net->nn[0])) return rc;
+    for (int l = 0; l < nl - 1; l++)
+        for (int j = 0; j < net->nn[l + 1]; j++) {
+            if (r >= rows.size() || (int)rows[r].size() < net->nn[l] + 1) return rc;
+            for (int i = 0; i < net->nn[l]; i++) net->w[l][i][j] = rows[r][i];
+            net->b[l][j] = rows[r][net->nn[l]];
+            r++;
+        }
+    if (!take(net->outbias, net->nn[nl - 1]) || !take(net->outscale, net->nn[nl - 1])) return rc;
     return SEXGPU_OK;
 }
 

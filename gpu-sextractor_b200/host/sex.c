@@ -18,6 +18,7 @@
  *   CHECKIMAGE_TYPE (NONE, SEGMENTATION, BACKGROUND, -BACKGROUND, FILTERED)
  *   CHECKIMAGE_NAME VERBOSE_TYPE
  *   WEIGHT_TYPE (NONE, MAP_VAR, MAP_RMS, MAP_WEIGHT) WEIGHT_IMAGE
+ *   STARNNW_NAME SEEING_FWHM PIXEL_SCALE (CLASS_STAR)
  * Other keywords of the reference are accepted and ignored.
  */
 #include <ctype.h>
@@ -35,7 +36,8 @@
 
 typedef struct {
     char catalog_name[1024], catalog_type[64], parameters_name[1024], filter_name[1024];
-    char check_type[64], check_name[1024], verbose[32], weight_image[1024];
+    char check_type[64], check_name[1024], verbose[32], weight_image[1024], nnw_name[1024];
+    int nnw_given;
     sexgpu_config cfg;
     float mask[1024];
 } prefs_t;
@@ -100,6 +102,12 @@ static void setpref(prefs_t *p, const char *key, char *val)
                          : !strncasecmp(val, "MAP_WEIGHT", 10) ? 3
                                                                : 0;
     else if (!strcasecmp(key, "WEIGHT_IMAGE")) snprintf(p->weight_image, sizeof p->weight_image, "%s", val);
+    else if (!strcasecmp(key, "SEEING_FWHM")) c->seeing_fwhm = atof(val);
+    else if (!strcasecmp(key, "PIXEL_SCALE")) c->pixel_scale = atof(val);
+    else if (!strcasecmp(key, "STARNNW_NAME")) {
+        snprintf(p->nnw_name, sizeof p->nnw_name, "%s", val);
+        p->nnw_given = 1;
+    }
 }
 
 static void readprefs(prefs_t *p, const char *path)
@@ -282,6 +290,7 @@ static const col_t COLS[] = {
     {"FLAGS", "%3d", "", "Extraction flags"},
     {"XPEAK_IMAGE", "%10d", "pixel", "x-coordinate of the brightest pixel"},
     {"YPEAK_IMAGE", "%10d", "pixel", "y-coordinate of the brightest pixel"},
+    {"CLASS_STAR", "%6.3f", "", "S/G classifier output"},
     {NULL, NULL, NULL, NULL}};
 
 static void print_col(FILE *f, int c, const sexgpu_object *o)
@@ -332,6 +341,7 @@ static void print_col(FILE *f, int c, const sexgpu_object *o)
     case 41: fprintf(f, fmt, o->flags); break;
     case 42: fprintf(f, fmt, o->peakx); break;
     case 43: fprintf(f, fmt, o->peaky); break;
+    case 44: fprintf(f, fmt, o->class_star); break;
     }
 }
 
@@ -345,7 +355,7 @@ static void printobj(FILE *f, const sexgpu_object *o)
             o->number, 0.0, 0.0, (float)(o->mx + 1.0), (float)(o->my + 1.0), o->flux_iso, o->fluxerr_iso,
             o->mag_iso, o->magerr_iso, o->flux_isocor, o->fluxerr_isocor, o->flux_aper, o->fluxerr_aper,
             o->mag_aper, o->magerr_aper, o->flux_auto, o->fluxerr_auto, o->mag_auto, o->magerr_auto, o->theta,
-            o->poserr_mx2, o->poserr_my2, o->poserr_mxy, o->flags, o->elong, o->ellip, 0.0f, o->peak,
+            o->poserr_mx2, o->poserr_my2, o->poserr_mxy, o->flags, o->elong, o->ellip, o->class_star, o->peak,
             o->kronfactor, o->bkg, o->fwhm);
 }
 
@@ -404,6 +414,7 @@ static double col_value(int c, const sexgpu_object *o)
     case 41: return o->flags;
     case 42: return o->peakx;
     case 43: return o->peaky;
+    case 44: return o->class_star;
     }
     return 0.0;
 }
@@ -559,6 +570,7 @@ int main(int argc, char **argv)
     strcpy(p.catalog_type, "ASCII_HEAD");
     strcpy(p.parameters_name, "default.param");
     strcpy(p.filter_name, "default.conv");
+    strcpy(p.nnw_name, "default.nnw");
     strcpy(p.check_type, "NONE");
     strcpy(p.check_name, "check.fits");
     /* src/main.c:65-121: configuration file first, then -KEY value overrides */
@@ -603,6 +615,14 @@ int main(int argc, char **argv)
             if (wmap[k] <= -1e30f) wmap[k] = p.cfg.weight_type == 3 ? 0.0f : 1e30f;
     }
     if ((rc = sexgpu_create(&ctx, 0)) != SEXGPU_OK) die("no usable CUDA device", NULL);
+    {
+        /* CLASS_STAR: the network of STARNNW_NAME (default.nnw when present) */
+        sexgpu_nnw net;
+        if (sexgpu_read_nnw(p.nnw_name, &net) == SEXGPU_OK)
+            sexgpu_set_nnw(ctx, &net);
+        else if (p.nnw_given)
+            die("cannot read the star/galaxy network ", p.nnw_name);
+    }
     objs = (sexgpu_object *)malloc(sizeof(sexgpu_object) * 1024);
     if (strcasecmp(p.check_type, "NONE")) {
         seg = (int32_t *)malloc(sizeof(int32_t) * (size_t)w * h);

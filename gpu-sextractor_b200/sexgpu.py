@@ -40,7 +40,35 @@ class Config(C.Structure):
         ("satur_level", C.c_double), ("gain", C.c_double), ("mag_zeropoint", C.c_double),
         ("phot_aperture", C.c_double), ("phot_autoparams", C.c_double * 2), ("mask_type", C.c_int),
         ("weight_type", C.c_int), ("numbering", C.c_int),
+        ("seeing_fwhm", C.c_double), ("pixel_scale", C.c_double),
     ]
+
+
+class NNW(C.Structure):
+    """sexgpu_nnw: star/galaxy network (CLASS_STAR)."""
+    _fields_ = [("nlayers", C.c_int32), ("nn", C.c_int32 * 3),
+                ("inbias", C.c_double * 10), ("inscale", C.c_double * 10),
+                ("outbias", C.c_double * 10), ("outscale", C.c_double * 10),
+                ("w", ((C.c_double * 10) * 10) * 2), ("b", (C.c_double * 10) * 2)]
+
+    @classmethod
+    def from_arrays(cls, nn, inbias, inscale, weights, biases, outbias, outscale):
+        """nn: neurons per layer; weights[l][i][j] from neuron i of layer l
+        to neuron j of layer l + 1; biases[l][j]."""
+        net = cls()
+        net.nlayers = len(nn)
+        for l, v in enumerate(nn):
+            net.nn[l] = int(v)
+        for i in range(nn[0]):
+            net.inbias[i], net.inscale[i] = float(inbias[i]), float(inscale[i])
+        for i in range(nn[-1]):
+            net.outbias[i], net.outscale[i] = float(outbias[i]), float(outscale[i])
+        for l in range(len(nn) - 1):
+            for j in range(nn[l + 1]):
+                net.b[l][j] = float(biases[l][j])
+                for i in range(nn[l]):
+                    net.w[l][i][j] = float(weights[l][i][j])
+        return net
 
 
 OBJECT_FIELDS = [
@@ -51,7 +79,7 @@ OBJECT_FIELDS = [
     ("dpeak", "f4"), ("peak", "f4"),
     ("mx", "f8"), ("my", "f8"), ("mx2", "f8"), ("my2", "f8"), ("mxy", "f8"),
     ("a", "f4"), ("b", "f4"), ("theta", "f4"), ("abcor", "f4"), ("cxx", "f4"), ("cyy", "f4"),
-    ("cxy", "f4"),
+    ("cxy", "f4"), ("class_star", "f4"),
     ("poserr_mx2", "f8"), ("poserr_my2", "f8"), ("poserr_mxy", "f8"),
     ("bkg", "f4"), ("thresh", "f4"), ("dthresh", "f4"), ("mthresh", "f4"), ("fwhm", "f4"),
     ("flux_iso", "f4"), ("fluxerr_iso", "f4"), ("mag_iso", "f4"), ("magerr_iso", "f4"),
@@ -86,6 +114,7 @@ class Stage(C.Structure):
 EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extract",
            "sexgpu_extract_device", "sexgpu_copy_results", "sexgpu_background", "sexgpu_filter",
            "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times", "sexgpu_set_param",
+           "sexgpu_read_nnw", "sexgpu_set_nnw",
            "sexgpu_background_noalloc", "sexgpu_extract_batch"]
 
 _lib = None
@@ -130,7 +159,7 @@ def default_config():
                 conv=DEFAULT_CONV, detect_minarea=5, deblend_nthresh=32, deblend_mincont=0.005,
                 clean_flag=1, clean_param=1.0, satur_level=50000.0, gain=0.0, mag_zeropoint=0.0,
                 phot_aperture=5.0, phot_autoparams=(2.5, 3.5), mask_type=2, weight_type=0,
-                numbering=0)
+                numbering=0, seeing_fwhm=1.2, pixel_scale=0.0)
 
 
 def make_config(**kw):
@@ -265,6 +294,10 @@ class Context:
         _check(lib().sexgpu_extract_batch(self.h, arr, n, workers), self.h, "sexgpu_extract_batch")
         return [(keep[i][2][:arr[i].nobj], arr[i].summary) for i in range(n)]
 
+    def set_nnw(self, net):
+        """CLASS_STAR network of later extractions (NNW), or None to switch it off."""
+        _check(lib().sexgpu_set_nnw(self.h, C.byref(net) if net is not None else None), self.h, "sexgpu_set_nnw")
+
     def set_param(self, name, value):
         """Execution parameter (results do not depend on it), e.g. kron_warp_max."""
         _check(lib().sexgpu_set_param(self.h, name.encode(), int(value)), self.h, "sexgpu_set_param")
@@ -286,6 +319,13 @@ def background_noalloc(d_img, d_sub, w, h, d_back, d_sigma, stream=0, **kw):
                                          C.c_void_p(stream))
     _check(rc, None, "sexgpu_background_noalloc")
     return s
+
+
+def read_nnw(path):
+    """Parse a SExtractor .nnw file into an NNW."""
+    net = NNW()
+    _check(lib().sexgpu_read_nnw(path.encode(), C.byref(net)), None, "sexgpu_read_nnw")
+    return net
 
 
 def getconv(path):

@@ -70,6 +70,8 @@ typedef struct {
     int     mask_type;          /* MASK_TYPE: 0 NONE, 1 BLANK, 2 CORRECT */
     int     weight_type;        /* WEIGHT_TYPE: 0 NONE, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT */
     int     numbering;          /* 0 completion order, 1 first-pixel order */
+    double  seeing_fwhm;        /* SEEING_FWHM (arcsec): CLASS_STAR input */
+    double  pixel_scale;        /* PIXEL_SCALE (arcsec/pixel); <= 0 means 1 (no WCS here) */
 } sexgpu_config;
 
 /* One catalogue row (0-based pixel coordinates unless stated). */
@@ -86,6 +88,7 @@ typedef struct {
     float   fdflux, dflux, flux, fluxerr, fdpeak, dpeak, peak;
     double  mx, my, mx2, my2, mxy;
     float   a, b, theta, abcor, cxx, cyy, cxy;
+    float   class_star;         /* CLASS_STAR (0 when no network is set) */
     double  poserr_mx2, poserr_my2, poserr_mxy;
     float   bkg, thresh, dthresh, mthresh, fwhm;
     float   flux_iso, fluxerr_iso, mag_iso, magerr_iso;
@@ -164,6 +167,27 @@ int sexgpu_getconv(const char *path, float *mask, int maxn, int *mw, int *mh);
 
 /* Fill cfg with the defaults of the reference's default.sex. */
 void sexgpu_default_config(sexgpu_config *cfg);
+
+/* Star/galaxy classifier (CLASS_STAR): a feed-forward network read from a
+ * SExtractor .nnw file (src/neurro.c getnnw; brainstruct, src/types.h:930).
+ * w[l][i][j] weighs neuron i of layer l into neuron j of layer l + 1. */
+#define SEXGPU_NNW_LAYERS 3
+#define SEXGPU_NNW_NEURONS 10
+typedef struct {
+    int32_t nlayers;                                   /* input, hidden..., output (2..3) */
+    int32_t nn[SEXGPU_NNW_LAYERS];                     /* neurons per layer (<= 10) */
+    double  inbias[SEXGPU_NNW_NEURONS], inscale[SEXGPU_NNW_NEURONS];
+    double  outbias[SEXGPU_NNW_NEURONS], outscale[SEXGPU_NNW_NEURONS];
+    double  w[SEXGPU_NNW_LAYERS - 1][SEXGPU_NNW_NEURONS][SEXGPU_NNW_NEURONS];
+    double  b[SEXGPU_NNW_LAYERS - 1][SEXGPU_NNW_NEURONS];
+} sexgpu_nnw;
+/* Parse a .nnw file; SEXGPU_ERR_ARG if it is not one or exceeds the limits. */
+int sexgpu_read_nnw(const char *path, sexgpu_nnw *net);
+/* Network of this context's later extractions (and its batch workers');
+ * NULL switches CLASS_STAR off (0 in every row).  With a network, CLASS_STAR
+ * is computed per object from its isophotal areas, FLUX_MAX, analysis
+ * threshold, SEEING_FWHM and PIXEL_SCALE (src/cuda/cudaanalyse.cu:2901-2920). */
+int sexgpu_set_nnw(sexgpu_ctx *ctx, const sexgpu_nnw *net);
 
 /* Background estimation and subtraction that allocates no device memory.
  *

@@ -23,7 +23,8 @@
  *   - endobject_gpu fills one output record per object, in object index
  *     order (src/types.h:417-455, NAPER = 1); NUMBER is left to the caller
  *     (src/scan.c:154); ALPHA/DELTA_J2000 are 0 as in the reference; CLASS_STAR
- *     (sprob) is 0;
+ *     (sprob) is computed when a network was given with sexgpu_compat_set_nnw
+ *     (0 otherwise);
  *   - errors print "*Error*: ..." to stderr and exit the process, as the
  *     reference's checkCudaErrors/exit(-1) do (a handler can replace that).
  *
@@ -39,6 +40,8 @@
 #define SEXGPU_COMPAT_H
 
 #include <stddef.h>
+
+#include "sexgpu.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -84,6 +87,10 @@ void sexgpu_compat_configure(double mag_zeropoint, double phot_aperture, double 
                              int mask_type, double back_value);
 /* device the state is created on (default 0); before init_device */
 void sexgpu_compat_set_device(int device);
+/* CLASS_STAR: the reference's brainstruct (read by getnnw, src/neurro.c)
+ * in this library's layout, and prefs.seeing_fwhm; endobject_gpu's pixscale
+ * argument gives the pixel scale.  NULL: CLASS_STAR (sprob) stays 0. */
+void sexgpu_compat_set_nnw(const sexgpu_nnw *net, double seeing_fwhm);
 /* called instead of exit() on an error, with the message */
 void sexgpu_compat_set_error_handler(void (*handler)(const char *msg));
 

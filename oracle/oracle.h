@@ -76,7 +76,23 @@ typedef struct {
     int     weight_type;        /* 0 NONE, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT */
     /* catalog order: 0 completion order, 1 first-pixel order */
     int     numbering;
+    /* star/galaxy classification (src/preflist.h:132, SEEING_FWHM; PIXEL_SCALE) */
+    double  seeing_fwhm;
+    double  pixel_scale;        /* <= 0: 1 */
+    const struct orc_nnw *nnw;  /* network, or NULL: CLASS_STAR 0 */
 } orc_config;
+
+/* Star/galaxy network (src/types.h:930 brainstruct; src/neurro.c) */
+#define ORC_NNW_LAYERS 3
+#define ORC_NNW_NEURONS 10
+typedef struct orc_nnw {
+    int32_t nlayers;
+    int32_t nn[ORC_NNW_LAYERS];
+    double  inbias[ORC_NNW_NEURONS], inscale[ORC_NNW_NEURONS];
+    double  outbias[ORC_NNW_NEURONS], outscale[ORC_NNW_NEURONS];
+    double  w[ORC_NNW_LAYERS - 1][ORC_NNW_NEURONS][ORC_NNW_NEURONS];
+    double  b[ORC_NNW_LAYERS - 1][ORC_NNW_NEURONS];
+} orc_nnw;
 
 /* One catalog row; 0-based pixel coordinates unless stated. */
 typedef struct {
@@ -91,6 +107,7 @@ typedef struct {
     float   fdflux, dflux, flux, fluxerr, fdpeak, dpeak, peak;
     double  mx, my, mx2, my2, mxy;
     float   a, b, theta, abcor, cxx, cyy, cxy;
+    float   class_star;         /* CLASS_STAR (0 without a network) */
     double  poserr_mx2, poserr_my2, poserr_mxy;
     float   bkg, thresh, dthresh, mthresh, fwhm;
     float   flux_iso, fluxerr_iso, mag_iso, magerr_iso;

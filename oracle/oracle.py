@@ -26,7 +26,35 @@ class OrcConfig(C.Structure):
         ("satur_level", C.c_double), ("gain", C.c_double), ("mag_zeropoint", C.c_double),
         ("phot_aperture", C.c_double), ("phot_autoparams", C.c_double * 2), ("mask_type", C.c_int),
         ("weight_type", C.c_int), ("numbering", C.c_int),
+        ("seeing_fwhm", C.c_double), ("pixel_scale", C.c_double), ("nnw", C.c_void_p),
     ]
+
+
+class NNW(C.Structure):
+    """orc_nnw: star/galaxy network (CLASS_STAR)."""
+    _fields_ = [("nlayers", C.c_int32), ("nn", C.c_int32 * 3),
+                ("inbias", C.c_double * 10), ("inscale", C.c_double * 10),
+                ("outbias", C.c_double * 10), ("outscale", C.c_double * 10),
+                ("w", ((C.c_double * 10) * 10) * 2), ("b", (C.c_double * 10) * 2)]
+
+    @classmethod
+    def from_arrays(cls, nn, inbias, inscale, weights, biases, outbias, outscale):
+        """nn: neurons per layer; weights[l][i][j] from neuron i of layer l
+        to neuron j of layer l + 1; biases[l][j]."""
+        net = cls()
+        net.nlayers = len(nn)
+        for l, v in enumerate(nn):
+            net.nn[l] = int(v)
+        for i in range(nn[0]):
+            net.inbias[i], net.inscale[i] = float(inbias[i]), float(inscale[i])
+        for i in range(nn[-1]):
+            net.outbias[i], net.outscale[i] = float(outbias[i]), float(outscale[i])
+        for l in range(len(nn) - 1):
+            for j in range(nn[l + 1]):
+                net.b[l][j] = float(biases[l][j])
+                for i in range(nn[l]):
+                    net.w[l][i][j] = float(weights[l][i][j])
+        return net
 
 
 OBJECT_FIELDS = [
@@ -37,7 +65,7 @@ OBJECT_FIELDS = [
     ("dpeak", "f4"), ("peak", "f4"),
     ("mx", "f8"), ("my", "f8"), ("mx2", "f8"), ("my2", "f8"), ("mxy", "f8"),
     ("a", "f4"), ("b", "f4"), ("theta", "f4"), ("abcor", "f4"), ("cxx", "f4"), ("cyy", "f4"),
-    ("cxy", "f4"),
+    ("cxy", "f4"), ("class_star", "f4"),
     ("poserr_mx2", "f8"), ("poserr_my2", "f8"), ("poserr_mxy", "f8"),
     ("bkg", "f4"), ("thresh", "f4"), ("dthresh", "f4"), ("mthresh", "f4"), ("fwhm", "f4"),
     ("flux_iso", "f4"), ("fluxerr_iso", "f4"), ("mag_iso", "f4"), ("magerr_iso", "f4"),
@@ -105,6 +133,10 @@ def make_config(**kw):
     cfg = OrcConfig()
     mask = np.ascontiguousarray(d.pop("conv"), dtype=np.float32)
     cfg._mask = mask  # keep alive
+    net = d.pop("nnw", None)
+    if net is not None:
+        cfg._nnw = net
+        cfg.nnw = C.cast(C.pointer(net), C.c_void_p)
     for k, v in d.items():
         if k == "phot_autoparams":
             cfg.phot_autoparams[0], cfg.phot_autoparams[1] = v
@@ -124,7 +156,7 @@ def default_config():
                 conv=DEFAULT_CONV, detect_minarea=5, deblend_nthresh=32, deblend_mincont=0.005,
                 clean_flag=1, clean_param=1.0, satur_level=50000.0, gain=0.0, mag_zeropoint=0.0,
                 phot_aperture=5.0, phot_autoparams=(2.5, 3.5), mask_type=2, weight_type=0,
-                numbering=0)
+                numbering=0, seeing_fwhm=1.2, pixel_scale=0.0)
 
 
 def background(img, **kw):

@@ -110,6 +110,7 @@ typedef struct {
     float kron, flux_auto, fluxerr_auto, mag_auto, magerr_auto;
     float mag_iso, magerr_iso, fluxerr_iso;
     float elong, ellip, polar;
+    float class_star;
 } obj_t;
 
 typedef struct {
@@ -1002,6 +1003,36 @@ static void autoflux(const frame_t *F, const int *alloc, obj_t *o, int self)
 }
 
 /* endobject, src/cuda/cudaanalyse.cu:2604-2900 (the parts that feed the catalog) */
+/* CLASS_STAR: src/cuda/cudaanalyse.cu:2901-2920 (inputs) and :599-632 /
+   src/neurro.c neurresp (response, logistic units, double arithmetic) */
+static float class_star(const orc_config *cfg, const obj_t *o)
+{
+    const orc_nnw *net = cfg->nnw;
+    double in[ORC_NNW_NEURONS], nx[ORC_NNW_NEURONS], fac2, fwhm = cfg->seeing_fwhm;
+    double pixscale = cfg->pixel_scale > 0.0 ? cfg->pixel_scale : 1.0;
+    int i, j = 0, k, l, last = net->nlayers - 1;
+    fac2 = fwhm / pixscale;
+    fac2 *= fac2;
+    in[j] = log10(o->iso[0] ? o->iso[0] / fac2 : 0.01);
+    in[++j] = o->athr > 0.0 ? log10(o->peak > 0.0 ? o->peak / o->athr : 0.1) : -1.0;
+    for (i = 1; i < ORC_NISO; i++)
+        in[++j] = log10(o->iso[i] ? o->iso[i] / fac2 : 0.01);
+    in[++j] = log10(fwhm);
+    for (i = 0; i < net->nn[0]; i++)
+        in[i] = in[i] * net->inscale[i] + net->inbias[i];
+    for (l = 0; l < last; l++) {
+        for (k = 0; k < net->nn[l + 1]; k++) {
+            double sum = net->b[l][k];
+            for (i = 0; i < net->nn[l]; i++)
+                sum += net->w[l][i][k] * in[i];
+            nx[k] = 1.0 / (1.0 + exp(-sum));
+        }
+        for (k = 0; k < net->nn[l + 1]; k++)
+            in[k] = nx[k];
+    }
+    return (float)((in[0] - net->outbias[0]) / net->outscale[0]);
+}
+
 static void endobject(const frame_t *F, const int *alloc, obj_t *o, int self)
 {
     const orc_config *cfg = F->cfg;
@@ -1031,6 +1062,7 @@ static void endobject(const frame_t *F, const int *alloc, obj_t *o, int self)
         o->flags |= ORC_OBJ_SATUR;
     o->mag_iso = o->flux > 0.0 ? -2.5 * log10(o->flux) + cfg->mag_zeropoint : 99.0;
     o->magerr_iso = o->flux > 0.0 ? 1.086 * o->fluxerr_iso / o->flux : 99.0;
+    o->class_star = cfg->nnw ? class_star(cfg, o) : 0.0f;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1317,7 +1349,7 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
             q->fdpeak = o->fdpeak; q->dpeak = o->dpeak; q->peak = o->peak;
             q->mx = o->mx; q->my = o->my; q->mx2 = o->mx2; q->my2 = o->my2; q->mxy = o->mxy;
             q->a = o->a; q->b = o->b; q->theta = o->theta; q->abcor = o->abcor;
-            q->cxx = o->cxx; q->cyy = o->cyy; q->cxy = o->cxy;
+            q->cxx = o->cxx; q->cyy = o->cyy; q->cxy = o->cxy; q->class_star = o->class_star;
             q->poserr_mx2 = o->poserr_mx2; q->poserr_my2 = o->poserr_my2; q->poserr_mxy = o->poserr_mxy;
             q->bkg = o->bkg; q->thresh = o->thresh; q->dthresh = o->dthr; q->mthresh = o->mthresh;
             q->fwhm = o->fwhm;

@@ -7,7 +7,7 @@
  *
  * usage: scan_like frame.f32 W H mask.f32 MASKW out_rows.bin out_sub.f32
  *        BACK_SIZE BACK_FILTERSIZE BACK_FILTTHRESH DETECT_THRESH ANALYSIS_THRESH
- *        MINAREA NTHRESH MINCONT CLEAN CLEAN_PARAM GAIN SATUR
+ *        MINAREA NTHRESH MINCONT CLEAN CLEAN_PARAM GAIN SATUR [NNW SEEING_FWHM PIXSCALE]
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -26,7 +26,7 @@ static void *slurp(const char *path, size_t bytes) {
 }
 
 int main(int argc, char **argv) {
-    if (argc != 20) {
+    if (argc != 20 && argc != 23) {
         fprintf(stderr, "usage: see the header of scan_like.c\n");
         return 2;
     }
@@ -40,6 +40,13 @@ int main(int argc, char **argv) {
     int clean = atoi(argv[16]);
     double clean_param = atof(argv[17]), gain = atof(argv[18]), satur = atof(argv[19]);
     int deb_maxarea = minarea < 3 ? minarea : 3; /* src/prefs.c:463 */
+
+    /* makeit(): the star/galaxy network when a .nnw file is given (argv[20]) */
+    if (argc > 20) {
+        sexgpu_nnw net;
+        if (sexgpu_read_nnw(argv[20], &net) != SEXGPU_OK) return 3;
+        sexgpu_compat_set_nnw(&net, atof(argv[21]));
+    }
 
     /* makeback() */
     float backmean = 0.0f, backsig = 0.0f;
@@ -60,7 +67,8 @@ int main(int argc, char **argv) {
     int *master = (int *)malloc((size_t)(numdetected + 1) * sizeof(int));
     run_clean(master, clean_param, 3000, numdetected);
     sexgpu_outobj *objlist = (sexgpu_outobj *)malloc((size_t)(numdetected + 1) * sizeof(sexgpu_outobj));
-    endobject_gpu(NULL, NULL, NULL, objlist, NULL, 0, h, w, h, backsig, thresh, satur, 1.0, 0.0, gain, numdetected);
+    endobject_gpu(NULL, NULL, NULL, objlist, NULL, 0, h, w, h, backsig, thresh, satur, argc > 22 ? atof(argv[22]) : 1.0,
+                  0.0, gain, numdetected);
     clear_detection();
     clear_device(img);
 

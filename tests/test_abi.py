@@ -59,7 +59,7 @@ def test_config_rejected_without_device_work():
 
 COMPAT_NAMES = ["init_device", "clear_device", "back_estimate", "cudaFilter", "init_detection", "run_detection",
                 "clear_detection", "init_deblend", "parcel_out", "clear_deblend", "analyse_gpu", "run_clean",
-                "endobject_gpu", "sexgpu_compat_configure", "sexgpu_compat_set_device",
+                "endobject_gpu", "sexgpu_compat_configure", "sexgpu_compat_set_device", "sexgpu_compat_set_nnw",
                 "sexgpu_compat_set_error_handler"]
 
 
@@ -119,3 +119,27 @@ int main(void) {
     import ctypes as C
     B = sexgpu.BatchFrame
     assert vals == [C.sizeof(B), B.objs.offset, B.status.offset, B.summary.offset]
+
+
+def test_read_nnw(tmp_path):
+    """sexgpu_read_nnw parses the .nnw layout (host code, no GPU needed)."""
+    import pytest
+    import sexgpu
+    from conftest import synthetic_nnw, write_nnw
+    net = synthetic_nnw(3)
+    path = tmp_path / "t.nnw"
+    write_nnw(str(path), net)
+    got = sexgpu.read_nnw(str(path))
+    nn, inbias, inscale, weights, biases, outbias, outscale = net
+    assert got.nlayers == 3 and list(got.nn) == nn
+    assert list(got.inbias) == list(inbias) and list(got.inscale) == list(inscale)
+    for l in range(2):
+        for j in range(nn[l + 1]):
+            assert got.b[l][j] == biases[l][j]
+            for i in range(nn[l]):
+                assert got.w[l][i][j] == weights[l][i][j]
+    assert got.outbias[0] == outbias[0] and got.outscale[0] == outscale[0]
+    bad = tmp_path / "bad.nnw"
+    bad.write_text("not a network\n1 2 3\n")
+    with pytest.raises(RuntimeError):
+        sexgpu.read_nnw(str(bad))

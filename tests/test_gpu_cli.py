@@ -106,18 +106,24 @@ def test_cli_fits_ldac_with_weight_map(tmp_path, masks):
     m = masks["gauss_2.5_5x5"]
     conv.write_text("CONV NONORM\n" + "\n".join(" ".join("%.9g" % v for v in row) for row in m) + "\n")
     par = tmp_path / "t.param"
-    par.write_text("NUMBER\nX_IMAGE\nY_IMAGE\nFLUX_ISO\nFLUXERR_ISO\nX2_IMAGE\nFLAGS\nFLUX_APER(1)\n")
+    par.write_text("NUMBER\nX_IMAGE\nY_IMAGE\nFLUX_ISO\nFLUXERR_ISO\nX2_IMAGE\nFLAGS\nFLUX_APER(1)\nCLASS_STAR\n")
+    from conftest import synthetic_nnw, write_nnw
+    net = synthetic_nnw(9)
+    nnw = tmp_path / "t.nnw"
+    write_nnw(str(nnw), net)
     cfgf = tmp_path / "t.sex"
     cfgf.write_text("CATALOG_TYPE FITS_LDAC\nFILTER_NAME %s\nPARAMETERS_NAME %s\nWEIGHT_TYPE MAP_VAR\n"
-                    "WEIGHT_IMAGE %s\nBACK_SIZE 64\n" % (conv, par, wfits))
+                    "WEIGHT_IMAGE %s\nBACK_SIZE 64\nSTARNNW_NAME %s\nSEEING_FWHM 0.9\nPIXEL_SCALE 0.3\n"
+                    % (conv, par, wfits, nnw))
     cat = tmp_path / "t.ldac"
     subprocess.check_call([SEX, str(fits), "-c", str(cfgf), "-CATALOG_NAME", str(cat), "-VERBOSE_TYPE", "QUIET"],
                           cwd=str(tmp_path))
     t = read_ldac_objects(str(cat))
-    o, _, _ = O.extract(img, conv=m, weight_type=1, weight=vm)
+    o, _, _ = O.extract(img, conv=m, weight_type=1, weight=vm, nnw=O.NNW.from_arrays(*net), seeing_fwhm=0.9,
+                        pixel_scale=0.3)
     assert len(t) == len(o) > 0
     assert list(t.dtype.names) == ["NUMBER", "X_IMAGE", "Y_IMAGE", "FLUX_ISO", "FLUXERR_ISO", "X2_IMAGE", "FLAGS",
-                                   "FLUX_APER"]
+                                   "FLUX_APER", "CLASS_STAR"]
     assert t.dtype["X2_IMAGE"] == np.dtype(">f8") and t.dtype["NUMBER"] == np.dtype(">i4")
     assert np.array_equal(t["NUMBER"], o["number"])
     assert np.array_equal(t["FLAGS"], o["flags"])
@@ -126,3 +132,5 @@ def test_cli_fits_ldac_with_weight_map(tmp_path, masks):
     assert np.array_equal(t["FLUXERR_ISO"], o["fluxerr_iso"])
     assert np.array_equal(t["X2_IMAGE"], o["mx2"])
     assert np.array_equal(t["FLUX_APER"], o["flux_aper"])
+    # CLASS_STAR: log10/exp of the GPU against glibc's (as in test_gpu_parity)
+    assert np.allclose(t["CLASS_STAR"], o["class_star"], rtol=0, atol=1e-6) and o["class_star"].std() > 0

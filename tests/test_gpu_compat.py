@@ -39,7 +39,7 @@ def harness(tmp_path_factory):
     return exe, d
 
 
-@pytest.mark.parametrize("case", ["c0", "crowded"])
+@pytest.mark.parametrize("case", ["c0", "crowded", "class_star"])
 def test_reference_call_sequence(gpu_ctx, masks, harness, case):
     exe, d = harness
     if case == "c0":
@@ -58,12 +58,24 @@ def test_reference_call_sequence(gpu_ctx, masks, harness, case):
     args = [exe, str(fimg), str(w), str(h), str(fmask), str(mask.shape[0]), str(frows), str(fsub),
             str(opts["back_size"]), str(opts["back_filtersize"]), "0.0", "1.5", "1.5", "5", "32", "0.005",
             str(opts["clean_flag"]), repr(opts["clean_param"]), repr(opts["gain"]), repr(opts["satur_level"])]
+    net = None
+    if case == "class_star":
+        from conftest import synthetic_nnw, write_nnw
+        net = synthetic_nnw(13)
+        write_nnw(str(d / "t.nnw"), net)
+        args += [str(d / "t.nnw"), "1.3", "0.5"]
+        opts.update(seeing_fwhm=1.3, pixel_scale=0.5)
     out = subprocess.run(args, capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stderr
     rows = np.fromfile(frows, OUTOBJ)
     sub_c = np.fromfile(fsub, np.float32).reshape(h, w)
 
-    g, seg, s, sub_g, cd_g = gpu_ctx.extract(img, conv=mask, numbering=1, want_maps=True, **opts)
+    if net is not None:
+        gpu_ctx.set_nnw(sexgpu.NNW.from_arrays(*net))
+    try:
+        g, seg, s, sub_g, cd_g = gpu_ctx.extract(img, conv=mask, numbering=1, want_maps=True, **opts)
+    finally:
+        gpu_ctx.set_nnw(None)
     assert np.array_equal(sub_c, sub_g)
     assert len(rows) == len(g) == s.nobj
     assert np.array_equal(rows["number"], np.arange(len(g)))
@@ -75,4 +87,5 @@ def test_reference_call_sequence(gpu_ctx, masks, harness, case):
         assert np.array_equal(rows[name], g[name].astype(rows[name].dtype)), name
     assert np.array_equal(rows["kronfactor"], g["kronfactor"])
     assert np.array_equal(rows["flag"].astype(np.int32), g["flags"])
-    assert not rows["alpha2000"].any() and not rows["sprob"].any()
+    assert not rows["alpha2000"].any()
+    assert np.array_equal(rows["sprob"], g["class_star"]) and (rows["sprob"].any() == (net is not None))

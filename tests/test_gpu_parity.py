@@ -20,6 +20,10 @@ RTOL_REORDERED = 1e-9
 REORDERED = {"poserr_mx2", "poserr_my2", "poserr_mxy", "fwhm"}
 RTOL_LOG = 2.5e-7
 LOGCOLS = {"mag_iso", "mag_auto", "mag_aper"}
+# CLASS_STAR goes through log10 and exp in double (CUDA's on the GPU, glibc's
+# in the oracle) before its single rounding to float
+ATOL_CLASS = 1e-6
+CLASSCOLS = {"class_star"}
 
 
 def compare_catalogs(g, o):
@@ -31,6 +35,8 @@ def compare_catalogs(g, o):
             ok = np.isclose(a, b, rtol=RTOL_REORDERED, atol=1e-12) | (np.isnan(a) & np.isnan(b))
         elif name in LOGCOLS:
             ok = np.isclose(a, b, rtol=RTOL_LOG, atol=0)
+        elif name in CLASSCOLS:
+            ok = np.isclose(a, b, rtol=0, atol=ATOL_CLASS)
         else:
             ok = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else (a == b)
         if ok.ndim > 1:
@@ -220,3 +226,24 @@ def test_kron_param_rejects_bad_values(gpu_ctx):
         gpu_ctx.set_param("kron_warp_max", 0)
     with pytest.raises(RuntimeError):
         gpu_ctx.set_param("no_such_parameter", 1)
+
+
+def test_class_star(masks):
+    """CLASS_STAR from a (seeded, synthetic) 10-10-1 network, against the
+    oracle; without a network the column is 0 and nothing else changes."""
+    import sexgpu
+    from conftest import synthetic_nnw
+    net = synthetic_nnw(5)
+    img = synth.frame_c1(seed=81, w=900, h=800, nsrc=5000)
+    kw = dict(conv=masks["gauss_2.5_5x5"], seeing_fwhm=1.1, pixel_scale=0.4)
+    with sexgpu.Context(0) as ctx:
+        g0, _, _ = ctx.extract(img, **kw)
+        assert not g0["class_star"].any()
+        ctx.set_nnw(sexgpu.NNW.from_arrays(*net))
+        g, gseg, gs = ctx.extract(img, **kw)
+    o, oseg, os_ = O.extract(img, nnw=O.NNW.from_arrays(*net), **kw)
+    assert np.array_equal(gseg, oseg)
+    compare_catalogs(g, o)
+    cs = g["class_star"]
+    assert len(g) > 500 and cs.std() > 0.01 and np.isfinite(cs).all()
+    assert np.array_equal(g0["flux_auto"], g["flux_auto"])
