@@ -29,6 +29,7 @@
 #include "k_deblend_local.cu"
 #include "k_analyse.cu"
 #include "k_post.cu"
+#include "k_fits.cu"
 
 using namespace sx;
 
@@ -86,6 +87,7 @@ struct sexgpu_ctx {
         skeys, svals, skalt, svalt, rows;
     DevBuf kitem[2], kchunk[2], kpart[2];  // queued Kron boxes
     DevBuf o_sprob;                        // CLASS_STAR per object
+    DevBuf fitsraw;                        // FITS data block as stored (sexgpu_extract_fits)
     DevBuf dnnw;                           // this context's copy of the CLASS_STAR network
     const sexgpu_nnw *nnw_dev = nullptr;   // network used (this context's or, for a batch worker, its owner's)
     int kron_warp_max = KR_WARP_MAX;
@@ -965,6 +967,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
         free_buf(ctx->kpart[i]);
     }
     free_buf(ctx->o_sprob);
+    free_buf(ctx->fitsraw);
     free_buf(ctx->dnnw);
     free_buf(ctx->dmask);
     for (auto &s : ctx->stages) cudaEventDestroy(s.ev);
@@ -1073,6 +1076,32 @@ int sexgpu_extract(sexgpu_ctx *ctx, const float *img, const float *var, int w, i
     long long N = (long long)w * h;
     EN(img, N * 4);
     CK(cudaMemcpyAsync(ctx->img.p, img, N * 4, cudaMemcpyHostToDevice, ctx->stream));
+    if (var) {
+        EN(var, N * 4);
+        CK(cudaMemcpyAsync(ctx->var.p, var, N * 4, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    int rc = sexgpu_extract_device(ctx, P<float>(ctx->img), var ? P<float>(ctx->var) : nullptr, w, h, cfg, sum);
+    if (rc) return rc;
+    return sexgpu_copy_results(ctx, objs, max_objects, nobj, segmap, sub, cd);
+}
+
+int sexgpu_extract_fits(sexgpu_ctx *ctx, const void *data, const sexgpu_fits_format *fmt, const float *var, int w,
+                        int h, const sexgpu_config *cfg, sexgpu_object *objs, int max_objects, int *nobj,
+                        int32_t *segmap, float *sub, float *cd, sexgpu_summary *sum) {
+    if (!ctx || !data || !fmt || w <= 0 || h <= 0) return SEXGPU_ERR_ARG;
+    const int bp = fmt->bitpix;
+    if (bp != 8 && bp != 16 && bp != 32 && bp != -32 && bp != -64) {
+        ctx->err = "unsupported BITPIX";
+        return SEXGPU_ERR_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    const long long N = (long long)w * h;
+    const size_t bytes = (size_t)N * (size_t)(bp < 0 ? -bp : bp) / 8;
+    EN(fitsraw, bytes);
+    EN(img, N * 4);
+    CK(cudaMemcpyAsync(ctx->fitsraw.p, data, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    launch_fits_to_float(ctx->fitsraw.p, bp, fmt->bscale, fmt->bzero, fmt->has_blank, fmt->blank, P<float>(ctx->img),
+                         N, ctx->stream);
     if (var) {
         EN(var, N * 4);
         CK(cudaMemcpyAsync(ctx->var.p, var, N * 4, cudaMemcpyHostToDevice, ctx->stream));

@@ -6,8 +6,9 @@
  * Reference: src/main.c:40 (argument loop :65-121), src/prefs.c:66 (readprefs,
  * `KEY value` lines, '#' comments), src/makeit.c:58 (per-image flow), and the
  * catalogue row of src/scan.c:331-406 (printobj).  The extraction itself is
- * the C ABI call sexgpu_extract() (include/sexgpu.h), which replaces
- * makeback() + scanimage().
+ * the C ABI call sexgpu_extract_fits() (include/sexgpu.h), which replaces
+ * read_body() + makeback() + scanimage(): the image's data block goes to the
+ * device as stored and is converted there.
  *
  * Supported keywords (the extraction settings of src/preflist.h):
  *   CATALOG_NAME CATALOG_TYPE (ASCII, ASCII_HEAD, FITS_LDAC) PARAMETERS_NAME
@@ -143,15 +144,14 @@ static double card_num(const char *hdr, int ncards, const char *key, double def,
 
 /* primary image of a FITS file as float (src/fits/fitsbody.c:195 read_body:
  * BITPIX 8/16/32/-32/-64, BSCALE/BZERO) */
-static float *read_fits(const char *path, int *w, int *h)
+/* the FITS data block of the primary HDU as stored, and its format */
+static unsigned char *read_fits_raw(const char *path, int *w, int *h, sexgpu_fits_format *fmt)
 {
     FILE *f = fopen(path, "rb");
     char *hdr = NULL;
-    int ncards = 0, end = 0, bitpix, naxis, i, found;
-    size_t n, bytes;
-    double bscale, bzero;
+    int ncards = 0, end = 0, naxis, i, found;
+    size_t bytes;
     unsigned char *raw;
-    float *img;
     if (!f) die("cannot open image ", path);
     while (!end) {
         hdr = (char *)realloc(hdr, (size_t)(ncards + 36) * 80);
@@ -160,47 +160,66 @@ static float *read_fits(const char *path, int *w, int *h)
             if (!strncmp(hdr + (size_t)(ncards + i) * 80, "END     ", 8)) end = 1;
         ncards += 36;
     }
-    bitpix = (int)card_num(hdr, ncards, "BITPIX", 0, &found);
+    fmt->bitpix = (int)card_num(hdr, ncards, "BITPIX", 0, &found);
     naxis = (int)card_num(hdr, ncards, "NAXIS", 0, &found);
     *w = (int)card_num(hdr, ncards, "NAXIS1", 0, &found);
     *h = (int)card_num(hdr, ncards, "NAXIS2", 0, &found);
-    bscale = card_num(hdr, ncards, "BSCALE", 1.0, &found);
-    bzero = card_num(hdr, ncards, "BZERO", 0.0, &found);
+    fmt->bscale = card_num(hdr, ncards, "BSCALE", 1.0, &found);
+    fmt->bzero = card_num(hdr, ncards, "BZERO", 0.0, &found);
+    fmt->blank = (int64_t)card_num(hdr, ncards, "BLANK", 0.0, &found);
+    fmt->has_blank = found && fmt->bitpix > 0;
     free(hdr);
     if (naxis < 2 || *w <= 0 || *h <= 0) die("not a 2-D image: ", path);
-    n = (size_t)*w * *h;
-    bytes = n * (size_t)(abs(bitpix) / 8);
+    if (fmt->bitpix != 8 && fmt->bitpix != 16 && fmt->bitpix != 32 && fmt->bitpix != -32 && fmt->bitpix != -64)
+        die("unsupported BITPIX in ", path);
+    bytes = (size_t)*w * *h * (size_t)(abs(fmt->bitpix) / 8);
     raw = (unsigned char *)malloc(bytes);
     if (fread(raw, 1, bytes, f) != bytes) die("truncated FITS data in ", path);
     fclose(f);
-    img = (float *)malloc(n * sizeof(float));
+    return raw;
+}
+
+/* the float frame of a data block, converted as src/fits/fitsbody.c:195
+ * (read_body) converts it, the same arithmetic sexgpu_extract_fits does on
+ * the device */
+static float *fits_to_float(const unsigned char *raw, const sexgpu_fits_format *fmt, size_t n)
+{
+    const float bs = (float)fmt->bscale, bz = (float)fmt->bzero;
+    const int bp = fmt->bitpix, bpp = abs(bp) / 8;
+    float *img = (float *)malloc(n * sizeof(float));
     for (size_t k = 0; k < n; k++) {
-        const unsigned char *q = raw + k * (size_t)(abs(bitpix) / 8);
-        double v;
-        switch (bitpix) {
-        case 8: v = q[0]; break;
-        case 16: v = (int16_t)((q[0] << 8) | q[1]); break;
-        case 32: v = (int32_t)(((uint32_t)q[0] << 24) | ((uint32_t)q[1] << 16) | ((uint32_t)q[2] << 8) | q[3]); break;
-        case -32: {
-            uint32_t u = ((uint32_t)q[0] << 24) | ((uint32_t)q[1] << 16) | ((uint32_t)q[2] << 8) | q[3];
+        const unsigned char *q = raw + k * (size_t)bpp;
+        float v;
+        if (bp == 8) {
+            v = (fmt->has_blank && q[0] == (unsigned char)fmt->blank) ? -1e30f : q[0] * bs + bz;
+        } else if (bp == 16) {
+            const short s = (short)((q[0] << 8) | q[1]);
+            v = (fmt->has_blank && s == (short)fmt->blank) ? -1e30f : s * bs + bz;
+        } else if (bp == 32) {
+            const int s = (int)(((uint32_t)q[0] << 24) | ((uint32_t)q[1] << 16) | ((uint32_t)q[2] << 8) | q[3]);
+            v = (fmt->has_blank && s == (int)fmt->blank) ? -1e30f : s * bs + bz;
+        } else if (bp == -32) {
+            const uint32_t u = ((uint32_t)q[0] << 24) | ((uint32_t)q[1] << 16) | ((uint32_t)q[2] << 8) | q[3];
             float fv;
             memcpy(&fv, &u, 4);
-            v = fv;
-            break;
-        }
-        case -64: {
+            v = (u & 0x7f800000u) == 0x7f800000u ? -1e30f : fv * bs + bz;
+        } else {
             uint64_t u = 0;
             double dv;
             for (int b = 0; b < 8; b++) u = (u << 8) | q[b];
             memcpy(&dv, &u, 8);
-            v = dv;
-            break;
+            v = ((u >> 32) & 0x7ff00000u) == 0x7ff00000u ? -1e30f : (float)(dv * bs + bz);
         }
-        default: die("unsupported BITPIX in ", path); v = 0;
-        }
-        img[k] = (float)(bscale * v + bzero);
-        if (img[k] != img[k]) img[k] = -1e30f;   /* NaN: unusable pixel */
+        img[k] = v;
     }
+    return img;
+}
+
+static float *read_fits(const char *path, int *w, int *h)
+{
+    sexgpu_fits_format fmt;
+    unsigned char *raw = read_fits_raw(path, w, h, &fmt);
+    float *img = fits_to_float(raw, &fmt, (size_t)*w * *h);
     free(raw);
     return img;
 }
@@ -556,7 +575,9 @@ int main(int argc, char **argv)
     prefs_t p;
     const char *image = NULL, *conf = "default.sex";
     int i, w, h, n = 0, rc, mw, mh;
-    float *img, *wmap = NULL;
+    float *img = NULL, *wmap = NULL;
+    unsigned char *raw;
+    sexgpu_fits_format fmt;
     sexgpu_object *objs;
     int32_t *seg = NULL;
     float *sub = NULL, *cd = NULL;
@@ -604,7 +625,7 @@ int main(int argc, char **argv)
         p.cfg.conv_w = mw;
         p.cfg.conv_h = mh;
     }
-    img = read_fits(image, &w, &h);
+    raw = read_fits_raw(image, &w, &h, &fmt);
     if (p.cfg.weight_type) {
         int ww, wh;
         if (!*p.weight_image) die("WEIGHT_IMAGE missing", NULL);
@@ -629,7 +650,8 @@ int main(int argc, char **argv)
         sub = (float *)malloc(sizeof(float) * (size_t)w * h);
         cd = (float *)malloc(sizeof(float) * (size_t)w * h);
     }
-    rc = sexgpu_extract(ctx, img, wmap, w, h, &p.cfg, objs, 1024, &n, seg, sub, cd, &s);
+    /* the data block goes to the device as stored and is converted there */
+    rc = sexgpu_extract_fits(ctx, raw, &fmt, wmap, w, h, &p.cfg, objs, 1024, &n, seg, sub, cd, &s);
     if (rc == SEXGPU_ERR_CAPACITY) {
         objs = (sexgpu_object *)realloc(objs, sizeof(sexgpu_object) * (size_t)(n + 1));
         rc = sexgpu_copy_results(ctx, objs, n, &n, NULL, NULL, NULL);
@@ -674,6 +696,7 @@ int main(int argc, char **argv)
         else if (!strcasecmp(p.check_type, "-BACKGROUND")) write_fits(p.check_name, sub, w, h, -32);
         else if (!strcasecmp(p.check_type, "FILTERED")) write_fits(p.check_name, cd, w, h, -32);
         else if (!strcasecmp(p.check_type, "BACKGROUND")) {
+            img = fits_to_float(raw, &fmt, (size_t)w * h);
             for (size_t k = 0; k < (size_t)w * h; k++) sub[k] = img[k] - sub[k];
             write_fits(p.check_name, sub, w, h, -32);
         }
@@ -684,6 +707,7 @@ int main(int argc, char **argv)
                 s.backmean, s.backsig, s.dthresh, s.ndetected, n, (double)(clock() - t0) / CLOCKS_PER_SEC);
     sexgpu_destroy(ctx);
     free(img);
+    free(raw);
     free(wmap);
     free(objs);
     free(seg);

@@ -107,6 +107,12 @@ class BatchFrame(C.Structure):
                 ("nobj", C.c_int32), ("status", C.c_int32), ("pad", C.c_int32), ("summary", Summary)]
 
 
+class FitsFormat(C.Structure):
+    """sexgpu_fits_format."""
+    _fields_ = [("bitpix", C.c_int32), ("has_blank", C.c_int32), ("blank", C.c_int64), ("bscale", C.c_double),
+                ("bzero", C.c_double)]
+
+
 class Stage(C.Structure):
     _fields_ = [("name", C.c_char * 24), ("launches", C.c_int32), ("ms", C.c_float)]
 
@@ -114,7 +120,7 @@ class Stage(C.Structure):
 EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extract",
            "sexgpu_extract_device", "sexgpu_copy_results", "sexgpu_background", "sexgpu_filter",
            "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times", "sexgpu_set_param",
-           "sexgpu_read_nnw", "sexgpu_set_nnw",
+           "sexgpu_read_nnw", "sexgpu_set_nnw", "sexgpu_extract_fits",
            "sexgpu_background_noalloc", "sexgpu_extract_batch"]
 
 _lib = None
@@ -248,6 +254,37 @@ class Context:
                                   _f(sub) if want_maps else None,
                                   _f(cd) if want_maps else None, C.byref(s))
         _check(rc, self.h, "sexgpu_extract")
+        if want_maps:
+            return objs[:n.value], seg, s, sub, cd
+        return objs[:n.value], seg, s
+
+    def extract_fits(self, data, bitpix, w, h, bscale=1.0, bzero=0.0, blank=None, max_objects=None,
+                     want_maps=False, segmap=True, weight=None, **kw):
+        """The FITS data block itself (bytes or uint8 array of w*h*|bitpix|/8
+        big-endian bytes) in; converted on the device as the FITS reader
+        converts it.  Returns what extract returns."""
+        cfg = make_config(**kw)
+        raw = np.frombuffer(bytes(data), np.uint8) if not isinstance(data, np.ndarray) else \
+            np.ascontiguousarray(data).view(np.uint8).ravel()
+        if raw.size != w * h * abs(bitpix) // 8:
+            raise ValueError("data block of %d bytes for %dx%d BITPIX %d" % (raw.size, w, h, bitpix))
+        fmt = FitsFormat(bitpix=bitpix, has_blank=blank is not None, blank=int(blank or 0), bscale=bscale,
+                         bzero=bzero)
+        wmap = np.ascontiguousarray(weight, np.float32) if weight is not None else None
+        if max_objects is None:
+            max_objects = w * h // max(1, cfg.detect_minarea) // 2 + 16
+        objs = np.zeros(max_objects, OBJECT_DTYPE)
+        seg = np.zeros((h, w), np.int32) if segmap else None
+        n = C.c_int()
+        s = Summary()
+        sub = np.zeros((h, w), np.float32) if want_maps else None
+        cd = np.zeros((h, w), np.float32) if want_maps else None
+        rc = lib().sexgpu_extract_fits(self.h, raw.ctypes.data_as(C.c_void_p), C.byref(fmt),
+                                       _f(wmap) if wmap is not None else None, w, h, C.byref(cfg),
+                                       objs.ctypes.data_as(C.c_void_p), max_objects, C.byref(n),
+                                       seg.ctypes.data_as(C.c_void_p) if segmap else None,
+                                       _f(sub) if want_maps else None, _f(cd) if want_maps else None, C.byref(s))
+        _check(rc, self.h, "sexgpu_extract_fits")
         if want_maps:
             return objs[:n.value], seg, s, sub, cd
         return objs[:n.value], seg, s

@@ -140,6 +140,24 @@ int sexgpu_extract(sexgpu_ctx *ctx, const float *img, const float *var, int w, i
                    const sexgpu_config *cfg, sexgpu_object *objs, int max_objects,
                    int *nobj, int32_t *segmap, float *sub, float *cd, sexgpu_summary *sum);
 
+/* FITS pixel data as stored in the file (src/fits/fitsbody.c:195 read_body) */
+typedef struct {
+    int32_t bitpix;             /* BITPIX: 8, 16, 32, -32, -64 */
+    int32_t has_blank;          /* a BLANK keyword is present (integer BITPIX) */
+    int64_t blank;              /* BLANK */
+    double  bscale, bzero;      /* BSCALE, BZERO */
+} sexgpu_fits_format;
+
+/* Same as sexgpu_extract for a frame given as the FITS data block itself
+ * (w*h pixels of |BITPIX|/8 big-endian bytes): the block crosses to the
+ * device at its stored size and is converted there as read_body does it
+ * (value * BSCALE + BZERO in float, with BSCALE and BZERO rounded to float;
+ * BITPIX -64 in double, rounded once; BLANK and non-finite values become
+ * -1e30, blank). */
+int sexgpu_extract_fits(sexgpu_ctx *ctx, const void *data, const sexgpu_fits_format *fmt, const float *var, int w,
+                        int h, const sexgpu_config *cfg, sexgpu_object *objs, int max_objects, int *nobj,
+                        int32_t *segmap, float *sub, float *cd, sexgpu_summary *sum);
+
 /* Same, for a frame already in device memory (d_img, d_var are device
  * pointers; d_img is not modified).  Results stay on the device; read them
  * with sexgpu_copy_results. */

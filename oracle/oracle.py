@@ -257,3 +257,28 @@ def ref_convolve(sub, mask):
     cd = np.zeros_like(sub)
     r.ref_convolve(_f(sub), w, h, _f(mask), mask.shape[1], mask.shape[0], _f(cd))
     return cd
+
+
+def fits_to_float(raw, bitpix, bscale=1.0, bzero=0.0, blank=None):
+    """The FITS data block (big-endian bytes) to the float32 frame, restating
+    read_body (src/fits/fitsbody.c:195): integer pixels (BITPIX 8 unsigned,
+    16/32 signed) -> value * bs + bz in float32 with bs, bz the float32
+    roundings of BSCALE, BZERO, BLANK -> -1e30; BITPIX -32: non-finite ->
+    -1e30, else value * bs + bz in float32; BITPIX -64: non-finite -> -1e30,
+    else value * bs + bz in float64 rounded once to float32."""
+    raw = np.frombuffer(bytes(raw), np.uint8) if not isinstance(raw, np.ndarray) else raw.view(np.uint8).ravel()
+    bs, bz = np.float32(bscale), np.float32(bzero)
+    code = {8: ">u1", 16: ">i2", 32: ">i4", -32: ">f4", -64: ">f8"}[bitpix]
+    v = raw.view(code)
+    if bitpix > 0:
+        out = v.astype(np.float32) * bs + bz
+        if blank is not None:
+            out[v == np.array(blank).astype(code)] = np.float32(-1e30)
+    elif bitpix == -32:
+        out = v.astype(np.float32) * bs + bz
+        out[~np.isfinite(v)] = np.float32(-1e30)
+    else:
+        with np.errstate(invalid="ignore", over="ignore"):
+            out = (v.astype(np.float64) * np.float64(bs) + np.float64(bz)).astype(np.float32)
+        out[~np.isfinite(v)] = np.float32(-1e30)
+    return out.astype(np.float32)
