@@ -88,6 +88,7 @@ struct sexgpu_ctx {
     DevBuf kitem[2], kchunk[2], kpart[2];  // queued Kron boxes
     DevBuf o_sprob;                        // CLASS_STAR per object
     DevBuf fitsraw;                        // FITS data block as stored (sexgpu_extract_fits)
+    DevBuf rmsd, rmsnode, rmsdnode, rmsu, rmsmap;  // background rms map (sexgpu_background_rms)
     DevBuf dnnw;                           // this context's copy of the CLASS_STAR network
     const sexgpu_nnw *nnw_dev = nullptr;   // network used (this context's or, for a batch worker, its owner's)
     int kron_warp_max = KR_WARP_MAX;
@@ -968,6 +969,11 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     }
     free_buf(ctx->o_sprob);
     free_buf(ctx->fitsraw);
+    free_buf(ctx->rmsd);
+    free_buf(ctx->rmsnode);
+    free_buf(ctx->rmsdnode);
+    free_buf(ctx->rmsu);
+    free_buf(ctx->rmsmap);
     free_buf(ctx->dnnw);
     free_buf(ctx->dmask);
     for (auto &s : ctx->stages) cudaEventDestroy(s.ev);
@@ -1109,6 +1115,35 @@ int sexgpu_extract_fits(sexgpu_ctx *ctx, const void *data, const sexgpu_fits_for
     int rc = sexgpu_extract_device(ctx, P<float>(ctx->img), var ? P<float>(ctx->var) : nullptr, w, h, cfg, sum);
     if (rc) return rc;
     return sexgpu_copy_results(ctx, objs, max_objects, nobj, segmap, sub, cd);
+}
+
+int sexgpu_background_rms(sexgpu_ctx *ctx, float *rms) {
+    if (!ctx || !rms) return SEXGPU_ERR_ARG;
+    const PipeState &ps = ctx->ps;
+    if (ps.stage < 1 || ps.Pm.w <= 0) {
+        ctx->err = "no extraction to take the rms map of";
+        return SEXGPU_ERR_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const FrameParams &Pm = ps.Pm;
+    const int w = Pm.w, h = Pm.h, nb = Pm.nbx * Pm.nby;
+    const long long N = (long long)w * h;
+    EN(rmsd, (size_t)nb * 4);
+    EN(rmsu, std::max((size_t)nb * 4 + 64, (size_t)h * Pm.nbx * 4));  // column spline, then row splines
+    EN(rmsnode, (size_t)h * Pm.nbx * 4);
+    EN(rmsdnode, (size_t)h * Pm.nbx * 4);
+    EN(rmsmap, (size_t)N * 4);
+    k_back_spline<<<(Pm.nbx + 127) / 128, 128, 0, st>>>(ps.B.sigma3, P<float>(ctx->rmsd), P<float>(ctx->rmsu), Pm.nbx,
+                                                        Pm.nby);
+    k_row_nodes<<<(h + 127) / 128, 128, 0, st>>>(ps.B.sigma3, P<float>(ctx->rmsd), Pm.nbx, Pm.nby, Pm.bh, h,
+                                                 P<float>(ctx->rmsnode), P<float>(ctx->rmsdnode),
+                                                 P<float>(ctx->rmsu));
+    k_rms_map<<<grid1(N, 256), 256, 0, st>>>(P<float>(ctx->rmsnode), P<float>(ctx->rmsdnode), ps.B.colk, ps.B.coldx,
+                                            Pm.nbx, w, N, P<float>(ctx->rmsmap));
+    CK(cudaMemcpyAsync(rms, ctx->rmsmap.p, (size_t)N * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SEXGPU_OK;
 }
 
 int sexgpu_background(sexgpu_ctx *ctx, float *img, int w, int h, const sexgpu_config *cfg, float *back,

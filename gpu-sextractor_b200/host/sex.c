@@ -16,7 +16,7 @@
  *   DEBLEND_NTHRESH DEBLEND_MINCONT CLEAN CLEAN_PARAM MASK_TYPE
  *   PHOT_APERTURES PHOT_AUTOPARAMS SATUR_LEVEL MAG_ZEROPOINT GAIN
  *   BACK_SIZE BACK_FILTERSIZE BACK_FILTTHRESH BACK_TYPE BACK_VALUE
- *   CHECKIMAGE_TYPE (NONE, SEGMENTATION, BACKGROUND, -BACKGROUND, FILTERED)
+ *   CHECKIMAGE_TYPE (NONE, SEGMENTATION, BACKGROUND, BACKGROUND_RMS, -BACKGROUND, FILTERED)
  *   CHECKIMAGE_NAME VERBOSE_TYPE
  *   WEIGHT_TYPE (NONE, MAP_VAR, MAP_RMS, MAP_WEIGHT) WEIGHT_IMAGE
  *   STARNNW_NAME SEEING_FWHM PIXEL_SCALE (CLASS_STAR)
@@ -695,6 +695,11 @@ int main(int argc, char **argv)
         if (!strcasecmp(p.check_type, "SEGMENTATION")) write_fits(p.check_name, seg, w, h, 32);
         else if (!strcasecmp(p.check_type, "-BACKGROUND")) write_fits(p.check_name, sub, w, h, -32);
         else if (!strcasecmp(p.check_type, "FILTERED")) write_fits(p.check_name, cd, w, h, -32);
+        else if (!strcasecmp(p.check_type, "BACKGROUND_RMS")) {
+            /* src/check.c:221: the rms map, made on the device */
+            if (sexgpu_background_rms(ctx, cd) != SEXGPU_OK) die("rms map: ", sexgpu_last_error(ctx));
+            write_fits(p.check_name, cd, w, h, -32);
+        }
         else if (!strcasecmp(p.check_type, "BACKGROUND")) {
             img = fits_to_float(raw, &fmt, (size_t)w * h);
             for (size_t k = 0; k < (size_t)w * h; k++) sub[k] = img[k] - sub[k];

@@ -120,7 +120,7 @@ class Stage(C.Structure):
 EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extract",
            "sexgpu_extract_device", "sexgpu_copy_results", "sexgpu_background", "sexgpu_filter",
            "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times", "sexgpu_set_param",
-           "sexgpu_read_nnw", "sexgpu_set_nnw", "sexgpu_extract_fits",
+           "sexgpu_read_nnw", "sexgpu_set_nnw", "sexgpu_extract_fits", "sexgpu_background_rms",
            "sexgpu_background_noalloc", "sexgpu_extract_batch"]
 
 _lib = None
@@ -288,6 +288,12 @@ class Context:
         if want_maps:
             return objs[:n.value], seg, s, sub, cd
         return objs[:n.value], seg, s
+
+    def background_rms(self, shape):
+        """Background rms map of the last extraction (h, w float32)."""
+        rms = np.zeros(shape, np.float32)
+        _check(lib().sexgpu_background_rms(self.h, _f(rms)), self.h, "sexgpu_background_rms")
+        return rms
 
     def extract_device(self, dev_ptr, w, h, wmap_ptr=None, **kw):
         """Frame (and weight map) already in device memory (e.g. torch tensor

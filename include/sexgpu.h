@@ -169,6 +169,11 @@ int sexgpu_extract_device(sexgpu_ctx *ctx, const float *d_img, const float *d_va
 int sexgpu_copy_results(sexgpu_ctx *ctx, sexgpu_object *objs, int max_objects, int *nobj,
                         int32_t *segmap, float *sub, float *cd);
 
+/* The background rms map of the last extraction (src/back.c:938
+ * backrmsline; the BACKGROUND_RMS check image, src/check.c:221): w*h host
+ * floats, the filtered sigma mesh map through the background's splines. */
+int sexgpu_background_rms(sexgpu_ctx *ctx, float *rms);
+
 /* Background only (makeback + subbackline): img (host, w*h) is replaced by
  * the background-subtracted frame; back/sigma (host, nbackx*nbacky, may be
  * NULL) receive the filtered mesh maps. */

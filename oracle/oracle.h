@@ -154,6 +154,8 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
 /* Read and normalise a .conv mask (src/filter.c:101-185).
  * Returns number of elements, or <0 on error. */
 int orc_getconv(const char *path, float *mask, int maxn, int *mw, int *mh);
+/* background rms map (w*h), src/back.c:938 backrmsline */
+int orc_background_rms(const float *img, int w, int h, const orc_config *cfg, float *rms);
 
 /* Small helpers exposed for unit tests. */
 float   orc_hmedian(float *ra, int n);

@@ -173,6 +173,16 @@ def background(img, **kw):
     return sub, back, sig, s
 
 
+def background_rms(img, **kw):
+    """Background rms map (w*h float32, backrmsline)."""
+    cfg = make_config(**kw)
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    rms = np.zeros_like(img)
+    h, w = img.shape
+    lib().orc_background_rms(_f(img), w, h, C.byref(cfg), _f(rms))
+    return rms
+
+
 def filter_image(sub, mask):
     sub = np.ascontiguousarray(sub, np.float32)
     mask = np.ascontiguousarray(mask, np.float32)
@@ -233,6 +243,18 @@ def ref_background(img, back_size=64, back_filtersize=3, back_filtthresh=0.0, ba
                      back_type, C.c_double(back_value), C.c_double(detect_thresh),
                      C.c_double(analysis_thresh), _f(back), _f(sig), _f(st))
     return sub, back, sig, st
+
+
+def ref_background_rms(img, back_size=64, back_filtersize=3, back_filtthresh=0.0):
+    """The reference's own makeback() + backrmsline() (None if not built)."""
+    r = ref()
+    if r is None:
+        return None
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    rms = np.zeros_like(img)
+    h, w = img.shape
+    r.ref_background_rms(_f(img), w, h, back_size, back_filtersize, C.c_double(back_filtthresh), _f(rms))
+    return rms
 
 
 def ref_getconv(path):

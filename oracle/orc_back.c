@@ -482,6 +482,33 @@ float orc_back_at(const float *b, int nx, int ny, int backw, int backh, int x, i
     return (float)((1 - dy) * (cdx * b0 + dx * b1) + dy * (dx * b2 + cdx * b3));
 }
 
+/* The background rms map (src/back.c:938 backrmsline): the filtered sigma
+   mesh map through the same y and x splines as the background. */
+int orc_background_rms(const float *img, int w, int h, const orc_config *cfg, float *rms)
+{
+    int bw = cfg->back_size < w ? cfg->back_size : w, bh = cfg->back_size < h ? cfg->back_size : h;
+    int nx = (w - 1) / bw + 1, ny = (h - 1) / bh + 1, y;
+    size_t p, nb = (size_t)nx * ny;
+    float *copy = (float *)malloc(sizeof(float) * (size_t)w * h);
+    float *sigma = (float *)malloc(sizeof(float) * nb), *dsigma = (float *)malloc(sizeof(float) * nb);
+    memcpy(copy, img, sizeof(float) * (size_t)w * h);
+    orc_background(copy, w, h, cfg, NULL, sigma, NULL, dsigma, NULL);
+    for (y = 0; y < h; y++) {
+        float *line = rms + (size_t)y * w;
+        for (p = 0; p < (size_t)w; p++)
+            line[p] = -0.0f;
+        /* the line minus the interpolated map: -0 - v = -v for every v (zeros
+           included), negated back exactly */
+        sub_back_line(sigma, dsigma, nx, ny, bw, bh, 0, 0.0f, y, line, w);
+        for (p = 0; p < (size_t)w; p++)
+            line[p] = -line[p];
+    }
+    free(copy);
+    free(sigma);
+    free(dsigma);
+    return 0;
+}
+
 int orc_background(float *img, int w, int h, const orc_config *cfg,
                    float *back_out, float *sigma_out, float *dback_out, float *dsigma_out,
                    orc_summary *sum)

@@ -134,3 +134,20 @@ def test_cli_fits_ldac_with_weight_map(tmp_path, masks):
     assert np.array_equal(t["FLUX_APER"], o["flux_aper"])
     # CLASS_STAR: log10/exp of the GPU against glibc's (as in test_gpu_parity)
     assert np.allclose(t["CLASS_STAR"], o["class_star"], rtol=0, atol=1e-6) and o["class_star"].std() > 0
+
+
+def test_cli_background_rms_check_image(tmp_path, masks):
+    if not os.path.exists(SEX):
+        subprocess.check_call(["make", "-s", "-C", os.path.dirname(SEX)])
+    img = synth.frame_c0(seed=4, w=300, h=200, nsrc=200)
+    fits = tmp_path / "img.fits"
+    write_fits(str(fits), img)
+    out = tmp_path / "rms.fits"
+    subprocess.check_call([SEX, str(fits), "-CATALOG_NAME", str(tmp_path / "c.cat"), "-CATALOG_TYPE", "ASCII",
+                           "-FILTER", "N", "-BACK_SIZE", "40", "-CHECKIMAGE_TYPE", "BACKGROUND_RMS",
+                           "-CHECKIMAGE_NAME", str(out), "-VERBOSE_TYPE", "QUIET"], cwd=str(tmp_path))
+    with open(out, "rb") as f:
+        raw = f.read()
+    got = np.frombuffer(raw[2880:2880 + 4 * 300 * 200], ">f4").reshape(200, 300)
+    ref = O.background_rms(img, back_size=40)
+    assert np.array_equal(got, ref)

@@ -247,3 +247,13 @@ def test_class_star(masks):
     cs = g["class_star"]
     assert len(g) > 500 and cs.std() > 0.01 and np.isfinite(cs).all()
     assert np.array_equal(g0["flux_auto"], g["flux_auto"])
+
+
+@pytest.mark.parametrize("w,h,bs,fs", [(512, 384, 64, 3), (333, 257, 50, 5), (1000, 37, 64, 3), (300, 300, 32, 1)])
+def test_background_rms_map(gpu_ctx, w, h, bs, fs):
+    """BACKGROUND_RMS of the last extraction against the oracle, bit for bit."""
+    img = synth.frame_c0(seed=15, w=w, h=h, nsrc=max(20, w * h // 800))
+    gpu_ctx.extract(img, back_size=bs, back_filtersize=fs)
+    g = gpu_ctx.background_rms(img.shape)
+    o = O.background_rms(img, back_size=bs, back_filtersize=fs)
+    assert g.tobytes() == o.tobytes()

@@ -86,3 +86,15 @@ def test_background_matches_reference_live(seed, w, h, bs):
     assert np.array_equal(back, rback) and np.array_equal(sig, rsig)
     assert np.array_equal(sub, rsub)
     assert (s.backmean, s.backsig, s.dthresh, s.thresh) == tuple(float(x) for x in rst)
+
+
+@pytest.mark.parametrize("bs,fs", [(64, 3), (50, 3), (32, 1), (128, 5)])
+def test_background_rms_matches_reference(bs, fs):
+    """The oracle's rms map (BACKGROUND_RMS) against the reference's own
+    makeback() + backrmsline() (src/back.c:938), bit for bit."""
+    if O.ref() is None:
+        pytest.skip("reference harness not built")
+    img = synth.frame_c0(seed=5, w=512, h=384)
+    a = O.background_rms(img, back_size=bs, back_filtersize=fs)
+    b = O.ref_background_rms(img, back_size=bs, back_filtersize=fs)
+    assert a.tobytes() == b.tobytes()
