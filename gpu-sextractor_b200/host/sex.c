@@ -20,6 +20,8 @@
  *   CHECKIMAGE_NAME VERBOSE_TYPE
  *   WEIGHT_TYPE (NONE, MAP_VAR, MAP_RMS, MAP_WEIGHT) WEIGHT_IMAGE
  *   STARNNW_NAME SEEING_FWHM PIXEL_SCALE (CLASS_STAR)
+ * Multi-extension files: every image extension is a frame of one batched
+ * extraction; catalogue rows carry EXT_NUMBER.
  * Other keywords of the reference are accepted and ignored.
  */
 #include <ctype.h>
@@ -179,6 +181,89 @@ static unsigned char *read_fits_raw(const char *path, int *w, int *h, sexgpu_fit
     return raw;
 }
 
+/* Every image HDU of a file (primary or XTENSION = 'IMAGE', NAXIS >= 2; the
+ * first plane of a cube), as stored: a multi-extension file gives one frame
+ * per CCD, as makeit() walks the extensions (src/makeit.c:164-228). */
+typedef struct {
+    int w, h;
+    sexgpu_fits_format fmt;
+    unsigned char *raw;
+} fits_image;
+
+static int card_has(const char *hdr, int ncards, const char *key, const char *text)
+{
+    char k[9];
+    snprintf(k, sizeof k, "%-8s", key);
+    for (int i = 0; i < ncards; i++)
+        if (!strncmp(hdr + (size_t)i * 80, k, 8)) {
+            char c[81];
+            memcpy(c, hdr + (size_t)i * 80, 80);
+            c[80] = 0;
+            return strstr(c + 8, text) != NULL;
+        }
+    return 0;
+}
+
+static int read_fits_images(const char *path, fits_image **out)
+{
+    FILE *f = fopen(path, "rb");
+    int nim = 0, cap = 0;
+    *out = NULL;
+    if (!f) die("cannot open image ", path);
+    for (int hdu = 0;; hdu++) {
+        char *hdr = NULL;
+        int ncards = 0, end = 0, found, i;
+        while (!end) {
+            hdr = (char *)realloc(hdr, (size_t)(ncards + 36) * 80);
+            if (fread(hdr + (size_t)ncards * 80, 80, 36, f) != 36) {
+                free(hdr);
+                if (hdu == 0) die("truncated FITS header in ", path);
+                fclose(f);
+                return nim;
+            }
+            for (i = 0; i < 36; i++)
+                if (!strncmp(hdr + (size_t)(ncards + i) * 80, "END     ", 8)) end = 1;
+            ncards += 36;
+        }
+        const int bitpix = (int)card_num(hdr, ncards, "BITPIX", 0, &found);
+        const int naxis = (int)card_num(hdr, ncards, "NAXIS", 0, &found);
+        size_t npix = naxis > 0 ? 1 : 0;
+        int dims[8] = {0};
+        for (i = 0; i < naxis && i < 8; i++) {
+            char key[16];
+            snprintf(key, sizeof key, "NAXIS%d", i + 1);
+            dims[i] = (int)card_num(hdr, ncards, key, 0, &found);
+            npix *= (size_t)(dims[i] > 0 ? dims[i] : 0);
+        }
+        const long pcount = (long)card_num(hdr, ncards, "PCOUNT", 0, &found);
+        const long gcount = (long)card_num(hdr, ncards, "GCOUNT", 1, &found);
+        const size_t bytes = (size_t)(abs(bitpix) / 8) * (size_t)gcount * (npix + (size_t)pcount);
+        const int image = (hdu == 0 || card_has(hdr, ncards, "XTENSION", "IMAGE")) && naxis >= 2 && dims[0] > 0 &&
+                          dims[1] > 0;
+        if (image) {
+            fits_image im;
+            im.w = dims[0];
+            im.h = dims[1];
+            im.fmt.bitpix = bitpix;
+            im.fmt.bscale = card_num(hdr, ncards, "BSCALE", 1.0, &found);
+            im.fmt.bzero = card_num(hdr, ncards, "BZERO", 0.0, &found);
+            im.fmt.blank = (int64_t)card_num(hdr, ncards, "BLANK", 0.0, &found);
+            im.fmt.has_blank = found && bitpix > 0;
+            if (bitpix != 8 && bitpix != 16 && bitpix != 32 && bitpix != -32 && bitpix != -64)
+                die("unsupported BITPIX in ", path);
+            const size_t plane = (size_t)im.w * im.h * (size_t)(abs(bitpix) / 8);
+            im.raw = (unsigned char *)malloc(plane);
+            if (fread(im.raw, 1, plane, f) != plane) die("truncated FITS data in ", path);
+            if (bytes > plane) fseek(f, (long)(bytes - plane), SEEK_CUR);
+            if (nim == cap) *out = (fits_image *)realloc(*out, sizeof(fits_image) * (size_t)(cap = cap ? 2 * cap : 4));
+            (*out)[nim++] = im;
+        } else if (bytes)
+            fseek(f, (long)bytes, SEEK_CUR);
+        if (bytes % 2880) fseek(f, (long)(2880 - bytes % 2880), SEEK_CUR);
+        free(hdr);
+    }
+}
+
 /* the float frame of a data block, converted as src/fits/fitsbody.c:195
  * (read_body) converts it, the same arithmetic sexgpu_extract_fits does on
  * the device */
@@ -310,7 +395,10 @@ static const col_t COLS[] = {
     {"XPEAK_IMAGE", "%10d", "pixel", "x-coordinate of the brightest pixel"},
     {"YPEAK_IMAGE", "%10d", "pixel", "y-coordinate of the brightest pixel"},
     {"CLASS_STAR", "%6.3f", "", "S/G classifier output"},
+    {"EXT_NUMBER", "%3d", "", "FITS extension number"},
     {NULL, NULL, NULL, NULL}};
+
+static int g_ext = 1;  /* extension of the rows being written (EXT_NUMBER) */
 
 static void print_col(FILE *f, int c, const sexgpu_object *o)
 {
@@ -361,6 +449,7 @@ static void print_col(FILE *f, int c, const sexgpu_object *o)
     case 42: fprintf(f, fmt, o->peakx); break;
     case 43: fprintf(f, fmt, o->peaky); break;
     case 44: fprintf(f, fmt, o->class_star); break;
+    case 45: fprintf(f, fmt, g_ext); break;
     }
 }
 
@@ -434,6 +523,7 @@ static double col_value(int c, const sexgpu_object *o)
     case 42: return o->peakx;
     case 43: return o->peaky;
     case 44: return o->class_star;
+    case 45: return g_ext;
     }
     return 0.0;
 }
@@ -466,11 +556,10 @@ static void card_int(FILE *f, const char *key, long v)
 /* FITS_LDAC catalogue (the layout of SExtractor's LDAC output): an empty
  * primary HDU, LDAC_IMHEAD (the image header as one character cell) and
  * LDAC_OBJECTS (one row per object, the .param columns, big-endian) */
-static void write_ldac(const char *path, const sexgpu_object *objs, int n, const int *sel, int ns, int w, int h)
+static FILE *ldac_open(const char *path)
 {
     FILE *f = fopen(path, "wb");
-    char card[81], hdr[6 * 80 + 1], form[32];
-    int k, ncard = 0, rowbytes = 0, nhdr = 6;
+    int ncard;
     if (!f) die("cannot write ", path);
     write_card(f, "SIMPLE  =                    T");
     write_card(f, "BITPIX  =                    8");
@@ -478,6 +567,14 @@ static void write_ldac(const char *path, const sexgpu_object *objs, int n, const
     write_card(f, "EXTEND  =                    T");
     write_card(f, "END");
     for (ncard = 5; ncard % 36; ncard++) write_card(f, "");
+    return f;
+}
+
+/* one image's LDAC_IMHEAD and LDAC_OBJECTS tables (one pair per extension) */
+static void ldac_write_ext(FILE *f, const sexgpu_object *objs, int n, const int *sel, int ns, int w, int h)
+{
+    char card[81], hdr[6 * 80 + 1], form[32];
+    int k, ncard = 0, rowbytes = 0, nhdr = 6;
     /* LDAC_IMHEAD */
     memset(hdr, ' ', sizeof hdr - 1);
     hdr[sizeof hdr - 1] = 0;
@@ -547,7 +644,6 @@ static void write_ldac(const char *path, const sexgpu_object *objs, int n, const
             }
         }
     pad_block(f, (long)rowbytes * n, 0);
-    fclose(f);
 }
 
 static int read_params(const char *path, int *sel, int maxsel)
@@ -570,11 +666,88 @@ static int read_params(const char *path, int *sel, int maxsel)
     return n;
 }
 
+/* ASCII / ASCII_HEAD rows of one image (the .param columns, or the
+ * reference's default row when there is no .param file) */
+static void write_ascii(FILE *cat, const prefs_t *p, const sexgpu_object *objs, int n, int head)
+{
+    int sel[64], ns = read_params(p->parameters_name, sel, 64), i, k;
+    if (ns == 0) {
+        for (i = 0; i < n; i++) printobj(cat, &objs[i]);
+        return;
+    }
+    if (head && !strcasecmp(p->catalog_type, "ASCII_HEAD"))
+        for (k = 0; k < ns; k++)
+            fprintf(cat, "#%4d %-22s %-58s [%s]\n", k + 1, COLS[sel[k]].name, COLS[sel[k]].comment, COLS[sel[k]].unit);
+    for (i = 0; i < n; i++) {
+        for (k = 0; k < ns; k++) {
+            if (k) fputc(' ', cat);
+            print_col(cat, sel[k], &objs[i]);
+        }
+        fputc('\n', cat);
+    }
+}
+
+/* A multi-extension file: every extension is a frame of one batched
+ * extraction (sexgpu_extract_batch: frames of uneven sizes on concurrent
+ * streams); NUMBER restarts in every extension and EXT_NUMBER tells them
+ * apart; FITS_LDAC gets one table pair per extension. */
+static int run_mef(const prefs_t *p, sexgpu_ctx *ctx, fits_image *ims, int nim)
+{
+    sexgpu_batch_frame *fr = (sexgpu_batch_frame *)calloc((size_t)nim, sizeof(sexgpu_batch_frame));
+    int k, rc, tot = 0;
+    if (strcasecmp(p->check_type, "NONE") || p->cfg.weight_type)
+        die("check images and weight maps need a single-image FITS file", NULL);
+    for (k = 0; k < nim; k++) {
+        const size_t npix = (size_t)ims[k].w * ims[k].h;
+        const int cap = (int)(npix / (size_t)(p->cfg.detect_minarea > 0 ? p->cfg.detect_minarea : 1) / 2 + 16);
+        fr[k].img = fits_to_float(ims[k].raw, &ims[k].fmt, npix);
+        fr[k].w = ims[k].w;
+        fr[k].h = ims[k].h;
+        fr[k].cfg = &p->cfg;
+        fr[k].objs = (sexgpu_object *)malloc(sizeof(sexgpu_object) * (size_t)cap);
+        fr[k].max_objects = cap;
+    }
+    rc = sexgpu_extract_batch(ctx, fr, nim, 4);
+    if (rc != SEXGPU_OK) {
+        fprintf(stderr, "sex: extraction failed (%d): %s\n", rc, sexgpu_last_error(ctx));
+        exit(EXIT_FAILURE);
+    }
+    if (strcasecmp(p->catalog_type, "NONE")) {
+        if (!strcasecmp(p->catalog_type, "FITS_LDAC")) {
+            int sel[64], ns = read_params(p->parameters_name, sel, 64);
+            FILE *f = ldac_open(p->catalog_name);
+            if (ns == 0)
+                for (ns = 0; COLS[ns].name; ns++) sel[ns] = ns;
+            for (k = 0; k < nim; k++) {
+                g_ext = k + 1;
+                ldac_write_ext(f, fr[k].objs, fr[k].nobj, sel, ns, fr[k].w, fr[k].h);
+            }
+            fclose(f);
+        } else {
+            FILE *cat = !strcmp(p->catalog_name, "STDOUT") ? stdout : fopen(p->catalog_name, "w");
+            if (!cat) die("cannot write ", p->catalog_name);
+            for (k = 0; k < nim; k++) {
+                g_ext = k + 1;
+                write_ascii(cat, p, fr[k].objs, fr[k].nobj, k == 0);
+            }
+            if (cat != stdout) fclose(cat);
+        }
+    }
+    for (k = 0; k < nim; k++) {
+        tot += fr[k].nobj;
+        free((void *)fr[k].img);
+        free(fr[k].objs);
+    }
+    free(fr);
+    return tot;
+}
+
 int main(int argc, char **argv)
 {
     prefs_t p;
     const char *image = NULL, *conf = "default.sex";
-    int i, w, h, n = 0, rc, mw, mh;
+    int i, w, h, n = 0, rc, mw, mh, nim;
+    fits_image *ims;
     float *img = NULL, *wmap = NULL;
     unsigned char *raw;
     sexgpu_fits_format fmt;
@@ -625,8 +798,13 @@ int main(int argc, char **argv)
         p.cfg.conv_w = mw;
         p.cfg.conv_h = mh;
     }
-    raw = read_fits_raw(image, &w, &h, &fmt);
-    if (p.cfg.weight_type) {
+    nim = read_fits_images(image, &ims);
+    if (nim == 0) die("no image in ", image);
+    raw = ims[0].raw;
+    fmt = ims[0].fmt;
+    w = ims[0].w;
+    h = ims[0].h;
+    if (p.cfg.weight_type && nim == 1) {
         int ww, wh;
         if (!*p.weight_image) die("WEIGHT_IMAGE missing", NULL);
         wmap = read_fits(p.weight_image, &ww, &wh);
@@ -643,6 +821,16 @@ int main(int argc, char **argv)
             sexgpu_set_nnw(ctx, &net);
         else if (p.nnw_given)
             die("cannot read the star/galaxy network ", p.nnw_name);
+    }
+    if (nim > 1) {
+        n = run_mef(&p, ctx, ims, nim);
+        if (strcasecmp(p.verbose, "QUIET"))
+            fprintf(stderr, "Extensions: %d / sextracted %d\n> All done (in %.2f s)\n", nim, n,
+                    (double)(clock() - t0) / CLOCKS_PER_SEC);
+        sexgpu_destroy(ctx);
+        for (i = 0; i < nim; i++) free(ims[i].raw);
+        free(ims);
+        return EXIT_SUCCESS;
     }
     objs = (sexgpu_object *)malloc(sizeof(sexgpu_object) * 1024);
     if (strcasecmp(p.check_type, "NONE")) {
@@ -664,29 +852,17 @@ int main(int argc, char **argv)
         FILE *cat = !strcmp(p.catalog_name, "STDOUT") ? stdout : fopen(p.catalog_name, "w");
         if (!cat) die("cannot write ", p.catalog_name);
         if (!strcasecmp(p.catalog_type, "ASCII_HEAD") || !strcasecmp(p.catalog_type, "ASCII")) {
-            int sel[64], ns = read_params(p.parameters_name, sel, 64), k;
-            if (ns == 0) {
-                for (i = 0; i < n; i++) printobj(cat, &objs[i]);
-            } else {
-                if (!strcasecmp(p.catalog_type, "ASCII_HEAD"))
-                    for (k = 0; k < ns; k++)
-                        fprintf(cat, "#%4d %-22s %-58s [%s]\n", k + 1, COLS[sel[k]].name, COLS[sel[k]].comment,
-                                COLS[sel[k]].unit);
-                for (i = 0; i < n; i++) {
-                    for (k = 0; k < ns; k++) {
-                        if (k) fputc(' ', cat);
-                        print_col(cat, sel[k], &objs[i]);
-                    }
-                    fputc('\n', cat);
-                }
-            }
+            write_ascii(cat, &p, objs, n, 1);
         } else if (!strcasecmp(p.catalog_type, "FITS_LDAC")) {
             int sel[64], ns = read_params(p.parameters_name, sel, 64);
+            FILE *f;
             if (cat != stdout) fclose(cat);
             cat = stdout;
             if (ns == 0)
                 for (ns = 0; COLS[ns].name; ns++) sel[ns] = ns;
-            write_ldac(p.catalog_name, objs, n, sel, ns, w, h);
+            f = ldac_open(p.catalog_name);
+            ldac_write_ext(f, objs, n, sel, ns, w, h);
+            fclose(f);
         } else
             for (i = 0; i < n; i++) printobj(cat, &objs[i]);
         if (cat != stdout) fclose(cat);
@@ -713,6 +889,7 @@ int main(int argc, char **argv)
     sexgpu_destroy(ctx);
     free(img);
     free(raw);
+    free(ims);
     free(wmap);
     free(objs);
     free(seg);

@@ -151,3 +151,57 @@ def test_cli_background_rms_check_image(tmp_path, masks):
     got = np.frombuffer(raw[2880:2880 + 4 * 300 * 200], ">f4").reshape(200, 300)
     ref = O.background_rms(img, back_size=40)
     assert np.array_equal(got, ref)
+
+
+def _hdu(cards, data):
+    hdr = "".join(c.ljust(80) for c in cards + ["END"])
+    hdr = hdr.ljust((len(hdr) + 2879) // 2880 * 2880)
+    data += b"\0" * ((2880 - len(data) % 2880) % 2880)
+    return hdr.encode() + data
+
+
+def test_cli_multi_extension_file(tmp_path, masks):
+    """A multi-extension file (empty primary HDU, three image extensions of
+    other sizes and BITPIX, a binary table between them): one batched
+    extraction, rows per extension with EXT_NUMBER, NUMBER restarting."""
+    if not os.path.exists(SEX):
+        subprocess.check_call(["make", "-s", "-C", os.path.dirname(SEX)])
+    frames = [synth.frame_c0(seed=51, w=300, h=200, nsrc=200), synth.frame_c0(seed=52, w=256, h=256, nsrc=250),
+              synth.frame_c0(seed=53, w=180, h=320, nsrc=150)]
+    blob = _hdu(["SIMPLE  =                    T", "BITPIX  =                    8", "NAXIS   =                    0",
+                 "EXTEND  =                    T"], b"")
+    expect = []
+    for k, img in enumerate(frames):
+        h, w = img.shape
+        if k == 1:
+            raw = np.clip(np.round((img - 800.0) / 0.5), -32767, 32767).astype(">i2").tobytes()
+            cards = ["BITPIX  =                   16", "BSCALE  =                  0.5", "BZERO   =                800.0"]
+            expect.append(O.fits_to_float(raw, 16, bscale=0.5, bzero=800.0).reshape(h, w))
+        else:
+            raw = img.astype(">f4").tobytes()
+            cards = ["BITPIX  =                  -32"]
+            expect.append(O.fits_to_float(raw, -32).reshape(h, w))
+        blob += _hdu(["XTENSION= 'IMAGE   '"] + cards + ["NAXIS   =                    2", "NAXIS1  = %20d" % w,
+                                                         "NAXIS2  = %20d" % h, "PCOUNT  =                    0",
+                                                         "GCOUNT  =                    1"], raw)
+        if k == 0:
+            blob += _hdu(["XTENSION= 'BINTABLE'", "BITPIX  =                    8", "NAXIS   =                    2",
+                          "NAXIS1  =                    8", "NAXIS2  =                   10",
+                          "PCOUNT  =                    0", "GCOUNT  =                    1",
+                          "TFIELDS =                    1", "TFORM1  = '1D      '"], b"\x01" * 80)
+    fits = tmp_path / "mef.fits"
+    fits.write_bytes(blob)
+    par = tmp_path / "t.param"
+    par.write_text("NUMBER\nEXT_NUMBER\nFLUX_ISO\nFLAGS\nX_IMAGE\n")
+    cat = tmp_path / "t.cat"
+    subprocess.check_call([SEX, str(fits), "-CATALOG_NAME", str(cat), "-CATALOG_TYPE", "ASCII_HEAD",
+                           "-PARAMETERS_NAME", str(par), "-FILTER", "N", "-VERBOSE_TYPE", "QUIET"], cwd=str(tmp_path))
+    rows = [l.split() for l in cat.read_text().splitlines() if l.strip() and not l.startswith("#")]
+    for k, img in enumerate(expect):
+        o, _, _ = O.extract(img, filter_flag=0)
+        mine = [r for r in rows if int(r[1]) == k + 1]
+        assert len(mine) == len(o) > 10
+        assert [int(r[0]) for r in mine] == list(o["number"])
+        assert [int(r[3]) for r in mine] == list(o["flags"])
+        assert np.array_equal(np.array([float(r[2]) for r in mine], np.float32),
+                              np.array(["%12.7g" % v for v in o["flux_iso"]], float).astype(np.float32))
