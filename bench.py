@@ -311,7 +311,7 @@ def host_state(frames):
             "memcpy_gb_s": round(2 * big.nbytes / dt / 1e9, 2)}
 
 
-def run_batch(ctx, frames, reps=3, workers=4, maxobj=400000):
+def run_batch(ctx, frames, reps=3, workers=8, maxobj=400000):
     """Plain path (sexgpu_extract, one frame after the other) against the
     batched form (sexgpu_extract_batch) on the same frames: host frames in,
     host catalogues out, wall clock around the whole batch; catalogues

@@ -742,7 +742,7 @@ static int dl_grid(K kernel, int nt, size_t smem, int *cache) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, nt, smem);
         cache[dev] = max(1, nsm) * max(1, per);
     }
-    return cache[dev];
+    return sx_share(cache[dev]);
 }
 
 static RootLists dl_lists(const int *lists, int *counts, size_t n, int a, int b = -1, int c = -1) {

@@ -422,16 +422,29 @@ void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const 
         if (mw * mh <= 121) memcpy(taps.m, M.host, sizeof(float) * mw * mh);
         const int bw = ST_TW + 2 * rxa, bh = ST_TH + 2 * (mh / 2);
         const size_t smem = 2 * sizeof(float) * (size_t)((bw * bh + 31) & ~31);
+        static int nsm_cache[64];
         int dev = 0, nsm = 148;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (dev >= 0 && dev < 64 && nsm_cache[dev] > 0) {
+            nsm = nsm_cache[dev];
+        } else {
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            if (dev >= 0 && dev < 64) nsm_cache[dev] = nsm;
+        }
 #define SP_LAUNCH(a, b, wt)                                                                              \
     do {                                                                                                \
         auto kern = k_sub_filter_pipe<a, b, wt>;                                                        \
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);             \
-        int per = 1;                                                                                    \
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, ST_THREADS, smem);                    \
-        const int grid = std::max(1, std::min(A.ntiles, nsm * std::max(per, 1)));                      \
+        static std::atomic<long long> cached{0};  /* (smem << 8) | resident CTAs, this instance */   \
+        long long c = cached.load();                                                                    \
+        int per = (int)(c & 255);                                                                       \
+        if ((c >> 8) != (long long)smem) {                                                              \
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);        \
+            per = 1;                                                                                    \
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, ST_THREADS, smem);                \
+            per = std::min(std::max(per, 1), 255);                                                      \
+            cached.store(((long long)smem << 8) | per);                                                 \
+        }                                                                                               \
+        const int grid = std::max(1, std::min(A.ntiles, sx_share(nsm * per)));                         \
         kern<<<grid, ST_THREADS, smem, st>>>(tmap, A, taps);                                            \
     } while (0)
 #define SP_MASK(wt)                    \

@@ -691,8 +691,15 @@ __global__ void k_write_rows(ObjBufs O, const unsigned *vals, int ns, float dthr
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ns) return;
     int o = (int)vals[k];
-    sexgpu_object q;
-    memset(&q, 0, sizeof(q));  // padding bytes too: rows are byte-for-byte reproducible
+    // built in a union with 16-byte words so that the row, padding bytes
+    // included, is stored as whole words (rows are byte-for-byte reproducible)
+    union {
+        sexgpu_object o;
+        uint4 v[sizeof(sexgpu_object) / 16];
+    } u;
+    static_assert(sizeof(sexgpu_object) % 16 == 0, "row size");
+    for (int i = 0; i < (int)(sizeof(sexgpu_object) / 16); i++) u.v[i] = make_uint4(0, 0, 0, 0);
+    sexgpu_object &q = u.o;
     q.number = k + 1;
     q.root = O.root[o];
     q.level = O.level[o];
@@ -753,9 +760,10 @@ __global__ void k_write_rows(ObjBufs O, const unsigned *vals, int ns, float dthr
     q.elong = q.a / q.b;
     q.ellip = 1 - q.b / q.a;
     q.polar = (q.a * q.a - q.b * q.b) / (q.a * q.a + q.b * q.b);
-    // byte copy: an assignment may store the members only and leave the
+    // whole words: an assignment may store the members only and leave the
     // padding of the destination row as it was
-    memcpy(rows + k, &q, sizeof(q));
+    uint4 *dst = reinterpret_cast<uint4 *>(rows + k);
+    for (int i = 0; i < (int)(sizeof(sexgpu_object) / 16); i++) dst[i] = u.v[i];
 }
 
 // segmentation map: NUMBER of the owning object, 0 elsewhere

@@ -39,6 +39,14 @@ struct DebBufs {
     int *rec;                           // merge record per element (k_dl_sweep -> k_dl_assign)
 };
 
+// Persistent grids (deblending classes, subtract/filter tiles) are sized to
+// the resident capacity divided by this (set per host thread; 1 by default,
+// the batch workers take the "batch_grid_div" parameter of their context:
+// measured on the 64-frame batch, whole-GPU grids with 8 workers were the
+// fastest).
+extern thread_local int sx_grid_div;
+inline int sx_share(int grid) { return sx_grid_div > 1 ? (grid + sx_grid_div - 1) / sx_grid_div : grid; }
+
 // Kron boxes too large for one warp, summed by whole CTAs (k_post.cu)
 constexpr int KR_CHUNK = 8192;     // box pixels per CTA work item
 constexpr int KR_THREADS = 256;

@@ -62,8 +62,13 @@ struct PipeState {
 };
 }  // namespace
 
+namespace sx {
+thread_local int sx_grid_div = 1;
+}
+
 struct sexgpu_ctx {
     int device = 0;
+    int batch_grid_div = 1;  // persistent-grid divisor of batch workers
     PipeState ps;
     cudaStream_t stream = nullptr;
     cudaStream_t side[2] = {nullptr, nullptr};  // fork/join helpers of the deblending
@@ -1310,7 +1315,7 @@ int sexgpu_getconv(const char *path, float *mask, int maxn, int *mw, int *mh) {
 int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframes, int workers) {
     if (!ctx || nframes < 0 || (nframes > 0 && !frames) || workers < 0) return SEXGPU_ERR_ARG;
     if (nframes == 0) return SEXGPU_OK;
-    if (workers == 0) workers = 4;
+    if (workers == 0) workers = 8;
     workers = std::min(workers, nframes);
     while ((int)ctx->workers.size() < workers) {
         sexgpu_ctx *w = nullptr;
@@ -1348,8 +1353,10 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
         have = need;
         return true;
     };
+    const int div = ctx->batch_grid_div > 0 ? ctx->batch_grid_div : 1;
     auto run = [&](sexgpu_ctx *wc) {
         cudaSetDevice(wc->device);
+        sx_grid_div = div;
         for (int k; (k = next.fetch_add(1)) < nframes;) {
             sexgpu_batch_frame &f = frames[order[k]];
             f.nobj = 0;
@@ -1398,6 +1405,7 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
     for (int i = 1; i < workers; i++) pool.emplace_back(run, ctx->workers[i]);
     run(ctx->workers[0]);
     for (auto &t : pool) t.join();
+    sx_grid_div = 1;
     for (int i = 0; i < nframes; i++)
         if (frames[i].status != SEXGPU_OK) {
             ctx->err = "frame " + std::to_string(i) + " failed";
@@ -1483,6 +1491,11 @@ int sexgpu_read_nnw(const char *path, sexgpu_nnw *net) {
 
 int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value) {
     if (!ctx || !name) return SEXGPU_ERR_ARG;
+    if (!strcmp(name, "batch_grid_div")) {
+        if (value < 0) return SEXGPU_ERR_ARG;
+        ctx->batch_grid_div = value;
+        return SEXGPU_OK;
+    }
     if (!strcmp(name, "kron_warp_max")) {
         if (value < 1) return SEXGPU_ERR_ARG;
         ctx->kron_warp_max = value;

@@ -254,7 +254,7 @@ typedef struct {
 /* Extraction of many frames of any sizes and settings (the batched form of
  * scanimage(); no counterpart in the reference, which handles one frame per
  * process).  The frames are taken largest first by `workers` device streams
- * of this context's device (0: 4), each with its own buffers, so that the
+ * of this context's device (0: 8), each with its own buffers, so that the
  * stages of different frames overlap on the GPU.  Every frame's results are
  * exactly those of sexgpu_extract on that frame.  Returns SEXGPU_OK if every
  * frame succeeded, else the status of the first failed frame (each frame's
@@ -278,7 +278,9 @@ int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max);
 /* Execution parameters of this context (and of its batch workers); results
  * do not depend on them.  "kron_warp_max": AUTO-photometry boxes of more
  * pixels than this are summed by whole thread blocks instead of one warp
- * (default 8192, >= 1).  Returns SEXGPU_ERR_ARG for an unknown name or value. */
+ * (default 8192, >= 1).  "batch_grid_div": the persistent grids of
+ * sexgpu_extract_batch's workers use 1/n of the resident capacity each
+ * (default 1).  Returns SEXGPU_ERR_ARG for an unknown name or value. */
 int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value);
 
 #ifdef __cplusplus
