@@ -554,19 +554,23 @@ __global__ void k_back_spline(const float *__restrict__ map, float *__restrict__
 
 // src/back.c:938-1040 (backrmsline): the rms map of every pixel from the
 // row nodes of the sigma map, the same x interpolation as the background
+// square: write rms * rms (the variance of WEIGHT_TYPE BACKGROUND)
 __global__ void k_rms_map(const float *__restrict__ node, const float *__restrict__ dnode, const int *__restrict__ colk,
-                          const float *__restrict__ coldx, int nbx, int w, long long n, float *__restrict__ out) {
+                          const float *__restrict__ coldx, int nbx, int w, long long n, float *__restrict__ out,
+                          int square) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const int y = (int)(p / w), x = (int)(p - (long long)y * w);
     const float *nd = node + (size_t)y * nbx, *dnd = dnode + (size_t)y * nbx;
+    float v;
     if (nbx <= 1) {
-        out[p] = nd[0];
-        return;
+        v = nd[0];
+    } else {
+        const int k = colk[x];
+        const float dx = coldx[x], cdx = 1 - dx;
+        v = (float)(cdx * (nd[k] + (cdx * cdx - 1) * dnd[k]) + dx * (nd[k + 1] + (dx * dx - 1) * dnd[k + 1]));
     }
-    const int k = colk[x];
-    const float dx = coldx[x], cdx = 1 - dx;
-    out[p] = (float)(cdx * (nd[k] + (cdx * cdx - 1) * dnd[k]) + dx * (nd[k + 1] + (dx * dx - 1) * dnd[k + 1]));
+    out[p] = square ? v * v : v;
 }
 
 // src/back.c:790-862: y-interpolated nodes of every image row and their

@@ -221,7 +221,7 @@ int check_config(const sexgpu_config *cfg, int w, int h) {
                              cfg->conv_h > SX_MAXCONV))
         return SEXGPU_ERR_ARG;
     if (cfg->detect_minarea < 1 || cfg->deblend_nthresh < 1 || cfg->deblend_nthresh > 64) return SEXGPU_ERR_ARG;
-    if (cfg->weight_type < 0 || cfg->weight_type > 3) return SEXGPU_ERR_ARG;
+    if (cfg->weight_type < 0 || cfg->weight_type > 4) return SEXGPU_ERR_ARG;
     if (!(cfg->seeing_fwhm > 0.0)) return SEXGPU_ERR_ARG;
     return SEXGPU_OK;
 }
@@ -407,7 +407,8 @@ unsigned grid1(long long n, int t) { return n > 0 ? (unsigned)((n + t - 1) / t) 
 // ---------------------------------------------------------------------------
 int pipe_begin(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, int h, const sexgpu_config *cfg) {
     int rc = check_config(cfg, w, h);
-    if (!rc && (cfg->weight_type != 0) != (d_wmap != nullptr)) rc = SEXGPU_ERR_ARG;
+    // MAP_VAR, MAP_RMS, MAP_WEIGHT need a weight map; NONE and BACKGROUND take none
+    if (!rc && (cfg->weight_type >= 1 && cfg->weight_type <= 3) != (d_wmap != nullptr)) rc = SEXGPU_ERR_ARG;
     if (rc) {
         ctx->err = "invalid configuration or frame size";
         return rc;
@@ -493,6 +494,25 @@ int pipe_begin(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, 
         launch_weight_var(B, d_wmap, Pm, P<float>(ctx->wratio), P<float>(ctx->wvar), d_sc, st);
         ps.wvar = P<float>(ctx->wvar);
         nl += Pm.wtype != 2 ? 3 : 1;
+    } else if (Pm.wtype == 4) {
+        // WEIGHT_TYPE BACKGROUND: the variance of every pixel is the square of
+        // the background rms map (the sigma mesh map through the background's
+        // splines, as BACKGROUND_RMS)
+        const int nbm = Pm.nbx * Pm.nby;
+        EN(wvar, N * 4);
+        EN(rmsd, (size_t)nbm * 4);
+        EN(rmsu, std::max((size_t)nbm * 4 + 64, (size_t)h * Pm.nbx * 4));
+        EN(rmsnode, (size_t)h * Pm.nbx * 4);
+        EN(rmsdnode, (size_t)h * Pm.nbx * 4);
+        k_back_spline<<<(Pm.nbx + 127) / 128, 128, 0, st>>>(B.sigma3, P<float>(ctx->rmsd), P<float>(ctx->rmsu), Pm.nbx,
+                                                            Pm.nby);
+        k_row_nodes<<<(h + 127) / 128, 128, 0, st>>>(B.sigma3, P<float>(ctx->rmsd), Pm.nbx, Pm.nby, Pm.bh, h,
+                                                     P<float>(ctx->rmsnode), P<float>(ctx->rmsdnode),
+                                                     P<float>(ctx->rmsu));
+        k_rms_map<<<grid1(N, 256), 256, 0, st>>>(P<float>(ctx->rmsnode), P<float>(ctx->rmsdnode), B.colk, B.coldx,
+                                                Pm.nbx, w, N, P<float>(ctx->wvar), 1);
+        ps.wvar = P<float>(ctx->wvar);
+        nl += 3;
     }
     stage_mark(ctx, "background", nl + 1);
     ps.stage = 1;
@@ -1145,7 +1165,7 @@ int sexgpu_background_rms(sexgpu_ctx *ctx, float *rms) {
                                                  P<float>(ctx->rmsnode), P<float>(ctx->rmsdnode),
                                                  P<float>(ctx->rmsu));
     k_rms_map<<<grid1(N, 256), 256, 0, st>>>(P<float>(ctx->rmsnode), P<float>(ctx->rmsdnode), ps.B.colk, ps.B.coldx,
-                                            Pm.nbx, w, N, P<float>(ctx->rmsmap));
+                                            Pm.nbx, w, N, P<float>(ctx->rmsmap), 0);
     CK(cudaMemcpyAsync(rms, ctx->rmsmap.p, (size_t)N * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return SEXGPU_OK;

@@ -18,7 +18,7 @@
  *   BACK_SIZE BACK_FILTERSIZE BACK_FILTTHRESH BACK_TYPE BACK_VALUE
  *   CHECKIMAGE_TYPE (NONE, SEGMENTATION, BACKGROUND, BACKGROUND_RMS, -BACKGROUND, FILTERED)
  *   CHECKIMAGE_NAME VERBOSE_TYPE
- *   WEIGHT_TYPE (NONE, MAP_VAR, MAP_RMS, MAP_WEIGHT) WEIGHT_IMAGE
+ *   WEIGHT_TYPE (NONE, MAP_VAR, MAP_RMS, MAP_WEIGHT, BACKGROUND) WEIGHT_IMAGE
  *   STARNNW_NAME SEEING_FWHM PIXEL_SCALE (CLASS_STAR)
  * Multi-extension files: every image extension is a frame of one batched
  * extraction; catalogue rows carry EXT_NUMBER.
@@ -103,6 +103,7 @@ static void setpref(prefs_t *p, const char *key, char *val)
         c->weight_type = !strncasecmp(val, "MAP_VAR", 7)      ? 1
                          : !strncasecmp(val, "MAP_RMS", 7)    ? 2
                          : !strncasecmp(val, "MAP_WEIGHT", 10) ? 3
+                         : !strncasecmp(val, "BACKGROUND", 10) ? 4
                                                                : 0;
     else if (!strcasecmp(key, "WEIGHT_IMAGE")) snprintf(p->weight_image, sizeof p->weight_image, "%s", val);
     else if (!strcasecmp(key, "SEEING_FWHM")) c->seeing_fwhm = atof(val);
@@ -804,7 +805,7 @@ int main(int argc, char **argv)
     fmt = ims[0].fmt;
     w = ims[0].w;
     h = ims[0].h;
-    if (p.cfg.weight_type && nim == 1) {
+    if (p.cfg.weight_type >= 1 && p.cfg.weight_type <= 3 && nim == 1) {
         int ww, wh;
         if (!*p.weight_image) die("WEIGHT_IMAGE missing", NULL);
         wmap = read_fits(p.weight_image, &ww, &wh);

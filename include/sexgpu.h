@@ -68,7 +68,8 @@ typedef struct {
     double  phot_aperture;      /* PHOT_APERTURES (one diameter) */
     double  phot_autoparams[2]; /* PHOT_AUTOPARAMS */
     int     mask_type;          /* MASK_TYPE: 0 NONE, 1 BLANK, 2 CORRECT */
-    int     weight_type;        /* WEIGHT_TYPE: 0 NONE, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT */
+    int     weight_type;        /* WEIGHT_TYPE: 0 NONE, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT,
+                                   4 BACKGROUND (variance from the background rms map, no map given) */
     int     numbering;          /* 0 completion order, 1 first-pixel order */
     double  seeing_fwhm;        /* SEEING_FWHM (arcsec): CLASS_STAR input */
     double  pixel_scale;        /* PIXEL_SCALE (arcsec/pixel); <= 0 means 1 (no WCS here) */

@@ -73,7 +73,7 @@ typedef struct {
     double  phot_autoparams[2]; /* PHOT_AUTOPARAMS */
     int     mask_type;          /* 0 NONE, 1 BLANK, 2 CORRECT */
     /* weighting */
-    int     weight_type;        /* 0 NONE, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT */
+    int     weight_type;        /* 0 NONE, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT, 4 BACKGROUND */
     /* catalog order: 0 completion order, 1 first-pixel order */
     int     numbering;
     /* star/galaxy classification (src/preflist.h:132, SEEING_FWHM; PIXEL_SCALE) */

@@ -1184,7 +1184,13 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
         float *sig = (float *)malloc(sizeof(float) * nbx * nby);
         back = (float *)malloc(sizeof(float) * nbx * nby);
         orc_background(sub, w, h, cfg, back, sig, NULL, NULL, &S);
-        if (var) {
+        if (cfg->weight_type == 4) {
+            /* WEIGHT_TYPE BACKGROUND: variance = (background rms map)^2 */
+            wvar = (float *)malloc(sizeof(float) * N);
+            orc_background_rms(img, w, h, cfg, wvar);
+            for (p = 0; p < N; p++)
+                wvar[p] = wvar[p] * wvar[p];
+        } else if (var) {
             float sigfac2;
             S.sigfac = weight_sigfac(var, cfg->weight_type, w, h, bw, bh, nbx, nby, sig);
             sigfac2 = S.sigfac * S.sigfac;

@@ -173,13 +173,14 @@ def test_full_size_c1(gpu_ctx, masks):
     assert len(g) > 50000
 
 
-@pytest.mark.parametrize("wtype", [1, 2, 3])
+@pytest.mark.parametrize("wtype", [1, 2, 3, 4])
 def test_weight_maps(gpu_ctx, masks, wtype):
     """WEIGHT_TYPE MAP_VAR / MAP_RMS / MAP_WEIGHT: variance 1.0 +- 20% (x64),
     2% of the pixels unusable in 8x8 blocks; per-pixel thresholds against the
     local rms, per-object thresholds, variance-weighted errors."""
     img, vm = synth.frame_c1(seed=4001, w=768, h=640, density=9e-3, var=True)
-    wmap = {1: vm, 2: np.sqrt(vm), 3: np.where(vm < 1e29, 1.0 / vm, 0.0).astype(np.float32)}[wtype]
+    # 4: WEIGHT_TYPE BACKGROUND, the variance is the background rms map squared (no map given)
+    wmap = {1: vm, 2: np.sqrt(vm), 3: np.where(vm < 1e29, 1.0 / vm, 0.0).astype(np.float32), 4: None}[wtype]
     kw = dict(conv=masks["gauss_4.0_7x7"], back_size=128, weight_type=wtype)
     g, gseg, gs = gpu_ctx.extract(img, weight=wmap, **kw)
     o, oseg, os_ = O.extract(img, weight=wmap, **kw)
