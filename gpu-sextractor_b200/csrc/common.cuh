@@ -352,6 +352,7 @@ struct FrameParams {
     int wtype;                      // weight map: 0 none, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT
     int wthr;                       // thresholds follow the local rms (weight map, relative thresholds)
     double seeing, pixscale;        // SEEING_FWHM, PIXEL_SCALE (CLASS_STAR)
+    int bp_local, bp_thick;         // BACKPHOTO_TYPE LOCAL, BACKPHOTO_THICK
 };
 
 // scalars computed on the device during one extraction

@@ -104,6 +104,7 @@ struct AnaArgs {
     const float *wvar;  // calibrated variance map, or null
     int wthr;           // analysis threshold follows the local rms
     double afac;        // ANALYSIS_THRESH
+    int bp_thick;       // BACKPHOTO_THICK (used when O.dbkg is set)
 };
 
 // Robust preanalysis of a deblended object over its final pixels
@@ -294,9 +295,13 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
         unsigned kbits = warp_select(pix, n, A.cd, n - A.minarea, hist[wid]);
         mthresh = __uint_as_float(kbits) - dthresh;
     }
+    // LOCAL photometry background (src/back.c:568 localback): the annulus mode,
+    // subtracted from the flux, threshold, peak and FWHM fit (analyse.c
+    // examineiso; the reference's GPU path keeps GLOBAL, dbkg = 0)
+    const float dbkg = A.O.dbkg ? A.O.dbkg[o] : 0.0f;
     // isophotal thresholds: lane k < 8 evaluates threshold k, every lane reads all
-    float othresh = thresh - 0.0f;
-    float opeak = peak - 0.0f;
+    float othresh = thresh - dbkg;
+    float opeak = peak - dbkg;
     float tk = 0.0f;
     if (opeak > 0.0 && othresh > 0.0 && lane < SX_NISO_)
         tk = othresh * pow((double)opeak / othresh, (double)lane / SX_NISO_);
@@ -309,7 +314,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
     float thresh0 = opeak / 5.0;
     if (thresh0 < othresh) thresh0 = othresh;
     double s = 0, sx = 0, sy = 0, sxx = 0, sxy = 0;
-    double sat = (double)(A.satur - 0.0);
+    double sat = (double)(A.satur - (double)dbkg);
     for (int i = lane; i < n; i += 32) {
         unsigned p = __ldg(pix + i);
         float v = __ldg(A.sub + p);
@@ -319,7 +324,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
             go = go && v > threshs[k];
             iso[k] += go;
         }
-        double pv = v - 0.0;
+        double pv = v - (double)dbkg;
         if (thresh0 > 0.0 && pv > thresh0 && pv < sat) {
             int iy = (int)fdiv(p, A.wdiv), ix = (int)p - iy * w;
             double dx = ix - mxo, dy = iy - myo;
@@ -357,6 +362,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
         }
     }
     double tvd = xs_double(stv);
+    if (A.O.dbkg) tvd -= (double)((float)n * dbkg);   // int * float: a float product
     double sigtv = A.wvar ? xs_double(svar) : (double)n * var;
     if (A.gain > 0.0 && tvd > 0.0) sigtv += tvd / A.gain;
     float fwhm = 0.0f;
@@ -370,7 +376,8 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
         }
     }
     int py = (int)fdiv((unsigned)peakpix, A.wdiv);
-    A.O.bkg[o] = bkg;
+    // the mode is added only where it was measured (src/back.c:659)
+    A.O.bkg[o] = A.O.dbkg && A.O.lstat[o].nlevels >= 0 ? bkg + dbkg : bkg;
     A.O.peak[o] = opeak;
     A.O.peakx[o] = peakpix - py * w + 1;
     A.O.peaky[o] = py + 1;
@@ -392,6 +399,13 @@ void launch_analyse(const AnaArgs &A, cudaStream_t st) {
     if (A.nobj <= 0) return;
     const unsigned grid = (A.nobj + AN_WARPS - 1) / AN_WARPS;
     k_analyse_robust<<<grid, AN_WARPS * 32, 0, st>>>(A);
+    if (A.O.dbkg) {
+        k_local_stat<<<(unsigned)((A.nobj + 127) / 128), 128, 0, st>>>(A.sub, A.w, A.h, A.bp_thick, A.O.xmin,
+                                                                         A.O.xmax, A.O.ymin, A.O.ymax, A.nobj,
+                                                                         A.O.lstat);
+        k_local_guess<<<(unsigned)A.nobj, GUESS_THREADS, 0, st>>>(A.sub, A.w, A.h, A.bp_thick, A.O.xmin, A.O.xmax,
+                                                                   A.O.ymin, A.O.ymax, A.O.lstat, A.O.dbkg);
+    }
     k_examineiso<<<grid, AN_WARPS * 32, 0, st>>>(A);
 }
 

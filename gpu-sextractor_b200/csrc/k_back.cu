@@ -237,40 +237,14 @@ __global__ void __launch_bounds__(32) k_mesh_stat_band(const float *__restrict__
 constexpr int GUESS_THREADS = 256;
 
 // src/back.c:297-339 (backhisto) + :347-432 (backguess), one CTA per mesh
-__global__ void __launch_bounds__(GUESS_THREADS) k_mesh_guess(const float *__restrict__ img, int w, int h, int bw,
-                                                                int bh, int nbx, int nby,
-                                                                const MeshStat *__restrict__ ms,
-                                                                float *__restrict__ back, float *__restrict__ sig) {
-    __shared__ int hist[SX_QUANTIF_NMAXLEVELS + 2];
-    __shared__ int pfx[SX_QUANTIF_NMAXLEVELS + 2];   // pfx[i] = sum_{k<i} hist[k]
+// src/back.c:347-432 (backguess) on a histogram already in shared memory,
+// for the whole CTA: the prefix sums, the clipping iteration with exact
+// integer moments and the median split, the mode; thread 0 writes the mode
+// and sigma to *back_out, *sig_out.
+__device__ void guess_from_hist(int *hist, int *pfx, const MeshStat &bm, float *back_out, float *sig_out) {
     __shared__ long long red[3][GUESS_THREADS / 32];
     __shared__ int sh_lcut, sh_hcut, sh_go;
-    int m = blockIdx.x;
-    int mx = m % nbx, my = m / nbx;
-    MeshStat bm = ms[m];
-    if (bm.mean <= -SX_BIG) {
-        if (threadIdx.x == 0) back[m] = sig[m] = -SX_BIG;
-        return;
-    }
-    int x0 = mx * bw, y0 = my * bh;
-    int mw = (mx == nbx - 1 && w % bw) ? w % bw : bw;
-    int mh = (my == nby - 1 && h % bh) ? h % bh : bh;
-    for (int i = threadIdx.x; i < SX_QUANTIF_NMAXLEVELS + 2; i += GUESS_THREADS) hist[i] = 0;
-    __syncthreads();
-    int nlevels = bm.nlevels;
-    float qscale = bm.qscale;
-    float cste = 0.499999 - bm.qzero / qscale;
-    // one warp per mesh row, lanes along the row (no index division)
-    for (int r = threadIdx.x >> 5; r < mh; r += GUESS_THREADS / 32) {
-        const float *row = img + (size_t)(y0 + r) * w + x0;
-        for (int x = threadIdx.x & 31; x < mw; x += 32) {
-            float b = __ldg(row + x) / qscale + cste;
-            if (b != b) continue;  // NaN: the host conversion yields INT_MIN
-            int bin = (int)b;
-            if (bin >= 0 && bin < nlevels) atomicAdd(&hist[bin], 1);
-        }
-    }
-    __syncthreads();
+    const int nlevels = bm.nlevels;
     // exclusive prefix of the histogram: 17 consecutive bins per thread
     {
         constexpr int PER = (SX_QUANTIF_NMAXLEVELS + 2 + GUESS_THREADS - 1) / GUESS_THREADS;
@@ -366,9 +340,188 @@ __global__ void __launch_bounds__(GUESS_THREADS) k_mesh_guess(const float *__res
                 mean = bm.qzero + med * bm.qscale;
         } else
             mean = bm.qzero + mea * bm.qscale;
-        back[m] = mean;
-        sig[m] = sig_ * bm.qscale;
+        *back_out = mean;
+        *sig_out = sig_ * bm.qscale;
     }
+}
+
+__global__ void __launch_bounds__(GUESS_THREADS) k_mesh_guess(const float *__restrict__ img, int w, int h, int bw,
+                                                                int bh, int nbx, int nby,
+                                                                const MeshStat *__restrict__ ms,
+                                                                float *__restrict__ back, float *__restrict__ sig) {
+    __shared__ int hist[SX_QUANTIF_NMAXLEVELS + 2];
+    __shared__ int pfx[SX_QUANTIF_NMAXLEVELS + 2];   // pfx[i] = sum_{k<i} hist[k]
+    int m = blockIdx.x;
+    int mx = m % nbx, my = m / nbx;
+    MeshStat bm = ms[m];
+    if (bm.mean <= -SX_BIG) {
+        if (threadIdx.x == 0) back[m] = sig[m] = -SX_BIG;
+        return;
+    }
+    int x0 = mx * bw, y0 = my * bh;
+    int mw = (mx == nbx - 1 && w % bw) ? w % bw : bw;
+    int mh = (my == nby - 1 && h % bh) ? h % bh : bh;
+    for (int i = threadIdx.x; i < SX_QUANTIF_NMAXLEVELS + 2; i += GUESS_THREADS) hist[i] = 0;
+    __syncthreads();
+    int nlevels = bm.nlevels;
+    float qscale = bm.qscale;
+    float cste = 0.499999 - bm.qzero / qscale;
+    // one warp per mesh row, lanes along the row (no index division)
+    for (int r = threadIdx.x >> 5; r < mh; r += GUESS_THREADS / 32) {
+        const float *row = img + (size_t)(y0 + r) * w + x0;
+        for (int x = threadIdx.x & 31; x < mw; x += 32) {
+            float b = __ldg(row + x) / qscale + cste;
+            if (b != b) continue;  // NaN: the host conversion yields INT_MIN
+            int bin = (int)b;
+            if (bin >= 0 && bin < nlevels) atomicAdd(&hist[bin], 1);
+        }
+    }
+    __syncthreads();
+    guess_from_hist(hist, pfx, bm, back + m, sig + m);
+}
+
+// ---------------------------------------------------------------------------
+// BACKPHOTO_TYPE LOCAL, src/back.c:568-660 (localback): the mode of the
+// background-subtracted pixels in a rectangular annulus, BACKPHOTO_THICK
+// wide, around the object's box widened by a quarter of its size.  The
+// reference collects the annulus pixels (per row the left and right strips,
+// then the rows above the box, then the rows below) and runs backstat (two
+// sequential double passes in that order), the histogram and backguess.
+// ---------------------------------------------------------------------------
+struct LocalBox {
+    int ok, ixmin, ixmax, iymin, iymax, bxmin, bxmax, bymin, bymax;
+};
+
+__device__ __forceinline__ LocalBox local_box(int xmin, int xmax, int ymin, int ymax, int w, int h, int pbs) {
+    LocalBox B;
+    const int oxsize = xmax - xmin + 1, oysize = ymax - ymin + 1;
+    const int bxnml = oxsize < w / 2 ? oxsize / 4 : (w - oxsize) / 4;
+    const int bynml = oysize < h / 2 ? oysize / 4 : (h - oysize) / 4;
+    B.ixmin = xmin - bxnml;
+    B.ixmax = xmax + 1 + bxnml;
+    B.iymin = ymin - bynml;
+    B.iymax = ymax + 1 + bynml;
+    B.bxmin = B.ixmin - pbs;
+    B.bxmax = B.ixmax + pbs;
+    B.bymin = B.iymin - pbs;
+    B.bymax = B.iymax + pbs;
+    B.ok = B.bymin >= 0 && B.bymax < h && B.bxmin >= 0 && B.bxmax < w;
+    return B;
+}
+
+// the annulus pixels in the reference's collection order
+template <class F>
+__device__ __forceinline__ void local_visit(const float *__restrict__ sub, int w, const LocalBox &B, int pbs, F f) {
+    for (int y = B.bymin; y < B.bymax; y++) {
+        const float *row = sub + (size_t)y * w;
+        for (int x = B.bxmin; x < B.bxmin + pbs; x++) f(row[x]);
+        for (int x = B.ixmax; x < B.ixmax + pbs; x++) f(row[x]);
+    }
+    for (int y = B.bymin; y < B.iymin; y++)
+        for (int x = B.ixmin; x < B.ixmax; x++) f(sub[(size_t)y * w + x]);
+    for (int y = B.iymax; y < B.bymax; y++)
+        for (int x = B.ixmin; x < B.ixmax; x++) f(sub[(size_t)y * w + x]);
+}
+
+// one thread per object: backstat over the valid annulus pixels (one mesh of
+// one column); nlevels = -1 marks "no local background" (annulus outside the
+// frame, or no valid pixel)
+__global__ void k_local_stat(const float *__restrict__ sub, int w, int h, int pbs, const int *__restrict__ xmin,
+                             const int *__restrict__ xmax, const int *__restrict__ ymin,
+                             const int *__restrict__ ymax, int n, MeshStat *__restrict__ ls) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    MeshStat s;
+    s.mean = s.sigma = s.lcut = s.hcut = s.qzero = s.qscale = 0.f;
+    s.nlevels = -1;
+    s.npix = 0;
+    const LocalBox B = local_box(xmin[o], xmax[o], ymin[o], ymax[o], w, h, pbs);
+    if (!B.ok) {
+        ls[o] = s;
+        return;
+    }
+    const double step = sqrt(2 / SX_PI) * SX_QUANTIF_NSIGMA / SX_QUANTIF_AMIN;
+    double mean = 0.0, sigma = 0.0, sig;
+    int npix = 0;
+    // a pixel left out adds +0.0 (the sums are never -0.0), see mesh_stat_seq
+    local_visit(sub, w, B, pbs, [&](float p) {
+        const double pix = p;
+        const bool in = pix > -SX_BIG;
+        mean += in ? pix : 0.0;
+        sigma += in ? pix * pix : 0.0;
+        npix += in;
+    });
+    if (!npix) {
+        ls[o] = s;
+        return;
+    }
+    mean /= (double)npix;
+    sigma = (sig = sigma / npix - mean * mean) > 0.0 ? sqrt(sig) : 0.0;
+    const float lcut = s.lcut = (float)(mean - 2.0 * sigma);
+    const float hcut = s.hcut = (float)(mean + 2.0 * sigma);
+    mean = sigma = 0.0;
+    int npix2 = 0;
+    local_visit(sub, w, B, pbs, [&](float p) {
+        const double pix = p;
+        const bool in = pix > -SX_BIG && pix <= hcut && pix >= lcut;
+        mean += in ? pix : 0.0;
+        sigma += in ? pix * pix : 0.0;
+        npix2 += in;
+    });
+    s.npix = npix2;
+    mean /= (double)npix2;
+    sig = sigma / npix2 - mean * mean;
+    sigma = sig > 0.0 ? sqrt(sig) : 0.0;
+    s.mean = mean;
+    s.sigma = sigma;
+    if ((s.nlevels = (int)(step * npix2 + 1)) > SX_QUANTIF_NMAXLEVELS) s.nlevels = SX_QUANTIF_NMAXLEVELS;
+    s.qscale = sigma > 0.0 ? 2 * SX_QUANTIF_NSIGMA * sigma / s.nlevels : 1.0;
+    s.qzero = mean - SX_QUANTIF_NSIGMA * sigma;
+    ls[o] = s;
+}
+
+// one CTA per object: the annulus histogram (integer counts, any order) and
+// backguess; dbkg = its mode, 0 without a local background
+__global__ void __launch_bounds__(GUESS_THREADS) k_local_guess(const float *__restrict__ sub, int w, int h, int pbs,
+                                                                 const int *__restrict__ xmin,
+                                                                 const int *__restrict__ xmax,
+                                                                 const int *__restrict__ ymin,
+                                                                 const int *__restrict__ ymax,
+                                                                 const MeshStat *__restrict__ ls, float *dbkg) {
+    __shared__ int hist[SX_QUANTIF_NMAXLEVELS + 2];
+    __shared__ int pfx[SX_QUANTIF_NMAXLEVELS + 2];
+    const int o = blockIdx.x;
+    const MeshStat bm = ls[o];
+    if (bm.nlevels < 0) {
+        if (threadIdx.x == 0) dbkg[o] = 0.0f;
+        return;
+    }
+    const LocalBox B = local_box(xmin[o], xmax[o], ymin[o], ymax[o], w, h, pbs);
+    for (int i = threadIdx.x; i < SX_QUANTIF_NMAXLEVELS + 2; i += GUESS_THREADS) hist[i] = 0;
+    __syncthreads();
+    const int nlevels = bm.nlevels;
+    const float qscale = bm.qscale, cste = 0.499999 - bm.qzero / qscale;
+    auto bin_of = [&](float p) {
+        if (!(p > -SX_BIG)) return;
+        const float b = p / qscale + cste;
+        if (b != b) return;
+        const int bin = (int)b;
+        if (bin >= 0 && bin < nlevels) atomicAdd(&hist[bin], 1);
+    };
+    const int sw = 2 * pbs, rows = B.bymax - B.bymin, iw = B.ixmax - B.ixmin;
+    for (int i = threadIdx.x; i < rows * sw; i += GUESS_THREADS) {
+        const int r = i / sw, c = i - r * sw;
+        bin_of(sub[(size_t)(B.bymin + r) * w + (c < pbs ? B.bxmin + c : B.ixmax + c - pbs)]);
+    }
+    const int nt = B.iymin - B.bymin, nb2 = B.bymax - B.iymax;
+    for (int i = threadIdx.x; i < (nt + nb2) * iw; i += GUESS_THREADS) {
+        const int r = i / iw, c = i - r * iw;
+        const int y = r < nt ? B.bymin + r : B.iymax + (r - nt);
+        bin_of(sub[(size_t)y * w + B.ixmin + c]);
+    }
+    __syncthreads();
+    float sg;
+    guess_from_hist(hist, pfx, bm, dbkg + o, &sg);
 }
 
 // src/back.c:455-480: bad meshes take the mean of the nearest valid meshes.

@@ -270,7 +270,7 @@ __device__ void aper_warp(const EndArgs &A, int o, double mx, double my, int &fl
         }
     }
     if (lane != 0) return;
-    tv -= area * 0.0;
+    if (A.O.dbkg) tv -= area * (double)A.O.dbkg[o];
     if (A.gain > 0.0 && tv > 0.0) sigtv += tv / A.gain;
     A.O.flux_aper[o] = tv;
     A.O.fluxerr_aper[o] = sqrt(sigtv);
@@ -496,7 +496,7 @@ __device__ void end_finish(const EndArgs &A, int o, int flags, float kron, bool 
         if ((float)areab > SX_CROWD_THRESHOLD * area) flags |= SX_OBJ_CROWDED;
         tv = xs_double(p2.s0);
         sigtv = A.wvar ? xs_double(p2.s1) : (double)area * var;
-        tv -= area * (double)0.0f;
+        if (A.O.dbkg) tv -= area * (double)A.O.dbkg[o];
         if (A.gain > 0.0 && tv > 0.0) sigtv += tv / A.gain;
         if (p2.s0.ovf | p2.s1.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
     } else
@@ -738,7 +738,7 @@ __global__ void k_write_rows(ObjBufs O, const unsigned *vals, int ns, float dthr
     q.poserr_my2 = O.pmy2[o];
     q.poserr_mxy = O.pmxy[o];
     q.bkg = O.bkg[o];
-    q.thresh = O.athr[o];
+    q.thresh = O.dbkg ? O.athr[o] - O.dbkg[o] : O.athr[o];
     q.dthresh = O.dthr[o];
     q.mthresh = O.mthresh[o];
     q.fwhm = O.fwhm[o];

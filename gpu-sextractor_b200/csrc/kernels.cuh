@@ -89,6 +89,8 @@ struct ObjBufs {
     int *fdnpix;
     float *dthr, *athr;                 // the raw object's detection / analysis thresholds
     float *sprob;                       // CLASS_STAR
+    float *dbkg;                        // LOCAL photometry background per object, or null (GLOBAL)
+    MeshStat *lstat;                    // LOCAL annulus statistics
     unsigned long long *sortkey;
 };
 

@@ -92,6 +92,8 @@ struct sexgpu_ctx {
         skeys, svals, skalt, svalt, rows;
     DevBuf kitem[2], kchunk[2], kpart[2];  // queued Kron boxes
     DevBuf o_sprob;                        // CLASS_STAR per object
+    DevBuf o_dbkg, o_lstat;                // BACKPHOTO_TYPE LOCAL: annulus mode, annulus statistics
+    bool cfg_local = false;                // the current extraction uses LOCAL photometry background
     DevBuf fitsraw;                        // FITS data block as stored (sexgpu_extract_fits)
     DevBuf rmsd, rmsnode, rmsdnode, rmsu, rmsmap;  // background rms map (sexgpu_background_rms)
     DevBuf dnnw;                           // this context's copy of the CLASS_STAR network
@@ -223,6 +225,8 @@ int check_config(const sexgpu_config *cfg, int w, int h) {
     if (cfg->detect_minarea < 1 || cfg->deblend_nthresh < 1 || cfg->deblend_nthresh > 64) return SEXGPU_ERR_ARG;
     if (cfg->weight_type < 0 || cfg->weight_type > 4) return SEXGPU_ERR_ARG;
     if (!(cfg->seeing_fwhm > 0.0)) return SEXGPU_ERR_ARG;
+    if (cfg->back_photo_type < 0 || cfg->back_photo_type > 1) return SEXGPU_ERR_ARG;
+    if (cfg->back_photo_type == 1 && (cfg->back_photo_thick < 1 || cfg->back_photo_thick > 256)) return SEXGPU_ERR_ARG;
     return SEXGPU_OK;
 }
 
@@ -263,6 +267,8 @@ void make_params(const sexgpu_config *cfg, int w, int h, FrameParams &P) {
     P.wthr = cfg->weight_type != 0 && cfg->thresh_type != 1;
     P.seeing = cfg->seeing_fwhm;
     P.pixscale = cfg->pixel_scale > 0.0 ? cfg->pixel_scale : 1.0;
+    P.bp_local = cfg->back_photo_type == 1;
+    P.bp_thick = cfg->back_photo_thick;
 }
 
 __global__ void k_init_scalars(FrameScalars *sc) {
@@ -392,6 +398,10 @@ int alloc_objects(sexgpu_ctx *ctx, int nobj) {
     O.magerr_iso = P<float>(ctx->o_d[8]);
     EN(o_sprob, n * sizeof(float));
     O.sprob = ctx->nnw_dev ? P<float>(ctx->o_sprob) : nullptr;
+    EN(o_dbkg, n * sizeof(float));
+    EN(o_lstat, n * sizeof(MeshStat));
+    O.dbkg = ctx->cfg_local ? P<float>(ctx->o_dbkg) : nullptr;
+    O.lstat = P<MeshStat>(ctx->o_lstat);
     O.fluxerr_iso = P<float>(ctx->o_d[9]);
     return SEXGPU_OK;
 }
@@ -704,6 +714,7 @@ int pipe_deblend(sexgpu_ctx *ctx) {
     rc = read_scalars(ctx);
     if (rc) return rc;
     const int nobj = ps.nobj = ctx->hsc.nobj;
+    ctx->cfg_local = Pm.bp_local != 0;
     rc = alloc_objects(ctx, nobj);
     if (rc) return rc;
     A.O = ctx->O;
@@ -753,6 +764,7 @@ int pipe_analyse(sexgpu_ctx *ctx) {
     AA.wvar = ps.wvar;
     AA.wthr = Pm.wthr;
     AA.afac = Pm.analysis_thresh;
+    AA.bp_thick = Pm.bp_thick;
     launch_analyse(AA, st);
     stage_mark(ctx, "analyse", 2 + radix_launches(bits_for(nobj), nrootpix) + scan_launches(nobj));
     ps.stage = 4;
@@ -993,6 +1005,8 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
         free_buf(ctx->kpart[i]);
     }
     free_buf(ctx->o_sprob);
+    free_buf(ctx->o_dbkg);
+    free_buf(ctx->o_lstat);
     free_buf(ctx->fitsraw);
     free_buf(ctx->rmsd);
     free_buf(ctx->rmsnode);
@@ -1058,6 +1072,8 @@ void sexgpu_default_config(sexgpu_config *c) {
     c->numbering = 0;
     c->seeing_fwhm = 1.2;
     c->pixel_scale = 0.0;
+    c->back_photo_type = 0;
+    c->back_photo_thick = 24;
 }
 
 const char *sexgpu_last_error(sexgpu_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }

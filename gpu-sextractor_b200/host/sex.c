@@ -20,6 +20,7 @@
  *   CHECKIMAGE_NAME VERBOSE_TYPE
  *   WEIGHT_TYPE (NONE, MAP_VAR, MAP_RMS, MAP_WEIGHT, BACKGROUND) WEIGHT_IMAGE
  *   STARNNW_NAME SEEING_FWHM PIXEL_SCALE (CLASS_STAR)
+ *   BACKPHOTO_TYPE (GLOBAL, LOCAL) BACKPHOTO_THICK
  * Multi-extension files: every image extension is a frame of one batched
  * extraction; catalogue rows carry EXT_NUMBER.
  * Other keywords of the reference are accepted and ignored.
@@ -108,6 +109,8 @@ static void setpref(prefs_t *p, const char *key, char *val)
     else if (!strcasecmp(key, "WEIGHT_IMAGE")) snprintf(p->weight_image, sizeof p->weight_image, "%s", val);
     else if (!strcasecmp(key, "SEEING_FWHM")) c->seeing_fwhm = atof(val);
     else if (!strcasecmp(key, "PIXEL_SCALE")) c->pixel_scale = atof(val);
+    else if (!strcasecmp(key, "BACKPHOTO_TYPE")) c->back_photo_type = !strncasecmp(val, "LOCAL", 5);
+    else if (!strcasecmp(key, "BACKPHOTO_THICK")) c->back_photo_thick = atoi(val);
     else if (!strcasecmp(key, "STARNNW_NAME")) {
         snprintf(p->nnw_name, sizeof p->nnw_name, "%s", val);
         p->nnw_given = 1;

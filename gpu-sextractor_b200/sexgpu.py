@@ -41,6 +41,7 @@ class Config(C.Structure):
         ("phot_aperture", C.c_double), ("phot_autoparams", C.c_double * 2), ("mask_type", C.c_int),
         ("weight_type", C.c_int), ("numbering", C.c_int),
         ("seeing_fwhm", C.c_double), ("pixel_scale", C.c_double),
+        ("back_photo_type", C.c_int), ("back_photo_thick", C.c_int),
     ]
 
 
@@ -165,7 +166,7 @@ def default_config():
                 conv=DEFAULT_CONV, detect_minarea=5, deblend_nthresh=32, deblend_mincont=0.005,
                 clean_flag=1, clean_param=1.0, satur_level=50000.0, gain=0.0, mag_zeropoint=0.0,
                 phot_aperture=5.0, phot_autoparams=(2.5, 3.5), mask_type=2, weight_type=0,
-                numbering=0, seeing_fwhm=1.2, pixel_scale=0.0)
+                numbering=0, seeing_fwhm=1.2, pixel_scale=0.0, back_photo_type=0, back_photo_thick=24)
 
 
 def make_config(**kw):

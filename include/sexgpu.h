@@ -73,6 +73,8 @@ typedef struct {
     int     numbering;          /* 0 completion order, 1 first-pixel order */
     double  seeing_fwhm;        /* SEEING_FWHM (arcsec): CLASS_STAR input */
     double  pixel_scale;        /* PIXEL_SCALE (arcsec/pixel); <= 0 means 1 (no WCS here) */
+    int     back_photo_type;    /* BACKPHOTO_TYPE: 0 GLOBAL, 1 LOCAL (annulus mode per object) */
+    int     back_photo_thick;   /* BACKPHOTO_THICK: LOCAL annulus thickness, 1..256 pixels */
 } sexgpu_config;
 
 /* One catalogue row (0-based pixel coordinates unless stated). */

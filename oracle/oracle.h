@@ -80,6 +80,9 @@ typedef struct {
     double  seeing_fwhm;
     double  pixel_scale;        /* <= 0: 1 */
     const struct orc_nnw *nnw;  /* network, or NULL: CLASS_STAR 0 */
+    /* photometry background (src/preflist.h BACKPHOTO_TYPE, BACKPHOTO_THICK) */
+    int     back_photo_type;    /* 0 GLOBAL, 1 LOCAL */
+    int     back_photo_thick;   /* annulus thickness (pixels) */
 } orc_config;
 
 /* Star/galaxy network (src/types.h:930 brainstruct; src/neurro.c) */
@@ -156,6 +159,9 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
 int orc_getconv(const char *path, float *mask, int maxn, int *mw, int *mh);
 /* background rms map (w*h), src/back.c:938 backrmsline */
 int orc_background_rms(const float *img, int w, int h, const orc_config *cfg, float *rms);
+/* src/back.c:568 localback for objects given by their boxes (4 ints each:
+   xmin, xmax, ymin, ymax) over a background-subtracted frame: dbkg per object */
+void orc_localback(const float *sub, int w, int h, int thick, const int *box, int nobj, float *dbkg);
 
 /* Small helpers exposed for unit tests. */
 float   orc_hmedian(float *ra, int n);

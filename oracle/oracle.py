@@ -27,6 +27,7 @@ class OrcConfig(C.Structure):
         ("phot_aperture", C.c_double), ("phot_autoparams", C.c_double * 2), ("mask_type", C.c_int),
         ("weight_type", C.c_int), ("numbering", C.c_int),
         ("seeing_fwhm", C.c_double), ("pixel_scale", C.c_double), ("nnw", C.c_void_p),
+        ("back_photo_type", C.c_int), ("back_photo_thick", C.c_int),
     ]
 
 
@@ -156,7 +157,7 @@ def default_config():
                 conv=DEFAULT_CONV, detect_minarea=5, deblend_nthresh=32, deblend_mincont=0.005,
                 clean_flag=1, clean_param=1.0, satur_level=50000.0, gain=0.0, mag_zeropoint=0.0,
                 phot_aperture=5.0, phot_autoparams=(2.5, 3.5), mask_type=2, weight_type=0,
-                numbering=0, seeing_fwhm=1.2, pixel_scale=0.0)
+                numbering=0, seeing_fwhm=1.2, pixel_scale=0.0, back_photo_type=0, back_photo_thick=24)
 
 
 def background(img, **kw):
@@ -181,6 +182,16 @@ def background_rms(img, **kw):
     h, w = img.shape
     lib().orc_background_rms(_f(img), w, h, C.byref(cfg), _f(rms))
     return rms
+
+
+def localback(sub, boxes, thick=24):
+    """LOCAL photometry background (localback) per object box (xmin, xmax, ymin, ymax)."""
+    sub = np.ascontiguousarray(sub, np.float32)
+    boxes = np.ascontiguousarray(boxes, np.int32).reshape(-1, 4)
+    out = np.zeros(len(boxes), np.float32)
+    h, w = sub.shape
+    lib().orc_localback(_f(sub), w, h, thick, boxes.ctypes.data_as(C.POINTER(C.c_int)), len(boxes), _f(out))
+    return out
 
 
 def filter_image(sub, mask):
@@ -255,6 +266,19 @@ def ref_background_rms(img, back_size=64, back_filtersize=3, back_filtthresh=0.0
     h, w = img.shape
     r.ref_background_rms(_f(img), w, h, back_size, back_filtersize, C.c_double(back_filtthresh), _f(rms))
     return rms
+
+
+def ref_localback(sub, boxes, thick=24):
+    """The reference's own localback() per object box (None if not built)."""
+    r = ref()
+    if r is None:
+        return None
+    sub = np.ascontiguousarray(sub, np.float32)
+    boxes = np.ascontiguousarray(boxes, np.int32).reshape(-1, 4)
+    out = np.zeros(len(boxes), np.float32)
+    h, w = sub.shape
+    r.ref_localback(_f(sub), w, h, thick, boxes.ctypes.data_as(C.POINTER(C.c_int)), len(boxes), _f(out))
+    return out
 
 
 def ref_getconv(path):

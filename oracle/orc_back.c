@@ -482,6 +482,20 @@ float orc_back_at(const float *b, int nx, int ny, int backw, int backh, int x, i
     return (float)((1 - dy) * (cdx * b0 + dx * b1) + dy * (dx * b2 + cdx * b3));
 }
 
+/* src/back.c:568-660 (localback), its statistics: the collected annulus
+   pixels as one mesh of one column (backstat), their histogram and the mode
+   (backguess) */
+void orc_local_stats(const float *buf, int n, float *bkg, float *sig)
+{
+    mesh_t bm;
+    int64_t *histo = (int64_t *)calloc(ORC_QUANTIF_NMAXLEVELS + 1, sizeof(int64_t));
+    memset(&bm, 0, sizeof(bm));
+    mesh_stat(buf, 1, 0, 0, 1, n, &bm);
+    mesh_histo(buf, 1, 0, 0, 1, n, &bm, histo);
+    mesh_guess(&bm, histo, bkg, sig);
+    free(histo);
+}
+
 /* The background rms map (src/back.c:938 backrmsline): the filtered sigma
    mesh map through the same y and x splines as the background. */
 int orc_background_rms(const float *img, int w, int h, const orc_config *cfg, float *rms)

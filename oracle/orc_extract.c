@@ -90,6 +90,7 @@ typedef struct {
     int root, level;
     float node_dthresh;
     float dthr, athr;      /* the raw object's detection / analysis thresholds */
+    float dbkg;            /* local background (BACKPHOTO_TYPE LOCAL), else 0 */
     int nnode;             /* pixels of the branch at its own level */
     int *nodepix;
     int n;                 /* final pixels (raster order) */
@@ -512,6 +513,50 @@ static int cmp_float_desc(const void *a, const void *b)
 }
 
 /* examineiso, src/cuda/cudaanalyse.cu:2176-2581 (GLOBAL background, CCD). */
+/* src/back.c:568-660 (localback): the mode of the background-subtracted
+   pixels in a rectangular annulus around the object's box, collected in the
+   reference's order (per row the left and right strips, then the rows above,
+   then the rows below); 0 when the annulus leaves the frame or holds no
+   valid pixel.  *applied tells whether the reference adds the mode to the
+   object's background (only when it was measured). */
+static float localback(const float *sub, int w, int h, int pbs, int xmin, int xmax, int ymin, int ymax,
+                       int *applied)
+{
+    const int oxsize = xmax - xmin + 1, oysize = ymax - ymin + 1;
+    const int bxnml = oxsize < w / 2 ? oxsize / 4 : (w - oxsize) / 4;
+    const int bynml = oysize < h / 2 ? oysize / 4 : (h - oysize) / 4;
+    const int ixmin = xmin - bxnml, ixmax = xmax + 1 + bxnml, iymin = ymin - bynml, iymax = ymax + 1 + bynml;
+    const int bxmin = ixmin - pbs, bxmax = ixmax + pbs, bymin = iymin - pbs, bymax = iymax + pbs;
+    float *buf, bkg = 0.0f, sig = 0.0f, pix;
+    int n = 0, x, y;
+    *applied = 0;
+    if (!(bymin >= 0 && bymax < h && bxmin >= 0 && bxmax < w))
+        return 0.0f;
+    buf = (float *)malloc(sizeof(float) * ((size_t)(bxmax - bxmin) * (bymax - bymin)));
+    for (y = bymin; y < bymax; y++) {
+        for (x = bxmin; x < bxmin + pbs; x++)
+            if ((pix = sub[(size_t)y * w + x]) > -ORC_BIGF)
+                buf[n++] = pix;
+        for (x = ixmax; x < ixmax + pbs; x++)
+            if ((pix = sub[(size_t)y * w + x]) > -ORC_BIGF)
+                buf[n++] = pix;
+    }
+    for (y = bymin; y < iymin; y++)
+        for (x = ixmin; x < ixmax; x++)
+            if ((pix = sub[(size_t)y * w + x]) > -ORC_BIGF)
+                buf[n++] = pix;
+    for (y = iymax; y < bymax; y++)
+        for (x = ixmin; x < ixmax; x++)
+            if ((pix = sub[(size_t)y * w + x]) > -ORC_BIGF)
+                buf[n++] = pix;
+    if (n) {
+        orc_local_stats(buf, n, &bkg, &sig);
+        *applied = 1;
+    }
+    free(buf);
+    return bkg;
+}
+
 static void examineiso(const frame_t *F, obj_t *o)
 {
     const orc_config *cfg = F->cfg;
@@ -523,6 +568,13 @@ static void examineiso(const frame_t *F, obj_t *o)
     xsum_t stv, svar;
 
     o->bkg = orc_back_at(F->back, F->nbx, F->nby, F->bw, F->bh, (int)(o->mx + 0.5), (int)(o->my + 0.5));
+    o->dbkg = 0.0f;
+    if (cfg->back_photo_type == 1) {
+        int applied;
+        o->dbkg = localback(F->sub, F->w, F->h, cfg->back_photo_thick, o->xmin, o->xmax, o->ymin, o->ymax, &applied);
+        if (applied)
+            o->bkg += o->dbkg;
+    }
     dbacknoise2 = F->backsig * F->backsig;
     xm = o->mx;
     ym = o->my;
@@ -593,13 +645,15 @@ static void examineiso(const frame_t *F, obj_t *o)
      * weight map, the pixels' variances (an exact sum) */
     sigtv = F->var ? xs_double(&svar) : (double)o->n * var;
     tvd = xs_double(&stv);
+    if (cfg->back_photo_type == 1)
+        tvd -= o->n * o->dbkg;  /* int * float: a float product, cudaanalyse.cu:2462 */
     if (cfg->gain > 0.0 && tvd > 0.0)
         sigtv += tvd / cfg->gain;
     o->npix = area;
     o->flux = tvd;
     o->fluxerr = sigtv;
-    o->thresh = o->athr - 0.0f;
-    o->peak = peak - 0.0f;
+    o->thresh = o->athr - o->dbkg;
+    o->peak = peak - o->dbkg;
     if (o->peak > 0.0 && o->thresh > 0.0)
         for (i = 0; i < ORC_NISO; i++)
             threshs[i] = o->thresh * pow((double)o->peak / o->thresh, (double)i / ORC_NISO);
@@ -620,10 +674,10 @@ static void examineiso(const frame_t *F, obj_t *o)
             thresh0 = o->thresh;
         if (thresh0 > 0.0) {
             double mx = o->mx, my = o->my, s = 0, sx = 0, sy = 0, sxx = 0, sxy = 0, dx, dy, d2, lpix, pv, b, inverr2, sat, d, bmax;
-            sat = (double)(cfg->satur_level - 0.0);
+            sat = (double)(cfg->satur_level - (double)o->dbkg);
             for (k = 0; k < o->n; k++) {
                 int p = o->pix[k];
-                pv = F->sub[p] - 0.0;
+                pv = F->sub[p] - (double)o->dbkg;
                 if (pv > thresh0 && pv < sat) {
                     dx = p % w - mx;
                     dy = p / w - my;
@@ -858,7 +912,7 @@ static void aperflux(const frame_t *F, const int *alloc, obj_t *o, int self)
                 tv += locarea * pix;
             }
         }
-    tv -= area * 0.0;
+    tv -= area * o->dbkg;
     if (cfg->gain > 0.0 && tv > 0.0)
         sigtv += tv / cfg->gain;
     o->flux_aper = tv;
@@ -989,7 +1043,7 @@ static void autoflux(const frame_t *F, const int *alloc, obj_t *o, int self)
             o->flags |= ORC_OBJ_CROWDED;
         tv = xs_double(&stv);
         sigtv = F->var ? xs_double(&svar) : (double)area * var;
-        tv -= area * (double)0.0f;
+        tv -= area * (double)o->dbkg;
         if (cfg->gain > 0.0 && tv > 0.0)
             sigtv += tv / cfg->gain;
     } else
@@ -1147,6 +1201,15 @@ static float weight_sigfac(const float *wmap, int wtype, int w, int h, int bw, i
     f = nr ? orc_hmedian(ratio, nr) : 1.0f;
     free(ratio);
     return f;
+}
+
+/* LOCAL photometry background of objects given by their boxes (xmin, xmax,
+   ymin, ymax per object, 0-based) over a background-subtracted frame */
+void orc_localback(const float *sub, int w, int h, int thick, const int *box, int nobj, float *dbkg)
+{
+    int i, applied;
+    for (i = 0; i < nobj; i++)
+        dbkg[i] = localback(sub, w, h, thick, box[4 * i], box[4 * i + 1], box[4 * i + 2], box[4 * i + 3], &applied);
 }
 
 int orc_extract(const float *img, const float *var, int w, int h, const orc_config *cfg,

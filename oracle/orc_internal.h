@@ -8,6 +8,7 @@
 #include <stdint.h>
 
 #define ORC_BIG                 1e+30
+void orc_local_stats(const float *buf, int n, float *bkg, float *sig);
 #define ORC_BIGF                1e+30f
 #define ORC_PI                  3.1415926535898
 #define ORC_EPS                 (1e-4)

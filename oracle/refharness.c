@@ -144,6 +144,35 @@ int ref_background(float *img, int w, int h, int back_size, int back_filtersize,
     return 0;
 }
 
+/* The reference's LOCAL photometry background, localback() (src/back.c:568),
+ * for objects given by their boxes (xmin, xmax, ymin, ymax per object) over a
+ * background-subtracted frame held whole in memory (strip = frame). */
+int ref_localback(const float *sub, int w, int h, int thick, const int *box, int nobj, float *dbkg)
+{
+    picstruct field;
+    objstruct obj;
+    int i;
+    memset(&field, 0, sizeof(field));
+    memset(&prefs, 0, sizeof(prefs));
+    prefs.pback_size = thick;
+    field.width = w;
+    field.height = h;
+    field.strip = (PIXTYPE *)sub;
+    field.stripheight = h;
+    field.ymin = 0;
+    field.ymax = h;
+    for (i = 0; i < nobj; i++) {
+        memset(&obj, 0, sizeof(obj));
+        obj.xmin = box[4 * i];
+        obj.xmax = box[4 * i + 1];
+        obj.ymin = box[4 * i + 2];
+        obj.ymax = box[4 * i + 3];
+        localback(&field, &obj);
+        dbkg[i] = obj.dbkg;
+    }
+    return 0;
+}
+
 /* The background rms map of the reference: makeback(), then backrmsline()
  * (src/back.c:938) for every row.  img is not modified. */
 int ref_background_rms(const float *img, int w, int h, int back_size, int back_filtersize,

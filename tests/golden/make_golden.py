@@ -12,6 +12,9 @@ src/filter.c and src/misc.c compiled unmodified) and records:
                       src/back.c:43,790); small cases keep the full frame
   filter.npz          SHA-256 of the reference's convolve() output
                       (src/filter.c:39) for each mask on a seeded frame
+  localback.npz       the reference's localback() (src/back.c:568, LOCAL
+                      photometry background) for seeded object boxes over a
+                      seeded background-subtracted frame, three thicknesses
 
 Frames are produced by gpu-sextractor_b200/synth.py (seeded, machine-
 independent), so the GPU tests regenerate the inputs and compare.
@@ -57,6 +60,38 @@ def frame(args):
     return img
 
 
+def local_frame(seed=31, h=300, w=260):
+    """Background-subtracted frame for the localback cases: noise, blobs,
+    an unusable corner and a few NaN pixels."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sub = rng.normal(0.0, 5.0, (h, w))
+    yy, xx = np.mgrid[0:h, 0:w]
+    for _ in range(40):
+        cx, cy, s, a = rng.uniform(0, w), rng.uniform(0, h), rng.uniform(1.0, 6.0), rng.uniform(20, 500)
+        sub += a * np.exp(-((xx - cx) ** 2 + (yy - cy) ** 2) / (2 * s * s))
+    sub = sub.astype(np.float32)
+    sub[:40, 200:] = -1e30
+    sub[rng.integers(0, h, 20), rng.integers(0, w, 20)] = np.nan
+    return sub
+
+
+def local_boxes(seed=32, h=300, w=260, n=300):
+    """Object boxes (xmin, xmax, ymin, ymax): random sizes and places, plus
+    boxes wider than half the frame, at the edges and inside the unusable
+    corner (an annulus without a valid pixel)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    bw, bh = rng.integers(1, 50, n), rng.integers(1, 50, n)
+    x0, y0 = rng.integers(0, w - bw), rng.integers(0, h - bh)
+    b = np.stack([x0, x0 + bw - 1, y0, y0 + bh - 1], 1)
+    extra = np.array([[0, w - 1, 0, h - 1], [60, 200, 100, 130], [100, 110, 20, 200], [30, 40, 30, 40],
+                      [215, 245, 8, 12], [218, 242, 5, 15], [0, 3, 100, 104], [w - 4, w - 1, 100, 104],
+                      [120, 122, 0, 2], [120, 122, h - 3, h - 1], [100, 229, 100, 110]])
+    return np.ascontiguousarray(np.concatenate([b, extra]), np.int32)
+
+
+LOCAL_THICK = [24, 6, 1]
+
+
 def sha(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
@@ -91,6 +126,12 @@ def main():
         cd = O.ref_convolve(sub, np.array(m, np.float32))
         fout[name] = np.array(sha(cd))
     np.savez_compressed(os.path.join(HERE, "filter.npz"), **fout)
+
+    sub, boxes = local_frame(), local_boxes()
+    lout = {"boxes": boxes}
+    for t in LOCAL_THICK:
+        lout["dbkg_%d" % t] = O.ref_localback(sub, boxes, t)
+    np.savez_compressed(os.path.join(HERE, "localback.npz"), **lout)
     print("golden fixtures written: %d masks, %d background cases" % (len(masks), len(BACK_CASES)))
 
 

@@ -146,6 +146,7 @@ def test_bad_pixels_and_nan(gpu_ctx):
     dict(deblend_mincont=0.0), dict(deblend_mincont=1.0), dict(deblend_nthresh=64, deblend_mincont=0.0005),
     dict(clean_param=2.0), dict(gain=4.0), dict(mask_type=0), dict(back_filtersize=1),
     dict(back_filtersize=5, back_filtthresh=3.0), dict(satur_level=2000.0), dict(phot_aperture=12.0),
+    dict(back_photo_type=1), dict(back_photo_type=1, back_photo_thick=6, gain=2.0, satur_level=3000.0),
 ])
 def test_options(gpu_ctx, masks, opts):
     img = synth.frame_c0(seed=3, w=512, h=400, nsrc=700)

@@ -98,3 +98,36 @@ def test_background_rms_matches_reference(bs, fs):
     a = O.background_rms(img, back_size=bs, back_filtersize=fs)
     b = O.ref_background_rms(img, back_size=bs, back_filtersize=fs)
     assert a.tobytes() == b.tobytes()
+
+
+def _golden_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def test_localback_matches_reference_golden():
+    """LOCAL photometry background: the oracle's annulus mode against the
+    reference's localback() (src/back.c:568) for 311 boxes, three annulus
+    thicknesses, bit for bit (boxes at the edges, wider than half the frame,
+    and with no valid annulus pixel included)."""
+    m = _golden_module()
+    z = np.load(os.path.join(GOLD, "localback.npz"))
+    sub, boxes = m.local_frame(), m.local_boxes()
+    assert np.array_equal(boxes, z["boxes"])
+    for t in m.LOCAL_THICK:
+        ref = z["dbkg_%d" % t]
+        assert (ref != 0).sum() > len(ref) // 2
+        assert O.localback(sub, boxes, t).view(np.uint32).tolist() == ref.view(np.uint32).tolist(), t
+
+
+@pytest.mark.skipif(O.ref() is None, reason="oracle/_ref not built (needs the reference tree)")
+@pytest.mark.parametrize("seed,thick", [(41, 24), (42, 3), (43, 50)])
+def test_localback_matches_reference_live(seed, thick):
+    m = _golden_module()
+    sub, boxes = m.local_frame(seed=seed), m.local_boxes(seed=seed + 100, n=500)
+    a = O.localback(sub, boxes, thick)
+    b = O.ref_localback(sub, boxes, thick)
+    assert a.view(np.uint32).tolist() == b.view(np.uint32).tolist()
