@@ -86,7 +86,9 @@ __device__ __forceinline__ void clean_test(const CleanObj &p, const CleanObj &q,
 
 // every pair closer than CLEAN_ZONE*(a_i+a_j) is tested once, by the object
 // of larger a (lower index on ties), which searches 20*a around itself; one
-// warp per object, lanes over the cells of the search box
+// warp per object.  The objects are packed by cell in row-major cell order,
+// so the cells of one row of the search box hold one contiguous range of
+// objects: the lanes stride over that range (coalesced, balanced).
 __global__ void k_clean_pairs(const CleanObj *__restrict__ packed, int n, double beta,
                               const int *__restrict__ cellstart, int *master, int gx, int gy) {
     const int lane = threadIdx.x & 31;
@@ -96,10 +98,9 @@ __global__ void k_clean_pairs(const CleanObj *__restrict__ packed, int n, double
     const double rad = 20.0 * me.a * 1.001 + 2.0;
     int x0 = max((int)floor((me.mx - rad) / CL_CELL), 0), x1 = min((int)floor((me.mx + rad) / CL_CELL), gx - 1);
     int y0 = max((int)floor((me.my - rad) / CL_CELL), 0), y1 = min((int)floor((me.my + rad) / CL_CELL), gy - 1);
-    int bw = x1 - x0 + 1, nc = bw * (y1 - y0 + 1);
-    for (int c = lane; c < nc; c += 32) {
-        int cell = (y0 + c / bw) * gx + x0 + c % bw;
-        for (int t = cellstart[cell]; t < cellstart[cell + 1]; t++) {
+    for (int cy = y0; cy <= y1; cy++) {
+        const int t1 = __ldg(cellstart + cy * gx + x1 + 1);
+        for (int t = __ldg(cellstart + cy * gx + x0) + lane; t < t1; t += 32) {
             const CleanObj o = packed[t];
             if (o.idx == me.idx) continue;
             if (o.a < me.a || (o.a == me.a && o.idx > me.idx)) {

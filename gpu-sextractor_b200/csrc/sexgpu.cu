@@ -69,6 +69,9 @@ thread_local int sx_grid_div = 1;
 struct sexgpu_ctx {
     int device = 0;
     int batch_grid_div = 1;  // persistent-grid divisor of batch workers
+    int batch_sync = 1;      // batch workers wait on blocking events (1) or spin (0)
+    int sync_block = 0;      // this context waits on a blocking event instead of spinning
+    cudaEvent_t ev_block = nullptr;
     PipeState ps;
     cudaStream_t stream = nullptr;
     cudaStream_t side[2] = {nullptr, nullptr};  // fork/join helpers of the deblending
@@ -284,9 +287,22 @@ __global__ void k_alloc_init(const int *lab, int *alloc, long long n) {
     if (p < n) alloc[p] = lab[p] >= 0 ? SX_ALLOC_OTHER : -1;
 }
 
+// Waits for the work queued on st: a spinning wait (the runtime's default
+// with few host threads), or, for a batch worker told so, a blocking event
+// wait that leaves the host core to the other workers.
+cudaError_t stream_wait(sexgpu_ctx *ctx, cudaStream_t st) {
+    if (!ctx->sync_block) return cudaStreamSynchronize(st);
+    if (!ctx->ev_block) {
+        cudaError_t e = cudaEventCreateWithFlags(&ctx->ev_block, cudaEventBlockingSync | cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = cudaEventRecord(ctx->ev_block, st);
+    return e == cudaSuccess ? cudaEventSynchronize(ctx->ev_block) : e;
+}
+
 int read_scalars(sexgpu_ctx *ctx) {
     CK(cudaMemcpyAsync(&ctx->hsc, ctx->sc.p, sizeof(FrameScalars), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK(stream_wait(ctx, ctx->stream));
     if (ctx->hsc.status & SX_ST_LOOP) {
         ctx->err = "device loop iteration cap reached";
         return SEXGPU_ERR_LOOP;
@@ -1022,6 +1038,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
         if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
     }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_block) cudaEventDestroy(ctx->ev_block);
     for (sexgpu_ctx *w : ctx->workers) sexgpu_destroy(w);
     if (ctx->stage_host) cudaFreeHost(ctx->stage_host);
     if (ctx->rows_host) cudaFreeHost(ctx->rows_host);
@@ -1111,7 +1128,7 @@ int sexgpu_copy_results(sexgpu_ctx *ctx, sexgpu_object *objs, int max_objects, i
     }
     if (sub && N > 0) CK(cudaMemcpyAsync(sub, ctx->sub.p, N * 4, cudaMemcpyDeviceToHost, st));
     if (cd && N > 0) CK(cudaMemcpyAsync(cd, ctx->cd.p, N * 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    CK(stream_wait(ctx, st));
     return rc;
 }
 
@@ -1365,6 +1382,7 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
     for (sexgpu_ctx *w : ctx->workers) {
         w->kron_warp_max = ctx->kron_warp_max;
         w->nnw_dev = ctx->nnw_dev;
+        w->sync_block = ctx->batch_sync;
     }
     // largest frames first, so that the last frames to start are short
     std::vector<int> order(nframes);
@@ -1427,7 +1445,7 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
             }
             if (n > 0) {
                 cudaError_t e = cudaMemcpyAsync(wc->rows_host, wc->rows.p, nb, cudaMemcpyDeviceToHost, wc->stream);
-                if (e == cudaSuccess) e = cudaStreamSynchronize(wc->stream);
+                if (e == cudaSuccess) e = stream_wait(wc, wc->stream);
                 if (e != cudaSuccess) {
                     f.status = set_err(wc, e, "catalogue copy");
                     continue;
@@ -1530,6 +1548,11 @@ int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value) {
     if (!strcmp(name, "batch_grid_div")) {
         if (value < 0) return SEXGPU_ERR_ARG;
         ctx->batch_grid_div = value;
+        return SEXGPU_OK;
+    }
+    if (!strcmp(name, "batch_sync")) {
+        if (value < 0 || value > 1) return SEXGPU_ERR_ARG;
+        ctx->batch_sync = value;
         return SEXGPU_OK;
     }
     if (!strcmp(name, "kron_warp_max")) {

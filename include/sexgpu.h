@@ -283,7 +283,10 @@ int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max);
  * pixels than this are summed by whole thread blocks instead of one warp
  * (default 8192, >= 1).  "batch_grid_div": the persistent grids of
  * sexgpu_extract_batch's workers use 1/n of the resident capacity each
- * (default 1).  Returns SEXGPU_ERR_ARG for an unknown name or value. */
+ * (default 1).  "batch_sync": 1 (default) makes the batch workers wait for
+ * their streams on blocking events, which leaves the host cores to the other
+ * workers and keeps batch times steady; 0 spins.  Returns SEXGPU_ERR_ARG for
+ * an unknown name or value. */
 int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value);
 
 #ifdef __cplusplus
