@@ -13,8 +13,10 @@
 namespace sx {
 
 constexpr int AN_WARPS = 8;
-// four resident CTAs per SM (at most 64 registers): these kernels wait on
-// pixel-list loads, and residency hides that better than registers saved
+// four resident CTAs per SM (at most 64 registers, a few spilled): these
+// kernels wait on pixel-list loads, and residency hides that better than
+// registers saved (analyse stage 1.37 ms at 4 CTAs/SM, 1.45 at 3 with fewer
+// spills, 1.65 at 2 with none; one 4096^2 frame)
 constexpr int AN_MINB = 4;
 
 __device__ __forceinline__ unsigned warp_max_u(unsigned v) {
@@ -93,7 +95,16 @@ __device__ unsigned warp_select(const unsigned *opix, int n, const float *cd, in
     return prefix;
 }
 
+// what the pixel pass of the robust preanalysis hands to its finishing
+// kernel (one thread per object)
+struct RobustRaw {
+    double mx, my, mx2, my2, mxy;
+    float rv, peak, cpeak;
+    int dnpix, area2, xmin, xmax, ymin, ymax, flags;
+};
+
 struct AnaArgs {
+    RobustRaw *raw;     // per-object scratch between the two robust kernels
     const float *cd, *sub, *back;
     const unsigned *opix;
     ObjBufs O;
@@ -109,7 +120,10 @@ struct AnaArgs {
 
 // Robust preanalysis of a deblended object over its final pixels
 // (src/cuda/cudaanalyse.cu:1906-2124); objects of level 0 kept the values of
-// the first preanalysis.
+// the first preanalysis.  One warp per object sums over the pixels; the
+// moments, ellipse and area correction are finished by k_robust_finish, one
+// thread per object, so that the double-precision tail does not run on one
+// lane of a warp.
 __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(AnaArgs A) {
     const int lane = threadIdx.x & 31;
     const int o = blockIdx.x * AN_WARPS + (threadIdx.x >> 5);
@@ -175,9 +189,36 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(AnaAr
     area2 = warp_sum_i(area2);
     if (lane != 0) return;
     if (srv.ovf | stv.ovf | smx.ovf | smy.ovf | smx2.ovf | smy2.ovf | smxy.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
+    RobustRaw R;
+    R.mx = xs_double(smx);
+    R.my = xs_double(smy);
+    R.mx2 = xs_double(smx2);
+    R.my2 = xs_double(smy2);
+    R.mxy = xs_double(smxy);
+    R.rv = rv;
+    R.peak = peak;
+    R.cpeak = cpeak;
+    R.dnpix = dnpix;
+    R.area2 = area2;
+    R.xmin = xmin;
+    R.xmax = xmax;
+    R.ymin = ymin;
+    R.ymax = ymax;
+    R.flags = flags;
+    A.raw[o] = R;
+    A.O.dflux[o] = xs_float(stv);
+}
+
+__global__ void k_robust_finish(AnaArgs A) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= A.nobj || A.O.level[o] == 0) return;
+    const RobustRaw R = A.raw[o];
+    const int xmin = R.xmin, ymin = R.ymin, flags = R.flags, dnpix = R.dnpix, area2 = R.area2;
+    const float rv = R.rv, peak = R.peak, cpeak = R.cpeak;
+    const double dth = A.O.dthr[o], dthresh2 = (dth + peak) / 2.0;
     double mxo = A.O.mx[o], myo = A.O.my[o];
-    double rvd = rv, mx = xs_double(smx), my = xs_double(smy);
-    double mx2 = xs_double(smx2), my2 = xs_double(smy2), mxy = xs_double(smxy);
+    double rvd = rv, mx = R.mx, my = R.my;
+    double mx2 = R.mx2, my2 = R.my2, mxy = R.mxy;
     double xm = mx / rvd, ym = my / rvd, xm2, ym2, xym;
     if (flags & SX_OBJ_MERGED) {
         double xn = mxo - xmin, yn = myo - ymin;
@@ -219,14 +260,13 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(AnaAr
     A.O.flags[o] = flags;
     A.O.singu[o] = singu;
     A.O.xmin[o] = xmin;
-    A.O.xmax[o] = xmax;
+    A.O.xmax[o] = R.xmax;
     A.O.ymin[o] = ymin;
-    A.O.ymax[o] = ymax;
+    A.O.ymax[o] = R.ymax;
     A.O.fdflux[o] = rv;
     A.O.fdpeak[o] = cpeak;
     A.O.dpeak[o] = peak;
     A.O.dnpix[o] = dnpix;
-    A.O.dflux[o] = xs_float(stv);
     A.O.mx[o] = xm + xmin;
     A.O.my[o] = ym + ymin;
     A.O.mx2[o] = xm2;
@@ -399,6 +439,7 @@ void launch_analyse(const AnaArgs &A, cudaStream_t st) {
     if (A.nobj <= 0) return;
     const unsigned grid = (A.nobj + AN_WARPS - 1) / AN_WARPS;
     k_analyse_robust<<<grid, AN_WARPS * 32, 0, st>>>(A);
+    k_robust_finish<<<(unsigned)((A.nobj + 127) / 128), 128, 0, st>>>(A);
     if (A.O.dbkg) {
         k_local_stat<<<(unsigned)((A.nobj + 127) / 128), 128, 0, st>>>(A.sub, A.w, A.h, A.bp_thick, A.O.xmin,
                                                                          A.O.xmax, A.O.ymin, A.O.ymax, A.nobj,

@@ -95,6 +95,7 @@ struct sexgpu_ctx {
         skeys, svals, skalt, svalt, rows;
     DevBuf kitem[2], kchunk[2], kpart[2];  // queued Kron boxes
     DevBuf o_sprob;                        // CLASS_STAR per object
+    DevBuf o_raw;                          // robust preanalysis scratch per object
     DevBuf o_dbkg, o_lstat;                // BACKPHOTO_TYPE LOCAL: annulus mode, annulus statistics
     bool cfg_local = false;                // the current extraction uses LOCAL photometry background
     DevBuf fitsraw;                        // FITS data block as stored (sexgpu_extract_fits)
@@ -759,6 +760,8 @@ int pipe_analyse(sexgpu_ctx *ctx) {
     radix_sort_pairs(keys, vals, P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), nrootpix, bits_for(nobj), tmp, st);
     exclusive_scan(O.n, O.off, nobj, nullptr, tmp, st);
     AnaArgs AA;
+    EN(o_raw, (size_t)(nobj + 1) * sizeof(RobustRaw));
+    AA.raw = P<RobustRaw>(ctx->o_raw);
     AA.cd = A.cd;
     AA.sub = A.sub;
     AA.back = B.back3;
@@ -782,7 +785,7 @@ int pipe_analyse(sexgpu_ctx *ctx) {
     AA.afac = Pm.analysis_thresh;
     AA.bp_thick = Pm.bp_thick;
     launch_analyse(AA, st);
-    stage_mark(ctx, "analyse", 2 + radix_launches(bits_for(nobj), nrootpix) + scan_launches(nobj));
+    stage_mark(ctx, "analyse", 3 + (Pm.bp_local ? 2 : 0) + radix_launches(bits_for(nobj), nrootpix) + scan_launches(nobj));
     ps.stage = 4;
     return SEXGPU_OK;
 }
@@ -1021,6 +1024,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
         free_buf(ctx->kpart[i]);
     }
     free_buf(ctx->o_sprob);
+    free_buf(ctx->o_raw);
     free_buf(ctx->o_dbkg);
     free_buf(ctx->o_lstat);
     free_buf(ctx->fitsraw);
