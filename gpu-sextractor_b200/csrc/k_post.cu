@@ -85,20 +85,26 @@ __device__ __forceinline__ void clean_test(const CleanObj &p, const CleanObj &q,
 }
 
 // every pair closer than CLEAN_ZONE*(a_i+a_j) is tested once, by the object
-// of larger a (lower index on ties), which searches 20*a around itself; one
-// warp per object.  The objects are packed by cell in row-major cell order,
-// so the cells of one row of the search box hold one contiguous range of
-// objects: the lanes stride over that range (coalesced, balanced).
-__global__ void k_clean_pairs(const CleanObj *__restrict__ packed, int n, double beta,
-                              const int *__restrict__ cellstart, int *master, int gx, int gy) {
-    const int lane = threadIdx.x & 31;
-    const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+// of larger a (lower index on ties), which searches 20*a around itself.  The
+// objects are packed by cell in row-major cell order, so the cells of one row
+// of the search box hold one contiguous range of objects: the lanes of a warp
+// stride over that range (coalesced, balanced).  One block of CL_PAIR_WARPS
+// warps per object, the warps taking the rows of its search box in turn, so
+// that the few objects with large boxes do not leave one warp running long
+// after the others.
+constexpr int CL_PAIR_WARPS = 4;
+
+__global__ void __launch_bounds__(CL_PAIR_WARPS * 32) k_clean_pairs(const CleanObj *__restrict__ packed, int n,
+                                                                    double beta, const int *__restrict__ cellstart,
+                                                                    int *master, int gx, int gy) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int k = blockIdx.x;
     if (k >= n) return;
     const CleanObj me = packed[k];
     const double rad = 20.0 * me.a * 1.001 + 2.0;
     int x0 = max((int)floor((me.mx - rad) / CL_CELL), 0), x1 = min((int)floor((me.mx + rad) / CL_CELL), gx - 1);
     int y0 = max((int)floor((me.my - rad) / CL_CELL), 0), y1 = min((int)floor((me.my + rad) / CL_CELL), gy - 1);
-    for (int cy = y0; cy <= y1; cy++) {
+    for (int cy = y0 + wid; cy <= y1; cy += CL_PAIR_WARPS) {
         const int t1 = __ldg(cellstart + cy * gx + x1 + 1);
         for (int t = __ldg(cellstart + cy * gx + x0) + lane; t < t1; t += 32) {
             const CleanObj o = packed[t];
@@ -127,6 +133,38 @@ __global__ void k_clean_chain(ObjBufs O, int n, unsigned *vkey, unsigned *vval, 
     int k = atomicAdd(nvict, 1);
     vkey[k] = (unsigned)m;
     vval[k] = (unsigned)i;
+}
+
+// victims in (master, index) order: one block sorts the (master << 32 |
+// index) keys, all distinct, in shared memory (bitonic network); larger
+// victim lists go through two stable radix sorts instead
+constexpr int CL_SORT_MAX = 4096;
+
+__global__ void __launch_bounds__(1024) k_victim_sort(unsigned *vkey, unsigned *vval, int nv) {
+    __shared__ unsigned long long s[CL_SORT_MAX];
+    int n2 = 1;
+    while (n2 < nv) n2 <<= 1;
+    for (int i = threadIdx.x; i < n2; i += blockDim.x)
+        s[i] = i < nv ? ((unsigned long long)vkey[i] << 32) | vval[i] : ~0ull;
+    __syncthreads();
+    for (int k = 2; k <= n2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const unsigned long long a = s[i], b = s[l];
+                    if ((a > b) == ((i & k) == 0)) {
+                        s[i] = b;
+                        s[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) {
+        vkey[i] = (unsigned)(s[i] >> 32);
+        vval[i] = (unsigned)s[i];
+    }
 }
 
 // victims sorted by (master, index): each segment head merges its segment
@@ -535,7 +573,9 @@ __device__ void end_finish(const EndArgs &A, int o, int flags, float kron, bool 
 }
 
 // after pass 1 (every lane holds its sums): pass 2 in this warp or queued
-__device__ void kron_after1(const EndArgs &A, int o, double mx, double my, int flags, const KronAcc &p1) {
+// defer_at: AUTO boxes of more pixels than this are queued for whole blocks
+__device__ void kron_after1(const EndArgs &A, int o, double mx, double my, int flags, const KronAcc &p1,
+                            int defer_at) {
     if ((p1.s0.ovf | p1.s1.ovf) && (threadIdx.x & 31) == 0) atomicOr(&A.sc->status, SX_ST_RANGE);
     float kron = 0.0f;
     KronGeo g;
@@ -546,7 +586,7 @@ __device__ void kron_after1(const EndArgs &A, int o, double mx, double my, int f
         return;
     }
     const int nn = kron_npix(g);
-    if (nn > A.K.warp_max && kron_defer(A, 1, o, flags, kron, g, nn)) return;
+    if (nn > defer_at && kron_defer(A, 1, o, flags, kron, g, nn)) return;
     kron_range<2>(A, o, mx, my, g, threadIdx.x & 31, nn, 32, p2);
     kacc_warp(p2);
     end_finish(A, o, flags, kron, true, p2);
@@ -569,7 +609,7 @@ __global__ void __launch_bounds__(128, 8) k_endobject(EndArgs A) {
     kacc_init(p1);
     kron_range<1>(A, o, mx, my, g, lane, nn, 32, p1);
     kacc_warp(p1);
-    kron_after1(A, o, mx, my, flags, p1);
+    kron_after1(A, o, mx, my, flags, p1, A.K.warp_max);
 }
 
 // queued boxes: one CTA per KR_CHUNK-pixel work item, partial sums per item
@@ -600,7 +640,12 @@ __global__ void __launch_bounds__(KR_THREADS) k_kron_chunks(EndArgs A) {
     }
 }
 
-// queued boxes: one warp per object merges its items' sums and continues
+// queued boxes: one warp per object merges its items' sums and continues;
+// the objects here have large Kron boxes, and their AUTO boxes of more than
+// KR_MERGE_MAX pixels go to the block queue too, so that this tail kernel
+// does not end on one warp summing thousands of pixels
+constexpr int KR_MERGE_MAX = 1024;
+
 template <int PASS>
 __global__ void k_kron_merge(EndArgs A) {
     const int lane = threadIdx.x & 31;
@@ -614,7 +659,7 @@ __global__ void k_kron_merge(EndArgs A) {
         for (int j = lane; j < it.nch; j += 32) kacc_merge(acc, A.K.part[PASS - 1][it.c0 + j]);
         kacc_warp(acc);
         if (PASS == 1)
-            kron_after1(A, it.o, A.O.mx[it.o], A.O.my[it.o], it.flags, acc);
+            kron_after1(A, it.o, A.O.mx[it.o], A.O.my[it.o], it.flags, acc, min(A.K.warp_max, KR_MERGE_MAX));
         else
             end_finish(A, it.o, it.flags, it.kron, true, acc);
     }

@@ -821,23 +821,30 @@ int pipe_clean(sexgpu_ctx *ctx) {
         exclusive_scan(cellcnt, cellcnt, ncell + 1, nullptr, tmp, st);
         k_clean_pack<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, Pm.clean_param, cellcnt, cellcur,
                                                        P<CleanObj>(ctx->amp), gx, gy);
-        k_clean_pairs<<<grid1(nobj, 4), 128, 0, st>>>(P<CleanObj>(ctx->amp), nobj, Pm.clean_param, cellcnt, O.master,
-                                                      gx, gy);
+        k_clean_pairs<<<(unsigned)nobj, CL_PAIR_WARPS * 32, 0, st>>>(P<CleanObj>(ctx->amp), nobj, Pm.clean_param,
+                                                                      cellcnt, O.master, gx, gy);
         CK(cudaMemsetAsync(&d_sc->nsurv, 0, 4, st));
         k_clean_chain<<<grid1(nobj, 256), 256, 0, st>>>(O, nobj, P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval),
                                                         &d_sc->nsurv);
         rc = read_scalars(ctx);
         if (rc) return rc;
         nv = ctx->hsc.nsurv;
-        radix_sort_pairs(P<unsigned>(ctx->vval), P<unsigned>(ctx->vkey), P<unsigned>(ctx->vkalt),
-                         P<unsigned>(ctx->vvalt), nv, bits_for(nobj), tmp, st);  // victims by index
-        radix_sort_pairs(P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval), P<unsigned>(ctx->vkalt),
-                         P<unsigned>(ctx->vvalt), nv, bits_for(nobj), tmp, st);  // then by master
+        int sort_launches = 0;
+        if (nv > 0 && nv <= CL_SORT_MAX) {
+            k_victim_sort<<<1, 1024, 0, st>>>(P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval), nv);
+            sort_launches = 1;
+        } else if (nv > 0) {
+            radix_sort_pairs(P<unsigned>(ctx->vval), P<unsigned>(ctx->vkey), P<unsigned>(ctx->vkalt),
+                             P<unsigned>(ctx->vvalt), nv, bits_for(nobj), tmp, st);  // victims by index
+            radix_sort_pairs(P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval), P<unsigned>(ctx->vkalt),
+                             P<unsigned>(ctx->vvalt), nv, bits_for(nobj), tmp, st);  // then by master
+            sort_launches = 2 * radix_launches(bits_for(nobj), nv);
+        }
         if (nv > 0) {
             k_clean_merge<<<grid1(nv, 128), 128, 0, st>>>(O, P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval), nv);
             k_alloc_victims<<<nobj, 128, 0, st>>>(O, vals, A.alloc, nobj);
         }
-        cl_launch = 6 + scan_launches(ncell + 1) + 2 * radix_launches(bits_for(nobj), nv);
+        cl_launch = 6 + scan_launches(ncell + 1) + sort_launches;
     } else if (nobj > 0) {
         CK(cudaMemsetAsync(O.fmaster, 0xff, (size_t)nobj * 4, st));
     }
