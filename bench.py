@@ -311,7 +311,7 @@ def host_state(frames):
             "memcpy_gb_s": round(2 * big.nbytes / dt / 1e9, 2)}
 
 
-def run_batch(ctx, frames, reps=3, workers=8, maxobj=400000):
+def run_batch(ctx, frames, reps=5, workers=8, maxobj=400000):
     """Plain path (sexgpu_extract, one frame after the other) against the
     batched form (sexgpu_extract_batch) on the same frames: host frames in,
     host catalogues out, wall clock around the whole batch; catalogues
@@ -322,7 +322,10 @@ def run_batch(ctx, frames, reps=3, workers=8, maxobj=400000):
     def batched():
         return [c for c, _ in ctx.extract_batch(frames, workers=workers, max_objects=maxobj)]
 
-    ref, got = plain(), batched()  # warm-up (first use allocates the workers' buffers)
+    # warm-up: the first uses size every worker's buffers (frames go to whichever
+    # worker is free, so a worker meets larger frames over several batches)
+    ref, got = plain(), batched()
+    batched()
     identical = len(ref) == len(got) and all(a.tobytes() == b.tobytes() for a, b in zip(ref, got))
     differing = []
     for i, (a, b) in enumerate(zip(ref, got)):

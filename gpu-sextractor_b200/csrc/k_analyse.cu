@@ -103,8 +103,17 @@ struct RobustRaw {
     int dnpix, area2, xmin, xmax, ymin, ymax, flags;
 };
 
+// what the pixel pass of examineiso hands to its finishing kernel
+struct ExamRaw {
+    XSum stv, svar;
+    double esum, emx2, emy2, emxy, s, sx, sy, sxx, sxy;
+    float opeak, thresh0, mthresh;
+    int peakpix, area;
+};
+
 struct AnaArgs {
     RobustRaw *raw;     // per-object scratch between the two robust kernels
+    ExamRaw *xraw;      // per-object scratch between the two examineiso kernels
     const float *cd, *sub, *back;
     const unsigned *opix;
     ObjBufs O;
@@ -292,7 +301,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
     const unsigned *pix = A.opix + off;
     const float dthresh = A.O.dthr[o], thresh = A.O.athr[o], gthresh = A.sc->thresh, backsig = A.sc->backsig;
     const double mxo = A.O.mx[o], myo = A.O.my[o];
-    double dbacknoise2 = backsig * backsig, var = backsig * backsig;
+    double dbacknoise2 = backsig * backsig;
     unsigned pk = 0u;
     unsigned long long best = 0ull;
     int area = 0;
@@ -386,10 +395,47 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
     sxx = warp_sum_d(sxx);
     sxy = warp_sum_d(sxy);
     if (lane != 0) return;
+    ExamRaw X;
+    X.stv = stv;
+    X.svar = svar;
+    X.esum = esum;
+    X.emx2 = emx2;
+    X.emy2 = emy2;
+    X.emxy = emxy;
+    X.s = s;
+    X.sx = sx;
+    X.sy = sy;
+    X.sxx = sxx;
+    X.sxy = sxy;
+    X.opeak = opeak;
+    X.thresh0 = thresh0;
+    X.mthresh = mthresh;
+    X.peakpix = (int)(0xffffffffu - (unsigned)(best & 0xffffffffu));
+    X.area = area;
+    A.xraw[o] = X;
+#pragma unroll
+    for (int k = 0; k < SX_NISO_; k++) A.O.iso[(size_t)o * SX_NISO_ + k] = iso[k];
+}
+
+// examineiso, per object: position errors, fluxes, FWHM fit, background
+// (one thread per object, so that this double-precision tail does not run on
+// one lane of a warp)
+__global__ void k_examine_finish(AnaArgs A) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= A.nobj) return;
+    const ExamRaw X = A.xraw[o];
+    const XSum stv = X.stv, svar = X.svar;
+    double esum = X.esum, emx2 = X.emx2, emy2 = X.emy2, emxy = X.emxy;
+    const double s = X.s, sx = X.sx, sy = X.sy, sxx = X.sxx, sxy = X.sxy;
+    const float opeak = X.opeak, thresh0 = X.thresh0, mthresh = X.mthresh;
+    const int peakpix = X.peakpix, area = X.area, n = A.O.n[o], w = A.w;
+    const double mxo = A.O.mx[o], myo = A.O.my[o];
+    const float backsig = A.sc->backsig;
+    const double var = backsig * backsig;
+    const float dbkg = A.O.dbkg ? A.O.dbkg[o] : 0.0f;
     const int singu = A.O.singu[o];
     const float fdflux = A.O.fdflux[o], a = A.O.a[o], b = A.O.b[o];
     float bkg = back_at(A.back, A.nbx, A.nby, A.bw, A.bh, (int)(mxo + 0.5), (int)(myo + 0.5));
-    int peakpix = (int)(0xffffffffu - (unsigned)(best & 0xffffffffu));
     {
         double flux2 = fdflux * fdflux;
         emx2 /= flux2;
@@ -430,8 +476,6 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
     A.O.pmxy[o] = emxy;
     A.O.fwhm[o] = fwhm;
     A.O.fdnpix[o] = n;
-#pragma unroll
-    for (int k = 0; k < SX_NISO_; k++) A.O.iso[(size_t)o * SX_NISO_ + k] = iso[k];
     if (stv.ovf | svar.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
 }
 
@@ -448,6 +492,7 @@ void launch_analyse(const AnaArgs &A, cudaStream_t st) {
                                                                    A.O.ymin, A.O.ymax, A.O.lstat, A.O.dbkg);
     }
     k_examineiso<<<grid, AN_WARPS * 32, 0, st>>>(A);
+    k_examine_finish<<<(unsigned)((A.nobj + 127) / 128), 128, 0, st>>>(A);
 }
 
 }  // namespace sx

@@ -611,14 +611,31 @@ __device__ unsigned select_kth(const float *v, int n, int k, unsigned lowkey, un
         }
         __syncthreads();
         __shared__ unsigned s_digit, s_k;
-        if (threadIdx.x == 0) {
-            unsigned c = 0, d = 0;
-            for (d = 0; d < 256; d++) {
-                if (c + hist[d] > (unsigned)k) break;
-                c += hist[d];
+        if (threadIdx.x < 32) {
+            // the digit holding rank k: lane l owns bins 8l..8l+7, a warp scan
+            // of the lane totals finds the owner, the owner its bin
+            const int lane = threadIdx.x;
+            unsigned c[8], tot = 0;
+#pragma unroll
+            for (int t = 0; t < 8; t++) tot += (c[t] = hist[lane * 8 + t]);
+            unsigned incl = tot;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
             }
-            s_digit = d;
-            s_k = k - c;
+            const unsigned sel = __ballot_sync(0xffffffffu, incl > (unsigned)k);
+            const int owner = sel ? __ffs(sel) - 1 : 31;
+            if (lane == owner) {
+                unsigned below = incl - tot, d = lane * 8;
+#pragma unroll
+                for (int t = 0; t < 8; t++)
+                    if (d == (unsigned)(lane * 8 + t) && below + c[t] <= (unsigned)k && t < 7) {
+                        below += c[t];
+                        d++;
+                    }
+                s_digit = d;
+                s_k = k - below;
+            }
         }
         __syncthreads();
         prefix |= s_digit << shift;
@@ -689,18 +706,22 @@ __global__ void k_back_spline(const float *__restrict__ map, float *__restrict__
     if (x >= nbx) return;
     float temp;
     if (nby > 1) {
+        // the previous step's values are carried in registers, not read back
+        // from the arrays just written (same operations, same order)
         float *ux = u + (size_t)x * nby;
+        float dprev = 0.0f, uprev = 0.0f;
         dmap[x] = ux[0] = 0.0;
         for (int y = 1; y < nby - 1; y++) {
-            temp = -1 / (dmap[(size_t)(y - 1) * nbx + x] + 4);
-            dmap[(size_t)y * nbx + x] = temp;
-            temp *= ux[y - 1] - 6 * (map[(size_t)(y + 1) * nbx + x] + map[(size_t)(y - 1) * nbx + x]
-                                     - 2 * map[(size_t)y * nbx + x]);
-            ux[y] = temp;
+            temp = -1 / (dprev + 4);
+            dmap[(size_t)y * nbx + x] = dprev = temp;
+            temp *= uprev - 6 * (map[(size_t)(y + 1) * nbx + x] + map[(size_t)(y - 1) * nbx + x]
+                                 - 2 * map[(size_t)y * nbx + x]);
+            ux[y] = uprev = temp;
         }
         dmap[(size_t)(nby - 1) * nbx + x] = 0.0;
+        float dnext = 0.0f;
         for (int y = nby - 2; y >= 1; y--)
-            dmap[(size_t)y * nbx + x] = (dmap[(size_t)y * nbx + x] * dmap[(size_t)(y + 1) * nbx + x] + ux[y]) / 6.0;
+            dmap[(size_t)y * nbx + x] = dnext = (dmap[(size_t)y * nbx + x] * dnext + ux[y]) / 6.0;
     } else
         dmap[x] = 0.0;
 }
@@ -753,15 +774,24 @@ __global__ void k_row_nodes(const float *__restrict__ back, const float *__restr
         const float *dblo = dback + (size_t)nbx * yl, *dbhi = dblo + nbx;
         for (int x = 0; x < nbx; x++) nd[x] = cdy * blo[x] + dy * bhi[x] + cdy3 * dblo[x] + dy3 * dbhi[x];
         if (nbx > 1) {
+            // node values recomputed and the previous step carried in
+            // registers instead of read back from this thread's own stores
+            // (the same operations in the same order, so the same values)
+            auto node_at = [&](int x) { return cdy * blo[x] + dy * bhi[x] + cdy3 * dblo[x] + dy3 * dbhi[x]; };
+            float dprev = 0.0f, uprev = 0.0f, nm = node_at(0), n0 = node_at(1);
             dnd[0] = uu[0] = 0.0;
             for (int x = 1; x < nbx - 1; x++) {
-                temp = -1 / (dnd[x - 1] + 4);
-                dnd[x] = temp;
-                temp *= uu[x - 1] - 6 * (nd[x + 1] + nd[x - 1] - 2 * nd[x]);
-                uu[x] = temp;
+                const float np = node_at(x + 1);
+                temp = -1 / (dprev + 4);
+                dnd[x] = dprev = temp;
+                temp *= uprev - 6 * (np + nm - 2 * n0);
+                uu[x] = uprev = temp;
+                nm = n0;
+                n0 = np;
             }
             dnd[nbx - 1] = 0.0;
-            for (int x = nbx - 2; x >= 1; x--) dnd[x] = (dnd[x] * dnd[x + 1] + uu[x]) / 6.0;
+            float dnext = 0.0f;
+            for (int x = nbx - 2; x >= 1; x--) dnd[x] = dnext = (dnd[x] * dnext + uu[x]) / 6.0;
         } else
             dnd[0] = 0.0;
     } else {

@@ -95,7 +95,7 @@ struct sexgpu_ctx {
         skeys, svals, skalt, svalt, rows;
     DevBuf kitem[2], kchunk[2], kpart[2];  // queued Kron boxes
     DevBuf o_sprob;                        // CLASS_STAR per object
-    DevBuf o_raw;                          // robust preanalysis scratch per object
+    DevBuf o_raw, o_xraw;                  // robust preanalysis / examineiso scratch per object
     DevBuf o_dbkg, o_lstat;                // BACKPHOTO_TYPE LOCAL: annulus mode, annulus statistics
     bool cfg_local = false;                // the current extraction uses LOCAL photometry background
     DevBuf fitsraw;                        // FITS data block as stored (sexgpu_extract_fits)
@@ -115,6 +115,10 @@ struct sexgpu_ctx {
     std::vector<std::string> stage_names;
     std::vector<int> stage_launches;
     std::vector<sexgpu_ctx *> workers;  // contexts of sexgpu_extract_batch
+    // buffers outgrown during a batch: freed when the batch ends, because
+    // cudaFree waits for the whole device and would stall the other workers
+    bool defer_free = false;
+    std::vector<void *> graveyard, host_graveyard;
     void *stage_host = nullptr;         // pinned staging of a batch worker's frames
     size_t stage_bytes = 0;
     void *rows_host = nullptr;          // pinned staging of a batch worker's catalogue rows
@@ -140,7 +144,12 @@ int set_err(sexgpu_ctx *c, cudaError_t e, const char *what) {
 int ensure(sexgpu_ctx *ctx, DevBuf &b, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (b.bytes >= bytes) return SEXGPU_OK;
-    if (b.p) cudaFree(b.p);
+    if (b.p) {
+        if (ctx->defer_free)
+            ctx->graveyard.push_back(b.p);
+        else
+            cudaFree(b.p);
+    }
     b.p = nullptr;
     b.bytes = 0;
     size_t want = bytes + bytes / 8;
@@ -762,6 +771,8 @@ int pipe_analyse(sexgpu_ctx *ctx) {
     AnaArgs AA;
     EN(o_raw, (size_t)(nobj + 1) * sizeof(RobustRaw));
     AA.raw = P<RobustRaw>(ctx->o_raw);
+    EN(o_xraw, (size_t)(nobj + 1) * sizeof(ExamRaw));
+    AA.xraw = P<ExamRaw>(ctx->o_xraw);
     AA.cd = A.cd;
     AA.sub = A.sub;
     AA.back = B.back3;
@@ -785,7 +796,7 @@ int pipe_analyse(sexgpu_ctx *ctx) {
     AA.afac = Pm.analysis_thresh;
     AA.bp_thick = Pm.bp_thick;
     launch_analyse(AA, st);
-    stage_mark(ctx, "analyse", 3 + (Pm.bp_local ? 2 : 0) + radix_launches(bits_for(nobj), nrootpix) + scan_launches(nobj));
+    stage_mark(ctx, "analyse", 4 + (Pm.bp_local ? 2 : 0) + radix_launches(bits_for(nobj), nrootpix) + scan_launches(nobj));
     ps.stage = 4;
     return SEXGPU_OK;
 }
@@ -1032,6 +1043,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     }
     free_buf(ctx->o_sprob);
     free_buf(ctx->o_raw);
+    free_buf(ctx->o_xraw);
     free_buf(ctx->o_dbkg);
     free_buf(ctx->o_lstat);
     free_buf(ctx->fitsraw);
@@ -1051,6 +1063,8 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_block) cudaEventDestroy(ctx->ev_block);
     for (sexgpu_ctx *w : ctx->workers) sexgpu_destroy(w);
+    for (void *p : ctx->graveyard) cudaFree(p);
+    for (void *p : ctx->host_graveyard) cudaFreeHost(p);
     if (ctx->stage_host) cudaFreeHost(ctx->stage_host);
     if (ctx->rows_host) cudaFreeHost(ctx->rows_host);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1394,6 +1408,7 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
         w->kron_warp_max = ctx->kron_warp_max;
         w->nnw_dev = ctx->nnw_dev;
         w->sync_block = ctx->batch_sync;
+        w->defer_free = true;
     }
     // largest frames first, so that the last frames to start are short
     std::vector<int> order(nframes);
@@ -1406,16 +1421,18 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
     // first and brings the catalogue rows back through another, so that the
     // transfers of different workers are DMA transfers that proceed in
     // parallel instead of queueing on the driver's pageable staging.
-    auto grow = [](void *&buf, size_t &have, size_t need) {
+    // pinned buffers grow with headroom; outgrown ones are freed after the batch
+    auto grow = [](sexgpu_ctx *wc, void *&buf, size_t &have, size_t need) {
         if (have >= need) return true;
-        if (buf) cudaFreeHost(buf);
+        if (buf) wc->host_graveyard.push_back(buf);
         buf = nullptr;
         have = 0;
-        if (cudaHostAlloc(&buf, need, cudaHostAllocPortable) != cudaSuccess) {
+        const size_t want = need + need / 4;
+        if (cudaHostAlloc(&buf, want, cudaHostAllocPortable) != cudaSuccess) {
             cudaGetLastError();
             return false;
         }
-        have = need;
+        have = want;
         return true;
     };
     const int div = ctx->batch_grid_div > 0 ? ctx->batch_grid_div : 1;
@@ -1431,7 +1448,7 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
             }
             const size_t bytes = (size_t)f.w * f.h * sizeof(float);
             const float *src = f.img, *wsrc = f.wmap;
-            if (grow(wc->stage_host, wc->stage_bytes, f.wmap ? 2 * bytes : bytes)) {
+            if (grow(wc, wc->stage_host, wc->stage_bytes, f.wmap ? 2 * bytes : bytes)) {
                 memcpy(wc->stage_host, f.img, bytes);
                 src = (const float *)wc->stage_host;
                 if (f.wmap) {
@@ -1440,7 +1457,7 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
                 }
             }
             const size_t rbytes = (size_t)f.max_objects * sizeof(sexgpu_object);
-            if (!grow(wc->rows_host, wc->rows_bytes, std::min(rbytes, (size_t)1 << 20))) {
+            if (!grow(wc, wc->rows_host, wc->rows_bytes, std::min(rbytes, (size_t)1 << 20))) {
                 f.status = sexgpu_extract(wc, src, wsrc, f.w, f.h, f.cfg, f.objs, f.max_objects, &f.nobj, nullptr,
                                           nullptr, nullptr, &f.summary);
                 continue;
@@ -1450,7 +1467,7 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
             if (f.status) continue;
             const int n = std::min(f.nobj, f.max_objects);
             const size_t nb = (size_t)n * sizeof(sexgpu_object);
-            if (n > 0 && !grow(wc->rows_host, wc->rows_bytes, nb)) {
+            if (n > 0 && !grow(wc, wc->rows_host, wc->rows_bytes, nb)) {
                 f.status = SEXGPU_ERR_NOMEM;
                 continue;
             }
@@ -1471,6 +1488,13 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
     run(ctx->workers[0]);
     for (auto &t : pool) t.join();
     sx_grid_div = 1;
+    for (sexgpu_ctx *w : ctx->workers) {
+        w->defer_free = false;
+        for (void *p : w->graveyard) cudaFree(p);
+        for (void *p : w->host_graveyard) cudaFreeHost(p);
+        w->graveyard.clear();
+        w->host_graveyard.clear();
+    }
     for (int i = 0; i < nframes; i++)
         if (frames[i].status != SEXGPU_OK) {
             ctx->err = "frame " + std::to_string(i) + " failed";
