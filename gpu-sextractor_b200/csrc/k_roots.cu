@@ -20,49 +20,6 @@ __global__ void k_count_labels(const int *__restrict__ lab, int *__restrict__ cn
     if (l >= 0 && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&cnt[l], __popc(same));
 }
 
-// flag[p] = 1 if p is the root (smallest pixel) of a component >= minarea
-__global__ void k_root_flags(const int *__restrict__ lab, const int *__restrict__ cnt, int *__restrict__ flag,
-                             long long n, int minarea) {
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    flag[p] = (lab[p] == (int)p && cnt[p] >= minarea) ? 1 : 0;
-}
-
-// flag2[p] = 1 if p belongs to a kept component (cnt at its root >= minarea)
-__global__ void k_pix_flags(const int *__restrict__ lab, const int *__restrict__ cnt, int *__restrict__ flag,
-                            long long n, int minarea) {
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    int l = lab[p];
-    flag[p] = (l >= 0 && cnt[l] >= minarea) ? 1 : 0;
-}
-
-// per root: size, first pixel; scanned root flags give the root id
-__global__ void k_root_setup(const int *__restrict__ lab, const int *__restrict__ cnt, const int *__restrict__ rid,
-                             int *__restrict__ rsize, int *__restrict__ rfirst, long long n, int minarea) {
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    if (lab[p] == (int)p && cnt[p] >= minarea) {
-        int r = rid[p];
-        rsize[r] = cnt[p];
-        rfirst[r] = (int)p;
-    }
-}
-
-// compaction of kept pixels in raster order with their root id as sort key
-__global__ void k_pix_compact(const int *__restrict__ lab, const int *__restrict__ cnt, const int *__restrict__ rid,
-                              const int *__restrict__ pos, unsigned *__restrict__ keys, unsigned *__restrict__ vals,
-                              long long n, int minarea) {
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    int l = lab[p];
-    if (l >= 0 && cnt[l] >= minarea) {
-        int j = pos[p];
-        keys[j] = (unsigned)rid[l];
-        vals[j] = (unsigned)p;
-    }
-}
-
 __global__ void k_pos2idx(const unsigned *__restrict__ vals, int *__restrict__ pos2idx, int m) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < m) pos2idx[vals[j]] = j;
@@ -94,6 +51,101 @@ __global__ void k_root_thresholds_global(int nroots, const FrameScalars *sc, flo
     if (r < nroots) {
         rdthr[r] = sc->dthresh;
         rathr[r] = sc->thresh;
+    }
+}
+
+// ---- the raw-object numbering and the kept-pixel compaction as two scans
+// whose inputs are computed on the fly (a root: lab[p] == p with at least
+// minarea pixels; a kept pixel: its root has at least minarea pixels).  The
+// tiles of SCAN_TILE pixels are those of the scan primitive (1024 threads, 4
+// consecutive pixels each), so the per-tile counts of k_root_tile_counts and
+// the in-tile prefixes of k_root_number / k_root_compact line up.
+__device__ __forceinline__ void root_kept_flags(const int *__restrict__ lab, const int *__restrict__ cnt, long long p,
+                                                long long n, int minarea, int &isroot, int &kept, int &l) {
+    l = p < n ? lab[p] : -1;
+    kept = l >= 0 && cnt[l] >= minarea;
+    isroot = kept && l == (int)p;
+}
+
+// per tile: number of roots and of kept pixels
+__global__ void __launch_bounds__(SCAN_THREADS) k_root_tile_counts(const int *__restrict__ lab,
+                                                                  const int *__restrict__ cnt, long long n,
+                                                                  int minarea, int *__restrict__ troots,
+                                                                  int *__restrict__ tkept) {
+    __shared__ int sh[32];
+    const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+    int cr = 0, ck = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        int r, kp, l;
+        root_kept_flags(lab, cnt, base + k, n, minarea, r, kp, l);
+        cr += r;
+        ck += kp;
+    }
+    int tot;
+    block_exclusive_scan(cr, sh, tot);
+    if (threadIdx.x == 0) troots[blockIdx.x] = tot;
+    block_exclusive_scan(ck, sh, tot);
+    if (threadIdx.x == 0) tkept[blockIdx.x] = tot;
+}
+
+// roots numbered in raster order: rid at the root pixel, size and first pixel
+__global__ void __launch_bounds__(SCAN_THREADS) k_root_number(const int *__restrict__ lab, const int *__restrict__ cnt,
+                                                             long long n, int minarea, const int *__restrict__ toff,
+                                                             int *__restrict__ rid, int *__restrict__ rsize,
+                                                             int *__restrict__ rfirst) {
+    __shared__ int sh[32];
+    const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+    int fr[SCAN_ITEMS], c = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        int kp, l;
+        root_kept_flags(lab, cnt, base + k, n, minarea, fr[k], kp, l);
+        c += fr[k];
+    }
+    int tot;
+    int id = block_exclusive_scan(c, sh, tot) + toff[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++)
+        if (fr[k]) {
+            const long long p = base + k;
+            rid[p] = id;
+            rsize[id] = cnt[p];
+            rfirst[id] = (int)p;
+            id++;
+        }
+}
+
+// kept pixels compacted in raster order with their root id as sort key; the
+// allocation map starts as "unassigned object pixel" / background and the
+// pixel -> list index map as -1
+__global__ void __launch_bounds__(SCAN_THREADS) k_root_compact(const int *__restrict__ lab, const int *__restrict__ cnt,
+                                                              long long n, int minarea, const int *__restrict__ toff,
+                                                              const int *__restrict__ rid, unsigned *__restrict__ keys,
+                                                              unsigned *__restrict__ vals, int *__restrict__ alloc,
+                                                              int *__restrict__ pos2idx) {
+    __shared__ int sh[32];
+    const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+    int fk[SCAN_ITEMS], lb[SCAN_ITEMS], c = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        int r;
+        root_kept_flags(lab, cnt, base + k, n, minarea, r, fk[k], lb[k]);
+        c += fk[k];
+    }
+    int tot;
+    int j = block_exclusive_scan(c, sh, tot) + toff[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        const long long p = base + k;
+        if (p >= n) break;
+        alloc[p] = lb[k] >= 0 ? SX_ALLOC_OTHER : -1;
+        pos2idx[p] = -1;
+        if (fk[k]) {
+            keys[j] = (unsigned)rid[lb[k]];
+            vals[j] = (unsigned)p;
+            j++;
+        }
     }
 }
 

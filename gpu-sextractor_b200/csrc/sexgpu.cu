@@ -292,11 +292,6 @@ __global__ void k_init_scalars(FrameScalars *sc) {
     *sc = z;
 }
 
-__global__ void k_alloc_init(const int *lab, int *alloc, long long n) {
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < n) alloc[p] = lab[p] >= 0 ? SX_ALLOC_OTHER : -1;
-}
-
 // Waits for the work queued on st: a spinning wait (the runtime's default
 // with few host threads), or, for a batch worker told so, a blocking event
 // wait that leaves the host core to the other workers.
@@ -465,7 +460,7 @@ int pipe_begin(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, 
     EN(lab, N * 4);
     EN(cnt, N * 4);
     EN(flag, N * 4);
-    EN(pos, N * 4);
+    EN(pos, std::max(N, 4 * ((N + SCAN_TILE - 1) / SCAN_TILE) + 4) * 4);  // or the four tile arrays of the root scans
     EN(alloc, N * 4);
     EN(pos2idx, N * 4);
     EN(keys, N * 4);
@@ -579,9 +574,13 @@ int pipe_detect(sexgpu_ctx *ctx) {
     int *lab = P<int>(ctx->lab), *cnt = P<int>(ctx->cnt), *flag = P<int>(ctx->flag), *pos = P<int>(ctx->pos);
     CK(cudaMemsetAsync(cnt, 0, N * 4, st));
     k_count_labels<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, N);
-    k_root_flags<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, flag, N, Pm.minarea);
-    int *d_tot = &d_sc->nroots;
-    exclusive_scan(flag, flag, N, d_tot, tmp, st);  // flag -> root id
+    // per-tile counts of roots and kept pixels, scanned into tile offsets
+    // (pos holds the two count arrays and the two offset arrays)
+    const int ntile = (int)((N + SCAN_TILE - 1) / SCAN_TILE);
+    int *troots = pos, *tkept = pos + ntile, *troff = pos + 2 * ntile, *tkoff = pos + 3 * ntile;
+    k_root_tile_counts<<<ntile, SCAN_THREADS, 0, st>>>(lab, cnt, N, Pm.minarea, troots, tkept);
+    exclusive_scan(troots, troff, ntile, &d_sc->nroots, tmp, st);
+    exclusive_scan(tkept, tkoff, ntile, nullptr, tmp, st);
     rc = read_scalars(ctx);
     if (rc) return rc;
     if (ctx->hsc.dthresh <= 0.0f || ctx->hsc.thresh <= 0.0f) {
@@ -612,12 +611,12 @@ int pipe_detect(sexgpu_ctx *ctx) {
     R.objbase = P<int>(ctx->robjbase);
     R.dthresh = P<float>(ctx->rdthr);
     R.thresh = P<float>(ctx->rathr);
-    k_root_setup<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, flag, R.size, R.first, N, Pm.minarea);
+    k_root_number<<<ntile, SCAN_THREADS, 0, st>>>(lab, cnt, N, Pm.minarea, troff, flag, R.size, R.first);
     exclusive_scan(R.size, R.off, nroots, &d_sc->nrootpix, tmp, st);
-    k_pix_flags<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, pos, N, Pm.minarea);
-    exclusive_scan(pos, pos, N, nullptr, tmp, st);
     unsigned *keys = P<unsigned>(ctx->keys), *vals = P<unsigned>(ctx->vals);
-    k_pix_compact<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, flag, pos, keys, vals, N, Pm.minarea);
+    int *pos2idx = P<int>(ctx->pos2idx);
+    k_root_compact<<<ntile, SCAN_THREADS, 0, st>>>(lab, cnt, N, Pm.minarea, tkoff, flag, keys, vals,
+                                                   P<int>(ctx->alloc), pos2idx);
     if (ps.wvar) {
         CK(cudaMemsetAsync(R.dthresh, 0x7f, (size_t)(nroots + 1) * 4, st));
         CK(cudaMemsetAsync(R.thresh, 0x7f, (size_t)(nroots + 1) * 4, st));
@@ -633,11 +632,8 @@ int pipe_detect(sexgpu_ctx *ctx) {
     radix_sort_pairs(keys, vals, P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), nrootpix, bits_for(nroots), tmp, st);
     unsigned *rpix = P<unsigned>(ctx->rpix);
     CK(cudaMemcpyAsync(rpix, vals, (size_t)nrootpix * 4, cudaMemcpyDeviceToDevice, st));
-    int *pos2idx = P<int>(ctx->pos2idx);
-    CK(cudaMemsetAsync(pos2idx, 0xff, N * 4, st));
     k_pos2idx<<<grid1(nrootpix, 256), 256, 0, st>>>(rpix, pos2idx, nrootpix);
-    k_alloc_init<<<grid1(N, 256), 256, 0, st>>>(lab, P<int>(ctx->alloc), N);
-    stage_mark(ctx, "roots", 9 + 3 * scan_launches(N) + scan_launches(nroots) + radix_launches(bits_for(nroots), nrootpix));
+    stage_mark(ctx, "roots", 6 + 2 * scan_launches(ntile) + scan_launches(nroots) + radix_launches(bits_for(nroots), nrootpix));
     ps.stage = 2;
     return SEXGPU_OK;
 }
