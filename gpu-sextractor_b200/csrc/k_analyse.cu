@@ -479,6 +479,96 @@ __global__ void k_examine_finish(AnaArgs A) {
     if (stv.ovf | svar.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
 }
 
+// Object pixel lists: the objects of one raw object are consecutive and
+// share out exactly its pixels, so ordering all pixels by object (raster
+// order inside each object) is a stable partition of every raw object's
+// pixel range by object.  One warp per raw object walks its pixels in order,
+// 32 at a time; lanes holding the same object take consecutive slots from
+// that object's cursor in shared memory.  A raw object that is one object is
+// copied; raw objects of more than OP_KMAX objects are left to
+// k_obj_partition_big (their cursors in dynamic shared memory).
+constexpr int OP_WARPS = 8;
+constexpr int OP_KMAX = 256;
+constexpr int OP_BIG_KMAX = 12288;  // cursors of k_obj_partition_big in shared memory (48 KB)
+constexpr int OP_BIG_GRID = 148;
+
+// one warp: the raw object's pixels in order, 32 at a time, each lane's
+// pixel to the next slot of its object (cursors c[0..K), any memory space)
+__device__ __forceinline__ void obj_partition_walk(const unsigned *__restrict__ rpix,
+                                                   const unsigned *__restrict__ objkey, int off, int P, int K, int ob,
+                                                   const int *__restrict__ ooff, unsigned *__restrict__ opix, int *c) {
+    const int lane = threadIdx.x & 31;
+    for (int k = lane; k < K; k += 32) c[k] = ooff[ob + k];
+    __syncwarp();
+    for (int i0 = 0; i0 < P; i0 += 32) {
+        const int i = i0 + lane;
+        const bool in = i < P;
+        const int key = in ? (int)objkey[off + i] - ob : -1;
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(grp) - 1;
+        const int rank = __popc(grp & ((1u << lane) - 1u));
+        int base = 0;
+        if (in && lane == leader) {
+            base = c[key];
+            c[key] = base + __popc(grp);
+        }
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (in) opix[base + rank] = rpix[off + i];
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(OP_WARPS * 32) k_obj_partition(const unsigned *__restrict__ rpix,
+                                                                 const unsigned *__restrict__ objkey,
+                                                                 const int *__restrict__ roff,
+                                                                 const int *__restrict__ rsize,
+                                                                 const int *__restrict__ rnkept,
+                                                                 const int *__restrict__ objbase,
+                                                                 const int *__restrict__ ooff, int nroots,
+                                                                 unsigned *__restrict__ opix) {
+    __shared__ int cur[OP_WARPS][OP_KMAX];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int r = blockIdx.x * OP_WARPS + wid;
+    if (r >= nroots) return;
+    const int off = roff[r], P = rsize[r], K = rnkept[r], ob = objbase[r];
+    if (K <= 1) {
+        for (int i = lane; i < P; i += 32) opix[off + i] = rpix[off + i];
+        return;
+    }
+    if (K > OP_KMAX) return;
+    obj_partition_walk(rpix, objkey, off, P, K, ob, ooff, opix, cur[wid]);
+}
+
+// raw objects of more than OP_KMAX objects: one warp each, cursors in dynamic
+// shared memory up to OP_BIG_KMAX objects, else in gcur (global)
+__global__ void __launch_bounds__(32) k_obj_partition_big(const unsigned *__restrict__ rpix,
+                                                          const unsigned *__restrict__ objkey,
+                                                          const int *__restrict__ roff, const int *__restrict__ rsize,
+                                                          const int *__restrict__ rnkept,
+                                                          const int *__restrict__ objbase,
+                                                          const int *__restrict__ ooff, int nroots,
+                                                          unsigned *__restrict__ opix, int *gcur) {
+    extern __shared__ int bigcur[];
+    for (int r = blockIdx.x; r < nroots; r += gridDim.x) {
+        const int K = rnkept[r];
+        if (K <= OP_KMAX) continue;
+        const int ob = objbase[r];
+        obj_partition_walk(rpix, objkey, roff[r], rsize[r], K, ob, ooff, opix,
+                           K <= OP_BIG_KMAX ? bigcur : gcur + ob);
+        __syncwarp();
+    }
+}
+
+// gcur: scratch of one int per object
+void launch_obj_partition(const unsigned *rpix, const unsigned *objkey, const RootBufs &R, const int *ooff,
+                          int nroots, unsigned *opix, int *gcur, cudaStream_t st) {
+    if (nroots <= 0) return;
+    k_obj_partition<<<(unsigned)((nroots + OP_WARPS - 1) / OP_WARPS), OP_WARPS * 32, 0, st>>>(
+        rpix, objkey, R.off, R.size, R.nkept, R.objbase, ooff, nroots, opix);
+    k_obj_partition_big<<<(unsigned)std::min(nroots, OP_BIG_GRID), 32, OP_BIG_KMAX * sizeof(int), st>>>(
+        rpix, objkey, R.off, R.size, R.nkept, R.objbase, ooff, nroots, opix, gcur);
+}
+
 void launch_analyse(const AnaArgs &A, cudaStream_t st) {
     if (A.nobj <= 0) return;
     const unsigned grid = (A.nobj + AN_WARPS - 1) / AN_WARPS;

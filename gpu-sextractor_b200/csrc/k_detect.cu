@@ -618,16 +618,24 @@ __global__ void k_ccl_border_ne(int *__restrict__ lab, int w, int h, int *status
     if (lab[p] >= 0 && lab[p - w + 1] >= 0) gunion(lab, p, p - w + 1, status);
 }
 
-__global__ void k_ccl_flatten(int *__restrict__ lab, long long n) {
+// every pixel to its root, and the component sizes: lanes of a warp holding
+// the same root add once to cnt (zeroed before)
+__global__ void k_ccl_flatten(int *__restrict__ lab, long long n, int *__restrict__ cnt) {
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    int l = lab[p];
-    if (l < 0) return;
-    int r = gfind(lab, (int)p);
-    if (r != l) lab[p] = r;
+    int r = -1;
+    if (p < n) {
+        const int l = lab[p];
+        if (l >= 0) {
+            r = gfind(lab, (int)p);
+            if (r != l) lab[p] = r;
+        }
+    }
+    const unsigned same = __match_any_sync(0xffffffffu, r);
+    if (r >= 0 && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&cnt[r], __popc(same));
 }
 
-void launch_ccl(int *lab, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st, int &launches) {
+// cnt: zeroed, w*h ints; receives the size of every component at its root
+void launch_ccl(int *lab, int *cnt, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st, int &launches) {
     dim3 grid((P.w + CC_TW - 1) / CC_TW, (P.h + CC_TH - 1) / CC_TH);
     k_ccl_local<<<grid, dim3(CC_TW, CC_TH), 0, st>>>(lab, P.w, P.h);
     int ntiles = grid.x * grid.y;
@@ -635,7 +643,7 @@ void launch_ccl(int *lab, const FrameParams &P, FrameScalars *d_sc, cudaStream_t
     k_ccl_border<<<ntiles, CC_TW + CC_TH, 0, st>>>(lab, P.w, P.h, status);
     k_ccl_border_ne<<<ntiles, CC_TH, 0, st>>>(lab, P.w, P.h, status);
     long long n = (long long)P.w * P.h;
-    k_ccl_flatten<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(lab, n);
+    k_ccl_flatten<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(lab, n, cnt);
     launches += 4;
 }
 

@@ -11,15 +11,6 @@
 
 namespace sx {
 
-// lanes of a warp holding the same label add once (neighbouring pixels
-// mostly share a component, so this removes most of the atomic traffic)
-__global__ void k_count_labels(const int *__restrict__ lab, int *__restrict__ cnt, long long n) {
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int l = p < n ? lab[p] : -1;
-    const unsigned same = __match_any_sync(0xffffffffu, l);
-    if (l >= 0 && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&cnt[l], __popc(same));
-}
-
 __global__ void k_pos2idx(const unsigned *__restrict__ vals, int *__restrict__ pos2idx, int m) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < m) pos2idx[vals[j]] = j;

@@ -113,7 +113,7 @@ void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const 
                        const FrameParams &P, FrameScalars *d_sc, const float *d_var, const ConvMask &M,
                        cudaStream_t st, int &launches);
 
-void launch_ccl(int *lab, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st, int &launches);
+void launch_ccl(int *lab, int *cnt, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st, int &launches);
 
 struct DebArgs {
     const float *cd, *sub;

@@ -567,13 +567,12 @@ int pipe_detect(sexgpu_ctx *ctx) {
     stage_mark(ctx, "sub_filter", nl);
 
     nl = 0;
-    launch_ccl(P<int>(ctx->lab), Pm, d_sc, st, nl);
+    int *lab = P<int>(ctx->lab), *cnt = P<int>(ctx->cnt), *flag = P<int>(ctx->flag), *pos = P<int>(ctx->pos);
+    CK(cudaMemsetAsync(cnt, 0, N * 4, st));
+    launch_ccl(lab, cnt, Pm, d_sc, st, nl);  // labels to roots, component sizes at the roots
     stage_mark(ctx, "ccl", nl);
 
     // ---- raw objects
-    int *lab = P<int>(ctx->lab), *cnt = P<int>(ctx->cnt), *flag = P<int>(ctx->flag), *pos = P<int>(ctx->pos);
-    CK(cudaMemsetAsync(cnt, 0, N * 4, st));
-    k_count_labels<<<grid1(N, 256), 256, 0, st>>>(lab, cnt, N);
     // per-tile counts of roots and kept pixels, scanned into tile offsets
     // (pos holds the two count arrays and the two offset arrays)
     const int ntile = (int)((N + SCAN_TILE - 1) / SCAN_TILE);
@@ -633,7 +632,7 @@ int pipe_detect(sexgpu_ctx *ctx) {
     unsigned *rpix = P<unsigned>(ctx->rpix);
     CK(cudaMemcpyAsync(rpix, vals, (size_t)nrootpix * 4, cudaMemcpyDeviceToDevice, st));
     k_pos2idx<<<grid1(nrootpix, 256), 256, 0, st>>>(rpix, pos2idx, nrootpix);
-    stage_mark(ctx, "roots", 6 + 2 * scan_launches(ntile) + scan_launches(nroots) + radix_launches(bits_for(nroots), nrootpix));
+    stage_mark(ctx, "roots", 5 + 2 * scan_launches(ntile) + scan_launches(nroots) + radix_launches(bits_for(nroots), nrootpix));
     ps.stage = 2;
     return SEXGPU_OK;
 }
@@ -751,19 +750,17 @@ int pipe_analyse(sexgpu_ctx *ctx) {
     if (ps.stage != 3) return SEXGPU_ERR_ARG;
     cudaStream_t st = ctx->stream;
     const FrameParams &Pm = ps.Pm;
-    const int w = ps.w, h = ps.h, nobj = ps.nobj, nrootpix = ps.nrootpix;
+    const int w = ps.w, h = ps.h, nobj = ps.nobj;
     const DebArgs &A = ps.A;
     const BackBufs &B = ps.B;
     FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
     int *tmp = P<int>(ctx->scan_tmp);
-    unsigned *keys = P<unsigned>(ctx->keys), *vals = P<unsigned>(ctx->vals);
+    unsigned *vals = P<unsigned>(ctx->vals);
     unsigned *rpix = P<unsigned>(ctx->rpix);
     // ---- object pixel lists (stable by object id: raster order inside)
     ObjBufs &O = ctx->O;
-    CK(cudaMemcpyAsync(keys, A.objkey, (size_t)nrootpix * 4, cudaMemcpyDeviceToDevice, st));
-    CK(cudaMemcpyAsync(vals, rpix, (size_t)nrootpix * 4, cudaMemcpyDeviceToDevice, st));
-    radix_sort_pairs(keys, vals, P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), nrootpix, bits_for(nobj), tmp, st);
     exclusive_scan(O.n, O.off, nobj, nullptr, tmp, st);
+    launch_obj_partition(rpix, A.objkey, ps.R, O.off, ps.nroots, vals, P<int>(ctx->kalt), st);
     AnaArgs AA;
     EN(o_raw, (size_t)(nobj + 1) * sizeof(RobustRaw));
     AA.raw = P<RobustRaw>(ctx->o_raw);
@@ -792,7 +789,7 @@ int pipe_analyse(sexgpu_ctx *ctx) {
     AA.afac = Pm.analysis_thresh;
     AA.bp_thick = Pm.bp_thick;
     launch_analyse(AA, st);
-    stage_mark(ctx, "analyse", 4 + (Pm.bp_local ? 2 : 0) + radix_launches(bits_for(nobj), nrootpix) + scan_launches(nobj));
+    stage_mark(ctx, "analyse", 6 + (Pm.bp_local ? 2 : 0) + scan_launches(nobj));
     ps.stage = 4;
     return SEXGPU_OK;
 }
