@@ -500,21 +500,32 @@ __device__ __forceinline__ void obj_partition_walk(const unsigned *__restrict__ 
     const int lane = threadIdx.x & 31;
     for (int k = lane; k < K; k += 32) c[k] = ooff[ob + k];
     __syncwarp();
-    for (int i0 = 0; i0 < P; i0 += 32) {
-        const int i = i0 + lane;
-        const bool in = i < P;
-        const int key = in ? (int)objkey[off + i] - ob : -1;
-        const unsigned grp = __match_any_sync(0xffffffffu, key);
-        const int leader = __ffs(grp) - 1;
-        const int rank = __popc(grp & ((1u << lane) - 1u));
-        int base = 0;
-        if (in && lane == leader) {
-            base = c[key];
-            c[key] = base + __popc(grp);
+    // OP_AHEAD chunks of 32 pixels per step: their loads are issued together,
+    // then the chunks take their slots in order
+    constexpr int OP_AHEAD = 4;
+    for (int i0 = 0; i0 < P; i0 += 32 * OP_AHEAD) {
+        int key[OP_AHEAD];
+        unsigned px[OP_AHEAD];
+#pragma unroll
+        for (int a = 0; a < OP_AHEAD; a++) {
+            const int i = i0 + a * 32 + lane;
+            key[a] = i < P ? (int)objkey[off + i] - ob : -1;
+            px[a] = i < P ? rpix[off + i] : 0u;
         }
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (in) opix[base + rank] = rpix[off + i];
-        __syncwarp();
+#pragma unroll
+        for (int a = 0; a < OP_AHEAD; a++) {
+            const unsigned grp = __match_any_sync(0xffffffffu, key[a]);
+            const int leader = __ffs(grp) - 1;
+            const int rank = __popc(grp & ((1u << lane) - 1u));
+            int base = 0;
+            if (key[a] >= 0 && lane == leader) {
+                base = c[key[a]];
+                c[key[a]] = base + __popc(grp);
+            }
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (key[a] >= 0) opix[base + rank] = px[a];
+            __syncwarp();
+        }
     }
 }
 
@@ -532,6 +543,7 @@ __global__ void __launch_bounds__(OP_WARPS * 32) k_obj_partition(const unsigned 
     if (r >= nroots) return;
     const int off = roff[r], P = rsize[r], K = rnkept[r], ob = objbase[r];
     if (K <= 1) {
+#pragma unroll 4
         for (int i = lane; i < P; i += 32) opix[off + i] = rpix[off + i];
         return;
     }
