@@ -221,7 +221,10 @@ def run_gpu(args):
     achieved = algo / (dom[2] / 1e3) / 1e9 if dom[2] > 0 else 0.0
     roofline = {"bound": "hbm", "kernel": dom[0], "achieved": round(achieved, 1), "peak": peak,
                 "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": None, "algorithmic_bytes": algo,
+                "traffic": NCU_TRAFFIC.get(dom[0]) if (w, h) == (4096, 4096) else None,
+                "traffic_source": "ncu launch list of prof_case.py --workload c1 (dram__bytes_read.sum + "
+                                  "dram__bytes_write.sum over the stage's launches, one frame)",
+                "algorithmic_bytes": algo,
                 "stage_ms": {s[0]: round(s[2], 4) for s in stages}}
     # algorithmic bytes of a frame (24N pixel stages + 8 B per pixel and
     # deblending level + 16 B per object pixel + 64 B per catalogue row)
@@ -356,6 +359,14 @@ def run_batch(ctx, frames, reps=5, workers=8, maxobj=400000):
             "objects_ratio": round(t_plain / t_batch, 3), "identical_catalogues": bool(identical),
             "host": host_state(frames),
             **({"differing": differing} if differing else {})}
+
+
+# DRAM bytes (read + write) per c1 frame of each stage's launches, from one
+# ncu launch-list capture of prof_case.py --workload c1 (its summary is kept
+# under profiles/)
+NCU_TRAFFIC = {"background": 134_600_000, "sub_filter": 207_900_000, "ccl": 275_300_000, "roots": 663_000_000,
+               "deblend": 967_700_000, "analyse": 391_200_000, "clean": 14_900_000, "endobject": 200_100_000,
+               "catalog": 24_600_000}
 
 
 def algorithmic_bytes(stage, N, s):
