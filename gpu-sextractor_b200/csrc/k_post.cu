@@ -209,7 +209,10 @@ __global__ void k_alloc_victims(ObjBufs O, const unsigned *opix, int *alloc, int
 // ---------------------------------------------------------------------------
 // photometry and FLAGS of the survivors
 // ---------------------------------------------------------------------------
+struct EndRaw;
+
 struct EndArgs {
+    EndRaw *raw;    // per-object scratch between the photometry warps and k_end_finish
     const float *sub;
     const int *alloc;
     ObjBufs O;
@@ -346,6 +349,13 @@ __device__ __forceinline__ int wsum(int v) {
 struct KronAcc {
     XSum s0, s1;  // pass 1: r*pix, pix;  pass 2: pix, variance
     int area, areab;
+};
+
+// what the photometry warps hand to k_end_finish (one thread per object)
+struct EndRaw {
+    KronAcc p2;     // pass-2 (AUTO) sums, when have2
+    float kron;
+    int flags, have2;
 };
 
 __device__ __forceinline__ void kacc_init(KronAcc &c) {
@@ -527,6 +537,25 @@ __device__ bool kron_defer(const EndArgs &A, int pass, int o, int flags, float k
 // catalogue columns of a survivor (lane 0 writes); p2 = pass-2 sums if any
 __device__ void end_finish(const EndArgs &A, int o, int flags, float kron, bool have2, const KronAcc &p2) {
     if ((threadIdx.x & 31) != 0) return;
+    EndRaw R;
+    R.p2 = p2;
+    R.kron = kron;
+    R.flags = flags;
+    R.have2 = have2;
+    A.raw[o] = R;
+}
+
+// catalogue columns of a survivor from its photometry sums: AUTO, ISOCOR and
+// ISO fluxes, magnitudes and errors, FLAGS (one thread per object, so that
+// this double-precision tail does not run on one lane of a warp)
+__global__ void k_end_finish(EndArgs A) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= A.n || A.O.fmaster[o] >= 0) return;
+    const EndRaw R = A.raw[o];
+    const KronAcc &p2 = R.p2;
+    const bool have2 = R.have2 != 0;
+    int flags = R.flags;
+    float kron = R.kron;
     const float backsig = A.sc->backsig;
     const double var = backsig * backsig;
     double tv, sigtv;
@@ -702,7 +731,8 @@ void launch_endobject(const EndArgs &E, int nobj, cudaStream_t st, int &launches
     k_kron_merge<1><<<KR_GRID / 2, 128, 0, st>>>(E);
     k_kron_chunks<2><<<KR_GRID, KR_THREADS, 0, st>>>(E);
     k_kron_merge<2><<<KR_GRID / 2, 128, 0, st>>>(E);
-    launches += 5;
+    k_end_finish<<<(unsigned)((nobj + 127) / 128), 128, 0, st>>>(E);
+    launches += 6;
     if (E.nnw) {
         k_class_star<<<(unsigned)((nobj + 127) / 128), 128, 0, st>>>(E.O, nobj, E.nnw, E.seeing, E.pixscale);
         launches += 1;

@@ -95,7 +95,7 @@ struct sexgpu_ctx {
         skeys, svals, skalt, svalt, rows;
     DevBuf kitem[2], kchunk[2], kpart[2];  // queued Kron boxes
     DevBuf o_sprob;                        // CLASS_STAR per object
-    DevBuf o_raw, o_xraw;                  // robust preanalysis / examineiso scratch per object
+    DevBuf o_raw, o_xraw, o_eraw;          // robust preanalysis / examineiso / photometry scratch per object
     DevBuf o_dbkg, o_lstat;                // BACKPHOTO_TYPE LOCAL: annulus mode, annulus statistics
     bool cfg_local = false;                // the current extraction uses LOCAL photometry background
     DevBuf fitsraw;                        // FITS data block as stored (sexgpu_extract_fits)
@@ -871,6 +871,8 @@ int pipe_end(sexgpu_ctx *ctx) {
     int rc = SEXGPU_OK;
     // ---- photometry / FLAGS
     EndArgs E;
+    EN(o_eraw, (size_t)(nobj + 1) * sizeof(EndRaw));
+    E.raw = P<EndRaw>(ctx->o_eraw);
     E.sub = A.sub;
     E.alloc = A.alloc;
     E.O = O;
@@ -918,13 +920,16 @@ int pipe_end(sexgpu_ctx *ctx) {
     const int ns = ctx->hsc.nsurv;
     k_surv_compact<<<grid1(nobj + 1, 256), 256, 0, st>>>(O, R.ymax, R.lastx, sflag, nobj, w, Pm.numbering,
                                                          P<unsigned>(ctx->skeys), P<unsigned>(ctx->svals));
+    // completion keys are below w*h; first-pixel numbering has all keys 0
+    // (the survivors are already in index order)
+    const int cbits = Pm.numbering == 0 ? bits_for((long long)w * h - 1) : 0;
     radix_sort_pairs(P<unsigned>(ctx->skeys), P<unsigned>(ctx->svals), P<unsigned>(ctx->skalt),
-                     P<unsigned>(ctx->svalt), ns, bits_for((long long)w * h), tmp, st);
+                     P<unsigned>(ctx->svalt), ns, cbits, tmp, st);
     k_number<<<grid1(ns + 1, 256), 256, 0, st>>>(O, P<unsigned>(ctx->svals), ns);
     EN(rows, (size_t)(ns + 1) * sizeof(sexgpu_object));
     k_write_rows<<<grid1(ns + 1, 128), 128, 0, st>>>(O, P<unsigned>(ctx->svals), ns, ctx->hsc.dthresh,
                                                      ctx->hsc.thresh, P<sexgpu_object>(ctx->rows));
-    stage_mark(ctx, "catalog", 5 + scan_launches(nobj) + radix_launches(bits_for((long long)w * h), ns));
+    stage_mark(ctx, "catalog", 5 + scan_launches(nobj) + radix_launches(cbits, ns));
     CK(cudaGetLastError());
     rc = read_scalars(ctx);
     if (rc) return rc;
@@ -1037,6 +1042,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     free_buf(ctx->o_sprob);
     free_buf(ctx->o_raw);
     free_buf(ctx->o_xraw);
+    free_buf(ctx->o_eraw);
     free_buf(ctx->o_dbkg);
     free_buf(ctx->o_lstat);
     free_buf(ctx->fitsraw);
