@@ -496,6 +496,18 @@ def _oracle_worker(args):
     return time.perf_counter() - t
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or None."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline(frame, cfg):
     """The oracle (single-threaded C restatement of the path) on one frame."""
     from oracle import oracle as O
@@ -504,7 +516,7 @@ def cpu_baseline(frame, cfg):
     dt = time.perf_counter() - t
     return {"value": round(1.0 / dt, 4), "unit": "frames/s", "cores": 1, "kind": "port",
             "sample": "one 4096x4096 frame of the workload, single thread (%d objects)" % len(objs),
-            "seconds": round(dt, 3)}
+            "seconds": round(dt, 3), "cpu_model": cpu_model(), "nproc": os.cpu_count()}
 
 
 def run_reference(args):
@@ -531,7 +543,8 @@ def run_reference(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "parallelism": "%d processes, one frame each per step" % ncpu},
             "cpu_baseline": {"value": round(fps, 4), "unit": "frames/s", "cores": ncpu, "kind": "port",
-                             "sample": "%d frames per step (one per worker), 4096x4096 each" % ncpu},
+                             "sample": "%d frames per step (one per worker), 4096x4096 each" % ncpu,
+                             "cpu_model": cpu_model(), "nproc": os.cpu_count()},
             "e2e": {"value": round(fps, 4), "unit": "frames/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
