@@ -136,6 +136,37 @@ def test_cli_fits_ldac_with_weight_map(tmp_path, masks):
     assert np.allclose(t["CLASS_STAR"], o["class_star"], rtol=0, atol=1e-6) and o["class_star"].std() > 0
 
 
+def test_cli_local_background(tmp_path, masks):
+    """BACKPHOTO_TYPE LOCAL / BACKPHOTO_THICK: the fluxes, BACKGROUND and
+    THRESHOLD of the FITS_LDAC catalogue against the oracle with the same
+    annulus."""
+    if not os.path.exists(SEX):
+        subprocess.check_call(["make", "-s", "-C", os.path.dirname(SEX)])
+    img = synth.frame_c0(seed=8, w=400, h=320, nsrc=300)
+    fits = tmp_path / "img.fits"
+    write_fits(str(fits), img)
+    conv = tmp_path / "g.conv"
+    m = masks["gauss_2.5_5x5"]
+    conv.write_text("CONV NONORM\n" + "\n".join(" ".join("%.9g" % v for v in row) for row in m) + "\n")
+    par = tmp_path / "t.param"
+    par.write_text("NUMBER\nFLUX_ISO\nFLUX_AUTO\nFLUX_APER(1)\nBACKGROUND\nTHRESHOLD\nFLUX_MAX\n")
+    cfgf = tmp_path / "t.sex"
+    cfgf.write_text("CATALOG_TYPE FITS_LDAC\nFILTER_NAME %s\nPARAMETERS_NAME %s\nBACKPHOTO_TYPE LOCAL\n"
+                    "BACKPHOTO_THICK 12\n" % (conv, par))
+    cat = tmp_path / "t.ldac"
+    subprocess.check_call([SEX, str(fits), "-c", str(cfgf), "-CATALOG_NAME", str(cat), "-VERBOSE_TYPE", "QUIET"],
+                          cwd=str(tmp_path))
+    t = read_ldac_objects(str(cat))
+    o, _, _ = O.extract(img, conv=m, back_photo_type=1, back_photo_thick=12)
+    g, _, _ = O.extract(img, conv=m)
+    assert len(t) == len(o) == len(g) > 0
+    assert (o["bkg"] != g["bkg"]).any()   # the annulus mode moved some backgrounds
+    assert np.array_equal(t["NUMBER"], o["number"])
+    for col, name in [("FLUX_ISO", "flux_iso"), ("FLUX_AUTO", "flux_auto"), ("FLUX_APER", "flux_aper"),
+                      ("BACKGROUND", "bkg"), ("THRESHOLD", "thresh"), ("FLUX_MAX", "peak")]:
+        assert np.array_equal(t[col], o[name]), col
+
+
 def test_cli_background_rms_check_image(tmp_path, masks):
     if not os.path.exists(SEX):
         subprocess.check_call(["make", "-s", "-C", os.path.dirname(SEX)])
