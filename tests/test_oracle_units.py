@@ -72,3 +72,31 @@ def test_deblended_objects_partition_their_roots():
     order = np.argsort(objs["number"])
     assert np.array_equal(counts, objs["fdnpix"][order])
     assert set(np.unique(objs["level"])) >= {0}
+
+
+def test_local_background_shifts_isophotal_photometry():
+    """BACKPHOTO_TYPE LOCAL in the oracle: the detection is unchanged; where a
+    local mode was measured, BACKGROUND moves by it, THRESHOLD and FLUX_MAX
+    drop by it and the isophotal flux drops by the float product
+    fdnpix * dbkg (src/back.c:568 localback, analyse.c examineiso).  CLEAN
+    off, so that every catalogue box is the box the annulus was built on."""
+    img = synth.frame_c0(seed=12, w=300, h=260, nsrc=200)
+    g, gseg, _ = O.extract(img, clean_flag=0)
+    o, oseg, _ = O.extract(img, clean_flag=0, back_photo_type=1, back_photo_thick=10)
+    assert np.array_equal(gseg, oseg) and len(g) == len(o) > 0
+    for name in ("number", "npix", "mx", "my", "flags", "fdnpix"):
+        assert np.array_equal(g[name], o[name]), name
+    d = (o["bkg"] - g["bkg"]).astype(np.float32)
+    moved = o["bkg"] != g["bkg"]
+    assert moved.sum() > len(o) // 2
+    # with a measured mode dbkg: bkg + dbkg (float), thresh - dbkg, peak - dbkg
+    dbkg = O.localback(O.background(img)[0], np.stack([o["xmin"], o["xmax"], o["ymin"], o["ymax"]], 1), 10)
+    assert np.array_equal(o["bkg"][moved], (g["bkg"] + dbkg)[moved])
+    assert np.array_equal(o["thresh"], (g["thresh"] - dbkg).astype(np.float32))
+    assert np.array_equal(o["peak"], (g["peak"] - dbkg).astype(np.float32))
+    # the catalogue holds float fluxes rounded from the exact double sums, so
+    # the global flux minus the float product matches to float rounding
+    flux = g["flux"].astype(np.float64) - (o["fdnpix"].astype(np.float32) * dbkg).astype(np.float64)
+    assert np.allclose(o["flux"], flux, rtol=1e-6, atol=1e-3)
+    assert not np.allclose(o["flux"][moved], g["flux"][moved], rtol=1e-6, atol=1e-3)
+    assert np.all(np.abs(d[moved]) > 0)
