@@ -370,7 +370,10 @@ NCU_TRAFFIC = {"background": 134_600_000, "sub_filter": 207_900_000, "ccl": 275_
 
 
 def algorithmic_bytes(stage, N, s):
-    """Compulsory bytes of one launch set of a stage."""
+    """Compulsory bytes of one launch set of a stage: the frame read by the
+    background; frame in, subtracted and filtered frames and label seeds out
+    for sub_filter; labels read and written by the CCL; 8 bytes (pixel index
+    and filtered value) per pixel and deblending level."""
     if stage == "background":
         return 4 * N                       # frame read once
     if stage == "sub_filter":

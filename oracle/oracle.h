@@ -63,7 +63,7 @@ typedef struct {
     int     deblend_nthresh;    /* DEBLEND_NTHRESH */
     double  deblend_mincont;    /* DEBLEND_MINCONT */
     /* cleaning */
-    int     clean_flag;         /* CLEAN */
+    int     clean_flag;         /* CLEAN: 1 on; 0 off; 2 off, with the CLEAN inputs (mthresh) measured */
     double  clean_param;        /* CLEAN_PARAM */
     /* photometry */
     double  satur_level;        /* SATUR_LEVEL */
@@ -162,6 +162,33 @@ int orc_background_rms(const float *img, int w, int h, const orc_config *cfg, fl
 /* src/back.c:568 localback for objects given by their boxes (4 ints each:
    xmin, xmax, ymin, ymax) over a background-subtracted frame: dbkg per object */
 void orc_localback(const float *sub, int w, int h, int thick, const int *box, int nobj, float *dbkg);
+
+/* Unit-level entry points (compared with the reference's own photom.c,
+ * clean.c and neurro.c by the tests). */
+typedef struct {
+    double  mx, my;                       /* in: position (0-based pixels) */
+    float   a, b, cxx, cyy, cxy, dbkg;    /* in: shape, local background */
+    float   flux_aper, fluxerr_aper, mag_aper, magerr_aper;   /* out */
+    float   kron, flux_auto, fluxerr_auto, mag_auto, magerr_auto;
+    int32_t flags;                        /* out: CROWDED, APERT_PB */
+} orc_phot_obj;
+/* aperture (PHOT_APERTURES) and AUTO photometry over a background-subtracted
+ * frame holding no other object */
+int orc_photometry(const float *sub, int w, int h, const orc_config *cfg, float backsig, orc_phot_obj *o, int n);
+/* FLUX_ISOCOR / FLUXERR_ISOCOR (src/photom.c:719) */
+void orc_isocor(float flux, float fluxerr, int fdnpix, float dthresh, float *flux_isocor, float *fluxerr_isocor);
+/* star/galaxy network response to net->nn[0] inputs (src/neurro.c:57) */
+double orc_nnw_response(const orc_nnw *net, const double *input);
+typedef struct {
+    double  mx, my;
+    float   a, b, cxx, cyy, cxy, abcor, dthresh, mthresh;
+    /* merged by CLEAN into the survivor (src/clean.c:234-287) */
+    int32_t fdnpix, dnpix;
+    float   fdflux, dflux, flux, fluxerr, fdpeak, dpeak, peak;
+    int32_t peakx, peaky, xmin, xmax, ymin, ymax, flags;
+    int32_t master;                       /* out: -1 survivor, else its survivor */
+} orc_clean_obj;
+int orc_clean_objects(orc_clean_obj *o, int n, int w, int h, double clean_param);
 
 /* Small helpers exposed for unit tests. */
 float   orc_hmedian(float *ra, int n);

@@ -1,7 +1,9 @@
 """ctypes binding of the CPU oracle (TEST INFRASTRUCTURE ONLY).
 
 Loads oracle/liboracle.so (the restatement) and, when it has been built,
-oracle/_ref/libsexref.so (the reference's own background/filter code).
+oracle/_ref/libsexref.so (the reference's own CPU code: background, filter,
+CLEAN, photometry, the star/galaxy network and the FITS pixel reader,
+compiled unmodified and driven by refharness.c / refmeasure.c).
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this.
 """
 import ctypes as C
@@ -91,10 +93,21 @@ _lib = None
 _ref = None
 
 
+def ref_src():
+    """The reference source directory oracle/Makefile reads (REFSRC), or
+    None when that tree is not present on this machine."""
+    try:
+        out = subprocess.run(["make", "-s", "-C", HERE, "print-refsrc"], capture_output=True, text=True,
+                             env=dict(os.environ)).stdout.strip()
+    except OSError:
+        return None
+    return out if out and os.path.isdir(out) else None
+
+
 def build(ref=True):
     subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
-    if ref and os.path.isdir(os.environ.get("REFSRC", "/root/reference/src")):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+    if ref:
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref-if-present"])
 
 
 def lib():
@@ -328,3 +341,176 @@ def fits_to_float(raw, bitpix, bscale=1.0, bzero=0.0, blank=None):
             out = (v.astype(np.float64) * np.float64(bs) + np.float64(bz)).astype(np.float32)
         out[~np.isfinite(v)] = np.float32(-1e30)
     return out.astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# Unit-level comparisons of the restatement with the reference's own
+# photom.c, clean.c, neurro.c and fits/fitsbody.c.
+
+class PhotObj(C.Structure):
+    """orc_phot_obj / ref_phot_obj (same layout)."""
+    _fields_ = [("mx", C.c_double), ("my", C.c_double),
+                ("a", C.c_float), ("b", C.c_float), ("cxx", C.c_float), ("cyy", C.c_float), ("cxy", C.c_float),
+                ("dbkg", C.c_float),
+                ("flux_aper", C.c_float), ("fluxerr_aper", C.c_float), ("mag_aper", C.c_float),
+                ("magerr_aper", C.c_float),
+                ("kron", C.c_float), ("flux_auto", C.c_float), ("fluxerr_auto", C.c_float),
+                ("mag_auto", C.c_float), ("magerr_auto", C.c_float), ("flags", C.c_int32)]
+
+
+PHOT_IN = ("mx", "my", "a", "b", "cxx", "cyy", "cxy", "dbkg")
+PHOT_OUT = ("flux_aper", "fluxerr_aper", "mag_aper", "magerr_aper", "kron", "flux_auto", "fluxerr_auto",
+            "mag_auto", "magerr_auto", "flags")
+
+
+def _phot_array(objs):
+    arr = (PhotObj * len(objs))()
+    for i, o in enumerate(objs):
+        for k in PHOT_IN:
+            setattr(arr[i], k, o[k])
+    return arr
+
+
+def _phot_out(arr):
+    return [{k: getattr(a, k) for k in PHOT_OUT} for a in arr]
+
+
+def photometry(sub, objs, backsig, phot_aperture=5.0, phot_autoparams=(2.5, 3.5), mask_type=2, gain=0.0,
+               mag_zeropoint=0.0):
+    """Aperture and AUTO photometry of objects (dicts of PHOT_IN) over a
+    background-subtracted frame holding no other object (the restatement)."""
+    sub = np.ascontiguousarray(sub, np.float32)
+    h, w = sub.shape
+    cfg = make_config(phot_aperture=phot_aperture, phot_autoparams=phot_autoparams, mask_type=mask_type,
+                      gain=gain, mag_zeropoint=mag_zeropoint)
+    arr = _phot_array(objs)
+    lib().orc_photometry(_f(sub), w, h, C.byref(cfg), C.c_float(backsig), arr, len(objs))
+    return _phot_out(arr)
+
+
+def ref_photometry(sub, objs, backsig, phot_aperture=5.0, phot_autoparams=(2.5, 3.5), mask_type=2, gain=0.0,
+                   mag_zeropoint=0.0):
+    """The same through the reference's computeaperflux()/computeautoflux()
+    (None if oracle/_ref is not built)."""
+    r = ref()
+    if r is None:
+        return None
+    sub = np.ascontiguousarray(sub, np.float32).copy()
+    h, w = sub.shape
+    arr = _phot_array(objs)
+    r.ref_photometry(_f(sub), w, h, C.c_double(phot_aperture), C.c_double(phot_autoparams[0]),
+                     C.c_double(phot_autoparams[1]), mask_type, C.c_double(gain), C.c_double(mag_zeropoint),
+                     C.c_float(backsig), arr, len(objs))
+    return _phot_out(arr)
+
+
+def isocor(flux, fluxerr, fdnpix, dthresh):
+    """FLUX_ISOCOR, FLUXERR_ISOCOR per object (restatement)."""
+    n = len(flux)
+    fi, fe = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    for i in range(n):
+        a, b = C.c_float(), C.c_float()
+        lib().orc_isocor(C.c_float(flux[i]), C.c_float(fluxerr[i]), int(fdnpix[i]), C.c_float(dthresh[i]),
+                         C.byref(a), C.byref(b))
+        fi[i], fe[i] = a.value, b.value
+    return fi, fe
+
+
+def ref_isocor(flux, fluxerr, fdnpix, dthresh):
+    """The same through the reference's computeisocorflux()."""
+    r = ref()
+    if r is None:
+        return None
+    f = np.ascontiguousarray(flux, np.float32)
+    e = np.ascontiguousarray(fluxerr, np.float32)
+    d = np.ascontiguousarray(dthresh, np.float32)
+    k = np.ascontiguousarray(fdnpix, np.int32)
+    n = len(f)
+    fi, fe = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    r.ref_isocor(_f(f), _f(e), k.ctypes.data_as(C.POINTER(C.c_int)), _f(d), n, _f(fi), _f(fe))
+    return fi, fe
+
+
+def nnw_response(net, inputs):
+    """First output of the network for each row of inputs (restatement)."""
+    lib().orc_nnw_response.restype = C.c_double
+    x = np.ascontiguousarray(inputs, np.float64)
+    return np.array([lib().orc_nnw_response(C.byref(net), row.ctypes.data_as(C.POINTER(C.c_double)))
+                     for row in x])
+
+
+def ref_neurresp(path, inputs):
+    """The reference's getnnw() + neurresp() on each row (None if not built);
+    returns (outputs, neurons per layer)."""
+    r = ref()
+    if r is None:
+        return None
+    x = np.ascontiguousarray(inputs, np.float64)
+    out = np.zeros(len(x), np.float64)
+    nn = np.zeros(3, np.int32)
+    r.ref_neurresp(path.encode(), x.ctypes.data_as(C.POINTER(C.c_double)), len(x),
+                   out.ctypes.data_as(C.POINTER(C.c_double)), nn.ctypes.data_as(C.POINTER(C.c_int)))
+    return out, nn
+
+
+class CleanObj(C.Structure):
+    """orc_clean_obj / ref_clean_obj (same layout)."""
+    _fields_ = [("mx", C.c_double), ("my", C.c_double)] + \
+        [(k, C.c_float) for k in ("a", "b", "cxx", "cyy", "cxy", "abcor", "dthresh", "mthresh")] + \
+        [("fdnpix", C.c_int32), ("dnpix", C.c_int32)] + \
+        [(k, C.c_float) for k in ("fdflux", "dflux", "flux", "fluxerr", "fdpeak", "dpeak", "peak")] + \
+        [(k, C.c_int32) for k in ("peakx", "peaky", "xmin", "xmax", "ymin", "ymax", "flags", "master")]
+
+
+CLEAN_FIELDS = [f[0] for f in CleanObj._fields_ if f[0] != "master"]
+
+
+def _clean_array(objs):
+    arr = (CleanObj * len(objs))()
+    for i, o in enumerate(objs):
+        for k in CLEAN_FIELDS:
+            setattr(arr[i], k, o[k])
+        arr[i].master = -1
+    return arr
+
+
+def clean_objects(objs, w, h, clean_param=1.0):
+    """CLEAN of objects (dicts of CLEAN_FIELDS, object-index order) by the
+    restatement: (master per object, -1 for survivors; merged rows)."""
+    arr = _clean_array(objs)
+    lib().orc_clean_objects(arr, len(objs), w, h, C.c_double(clean_param))
+    return np.array([a.master for a in arr]), [{k: getattr(a, k) for k in CLEAN_FIELDS} for a in arr]
+
+
+def ref_clean(objs, clean_param=1.0):
+    """The reference's sequential clean()/addcleanobj() over the same objects
+    in the same order: (survive flags, rows with the survivors' merged
+    attributes), or None if oracle/_ref is not built."""
+    r = ref()
+    if r is None:
+        return None
+    arr = _clean_array(objs)
+    surv = np.zeros(len(objs), np.int32)
+    r.ref_clean(arr, len(objs), C.c_double(clean_param), surv.ctypes.data_as(C.POINTER(C.c_int)))
+    return surv.astype(bool), [{k: getattr(a, k) for k in CLEAN_FIELDS} for a in arr]
+
+
+def ref_read_body(raw, bitpix, bscale=1.0, bzero=0.0, blank=None, bitsgn=1):
+    """The reference's read_body() on a FITS data block (big-endian bytes as
+    stored), through a temporary file; bitsgn as the header's BITSGN (the
+    reference's header reader defaults it to 1).  None if not built."""
+    import tempfile
+    r = ref()
+    if r is None:
+        return None
+    raw = bytes(raw)
+    n = len(raw) // (abs(bitpix) // 8)
+    out = np.zeros(n, np.float32)
+    with tempfile.NamedTemporaryFile(suffix=".raw") as f:
+        f.write(raw)
+        f.flush()
+        rc = r.ref_read_body(f.name.encode(), bitpix, C.c_double(bscale), C.c_double(bzero),
+                             1 if blank is not None else 0, int(blank or 0), bitsgn, C.c_size_t(n), _f(out))
+    if rc != 0:
+        raise RuntimeError("ref_read_body failed")
+    return out

@@ -1059,19 +1059,13 @@ static void autoflux(const frame_t *F, const int *alloc, obj_t *o, int self)
 /* endobject, src/cuda/cudaanalyse.cu:2604-2900 (the parts that feed the catalog) */
 /* CLASS_STAR: src/cuda/cudaanalyse.cu:2901-2920 (inputs) and :599-632 /
    src/neurro.c neurresp (response, logistic units, double arithmetic) */
-static float class_star(const orc_config *cfg, const obj_t *o)
+/* src/neurro.c:57-78 (neurresp): the network's layers in double with
+ * logistic units (src/neurro.c:85-89); in[] holds nn[0] inputs and is
+ * overwritten; returns the first output */
+static double nnw_response(const orc_nnw *net, double *in)
 {
-    const orc_nnw *net = cfg->nnw;
-    double in[ORC_NNW_NEURONS], nx[ORC_NNW_NEURONS], fac2, fwhm = cfg->seeing_fwhm;
-    double pixscale = cfg->pixel_scale > 0.0 ? cfg->pixel_scale : 1.0;
-    int i, j = 0, k, l, last = net->nlayers - 1;
-    fac2 = fwhm / pixscale;
-    fac2 *= fac2;
-    in[j] = log10(o->iso[0] ? o->iso[0] / fac2 : 0.01);
-    in[++j] = o->athr > 0.0 ? log10(o->peak > 0.0 ? o->peak / o->athr : 0.1) : -1.0;
-    for (i = 1; i < ORC_NISO; i++)
-        in[++j] = log10(o->iso[i] ? o->iso[i] / fac2 : 0.01);
-    in[++j] = log10(fwhm);
+    double nx[ORC_NNW_NEURONS];
+    int i, k, l, last = net->nlayers - 1;
     for (i = 0; i < net->nn[0]; i++)
         in[i] = in[i] * net->inscale[i] + net->inbias[i];
     for (l = 0; l < last; l++) {
@@ -1084,19 +1078,29 @@ static float class_star(const orc_config *cfg, const obj_t *o)
         for (k = 0; k < net->nn[l + 1]; k++)
             in[k] = nx[k];
     }
-    return (float)((in[0] - net->outbias[0]) / net->outscale[0]);
+    return (in[0] - net->outbias[0]) / net->outscale[0];
 }
 
-static void endobject(const frame_t *F, const int *alloc, obj_t *o, int self)
+static float class_star(const orc_config *cfg, const obj_t *o)
 {
-    const orc_config *cfg = F->cfg;
-    double ati;
-    o->elong = o->a / o->b;
-    o->ellip = 1 - o->b / o->a;
-    o->polar = (o->a * o->a - o->b * o->b) / (o->a * o->a + o->b * o->b);
-    o->fluxerr_iso = sqrt(o->fluxerr);
-    /* computeisocorflux, :62-98 */
-    ati = (o->flux > 0.0) ? (o->fdnpix * o->dthr / o->flux) : 0.0;
+    const orc_nnw *net = cfg->nnw;
+    double in[ORC_NNW_NEURONS], fac2, fwhm = cfg->seeing_fwhm;
+    double pixscale = cfg->pixel_scale > 0.0 ? cfg->pixel_scale : 1.0;
+    int i, j = 0;
+    fac2 = fwhm / pixscale;
+    fac2 *= fac2;
+    in[j] = log10(o->iso[0] ? o->iso[0] / fac2 : 0.01);
+    in[++j] = o->athr > 0.0 ? log10(o->peak > 0.0 ? o->peak / o->athr : 0.1) : -1.0;
+    for (i = 1; i < ORC_NISO; i++)
+        in[++j] = log10(o->iso[i] ? o->iso[i] / fac2 : 0.01);
+    in[++j] = log10(fwhm);
+    return (float)nnw_response(net, in);
+}
+
+/* computeisocorflux, src/cuda/cudaanalyse.cu:62-98 (src/photom.c:719) */
+static void isocorflux(obj_t *o)
+{
+    double ati = (o->flux > 0.0) ? (o->fdnpix * o->dthr / o->flux) : 0.0;
     if (ati > 1.0)
         ati = 1.0;
     else if (ati < 0.0)
@@ -1110,6 +1114,16 @@ static void endobject(const frame_t *F, const int *alloc, obj_t *o, int self)
         o->fluxerr_isocor = sqrt(sigtv + dati * dati) * o->flux;
     } else
         o->fluxerr_isocor = sqrt(o->fluxerr);
+}
+
+static void endobject(const frame_t *F, const int *alloc, obj_t *o, int self)
+{
+    const orc_config *cfg = F->cfg;
+    o->elong = o->a / o->b;
+    o->ellip = 1 - o->b / o->a;
+    o->polar = (o->a * o->a - o->b * o->b) / (o->a * o->a + o->b * o->b);
+    o->fluxerr_iso = sqrt(o->fluxerr);
+    isocorflux(o);
     aperflux(F, alloc, o, self);
     autoflux(F, alloc, o, self);
     if (o->peak + o->bkg >= cfg->satur_level)
@@ -1366,7 +1380,7 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
         o->master = o->final_master = -1;
         examineiso(&F, o);
     }
-    if (cfg->clean_flag)
+    if (cfg->clean_flag == 1)
         run_clean(&F, objs, nobj);
 
     /* allocation map: object (after CLEAN merges) or OTHER for above
@@ -1514,4 +1528,149 @@ double orc_xsum_floats(const float *v, int n, int e0)
     for (i = 0; i < n; i++)
         xs_add(&s, v[i]);
     return xs_double(&s);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Unit-level entry points.  The tests compare them with the reference's own
+ * src/photom.c, src/clean.c and src/neurro.c compiled unmodified
+ * (oracle/_ref). */
+
+/* Aperture and AUTO photometry (aperflux, autoflux above) of objects given
+ * by their position and shape over a background-subtracted frame in which no
+ * pixel belongs to another object. */
+int orc_photometry(const float *sub, int w, int h, const orc_config *cfg, float backsig, orc_phot_obj *po, int n)
+{
+    frame_t F;
+    obj_t o;
+    int i, *alloc = (int *)malloc(sizeof(int) * (size_t)w * h);
+    if (!alloc)
+        return -1;
+    for (i = 0; i < w * h; i++)
+        alloc[i] = -1;
+    memset(&F, 0, sizeof(F));
+    F.w = w;
+    F.h = h;
+    F.sub = sub;
+    F.cfg = cfg;
+    F.backsig = backsig;
+    for (i = 0; i < n; i++) {
+        memset(&o, 0, sizeof(o));
+        o.mx = po[i].mx;
+        o.my = po[i].my;
+        o.a = po[i].a;
+        o.b = po[i].b;
+        o.cxx = po[i].cxx;
+        o.cyy = po[i].cyy;
+        o.cxy = po[i].cxy;
+        o.dbkg = po[i].dbkg;
+        aperflux(&F, alloc, &o, 0);
+        autoflux(&F, alloc, &o, 0);
+        po[i].flux_aper = o.flux_aper;
+        po[i].fluxerr_aper = o.fluxerr_aper;
+        po[i].mag_aper = o.mag_aper;
+        po[i].magerr_aper = o.magerr_aper;
+        po[i].kron = o.kron;
+        po[i].flux_auto = o.flux_auto;
+        po[i].fluxerr_auto = o.fluxerr_auto;
+        po[i].mag_auto = o.mag_auto;
+        po[i].magerr_auto = o.magerr_auto;
+        po[i].flags = o.flags;
+    }
+    free(alloc);
+    return 0;
+}
+
+/* Corrected isophotal flux (isocorflux above) from an object's isophotal
+ * flux, its variance sum, fdnpix and detection threshold. */
+void orc_isocor(float flux, float fluxerr, int fdnpix, float dthresh, float *flux_isocor, float *fluxerr_isocor)
+{
+    obj_t o;
+    memset(&o, 0, sizeof(o));
+    o.flux = flux;
+    o.fluxerr = fluxerr;
+    o.fdnpix = fdnpix;
+    o.dthr = dthresh;
+    isocorflux(&o);
+    *flux_isocor = o.flux_isocor;
+    *fluxerr_isocor = o.fluxerr_isocor;
+}
+
+/* The star/galaxy network's response to nn[0] inputs (nnw_response above). */
+double orc_nnw_response(const orc_nnw *net, const double *input)
+{
+    double in[ORC_NNW_NEURONS];
+    int i;
+    for (i = 0; i < net->nn[0] && i < ORC_NNW_NEURONS; i++)
+        in[i] = input[i];
+    return nnw_response(net, in);
+}
+
+/* CLEAN (run_clean above) over objects given by their measurements, in
+ * object-index order; on return master[i] is -1 for a survivor, else the
+ * survivor it was merged into, and the survivors carry the merged
+ * attributes. */
+int orc_clean_objects(orc_clean_obj *co, int n, int w, int h, double clean_param)
+{
+    frame_t F;
+    orc_config cfg;
+    obj_t *o = (obj_t *)calloc(n + 1, sizeof(obj_t));
+    int i;
+    if (!o)
+        return -1;
+    memset(&F, 0, sizeof(F));
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.clean_param = clean_param;
+    F.w = w;
+    F.h = h;
+    F.cfg = &cfg;
+    for (i = 0; i < n; i++) {
+        o[i].mx = co[i].mx;
+        o[i].my = co[i].my;
+        o[i].a = co[i].a;
+        o[i].b = co[i].b;
+        o[i].cxx = co[i].cxx;
+        o[i].cyy = co[i].cyy;
+        o[i].cxy = co[i].cxy;
+        o[i].abcor = co[i].abcor;
+        o[i].dthr = co[i].dthresh;
+        o[i].mthresh = co[i].mthresh;
+        o[i].fdnpix = co[i].fdnpix;
+        o[i].dnpix = co[i].dnpix;
+        o[i].fdflux = co[i].fdflux;
+        o[i].dflux = co[i].dflux;
+        o[i].flux = co[i].flux;
+        o[i].fluxerr = co[i].fluxerr;
+        o[i].fdpeak = co[i].fdpeak;
+        o[i].dpeak = co[i].dpeak;
+        o[i].peak = co[i].peak;
+        o[i].peakx = co[i].peakx;
+        o[i].peaky = co[i].peaky;
+        o[i].xmin = co[i].xmin;
+        o[i].xmax = co[i].xmax;
+        o[i].ymin = co[i].ymin;
+        o[i].ymax = co[i].ymax;
+        o[i].flags = co[i].flags;
+    }
+    run_clean(&F, o, n);
+    for (i = 0; i < n; i++) {
+        co[i].master = o[i].final_master;
+        co[i].fdnpix = o[i].fdnpix;
+        co[i].dnpix = o[i].dnpix;
+        co[i].fdflux = o[i].fdflux;
+        co[i].dflux = o[i].dflux;
+        co[i].flux = o[i].flux;
+        co[i].fluxerr = o[i].fluxerr;
+        co[i].fdpeak = o[i].fdpeak;
+        co[i].dpeak = o[i].dpeak;
+        co[i].peak = o[i].peak;
+        co[i].peakx = o[i].peakx;
+        co[i].peaky = o[i].peaky;
+        co[i].xmin = o[i].xmin;
+        co[i].xmax = o[i].xmax;
+        co[i].ymin = o[i].ymin;
+        co[i].ymax = o[i].ymax;
+        co[i].flags = o[i].flags;
+    }
+    free(o);
+    return 0;
 }

@@ -30,13 +30,7 @@ prefstruct prefs;
 char gstr[MAXCHAR];
 static picstruct *cur_field;
 
-void error(int num, char *msg1, char *msg2)
-{
-    fprintf(stderr, "refharness error: %s%s\n", msg1, msg2);
-    exit(num);
-}
-
-void warning(char *msg1, char *msg2) { (void)msg1; (void)msg2; }
+/* error() and warning() are the reference's own (src/fits/fitsmisc.c) */
 
 
 

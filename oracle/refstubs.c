@@ -8,7 +8,6 @@
 #define STUB(name) void name(void) { fprintf(stderr, "refharness: " #name " not available\n"); abort(); }
 STUB(copyimage)
 STUB(pasteimage)
-STUB(mergeflags)
 STUB(fitsread)
 STUB(read_cat)
 STUB(close_cat)

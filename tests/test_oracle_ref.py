@@ -69,9 +69,10 @@ def test_filter_matches_reference_golden(masks):
 
 
 def test_getconv_matches_reference(masks):
-    cfgdir = "/root/reference/config"
-    if not os.path.isdir(cfgdir):
+    src = O.ref_src()
+    if src is None:
         pytest.skip("reference tree not present")
+    cfgdir = os.path.join(os.path.dirname(src), "config")
     for name, m in masks.items():
         assert np.array_equal(O.getconv(os.path.join(cfgdir, name + ".conv")), m), name
 
