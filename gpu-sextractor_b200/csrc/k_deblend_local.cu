@@ -13,6 +13,11 @@
 //    are packed (16-bit element indices; about 45 B per pixel in the sweep,
 //    34 B in the assignment); grids are persistent, sized to the resident
 //    capacity, and take objects from a device-side cursor;
+//  * for objects whose state lives in the global arena, the part of it on the
+//    sweep's dependent chains -- the union-find parents and the pixel levels,
+//    5 B per pixel -- is kept in shared memory instead (the "hybrid" form:
+//    every find, link and activity test of the unions is an on-chip access;
+//    sizes, fluxes and branch lists stay in the arena);
 //  * a branch flux is one 64-bit fixed-scale integer (units of 2^(e0-23),
 //    e0 the exponent of the detection threshold, every cd of the object being
 //    at least that threshold).  The object's range is checked first: when
@@ -117,7 +122,7 @@ __device__ __forceinline__ unsigned long long dl_term(float c, int e0) {
 
 // pixels first active at level L: activate, then join to active neighbours
 template <int NT>
-__device__ __forceinline__ void dl_activate_union(const DebArgs &A, int off, int P, int L, int b0, int b1,
+__device__ __forceinline__ void dl_activate_union(const DebArgs &A, int off, int ucap, int L, int b0, int b1,
                                                   const unsigned short *order, int *par, const unsigned char *lev,
                                                   int *status) {
     for (int i = b0 + (int)threadIdx.x; i < b1; i += NT) par[order[i]] = order[i];
@@ -139,7 +144,7 @@ __device__ __forceinline__ void dl_activate_union(const DebArgs &A, int off, int
         for (int q = 0; q < 8; q++) act[q] = nb[q] >= 0 && lev[nb[q] - off] >= L;
 #pragma unroll
         for (int q = 0; q < 8; q++)
-            if (act[q]) sunion(par, e, nb[q] - off, P, status);
+            if (act[q]) sunion(par, e, nb[q] - off, ucap, status);
     }
     __syncthreads();
 }
@@ -189,9 +194,11 @@ __device__ __forceinline__ void dl_levels(const DebArgs &A, int P, const unsigne
 // ---------------------------------------------------------------------------
 // sweep: branch tree, MINCONT cut, kept branches
 // ---------------------------------------------------------------------------
+// hyb: for an arena object, shared memory holding its union-find parents
+// (4 B per pixel) and levels (1 B per pixel), or null
 template <int NT>
 __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, unsigned char *base, int cap,
-                                              int *glist, int *gcount) {
+                                              int *glist, int *gcount, unsigned char *hyb) {
     __shared__ float thr[DB_MAXLEV];
     __shared__ int lvcnt[DB_MAXLEV + 1], lvstart[DB_MAXLEV + 1], lvcur[DB_MAXLEV];
     __shared__ int s_nrl[2], s_nn[2], s_nkept;
@@ -216,7 +223,11 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     unsigned short *const rl0 = order + cap;
     unsigned short *const nid = order + 3 * cap;
     unsigned short *const ndr0 = order + 4 * cap;
-    unsigned char *const lev = reinterpret_cast<unsigned char *>(order + 6 * cap);
+    unsigned char *lev = reinterpret_cast<unsigned char *>(order + 6 * cap);
+    if (hyb) {
+        par = reinterpret_cast<int *>(hyb);
+        lev = hyb + 4 * (size_t)P;
+    }
 #define NDS(s) (nds0 + (s) * cap)
 #define NFL(s) (nfl0 + (s) * cap)
 #define RL(s) (rl0 + (s) * cap)
@@ -228,6 +239,9 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     int *rec = A.D.rec + off;
     const int e0 = A.sc->e0cd;
     int *status = &A.sc->status;
+    // walk cap of the union-find: the object's size (no walk is longer), or
+    // a smaller cap set for a failure test
+    const int ucap = A.loop_cap > 0 ? min(P, A.loop_cap) : P;
 
     // fdpeak, exact fdflux, completion keys (as k_deblend_sweep)
     if (tid == 0) {
@@ -301,12 +315,12 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
                 NFL(prv)[i] = (NFL(prv)[i] & ~1u) | (lhs > value0 ? 1u : 0u);
             }
         // (b) activation and unions
-        dl_activate_union<NT>(A, off, P, L, b0, b1, order, par, lev, status);
+        dl_activate_union<NT>(A, off, ucap, L, b0, b1, order, par, lev, status);
         // (c) roots that joined another component hand over size and flux
         for (int i = tid; i < nold + cnt; i += NT) {
             const int c = i < nold ? RL(prv)[i] : order[b0 + i - nold];
             if (par[c] != c) {
-                const int rt = sfind_c(par, c, P, status);
+                const int rt = sfind_c(par, c, ucap, status);
                 atomicAdd(&sz[rt], sz[c]);
                 atomicAdd(&acc[rt], acc[c]);
                 rec[c] = (lev[c] << 24) | (L << 16) | rt;  // absorbed at level L by rt
@@ -331,7 +345,7 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
         __syncthreads();
         // (e) children report to their parent
         for (int i = tid; i < nprev; i += NT) {
-            const int p = nid[sfind_c(par, NDR(prv)[i], P, status)];
+            const int p = nid[sfind_c(par, NDR(prv)[i], ucap, status)];
             const unsigned f = NFL(prv)[i];
             NDS(prv)[i] = p;
             if (f & 1u) atomicAdd(&NDS(cur)[p], 1);
@@ -646,10 +660,11 @@ __device__ __forceinline__ int rl_item(const RootLists &L, int c) {
 }
 
 // cap > 0: per-object state in dynamic shared memory of cap elements;
-// cap == 0: in the global arena
+// cap == 0: in the global arena, with the parents and levels of objects of
+// at most hyb pixels in dynamic shared memory (5 * hyb bytes) when hyb > 0
 template <int NT>
 __global__ void __launch_bounds__(NT) k_dl_sweep(const __grid_constant__ DebArgs A, const RootLists L, int *cursor,
-                                                 int cap, int *glist, int *gcount) {
+                                                 int cap, int *glist, int *gcount, int hyb) {
     extern __shared__ __align__(16) unsigned char dl_smem[];
     __shared__ int s_item;
     for (;;) {
@@ -658,7 +673,8 @@ __global__ void __launch_bounds__(NT) k_dl_sweep(const __grid_constant__ DebArgs
         const int r = s_item;
         __syncthreads();
         if (r < 0) break;
-        dl_sweep_root<NT>(A, r, cap ? dl_smem : nullptr, cap, glist, gcount);
+        unsigned char *h = (!cap && hyb > 0 && A.R.size[r] <= hyb) ? dl_smem : nullptr;
+        dl_sweep_root<NT>(A, r, cap ? dl_smem : nullptr, cap, glist, gcount, h);
         __syncthreads();
     }
 }
@@ -685,8 +701,9 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 32 : NT == 64 ? 16 : 4) k_dl_as
 // Size classes (list k at lists + k * nroots, its length in counts[k]):
 //   8  <= 64 pixels              shared memory, one warp
 //   0  (64, 256]                 shared memory, one warp
-//   1  (1024, 2048]   2 (256, 1024]       arena, 64 threads
-//   3  > 8192   4 (4096, 8192]   5 (2048, 4096]   arena, 256 threads
+//   1  (1024, 2048]   2 (256, 1024]       arena (hybrid), 64 threads
+//   4  (4096, 8192]   5 (2048, 4096]      arena (hybrid), 256 threads
+//   3  (8192, 32767]             arena (hybrid), 1024 threads
 //   6  > 32767 pixels            128-bit global kernels
 //   7  objects the compact sweeps hand over (flux range beyond 64 bits)
 // Every list holds its objects largest first (a stable sort of the roots by
@@ -730,19 +747,18 @@ __global__ void k_class_fill(const int *size, const unsigned *sorted, int n, con
     if (i == bnd[DL_NLISTS + t]) counts[t] = i - bnd[t] + 1;
 }
 
-// resident CTAs of a kernel on this device (cached per kernel and device)
+// resident CTAs of a kernel on this device (cached per kernel and device; the
+// first launch on a device also raises the kernel's dynamic shared memory
+// limit to smem when that is above the default 48 KB)
 template <typename K>
-static int dl_grid(K kernel, int nt, size_t smem, int *cache) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) dev = 0;
-    if (!cache[dev]) {
+static int dl_grid(K kernel, int nt, size_t smem, DevCache &cache) {
+    return sx_share(cache.get([&](int dev) {
         int nsm = 0, per = 0;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, nt, smem);
-        cache[dev] = max(1, nsm) * max(1, per);
-    }
-    return sx_share(cache[dev]);
+        return max(1, nsm) * max(1, per);
+    }));
 }
 
 static RootLists dl_lists(const int *lists, int *counts, size_t n, int a, int b = -1, int c = -1) {
@@ -775,25 +791,36 @@ int deblend_split_launches(int nroots) { return nroots > 0 ? 3 + radix_launches(
 // The large size classes go first, on two side streams, so that their long
 // per-object latency overlaps the many small objects on the main stream; the
 // objects handed over by the compact sweeps are swept last, after the join.
+// hybrid tiers: largest object of each arena kernel (its parents and levels
+// take 5 B per pixel of shared memory)
+constexpr int DL_HYB3 = DL_ARENA_MAX;  // class 3: 1024-thread CTAs, about 160 KB
+constexpr int DL_HYB45 = 4 * DL_MID;   // classes 4, 5: 256-thread CTAs, 40 KB
+constexpr int DL_HYB12 = DL_MID;       // classes 1, 2: 64-thread CTAs, 10 KB
+constexpr int DL_HYB_BYTES = 5;
+
 void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S) {
     if (nroots <= 0) return;
-    static int g0[64], g1[64], g2[64], g3[64], g4[64];
+    static DevCache g0, g1, g2, g3, g4, g5;
     const size_t n = (size_t)nroots;
     int *glist = const_cast<int *>(lists) + 7 * n;
     const size_t m0 = DL_CAP0 * DL_SWEEP_BYTES, m1 = DL_CAP1 * DL_SWEEP_BYTES;
+    const size_t h3 = (size_t)DL_HYB3 * DL_HYB_BYTES, h45 = (size_t)DL_HYB45 * DL_HYB_BYTES,
+                 h12 = (size_t)DL_HYB12 * DL_HYB_BYTES;
     cudaEventRecord(S.fork, S.main);
     cudaStreamWaitEvent(S.side[0], S.fork, 0);
     cudaStreamWaitEvent(S.side[1], S.fork, 0);
     const int grid3 = min(nroots, dl_grid(k_deblend_sweep, DB_THREADS, 0, g3));
     k_deblend_sweep<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 6 * n, counts + 6, DL_SCUR(6));
-    k_dl_sweep<256><<<min(nroots, dl_grid(k_dl_sweep<256>, 256, 0, g2)), 256, 0, S.side[1]>>>(
-        A, dl_lists(lists, counts, n, 3, 4, 5), DL_SCUR(3), 0, glist, counts + 7);
-    k_dl_sweep<64><<<min(nroots, dl_grid(k_dl_sweep<64>, 64, 0, g1)), 64, 0, S.main>>>(
-        A, dl_lists(lists, counts, n, 1, 2), DL_SCUR(1), 0, glist, counts + 7);
+    k_dl_sweep<256><<<min(nroots, dl_grid(k_dl_sweep<256>, 256, h45, g2)), 256, h45, S.side[0]>>>(
+        A, dl_lists(lists, counts, n, 4, 5), DL_SCUR(4), 0, glist, counts + 7, DL_HYB45);
+    k_dl_sweep<1024><<<min(nroots, dl_grid(k_dl_sweep<1024>, 1024, h3, g5)), 1024, h3, S.side[1]>>>(
+        A, dl_lists(lists, counts, n, 3), DL_SCUR(3), 0, glist, counts + 7, DL_HYB3);
+    k_dl_sweep<64><<<min(nroots, dl_grid(k_dl_sweep<64>, 64, h12, g1)), 64, h12, S.main>>>(
+        A, dl_lists(lists, counts, n, 1, 2), DL_SCUR(1), 0, glist, counts + 7, DL_HYB12);
     k_dl_sweep<32><<<min(nroots, dl_grid(k_dl_sweep<32>, 32, m0, g0)), 32, m0, S.main>>>(
-        A, dl_lists(lists, counts, n, 0), DL_SCUR(0), DL_CAP0, glist, counts + 7);
+        A, dl_lists(lists, counts, n, 0), DL_SCUR(0), DL_CAP0, glist, counts + 7, 0);
     k_dl_sweep<32><<<min(nroots, dl_grid(k_dl_sweep<32>, 32, m1, g4)), 32, m1, S.main>>>(
-        A, dl_lists(lists, counts, n, 8), DL_SCUR(8), DL_CAP1, glist, counts + 7);
+        A, dl_lists(lists, counts, n, 8), DL_SCUR(8), DL_CAP1, glist, counts + 7, 0);
     cudaEventRecord(S.join[0], S.side[0]);
     cudaEventRecord(S.join[1], S.side[1]);
     cudaStreamWaitEvent(S.main, S.join[0], 0);
@@ -803,7 +830,7 @@ void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int n
 
 void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S) {
     if (nroots <= 0) return;
-    static int g0[64], g1[64], g2[64], g3[64], g4[64];
+    static DevCache g0, g1, g2, g3, g4;
     const size_t n = (size_t)nroots;
     const size_t m0 = DL_CAP0 * DL_ASSIGN_BYTES, m1 = DL_CAP1 * DL_ASSIGN_BYTES;
     cudaEventRecord(S.fork, S.main);

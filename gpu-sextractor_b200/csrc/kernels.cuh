@@ -1,5 +1,6 @@
 // kernels.cuh -- buffers and launchers shared by the stages of libsexgpu.
 #pragma once
+#include <atomic>
 #include "common.cuh"
 
 namespace sx {
@@ -46,6 +47,25 @@ struct DebBufs {
 // fastest).
 extern thread_local int sx_grid_div;
 inline int sx_share(int grid) { return sx_grid_div > 1 ? (grid + sx_grid_div - 1) / sx_grid_div : grid; }
+
+// A value per device computed on first use (resident grid sizes, device
+// attributes), for the current device.  Several host threads (batch workers)
+// may ask at once: the slots are atomic, and a value computed twice is
+// computed the same way; 0 means "not computed yet".
+struct DevCache {
+    std::atomic<int> v[64];
+    template <class F> int get(F compute) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= 64) return compute(dev);
+        int x = v[dev].load(std::memory_order_relaxed);
+        if (x == 0) {
+            x = compute(dev);
+            v[dev].store(x, std::memory_order_relaxed);
+        }
+        return x;
+    }
+};
 
 // Kron boxes too large for one warp, summed by whole CTAs (k_post.cu)
 constexpr int KR_CHUNK = 8192;     // box pixels per CTA work item
@@ -128,6 +148,7 @@ struct DebArgs {
     int w, h, N, debminarea;
     FastDiv wdiv;
     double mincont;
+    int loop_cap;               // > 0: cap on union-find walks (failure tests); 0: the object's size
 };
 
 // the main stream, two side streams and the events that fork and join them

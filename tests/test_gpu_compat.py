@@ -89,3 +89,67 @@ def test_reference_call_sequence(gpu_ctx, masks, harness, case):
     assert np.array_equal(rows["flag"].astype(np.int32), g["flags"])
     assert not rows["alpha2000"].any()
     assert np.array_equal(rows["sprob"], g["class_star"]) and (rows["sprob"].any() == (net is not None))
+
+
+REF_SCAN = os.path.join(ROOT, "oracle", "_ref", "ref_scan")
+
+# the columns and formats of the reference's printobj() (src/scan.c:331-403)
+PRINTOBJ = [("number", "%10d"), ("alpha2000", "%11.7f"), ("delta2000", "%+11.7f"), ("sposx", "%10.3f"),
+            ("sposy", "%10.3f"), ("flux_iso", "%12.7g"), ("fluxerr_iso", "%12.7g"), ("mag_iso", "%8.4f"),
+            ("magerr_iso", "%8.4f"), ("flux_isocor", "%12.7g"), ("fluxerr_isocor", "%12.7g"),
+            ("flux_aper", "%12.7g"), ("fluxerr_aper", "%12.7g"), ("mag_aper", "%8.4f"), ("magerr_aper", "%8.4f"),
+            ("flux_auto", "%12.7g"), ("fluxerr_auto", "%12.7g"), ("mag_auto", "%8.4f"), ("magerr_auto", "%8.4f"),
+            ("theta", "%5.1f"), ("poserr_mx2", "%15.10e"), ("poserr_my2", "%15.10e"), ("poserr_mxy", "%15.10e"),
+            ("flag", "%3d"), ("elong", "%8.3f"), ("ellip", "%8.3f"), ("sprob", "%5.2f"), ("peak", "%12.7g"),
+            ("kronfactor", "%5.2f"), ("bkg", "%12.7g"), ("fwhm", "%8.2f")]
+
+
+def printobj_lines(g):
+    """The catalogue rows of sexgpu_extract (first-pixel order) printed as the
+    reference's printobj() prints its records."""
+    out = []
+    for i, r in enumerate(g):
+        v = {"number": i, "alpha2000": 0.0, "delta2000": 0.0,
+             "sposx": float(np.float32(r["mx"] + 1.0)), "sposy": float(np.float32(r["my"] + 1.0)),
+             "flag": int(r["flags"]), "sprob": float(r["class_star"])}
+        for name, _ in PRINTOBJ:
+            if name not in v:
+                v[name] = float(r[name])
+        out.append(" ".join(fmt % v[name] for name, fmt in PRINTOBJ))
+    return out
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SCAN), reason="oracle/_ref/ref_scan not built (needs the reference tree)")
+@pytest.mark.parametrize("case", ["c0", "crowded"])
+def test_reference_scan_c_links_unchanged(gpu_ctx, masks, tmp_path, case):
+    """The drop-in: the reference's own src/scan.c, src/back.c and src/misc.c,
+    compiled unmodified and linked against libsexgpu_compat.so
+    (oracle/_ref/ref_scan, driver oracle/refscan.c), run makeback() and
+    scanimage() and print the catalogue with the reference's printobj().  Its
+    text equals the catalogue of sexgpu_extract printed the same way."""
+    if case == "c0":
+        img = synth.frame_c0(seed=41, w=700, h=512, nsrc=700)
+        mask = masks["default"]
+        opts = dict(back_size=64, back_filtersize=3, clean_flag=1, clean_param=1.0, gain=0.0, satur_level=50000.0,
+                    detect_minarea=5, deblend_nthresh=32, deblend_mincont=0.005)
+    else:
+        img = synth.frame_c1(seed=42, w=900, h=640, nsrc=6000)
+        mask = masks["gauss_2.5_5x5"]
+        opts = dict(back_size=32, back_filtersize=5, clean_flag=1, clean_param=1.2, gain=1.5, satur_level=4e4,
+                    detect_minarea=3, deblend_nthresh=48, deblend_mincont=0.001)
+    h, w = img.shape
+    fimg, fmask, fcat = tmp_path / "img.f32", tmp_path / "mask.f32", tmp_path / "ref.cat"
+    img.astype(np.float32).tofile(fimg)
+    mask.astype(np.float32).tofile(fmask)
+    args = [REF_SCAN, str(fimg), str(w), str(h), str(fmask), str(mask.shape[1]), str(mask.shape[0]), str(fcat),
+            str(opts["back_size"]), str(opts["back_filtersize"]), "0.0", "1.5", "1.5", str(opts["detect_minarea"]),
+            str(opts["deblend_nthresh"]), repr(opts["deblend_mincont"]), str(opts["clean_flag"]),
+            repr(opts["clean_param"]), repr(opts["gain"]), repr(opts["satur_level"])]
+    out = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr + out.stdout
+    ref_lines = [ln.rstrip("\n") for ln in open(fcat)]
+    g, seg, s = gpu_ctx.extract(img, conv=mask, numbering=1, **opts)
+    assert "sextracted %d" % len(g) in out.stdout
+    ours = printobj_lines(g)
+    assert len(ref_lines) == len(ours) > 50
+    assert ref_lines == ours
