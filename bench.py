@@ -35,7 +35,18 @@ import numpy as np  # noqa: E402
 
 METRIC = "4096² frames/s & Mobj/s on 1 B200, batched vs plain, catalog err vs FP64"
 WORKLOAD = "c1: 4096x4096 float32, 200k injected sources (43% px above threshold), gauss_2.5_5x5"
+WORKLOAD_LITERAL = ("c1 literal: 4096x4096 float32, 167,000 injected sources with fluxes 1e2-1e6 ADU "
+                    "(the configuration's generator as written), gauss_2.5_5x5")
 L2_FLUSH_BYTES = 256 << 20
+
+
+def bench_config(world):
+    """The `config` object of both arms (identical, so the two lines compare
+    the same workload)."""
+    return {"workload": WORKLOAD, "frame": [4096, 4096],
+            "l2": "GPU arm: flushed between steps (256 MB write outside the timed window)",
+            "parallelism": "frame-sharded: every unit of work extracts whole frames; %d GPU(s) or the "
+                           "host cores" % world}
 
 
 def load_mask(name):
@@ -222,7 +233,7 @@ def run_gpu(args):
     roofline = {"bound": "hbm", "kernel": dom[0], "achieved": round(achieved, 1), "peak": peak,
                 "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": NCU_TRAFFIC.get(dom[0]) if (w, h) == (4096, 4096) else None,
-                "traffic_source": "ncu launch list of prof_case.py --workload c1 (dram__bytes_read.sum + "
+                "traffic_source": "ncu launch list of bench.py --profile-case c1 (dram__bytes_read.sum + "
                                   "dram__bytes_write.sum over the stage's launches, one frame)",
                 "algorithmic_bytes": algo,
                 "stage_ms": {s[0]: round(s[2], 4) for s in stages}}
@@ -234,11 +245,11 @@ def run_gpu(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_dev, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded; stands in for the paper's unpublished 4096^2 frames)",
-        "config": {"workload": WORKLOAD, "frame": [h, w], "objects": int(summ.nobj),
-                   "raw_objects": int(summ.nraw), "pixels_above_threshold": int(summ.npix_above),
-                   "raw_object_pixels": int(summ.nraw_pix), "pixel_levels": int(summ.level_pix),
-                   "l2": "flushed between steps (256 MB write outside the timed window)",
-                   "parallelism": "frame-sharded replicas" if world > 1 else "single GPU"},
+        "config": bench_config(world),
+        "workload_stats": {"objects": int(summ.nobj), "raw_objects": int(summ.nraw),
+                           "pixels_above_threshold": int(summ.npix_above),
+                           "raw_object_pixels": int(summ.nraw_pix), "pixel_levels": int(summ.level_pix),
+                           "parallelism": "frame-sharded replicas" if world > 1 else "single GPU"},
         "mobj_per_s": round(frames_dev * summ.nobj / 1e6, 4),
         "e2e": {"value": round(frames_e2e, 3), "unit": "frames/s", "ms_per_step": round(ms_e2e, 4),
                 "mobj_per_s": round(frames_e2e * nobj / 1e6, 4),
@@ -249,38 +260,20 @@ def run_gpu(args):
                            "frac": round(frame_bytes / (peak * 1e9) / (ms_dev / 1e3), 4)},
         "clocks": clk,
     }
-    if rank == 0:
-        line["catalog_err_fp64"] = catalog_err(ctx, frame, cfg)
     if world == 1 and not args.no_batch:
         line["batch"] = run_batch(ctx, c3_frames())
+    if world == 1 and not args.no_literal:
+        line["c1_literal"] = run_literal(ctx, torch, dev, stream, cfg, flush)
     if world == 1 and not args.no_c4:
         line["c4"] = run_c4(ctx, torch, dev, stream, peak)
     if rank == 0 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(frame, cfg)
+        line["cpu_baseline"], line["catalog_err_fp64"] = cpu_baseline(frame, cfg, ctx)
     if rank == 0:
         print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     ctx.close()
-
-
-def catalog_err(ctx, frame, cfg, tol=1e-5):
-    """Per-column error of the catalogue against a float64 recomputation
-    from the same segmentation (fp64check).  CLEAN is off for this one
-    extraction so that every row is the measurement of its own segmentation
-    pixels (a CLEAN merge adds fluxes but keeps the master's moments)."""
-    import fp64check
-    kw = dict(cfg)
-    kw["clean_flag"] = 0
-    cat, seg, s, sub, cd = ctx.extract(frame, max_objects=400000, want_maps=True, **kw)
-    rep = fp64check.catalog_error(cat, seg, sub, cd, s.thresh, s.dthresh, s.backsig, gain=kw.get("gain", 0.0))
-    worst = fp64check.worst(rep)
-    return {"settings": "workload frame with CLEAN off; float64 recomputation from the GPU's segmentation, "
-                        "subtracted and filtered frames; mag_iso and theta_deg are absolute errors",
-            "tolerance_rel": tol, "worst_rel": worst, "within": worst is not None and worst <= tol,
-            "columns": {k: {kk: (round(vv, 12) if isinstance(vv, float) else vv) for kk, vv in v.items()}
-                        for k, v in rep.items()}}
 
 
 def _c3_base(job):
@@ -362,7 +355,7 @@ def run_batch(ctx, frames, reps=5, workers=8, maxobj=400000):
 
 
 # DRAM bytes (read + write) per c1 frame of each stage's launches, from one
-# ncu launch-list capture of prof_case.py --workload c1 (its summary is kept
+# ncu launch-list capture of bench.py --profile-case c1 (its summary is kept
 # under profiles/)
 NCU_TRAFFIC = {"background": 134_600_000, "sub_filter": 207_900_000, "ccl": 275_300_000, "roots": 663_000_000,
                "deblend": 967_700_000, "analyse": 391_200_000, "clean": 14_900_000, "endobject": 200_100_000,
@@ -385,6 +378,61 @@ def algorithmic_bytes(stage, N, s):
     if stage == "deblend":
         return 8 * int(s.level_pix)        # index + cd per pixel and level
     return 4 * N
+
+
+def run_literal(ctx, torch, dev, stream, cfg, flush, steps=5):
+    """The configuration's own generator as written (167,000 sources, fluxes
+    1e2-1e6 ADU) on the plain path: device-resident ms per frame and one
+    end-to-end call through sexgpu_extract with pinned host buffers per step,
+    L2 flushed before each; and whether the 50 ms per frame target holds."""
+    import ctypes as C
+    import sexgpu
+    import synth
+    frame = synth.frame_c1(seed=1000, nsrc=167000, fmin=1e2)
+    h, w = frame.shape
+    d_img = torch.from_numpy(frame).to(dev)
+    h_img = torch.from_numpy(frame).pin_memory()
+    maxobj = 400000
+    h_rows = torch.empty(maxobj * sexgpu.OBJECT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    c = sexgpu.make_config(**cfg)
+
+    def e2e():
+        n = C.c_int()
+        s = sexgpu.Summary()
+        rc = sexgpu.lib().sexgpu_extract(ctx.h, C.c_void_p(h_img.data_ptr()), None, w, h, C.byref(c),
+                                         C.c_void_p(h_rows.data_ptr()), maxobj, C.byref(n), None, None, None,
+                                         C.byref(s))
+        if rc != 0:
+            raise RuntimeError("sexgpu_extract failed %d" % rc)
+        return n.value
+
+    def dev_step():
+        return ctx.extract_device(d_img.data_ptr(), w, h, **cfg)
+
+    for _ in range(3):
+        s = dev_step()
+        e2e()
+    ms_dev, ms_e2e = [], []
+    for _ in range(steps):
+        for fn, out in ((dev_step, ms_dev), (e2e, ms_e2e)):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            out.append(e0.elapsed_time(e1))
+    md, me = float(np.median(ms_dev)), float(np.median(ms_e2e))
+    return {"workload": WORKLOAD_LITERAL, "frame": [h, w], "objects": int(s.nobj), "raw_objects": int(s.nraw),
+            "pixels_above_threshold": int(s.npix_above), "raw_object_pixels": int(s.nraw_pix),
+            "ms_per_frame": round(md, 3), "frames_per_s": round(1e3 / md, 2),
+            "mobj_per_s": round(s.nobj / md / 1e3, 4), "e2e_ms_per_frame": round(me, 3),
+            "e2e_frames_per_s": round(1e3 / me, 2), "steps": steps, "timing": "median of %d steps" % steps,
+            "target_ms": 50.0, "target_holds": bool(me <= 50.0),
+            "stage_ms": {n: round(t, 4) for n, _, t in ctx.stage_times()}}
 
 
 C4_WORKLOAD = ("c4: one 16384x16384 float32 frame with 2.5 M injected sources (c1 generator) and a MAP_VAR "
@@ -511,15 +559,50 @@ def cpu_model():
     return None
 
 
-def cpu_baseline(frame, cfg):
-    """The oracle (single-threaded C restatement of the path) on one frame."""
+# float columns of the catalogue rows the FP64 report covers, and the cause of
+# the rows a column may have above its tolerance
+FP64_NOTES = {
+    "fwhm": "ill-conditioned log-linear fit (src/cuda/cudaanalyse.cu:2521-2578): when the selected pixels are "
+            "nearly equidistant its determinant nearly cancels and rounding moves the result",
+    "theta": "ill-conditioned for near-round objects (a ~ b): the angle is undefined in the limit",
+    "cxy": "the inverse moment matrix where its determinant nearly cancels (relative to sqrt(cxx cyy))",
+    "cxx": "the inverse moment matrix where its determinant nearly cancels",
+    "cyy": "the inverse moment matrix where its determinant nearly cancels",
+    "flux_aper": "a sub-pixel sample on the aperture circle falls the other way with double positions",
+    "kronfactor": "a pixel on the Kron ellipse falls the other way with double shapes",
+}
+
+
+def cpu_baseline(frame, cfg, ctx):
+    """The CPU leg: the oracle (single-threaded C restatement of the path)
+    timed on one frame; then, untimed, the oracle's FP64 twin of the same
+    frame as the checker of the GPU catalogue's floating-point columns: per
+    column the max and RMS error of the GPU's float32 rows against the
+    double-precision measurements of the same objects."""
     from oracle import oracle as O
     t = time.perf_counter()
     objs, _, s = O.extract(frame, **cfg)
     dt = time.perf_counter() - t
-    return {"value": round(1.0 / dt, 4), "unit": "frames/s", "cores": 1, "kind": "port",
+    base = {"value": round(1.0 / dt, 4), "unit": "frames/s", "cores": 1, "kind": "port",
             "sample": "one 4096x4096 frame of the workload, single thread (%d objects)" % len(objs),
             "seconds": round(dt, 3), "cpu_model": cpu_model(), "nproc": os.cpu_count()}
+    cat = ctx.extract(frame, max_objects=400000, segmap=False, **cfg)[0]
+    _, rows64, _, _ = O.extract_fp64(frame, max_objects=400000, **cfg)
+    if len(rows64) != len(cat) or not np.array_equal(rows64["number"], cat["number"]):
+        return base, {"error": "catalogue rows differ from the oracle's"}
+    rep = O.fp64_errors(cat, rows64)
+    over = {k: v["over"] for k, v in rep.items() if v["over"]}
+    err = {"settings": "the workload frame and settings (CLEAN on); GPU float32 catalogue against the FP64 "
+                       "oracle (oracle/orc_fp64.c: the same objects measured with long double sums and double "
+                       "arithmetic)",
+           "rows": int(len(cat)),
+           "metrics": "rel: |a-b|/|b|; abs: |a-b| (mag, pixels, bounded columns); deg: THETA in degrees; "
+                      "scaled: cross term / sqrt(product of the diagonal terms)",
+           "within": not over, "columns_over": over,
+           "notes": {k: FP64_NOTES[k] for k in over if k in FP64_NOTES},
+           "columns": {k: {kk: (float("%.4g" % vv) if isinstance(vv, float) else vv) for kk, vv in v.items()}
+                       for k, v in rep.items()}}
+    return base, err
 
 
 def run_reference(args):
@@ -544,7 +627,7 @@ def run_reference(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(dt / args.steps * 1e3, 2), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "parallelism": "%d processes, one frame each per step" % ncpu},
+            "config": bench_config(world),
             "cpu_baseline": {"value": round(fps, 4), "unit": "frames/s", "cores": ncpu, "kind": "port",
                              "sample": "%d frames per step (one per worker), 4096x4096 each" % ncpu,
                              "cpu_model": cpu_model(), "nproc": os.cpu_count()},
@@ -553,8 +636,41 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+PROFILE_CASES = ("c0", "c1", "c1lit", "c2")
+
+
+def profile_case(name, iters):
+    """One workload frame extracted `iters` times through the C ABI with the
+    frame resident on the device, nothing else: the command the ncu
+    summaries under profiles/ capture (python bench.py --profile-case c1
+    --iters 2)."""
+    import torch
+    import sexgpu
+    import synth
+    if name == "c0":
+        frame, cfg = synth.frame_c0(seed=0), dict(conv=load_mask("default"))
+    elif name == "c1":
+        frame, cfg = make_frame(1000), workload_config()
+    elif name == "c1lit":
+        frame, cfg = synth.frame_c1(seed=1000, nsrc=167000, fmin=1e2), workload_config()
+    else:
+        frame = synth.frame_c2(seed=2000)
+        cfg = dict(workload_config(), deblend_nthresh=64, deblend_mincont=0.0005)
+    h, w = frame.shape
+    d = torch.from_numpy(frame).cuda()
+    with sexgpu.Context(0) as ctx:
+        for _ in range(iters):
+            s = ctx.extract_device(d.data_ptr(), w, h, **cfg)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": name, "objects": s.nobj, "raw": s.nraw, "stages": ctx.stage_times()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile-case", choices=PROFILE_CASES,
+                    help="extract one workload frame --iters times and print its stage times (for ncu)")
+    ap.add_argument("--iters", type=int, default=2)
+    ap.add_argument("--no-literal", action="store_true", help="skip the line of the literal c1 generator")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
@@ -563,6 +679,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the 16384^2 weighted frame (c4)")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case, args.iters)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

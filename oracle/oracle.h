@@ -157,6 +157,8 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
 /* Read and normalise a .conv mask (src/filter.c:101-185).
  * Returns number of elements, or <0 on error. */
 int orc_getconv(const char *path, float *mask, int maxn, int *mw, int *mh);
+/* background map (w*h), src/back.c:790 subbackline's backline */
+int orc_background_map(const float *img, int w, int h, const orc_config *cfg, float *out);
 /* background rms map (w*h), src/back.c:938 backrmsline */
 int orc_background_rms(const float *img, int w, int h, const orc_config *cfg, float *rms);
 /* src/back.c:568 localback for objects given by their boxes (4 ints each:
@@ -189,6 +191,26 @@ typedef struct {
     int32_t master;                       /* out: -1 survivor, else its survivor */
 } orc_clean_obj;
 int orc_clean_objects(orc_clean_obj *o, int n, int w, int h, double clean_param);
+
+/* The FP64 oracle (orc_fp64.c): the floating-point catalogue columns of an
+ * extraction, recomputed in double over the same objects (the FP32 oracle's
+ * segmentation, deblending, CLEAN and areas); one row per catalogue row. */
+typedef struct {
+    int32_t number;
+    double  fdflux, dflux, flux, fluxerr, fdpeak, dpeak, peak;
+    double  mx, my, mx2, my2, mxy;
+    double  a, b, theta, abcor, cxx, cyy, cxy;
+    double  class_star;
+    double  poserr_mx2, poserr_my2, poserr_mxy;
+    double  bkg, thresh, fwhm;
+    double  flux_iso, fluxerr_iso, mag_iso, magerr_iso;
+    double  flux_isocor, fluxerr_isocor;
+    double  flux_aper, fluxerr_aper, mag_aper, magerr_aper;
+    double  kronfactor, flux_auto, fluxerr_auto, mag_auto, magerr_auto;
+    double  elong, ellip, polar;
+} orc_object64;
+/* the next orc_extract also writes the FP64 rows into out (up to max rows) */
+void orc_set_fp64_rows(orc_object64 *out, int max);
 
 /* Small helpers exposed for unit tests. */
 float   orc_hmedian(float *ra, int n);

@@ -197,6 +197,29 @@ def background_rms(img, **kw):
     return rms
 
 
+def background_map(img, **kw):
+    """Background map (w*h float32, subbackline's backline)."""
+    cfg = make_config(**kw)
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    out = np.zeros_like(img)
+    h, w = img.shape
+    lib().orc_background_map(_f(img), w, h, C.byref(cfg), _f(out))
+    return out
+
+
+def ref_background_map(img, back_size=64, back_filtersize=3, back_filtthresh=0.0, back_type=0, back_value=0.0):
+    """The reference's own makeback() + subbackline() backline (None if not built)."""
+    r = ref()
+    if r is None:
+        return None
+    img = np.ascontiguousarray(img, dtype=np.float32)
+    out = np.zeros_like(img)
+    h, w = img.shape
+    r.ref_background_map(_f(img), w, h, back_size, back_filtersize, C.c_double(back_filtthresh), back_type,
+                         C.c_double(back_value), _f(out))
+    return out
+
+
 def localback(sub, boxes, thick=24):
     """LOCAL photometry background (localback) per object box (xmin, xmax, ymin, ymax)."""
     sub = np.ascontiguousarray(sub, np.float32)
@@ -514,3 +537,94 @@ def ref_read_body(raw, bitpix, bscale=1.0, bzero=0.0, blank=None, bitsgn=1):
     if rc != 0:
         raise RuntimeError("ref_read_body failed")
     return out
+
+
+def _extract_job(job):
+    img, kw, weight, max_objects = job
+    cat, seg, s = extract(img, max_objects=max_objects, weight=weight, **kw)
+    return cat, seg, (s.nraw, s.nraw_pix, s.ndetected, s.nobj, s.backsig)
+
+
+def extract_many(jobs, processes=None, max_objects=None):
+    """extract() of several frames in a pool of spawned processes (the oracle
+    is single-threaded): jobs are (img, kw) or (img, kw, weight); returns
+    (catalogue, segmap, (nraw, nraw_pix, ndetected, nobj, backsig)) per
+    frame, in order."""
+    import multiprocessing as mp
+    work = [(j[0], j[1], j[2] if len(j) > 2 else None, max_objects) for j in jobs]
+    n = processes or min(len(work), os.cpu_count() or 1, 16)
+    if n <= 1:
+        return [_extract_job(j) for j in work]
+    with mp.get_context("spawn").Pool(n) as pool:
+        return pool.map(_extract_job, work, chunksize=1)
+
+
+OBJECT64_FLOATS = ["fdflux", "dflux", "flux", "fluxerr", "fdpeak", "dpeak", "peak", "mx", "my", "mx2", "my2", "mxy",
+                   "a", "b", "theta", "abcor", "cxx", "cyy", "cxy", "class_star", "poserr_mx2", "poserr_my2",
+                   "poserr_mxy", "bkg", "thresh", "fwhm", "flux_iso", "fluxerr_iso", "mag_iso", "magerr_iso",
+                   "flux_isocor", "fluxerr_isocor", "flux_aper", "fluxerr_aper", "mag_aper", "magerr_aper",
+                   "kronfactor", "flux_auto", "fluxerr_auto", "mag_auto", "magerr_auto", "elong", "ellip", "polar"]
+OBJECT64_DTYPE = np.dtype([("number", "i4")] + [(n, "f8") for n in OBJECT64_FLOATS], align=True)
+
+
+def extract_fp64(img, max_objects=None, weight=None, **kw):
+    """extract() with the FP64 oracle beside it: returns (catalogue,
+    FP64 rows, segmap, summary); FP64 row k holds the floating-point columns
+    of catalogue row k recomputed in double over the same object."""
+    img = np.ascontiguousarray(img, np.float32)
+    h, w = img.shape
+    if max_objects is None:
+        max_objects = w * h // max(1, kw.get("detect_minarea", 5)) // 2 + 16
+    rows = np.zeros(max_objects, OBJECT64_DTYPE)
+    lib().orc_set_fp64_rows(rows.ctypes.data_as(C.c_void_p), max_objects)
+    cat, seg, s = extract(img, max_objects=max_objects, weight=weight, **kw)
+    return cat, rows[:len(cat)], seg, s
+
+
+# Error of a float32 catalogue column against the FP64 oracle, per column:
+#   "rel"   |a - b| / |b|
+#   "abs"   |a - b| (magnitudes in mag, positions in pixels, CLASS_STAR,
+#           ELLIPTICITY and polarisation, which are bounded and can be 0)
+#   "deg"   the angle difference in degrees, modulo 180 (THETA)
+#   ("scaled", u, v)  |a - b| / sqrt(|u_b v_b|): a cross term against the
+#           diagonal terms of the same matrix (it can be 0 for round objects)
+FP64_METRIC = {"mx": "abs", "my": "abs", "theta": "deg", "ellip": "abs", "polar": "abs", "class_star": "abs",
+               "mag_iso": "abs", "mag_aper": "abs", "mag_auto": "abs",
+               "mxy": ("scaled", "mx2", "my2"), "cxy": ("scaled", "cxx", "cyy"),
+               "poserr_mxy": ("scaled", "poserr_mx2", "poserr_my2")}
+# tolerances: 1e-5 relative, and its equivalents
+FP64_TOL = {"rel": 1e-5, "abs": 1e-5, "deg": 0.01, "scaled": 1e-5}
+FP64_TOL_COL = {"mx": 1e-4, "my": 1e-4, "mag_iso": 2e-5, "mag_aper": 2e-5, "mag_auto": 2e-5}
+# columns that are not float32 measurements of the catalogue row
+FP64_SKIP = {"thresh", "bkg"}
+
+
+def fp64_errors(cat, rows64, columns=None):
+    """Per-column error of catalogue rows against their FP64 oracle rows:
+    {column: {metric, n, max, rms, tol, over}} (over = rows above tol)."""
+    rep = {}
+    for name in columns or OBJECT64_FLOATS:
+        if name in FP64_SKIP or name not in cat.dtype.names:
+            continue
+        a = cat[name].astype(np.float64)
+        b = rows64[name].astype(np.float64)
+        m = FP64_METRIC.get(name, "rel")
+        if m == "rel":
+            err = np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+        elif m == "abs":
+            err = np.abs(a - b)
+        elif m == "deg":
+            d = np.abs(a - b) % 180.0
+            err = np.minimum(d, 180.0 - d)
+        else:
+            scale = np.sqrt(np.abs(rows64[m[1]] * rows64[m[2]]))
+            err = np.abs(a - b) / np.maximum(scale, 1e-300)
+        kind = m if isinstance(m, str) else m[0]
+        tol = FP64_TOL_COL.get(name, FP64_TOL[kind])
+        ok = np.isfinite(err)
+        err = err[ok]
+        rep[name] = {"metric": kind, "n": int(err.size),
+                     "max": float(err.max()) if err.size else None,
+                     "rms": float(np.sqrt(np.mean(err * err))) if err.size else None,
+                     "tol": tol, "over": int((err > tol).sum())}
+    return rep

@@ -523,6 +523,33 @@ int orc_background_rms(const float *img, int w, int h, const orc_config *cfg, fl
     return 0;
 }
 
+/* The background map (src/back.c:790 subbackline's backline, the
+   BACKGROUND check image): every line of -0 minus the interpolated map,
+   negated back exactly (backmean everywhere for an absolute background). */
+int orc_background_map(const float *img, int w, int h, const orc_config *cfg, float *out)
+{
+    int bw = cfg->back_size < w ? cfg->back_size : w, bh = cfg->back_size < h ? cfg->back_size : h;
+    int nx = (w - 1) / bw + 1, ny = (h - 1) / bh + 1, y;
+    size_t p, nb = (size_t)nx * ny;
+    float *copy = (float *)malloc(sizeof(float) * (size_t)w * h);
+    float *back = (float *)malloc(sizeof(float) * nb), *dback = (float *)malloc(sizeof(float) * nb);
+    orc_summary s;
+    memcpy(copy, img, sizeof(float) * (size_t)w * h);
+    orc_background(copy, w, h, cfg, back, NULL, dback, NULL, &s);
+    for (y = 0; y < h; y++) {
+        float *line = out + (size_t)y * w;
+        for (p = 0; p < (size_t)w; p++)
+            line[p] = -0.0f;
+        sub_back_line(back, dback, nx, ny, bw, bh, cfg->back_type, s.backmean, y, line, w);
+        for (p = 0; p < (size_t)w; p++)
+            line[p] = -line[p];
+    }
+    free(copy);
+    free(back);
+    free(dback);
+    return 0;
+}
+
 int orc_background(float *img, int w, int h, const orc_config *cfg,
                    float *back_out, float *sigma_out, float *dback_out, float *dsigma_out,
                    orc_summary *sum)

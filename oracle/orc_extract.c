@@ -86,61 +86,6 @@ typedef struct {
     int parent;            /* node index at level-1 */
 } node_t;
 
-typedef struct {
-    int root, level;
-    float node_dthresh;
-    float dthr, athr;      /* the raw object's detection / analysis thresholds */
-    float dbkg;            /* local background (BACKPHOTO_TYPE LOCAL), else 0 */
-    int nnode;             /* pixels of the branch at its own level */
-    int *nodepix;
-    int n;                 /* final pixels (raster order) */
-    int *pix;
-    /* preanalysis */
-    int xmin, xmax, ymin, ymax, dnpix, flags, singuflag;
-    float fdflux, dflux, fdpeak, dpeak;
-    double mx, my, mx2, my2, mxy;
-    float a, b, theta, abcor, cxx, cyy, cxy;
-    /* examineiso */
-    int npix, peakx, peaky, iso[ORC_NISO];
-    float flux, fluxerr, peak, bkg, thresh, mthresh, fwhm;
-    double poserr_mx2, poserr_my2, poserr_mxy;
-    /* clean */
-    int master, final_master, fdnpix;
-    /* endobject */
-    float flux_isocor, fluxerr_isocor, flux_aper, fluxerr_aper, mag_aper, magerr_aper;
-    float kron, flux_auto, fluxerr_auto, mag_auto, magerr_auto;
-    float mag_iso, magerr_iso, fluxerr_iso;
-    float elong, ellip, polar;
-    float class_star;
-} obj_t;
-
-typedef struct {
-    int w, h;
-    const float *sub, *cd;
-    const orc_config *cfg;
-    float dthresh, thresh, backsig;
-    const float *back;
-    int nbx, nby, bw, bh;
-    int minarea, debminarea;
-    /* weight map: calibrated variance per pixel (ORC_BIGF where unusable),
-     * NULL without one; wthr: thresholds follow the local rms */
-    const float *var;
-    int wthr;
-} frame_t;
-
-/* Pixel thresholds with a weight map (SExtractor manual, weight maps: a
- * relative threshold is taken against the local rms): DETECT_THRESH (or
- * ANALYSIS_THRESH) x sqrt(variance); the global value otherwise. */
-static inline int pix_bad(const frame_t *F, size_t p) { return F->var && !(F->var[p] < ORC_BIGF); }
-static inline float pix_dthr(const frame_t *F, size_t p)
-{
-    return F->wthr ? (float)(F->cfg->detect_thresh * sqrt((double)F->var[p])) : F->dthresh;
-}
-static inline float pix_athr(const frame_t *F, size_t p)
-{
-    return F->wthr ? (float)(F->cfg->analysis_thresh * sqrt((double)F->var[p])) : F->thresh;
-}
-
 /* ------------------------------------------------------------------------ */
 /* Branch CCL inside one root at threshold t: labels lab[k] (index into the
  * root's raster-ordered pixel list) get the smallest member position; -1 for
@@ -1134,6 +1079,16 @@ static void endobject(const frame_t *F, const int *alloc, obj_t *o, int self)
 }
 
 /* ------------------------------------------------------------------------ */
+/* rows of the FP64 twin asked for by orc_set_fp64_rows (one extraction) */
+static orc_object64 *g_out64;
+static int g_max64;
+
+void orc_set_fp64_rows(orc_object64 *out, int max)
+{
+    g_out64 = out;
+    g_max64 = max;
+}
+
 typedef struct {
     int ymax, lastx, idx;
 } okey_t;
@@ -1413,6 +1368,14 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
         qsort(keys, ns, sizeof(okey_t), cmp_okey);
         for (k = 0; k < ns; k++)
             number[keys[k].idx] = k + 1;
+        if (g_out64) {
+            int *rows = (int *)malloc(sizeof(int) * (ns + 1));
+            for (k = 0; k < ns; k++)
+                rows[k] = keys[k].idx;
+            orc_measure64(&F, alloc, objs, nobj, rows, ns < g_max64 ? ns : g_max64, g_out64);
+            free(rows);
+            g_out64 = NULL;
+        }
         for (k = 0; k < ns && nout < max_objects; k++) {
             obj_t *o = &objs[keys[k].idx];
             orc_object *q = &out[nout++];

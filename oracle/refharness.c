@@ -167,6 +167,60 @@ int ref_localback(const float *sub, int w, int h, int thick, const int *box, int
     return 0;
 }
 
+/* The background map of the reference: makeback(), then subbackline()
+ * (src/back.c:790) for every row, keeping the backline it fills (what
+ * src/readimage.c:114 writes to the BACKGROUND check image).  img is not
+ * modified. */
+int ref_background_map(const float *img, int w, int h, int back_size, int back_filtersize, double back_filtthresh,
+                       int back_type, double back_value, float *out)
+{
+    picstruct field;
+    int y;
+    float *copy = (float *)malloc(sizeof(float) * (size_t)w * h);
+    memcpy(copy, img, sizeof(float) * (size_t)w * h);
+    memset(&field, 0, sizeof(field));
+    memset(&prefs, 0, sizeof(prefs));
+    prefs.backfthresh = back_filtthresh;
+    prefs.ndthresh = prefs.nthresh = 1;
+    prefs.dthresh[0] = prefs.thresh[0] = 1.5;
+    prefs.thresh_type[0] = prefs.thresh_type[1] = THRESH_RELATIVE;
+    prefs.back_val[0] = prefs.back_val[1] = back_value;
+    prefs.detect_type = CCD;
+    prefs.verbose_type = QUIET;
+    field.width = w;
+    field.height = h;
+    field.flags = DETECT_FIELD;
+    field.pixscale = 1.0;
+    field.ngamma = 4.0 / log(10.0);
+    field.backw = back_size < w ? back_size : w;
+    field.backh = back_size < h ? back_size : h;
+    field.nbackp = field.backw * field.backh;
+    field.nbackx = (w - 1) / field.backw + 1;
+    field.nbacky = (h - 1) / field.backh + 1;
+    field.nback = field.nbackx * field.nbacky;
+    field.nbackfx = field.nbackx > 1 ? back_filtersize : 1;
+    field.nbackfy = field.nbacky > 1 ? back_filtersize : 1;
+    field.back_type = back_type ? BACK_ABSOLUTE : BACK_RELATIVE;
+    field.strip = copy;
+    field.stripheight = h;
+    field.ymin = 0;
+    field.ymax = h;
+    field.backline = (PIXTYPE *)malloc(sizeof(PIXTYPE) * w);
+    cur_field = &field;
+    makeback(&field);
+    for (y = 0; y < h; y++) {
+        subbackline(&field, y, copy + (size_t)y * w);
+        memcpy(out + (size_t)y * w, field.backline, sizeof(float) * w);
+    }
+    free(field.back);
+    free(field.sigma);
+    free(field.dback);
+    free(field.dsigma);
+    free(field.backline);
+    free(copy);
+    return 0;
+}
+
 /* The background rms map of the reference: makeback(), then backrmsline()
  * (src/back.c:938) for every row.  img is not modified. */
 int ref_background_rms(const float *img, int w, int h, int back_size, int back_filtersize,
