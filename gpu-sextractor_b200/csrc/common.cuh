@@ -36,6 +36,7 @@ __device__ __forceinline__ float sx_unblank(float v) { return v != v ? -1e+30f :
 #define SX_ST_RANGE 1
 #define SX_ST_LOOP 2
 #define SX_ST_CAPACITY 4
+#define SX_ST_LOAD 8     // a tile load of the subtract/filter pipeline did not complete in time
 
 #define SX_ALLOC_OTHER 0x7fffffff
 
@@ -353,6 +354,7 @@ struct FrameParams {
     int wthr;                       // thresholds follow the local rms (weight map, relative thresholds)
     double seeing, pixscale;        // SEEING_FWHM, PIXEL_SCALE (CLASS_STAR)
     int bp_local, bp_thick;         // BACKPHOTO_TYPE LOCAL, BACKPHOTO_THICK
+    int loop_cap;                   // > 0: cap on union-find walks and retries (failure tests); 0: built-in caps
 };
 
 // scalars computed on the device during one extraction

@@ -911,14 +911,14 @@ void launch_background(BackBufs &B, const float *img, const FrameParams &P, Fram
     const size_t band_bytes = (size_t)BAND_STAGES * 32 * stride * sizeof(float);
     constexpr int BAND_SMEM_MAX = 200 * 1024;
     if (band_bytes <= BAND_SMEM_MAX) {
-        static bool attr_set[64];
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        // the shared memory limit of both instances, once per device (host
+        // threads of a batch may get here at the same time)
+        static DevCache attr_set;
+        attr_set.get([](int) {
             cudaFuncSetAttribute(k_mesh_stat_band<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, BAND_SMEM_MAX);
             cudaFuncSetAttribute(k_mesh_stat_band<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, BAND_SMEM_MAX);
-            attr_set[dev] = true;
-        }
+            return 1;
+        });
         dim3 grid((P.nbx + 31) / 32, P.nby);
         if (vec)
             k_mesh_stat_band<true><<<grid, 32, band_bytes, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, stride, B.ms);

@@ -37,6 +37,17 @@ __device__ __forceinline__ float bkg_at(int x, int y, const BackBufs &B, int nbx
     return (float)(cdx * (nd[k] + (cdx * cdx - 1) * dnd[k]) + dx * (nd[k + 1] + (dx * dx - 1) * dnd[k + 1]));
 }
 
+// The background map of every pixel, the values src/back.c:790-936
+// (subbackline) writes into backline and subtracts: the BACKGROUND check
+// image (src/readimage.c:114); backmean everywhere for an absolute background.
+__global__ void k_back_map(BackBufs B, int nbx, int back_type, const FrameScalars *sc, int w, long long n,
+                           float *__restrict__ out) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int y = (int)(p / w), x = (int)(p - (long long)y * w);
+    out[p] = bkg_at(x, y, B, nbx, back_type, sc->backmean);
+}
+
 __global__ void __launch_bounds__(SF_TX *SF_TY) k_sub_filter(const float *__restrict__ img, float *__restrict__ sub,
                                                               float *__restrict__ cd, int *__restrict__ lab,
                                                               BackBufs B, int w, int h, int nbx, int back_type,
@@ -346,11 +357,13 @@ __global__ void __launch_bounds__(ST_THREADS) k_sub_filter_pipe(const __grid_con
         __syncthreads();
     }
     if (failed) {
-        // a load did not complete in time: report it and give the copies
-        // still in flight one more bounded wait, so that none is left writing
-        // into a finished CTA's shared memory
+        // A load did not complete in time: report it, and give the copies
+        // still in flight one more bounded wait before the CTA exits.  A copy
+        // that outlasts that wait too may still write into shared memory after
+        // the CTA has gone, so this status (SEXGPU_ERR_LOAD) tells the caller
+        // to destroy the context rather than use it again.
         if (tid == 0) {
-            atomicOr(&A.sc->status, SX_ST_LOOP);
+            atomicOr(&A.sc->status, SX_ST_LOAD);
             sp_wait(bar0, 0);
             sp_wait(bar0, 1);
             sp_wait(bar1, 0);
@@ -370,18 +383,17 @@ __global__ void __launch_bounds__(ST_THREADS) k_sub_filter_pipe(const __grid_con
 
 // a 2D float tensor map of the frame with the tile box of this mask, or false
 static bool make_frame_tmap(CUtensorMap *m, const float *img, int w, int h, int rxa, int ry) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    static bool looked = false;
-    if (!looked) {
-        looked = true;
+    // the driver's encoder, looked up once (a function-local static is
+    // initialised once even when host threads arrive together)
+    static const PFN_cuTensorMapEncodeTiled_v12000 encode = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
         cudaDriverEntryPointQueryResult q;
         void *fn = nullptr;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-        else
-            cudaGetLastError();
-    }
+            return (PFN_cuTensorMapEncodeTiled_v12000)fn;
+        cudaGetLastError();
+        return nullptr;
+    }();
     if (!encode || ((uintptr_t)img & 15) || (w % 4) != 0) return false;
     const cuuint64_t dims[2] = {(cuuint64_t)w, (cuuint64_t)h};
     const cuuint64_t strides[1] = {(cuuint64_t)w * 4};
@@ -422,27 +434,28 @@ void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const 
         if (mw * mh <= 121) memcpy(taps.m, M.host, sizeof(float) * mw * mh);
         const int bw = ST_TW + 2 * rxa, bh = ST_TH + 2 * (mh / 2);
         const size_t smem = 2 * sizeof(float) * (size_t)((bw * bh + 31) & ~31);
-        static int nsm_cache[64];
-        int dev = 0, nsm = 148;
-        cudaGetDevice(&dev);
-        if (dev >= 0 && dev < 64 && nsm_cache[dev] > 0) {
-            nsm = nsm_cache[dev];
-        } else {
-            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            if (dev >= 0 && dev < 64) nsm_cache[dev] = nsm;
-        }
+        static DevCache nsm_cache;
+        const int nsm = nsm_cache.get([](int dev) {
+            int n = 148;
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+            return n > 0 ? n : 148;
+        });
 #define SP_LAUNCH(a, b, wt)                                                                              \
     do {                                                                                                \
         auto kern = k_sub_filter_pipe<a, b, wt>;                                                        \
-        static std::atomic<long long> cached{0};  /* (smem << 8) | resident CTAs, this instance */   \
-        long long c = cached.load();                                                                    \
+        /* (smem << 8) | resident CTAs of this instance, per device */                                 \
+        static std::atomic<long long> cached[64];                                                       \
+        int dev_ = 0;                                                                                   \
+        cudaGetDevice(&dev_);                                                                           \
+        std::atomic<long long> &slot = cached[dev_ >= 0 && dev_ < 64 ? dev_ : 0];                      \
+        long long c = slot.load(std::memory_order_relaxed);                                             \
         int per = (int)(c & 255);                                                                       \
         if ((c >> 8) != (long long)smem) {                                                              \
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);        \
             per = 1;                                                                                    \
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, ST_THREADS, smem);                \
             per = std::min(std::max(per, 1), 255);                                                      \
-            cached.store(((long long)smem << 8) | per);                                                 \
+            slot.store(((long long)smem << 8) | per, std::memory_order_relaxed);                        \
         }                                                                                               \
         const int grid = std::max(1, std::min(A.ntiles, sx_share(nsm * per)));                         \
         kern<<<grid, ST_THREADS, smem, st>>>(tmap, A, taps);                                            \
@@ -552,20 +565,26 @@ __global__ void __launch_bounds__(CC_TW *CC_TH) k_ccl_local(int *__restrict__ la
     }
 }
 
-__device__ __forceinline__ int gfind(const int *L, int a) {
-    int n = 0;
-    while (true) {
+// walk to the root; a walk longer than cap steps sets SX_ST_LOOP and stops
+__device__ __forceinline__ int gfind(const int *L, int a, int cap, int *status) {
+    for (int n = 0; n <= cap; n++) {
         int p = L[a];
         if (p == a) return a;
         a = p;
-        if (++n > (1 << 28)) return a;
     }
+    atomicOr(status, SX_ST_LOOP);
+    return a;
 }
 
-__device__ __forceinline__ void gunion(int *L, int a, int b, int *status) {
-    for (int it = 0; it < (1 << 20); it++) {
-        a = gfind(L, a);
-        b = gfind(L, b);
+// walk and link caps: the built-in ones, or a smaller cap set for a test
+__device__ __forceinline__ int ccl_walk_cap(int loop_cap) { return loop_cap > 0 ? loop_cap : (1 << 28); }
+__device__ __forceinline__ int ccl_link_cap(int loop_cap) { return loop_cap > 0 ? loop_cap : (1 << 20); }
+
+__device__ __forceinline__ void gunion(int *L, int a, int b, int *status, int loop_cap) {
+    const int wcap = ccl_walk_cap(loop_cap), lcap = ccl_link_cap(loop_cap);
+    for (int it = 0; it < lcap; it++) {
+        a = gfind(L, a, wcap, status);
+        b = gfind(L, b, wcap, status);
         if (a == b) return;
         if (a < b) {
             int t = a;
@@ -581,7 +600,7 @@ __device__ __forceinline__ void gunion(int *L, int a, int b, int *status) {
 
 // unions across tile borders: pixels on the first row or first/last column
 // of a tile look at their backward neighbours in other tiles
-__global__ void k_ccl_border(int *__restrict__ lab, int w, int h, int *status) {
+__global__ void k_ccl_border(int *__restrict__ lab, int w, int h, int *status, int loop_cap) {
     int tilesx = (w + CC_TW - 1) / CC_TW;
     int tile = blockIdx.x, k = threadIdx.x;           // k < CC_TW + CC_TH
     int tx0 = (tile % tilesx) * CC_TW, ty0 = (tile / tilesx) * CC_TH;
@@ -598,35 +617,35 @@ __global__ void k_ccl_border(int *__restrict__ lab, int w, int h, int *status) {
     int p = y * w + x;
     if (lab[p] < 0) return;
     // W neighbour (other tile when x is the tile's first column)
-    if (x == tx0 && x > 0 && lab[p - 1] >= 0) gunion(lab, p, p - 1, status);
+    if (x == tx0 && x > 0 && lab[p - 1] >= 0) gunion(lab, p, p - 1, status, loop_cap);
     if (y > 0) {
         // NW: other tile when x or y is on the tile's first column/row
-        if (x > 0 && (x == tx0 || y == ty0) && lab[p - w - 1] >= 0) gunion(lab, p, p - w - 1, status);
-        if (y == ty0 && lab[p - w] >= 0) gunion(lab, p, p - w, status);
-        if (x < w - 1 && (y == ty0 || x == tx0 + CC_TW - 1) && lab[p - w + 1] >= 0) gunion(lab, p, p - w + 1, status);
+        if (x > 0 && (x == tx0 || y == ty0) && lab[p - w - 1] >= 0) gunion(lab, p, p - w - 1, status, loop_cap);
+        if (y == ty0 && lab[p - w] >= 0) gunion(lab, p, p - w, status, loop_cap);
+        if (x < w - 1 && (y == ty0 || x == tx0 + CC_TW - 1) && lab[p - w + 1] >= 0) gunion(lab, p, p - w + 1, status, loop_cap);
     }
 }
 
 // the last column of each tile also looks NE into the next tile (row y-1)
-__global__ void k_ccl_border_ne(int *__restrict__ lab, int w, int h, int *status) {
+__global__ void k_ccl_border_ne(int *__restrict__ lab, int w, int h, int *status, int loop_cap) {
     int tilesx = (w + CC_TW - 1) / CC_TW;
     int tile = blockIdx.x, k = threadIdx.x;  // k in [1, CC_TH)
     if (k == 0 || k >= CC_TH) return;
     int x = (tile % tilesx) * CC_TW + CC_TW - 1, y = (tile / tilesx) * CC_TH + k;
     if (x >= w - 1 || y >= h) return;
     int p = y * w + x;
-    if (lab[p] >= 0 && lab[p - w + 1] >= 0) gunion(lab, p, p - w + 1, status);
+    if (lab[p] >= 0 && lab[p - w + 1] >= 0) gunion(lab, p, p - w + 1, status, loop_cap);
 }
 
 // every pixel to its root, and the component sizes: lanes of a warp holding
 // the same root add once to cnt (zeroed before)
-__global__ void k_ccl_flatten(int *__restrict__ lab, long long n, int *__restrict__ cnt) {
+__global__ void k_ccl_flatten(int *__restrict__ lab, long long n, int *__restrict__ cnt, int *status, int loop_cap) {
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int r = -1;
     if (p < n) {
         const int l = lab[p];
         if (l >= 0) {
-            r = gfind(lab, (int)p);
+            r = gfind(lab, (int)p, ccl_walk_cap(loop_cap), status);
             if (r != l) lab[p] = r;
         }
     }
@@ -640,10 +659,10 @@ void launch_ccl(int *lab, int *cnt, const FrameParams &P, FrameScalars *d_sc, cu
     k_ccl_local<<<grid, dim3(CC_TW, CC_TH), 0, st>>>(lab, P.w, P.h);
     int ntiles = grid.x * grid.y;
     int *status = &d_sc->status;
-    k_ccl_border<<<ntiles, CC_TW + CC_TH, 0, st>>>(lab, P.w, P.h, status);
-    k_ccl_border_ne<<<ntiles, CC_TH, 0, st>>>(lab, P.w, P.h, status);
+    k_ccl_border<<<ntiles, CC_TW + CC_TH, 0, st>>>(lab, P.w, P.h, status, P.loop_cap);
+    k_ccl_border_ne<<<ntiles, CC_TH, 0, st>>>(lab, P.w, P.h, status, P.loop_cap);
     long long n = (long long)P.w * P.h;
-    k_ccl_flatten<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(lab, n, cnt);
+    k_ccl_flatten<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(lab, n, cnt, status, P.loop_cap);
     launches += 4;
 }
 

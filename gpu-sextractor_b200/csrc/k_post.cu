@@ -120,7 +120,10 @@ __global__ void __launch_bounds__(CL_PAIR_WARPS * 32) k_clean_pairs(const CleanO
 }
 
 // end of the master chain; victims with a master get sort keys for merging
-__global__ void k_clean_chain(ObjBufs O, int n, unsigned *vkey, unsigned *vval, int *nvict) {
+// the chain of masters of a victim ends at a survivor after fewer than n
+// steps (masters have smaller indices); cap: a smaller bound set for a
+// failure test (0: n); running out sets SX_ST_LOOP
+__global__ void k_clean_chain(ObjBufs O, int n, unsigned *vkey, unsigned *vval, int *nvict, int *status, int cap) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int m = O.master[i];
@@ -128,7 +131,10 @@ __global__ void k_clean_chain(ObjBufs O, int n, unsigned *vkey, unsigned *vval, 
         O.fmaster[i] = -1;
         return;
     }
-    for (int it = 0; it < n && O.master[m] != 0x7fffffff; it++) m = O.master[m];
+    const int lim = cap > 0 && cap < n ? cap : n;
+    int it = 0;
+    for (; it < lim && O.master[m] != 0x7fffffff; it++) m = O.master[m];
+    if (O.master[m] != 0x7fffffff) atomicOr(status, SX_ST_LOOP);
     O.fmaster[i] = m;
     int k = atomicAdd(nvict, 1);
     vkey[k] = (unsigned)m;

@@ -121,17 +121,19 @@ __global__ void k_sub_only(const float *__restrict__ img, float *__restrict__ su
     sub[p] = sx_unblank(img[p]) - sx::bkg_at(x, y, B, nbx, back_type, sc->backmean);
 }
 
-__global__ void k_init(FrameScalars *sc) {
-    FrameScalars z;
-    memset(&z, 0, sizeof(z));
-    z.e0sub = 1000;
-    *sc = z;
-}
-
 }  // namespace sx_noalloc
 
+extern "C" int sexgpu_background_meshes(int w, int h, int back_size, int *nbackx, int *nbacky) {
+    if (w <= 0 || h <= 0 || back_size < 1 || !nbackx || !nbacky) return SEXGPU_ERR_ARG;
+    const int bw = back_size < w ? back_size : w, bh = back_size < h ? back_size : h;  // src/field.c:124-127
+    *nbackx = (w - 1) / bw + 1;
+    *nbacky = (h - 1) / bh + 1;
+    return SEXGPU_OK;
+}
+
 extern "C" int sexgpu_background_noalloc(const float *d_img, float *d_sub, int w, int h, const sexgpu_config *cfg,
-                                         float *d_back, float *d_sigma, sexgpu_summary *sum, void *stream) {
+                                         float *d_back, float *d_sigma, int mesh_capacity, sexgpu_summary *sum,
+                                         void *stream) {
     using namespace sx_noalloc;
     if (!d_img || !d_sub || !d_back || !d_sigma || !cfg || w <= 0 || h <= 0) return SEXGPU_ERR_ARG;
     if (cfg->back_size < 1 || cfg->back_filtersize < 1 || cfg->back_filtersize > 11) return SEXGPU_ERR_ARG;
@@ -140,6 +142,8 @@ extern "C" int sexgpu_background_noalloc(const float *d_img, float *d_sub, int w
     if (w > MAX_W || h > MAX_H || (long long)Pm.nbx * Pm.nby > MAX_MESH ||
         (long long)h * Pm.nbx > MAX_ROWNODES)
         return SEXGPU_ERR_NOALLOC_LIMIT;
+    // the caller's mesh maps must hold nbackx * nbacky floats each
+    if ((long long)mesh_capacity < (long long)Pm.nbx * Pm.nby) return SEXGPU_ERR_ARG;
     unsigned char *base = nullptr;
     cudaError_t e = scratch_on_current_device(&base);
     if (e != cudaSuccess) return SEXGPU_ERR_CUDA;
@@ -160,7 +164,7 @@ extern "C" int sexgpu_background_noalloc(const float *d_img, float *d_sub, int w
     B.colk = (int *)(base + OFF_COLK);
     B.coldx = (float *)(base + OFF_COLDX);
     int nl = 0;
-    k_init<<<1, 1, 0, st>>>(d_sc);
+    k_init_scalars<<<1, 1, 0, st>>>(d_sc);  // the pipeline's initial scalars (sigfac 1)
     k_col_table<<<(w + 255) / 256, 256, 0, st>>>(w, Pm.nbx, Pm.bw, B.colk, B.coldx);
     sx::launch_background(B, d_img, Pm, d_sc, st, nl);
     long long n = (long long)w * h;

@@ -103,6 +103,7 @@ struct sexgpu_ctx {
     DevBuf dnnw;                           // this context's copy of the CLASS_STAR network
     const sexgpu_nnw *nnw_dev = nullptr;   // network used (this context's or, for a batch worker, its owner's)
     int kron_warp_max = KR_WARP_MAX;
+    int loop_cap = 0;  // "loop_cap" parameter: cap on device walks, for failure tests (0: built-in caps)
     DevBuf sc;
     FrameScalars hsc;
     ObjBufs O;
@@ -282,6 +283,7 @@ void make_params(const sexgpu_config *cfg, int w, int h, FrameParams &P) {
     P.pixscale = cfg->pixel_scale > 0.0 ? cfg->pixel_scale : 1.0;
     P.bp_local = cfg->back_photo_type == 1;
     P.bp_thick = cfg->back_photo_thick;
+    P.loop_cap = 0;
 }
 
 __global__ void k_init_scalars(FrameScalars *sc) {
@@ -308,6 +310,10 @@ cudaError_t stream_wait(sexgpu_ctx *ctx, cudaStream_t st) {
 int read_scalars(sexgpu_ctx *ctx) {
     CK(cudaMemcpyAsync(&ctx->hsc, ctx->sc.p, sizeof(FrameScalars), cudaMemcpyDeviceToHost, ctx->stream));
     CK(stream_wait(ctx, ctx->stream));
+    if (ctx->hsc.status & SX_ST_LOAD) {
+        ctx->err = "a tile load did not complete in time; destroy this context";
+        return SEXGPU_ERR_LOAD;
+    }
     if (ctx->hsc.status & SX_ST_LOOP) {
         ctx->err = "device loop iteration cap reached";
         return SEXGPU_ERR_LOOP;
@@ -449,6 +455,7 @@ int pipe_begin(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, 
     ps.stage = 0;
     FrameParams &Pm = ps.Pm;
     make_params(cfg, w, h, Pm);
+    Pm.loop_cap = ctx->loop_cap;
     ps.w = w;
     ps.h = h;
     ps.d_img = d_img;
@@ -718,6 +725,7 @@ int pipe_deblend(sexgpu_ctx *ctx) {
     A.N = Pm.nthresh;
     A.debminarea = Pm.debminarea;
     A.mincont = Pm.mincont;
+    A.loop_cap = Pm.loop_cap;
     A.wdiv = make_fastdiv((unsigned)w);
     EN(rlists, (size_t)(DL_NLISTS * (nroots + 1)) * 4);
     EN(rcounts, 5 * DL_NLISTS * 4);
@@ -829,7 +837,7 @@ int pipe_clean(sexgpu_ctx *ctx) {
                                                                       cellcnt, O.master, gx, gy);
         CK(cudaMemsetAsync(&d_sc->nsurv, 0, 4, st));
         k_clean_chain<<<grid1(nobj, 256), 256, 0, st>>>(O, nobj, P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval),
-                                                        &d_sc->nsurv);
+                                                        &d_sc->nsurv, &d_sc->status, Pm.loop_cap);
         rc = read_scalars(ctx);
         if (rc) return rc;
         nv = ctx->hsc.nsurv;
@@ -1228,6 +1236,25 @@ int sexgpu_background_rms(sexgpu_ctx *ctx, float *rms) {
     return SEXGPU_OK;
 }
 
+int sexgpu_background_map(sexgpu_ctx *ctx, float *back) {
+    if (!ctx || !back) return SEXGPU_ERR_ARG;
+    const PipeState &ps = ctx->ps;
+    if (ps.stage < 1 || ps.Pm.w <= 0) {
+        ctx->err = "no extraction to take the background map of";
+        return SEXGPU_ERR_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const FrameParams &Pm = ps.Pm;
+    const long long N = (long long)Pm.w * Pm.h;
+    EN(rmsmap, (size_t)N * 4);
+    k_back_map<<<grid1(N, 256), 256, 0, st>>>(ps.B, Pm.nbx, Pm.back_type, P<FrameScalars>(ctx->sc), Pm.w, N,
+                                             P<float>(ctx->rmsmap));
+    CK(cudaMemcpyAsync(back, ctx->rmsmap.p, (size_t)N * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SEXGPU_OK;
+}
+
 int sexgpu_background(sexgpu_ctx *ctx, float *img, int w, int h, const sexgpu_config *cfg, float *back,
                       float *sigma, sexgpu_summary *sum) {
     if (!ctx || !img || !cfg) return SEXGPU_ERR_ARG;
@@ -1592,6 +1619,11 @@ int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value) {
     if (!strcmp(name, "kron_warp_max")) {
         if (value < 1) return SEXGPU_ERR_ARG;
         ctx->kron_warp_max = value;
+        return SEXGPU_OK;
+    }
+    if (!strcmp(name, "loop_cap")) {
+        if (value < 0) return SEXGPU_ERR_ARG;
+        ctx->loop_cap = value;
         return SEXGPU_OK;
     }
     ctx->err = std::string("unknown parameter ") + name;

@@ -16,8 +16,8 @@
  *   DEBLEND_NTHRESH DEBLEND_MINCONT CLEAN CLEAN_PARAM MASK_TYPE
  *   PHOT_APERTURES PHOT_AUTOPARAMS SATUR_LEVEL MAG_ZEROPOINT GAIN
  *   BACK_SIZE BACK_FILTERSIZE BACK_FILTTHRESH BACK_TYPE BACK_VALUE
- *   CHECKIMAGE_TYPE (NONE, SEGMENTATION, BACKGROUND, BACKGROUND_RMS, -BACKGROUND, FILTERED)
- *   CHECKIMAGE_NAME VERBOSE_TYPE
+ *   CHECKIMAGE_TYPE (NONE, SEGMENTATION, BACKGROUND, BACKGROUND_RMS, -BACKGROUND, FILTERED; a list,
+ *   one CHECKIMAGE_NAME per type) CHECKIMAGE_NAME VERBOSE_TYPE
  *   WEIGHT_TYPE (NONE, MAP_VAR, MAP_RMS, MAP_WEIGHT, BACKGROUND) WEIGHT_IMAGE
  *   STARNNW_NAME SEEING_FWHM PIXEL_SCALE (CLASS_STAR)
  *   BACKPHOTO_TYPE (GLOBAL, LOCAL) BACKPHOTO_THICK
@@ -872,19 +872,30 @@ int main(int argc, char **argv)
         if (cat != stdout) fclose(cat);
     }
     if (seg) {
-        if (!strcasecmp(p.check_type, "SEGMENTATION")) write_fits(p.check_name, seg, w, h, 32);
-        else if (!strcasecmp(p.check_type, "-BACKGROUND")) write_fits(p.check_name, sub, w, h, -32);
-        else if (!strcasecmp(p.check_type, "FILTERED")) write_fits(p.check_name, cd, w, h, -32);
-        else if (!strcasecmp(p.check_type, "BACKGROUND_RMS")) {
-            /* src/check.c:221: the rms map, made on the device */
-            if (sexgpu_background_rms(ctx, cd) != SEXGPU_OK) die("rms map: ", sexgpu_last_error(ctx));
-            write_fits(p.check_name, cd, w, h, -32);
+        /* CHECKIMAGE_TYPE and CHECKIMAGE_NAME are lists, paired in order
+           (src/prefs.c: one check image per type) */
+        char types[sizeof p.check_type], names[sizeof p.check_name], *ts = NULL, *ns = NULL, *t, *nm;
+        float *map = NULL;
+        snprintf(types, sizeof types, "%s", p.check_type);
+        snprintf(names, sizeof names, "%s", p.check_name);
+        for (t = strtok_r(types, ", \t", &ts), nm = strtok_r(names, ", \t", &ns); t;
+             t = strtok_r(NULL, ", \t", &ts), nm = strtok_r(NULL, ", \t", &ns)) {
+            if (!nm) die("CHECKIMAGE_NAME has fewer names than CHECKIMAGE_TYPE has types", NULL);
+            if (!strcasecmp(t, "SEGMENTATION")) write_fits(nm, seg, w, h, 32);
+            else if (!strcasecmp(t, "-BACKGROUND")) write_fits(nm, sub, w, h, -32);
+            else if (!strcasecmp(t, "FILTERED")) write_fits(nm, cd, w, h, -32);
+            else if (!strcasecmp(t, "BACKGROUND_RMS") || !strcasecmp(t, "BACKGROUND")) {
+                /* src/check.c:221 (the rms map) and src/readimage.c:114 (the
+                   background subtracted from every pixel), made on the device */
+                int r;
+                if (!map && !(map = (float *)malloc(sizeof(float) * (size_t)w * h))) die("out of memory", NULL);
+                r = !strcasecmp(t, "BACKGROUND") ? sexgpu_background_map(ctx, map) : sexgpu_background_rms(ctx, map);
+                if (r != SEXGPU_OK) die("background map: ", sexgpu_last_error(ctx));
+                write_fits(nm, map, w, h, -32);
+            } else if (strcasecmp(t, "NONE"))
+                die("unsupported CHECKIMAGE_TYPE ", t);
         }
-        else if (!strcasecmp(p.check_type, "BACKGROUND")) {
-            img = fits_to_float(raw, &fmt, (size_t)w * h);
-            for (size_t k = 0; k < (size_t)w * h; k++) sub[k] = img[k] - sub[k];
-            write_fits(p.check_name, sub, w, h, -32);
-        }
+        free(map);
     }
     if (strcasecmp(p.verbose, "QUIET"))
         fprintf(stderr, "Background: %g RMS: %g / Threshold: %g\nObjects: detected %d / sextracted %d\n"

@@ -24,7 +24,8 @@ OK = 0
 ERRORS = {-1: "bad argument", -2: "CUDA error", -3: "out of device memory",
           -4: "exact sum out of range", -5: "buffer too small", -6: "no CUDA device",
           -7: "zero or negative threshold", -8: "device loop cap reached",
-          -9: "frame beyond the fixed scratch of the no-allocation entry point"}
+          -9: "frame beyond the fixed scratch of the no-allocation entry point",
+          -10: "tile load timed out (destroy the context)"}
 
 
 class Config(C.Structure):
@@ -122,7 +123,8 @@ EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extra
            "sexgpu_extract_device", "sexgpu_copy_results", "sexgpu_background", "sexgpu_filter",
            "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times", "sexgpu_set_param",
            "sexgpu_read_nnw", "sexgpu_set_nnw", "sexgpu_extract_fits", "sexgpu_background_rms",
-           "sexgpu_background_noalloc", "sexgpu_extract_batch"]
+           "sexgpu_background_noalloc", "sexgpu_background_meshes", "sexgpu_background_map",
+           "sexgpu_extract_batch"]
 
 _lib = None
 
@@ -290,6 +292,13 @@ class Context:
             return objs[:n.value], seg, s, sub, cd
         return objs[:n.value], seg, s
 
+    def background_map(self, shape):
+        """Background map of the last extraction (h, w float32): the value
+        subtracted from every pixel (the BACKGROUND check image)."""
+        back = np.zeros(shape, np.float32)
+        _check(lib().sexgpu_background_map(self.h, _f(back)), self.h, "sexgpu_background_map")
+        return back
+
     def background_rms(self, shape):
         """Background rms map of the last extraction (h, w float32)."""
         rms = np.zeros(shape, np.float32)
@@ -352,14 +361,23 @@ class Context:
         return [(st[i].name.decode(), st[i].launches, st[i].ms) for i in range(max(n, 0))]
 
 
-def background_noalloc(d_img, d_sub, w, h, d_back, d_sigma, stream=0, **kw):
+def background_meshes(w, h, back_size):
+    """(nbackx, nbacky) of a w x h frame (sexgpu_background_meshes)."""
+    nx, ny = C.c_int(), C.c_int()
+    _check(lib().sexgpu_background_meshes(w, h, back_size, C.byref(nx), C.byref(ny)), None,
+           "sexgpu_background_meshes")
+    return nx.value, ny.value
+
+
+def background_noalloc(d_img, d_sub, w, h, d_back, d_sigma, mesh_capacity, stream=0, **kw):
     """sexgpu_background_noalloc on caller-owned device buffers (device
-    pointers as ints).  For callers that cannot allocate device memory: the
-    library works in a fixed device array; see include/sexgpu.h for limits."""
+    pointers as ints; d_back and d_sigma hold mesh_capacity floats each).
+    For callers that cannot allocate device memory: the library works in a
+    fixed device array; see include/sexgpu.h for limits."""
     cfg = make_config(**kw)
     s = Summary()
     rc = lib().sexgpu_background_noalloc(C.c_void_p(d_img), C.c_void_p(d_sub), w, h, C.byref(cfg),
-                                         C.c_void_p(d_back), C.c_void_p(d_sigma), C.byref(s),
+                                         C.c_void_p(d_back), C.c_void_p(d_sigma), int(mesh_capacity), C.byref(s),
                                          C.c_void_p(stream))
     _check(rc, None, "sexgpu_background_noalloc")
     return s

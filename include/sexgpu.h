@@ -41,6 +41,7 @@ extern "C" {
 #define SEXGPU_ERR_THRESH     -7   /* zero or negative threshold (src/back.c:196) */
 #define SEXGPU_ERR_LOOP       -8   /* a bounded device loop hit its iteration cap */
 #define SEXGPU_ERR_NOALLOC_LIMIT -9 /* frame beyond the fixed scratch of sexgpu_background_noalloc */
+#define SEXGPU_ERR_LOAD      -10   /* a tile load did not complete in time: destroy the context */
 
 #define SEXGPU_NISO 8
 
@@ -177,6 +178,12 @@ int sexgpu_copy_results(sexgpu_ctx *ctx, sexgpu_object *objs, int max_objects, i
  * floats, the filtered sigma mesh map through the background's splines. */
 int sexgpu_background_rms(sexgpu_ctx *ctx, float *rms);
 
+/* The background map of the last extraction (src/back.c:790 subbackline's
+ * backline; the BACKGROUND check image, src/readimage.c:114): w*h host
+ * floats, the value subtracted from every pixel (backmean everywhere for an
+ * absolute background). */
+int sexgpu_background_map(sexgpu_ctx *ctx, float *back);
+
 /* Background only (makeback + subbackline): img (host, w*h) is replaced by
  * the background-subtracted frame; back/sigma (host, nbackx*nbacky, may be
  * NULL) receive the filtered mesh maps. */
@@ -215,6 +222,11 @@ int sexgpu_read_nnw(const char *path, sexgpu_nnw *net);
  * threshold, SEEING_FWHM and PIXEL_SCALE (src/cuda/cudaanalyse.cu:2901-2920). */
 int sexgpu_set_nnw(sexgpu_ctx *ctx, const sexgpu_nnw *net);
 
+/* Background mesh grid of a w x h frame and BACK_SIZE back_size
+ * (src/field.c:124-135): bw = min(back_size, w), bh = min(back_size, h),
+ * nbackx = (w - 1) / bw + 1, nbacky = (h - 1) / bh + 1.  Host only. */
+int sexgpu_background_meshes(int w, int h, int back_size, int *nbackx, int *nbacky);
+
 /* Background estimation and subtraction that allocates no device memory.
  *
  * No counterpart in the reference.  For callers that cannot call cudaMalloc or
@@ -226,11 +238,14 @@ int sexgpu_set_nnw(sexgpu_ctx *ctx, const sexgpu_nnw *net);
  * process exits.
  *
  * d_img (w*h floats) is the frame and d_sub (w*h) receives the background-
- * subtracted frame; d_back and d_sigma (nbackx*nbacky floats) receive the
- * filtered mesh maps; all four are device pointers.  stream is a
- * cudaStream_t (NULL: the default stream).  sum (host, may be NULL) receives
- * the global background, its rms and the thresholds, after which the call has
- * synchronised the stream.  Results equal those of sexgpu_background.
+ * subtracted frame; d_back and d_sigma receive the filtered mesh maps,
+ * nbackx*nbacky floats each (sexgpu_background_meshes gives the counts);
+ * mesh_capacity is the number of floats each of them holds, and a capacity
+ * below nbackx*nbacky returns SEXGPU_ERR_ARG before anything is written.  All
+ * four are device pointers.  stream is a cudaStream_t (NULL: the default
+ * stream).  sum (host, may be NULL) receives the global background, its rms
+ * and the thresholds, after which the call has synchronised the stream.
+ * Results equal those of sexgpu_background.
  *
  * Limits: w, h <= 16384, nbackx*nbacky <= 16384, h*nbackx <= 1048576;
  * larger frames return SEXGPU_ERR_NOALLOC_LIMIT.  The first call on a device
@@ -238,7 +253,7 @@ int sexgpu_set_nnw(sexgpu_ctx *ctx, const sexgpu_nnw *net);
  * stream capture).  All calls share the array: calls that overlap on the GPU
  * race and must be serialised by the caller. */
 int sexgpu_background_noalloc(const float *d_img, float *d_sub, int w, int h, const sexgpu_config *cfg,
-                              float *d_back, float *d_sigma, sexgpu_summary *sum, void *stream);
+                              float *d_back, float *d_sigma, int mesh_capacity, sexgpu_summary *sum, void *stream);
 
 /* One frame of a batch: inputs, the caller's catalogue buffer, and outputs. */
 typedef struct {
@@ -285,8 +300,12 @@ int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max);
  * sexgpu_extract_batch's workers use 1/n of the resident capacity each
  * (default 1).  "batch_sync": 1 (default) makes the batch workers wait for
  * their streams on blocking events, which leaves the host cores to the other
- * workers and keeps batch times steady; 0 spins.  Returns SEXGPU_ERR_ARG for
- * an unknown name or value. */
+ * workers and keeps batch times steady; 0 spins.  "loop_cap": n > 0 caps
+ * every union-find walk, union retry and CLEAN chain walk of the following
+ * extractions at n steps (a walk that runs out returns SEXGPU_ERR_LOOP and the
+ * context stays usable); 0 (default) keeps the built-in caps, which no valid
+ * frame reaches -- it exists to test the error path.  Returns SEXGPU_ERR_ARG
+ * for an unknown name or value. */
 int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value);
 
 #ifdef __cplusplus
