@@ -348,6 +348,8 @@ struct FrameParams {
     int clean_flag;
     double clean_param;
     double satur_level, gain, mag_zeropoint, aperture;
+    int naper;                      // PHOT_APERTURES diameters (>= 1); aperture = apertures[0]
+    double apertures[SEXGPU_MAXAPER];
     double autoparam0, autoparam1;
     int mask_type, numbering;
     int wtype;                      // weight map: 0 none, 1 MAP_VAR, 2 MAP_RMS, 3 MAP_WEIGHT

@@ -48,7 +48,8 @@ constexpr int DL_CAP0 = 256;                   // shared-memory tier (one warp p
 constexpr int DL_CAP1 = 64;                    // its small-object half (more warps resident per SM)
 constexpr int DL_MID = SX_DL_MID;              // arena tier with 64-thread CTAs up to here, 256 above
 constexpr int DL_ARENA_MAX = SX_DL_ARENA_MAX;  // at most 32767: element indices are 16-bit
-constexpr int DL_SWEEP_BYTES = 45;   // shared bytes per pixel, sweep
+constexpr int DL_SWEEP_BYTES = 62;   // shared bytes per pixel, sweep (with the neighbour table)
+constexpr int DL_NO_NBR = 0xffff;    // no neighbour in the object
 constexpr int DL_ASSIGN_BYTES = 34;  // shared bytes per pixel, assignment
 constexpr int DL_ARENA_BYTES = 48;   // global arena bytes per pixel (either pass)
 
@@ -120,13 +121,29 @@ __device__ __forceinline__ unsigned long long dl_term(float c, int e0) {
     return (unsigned long long)((u & 0x7fffffu) | 0x800000u) << sh;
 }
 
-// pixels first active at level L: activate, then join to active neighbours
+// pixels first active at level L: activate, then join to active neighbours.
+// nbr: the element index of every pixel's eight neighbours (DL_NO_NBR for
+// none), preloaded in shared memory with stride ncap, or null to look them up
+// in the frame-wide map
 template <int NT>
 __device__ __forceinline__ void dl_activate_union(const DebArgs &A, int off, int ucap, int L, int b0, int b1,
                                                   const unsigned short *order, int *par, const unsigned char *lev,
-                                                  int *status) {
+                                                  int *status, const unsigned short *nbr, int ncap) {
     for (int i = b0 + (int)threadIdx.x; i < b1; i += NT) par[order[i]] = order[i];
     __syncthreads();
+    if (nbr) {
+        for (int i = b0 + (int)threadIdx.x; i < b1; i += NT) {
+            const int e = order[i];
+            int nb[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) nb[q] = nbr[q * ncap + e];
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (nb[q] != DL_NO_NBR && lev[nb[q]] >= L) sunion(par, e, nb[q], ucap, status);
+        }
+        __syncthreads();
+        return;
+    }
     for (int i = b0 + (int)threadIdx.x; i < b1; i += NT) {
         const int e = order[i];
         const int p = (int)A.rpix[off + e];
@@ -208,6 +225,8 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     const int tid = threadIdx.x;
     const int off = A.R.off[r], P = A.R.size[r];
     const unsigned *pix = A.rpix + off;
+    // shared-memory tier: the whole state, and a neighbour table, on chip
+    const bool smem_tier = base != nullptr;
     if (!base) {  // global-memory arena: 48 B per element at the root's offset
         base = A.D.arena + (size_t)off * DL_ARENA_BYTES;
         cap = P;
@@ -224,6 +243,10 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     unsigned short *const nid = order + 3 * cap;
     unsigned short *const ndr0 = order + 4 * cap;
     unsigned char *lev = reinterpret_cast<unsigned char *>(order + 6 * cap);
+    // the eight neighbours of every pixel as element indices (16 B per pixel
+    // after the levels), in the shared-memory tier
+    unsigned short *const nbr =
+        smem_tier ? reinterpret_cast<unsigned short *>(lev + ((cap + 1) & ~1)) : nullptr;
     if (hyb) {
         par = reinterpret_cast<int *>(hyb);
         lev = hyb + 4 * (size_t)P;
@@ -291,6 +314,28 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     block_thresholds(A, A.R.dthresh[r], fdpeak, thr);
     __syncthreads();
     dl_levels<NT>(A, P, pix, thr, lev, order, lvcnt, lvstart, lvcur, true);
+    if (smem_tier) {
+        // one pass over the pixels with every lookup in flight together: the
+        // sizes and exact flux terms every element starts with (only roots
+        // are ever added to, and a pixel is no root before it is active), and
+        // the element index of each of its neighbours
+        for (int k = tid; k < P; k += NT) {
+            const int p = (int)pix[k];
+            const int y = (int)fdiv((unsigned)p, A.wdiv), x = p - y * A.w;
+            int nb[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int ddx[8] = {-1, 0, 1, -1, 1, -1, 0, 1}, ddy[8] = {-1, -1, -1, 0, 0, 1, 1, 1};
+                const int nx = x + ddx[q], ny = y + ddy[q];
+                nb[q] = (nx < 0 || ny < 0 || nx >= A.w || ny >= A.h) ? -1 : __ldg(A.pos2idx + (size_t)ny * A.w + nx);
+            }
+            sz[k] = 1;
+            acc[k] = dl_term(A.cd[p], e0);
+#pragma unroll
+            for (int q = 0; q < 8; q++) nbr[q * cap + k] = nb[q] >= 0 ? (unsigned short)(nb[q] - off) : DL_NO_NBR;
+        }
+        __syncthreads();
+    }
 
     int cur = 0, lastL = -1;
     for (int L = A.N - 1; L >= 0; L--) {
@@ -304,8 +349,10 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
         // level L+1 when the levels since the last populated one were empty
         for (int i = b0 + tid; i < b1; i += NT) {
             const int e = order[i];
-            sz[e] = 1;
-            acc[e] = dl_term(A.cd[pix[e]], e0);
+            if (!smem_tier) {
+                sz[e] = 1;
+                acc[e] = dl_term(A.cd[pix[e]], e0);
+            }
             rec[e] = (L << 24) | 0x00ffffff;  // active from level L, not absorbed yet
         }
         if (lastL > cl)
@@ -315,7 +362,7 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
                 NFL(prv)[i] = (NFL(prv)[i] & ~1u) | (lhs > value0 ? 1u : 0u);
             }
         // (b) activation and unions
-        dl_activate_union<NT>(A, off, ucap, L, b0, b1, order, par, lev, status);
+        dl_activate_union<NT>(A, off, ucap, L, b0, b1, order, par, lev, status, nbr, cap);
         // (c) roots that joined another component hand over size and flux
         for (int i = tid; i < nold + cnt; i += NT) {
             const int c = i < nold ? RL(prv)[i] : order[b0 + i - nold];
@@ -390,8 +437,11 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
 // ---------------------------------------------------------------------------
 // assignment: ownership of the kept branches, their preanalysis, gatherup
 // ---------------------------------------------------------------------------
+// gtab: shared memory for the centres and shapes of up to gcap kept
+// branches (32 B each), staged for the gatherup; null when the kernel has none
 template <int NT>
-__device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, unsigned char *base, int cap) {
+__device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, unsigned char *base, int cap,
+                                               unsigned char *gtab, int gcap) {
     __shared__ float thr[DB_MAXLEV];
     const int tid = threadIdx.x, lane = tid & 31;
     const int off = A.R.off[r], P = A.R.size[r];
@@ -609,6 +659,23 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
         A.O.n[o] = bcnt[k];
     }
     __syncthreads();
+    // the kept branches' centres and shapes in shared memory for the
+    // gatherup, when there is room (the same values and types as the columns)
+    const bool staged = gtab != nullptr && K <= gcap;
+    double *gmx = reinterpret_cast<double *>(gtab), *gmy = gmx + gcap;
+    float *gcxx = reinterpret_cast<float *>(gmy + gcap), *gcyy = gcxx + gcap, *gcxy = gcyy + gcap,
+          *gabc = gcxy + gcap;
+    if (staged && !whole) {
+        for (int i = tid; i < K; i += NT) {
+            gmx[i] = A.O.mx[ob + i];
+            gmy[i] = A.O.my[ob + i];
+            gcxx[i] = A.O.cxx[ob + i];
+            gcyy[i] = A.O.cyy[ob + i];
+            gcxy[i] = A.O.cxy[ob + i];
+            gabc[i] = A.O.abcor[ob + i];
+        }
+        __syncthreads();
+    }
     // gatherup (cudadeblend.cu:1262-1360): the nearest kept branch in the
     // elliptical metric, first in order on ties
     for (int e = tid; e < P; e += NT) {
@@ -618,14 +685,26 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
             const int y = (int)fdiv(p, A.wdiv), x = (int)p - y * A.w;
             int iclst = 0;
             float distmin = 1e+31f, dx, dy, dist;
-            for (int i = 0; i < K; i++) {
-                const int o = ob + i;
-                dx = x - A.O.mx[o];
-                dy = y - A.O.my[o];
-                dist = 0.5 * (A.O.cxx[o] * dx * dx + A.O.cyy[o] * dy * dy + A.O.cxy[o] * dx * dy) / A.O.abcor[o];
-                if (dist < distmin) {
-                    distmin = dist;
-                    iclst = i;
+            if (staged) {
+                for (int i = 0; i < K; i++) {
+                    dx = x - gmx[i];
+                    dy = y - gmy[i];
+                    dist = 0.5 * (gcxx[i] * dx * dx + gcyy[i] * dy * dy + gcxy[i] * dx * dy) / gabc[i];
+                    if (dist < distmin) {
+                        distmin = dist;
+                        iclst = i;
+                    }
+                }
+            } else {
+                for (int i = 0; i < K; i++) {
+                    const int o = ob + i;
+                    dx = x - A.O.mx[o];
+                    dy = y - A.O.my[o];
+                    dist = 0.5 * (A.O.cxx[o] * dx * dx + A.O.cyy[o] * dy * dy + A.O.cxy[o] * dx * dy) / A.O.abcor[o];
+                    if (dist < distmin) {
+                        distmin = dist;
+                        iclst = i;
+                    }
                 }
             }
             k = iclst;
@@ -679,12 +758,15 @@ __global__ void __launch_bounds__(NT) k_dl_sweep(const __grid_constant__ DebArgs
     }
 }
 
-// at most 64 registers (32 one-warp, 16 two-warp or 4 eight-warp CTAs per
-// SM): the assignment waits on its chain walks and gathers, so residency
-// pays more than the registers it costs
+// at most 64 registers (32 one-warp, 16 two-warp, 4 eight-warp or one
+// 32-warp CTAs per SM): the assignment waits on its chain walks and gathers,
+// so residency pays more than the registers it costs.
+// cap > 0: per-object state in dynamic shared memory of cap elements;
+// cap == 0: in the global arena, with the gatherup's table of up to gcap
+// kept branches in dynamic shared memory (DL_GTAB_BYTES each) when gcap > 0
 template <int NT>
-__global__ void __launch_bounds__(NT, NT == 32 ? 32 : NT == 64 ? 16 : 4) k_dl_assign(const __grid_constant__ DebArgs A, const RootLists L, int *cursor,
-                                                  int cap) {
+__global__ void __launch_bounds__(NT, NT == 32 ? 32 : NT == 64 ? 16 : NT == 256 ? 4 : 1)
+    k_dl_assign(const __grid_constant__ DebArgs A, const RootLists L, int *cursor, int cap, int gcap) {
     extern __shared__ __align__(16) unsigned char dl_smem[];
     __shared__ int s_item;
     for (;;) {
@@ -693,7 +775,7 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 32 : NT == 64 ? 16 : 4) k_dl_as
         const int r = s_item;
         __syncthreads();
         if (r < 0) break;
-        dl_assign_root<NT>(A, r, cap ? dl_smem : nullptr, cap);
+        dl_assign_root<NT>(A, r, cap ? dl_smem : nullptr, cap, (!cap && gcap > 0) ? dl_smem : nullptr, gcap);
         __syncthreads();
     }
 }
@@ -788,9 +870,11 @@ int deblend_split_launches(int nroots) { return nroots > 0 ? 3 + radix_launches(
 #define DL_SCUR(k) (counts + DL_NLISTS + (k))
 #define DL_ACUR(k) (counts + 2 * DL_NLISTS + (k))
 
-// The large size classes go first, on two side streams, so that their long
-// per-object latency overlaps the many small objects on the main stream; the
-// objects handed over by the compact sweeps are swept last, after the join.
+// Three streams run the size classes side by side, balanced by their measured
+// times on the c1 frame: side stream 0 the 128-bit global class and classes
+// 4-5, side stream 1 the largest objects (class 3) and then classes 1-2, the
+// main stream the shared-memory classes.  The objects handed over by the
+// compact sweeps are swept last, after the join.
 // hybrid tiers: largest object of each arena kernel (its parents and levels
 // take 5 B per pixel of shared memory)
 constexpr int DL_HYB3 = DL_ARENA_MAX;  // class 3: 1024-thread CTAs, about 160 KB
@@ -815,7 +899,7 @@ void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int n
         A, dl_lists(lists, counts, n, 4, 5), DL_SCUR(4), 0, glist, counts + 7, DL_HYB45);
     k_dl_sweep<1024><<<min(nroots, dl_grid(k_dl_sweep<1024>, 1024, h3, g5)), 1024, h3, S.side[1]>>>(
         A, dl_lists(lists, counts, n, 3), DL_SCUR(3), 0, glist, counts + 7, DL_HYB3);
-    k_dl_sweep<64><<<min(nroots, dl_grid(k_dl_sweep<64>, 64, h12, g1)), 64, h12, S.main>>>(
+    k_dl_sweep<64><<<min(nroots, dl_grid(k_dl_sweep<64>, 64, h12, g1)), 64, h12, S.side[1]>>>(
         A, dl_lists(lists, counts, n, 1, 2), DL_SCUR(1), 0, glist, counts + 7, DL_HYB12);
     k_dl_sweep<32><<<min(nroots, dl_grid(k_dl_sweep<32>, 32, m0, g0)), 32, m0, S.main>>>(
         A, dl_lists(lists, counts, n, 0), DL_SCUR(0), DL_CAP0, glist, counts + 7, 0);
@@ -828,25 +912,34 @@ void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int n
     k_deblend_sweep<<<grid3, DB_THREADS, 0, S.main>>>(A, glist, counts + 7, DL_SCUR(7));
 }
 
+// kept branches whose centres and shapes the gatherup stages in shared
+// memory (more go through global memory)
+constexpr int DL_GTAB_BYTES = 32;
+constexpr int DL_GTAB_BIG = 1024;  // classes 3, 4, 5: 32 KB
+constexpr int DL_GTAB_MID = 128;   // classes 1, 2: 4 KB
+
 void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S) {
     if (nroots <= 0) return;
-    static DevCache g0, g1, g2, g3, g4;
+    static DevCache g0, g1, g2, g3, g4, g5;
     const size_t n = (size_t)nroots;
     const size_t m0 = DL_CAP0 * DL_ASSIGN_BYTES, m1 = DL_CAP1 * DL_ASSIGN_BYTES;
+    const size_t tb = (size_t)DL_GTAB_BIG * DL_GTAB_BYTES, tm = (size_t)DL_GTAB_MID * DL_GTAB_BYTES;
     cudaEventRecord(S.fork, S.main);
     cudaStreamWaitEvent(S.side[0], S.fork, 0);
     cudaStreamWaitEvent(S.side[1], S.fork, 0);
     const int grid3 = min(nroots, dl_grid(k_deblend_assign, DB_THREADS, 0, g3));
     k_deblend_assign<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 6 * n, counts + 6, DL_ACUR(6));
     k_deblend_assign<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 7 * n, counts + 7, DL_ACUR(7));
-    k_dl_assign<256><<<min(nroots, dl_grid(k_dl_assign<256>, 256, 0, g2)), 256, 0, S.side[1]>>>(
-        A, dl_lists(lists, counts, n, 3, 4, 5), DL_ACUR(3), 0);
-    k_dl_assign<64><<<min(nroots, dl_grid(k_dl_assign<64>, 64, 0, g1)), 64, 0, S.main>>>(
-        A, dl_lists(lists, counts, n, 1, 2), DL_ACUR(1), 0);
+    k_dl_assign<256><<<min(nroots, dl_grid(k_dl_assign<256>, 256, tb, g2)), 256, tb, S.side[0]>>>(
+        A, dl_lists(lists, counts, n, 4, 5), DL_ACUR(4), 0, DL_GTAB_BIG);
+    k_dl_assign<1024><<<min(nroots, dl_grid(k_dl_assign<1024>, 1024, tb, g5)), 1024, tb, S.side[1]>>>(
+        A, dl_lists(lists, counts, n, 3), DL_ACUR(3), 0, DL_GTAB_BIG);
+    k_dl_assign<64><<<min(nroots, dl_grid(k_dl_assign<64>, 64, tm, g1)), 64, tm, S.side[1]>>>(
+        A, dl_lists(lists, counts, n, 1, 2), DL_ACUR(1), 0, DL_GTAB_MID);
     k_dl_assign<32><<<min(nroots, dl_grid(k_dl_assign<32>, 32, m0, g0)), 32, m0, S.main>>>(
-        A, dl_lists(lists, counts, n, 0), DL_ACUR(0), DL_CAP0);
+        A, dl_lists(lists, counts, n, 0), DL_ACUR(0), DL_CAP0, 0);
     k_dl_assign<32><<<min(nroots, dl_grid(k_dl_assign<32>, 32, m1, g4)), 32, m1, S.main>>>(
-        A, dl_lists(lists, counts, n, 8), DL_ACUR(8), DL_CAP1);
+        A, dl_lists(lists, counts, n, 8), DL_ACUR(8), DL_CAP1, 0);
     cudaEventRecord(S.join[0], S.side[0]);
     cudaEventRecord(S.join[1], S.side[1]);
     cudaStreamWaitEvent(S.main, S.join[0], 0);

@@ -225,22 +225,26 @@ struct EndArgs {
     FrameScalars *sc;
     int w, h, n, mask_type;
     double aperture, autoparam0, autoparam1, gain, zp, satur;
+    int naper;                          // apertures (>= 1); the first is `aperture`
+    double apertures[SEXGPU_MAXAPER];
     const float *wvar;  // calibrated variance map, or null
     KronBufs K;         // queued Kron boxes
     const sexgpu_nnw *nnw;  // CLASS_STAR network (device), or null
     double seeing, pixscale;
 };
 
-// src/cuda/cudaanalyse.cu:104-287 (computeaperflux, one aperture).  The
-// lanes of the warp evaluate 32 aperture pixels at a time (sub-pixel area,
-// masked value); the three double sums then take the terms one by one in the
-// raster order of the sequential loop, so the rounding is that loop's.
-__device__ void aper_warp(const EndArgs &A, int o, double mx, double my, int &flags) {
+// src/cuda/cudaanalyse.cu:104-287 (computeaperflux, aperture k of diameter
+// `diameter`).  The lanes of the warp evaluate 32 aperture pixels at a time
+// (sub-pixel area, masked value); the three double sums then take the terms
+// one by one in the raster order of the sequential loop, so the rounding is
+// that loop's.  The first aperture fills the catalogue columns; with several,
+// every one goes to O.aper.
+__device__ void aper_warp(const EndArgs &A, int o, double mx, double my, int &flags, double diameter, int k) {
     const int lane = threadIdx.x & 31, w = A.w, h = A.h;
     const int corrflag = (A.mask_type == 2);
     const float backsig = A.sc->backsig;
     const double var = backsig * backsig;
-    const float raper = A.aperture / 2.0;
+    const float raper = diameter / 2.0;
     const float raper2 = raper * raper;
     const float rintlim = raper - 0.75;
     const float rintlim2 = (rintlim > 0.0) ? rintlim * rintlim : 0.0;
@@ -320,10 +324,15 @@ __device__ void aper_warp(const EndArgs &A, int o, double mx, double my, int &fl
     if (lane != 0) return;
     if (A.O.dbkg) tv -= area * (double)A.O.dbkg[o];
     if (A.gain > 0.0 && tv > 0.0) sigtv += tv / A.gain;
-    A.O.flux_aper[o] = tv;
-    A.O.fluxerr_aper[o] = sqrt(sigtv);
-    A.O.mag_aper[o] = tv > 0.0 ? -2.5 * log10(tv) + A.zp : 99.0;
-    A.O.magerr_aper[o] = tv > 0.0 ? 1.086 * sqrt(sigtv) / tv : 99.0;
+    const float f = tv, fe = sqrt(sigtv), mg = tv > 0.0 ? -2.5 * log10(tv) + A.zp : 99.0,
+                me = tv > 0.0 ? 1.086 * sqrt(sigtv) / tv : 99.0;
+    if (k == 0) {
+        A.O.flux_aper[o] = f;
+        A.O.fluxerr_aper[o] = fe;
+        A.O.mag_aper[o] = mg;
+        A.O.magerr_aper[o] = me;
+    }
+    if (A.naper > 1) A.O.aper[(size_t)o * A.naper + k] = make_float4(f, fe, mg, me);
 }
 
 #define SX_RINT(x) (int)(floor(x + 0.5))
@@ -635,7 +644,7 @@ __global__ void __launch_bounds__(128, 8) k_endobject(EndArgs A) {
     if (A.O.fmaster[o] >= 0) return;
     int flags = A.O.flags[o];
     const double mx = A.O.mx[o], my = A.O.my[o];
-    aper_warp(A, o, mx, my, flags);
+    for (int k = 0; k < A.naper; k++) aper_warp(A, o, mx, my, flags, A.apertures[k], k);
     KronGeo g;
     kron_geo1(A, o, mx, my, g, flags);
     const int nn = kron_npix(g);
@@ -846,6 +855,17 @@ __global__ void k_write_rows(ObjBufs O, const unsigned *vals, int ns, float dthr
     // padding of the destination row as it was
     uint4 *dst = reinterpret_cast<uint4 *>(rows + k);
     for (int i = 0; i < (int)(sizeof(sexgpu_object) / 16); i++) dst[i] = u.v[i];
+}
+
+// every aperture of the catalogue rows, in catalogue order (naper per row)
+__global__ void k_write_apers(ObjBufs O, const unsigned *order, int ns, int naper, float4 *out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= ns) return;
+    const int o = (int)order[r];
+    for (int k = 0; k < naper; k++)
+        out[(size_t)r * naper + k] = naper > 1 ? O.aper[(size_t)o * naper + k]
+                                               : make_float4(O.flux_aper[o], O.fluxerr_aper[o], O.mag_aper[o],
+                                                             O.magerr_aper[o]);
 }
 
 // segmentation map: NUMBER of the owning object, 0 elsewhere

@@ -112,6 +112,7 @@ struct ObjBufs {
     float *dbkg;                        // LOCAL photometry background per object, or null (GLOBAL)
     MeshStat *lstat;                    // LOCAL annulus statistics
     unsigned long long *sortkey;
+    float4 *aper;                       // every aperture: (flux, error, mag, mag error), naper per object
 };
 
 void launch_background(BackBufs &B, const float *img, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st,

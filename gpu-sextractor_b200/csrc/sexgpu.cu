@@ -97,6 +97,7 @@ struct sexgpu_ctx {
     DevBuf o_sprob;                        // CLASS_STAR per object
     DevBuf o_raw, o_xraw, o_eraw;          // robust preanalysis / examineiso / photometry scratch per object
     DevBuf o_dbkg, o_lstat;                // BACKPHOTO_TYPE LOCAL: annulus mode, annulus statistics
+    DevBuf o_aper, aperrows;               // every aperture per object; per catalogue row
     bool cfg_local = false;                // the current extraction uses LOCAL photometry background
     DevBuf fitsraw;                        // FITS data block as stored (sexgpu_extract_fits)
     DevBuf rmsd, rmsnode, rmsdnode, rmsu, rmsmap;  // background rms map (sexgpu_background_rms)
@@ -241,6 +242,9 @@ int check_config(const sexgpu_config *cfg, int w, int h) {
     if (!(cfg->seeing_fwhm > 0.0)) return SEXGPU_ERR_ARG;
     if (cfg->back_photo_type < 0 || cfg->back_photo_type > 1) return SEXGPU_ERR_ARG;
     if (cfg->back_photo_type == 1 && (cfg->back_photo_thick < 1 || cfg->back_photo_thick > 256)) return SEXGPU_ERR_ARG;
+    if (cfg->naper < 0 || cfg->naper > SEXGPU_MAXAPER) return SEXGPU_ERR_ARG;
+    for (int k = 0; k < cfg->naper; k++)
+        if (!(cfg->phot_apertures[k] > 0.0)) return SEXGPU_ERR_ARG;
     return SEXGPU_OK;
 }
 
@@ -272,7 +276,10 @@ void make_params(const sexgpu_config *cfg, int w, int h, FrameParams &P) {
     P.satur_level = cfg->satur_level;
     P.gain = cfg->gain;
     P.mag_zeropoint = cfg->mag_zeropoint;
-    P.aperture = cfg->phot_aperture;
+    P.naper = cfg->naper > 0 ? cfg->naper : 1;
+    for (int k = 0; k < SEXGPU_MAXAPER; k++)
+        P.apertures[k] = k < cfg->naper ? cfg->phot_apertures[k] : cfg->phot_aperture;
+    P.aperture = P.apertures[0];
     P.autoparam0 = cfg->phot_autoparams[0];
     P.autoparam1 = cfg->phot_autoparams[1];
     P.mask_type = cfg->mask_type;
@@ -427,6 +434,9 @@ int alloc_objects(sexgpu_ctx *ctx, int nobj) {
     O.sprob = ctx->nnw_dev ? P<float>(ctx->o_sprob) : nullptr;
     EN(o_dbkg, n * sizeof(float));
     EN(o_lstat, n * sizeof(MeshStat));
+    const int naper = ctx->ps.Pm.naper > 1 ? ctx->ps.Pm.naper : 1;
+    EN(o_aper, n * naper * sizeof(float4));
+    O.aper = P<float4>(ctx->o_aper);
     O.dbkg = ctx->cfg_local ? P<float>(ctx->o_dbkg) : nullptr;
     O.lstat = P<MeshStat>(ctx->o_lstat);
     O.fluxerr_iso = P<float>(ctx->o_d[9]);
@@ -890,6 +900,8 @@ int pipe_end(sexgpu_ctx *ctx) {
     E.n = nobj;
     E.mask_type = Pm.mask_type;
     E.aperture = Pm.aperture;
+    E.naper = Pm.naper;
+    for (int k = 0; k < SEXGPU_MAXAPER; k++) E.apertures[k] = Pm.apertures[k];
     E.autoparam0 = Pm.autoparam0;
     E.autoparam1 = Pm.autoparam1;
     E.gain = Pm.gain;
@@ -1053,6 +1065,8 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     free_buf(ctx->o_eraw);
     free_buf(ctx->o_dbkg);
     free_buf(ctx->o_lstat);
+    free_buf(ctx->o_aper);
+    free_buf(ctx->aperrows);
     free_buf(ctx->fitsraw);
     free_buf(ctx->rmsd);
     free_buf(ctx->rmsnode);
@@ -1232,6 +1246,28 @@ int sexgpu_background_rms(sexgpu_ctx *ctx, float *rms) {
     k_rms_map<<<grid1(N, 256), 256, 0, st>>>(P<float>(ctx->rmsnode), P<float>(ctx->rmsdnode), ps.B.colk, ps.B.coldx,
                                             Pm.nbx, w, N, P<float>(ctx->rmsmap), 0);
     CK(cudaMemcpyAsync(rms, ctx->rmsmap.p, (size_t)N * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SEXGPU_OK;
+}
+
+int sexgpu_copy_apertures(sexgpu_ctx *ctx, float *out, int max_rows, int *nrows, int *naper) {
+    if (!ctx || (!out && max_rows > 0)) return SEXGPU_ERR_ARG;
+    const PipeState &ps = ctx->ps;
+    if (ps.stage != 6) {
+        ctx->err = "no finished extraction";
+        return SEXGPU_ERR_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    const int ns = ps.ns, na = ps.Pm.naper;
+    if (nrows) *nrows = ns;
+    if (naper) *naper = na;
+    if (ns > max_rows) return SEXGPU_ERR_CAPACITY;
+    if (ns == 0) return SEXGPU_OK;
+    cudaStream_t st = ctx->stream;
+    EN(aperrows, (size_t)ns * na * sizeof(float4));
+    k_write_apers<<<grid1(ns, 128), 128, 0, st>>>(ctx->O, P<unsigned>(ctx->svals), ns, na,
+                                                  P<float4>(ctx->aperrows));
+    CK(cudaMemcpyAsync(out, ctx->aperrows.p, (size_t)ns * na * sizeof(float4), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return SEXGPU_OK;
 }

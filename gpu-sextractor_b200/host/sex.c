@@ -88,7 +88,15 @@ static void setpref(prefs_t *p, const char *key, char *val)
     else if (!strcasecmp(key, "CLEAN_PARAM")) c->clean_param = atof(val);
     else if (!strcasecmp(key, "MASK_TYPE"))
         c->mask_type = !strncasecmp(val, "NONE", 4) ? 0 : !strncasecmp(val, "BLANK", 5) ? 1 : 2;
-    else if (!strcasecmp(key, "PHOT_APERTURES")) c->phot_aperture = atof(val);
+    else if (!strcasecmp(key, "PHOT_APERTURES")) {
+        /* one diameter, or a list: the FLUX_APER columns become vectors */
+        char *tok, *save = NULL;
+        c->naper = 0;
+        for (tok = strtok_r(val, ", \t", &save); tok && c->naper < SEXGPU_MAXAPER; tok = strtok_r(NULL, ", \t", &save))
+            c->phot_apertures[c->naper++] = atof(tok);
+        if (c->naper > 0) c->phot_aperture = c->phot_apertures[0];
+        if (c->naper == 1) c->naper = 0;
+    }
     else if (!strcasecmp(key, "PHOT_AUTOPARAMS")) {
         c->phot_autoparams[0] = atof(val);
         if ((comma = strchr(val, ','))) c->phot_autoparams[1] = atof(comma + 1);
@@ -403,10 +411,24 @@ static const col_t COLS[] = {
     {NULL, NULL, NULL, NULL}};
 
 static int g_ext = 1;  /* extension of the rows being written (EXT_NUMBER) */
+/* every aperture of the rows being written (rows x g_naper x 4: flux, error,
+   mag, mag error), when PHOT_APERTURES has several diameters */
+static const float *g_aper;
+static int g_naper = 1;
 
-static void print_col(FILE *f, int c, const sexgpu_object *o)
+/* values a column holds per row: the aperture columns are vectors */
+static int col_width(int c) { return (c >= 14 && c <= 17 && g_aper) ? g_naper : 1; }
+
+static void print_col(FILE *f, int c, const sexgpu_object *o, int row)
 {
     const char *fmt = COLS[c].fmt;
+    if (col_width(c) > 1) {
+        for (int k = 0; k < g_naper; k++) {
+            if (k) fputc(' ', f);
+            fprintf(f, fmt, g_aper[((size_t)row * g_naper + k) * 4 + (c - 14)]);
+        }
+        return;
+    }
     switch (c) {
     case 0: fprintf(f, fmt, o->number); break;
     case 1: fprintf(f, fmt, o->mx + 1.0); break;
@@ -608,7 +630,7 @@ static void ldac_write_ext(FILE *f, const sexgpu_object *objs, int n, const int 
     fwrite(hdr, 1, 80 * nhdr, f);
     pad_block(f, 80 * nhdr, 0);
     /* LDAC_OBJECTS */
-    for (k = 0; k < ns; k++) rowbytes += col_type(sel[k]) == 'D' ? 8 : 4;
+    for (k = 0; k < ns; k++) rowbytes += (col_type(sel[k]) == 'D' ? 8 : 4) * col_width(sel[k]);
     ncard = 0;
     card_str(f, "XTENSION", "BINTABLE"); ncard++;
     card_int(f, "BITPIX", 8); ncard++;
@@ -623,7 +645,7 @@ static void ldac_write_ext(FILE *f, const sexgpu_object *objs, int n, const int 
         snprintf(key, sizeof key, "TTYPE%d", k + 1);
         card_str(f, key, COLS[sel[k]].name); ncard++;
         snprintf(key, sizeof key, "TFORM%d", k + 1);
-        snprintf(form, sizeof form, "1%c", col_type(sel[k]));
+        snprintf(form, sizeof form, "%d%c", col_width(sel[k]), col_type(sel[k]));
         card_str(f, key, form); ncard++;
         if (*COLS[sel[k]].unit) {
             snprintf(key, sizeof key, "TUNIT%d", k + 1);
@@ -637,6 +659,13 @@ static void ldac_write_ext(FILE *f, const sexgpu_object *objs, int n, const int 
         for (k = 0; k < ns; k++) {
             double v = col_value(sel[k], &objs[i]);
             char t = col_type(sel[k]);
+            if (col_width(sel[k]) > 1) {
+                for (int a = 0; a < g_naper; a++) {
+                    float fv = g_aper[((size_t)i * g_naper + a) * 4 + (sel[k] - 14)];
+                    put_be(f, &fv, 4);
+                }
+                continue;
+            }
             if (t == 'J') {
                 int32_t iv = (int32_t)v;
                 put_be(f, &iv, 4);
@@ -680,12 +709,12 @@ static void write_ascii(FILE *cat, const prefs_t *p, const sexgpu_object *objs, 
         return;
     }
     if (head && !strcasecmp(p->catalog_type, "ASCII_HEAD"))
-        for (k = 0; k < ns; k++)
-            fprintf(cat, "#%4d %-22s %-58s [%s]\n", k + 1, COLS[sel[k]].name, COLS[sel[k]].comment, COLS[sel[k]].unit);
+        for (k = 0, i = 1; k < ns; i += col_width(sel[k]), k++)
+            fprintf(cat, "#%4d %-22s %-58s [%s]\n", i, COLS[sel[k]].name, COLS[sel[k]].comment, COLS[sel[k]].unit);
     for (i = 0; i < n; i++) {
         for (k = 0; k < ns; k++) {
             if (k) fputc(' ', cat);
-            print_col(cat, sel[k], &objs[i]);
+            print_col(cat, sel[k], &objs[i], i);
         }
         fputc('\n', cat);
     }
@@ -699,8 +728,8 @@ static int run_mef(const prefs_t *p, sexgpu_ctx *ctx, fits_image *ims, int nim)
 {
     sexgpu_batch_frame *fr = (sexgpu_batch_frame *)calloc((size_t)nim, sizeof(sexgpu_batch_frame));
     int k, rc, tot = 0;
-    if (strcasecmp(p->check_type, "NONE") || p->cfg.weight_type)
-        die("check images and weight maps need a single-image FITS file", NULL);
+    if (strcasecmp(p->check_type, "NONE") || p->cfg.weight_type || p->cfg.naper > 1)
+        die("check images, weight maps and several PHOT_APERTURES need a single-image FITS file", NULL);
     for (k = 0; k < nim; k++) {
         const size_t npix = (size_t)ims[k].w * ims[k].h;
         const int cap = (int)(npix / (size_t)(p->cfg.detect_minarea > 0 ? p->cfg.detect_minarea : 1) / 2 + 16);
@@ -851,6 +880,14 @@ int main(int argc, char **argv)
     if (rc != SEXGPU_OK) {
         fprintf(stderr, "sex: extraction failed (%d): %s\n", rc, sexgpu_last_error(ctx));
         return EXIT_FAILURE;
+    }
+    if (p.cfg.naper > 1) {
+        /* the aperture vectors of the rows (src/photom.c:36, one call per
+           diameter in the reference's own CPU code) */
+        float *ap = (float *)malloc(sizeof(float) * 4 * (size_t)(n + 1) * p.cfg.naper);
+        if (!ap || sexgpu_copy_apertures(ctx, ap, n, NULL, &g_naper) != SEXGPU_OK)
+            die("apertures: ", sexgpu_last_error(ctx));
+        g_aper = ap;
     }
     if (strcasecmp(p.catalog_type, "NONE")) {
         FILE *cat = !strcmp(p.catalog_name, "STDOUT") ? stdout : fopen(p.catalog_name, "w");

@@ -43,6 +43,7 @@ class Config(C.Structure):
         ("weight_type", C.c_int), ("numbering", C.c_int),
         ("seeing_fwhm", C.c_double), ("pixel_scale", C.c_double),
         ("back_photo_type", C.c_int), ("back_photo_thick", C.c_int),
+        ("naper", C.c_int), ("phot_apertures", C.c_double * 16),
     ]
 
 
@@ -123,7 +124,7 @@ EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extra
            "sexgpu_extract_device", "sexgpu_copy_results", "sexgpu_background", "sexgpu_filter",
            "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times", "sexgpu_set_param",
            "sexgpu_read_nnw", "sexgpu_set_nnw", "sexgpu_extract_fits", "sexgpu_background_rms",
-           "sexgpu_background_noalloc", "sexgpu_background_meshes", "sexgpu_background_map",
+           "sexgpu_background_noalloc", "sexgpu_background_meshes", "sexgpu_background_map", "sexgpu_copy_apertures",
            "sexgpu_extract_batch"]
 
 _lib = None
@@ -180,6 +181,10 @@ def make_config(**kw):
     for k, v in d.items():
         if k == "phot_autoparams":
             cfg.phot_autoparams[0], cfg.phot_autoparams[1] = v
+        elif k == "phot_apertures":
+            cfg.naper = len(v)
+            for i, a in enumerate(v):
+                cfg.phot_apertures[i] = a
         else:
             setattr(cfg, k, v)
     cfg.conv = _f(mask)
@@ -291,6 +296,18 @@ class Context:
         if want_maps:
             return objs[:n.value], seg, s, sub, cd
         return objs[:n.value], seg, s
+
+    def apertures(self):
+        """Every aperture of the last extraction's catalogue rows: float32
+        array (rows, naper, 4) of flux, error, magnitude, magnitude error."""
+        n, na = C.c_int(), C.c_int()
+        rc = lib().sexgpu_copy_apertures(self.h, None, 0, C.byref(n), C.byref(na))
+        if rc not in (OK, -5):
+            _check(rc, self.h, "sexgpu_copy_apertures")
+        out = np.zeros((n.value, na.value, 4), np.float32)
+        _check(lib().sexgpu_copy_apertures(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), n.value, None, None),
+               self.h, "sexgpu_copy_apertures")
+        return out
 
     def background_map(self, shape):
         """Background map of the last extraction (h, w float32): the value

@@ -44,6 +44,7 @@ extern "C" {
 #define SEXGPU_ERR_LOAD      -10   /* a tile load did not complete in time: destroy the context */
 
 #define SEXGPU_NISO 8
+#define SEXGPU_MAXAPER 16   /* PHOT_APERTURES diameters per extraction */
 
 /* Extraction settings; names follow the .sex keywords (src/preflist.h). */
 typedef struct {
@@ -76,6 +77,12 @@ typedef struct {
     double  pixel_scale;        /* PIXEL_SCALE (arcsec/pixel); <= 0 means 1 (no WCS here) */
     int     back_photo_type;    /* BACKPHOTO_TYPE: 0 GLOBAL, 1 LOCAL (annulus mode per object) */
     int     back_photo_thick;   /* BACKPHOTO_THICK: LOCAL annulus thickness, 1..256 pixels */
+    /* PHOT_APERTURES with several diameters (the reference allows one,
+       src/define.h:50): naper of phot_apertures[]; 0 means phot_aperture
+       alone.  The catalogue row carries the first aperture; all of them are
+       read with sexgpu_copy_apertures. */
+    int     naper;
+    double  phot_apertures[SEXGPU_MAXAPER];
 } sexgpu_config;
 
 /* One catalogue row (0-based pixel coordinates unless stated). */
@@ -279,6 +286,14 @@ typedef struct {
  * own status is in frames[i].status).  Not for use on the same context from
  * two threads at once. */
 int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframes, int workers);
+
+/* Aperture photometry of every aperture of the last extraction (FLUX_APER,
+ * FLUXERR_APER, MAG_APER, MAGERR_APER as vectors), in catalogue order: out
+ * receives rows x naper x 4 floats (flux, error, magnitude, magnitude
+ * error) for up to max_rows rows; *nrows and *naper (may be NULL) receive
+ * the catalogue length and the number of apertures.  SEXGPU_ERR_CAPACITY
+ * when the catalogue is longer than max_rows (nothing is copied). */
+int sexgpu_copy_apertures(sexgpu_ctx *ctx, float *out, int max_rows, int *nrows, int *naper);
 
 /* Last CUDA error string of this context (empty if none). */
 const char *sexgpu_last_error(sexgpu_ctx *ctx);

@@ -43,6 +43,8 @@ extern "C" {
 
 #define ORC_NISO 8
 
+#define ORC_MAXAPER 16
+
 typedef struct {
     /* background (src/preflist.h:48-59) */
     int     back_size;          /* BACK_SIZE, square meshes */
@@ -83,6 +85,10 @@ typedef struct {
     /* photometry background (src/preflist.h BACKPHOTO_TYPE, BACKPHOTO_THICK) */
     int     back_photo_type;    /* 0 GLOBAL, 1 LOCAL */
     int     back_photo_thick;   /* annulus thickness (pixels) */
+    /* several PHOT_APERTURES diameters: naper of phot_apertures[] (0: the
+       single phot_aperture); the row's FLUX_APER columns hold the first */
+    int     naper;
+    double  phot_apertures[ORC_MAXAPER];
 } orc_config;
 
 /* Star/galaxy network (src/types.h:930 brainstruct; src/neurro.c) */
@@ -118,6 +124,7 @@ typedef struct {
     float   flux_aper, fluxerr_aper, mag_aper, magerr_aper;
     float   kronfactor, flux_auto, fluxerr_auto, mag_auto, magerr_auto;
     float   elong, ellip, polar;
+    float   aper[ORC_MAXAPER][4];  /* every aperture: flux, error, mag, mag error */
 } orc_object;
 
 typedef struct {

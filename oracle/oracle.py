@@ -30,6 +30,7 @@ class OrcConfig(C.Structure):
         ("weight_type", C.c_int), ("numbering", C.c_int),
         ("seeing_fwhm", C.c_double), ("pixel_scale", C.c_double), ("nnw", C.c_void_p),
         ("back_photo_type", C.c_int), ("back_photo_thick", C.c_int),
+        ("naper", C.c_int), ("phot_apertures", C.c_double * 16),
     ]
 
 
@@ -76,6 +77,7 @@ OBJECT_FIELDS = [
     ("flux_aper", "f4"), ("fluxerr_aper", "f4"), ("mag_aper", "f4"), ("magerr_aper", "f4"),
     ("kronfactor", "f4"), ("flux_auto", "f4"), ("fluxerr_auto", "f4"), ("mag_auto", "f4"),
     ("magerr_auto", "f4"), ("elong", "f4"), ("ellip", "f4"), ("polar", "f4"),
+    ("aper", "f4", (16, 4)),
 ]
 OBJECT_DTYPE = np.dtype(OBJECT_FIELDS, align=True)
 
@@ -154,6 +156,10 @@ def make_config(**kw):
     for k, v in d.items():
         if k == "phot_autoparams":
             cfg.phot_autoparams[0], cfg.phot_autoparams[1] = v
+        elif k == "phot_apertures":
+            cfg.naper = len(v)
+            for i, a in enumerate(v):
+                cfg.phot_apertures[i] = a
         else:
             setattr(cfg, k, v)
     cfg.conv = _f(mask)

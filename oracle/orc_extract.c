@@ -788,7 +788,7 @@ static void run_clean(const frame_t *F, obj_t *o, int n)
  * Pixels at or below -BIG (blank or NaN input pixels) are replaced like
  * pixels of other objects, as the CPU computeaperflux does (src/photom.c:128-
  * 145): the GPU kernel drops that test and would sum the -BIG sentinel. */
-static void aperflux(const frame_t *F, const int *alloc, obj_t *o, int self)
+static void aperflux(const frame_t *F, const int *alloc, obj_t *o, int self, double diameter, int k)
 {
     const orc_config *cfg = F->cfg;
     float r2, raper, raper2, rintlim, rintlim2, rextlim2, dx, dx1, dy, dy2, offsetx, offsety, scalex, scaley, scale2, locarea;
@@ -797,7 +797,7 @@ static void aperflux(const frame_t *F, const int *alloc, obj_t *o, int self)
 
     corrflag = (cfg->mask_type == 2);
     var = F->backsig * F->backsig;
-    raper = cfg->phot_aperture / 2.0;
+    raper = diameter / 2.0;
     raper2 = raper * raper;
     rintlim = raper - 0.75;
     rintlim2 = (rintlim > 0.0) ? rintlim * rintlim : 0.0;
@@ -860,10 +860,16 @@ static void aperflux(const frame_t *F, const int *alloc, obj_t *o, int self)
     tv -= area * o->dbkg;
     if (cfg->gain > 0.0 && tv > 0.0)
         sigtv += tv / cfg->gain;
-    o->flux_aper = tv;
-    o->fluxerr_aper = sqrt(sigtv);
-    o->mag_aper = tv > 0.0 ? -2.5 * log10(tv) + cfg->mag_zeropoint : 99.0;
-    o->magerr_aper = tv > 0.0 ? 1.086 * sqrt(sigtv) / tv : 99.0;
+    o->aper[k][0] = tv;
+    o->aper[k][1] = sqrt(sigtv);
+    o->aper[k][2] = tv > 0.0 ? -2.5 * log10(tv) + cfg->mag_zeropoint : 99.0;
+    o->aper[k][3] = tv > 0.0 ? 1.086 * sqrt(sigtv) / tv : 99.0;
+    if (k == 0) {
+        o->flux_aper = o->aper[0][0];
+        o->fluxerr_aper = o->aper[0][1];
+        o->mag_aper = o->aper[0][2];
+        o->magerr_aper = o->aper[0][3];
+    }
 }
 
 #define RINT(x) (int)(floor(x + 0.5))
@@ -1069,7 +1075,12 @@ static void endobject(const frame_t *F, const int *alloc, obj_t *o, int self)
     o->polar = (o->a * o->a - o->b * o->b) / (o->a * o->a + o->b * o->b);
     o->fluxerr_iso = sqrt(o->fluxerr);
     isocorflux(o);
-    aperflux(F, alloc, o, self);
+    {
+        /* every PHOT_APERTURES diameter, in order */
+        int k, na = cfg->naper > 0 ? cfg->naper : 1;
+        for (k = 0; k < na; k++)
+            aperflux(F, alloc, o, self, cfg->naper > 0 ? cfg->phot_apertures[k] : cfg->phot_aperture, k);
+    }
     autoflux(F, alloc, o, self);
     if (o->peak + o->bkg >= cfg->satur_level)
         o->flags |= ORC_OBJ_SATUR;
@@ -1406,6 +1417,7 @@ int orc_extract(const float *img, const float *var, int w, int h, const orc_conf
             q->kronfactor = o->kron; q->flux_auto = o->flux_auto; q->fluxerr_auto = o->fluxerr_auto;
             q->mag_auto = o->mag_auto; q->magerr_auto = o->magerr_auto;
             q->elong = o->elong; q->ellip = o->ellip; q->polar = o->polar;
+            memcpy(q->aper, o->aper, sizeof(q->aper));
         }
         if (segmap) {
             for (p = 0; p < N; p++)
@@ -1526,7 +1538,7 @@ int orc_photometry(const float *sub, int w, int h, const orc_config *cfg, float 
         o.cyy = po[i].cyy;
         o.cxy = po[i].cxy;
         o.dbkg = po[i].dbkg;
-        aperflux(&F, alloc, &o, 0);
+        aperflux(&F, alloc, &o, 0, cfg->phot_aperture, 0);
         autoflux(&F, alloc, &o, 0);
         po[i].flux_aper = o.flux_aper;
         po[i].fluxerr_aper = o.fluxerr_aper;

@@ -70,6 +70,7 @@ typedef struct {
     float mag_iso, magerr_iso, fluxerr_iso;
     float elong, ellip, polar;
     float class_star;
+    float aper[ORC_MAXAPER][4];  /* every aperture: flux, error, mag, mag error */
 } obj_t;
 
 typedef struct {

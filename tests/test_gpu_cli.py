@@ -86,8 +86,12 @@ def read_ldac_objects(path):
         nbytes = int(cards.get("NAXIS1", 0)) * int(cards.get("NAXIS2", 0)) if cards.get("NAXIS") == "2" else 0
         if cards.get("EXTNAME") == "LDAC_OBJECTS":
             code = {"J": ">i4", "E": ">f4", "D": ">f8"}
-            dt = np.dtype([(cards["TTYPE%d" % (k + 1)], code[cards["TFORM%d" % (k + 1)][-1]])
-                           for k in range(int(cards["TFIELDS"]))])
+            fields = []
+            for k in range(int(cards["TFIELDS"])):
+                form = cards["TFORM%d" % (k + 1)]
+                rep = int(form[:-1] or 1)
+                fields.append((cards["TTYPE%d" % (k + 1)], code[form[-1]]) + (((rep,),) if rep > 1 else ()))
+            dt = np.dtype(fields)
             assert dt.itemsize == int(cards["NAXIS1"])
             return np.frombuffer(raw[pos:pos + nbytes], dt)
         pos += (nbytes + 2879) // 2880 * 2880
@@ -236,3 +240,115 @@ def test_cli_multi_extension_file(tmp_path, masks):
         assert [int(r[3]) for r in mine] == list(o["flags"])
         assert np.array_equal(np.array([float(r[2]) for r in mine], np.float32),
                               np.array(["%12.7g" % v for v in o["flux_iso"]], float).astype(np.float32))
+
+
+def read_fits_f32(path, w, h):
+    with open(path, "rb") as f:
+        raw = f.read()
+    return np.frombuffer(raw[2880:2880 + 4 * w * h], ">f4").reshape(h, w).astype(np.float32)
+
+
+def test_cli_check_image_list(tmp_path, masks):
+    """CHECKIMAGE_TYPE and CHECKIMAGE_NAME lists (src/check.c:181-489): the
+    segmentation, background (src/readimage.c:114, the backline the
+    reference subtracts), background-subtracted, filtered and rms images of
+    one run, each against the oracle, bit for bit."""
+    if not os.path.exists(SEX):
+        subprocess.check_call(["make", "-s", "-C", os.path.dirname(SEX)])
+    w, h = 420, 310
+    img = synth.frame_c0(seed=13, w=w, h=h, nsrc=300)
+    fits = tmp_path / "img.fits"
+    write_fits(str(fits), img)
+    conv = tmp_path / "g.conv"
+    m = masks["gauss_2.5_5x5"]
+    conv.write_text("CONV NONORM\n" + "\n".join(" ".join("%.9g" % v for v in row) for row in m) + "\n")
+    kinds = ["SEGMENTATION", "BACKGROUND", "-BACKGROUND", "FILTERED", "BACKGROUND_RMS"]
+    names = [str(tmp_path / ("chk%d.fits" % i)) for i in range(len(kinds))]
+    cfgf = tmp_path / "t.sex"
+    cfgf.write_text("CATALOG_TYPE NONE\nFILTER_NAME %s\nBACK_SIZE 50\nBACK_FILTERSIZE 5\n"
+                    "CHECKIMAGE_TYPE %s\nCHECKIMAGE_NAME %s\nVERBOSE_TYPE QUIET\n"
+                    % (conv, ", ".join(kinds), ",".join(names)))
+    subprocess.check_call([SEX, str(fits), "-c", str(cfgf)], cwd=str(tmp_path))
+    kw = dict(conv=m, back_size=50, back_filtersize=5)
+    o, oseg, s, osub, ocd = O.extract(img, want_maps=True, **kw)
+    assert np.array_equal(read_fits_i32(names[0], w, h), oseg)
+    assert read_fits_f32(names[1], w, h).tobytes() == O.background_map(img, **kw).tobytes()
+    assert read_fits_f32(names[2], w, h).tobytes() == osub.tobytes()
+    assert read_fits_f32(names[3], w, h).tobytes() == ocd.tobytes()
+    assert read_fits_f32(names[4], w, h).tobytes() == O.background_rms(img, **kw).tobytes()
+
+
+def test_cli_reference_test_image(tmp_path, masks):
+    """The reference's own test image (tests/galaxies.fits, BITPIX 16 with
+    BSCALE/BZERO), copied into oracle/_ref by the oracle recipe, through the
+    sex command line with and without its weight map: the catalogue and the
+    segmentation against the oracle on the same pixels."""
+    src = os.path.join(ROOT, "oracle", "_ref", "galaxies.fits")
+    wsrc = os.path.join(ROOT, "oracle", "_ref", "galaxies.weight.fits")
+    if not os.path.exists(src):
+        pytest.skip("the reference's test image is not in oracle/_ref")
+    if not os.path.exists(SEX):
+        subprocess.check_call(["make", "-s", "-C", os.path.dirname(SEX)])
+    from test_oracle_pins import read_fits_image
+    hdr, raw = read_fits_image(src)
+    w, h = int(hdr["NAXIS1"]), int(hdr["NAXIS2"])
+    img = O.fits_to_float(raw, int(hdr["BITPIX"]), float(hdr["BSCALE"]), float(hdr["BZERO"])).reshape(h, w)
+    conv = tmp_path / "d.conv"
+    m = masks["default"]
+    conv.write_text("CONV NONORM\n" + "\n".join(" ".join("%.9g" % v for v in row) for row in m) + "\n")
+    for weighted in (False, True):
+        cat, seg = tmp_path / "g.cat", tmp_path / "seg.fits"
+        cfg = ("CATALOG_TYPE ASCII\nFILTER_NAME %s\nDETECT_MINAREA 5\nDETECT_THRESH 1.5\nANALYSIS_THRESH 2\n"
+               "BACK_SIZE 64\nCHECKIMAGE_TYPE SEGMENTATION\nCHECKIMAGE_NAME %s\nVERBOSE_TYPE QUIET\n" % (conv, seg))
+        kw = dict(conv=m, detect_minarea=5, detect_thresh=1.5, analysis_thresh=2.0, back_size=64)
+        wm = None
+        if weighted:
+            cfg += "WEIGHT_TYPE MAP_WEIGHT\nWEIGHT_IMAGE %s\n" % wsrc
+            whdr, wraw = read_fits_image(wsrc)
+            wm = O.fits_to_float(wraw, int(whdr["BITPIX"])).reshape(h, w)
+            kw["weight_type"] = 3
+        cfgf = tmp_path / "t.sex"
+        cfgf.write_text(cfg)
+        subprocess.check_call([SEX, src, "-c", str(cfgf), "-CATALOG_NAME", str(cat)], cwd=str(tmp_path))
+        rows = [l.split() for l in cat.read_text().splitlines() if l.strip()]
+        o, oseg, s = O.extract(img, weight=wm, **kw)
+        assert len(rows) == len(o) > 50
+        assert [int(r[0]) for r in rows] == list(o["number"])
+        assert [int(r[23]) for r in rows] == list(o["flags"])
+        assert np.array_equal(read_fits_i32(str(seg), w, h), oseg)
+
+
+def test_cli_several_apertures(tmp_path, masks):
+    """PHOT_APERTURES 3,6,12: FLUX_APER and MAG_APER become vectors in the
+    ASCII_HEAD catalogue (three columns each, numbered as such in the header)
+    and in FITS_LDAC (TFORM 3E), against the oracle's apertures."""
+    if not os.path.exists(SEX):
+        subprocess.check_call(["make", "-s", "-C", os.path.dirname(SEX)])
+    img = synth.frame_c0(seed=17, w=500, h=400, nsrc=400)
+    fits = tmp_path / "img.fits"
+    write_fits(str(fits), img)
+    conv = tmp_path / "g.conv"
+    m = masks["default"]
+    conv.write_text("CONV NONORM\n" + "\n".join(" ".join("%.9g" % v for v in row) for row in m) + "\n")
+    par = tmp_path / "t.param"
+    par.write_text("NUMBER\nFLUX_APER(3)\nMAG_APER(3)\nFLAGS\n")
+    cfgf = tmp_path / "t.sex"
+    cfgf.write_text("FILTER_NAME %s\nPARAMETERS_NAME %s\nPHOT_APERTURES 3, 6,12\nMAG_ZEROPOINT 25\n"
+                    "VERBOSE_TYPE QUIET\n" % (conv, par))
+    cat, ldac = tmp_path / "t.cat", tmp_path / "t.ldac"
+    subprocess.check_call([SEX, str(fits), "-c", str(cfgf), "-CATALOG_TYPE", "ASCII_HEAD", "-CATALOG_NAME", str(cat)],
+                          cwd=str(tmp_path))
+    subprocess.check_call([SEX, str(fits), "-c", str(cfgf), "-CATALOG_TYPE", "FITS_LDAC", "-CATALOG_NAME",
+                           str(ldac)], cwd=str(tmp_path))
+    lines = cat.read_text().splitlines()
+    head = [l for l in lines if l.startswith("#")]
+    assert [l.split()[1] for l in head] == ["1", "2", "5", "8"]
+    rows = [l.split() for l in lines if l.strip() and not l.startswith("#")]
+    o, _, _ = O.extract(img, conv=m, phot_apertures=[3.0, 6.0, 12.0], mag_zeropoint=25.0)
+    assert len(rows) == len(o) > 50
+    for r, q in zip(rows, o):
+        assert r[1:4] == ["%.7g" % q["aper"][k][0] for k in range(3)]
+        assert r[4:7] == ["%.4f" % q["aper"][k][2] for k in range(3)]
+    t = read_ldac_objects(str(ldac))
+    assert t["FLUX_APER"].shape == (len(o), 3)
+    assert np.array_equal(t["FLUX_APER"].astype(np.float32), o["aper"][:, :3, 0])

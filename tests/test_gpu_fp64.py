@@ -8,8 +8,8 @@ degree for THETA, cross terms against the diagonal terms).  A column may
 exceed it on at most 0.1% of the rows, only for the ill-conditioned
 measurements named here (the FWHM fit, the angle of near-round objects, the
 inverse moment matrix CXX/CYY/CXY where its determinant nearly cancels, a
-pixel on an aperture boundary); the RMS stays below 1e-6 for all columns but
-FWHM.
+pixel on an aperture boundary); the RMS stays below 1e-6 for all the other
+columns.
 """
 import numpy as np
 import pytest
@@ -41,5 +41,5 @@ def test_catalogue_against_fp64_oracle(gpu_ctx, masks, case):
             assert r["over"] <= max(3, 0.001 * r["n"]), (name, r)
         else:
             assert r["over"] == 0, (name, r)
-        if name != "fwhm":
-            assert r["rms"] < 1e-6 or r["metric"] == "deg" and r["rms"] < 1e-3, (name, r)
+        if name not in ILL_CONDITIONED:
+            assert r["rms"] < 1e-6, (name, r)

@@ -259,3 +259,37 @@ def test_background_rms_map(gpu_ctx, w, h, bs, fs):
     g = gpu_ctx.background_rms(img.shape)
     o = O.background_rms(img, back_size=bs, back_filtersize=fs)
     assert g.tobytes() == o.tobytes()
+
+
+@pytest.mark.parametrize("kw", [dict(back_size=64), dict(back_size=37, back_filtersize=5),
+                                dict(back_size=40, back_type=1, back_value=1234.5)])
+def test_background_map(gpu_ctx, masks, kw):
+    """sexgpu_background_map: the background subtracted from every pixel (the
+    BACKGROUND check image) against the oracle's, bit for bit."""
+    img = synth.frame_c0(seed=8, w=500, h=350, nsrc=200)
+    gpu_ctx.extract(img, conv=masks["default"], **kw)
+    assert gpu_ctx.background_map(img.shape).tobytes() == O.background_map(img, **kw).tobytes()
+
+
+@pytest.mark.parametrize("mask_type,gain", [(2, 0.0), (0, 3.0)])
+def test_several_apertures(gpu_ctx, masks, mask_type, gain):
+    """PHOT_APERTURES with several diameters (the reference allows one,
+    src/define.h:50, src/cuda/cudaanalyse.cu:3363): every aperture of every
+    row against the oracle; the row's FLUX_APER columns are the first."""
+    img = synth.frame_c1(seed=23, w=900, h=700, nsrc=6000)
+    aps = [1.5, 5.0, 8.5, 14.0, 30.0]
+    kw = dict(conv=masks["gauss_2.5_5x5"], phot_apertures=aps, mask_type=mask_type, gain=gain,
+              mag_zeropoint=25.0)
+    g, gseg, _ = gpu_ctx.extract(img, **kw)
+    ga = gpu_ctx.apertures()
+    o, oseg, _ = O.extract(img, **kw)
+    assert np.array_equal(gseg, oseg)
+    compare_catalogs(g, o)
+    oa = o["aper"][:, :len(aps), :]
+    assert ga.shape == oa.shape == (len(g), len(aps), 4)
+    for k in (0, 1, 3):  # flux, error, magnitude error
+        assert ga[:, :, k].tobytes() == oa[:, :, k].tobytes(), k
+    assert np.allclose(ga[:, :, 2], oa[:, :, 2], rtol=RTOL_LOG, atol=0)
+    assert np.array_equal(ga[:, 0, 0], g["flux_aper"])
+    # a wider aperture holds more flux on average
+    assert (np.median(ga[:, 4, 0]) > np.median(ga[:, 1, 0]))

@@ -132,3 +132,13 @@ def test_localback_matches_reference_live(seed, thick):
     a = O.localback(sub, boxes, thick)
     b = O.ref_localback(sub, boxes, thick)
     assert a.view(np.uint32).tolist() == b.view(np.uint32).tolist()
+
+
+@pytest.mark.skipif(O.ref() is None, reason="oracle/_ref not built (needs the reference tree)")
+@pytest.mark.parametrize("kw", [dict(back_size=64), dict(back_size=37, back_filtersize=5), dict(back_size=384),
+                                dict(back_size=40, back_type=1, back_value=1234.5)])
+def test_background_map_matches_reference(kw):
+    """The oracle's background map (the BACKGROUND check image) against the
+    backline the reference's subbackline() (src/back.c:790) fills, bit for bit."""
+    img = synth.frame_c0(seed=5, w=512, h=384)
+    assert O.background_map(img, **kw).tobytes() == O.ref_background_map(img, **kw).tobytes()
