@@ -287,3 +287,31 @@ int ref_read_body(const char *path, int bitpix, double bscale, double bzero, int
     fclose(cat.file);
     return 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* The layout of the reference's catalogue record, outobjstruct
+ * (src/types.h:417-455): sizeof, then the offset of every member in order. */
+#include <stddef.h>
+int ref_outobj_layout(int *out, int max)
+{
+    const int v[] = {(int)sizeof(outobjstruct), (int)offsetof(outobjstruct, number),
+        (int)offsetof(outobjstruct, alpha2000), (int)offsetof(outobjstruct, delta2000),
+        (int)offsetof(outobjstruct, sposx), (int)offsetof(outobjstruct, sposy),
+        (int)offsetof(outobjstruct, flux_iso), (int)offsetof(outobjstruct, fluxerr_iso),
+        (int)offsetof(outobjstruct, mag_iso), (int)offsetof(outobjstruct, magerr_iso),
+        (int)offsetof(outobjstruct, flux_isocor), (int)offsetof(outobjstruct, fluxerr_isocor),
+        (int)offsetof(outobjstruct, flux_aper), (int)offsetof(outobjstruct, fluxerr_aper),
+        (int)offsetof(outobjstruct, mag_aper), (int)offsetof(outobjstruct, magerr_aper),
+        (int)offsetof(outobjstruct, flux_auto), (int)offsetof(outobjstruct, fluxerr_auto),
+        (int)offsetof(outobjstruct, mag_auto), (int)offsetof(outobjstruct, magerr_auto),
+        (int)offsetof(outobjstruct, theta), (int)offsetof(outobjstruct, poserr_mx2),
+        (int)offsetof(outobjstruct, poserr_my2), (int)offsetof(outobjstruct, poserr_mxy),
+        (int)offsetof(outobjstruct, flag), (int)offsetof(outobjstruct, elong),
+        (int)offsetof(outobjstruct, ellip), (int)offsetof(outobjstruct, sprob),
+        (int)offsetof(outobjstruct, peak), (int)offsetof(outobjstruct, kronfactor),
+        (int)offsetof(outobjstruct, bkg), (int)offsetof(outobjstruct, fwhm)};
+    int i, n = (int)(sizeof(v) / sizeof(v[0]));
+    for (i = 0; i < n && i < max; i++)
+        out[i] = v[i];
+    return n;
+}

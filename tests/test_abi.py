@@ -143,3 +143,35 @@ def test_read_nnw(tmp_path):
     bad.write_text("not a network\n1 2 3\n")
     with pytest.raises(RuntimeError):
         sexgpu.read_nnw(str(bad))
+
+
+OUTOBJ_MEMBERS = ["number", "alpha2000", "delta2000", "sposx", "sposy", "flux_iso", "fluxerr_iso", "mag_iso",
+                  "magerr_iso", "flux_isocor", "fluxerr_isocor", "flux_aper", "fluxerr_aper", "mag_aper",
+                  "magerr_aper", "flux_auto", "fluxerr_auto", "mag_auto", "magerr_auto", "theta", "poserr_mx2",
+                  "poserr_my2", "poserr_mxy", "flag", "elong", "ellip", "sprob", "peak", "kronfactor", "bkg",
+                  "fwhm"]
+
+
+def test_compat_record_layout_matches_reference_header():
+    """sizeof and every member offset of sexgpu_outobj equal those of the
+    reference's own outobjstruct (src/types.h:417-455), compiled from its
+    header into oracle/_ref; skipped where the reference tree is absent."""
+    import ctypes as C
+    from oracle import oracle as O
+    r = O.ref()
+    if r is None:
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    buf = (C.c_int * 64)()
+    n = r.ref_outobj_layout(buf, 64)
+    ref = list(buf[:n])
+    prog = "#include <stdio.h>\n#include <stddef.h>\n#include \"sexgpu_compat.h\"\nint main(void){printf(\"%d" + \
+        " %d" * len(OUTOBJ_MEMBERS) + "\\n\", (int)sizeof(sexgpu_outobj)" + \
+        "".join(", (int)offsetof(sexgpu_outobj, %s)" % m for m in OUTOBJ_MEMBERS) + ");return 0;}\n"
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(prog)
+        exe = os.path.join(d, "t")
+        subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe])
+        ours = [int(v) for v in subprocess.check_output([exe]).split()]
+    assert n == 1 + len(OUTOBJ_MEMBERS)
+    assert ours == ref
