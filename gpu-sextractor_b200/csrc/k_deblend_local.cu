@@ -48,8 +48,7 @@ constexpr int DL_CAP0 = 256;                   // shared-memory tier (one warp p
 constexpr int DL_CAP1 = 64;                    // its small-object half (more warps resident per SM)
 constexpr int DL_MID = SX_DL_MID;              // arena tier with 64-thread CTAs up to here, 256 above
 constexpr int DL_ARENA_MAX = SX_DL_ARENA_MAX;  // at most 32767: element indices are 16-bit
-constexpr int DL_SWEEP_BYTES = 62;   // shared bytes per pixel, sweep (with the neighbour table)
-constexpr int DL_NO_NBR = 0xffff;    // no neighbour in the object
+constexpr int DL_SWEEP_BYTES = 45;   // shared bytes per pixel, sweep
 constexpr int DL_ASSIGN_BYTES = 34;  // shared bytes per pixel, assignment
 constexpr int DL_ARENA_BYTES = 48;   // global arena bytes per pixel (either pass)
 
@@ -121,29 +120,13 @@ __device__ __forceinline__ unsigned long long dl_term(float c, int e0) {
     return (unsigned long long)((u & 0x7fffffu) | 0x800000u) << sh;
 }
 
-// pixels first active at level L: activate, then join to active neighbours.
-// nbr: the element index of every pixel's eight neighbours (DL_NO_NBR for
-// none), preloaded in shared memory with stride ncap, or null to look them up
-// in the frame-wide map
+// pixels first active at level L: activate, then join to active neighbours
 template <int NT>
 __device__ __forceinline__ void dl_activate_union(const DebArgs &A, int off, int ucap, int L, int b0, int b1,
                                                   const unsigned short *order, int *par, const unsigned char *lev,
-                                                  int *status, const unsigned short *nbr, int ncap) {
+                                                  int *status) {
     for (int i = b0 + (int)threadIdx.x; i < b1; i += NT) par[order[i]] = order[i];
     __syncthreads();
-    if (nbr) {
-        for (int i = b0 + (int)threadIdx.x; i < b1; i += NT) {
-            const int e = order[i];
-            int nb[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) nb[q] = nbr[q * ncap + e];
-#pragma unroll
-            for (int q = 0; q < 8; q++)
-                if (nb[q] != DL_NO_NBR && lev[nb[q]] >= L) sunion(par, e, nb[q], ucap, status);
-        }
-        __syncthreads();
-        return;
-    }
     for (int i = b0 + (int)threadIdx.x; i < b1; i += NT) {
         const int e = order[i];
         const int p = (int)A.rpix[off + e];
@@ -225,8 +208,6 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     const int tid = threadIdx.x;
     const int off = A.R.off[r], P = A.R.size[r];
     const unsigned *pix = A.rpix + off;
-    // shared-memory tier: the whole state, and a neighbour table, on chip
-    const bool smem_tier = base != nullptr;
     if (!base) {  // global-memory arena: 48 B per element at the root's offset
         base = A.D.arena + (size_t)off * DL_ARENA_BYTES;
         cap = P;
@@ -243,10 +224,6 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     unsigned short *const nid = order + 3 * cap;
     unsigned short *const ndr0 = order + 4 * cap;
     unsigned char *lev = reinterpret_cast<unsigned char *>(order + 6 * cap);
-    // the eight neighbours of every pixel as element indices (16 B per pixel
-    // after the levels), in the shared-memory tier
-    unsigned short *const nbr =
-        smem_tier ? reinterpret_cast<unsigned short *>(lev + ((cap + 1) & ~1)) : nullptr;
     if (hyb) {
         par = reinterpret_cast<int *>(hyb);
         lev = hyb + 4 * (size_t)P;
@@ -314,29 +291,6 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     block_thresholds(A, A.R.dthresh[r], fdpeak, thr);
     __syncthreads();
     dl_levels<NT>(A, P, pix, thr, lev, order, lvcnt, lvstart, lvcur, true);
-    if (smem_tier) {
-        // one pass over the pixels with every lookup in flight together: the
-        // sizes and exact flux terms every element starts with (only roots
-        // are ever added to, and a pixel is no root before it is active), and
-        // the element index of each of its neighbours
-        for (int k = tid; k < P; k += NT) {
-            const int p = (int)pix[k];
-            const int y = (int)fdiv((unsigned)p, A.wdiv), x = p - y * A.w;
-            int nb[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const int ddx[8] = {-1, 0, 1, -1, 1, -1, 0, 1}, ddy[8] = {-1, -1, -1, 0, 0, 1, 1, 1};
-                const int nx = x + ddx[q], ny = y + ddy[q];
-                nb[q] = (nx < 0 || ny < 0 || nx >= A.w || ny >= A.h) ? -1 : __ldg(A.pos2idx + (size_t)ny * A.w + nx);
-            }
-            sz[k] = 1;
-            acc[k] = dl_term(A.cd[p], e0);
-#pragma unroll
-            for (int q = 0; q < 8; q++) nbr[q * cap + k] = nb[q] >= 0 ? (unsigned short)(nb[q] - off) : DL_NO_NBR;
-        }
-        __syncthreads();
-    }
-
     int cur = 0, lastL = -1;
     for (int L = A.N - 1; L >= 0; L--) {
         const int cnt = lvcnt[L];
@@ -349,10 +303,8 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
         // level L+1 when the levels since the last populated one were empty
         for (int i = b0 + tid; i < b1; i += NT) {
             const int e = order[i];
-            if (!smem_tier) {
-                sz[e] = 1;
-                acc[e] = dl_term(A.cd[pix[e]], e0);
-            }
+            sz[e] = 1;
+            acc[e] = dl_term(A.cd[pix[e]], e0);
             rec[e] = (L << 24) | 0x00ffffff;  // active from level L, not absorbed yet
         }
         if (lastL > cl)
@@ -362,7 +314,7 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
                 NFL(prv)[i] = (NFL(prv)[i] & ~1u) | (lhs > value0 ? 1u : 0u);
             }
         // (b) activation and unions
-        dl_activate_union<NT>(A, off, ucap, L, b0, b1, order, par, lev, status, nbr, cap);
+        dl_activate_union<NT>(A, off, ucap, L, b0, b1, order, par, lev, status);
         // (c) roots that joined another component hand over size and flux
         for (int i = tid; i < nold + cnt; i += NT) {
             const int c = i < nold ? RL(prv)[i] : order[b0 + i - nold];
@@ -899,7 +851,7 @@ void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int n
         A, dl_lists(lists, counts, n, 4, 5), DL_SCUR(4), 0, glist, counts + 7, DL_HYB45);
     k_dl_sweep<1024><<<min(nroots, dl_grid(k_dl_sweep<1024>, 1024, h3, g5)), 1024, h3, S.side[1]>>>(
         A, dl_lists(lists, counts, n, 3), DL_SCUR(3), 0, glist, counts + 7, DL_HYB3);
-    k_dl_sweep<64><<<min(nroots, dl_grid(k_dl_sweep<64>, 64, h12, g1)), 64, h12, S.side[1]>>>(
+    k_dl_sweep<64><<<min(nroots, dl_grid(k_dl_sweep<64>, 64, h12, g1)), 64, h12, S.main>>>(
         A, dl_lists(lists, counts, n, 1, 2), DL_SCUR(1), 0, glist, counts + 7, DL_HYB12);
     k_dl_sweep<32><<<min(nroots, dl_grid(k_dl_sweep<32>, 32, m0, g0)), 32, m0, S.main>>>(
         A, dl_lists(lists, counts, n, 0), DL_SCUR(0), DL_CAP0, glist, counts + 7, 0);
@@ -934,7 +886,7 @@ void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int 
         A, dl_lists(lists, counts, n, 4, 5), DL_ACUR(4), 0, DL_GTAB_BIG);
     k_dl_assign<1024><<<min(nroots, dl_grid(k_dl_assign<1024>, 1024, tb, g5)), 1024, tb, S.side[1]>>>(
         A, dl_lists(lists, counts, n, 3), DL_ACUR(3), 0, DL_GTAB_BIG);
-    k_dl_assign<64><<<min(nroots, dl_grid(k_dl_assign<64>, 64, tm, g1)), 64, tm, S.side[1]>>>(
+    k_dl_assign<64><<<min(nroots, dl_grid(k_dl_assign<64>, 64, tm, g1)), 64, tm, S.main>>>(
         A, dl_lists(lists, counts, n, 1, 2), DL_ACUR(1), 0, DL_GTAB_MID);
     k_dl_assign<32><<<min(nroots, dl_grid(k_dl_assign<32>, 32, m0, g0)), 32, m0, S.main>>>(
         A, dl_lists(lists, counts, n, 0), DL_ACUR(0), DL_CAP0, 0);

@@ -38,8 +38,14 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *sh_warp, int &to
     return base + x - v;
 }
 
-__global__ void k_tile_sums(const int *__restrict__ in, int n, int *__restrict__ sums) {
+// The element count of a scan or sort: n, or, when the count is only known on
+// the device (a launch sized before the count exists, as in a captured graph),
+// the smaller of n and *n_dev.
+__device__ __forceinline__ int dev_count(int n, const int *n_dev) { return n_dev ? min(n, max(*n_dev, 0)) : n; }
+
+__global__ void k_tile_sums(const int *__restrict__ in, int n, int *__restrict__ sums, const int *n_dev) {
     __shared__ int sh[32];
+    n = dev_count(n, n_dev);
     long long base = (long long)blockIdx.x * SCAN_TILE;
     int acc = 0;
 #pragma unroll
@@ -53,8 +59,9 @@ __global__ void k_tile_sums(const int *__restrict__ in, int n, int *__restrict__
 }
 
 __global__ void k_tile_scan(const int *__restrict__ in, int *__restrict__ out, int n,
-                            const int *__restrict__ offs, int *total) {
+                            const int *__restrict__ offs, int *total, const int *n_dev) {
     __shared__ int sh[32];
+    n = dev_count(n, n_dev);
     long long base = (long long)blockIdx.x * SCAN_TILE;
     int v[SCAN_ITEMS], acc = 0;
 #pragma unroll
@@ -84,21 +91,23 @@ size_t scan_temp_ints(long long n) {
 }
 
 // out[i] = sum_{j<i} in[j]; *total (device, may be NULL) = sum of all.
-// in and out may alias.  tmp: scan_temp_ints(n) ints.
-void exclusive_scan(const int *in, int *out, long long n, int *total, int *tmp, cudaStream_t st) {
+// in and out may alias.  tmp: scan_temp_ints(n) ints.  n_dev (device, may
+// be NULL): the count, at most n, when only the device knows it; the launch
+// is sized for n.
+void exclusive_scan(const int *in, int *out, long long n, int *total, int *tmp, cudaStream_t st, const int *n_dev) {
     if (n <= 0) {
         if (total) cudaMemsetAsync(total, 0, sizeof(int), st);
         return;
     }
     int nt = (int)((n + SCAN_TILE - 1) / SCAN_TILE);
     if (nt == 1) {
-        k_tile_scan<<<1, SCAN_THREADS, 0, st>>>(in, out, (int)n, nullptr, total);
+        k_tile_scan<<<1, SCAN_THREADS, 0, st>>>(in, out, (int)n, nullptr, total, n_dev);
         return;
     }
     int *sums = tmp, *offs = tmp + nt;
-    k_tile_sums<<<nt, SCAN_THREADS, 0, st>>>(in, (int)n, sums);
-    exclusive_scan(sums, offs, nt, nullptr, tmp + 2 * nt + 2, st);
-    k_tile_scan<<<nt, SCAN_THREADS, 0, st>>>(in, out, (int)n, offs, total);
+    k_tile_sums<<<nt, SCAN_THREADS, 0, st>>>(in, (int)n, sums, n_dev);
+    exclusive_scan(sums, offs, nt, nullptr, tmp + 2 * nt + 2, st, nullptr);
+    k_tile_scan<<<nt, SCAN_THREADS, 0, st>>>(in, out, (int)n, offs, total, n_dev);
 }
 
 // ---------------------------------------------------------------------------
@@ -113,8 +122,9 @@ constexpr int RS_BITS = 8;
 constexpr int RS_DIGITS = 1 << RS_BITS;
 
 __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const unsigned *__restrict__ keys, int n, int shift,
-                                                          int ntiles, int *__restrict__ hist) {
+                                                          int ntiles, int *__restrict__ hist, const int *n_dev) {
     __shared__ int h[RS_DIGITS];
+    n = dev_count(n, n_dev);
     for (int i = threadIdx.x; i < RS_DIGITS; i += RS_THREADS) h[i] = 0;
     __syncthreads();
     long long base = (long long)blockIdx.x * RS_TILE;
@@ -131,8 +141,10 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const unsigned *__res
                                                              const unsigned *__restrict__ vin,
                                                              unsigned *__restrict__ kout,
                                                              unsigned *__restrict__ vout, int n, int shift,
-                                                             int ntiles, const int *__restrict__ offs) {
+                                                             int ntiles, const int *__restrict__ offs,
+                                                             const int *n_dev) {
     __shared__ int cnt[RS_WARPS][RS_DIGITS];
+    n = dev_count(n, n_dev);
     __shared__ int gbase[RS_DIGITS];
     int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < RS_WARPS * RS_DIGITS; i += RS_THREADS) (&cnt[0][0])[i] = 0;
@@ -186,9 +198,11 @@ size_t radix_temp_ints(long long n) {
 }
 
 // Stable sort by the low keybits bits of keys.  Result ends in (keys, vals);
-// (kalt, valt) are scratch of n elements each.
+// (kalt, valt) are scratch of n elements each.  n_dev (device, may be NULL):
+// the count, at most n, when only the device knows it (elements beyond it
+// are left as they are).
 void radix_sort_pairs(unsigned *keys, unsigned *vals, unsigned *kalt, unsigned *valt, long long n,
-                      int keybits, int *tmp, cudaStream_t st) {
+                      int keybits, int *tmp, cudaStream_t st, const int *n_dev) {
     if (n <= 1) return;
     int nt = (int)((n + RS_TILE - 1) / RS_TILE);
     long long h = (long long)nt * RS_DIGITS;
@@ -197,9 +211,9 @@ void radix_sort_pairs(unsigned *keys, unsigned *vals, unsigned *kalt, unsigned *
     int passes = (keybits + RS_BITS - 1) / RS_BITS;
     for (int p = 0; p < passes; p++) {
         int shift = p * RS_BITS;
-        k_rs_hist<<<nt, RS_THREADS, 0, st>>>(ka, (int)n, shift, nt, hist);
-        exclusive_scan(hist, offs, h, nullptr, stmp, st);
-        k_rs_scatter<<<nt, RS_THREADS, 0, st>>>(ka, va, kb, vb, (int)n, shift, nt, offs);
+        k_rs_hist<<<nt, RS_THREADS, 0, st>>>(ka, (int)n, shift, nt, hist, n_dev);
+        exclusive_scan(hist, offs, h, nullptr, stmp, st, nullptr);
+        k_rs_scatter<<<nt, RS_THREADS, 0, st>>>(ka, va, kb, vb, (int)n, shift, nt, offs, n_dev);
         unsigned *t = ka; ka = kb; kb = t;
         t = va; va = vb; vb = t;
     }
