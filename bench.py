@@ -260,6 +260,9 @@ def run_gpu(args):
                            "frac": round(frame_bytes / (peak * 1e9) / (ms_dev / 1e3), 4)},
         "clocks": clk,
     }
+    if world == 1 and not args.no_graph:
+        line["graph"] = run_graph_arm(sexgpu, dev, stream, timed, d_img, h_img, w, h, cfg, rows_np, nobj,
+                                      args.steps)
     if world == 1 and not args.no_batch:
         line["batch"] = run_batch(ctx, c3_frames())
     if world == 1 and not args.no_literal:
@@ -274,6 +277,50 @@ def run_gpu(args):
         dist.barrier()
         dist.destroy_process_group()
     ctx.close()
+
+
+def run_graph_arm(sexgpu, dev, stream, timed, d_img, h_img, w, h, cfg, rows_plain, nobj, steps):
+    """The same frame through captured graphs ("graph" parameter): device-
+    resident and end to end (host frame in, rows out), timed like the plain
+    form, with the rows compared byte for byte with the plain form's."""
+    import ctypes as C
+    import torch
+    g = sexgpu.Context(dev.index)
+    g.set_stream(stream.cuda_stream)
+    g.set_param("graph", 1)
+    maxobj = len(rows_plain)
+    h_rows = torch.empty(maxobj * sexgpu.OBJECT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    c = sexgpu.make_config(**cfg)
+
+    def dev_step():
+        g.extract_device(d_img.data_ptr(), w, h, **cfg)
+
+    def e2e_step():
+        n = C.c_int()
+        s = sexgpu.Summary()
+        rc = sexgpu.lib().sexgpu_extract(g.h, C.c_void_p(h_img.data_ptr()), None, w, h, C.byref(c),
+                                         C.c_void_p(h_rows.data_ptr()), maxobj, C.byref(n), None, None, None,
+                                         C.byref(s))
+        if rc != 0:
+            raise RuntimeError("sexgpu_extract failed %d" % rc)
+        return n.value
+
+    for _ in range(3):  # plain (counts), capacity form + capture, replay
+        dev_step()
+        e2e_step()
+    t_dev = timed(dev_step, steps)
+    replayed_dev, kernels, _ = g.graph_stats()
+    t_e2e = timed(e2e_step, steps)
+    n = e2e_step()
+    replayed_e2e = g.graph_stats()[0]
+    rows = h_rows.numpy().view(sexgpu.OBJECT_DTYPE)[:n]
+    same = n == nobj and rows.tobytes() == rows_plain[:nobj].tobytes()
+    g.close()
+    return {"ms_per_frame": round(t_dev / steps, 4), "frames_per_s": round(steps / (t_dev / 1e3), 3),
+            "e2e_ms_per_frame": round(t_e2e / steps, 4), "e2e_frames_per_s": round(steps / (t_e2e / 1e3), 3),
+            "kernels_per_frame": kernels, "replayed": bool(replayed_dev and replayed_e2e),
+            "identical_rows": bool(same),
+            "timing": "CUDA events around each graph launch and its scalar read-back, L2 flushed before each"}
 
 
 def _c3_base(job):
@@ -677,6 +724,7 @@ def main():
     ap.add_argument("--impl", default="sexgpu")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="skip the captured-graph arm")
     ap.add_argument("--no-c4", action="store_true", help="skip the 16384^2 weighted frame (c4)")
     args = ap.parse_args()
     if args.profile_case:

@@ -35,8 +35,14 @@ __device__ __forceinline__ float sx_unblank(float v) { return v != v ? -1e+30f :
 // device status word bits
 #define SX_ST_RANGE 1
 #define SX_ST_LOOP 2
-#define SX_ST_CAPACITY 4
+#define SX_ST_CAPACITY 4  // a count beyond the capacity a captured pipeline was sized for
 #define SX_ST_LOAD 8     // a tile load of the subtract/filter pipeline did not complete in time
+#define SX_ST_THRESH 16   // zero or negative detection or analysis threshold
+#define SX_ST_STOP (SX_ST_RANGE | SX_ST_LOOP | SX_ST_CAPACITY | SX_ST_LOAD | SX_ST_THRESH)
+
+// A count known on the device only: *n_dev, at most the capacity n the launch
+// was sized for; n itself when n_dev is null (the count known on the host).
+__device__ __forceinline__ int sx_count(int n, const int *n_dev) { return n_dev ? min(n, max(*n_dev, 0)) : n; }
 
 #define SX_ALLOC_OTHER 0x7fffffff
 
@@ -372,6 +378,7 @@ struct FrameScalars {
     int nsurv;                      // after CLEAN
     int e0sub;                      // smallest exponent of a non-zero |sub|
     int kitems[2], kchunks[2];      // queued Kron boxes and their work items (pass 1, 2)
+    int nvbig;                      // CLEAN victims when too many for the one-block sort, else 0
     unsigned long long levpix;      // sum of the deblending level of every raw-object pixel
 };
 

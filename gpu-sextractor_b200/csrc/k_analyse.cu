@@ -119,6 +119,7 @@ struct AnaArgs {
     ObjBufs O;
     FrameScalars *sc;
     int w, h, nbx, nby, bw, bh, nobj, minarea, clean_flag;
+    const int *nobj_dev;  // the object count on the device (nobj is then the capacity), or null
     FastDiv wdiv;
     double gain, satur;
     const float *wvar;  // calibrated variance map, or null
@@ -136,7 +137,7 @@ struct AnaArgs {
 __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(AnaArgs A) {
     const int lane = threadIdx.x & 31;
     const int o = blockIdx.x * AN_WARPS + (threadIdx.x >> 5);
-    if (o >= A.nobj || A.O.level[o] == 0) return;
+    if (o >= sx_count(A.nobj, A.nobj_dev) || A.O.level[o] == 0) return;
     const int n = A.O.n[o], off = A.O.off[o], w = A.w, h = A.h;
     const unsigned *pix = A.opix + off;
     const float dthresh = A.O.dthr[o];
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(AnaAr
 
 __global__ void k_robust_finish(AnaArgs A) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= A.nobj || A.O.level[o] == 0) return;
+    if (o >= sx_count(A.nobj, A.nobj_dev) || A.O.level[o] == 0) return;
     const RobustRaw R = A.raw[o];
     const int xmin = R.xmin, ymin = R.ymin, flags = R.flags, dnpix = R.dnpix, area2 = R.area2;
     const float rv = R.rv, peak = R.peak, cpeak = R.cpeak;
@@ -296,7 +297,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
     __shared__ __align__(16) unsigned hist[AN_WARPS][256];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int o = blockIdx.x * AN_WARPS + wid;
-    if (o >= A.nobj) return;
+    if (o >= sx_count(A.nobj, A.nobj_dev)) return;
     const int n = A.O.n[o], off = A.O.off[o], w = A.w;
     const unsigned *pix = A.opix + off;
     const float dthresh = A.O.dthr[o], thresh = A.O.athr[o], gthresh = A.sc->thresh, backsig = A.sc->backsig;
@@ -422,7 +423,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
 // one lane of a warp)
 __global__ void k_examine_finish(AnaArgs A) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= A.nobj) return;
+    if (o >= sx_count(A.nobj, A.nobj_dev)) return;
     const ExamRaw X = A.xraw[o];
     const XSum stv = X.stv, svar = X.svar;
     double esum = X.esum, emx2 = X.emx2, emy2 = X.emy2, emxy = X.emxy;
@@ -536,11 +537,11 @@ __global__ void __launch_bounds__(OP_WARPS * 32) k_obj_partition(const unsigned 
                                                                  const int *__restrict__ rnkept,
                                                                  const int *__restrict__ objbase,
                                                                  const int *__restrict__ ooff, int nroots,
-                                                                 unsigned *__restrict__ opix) {
+                                                                 const int *nroots_dev, unsigned *__restrict__ opix) {
     __shared__ int cur[OP_WARPS][OP_KMAX];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int r = blockIdx.x * OP_WARPS + wid;
-    if (r >= nroots) return;
+    if (r >= sx_count(nroots, nroots_dev)) return;
     const int off = roff[r], P = rsize[r], K = rnkept[r], ob = objbase[r];
     if (K <= 1) {
 #pragma unroll 4
@@ -559,8 +560,10 @@ __global__ void __launch_bounds__(32) k_obj_partition_big(const unsigned *__rest
                                                           const int *__restrict__ rnkept,
                                                           const int *__restrict__ objbase,
                                                           const int *__restrict__ ooff, int nroots,
-                                                          unsigned *__restrict__ opix, int *gcur) {
+                                                          const int *nroots_dev, unsigned *__restrict__ opix,
+                                                          int *gcur) {
     extern __shared__ int bigcur[];
+    nroots = sx_count(nroots, nroots_dev);
     for (int r = blockIdx.x; r < nroots; r += gridDim.x) {
         const int K = rnkept[r];
         if (K <= OP_KMAX) continue;
@@ -571,14 +574,15 @@ __global__ void __launch_bounds__(32) k_obj_partition_big(const unsigned *__rest
     }
 }
 
-// gcur: scratch of one int per object
+// gcur: scratch of one int per object.  nroots_dev (device, or null): the
+// number of roots when only the device knows it; nroots is then the capacity.
 void launch_obj_partition(const unsigned *rpix, const unsigned *objkey, const RootBufs &R, const int *ooff,
-                          int nroots, unsigned *opix, int *gcur, cudaStream_t st) {
+                          int nroots, const int *nroots_dev, unsigned *opix, int *gcur, cudaStream_t st) {
     if (nroots <= 0) return;
     k_obj_partition<<<(unsigned)((nroots + OP_WARPS - 1) / OP_WARPS), OP_WARPS * 32, 0, st>>>(
-        rpix, objkey, R.off, R.size, R.nkept, R.objbase, ooff, nroots, opix);
+        rpix, objkey, R.off, R.size, R.nkept, R.objbase, ooff, nroots, nroots_dev, opix);
     k_obj_partition_big<<<(unsigned)std::min(nroots, OP_BIG_GRID), 32, OP_BIG_KMAX * sizeof(int), st>>>(
-        rpix, objkey, R.off, R.size, R.nkept, R.objbase, ooff, nroots, opix, gcur);
+        rpix, objkey, R.off, R.size, R.nkept, R.objbase, ooff, nroots, nroots_dev, opix, gcur);
 }
 
 void launch_analyse(const AnaArgs &A, cudaStream_t st) {
@@ -589,9 +593,10 @@ void launch_analyse(const AnaArgs &A, cudaStream_t st) {
     if (A.O.dbkg) {
         k_local_stat<<<(unsigned)((A.nobj + 127) / 128), 128, 0, st>>>(A.sub, A.w, A.h, A.bp_thick, A.O.xmin,
                                                                          A.O.xmax, A.O.ymin, A.O.ymax, A.nobj,
-                                                                         A.O.lstat);
+                                                                         A.nobj_dev, A.O.lstat);
         k_local_guess<<<(unsigned)A.nobj, GUESS_THREADS, 0, st>>>(A.sub, A.w, A.h, A.bp_thick, A.O.xmin, A.O.xmax,
-                                                                   A.O.ymin, A.O.ymax, A.O.lstat, A.O.dbkg);
+                                                                   A.O.ymin, A.O.ymax, A.nobj, A.nobj_dev, A.O.lstat,
+                                                                   A.O.dbkg);
     }
     k_examineiso<<<grid, AN_WARPS * 32, 0, st>>>(A);
     k_examine_finish<<<(unsigned)((A.nobj + 127) / 128), 128, 0, st>>>(A);

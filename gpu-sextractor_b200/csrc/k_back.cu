@@ -428,9 +428,9 @@ __device__ __forceinline__ void local_visit(const float *__restrict__ sub, int w
 // frame, or no valid pixel)
 __global__ void k_local_stat(const float *__restrict__ sub, int w, int h, int pbs, const int *__restrict__ xmin,
                              const int *__restrict__ xmax, const int *__restrict__ ymin,
-                             const int *__restrict__ ymax, int n, MeshStat *__restrict__ ls) {
+                             const int *__restrict__ ymax, int n, const int *n_dev, MeshStat *__restrict__ ls) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= n) return;
+    if (o >= sx_count(n, n_dev)) return;
     MeshStat s;
     s.mean = s.sigma = s.lcut = s.hcut = s.qzero = s.qscale = 0.f;
     s.nlevels = -1;
@@ -486,11 +486,13 @@ __global__ void __launch_bounds__(GUESS_THREADS) k_local_guess(const float *__re
                                                                  const int *__restrict__ xmin,
                                                                  const int *__restrict__ xmax,
                                                                  const int *__restrict__ ymin,
-                                                                 const int *__restrict__ ymax,
+                                                                 const int *__restrict__ ymax, int n,
+                                                                 const int *n_dev,
                                                                  const MeshStat *__restrict__ ls, float *dbkg) {
     __shared__ int hist[SX_QUANTIF_NMAXLEVELS + 2];
     __shared__ int pfx[SX_QUANTIF_NMAXLEVELS + 2];
     const int o = blockIdx.x;
+    if (o >= sx_count(n, n_dev)) return;
     const MeshStat bm = ls[o];
     if (bm.nlevels < 0) {
         if (threadIdx.x == 0) dbkg[o] = 0.0f;

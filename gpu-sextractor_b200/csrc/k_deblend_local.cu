@@ -732,7 +732,8 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 32 : NT == 64 ? 16 : NT == 256 
     }
 }
 
-// Size classes (list k at lists + k * nroots, its length in counts[k]):
+// Size classes (list k at lists + k * n, n the number of roots or the
+// capacity the launches were sized for; its length in counts[k]):
 //   8  <= 64 pixels              shared memory, one warp
 //   0  (64, 256]                 shared memory, one warp
 //   1  (1024, 2048]   2 (256, 1024]       arena (hybrid), 64 threads
@@ -756,15 +757,16 @@ __device__ __forceinline__ int dl_class(int s) {
 }
 
 // sort keys: larger objects first (sizes above 65535 tie, all in class 6)
-__global__ void k_root_keys(const int *size, int n, unsigned *keys, unsigned *vals) {
+__global__ void k_root_keys(const int *size, int n, const int *n_dev, unsigned *keys, unsigned *vals) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
+    if (r >= sx_count(n, n_dev)) return;
     keys[r] = 65535u - (unsigned)min(size[r], 65535);
     vals[r] = (unsigned)r;
 }
 
 // first and last sorted position of every size class present
-__global__ void k_class_bounds(const int *size, const unsigned *sorted, int n, int *bnd) {
+__global__ void k_class_bounds(const int *size, const unsigned *sorted, int n, const int *n_dev, int *bnd) {
+    n = sx_count(n, n_dev);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int t = dl_class(size[sorted[i]]);
@@ -772,10 +774,10 @@ __global__ void k_class_bounds(const int *size, const unsigned *sorted, int n, i
     if (i == n - 1 || dl_class(size[sorted[i + 1]]) != t) bnd[DL_NLISTS + t] = i;
 }
 
-__global__ void k_class_fill(const int *size, const unsigned *sorted, int n, const int *bnd, int *lists,
-                             int *counts) {
+__global__ void k_class_fill(const int *size, const unsigned *sorted, int n, const int *n_dev, const int *bnd,
+                             int *lists, int *counts) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= sx_count(n, n_dev)) return;
     const int t = dl_class(size[sorted[i]]);
     lists[(size_t)t * n + (i - bnd[t])] = (int)sorted[i];
     if (i == bnd[DL_NLISTS + t]) counts[t] = i - bnd[t] + 1;
@@ -805,16 +807,18 @@ static RootLists dl_lists(const int *lists, int *counts, size_t n, int a, int b 
     return L;
 }
 
-// keys, vals, kalt, valt: scratch of nroots elements each; tmp: sort scratch
-void launch_deblend_split(const int *size, int nroots, int *lists, int *counts, unsigned *keys, unsigned *vals,
-                          unsigned *kalt, unsigned *valt, int *tmp, cudaStream_t st) {
+// keys, vals, kalt, valt: scratch of nroots elements each; tmp: sort scratch.
+// nroots_dev (device, or null): the number of roots, at most nroots, when
+// only the device knows it; nroots is then the capacity (the list stride).
+void launch_deblend_split(const int *size, int nroots, const int *nroots_dev, int *lists, int *counts,
+                          unsigned *keys, unsigned *vals, unsigned *kalt, unsigned *valt, int *tmp, cudaStream_t st) {
     cudaMemsetAsync(counts, 0, 3 * DL_NLISTS * sizeof(int), st);
     if (nroots <= 0) return;
     const unsigned g = (unsigned)((nroots + 255) / 256);
-    k_root_keys<<<g, 256, 0, st>>>(size, nroots, keys, vals);
-    radix_sort_pairs(keys, vals, kalt, valt, nroots, 16, tmp, st);
-    k_class_bounds<<<g, 256, 0, st>>>(size, vals, nroots, counts + 3 * DL_NLISTS);
-    k_class_fill<<<g, 256, 0, st>>>(size, vals, nroots, counts + 3 * DL_NLISTS, lists, counts);
+    k_root_keys<<<g, 256, 0, st>>>(size, nroots, nroots_dev, keys, vals);
+    radix_sort_pairs(keys, vals, kalt, valt, nroots, 16, tmp, st, nroots_dev);
+    k_class_bounds<<<g, 256, 0, st>>>(size, vals, nroots, nroots_dev, counts + 3 * DL_NLISTS);
+    k_class_fill<<<g, 256, 0, st>>>(size, vals, nroots, nroots_dev, counts + 3 * DL_NLISTS, lists, counts);
 }
 
 int deblend_split_launches(int nroots) { return nroots > 0 ? 3 + radix_launches(16, nroots) : 0; }

@@ -31,17 +31,17 @@ __device__ __forceinline__ int clean_cell(double mx, double my, int gx, int gy) 
     return cy * gx + cx;
 }
 
-__global__ void k_clean_count(ObjBufs O, int n, int *cellcnt, int gx, int gy) {
+__global__ void k_clean_count(ObjBufs O, int n, const int *n_dev, int *cellcnt, int gx, int gy) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= sx_count(n, n_dev)) return;
     O.master[i] = 0x7fffffff;
     atomicAdd(&cellcnt[clean_cell(O.mx[i], O.my[i], gx, gy)], 1);
 }
 
-__global__ void k_clean_pack(ObjBufs O, int n, double beta, const int *cellstart, int *cellcur, CleanObj *packed,
-                             int gx, int gy) {
+__global__ void k_clean_pack(ObjBufs O, int n, const int *n_dev, double beta, const int *cellstart, int *cellcur,
+                             CleanObj *packed, int gx, int gy) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= sx_count(n, n_dev)) return;
     CleanObj c;
     double unitarea = SX_PI * O.a[i] * O.b[i];
     c.amp = O.fdflux[i] / (2 * unitarea * O.abcor[i]);
@@ -95,11 +95,12 @@ __device__ __forceinline__ void clean_test(const CleanObj &p, const CleanObj &q,
 constexpr int CL_PAIR_WARPS = 4;
 
 __global__ void __launch_bounds__(CL_PAIR_WARPS * 32) k_clean_pairs(const CleanObj *__restrict__ packed, int n,
-                                                                    double beta, const int *__restrict__ cellstart,
+                                                                    const int *n_dev, double beta,
+                                                                    const int *__restrict__ cellstart,
                                                                     int *master, int gx, int gy) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int k = blockIdx.x;
-    if (k >= n) return;
+    if (k >= sx_count(n, n_dev)) return;
     const CleanObj me = packed[k];
     const double rad = 20.0 * me.a * 1.001 + 2.0;
     int x0 = max((int)floor((me.mx - rad) / CL_CELL), 0), x1 = min((int)floor((me.mx + rad) / CL_CELL), gx - 1);
@@ -123,7 +124,9 @@ __global__ void __launch_bounds__(CL_PAIR_WARPS * 32) k_clean_pairs(const CleanO
 // the chain of masters of a victim ends at a survivor after fewer than n
 // steps (masters have smaller indices); cap: a smaller bound set for a
 // failure test (0: n); running out sets SX_ST_LOOP
-__global__ void k_clean_chain(ObjBufs O, int n, unsigned *vkey, unsigned *vval, int *nvict, int *status, int cap) {
+__global__ void k_clean_chain(ObjBufs O, int n, const int *n_dev, unsigned *vkey, unsigned *vval, int *nvict,
+                              int *status, int cap) {
+    n = sx_count(n, n_dev);
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int m = O.master[i];
@@ -143,11 +146,17 @@ __global__ void k_clean_chain(ObjBufs O, int n, unsigned *vkey, unsigned *vval, 
 
 // victims in (master, index) order: one block sorts the (master << 32 |
 // index) keys, all distinct, in shared memory (bitonic network); larger
-// victim lists go through two stable radix sorts instead
+// victim lists go through two stable radix sorts instead.  With the count on
+// the device (nv_dev), a list too long for the block is left alone and its
+// length written to *big (0 otherwise): the count of the radix sorts.
 constexpr int CL_SORT_MAX = 4096;
 
-__global__ void __launch_bounds__(1024) k_victim_sort(unsigned *vkey, unsigned *vval, int nv) {
+__global__ void __launch_bounds__(1024) k_victim_sort(unsigned *vkey, unsigned *vval, int nv, const int *nv_dev,
+                                                      int *big) {
     __shared__ unsigned long long s[CL_SORT_MAX];
+    nv = sx_count(nv, nv_dev);
+    if (big && threadIdx.x == 0) *big = nv > CL_SORT_MAX ? nv : 0;
+    if (nv > CL_SORT_MAX) return;
     int n2 = 1;
     while (n2 < nv) n2 <<= 1;
     for (int i = threadIdx.x; i < n2; i += blockDim.x)
@@ -174,7 +183,8 @@ __global__ void __launch_bounds__(1024) k_victim_sort(unsigned *vkey, unsigned *
 }
 
 // victims sorted by (master, index): each segment head merges its segment
-__global__ void k_clean_merge(ObjBufs O, const unsigned *vkey, const unsigned *vval, int nv) {
+__global__ void k_clean_merge(ObjBufs O, const unsigned *vkey, const unsigned *vval, int nv, const int *nv_dev) {
+    nv = sx_count(nv, nv_dev);
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nv) return;
     if (k > 0 && vkey[k - 1] == vkey[k]) return;
@@ -203,9 +213,9 @@ __global__ void k_clean_merge(ObjBufs O, const unsigned *vkey, const unsigned *v
 }
 
 // pixels of cleaned objects belong to their master in the allocation map
-__global__ void k_alloc_victims(ObjBufs O, const unsigned *opix, int *alloc, int n) {
+__global__ void k_alloc_victims(ObjBufs O, const unsigned *opix, int *alloc, int n, const int *n_dev) {
     int o = blockIdx.x;
-    if (o >= n) return;
+    if (o >= sx_count(n, n_dev)) return;
     int m = O.fmaster[o];
     if (m < 0) return;
     int off = O.off[o], cnt = O.n[o];
@@ -224,6 +234,7 @@ struct EndArgs {
     ObjBufs O;
     FrameScalars *sc;
     int w, h, n, mask_type;
+    const int *n_dev;   // the object count on the device (n is then the capacity), or null
     double aperture, autoparam0, autoparam1, gain, zp, satur;
     int naper;                          // apertures (>= 1); the first is `aperture`
     double apertures[SEXGPU_MAXAPER];
@@ -565,7 +576,7 @@ __device__ void end_finish(const EndArgs &A, int o, int flags, float kron, bool 
 // this double-precision tail does not run on one lane of a warp)
 __global__ void k_end_finish(EndArgs A) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= A.n || A.O.fmaster[o] >= 0) return;
+    if (o >= sx_count(A.n, A.n_dev) || A.O.fmaster[o] >= 0) return;
     const EndRaw R = A.raw[o];
     const KronAcc &p2 = R.p2;
     const bool have2 = R.have2 != 0;
@@ -640,7 +651,7 @@ __device__ void kron_after1(const EndArgs &A, int o, double mx, double my, int f
 __global__ void __launch_bounds__(128, 8) k_endobject(EndArgs A) {
     const int lane = threadIdx.x & 31;
     const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (o >= A.n) return;
+    if (o >= sx_count(A.n, A.n_dev)) return;
     if (A.O.fmaster[o] >= 0) return;
     int flags = A.O.flags[o];
     const double mx = A.O.mx[o], my = A.O.my[o];
@@ -713,9 +724,10 @@ __global__ void k_kron_merge(EndArgs A) {
 // :599-632 (src/neurro.c neurresp): inputs are log10 of the eight isophotal
 // areas in seeing units and of FLUX_MAX over the threshold, plus log10 of the
 // seeing; every layer applies the logistic function; double arithmetic.
-__global__ void k_class_star(ObjBufs O, int n, const sexgpu_nnw *__restrict__ net, double fwhm, double pixscale) {
+__global__ void k_class_star(ObjBufs O, int n, const int *n_dev, const sexgpu_nnw *__restrict__ net, double fwhm,
+                             double pixscale) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= n || O.fmaster[o] >= 0) return;
+    if (o >= sx_count(n, n_dev) || O.fmaster[o] >= 0) return;
     double fac2 = fwhm / pixscale;
     fac2 *= fac2;
     const float thresh = O.athr[o], peak = O.peak[o];
@@ -749,7 +761,8 @@ void launch_endobject(const EndArgs &E, int nobj, cudaStream_t st, int &launches
     k_end_finish<<<(unsigned)((nobj + 127) / 128), 128, 0, st>>>(E);
     launches += 6;
     if (E.nnw) {
-        k_class_star<<<(unsigned)((nobj + 127) / 128), 128, 0, st>>>(E.O, nobj, E.nnw, E.seeing, E.pixscale);
+        k_class_star<<<(unsigned)((nobj + 127) / 128), 128, 0, st>>>(E.O, nobj, E.n_dev, E.nnw, E.seeing,
+                                                                      E.pixscale);
         launches += 1;
     }
 }
@@ -758,29 +771,28 @@ void launch_endobject(const EndArgs &E, int nobj, cudaStream_t st, int &launches
 // catalogue order and output
 // ---------------------------------------------------------------------------
 // survivors compacted in index order (scan of the survivor flags)
-__global__ void k_surv_flags(ObjBufs O, int n, int *flag) {
+__global__ void k_surv_flags(ObjBufs O, int n, const int *n_dev, int *flag) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) flag[i] = O.fmaster[i] < 0 ? 1 : 0;
+    if (i < sx_count(n, n_dev)) flag[i] = O.fmaster[i] < 0 ? 1 : 0;
 }
 
-__global__ void k_surv_compact(ObjBufs O, const int *rymax, const int *rlastx, const int *pos, int n, int w,
-                               int numbering, unsigned *keys, unsigned *vals) {
+__global__ void k_surv_compact(ObjBufs O, const int *rymax, const int *rlastx, const int *pos, int n,
+                               const int *n_dev, int w, int numbering, unsigned *keys, unsigned *vals) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || O.fmaster[i] >= 0) return;
+    if (i >= sx_count(n, n_dev) || O.fmaster[i] >= 0) return;
     int r = O.root[i], j = pos[i];
     keys[j] = numbering == 0 ? (unsigned)rymax[r] * (unsigned)w + (unsigned)rlastx[r] : 0u;
     vals[j] = (unsigned)i;
 }
 
-__global__ void k_number(ObjBufs O, const unsigned *vals, int ns) {
+__global__ void k_number(ObjBufs O, const unsigned *vals, int ns, const int *ns_dev) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < ns) O.number[vals[k]] = k + 1;
+    if (k < sx_count(ns, ns_dev)) O.number[vals[k]] = k + 1;
 }
 
-__global__ void k_write_rows(ObjBufs O, const unsigned *vals, int ns, float dthresh, float thresh,
-                             sexgpu_object *rows) {
+__global__ void k_write_rows(ObjBufs O, const unsigned *vals, int ns, const int *ns_dev, sexgpu_object *rows) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= ns) return;
+    if (k >= sx_count(ns, ns_dev)) return;
     int o = (int)vals[k];
     // built in a union with 16-byte words so that the row, padding bytes
     // included, is stored as whole words (rows are byte-for-byte reproducible)

@@ -11,9 +11,15 @@
 
 namespace sx {
 
-__global__ void k_pos2idx(const unsigned *__restrict__ vals, int *__restrict__ pos2idx, int m) {
+__global__ void k_pos2idx(const unsigned *__restrict__ vals, unsigned *__restrict__ rpix, int *__restrict__ pos2idx,
+                          int m, const int *m_dev) {
+    m = sx_count(m, m_dev);
     int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < m) pos2idx[vals[j]] = j;
+    if (j < m) {
+        const unsigned p = vals[j];
+        rpix[j] = p;
+        pos2idx[p] = j;
+    }
 }
 
 // Each raw object's thresholds: the smallest detection and analysis threshold
@@ -37,7 +43,9 @@ __global__ void k_root_thresholds(const int *__restrict__ lab, const int *__rest
 }
 
 // without a weight map every raw object has the global thresholds
-__global__ void k_root_thresholds_global(int nroots, const FrameScalars *sc, float *rdthr, float *rathr) {
+__global__ void k_root_thresholds_global(int nroots, const int *nroots_dev, const FrameScalars *sc, float *rdthr,
+                                         float *rathr) {
+    nroots = sx_count(nroots, nroots_dev);
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < nroots) {
         rdthr[r] = sc->dthresh;

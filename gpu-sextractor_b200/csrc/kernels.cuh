@@ -158,8 +158,8 @@ struct DebStreams {
     cudaEvent_t fork, join[2];
 };
 
-void launch_deblend_split(const int *size, int nroots, int *lists, int *counts, unsigned *keys, unsigned *vals,
-                          unsigned *kalt, unsigned *valt, int *tmp, cudaStream_t st);
+void launch_deblend_split(const int *size, int nroots, const int *nroots_dev, int *lists, int *counts,
+                          unsigned *keys, unsigned *vals, unsigned *kalt, unsigned *valt, int *tmp, cudaStream_t st);
 int deblend_split_launches(int nroots);
 void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S);
 void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S);

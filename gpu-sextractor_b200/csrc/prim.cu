@@ -197,6 +197,15 @@ size_t radix_temp_ints(long long n) {
     return (size_t)(2 * h + scan_temp_ints(h) + 4);
 }
 
+__global__ void k_copy_pairs(const unsigned *__restrict__ ka, const unsigned *__restrict__ va,
+                             unsigned *__restrict__ kb, unsigned *__restrict__ vb, int n, const int *n_dev) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < dev_count(n, n_dev)) {
+        kb[i] = ka[i];
+        vb[i] = va[i];
+    }
+}
+
 // Stable sort by the low keybits bits of keys.  Result ends in (keys, vals);
 // (kalt, valt) are scratch of n elements each.  n_dev (device, may be NULL):
 // the count, at most n, when only the device knows it (elements beyond it
@@ -218,8 +227,13 @@ void radix_sort_pairs(unsigned *keys, unsigned *vals, unsigned *kalt, unsigned *
         t = va; va = vb; vb = t;
     }
     if (ka != keys) {
-        cudaMemcpyAsync(keys, ka, n * sizeof(unsigned), cudaMemcpyDeviceToDevice, st);
-        cudaMemcpyAsync(vals, va, n * sizeof(unsigned), cudaMemcpyDeviceToDevice, st);
+        if (n_dev) {
+            // only the sorted elements: those beyond the count stay as they are
+            k_copy_pairs<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ka, va, keys, vals, (int)n, n_dev);
+        } else {
+            cudaMemcpyAsync(keys, ka, n * sizeof(unsigned), cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(vals, va, n * sizeof(unsigned), cudaMemcpyDeviceToDevice, st);
+        }
     }
 }
 

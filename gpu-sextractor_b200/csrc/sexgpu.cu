@@ -5,7 +5,10 @@
 // background (makeback), filter + threshold, connected components, deblending
 // (init_deblend/parcel_out), analysis (analyse_gpu), CLEAN (run_clean),
 // photometry/FLAGS (endobject_gpu), catalogue.  All stages run on one CUDA
-// stream; the host reads back four counts per frame to size launches.
+// stream (the deblending forks two more).  In the plain form the host reads
+// back the counts between stages to size the launches; in the capacity form
+// the launches are sized by capacities learned from an earlier frame, the
+// counts stay on the device, and the whole frame is one CUDA graph.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -56,6 +59,14 @@ struct PipeState {
     const float *wvar = nullptr;  // calibrated variance map (weight map given), else null
     int nroots = 0, nrootpix = 0, nobj = 0, ns = 0;
     int stage = 0;  // last completed: 1 background ... 6 catalogue
+    // capacity form: launches sized by these capacities, counts read on the
+    // device only (k_gate stands in for the host checks between stages)
+    bool capf = false;
+    int cap_roots = 0, cap_rootpix = 0, cap_obj = 0;
+    // while the stages are captured: pinned host memory that the frame's
+    // constants (column tables, mask) are copied from, so that the graph holds
+    // its own uploads (8 w + 4 SX_MAXCONV^2 bytes)
+    unsigned char *pin = nullptr;
     BackBufs B;
     RootBufs R;
     DebArgs A;
@@ -65,6 +76,25 @@ struct PipeState {
 namespace sx {
 thread_local int sx_grid_div = 1;
 }
+
+// A captured frame: the graph of the capacity form for one frame geometry,
+// configuration, detection mask and input buffers.
+struct GraphEntry {
+    FrameParams Pm;
+    std::vector<float> mask;
+    const float *d_img = nullptr, *d_wmap = nullptr;
+    const sexgpu_nnw *nnw = nullptr;
+    int kron_warp_max = 0, grid_div = 1;
+    int cap_roots = 0, cap_rootpix = 0, cap_obj = 0;  // 0: not learned yet
+    cudaGraphExec_t exec = nullptr;
+    unsigned char *pin = nullptr;  // pinned constants the graph uploads (PipeState::pin)
+    PipeState ps;                  // host state of the captured frame, restored on replay
+    ObjBufs O;
+    unsigned long long gen = 0;  // allocation generation the graph's pointers belong to
+    bool no_graph = false;       // capture failed: the capacity form runs uncaptured
+    int kernels = 0;             // kernel nodes of the graph
+    unsigned long long used = 0;
+};
 
 struct sexgpu_ctx {
     int device = 0;
@@ -105,6 +135,13 @@ struct sexgpu_ctx {
     const sexgpu_nnw *nnw_dev = nullptr;   // network used (this context's or, for a batch worker, its owner's)
     int kron_warp_max = KR_WARP_MAX;
     int loop_cap = 0;  // "loop_cap" parameter: cap on device walks, for failure tests (0: built-in caps)
+    int graph_mode = 0;                  // "graph" parameter: extract through captured graphs
+    unsigned long long gen = 0;          // bumped by every device allocation (graphs hold pointers)
+    std::vector<GraphEntry> graphs;      // captured frames, least recently used evicted
+    unsigned long long graph_clock = 0;
+    FrameScalars *hsc_pin = nullptr;     // pinned copy of the frame scalars (capacity form)
+    int last_graph = 0;                  // the last extraction replayed a graph
+    int last_kernels = 0;                // kernel launches of the last extraction
     DevBuf sc;
     FrameScalars hsc;
     ObjBufs O;
@@ -162,6 +199,7 @@ int ensure(sexgpu_ctx *ctx, DevBuf &b, size_t bytes) {
         return SEXGPU_ERR_NOMEM;
     }
     b.bytes = want;
+    ctx->gen++;
     return SEXGPU_OK;
 }
 
@@ -173,9 +211,12 @@ int ensure(sexgpu_ctx *ctx, DevBuf &b, size_t bytes) {
 
 template <class T> T *P(DevBuf &b) { return (T *)b.p; }
 
+// stage timing (plain form only: a graph has no per-stage events)
 void stage_begin(sexgpu_ctx *ctx) {
     ctx->stage_names.clear();
     ctx->stage_launches.clear();
+    ctx->stage_ms.clear();
+    if (ctx->ps.capf) return;  // (no event calls while the stages may be captured)
     for (auto &s : ctx->stages) cudaEventDestroy(s.ev);
     ctx->stages.clear();
     if (!ctx->ev0) cudaEventCreate(&ctx->ev0);
@@ -183,6 +224,7 @@ void stage_begin(sexgpu_ctx *ctx) {
 }
 
 void stage_mark(sexgpu_ctx *ctx, const char *name, int launches) {
+    if (ctx->ps.capf) return;
     StageRec s;
     s.name = name;
     s.launches = launches;
@@ -301,6 +343,23 @@ __global__ void k_init_scalars(FrameScalars *sc) {
     *sc = z;
 }
 
+// Capacity form: the checks the plain form makes on the host between stages.
+// An error so far, a zero or negative threshold (check_thr) or a count beyond
+// the capacity the launches were sized for sets the counts the later stages
+// read to 0, and the nl deblending list lengths at lists, so that the rest of
+// the frame does nothing; the status tells the host afterwards.
+__global__ void k_gate(FrameScalars *sc, int check_thr, int cap_roots, int cap_rootpix, int cap_obj, int *lists,
+                       int nl) {
+    int st = sc->status;
+    if (check_thr && (sc->dthresh <= 0.0f || sc->thresh <= 0.0f)) st |= SX_ST_THRESH;
+    if (sc->nroots > cap_roots || sc->nrootpix > cap_rootpix || sc->nobj > cap_obj) st |= SX_ST_CAPACITY;
+    sc->status = st;
+    if (st & SX_ST_STOP) {
+        sc->nroots = sc->nrootpix = sc->nobj = sc->nsurv = 0;
+        for (int k = 0; k < nl; k++) lists[k] = 0;
+    }
+}
+
 // Waits for the work queued on st: a spinning wait (the runtime's default
 // with few host threads), or, for a batch worker told so, a blocking event
 // wait that leaves the host core to the other workers.
@@ -341,7 +400,13 @@ int load_mask(sexgpu_ctx *ctx, const float *mask, int mw, int mh) {
     }
     ctx->hmask.assign(mask, mask + (size_t)mw * mh);
     EN(dmask, sizeof(float) * SX_MAXCONV * SX_MAXCONV);
-    CK(cudaMemcpyAsync(ctx->dmask.p, ctx->hmask.data(), sizeof(float) * mw * mh, cudaMemcpyHostToDevice, ctx->stream));
+    const float *src = ctx->hmask.data();
+    if (ctx->ps.pin) {  // being captured: upload from the graph's pinned copy
+        float *pm = reinterpret_cast<float *>(ctx->ps.pin + (size_t)8 * ctx->ps.w);
+        memcpy(pm, src, sizeof(float) * mw * mh);
+        src = pm;
+    }
+    CK(cudaMemcpyAsync(ctx->dmask.p, src, sizeof(float) * mw * mh, cudaMemcpyHostToDevice, ctx->stream));
     ctx->cmask.dev = P<float>(ctx->dmask);
     ctx->cmask.host = ctx->hmask.data();
     ctx->cmask.mw = mw;
@@ -519,8 +584,15 @@ int pipe_begin(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, 
     int *tmp = P<int>(ctx->scan_tmp);
 
     column_table(w, Pm.nbx, Pm.bw, ctx->colk_h, ctx->coldx_h);
-    CK(cudaMemcpyAsync(B.colk, ctx->colk_h.data(), w * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(B.coldx, ctx->coldx_h.data(), w * 4, cudaMemcpyHostToDevice, st));
+    const void *src_k = ctx->colk_h.data(), *src_dx = ctx->coldx_h.data();
+    if (ps.pin) {  // being captured: upload from the graph's pinned copy
+        memcpy(ps.pin, src_k, (size_t)w * 4);
+        memcpy(ps.pin + (size_t)w * 4, src_dx, (size_t)w * 4);
+        src_k = ps.pin;
+        src_dx = ps.pin + (size_t)w * 4;
+    }
+    CK(cudaMemcpyAsync(B.colk, src_k, w * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(B.coldx, src_dx, w * 4, cudaMemcpyHostToDevice, st));
     rc = load_mask(ctx, cfg->filter_flag ? cfg->conv : nullptr, cfg->conv_w, cfg->conv_h);
     if (rc) return rc;
 
@@ -597,24 +669,36 @@ int pipe_detect(sexgpu_ctx *ctx) {
     k_root_tile_counts<<<ntile, SCAN_THREADS, 0, st>>>(lab, cnt, N, Pm.minarea, troots, tkept);
     exclusive_scan(troots, troff, ntile, &d_sc->nroots, tmp, st);
     exclusive_scan(tkept, tkoff, ntile, nullptr, tmp, st);
-    rc = read_scalars(ctx);
-    if (rc) return rc;
-    if (ctx->hsc.dthresh <= 0.0f || ctx->hsc.thresh <= 0.0f) {
-        ctx->err = "zero or negative threshold";
-        return SEXGPU_ERR_THRESH;
+    // roots (the capacity in the capacity form) and the length of the root
+    // arrays: in the capacity form, the most roots the frame can hold (each
+    // has minarea pixels), since they are numbered before the gate checks
+    int nroots, rlen;
+    if (ps.capf) {
+        nroots = ps.cap_roots;
+        rlen = (int)(N / std::max(Pm.minarea, 1));
+        k_gate<<<1, 1, 0, st>>>(d_sc, 1, ps.cap_roots, ps.cap_rootpix, ps.cap_obj, nullptr, 0);
+    } else {
+        rc = read_scalars(ctx);
+        if (rc) return rc;
+        if (ctx->hsc.dthresh <= 0.0f || ctx->hsc.thresh <= 0.0f) {
+            ctx->err = "zero or negative threshold";
+            return SEXGPU_ERR_THRESH;
+        }
+        nroots = rlen = ctx->hsc.nroots;
     }
-    const int nroots = ps.nroots = ctx->hsc.nroots;
-    EN(rsize, (nroots + 1) * 4);
-    EN(roff, (nroots + 1) * 4);
-    EN(rfirst, (nroots + 1) * 4);
-    EN(rymax, (nroots + 1) * 4);
-    EN(rlastx, (nroots + 1) * 4);
-    EN(rfdpeak, (nroots + 1) * 4);
-    EN(rfdflux, (nroots + 1) * 4);
-    EN(rnkept, (nroots + 1) * 4);
-    EN(robjbase, (nroots + 1) * 4);
-    EN(rdthr, (nroots + 1) * 4);
-    EN(rathr, (nroots + 1) * 4);
+    ps.nroots = nroots;
+    const int *nroots_dev = ps.capf ? &d_sc->nroots : nullptr;
+    EN(rsize, ((size_t)rlen + 1) * 4);
+    EN(roff, ((size_t)rlen + 1) * 4);
+    EN(rfirst, ((size_t)rlen + 1) * 4);
+    EN(rymax, ((size_t)rlen + 1) * 4);
+    EN(rlastx, ((size_t)rlen + 1) * 4);
+    EN(rfdpeak, ((size_t)rlen + 1) * 4);
+    EN(rfdflux, ((size_t)rlen + 1) * 4);
+    EN(rnkept, ((size_t)rlen + 1) * 4);
+    EN(robjbase, ((size_t)rlen + 1) * 4);
+    EN(rdthr, ((size_t)rlen + 1) * 4);
+    EN(rathr, ((size_t)rlen + 1) * 4);
     RootBufs &R = ps.R;
     R.size = P<int>(ctx->rsize);
     R.off = P<int>(ctx->roff);
@@ -628,7 +712,7 @@ int pipe_detect(sexgpu_ctx *ctx) {
     R.dthresh = P<float>(ctx->rdthr);
     R.thresh = P<float>(ctx->rathr);
     k_root_number<<<ntile, SCAN_THREADS, 0, st>>>(lab, cnt, N, Pm.minarea, troff, flag, R.size, R.first);
-    exclusive_scan(R.size, R.off, nroots, &d_sc->nrootpix, tmp, st);
+    exclusive_scan(R.size, R.off, nroots, &d_sc->nrootpix, tmp, st, nroots_dev);
     unsigned *keys = P<unsigned>(ctx->keys), *vals = P<unsigned>(ctx->vals);
     int *pos2idx = P<int>(ctx->pos2idx);
     k_root_compact<<<ntile, SCAN_THREADS, 0, st>>>(lab, cnt, N, Pm.minarea, tkoff, flag, keys, vals,
@@ -640,15 +724,24 @@ int pipe_detect(sexgpu_ctx *ctx) {
                                                          Pm.detect_thresh, Pm.analysis_thresh, d_sc,
                                                          (int *)R.dthresh, (int *)R.thresh);
     } else {
-        k_root_thresholds_global<<<grid1(nroots, 256), 256, 0, st>>>(nroots, d_sc, R.dthresh, R.thresh);
+        k_root_thresholds_global<<<grid1(nroots, 256), 256, 0, st>>>(nroots, nroots_dev, d_sc, R.dthresh,
+                                                                       R.thresh);
     }
-    rc = read_scalars(ctx);
-    if (rc) return rc;
-    const int nrootpix = ps.nrootpix = ctx->hsc.nrootpix;
-    radix_sort_pairs(keys, vals, P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), nrootpix, bits_for(nroots), tmp, st);
+    int nrootpix;
+    if (ps.capf) {
+        nrootpix = ps.cap_rootpix;
+        k_gate<<<1, 1, 0, st>>>(d_sc, 0, ps.cap_roots, ps.cap_rootpix, ps.cap_obj, nullptr, 0);
+    } else {
+        rc = read_scalars(ctx);
+        if (rc) return rc;
+        nrootpix = ctx->hsc.nrootpix;
+    }
+    ps.nrootpix = nrootpix;
+    const int *nrootpix_dev = ps.capf ? &d_sc->nrootpix : nullptr;
+    radix_sort_pairs(keys, vals, P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), nrootpix, bits_for(nroots), tmp, st,
+                     nrootpix_dev);
     unsigned *rpix = P<unsigned>(ctx->rpix);
-    CK(cudaMemcpyAsync(rpix, vals, (size_t)nrootpix * 4, cudaMemcpyDeviceToDevice, st));
-    k_pos2idx<<<grid1(nrootpix, 256), 256, 0, st>>>(rpix, pos2idx, nrootpix);
+    k_pos2idx<<<grid1(nrootpix, 256), 256, 0, st>>>(vals, rpix, pos2idx, nrootpix, nrootpix_dev);
     stage_mark(ctx, "roots", 5 + 2 * scan_launches(ntile) + scan_launches(nroots) + radix_launches(bits_for(nroots), nrootpix));
     ps.stage = 2;
     return SEXGPU_OK;
@@ -746,13 +839,22 @@ int pipe_deblend(sexgpu_ctx *ctx) {
     S.fork = ctx->ev_fork;
     S.join[0] = ctx->ev_join[0];
     S.join[1] = ctx->ev_join[1];
-    launch_deblend_split(R.size, nroots, P<int>(ctx->rlists), P<int>(ctx->rcounts), P<unsigned>(ctx->keys),
+    const int *nroots_dev = ps.capf ? &d_sc->nroots : nullptr;
+    launch_deblend_split(R.size, nroots, nroots_dev, P<int>(ctx->rlists), P<int>(ctx->rcounts), P<unsigned>(ctx->keys),
                          P<unsigned>(ctx->vals), P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), tmp, st);
     launch_deblend_sweep(A, P<int>(ctx->rlists), P<int>(ctx->rcounts), nroots, S);
-    exclusive_scan(R.nkept, R.objbase, nroots, &d_sc->nobj, tmp, st);
-    rc = read_scalars(ctx);
-    if (rc) return rc;
-    const int nobj = ps.nobj = ctx->hsc.nobj;
+    exclusive_scan(R.nkept, R.objbase, nroots, &d_sc->nobj, tmp, st, nroots_dev);
+    int nobj;
+    if (ps.capf) {
+        // a stop also empties the size-class lists, so that no branch is assigned
+        nobj = ps.cap_obj;
+        k_gate<<<1, 1, 0, st>>>(d_sc, 0, ps.cap_roots, ps.cap_rootpix, ps.cap_obj, P<int>(ctx->rcounts), DL_NLISTS);
+    } else {
+        rc = read_scalars(ctx);
+        if (rc) return rc;
+        nobj = ctx->hsc.nobj;
+    }
+    ps.nobj = nobj;
     ctx->cfg_local = Pm.bp_local != 0;
     rc = alloc_objects(ctx, nobj);
     if (rc) return rc;
@@ -777,8 +879,10 @@ int pipe_analyse(sexgpu_ctx *ctx) {
     unsigned *rpix = P<unsigned>(ctx->rpix);
     // ---- object pixel lists (stable by object id: raster order inside)
     ObjBufs &O = ctx->O;
-    exclusive_scan(O.n, O.off, nobj, nullptr, tmp, st);
-    launch_obj_partition(rpix, A.objkey, ps.R, O.off, ps.nroots, vals, P<int>(ctx->kalt), st);
+    const int *nobj_dev = ps.capf ? &d_sc->nobj : nullptr;
+    exclusive_scan(O.n, O.off, nobj, nullptr, tmp, st, nobj_dev);
+    launch_obj_partition(rpix, A.objkey, ps.R, O.off, ps.nroots, ps.capf ? &d_sc->nroots : nullptr, vals,
+                         P<int>(ctx->kalt), st);
     AnaArgs AA;
     EN(o_raw, (size_t)(nobj + 1) * sizeof(RobustRaw));
     AA.raw = P<RobustRaw>(ctx->o_raw);
@@ -797,6 +901,7 @@ int pipe_analyse(sexgpu_ctx *ctx) {
     AA.bw = Pm.bw;
     AA.bh = Pm.bh;
     AA.nobj = nobj;
+    AA.nobj_dev = nobj_dev;
     AA.minarea = Pm.minarea;
     AA.clean_flag = Pm.clean_flag;
     AA.gain = Pm.gain;
@@ -839,21 +944,39 @@ int pipe_clean(sexgpu_ctx *ctx) {
         int *cellcnt = P<int>(ctx->cellhead), *cellcur = P<int>(ctx->cellnext);
         CK(cudaMemsetAsync(cellcnt, 0, (size_t)(ncell + 1) * 4, st));
         CK(cudaMemsetAsync(cellcur, 0, (size_t)(ncell + 1) * 4, st));
-        k_clean_count<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, cellcnt, gx, gy);
+        const int *nobj_dev = ps.capf ? &d_sc->nobj : nullptr;
+        k_clean_count<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, nobj_dev, cellcnt, gx, gy);
         exclusive_scan(cellcnt, cellcnt, ncell + 1, nullptr, tmp, st);
-        k_clean_pack<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, Pm.clean_param, cellcnt, cellcur,
+        k_clean_pack<<<grid1(nobj, 128), 128, 0, st>>>(O, nobj, nobj_dev, Pm.clean_param, cellcnt, cellcur,
                                                        P<CleanObj>(ctx->amp), gx, gy);
-        k_clean_pairs<<<(unsigned)nobj, CL_PAIR_WARPS * 32, 0, st>>>(P<CleanObj>(ctx->amp), nobj, Pm.clean_param,
-                                                                      cellcnt, O.master, gx, gy);
+        k_clean_pairs<<<(unsigned)nobj, CL_PAIR_WARPS * 32, 0, st>>>(P<CleanObj>(ctx->amp), nobj, nobj_dev,
+                                                                      Pm.clean_param, cellcnt, O.master, gx, gy);
         CK(cudaMemsetAsync(&d_sc->nsurv, 0, 4, st));
-        k_clean_chain<<<grid1(nobj, 256), 256, 0, st>>>(O, nobj, P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval),
-                                                        &d_sc->nsurv, &d_sc->status, Pm.loop_cap);
+        k_clean_chain<<<grid1(nobj, 256), 256, 0, st>>>(O, nobj, nobj_dev, P<unsigned>(ctx->vkey),
+                                                        P<unsigned>(ctx->vval), &d_sc->nsurv, &d_sc->status,
+                                                        Pm.loop_cap);
+        if (ps.capf) {
+            // the victim count stays on the device: the one-block sort takes
+            // short lists, the radix sorts (counted by nvbig) long ones
+            unsigned *vkey = P<unsigned>(ctx->vkey), *vval = P<unsigned>(ctx->vval);
+            k_gate<<<1, 1, 0, st>>>(d_sc, 0, ps.cap_roots, ps.cap_rootpix, ps.cap_obj, nullptr, 0);
+            k_victim_sort<<<1, 1024, 0, st>>>(vkey, vval, nobj, &d_sc->nsurv, &d_sc->nvbig);
+            radix_sort_pairs(vval, vkey, P<unsigned>(ctx->vkalt), P<unsigned>(ctx->vvalt), nobj, bits_for(nobj), tmp,
+                             st, &d_sc->nvbig);
+            radix_sort_pairs(vkey, vval, P<unsigned>(ctx->vkalt), P<unsigned>(ctx->vvalt), nobj, bits_for(nobj), tmp,
+                             st, &d_sc->nvbig);
+            k_clean_merge<<<grid1(nobj, 128), 128, 0, st>>>(O, vkey, vval, nobj, &d_sc->nsurv);
+            k_alloc_victims<<<nobj, 128, 0, st>>>(O, vals, A.alloc, nobj, nobj_dev);
+            stage_mark(ctx, "clean", 0);
+            ps.stage = 5;
+            return SEXGPU_OK;
+        }
         rc = read_scalars(ctx);
         if (rc) return rc;
         nv = ctx->hsc.nsurv;
         int sort_launches = 0;
         if (nv > 0 && nv <= CL_SORT_MAX) {
-            k_victim_sort<<<1, 1024, 0, st>>>(P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval), nv);
+            k_victim_sort<<<1, 1024, 0, st>>>(P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval), nv, nullptr, nullptr);
             sort_launches = 1;
         } else if (nv > 0) {
             radix_sort_pairs(P<unsigned>(ctx->vval), P<unsigned>(ctx->vkey), P<unsigned>(ctx->vkalt),
@@ -863,8 +986,9 @@ int pipe_clean(sexgpu_ctx *ctx) {
             sort_launches = 2 * radix_launches(bits_for(nobj), nv);
         }
         if (nv > 0) {
-            k_clean_merge<<<grid1(nv, 128), 128, 0, st>>>(O, P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval), nv);
-            k_alloc_victims<<<nobj, 128, 0, st>>>(O, vals, A.alloc, nobj);
+            k_clean_merge<<<grid1(nv, 128), 128, 0, st>>>(O, P<unsigned>(ctx->vkey), P<unsigned>(ctx->vval), nv,
+                                                          nullptr);
+            k_alloc_victims<<<nobj, 128, 0, st>>>(O, vals, A.alloc, nobj, nullptr);
         }
         cl_launch = 6 + scan_launches(ncell + 1) + sort_launches;
     } else if (nobj > 0) {
@@ -898,6 +1022,8 @@ int pipe_end(sexgpu_ctx *ctx) {
     E.w = w;
     E.h = h;
     E.n = nobj;
+    const int *nobj_dev = ps.capf ? &d_sc->nobj : nullptr;
+    E.n_dev = nobj_dev;
     E.mask_type = Pm.mask_type;
     E.aperture = Pm.aperture;
     E.naper = Pm.naper;
@@ -933,24 +1059,39 @@ int pipe_end(sexgpu_ctx *ctx) {
     EN(svalt, (size_t)(nobj + 1) * 4);
     int *sflag = P<int>(ctx->cnt);  // free now
     CK(cudaMemsetAsync(O.number, 0, (size_t)(nobj + 1) * 4, st));
-    k_surv_flags<<<grid1(nobj + 1, 256), 256, 0, st>>>(O, nobj, sflag);
-    exclusive_scan(sflag, sflag, nobj, &d_sc->nsurv, tmp, st);
-    rc = read_scalars(ctx);
-    if (rc) return rc;
-    const int ns = ctx->hsc.nsurv;
-    k_surv_compact<<<grid1(nobj + 1, 256), 256, 0, st>>>(O, R.ymax, R.lastx, sflag, nobj, w, Pm.numbering,
+    k_surv_flags<<<grid1(nobj + 1, 256), 256, 0, st>>>(O, nobj, nobj_dev, sflag);
+    exclusive_scan(sflag, sflag, nobj, &d_sc->nsurv, tmp, st, nobj_dev);
+    int ns;
+    if (ps.capf) {
+        ns = nobj;
+        k_gate<<<1, 1, 0, st>>>(d_sc, 0, ps.cap_roots, ps.cap_rootpix, ps.cap_obj, nullptr, 0);
+    } else {
+        rc = read_scalars(ctx);
+        if (rc) return rc;
+        ns = ctx->hsc.nsurv;
+    }
+    const int *ns_dev = ps.capf ? &d_sc->nsurv : nullptr;
+    k_surv_compact<<<grid1(nobj + 1, 256), 256, 0, st>>>(O, R.ymax, R.lastx, sflag, nobj, nobj_dev, w, Pm.numbering,
                                                          P<unsigned>(ctx->skeys), P<unsigned>(ctx->svals));
     // completion keys are below w*h; first-pixel numbering has all keys 0
     // (the survivors are already in index order)
     const int cbits = Pm.numbering == 0 ? bits_for((long long)w * h - 1) : 0;
     radix_sort_pairs(P<unsigned>(ctx->skeys), P<unsigned>(ctx->svals), P<unsigned>(ctx->skalt),
-                     P<unsigned>(ctx->svalt), ns, cbits, tmp, st);
-    k_number<<<grid1(ns + 1, 256), 256, 0, st>>>(O, P<unsigned>(ctx->svals), ns);
+                     P<unsigned>(ctx->svalt), ns, cbits, tmp, st, ns_dev);
+    k_number<<<grid1(ns + 1, 256), 256, 0, st>>>(O, P<unsigned>(ctx->svals), ns, ns_dev);
     EN(rows, (size_t)(ns + 1) * sizeof(sexgpu_object));
-    k_write_rows<<<grid1(ns + 1, 128), 128, 0, st>>>(O, P<unsigned>(ctx->svals), ns, ctx->hsc.dthresh,
-                                                     ctx->hsc.thresh, P<sexgpu_object>(ctx->rows));
+    k_write_rows<<<grid1(ns + 1, 128), 128, 0, st>>>(O, P<unsigned>(ctx->svals), ns, ns_dev,
+                                                     P<sexgpu_object>(ctx->rows));
     stage_mark(ctx, "catalog", 5 + scan_launches(nobj) + radix_launches(cbits, ns));
     CK(cudaGetLastError());
+    if (ps.capf) {
+        // the scalars come back with the frame; the host reads them after the
+        // stream (or the graph) has finished
+        CK(cudaMemcpyAsync(ctx->hsc_pin, d_sc, sizeof(FrameScalars), cudaMemcpyDeviceToHost, st));
+        ps.ns = ns;
+        ps.stage = 6;
+        return SEXGPU_OK;
+    }
     rc = read_scalars(ctx);
     if (rc) return rc;
     stage_collect(ctx);
@@ -972,6 +1113,222 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w
     if (!rc) rc = pipe_clean(ctx);
     if (!rc) rc = pipe_end(ctx);
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Extraction through captured graphs ("graph" parameter).  A frame kind (the
+// frame geometry, the configuration, the detection mask, the input buffers)
+// is first extracted in the plain form, which gives its counts; capacities a
+// quarter above them size the capacity form, which the next frame of that
+// kind runs uncaptured (allocating what it needs) and then captures: from the
+// frame after on, a frame is one cudaGraphLaunch and one wait for the
+// scalars.  A frame whose counts exceed the capacities is extracted again in
+// the plain form and the capacities grow.
+// ---------------------------------------------------------------------------
+constexpr int GRAPH_CACHE = 8;  // frame kinds kept per context
+
+int cap_of(long long count, long long bound) {
+    const long long c = count + count / 4 + 256;
+    return (int)std::max(0ll, std::min(c, bound));
+}
+
+void learn_caps(const sexgpu_ctx *ctx, GraphEntry &e, long long N, int minarea) {
+    e.cap_roots = std::max(e.cap_roots, cap_of(ctx->hsc.nroots, N / std::max(minarea, 1)));
+    e.cap_rootpix = std::max(e.cap_rootpix, cap_of(ctx->hsc.nrootpix, N));
+    e.cap_obj = std::max(e.cap_obj, cap_of(ctx->hsc.nobj, N));
+}
+
+void drop_graph(GraphEntry &e) {
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+    if (e.pin) cudaFreeHost(e.pin);
+    e.exec = nullptr;
+    e.pin = nullptr;
+}
+
+// status of a capacity-form frame from its scalars: 1 when it must be
+// extracted again in the plain form (a count beyond its capacity)
+int capacity_status(sexgpu_ctx *ctx) {
+    const int s = ctx->hsc.status;
+    if (s & SX_ST_LOAD) {
+        ctx->err = "a tile load did not complete in time; destroy this context";
+        return SEXGPU_ERR_LOAD;
+    }
+    if (s & SX_ST_CAPACITY) return 1;
+    if (s & SX_ST_LOOP) {
+        ctx->err = "device loop iteration cap reached";
+        return SEXGPU_ERR_LOOP;
+    }
+    if (s & SX_ST_RANGE) {
+        ctx->err = "exact sum out of range";
+        return SEXGPU_ERR_RANGE;
+    }
+    if (s & SX_ST_THRESH) {
+        ctx->err = "zero or negative threshold";
+        return SEXGPU_ERR_THRESH;
+    }
+    return SEXGPU_OK;
+}
+
+void set_caps(PipeState &ps, const GraphEntry &e) {
+    ps.cap_roots = e.cap_roots;
+    ps.cap_rootpix = e.cap_rootpix;
+    ps.cap_obj = e.cap_obj;
+}
+
+// Captures the capacity form of the frame just extracted; a capture that
+// fails leaves the frame kind to the uncaptured capacity form.
+void capture_graph(sexgpu_ctx *ctx, GraphEntry &e, const float *d_img, const float *d_wmap, int w, int h,
+                   const sexgpu_config *cfg) {
+    PipeState &ps = ctx->ps;
+    cudaStream_t st = ctx->stream;
+    if (!e.pin && cudaMallocHost((void **)&e.pin, (size_t)8 * w + 4 * SX_MAXCONV * SX_MAXCONV) != cudaSuccess) {
+        cudaGetLastError();
+        e.pin = nullptr;
+        e.no_graph = true;
+        return;
+    }
+    const unsigned long long gen0 = ctx->gen;
+    cudaGraph_t g = nullptr;
+    ps.capf = true;
+    ps.pin = e.pin;
+    set_caps(ps, e);
+    int rc = SEXGPU_ERR_CUDA;
+    cudaError_t ce = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+        rc = run_pipeline(ctx, d_img, d_wmap, w, h, cfg);
+        ce = cudaStreamEndCapture(st, &g);
+    }
+    ps.capf = false;
+    ps.pin = nullptr;
+    if (ce == cudaSuccess && rc == SEXGPU_OK && g && ctx->gen == gen0) {
+        size_t n = 0;
+        if (cudaGraphGetNodes(g, nullptr, &n) == cudaSuccess) {
+            std::vector<cudaGraphNode_t> nodes(n);
+            cudaGraphGetNodes(g, nodes.data(), &n);
+            e.kernels = 0;
+            for (cudaGraphNode_t nd : nodes) {
+                cudaGraphNodeType t;
+                if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) e.kernels++;
+            }
+        }
+        ce = cudaGraphInstantiate(&e.exec, g, 0);
+        if (ce != cudaSuccess) e.exec = nullptr;
+    }
+    if (g) cudaGraphDestroy(g);
+    if (!e.exec) {
+        cudaGetLastError();
+        e.no_graph = true;
+        return;
+    }
+    e.gen = ctx->gen;
+    e.ps = ps;
+    e.O = ctx->O;
+}
+
+// host state after a capacity-form frame (the counts come from its scalars)
+void finish_capacity(sexgpu_ctx *ctx, int w, int h) {
+    PipeState &ps = ctx->ps;
+    ps.nroots = ctx->hsc.nroots;
+    ps.nrootpix = ctx->hsc.nrootpix;
+    ps.nobj = ctx->hsc.nobj;
+    ps.ns = ctx->hsc.nsurv;
+    ps.stage = 6;
+    ctx->last_w = w;
+    ctx->last_h = h;
+    ctx->last_nobj = ctx->hsc.nobj;
+    ctx->last_ns = ctx->hsc.nsurv;
+}
+
+int run_graph(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, int h, const sexgpu_config *cfg) {
+    ctx->last_graph = 0;
+    ctx->last_kernels = 0;
+    if (check_config(cfg, w, h) || (cfg->weight_type >= 1 && cfg->weight_type <= 3) != (d_wmap != nullptr))
+        return run_pipeline(ctx, d_img, d_wmap, w, h, cfg);  // reports the error
+    FrameParams Pm;
+    make_params(cfg, w, h, Pm);
+    Pm.loop_cap = ctx->loop_cap;
+    std::vector<float> mask(1, 1.0f);
+    if (cfg->filter_flag) mask.assign(cfg->conv, cfg->conv + (size_t)cfg->conv_w * cfg->conv_h);
+    GraphEntry *e = nullptr;
+    for (GraphEntry &x : ctx->graphs)
+        if (!memcmp(&x.Pm, &Pm, sizeof(Pm)) && x.mask == mask && x.d_img == d_img && x.d_wmap == d_wmap &&
+            x.nnw == ctx->nnw_dev && x.kron_warp_max == ctx->kron_warp_max && x.grid_div == sx_grid_div) {
+            e = &x;
+            break;
+        }
+    if (!e) {
+        if ((int)ctx->graphs.size() >= GRAPH_CACHE) {
+            auto old = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
+                                        [](const GraphEntry &a, const GraphEntry &b) { return a.used < b.used; });
+            drop_graph(*old);
+            ctx->graphs.erase(old);
+        }
+        ctx->graphs.emplace_back();
+        e = &ctx->graphs.back();
+        e->Pm = Pm;
+        e->mask = mask;
+        e->d_img = d_img;
+        e->d_wmap = d_wmap;
+        e->nnw = ctx->nnw_dev;
+        e->kron_warp_max = ctx->kron_warp_max;
+        e->grid_div = sx_grid_div;
+    }
+    e->used = ++ctx->graph_clock;
+    const long long N = (long long)w * h;
+    if (!e->cap_obj) {  // a new frame kind: the plain form, and its counts
+        int rc = run_pipeline(ctx, d_img, d_wmap, w, h, cfg);
+        if (!rc) learn_caps(ctx, *e, N, Pm.minarea);
+        return rc;
+    }
+    if (!ctx->hsc_pin) {
+        if (cudaMallocHost((void **)&ctx->hsc_pin, sizeof(FrameScalars)) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->hsc_pin = nullptr;
+            ctx->err = "pinned host allocation failed";
+            return SEXGPU_ERR_NOMEM;
+        }
+    }
+    cudaStream_t st = ctx->stream;
+    const bool replay = e->exec && e->gen == ctx->gen;
+    int rc = SEXGPU_OK;
+    if (replay) {
+        ctx->ps = e->ps;
+        ctx->O = e->O;
+        ctx->cfg_local = Pm.bp_local != 0;
+        ctx->hmask = mask;
+        ctx->stage_ms.clear();
+        ctx->stage_names.clear();
+        ctx->stage_launches.clear();
+        CK(cudaGraphLaunch(e->exec, st));
+        ctx->last_graph = 1;
+        ctx->last_kernels = e->kernels;
+    } else {
+        drop_graph(*e);
+        ctx->ps.capf = true;
+        set_caps(ctx->ps, *e);
+        rc = run_pipeline(ctx, d_img, d_wmap, w, h, cfg);
+        ctx->ps.capf = false;
+        if (rc) return rc;
+    }
+    CK(stream_wait(ctx, st));
+    ctx->hsc = *ctx->hsc_pin;
+    rc = capacity_status(ctx);
+    if (rc == 1) {  // counts beyond the capacities: plain form, larger capacities
+        ctx->last_graph = 0;
+        ctx->last_kernels = 0;
+        drop_graph(*e);
+        e->no_graph = false;
+        rc = run_pipeline(ctx, d_img, d_wmap, w, h, cfg);
+        if (!rc) learn_caps(ctx, *e, N, Pm.minarea);
+        return rc;
+    }
+    if (rc) return rc;
+    finish_capacity(ctx, w, h);
+    if (!replay && !e->no_graph) {
+        capture_graph(ctx, *e, d_img, d_wmap, w, h, cfg);
+        finish_capacity(ctx, w, h);
+    }
+    return SEXGPU_OK;
 }
 
 
@@ -1083,6 +1440,9 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_block) cudaEventDestroy(ctx->ev_block);
+    for (GraphEntry &e : ctx->graphs) drop_graph(e);
+    ctx->graphs.clear();
+    if (ctx->hsc_pin) cudaFreeHost(ctx->hsc_pin);
     for (sexgpu_ctx *w : ctx->workers) sexgpu_destroy(w);
     for (void *p : ctx->graveyard) cudaFree(p);
     for (void *p : ctx->host_graveyard) cudaFreeHost(p);
@@ -1146,7 +1506,7 @@ int sexgpu_extract_device(sexgpu_ctx *ctx, const float *d_img, const float *d_va
     if (!ctx || !d_img) return SEXGPU_ERR_ARG;
     cudaSetDevice(ctx->device);
     ctx->err.clear();
-    int rc = run_pipeline(ctx, d_img, d_var, w, h, cfg);
+    int rc = ctx->graph_mode ? run_graph(ctx, d_img, d_var, w, h, cfg) : run_pipeline(ctx, d_img, d_var, w, h, cfg);
     if (rc == SEXGPU_OK && sum) {
         FrameParams Pm;
         make_params(cfg, w, h, Pm);
@@ -1657,6 +2017,11 @@ int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value) {
         ctx->kron_warp_max = value;
         return SEXGPU_OK;
     }
+    if (!strcmp(name, "graph")) {
+        if (value < 0 || value > 1) return SEXGPU_ERR_ARG;
+        ctx->graph_mode = value;
+        return SEXGPU_OK;
+    }
     if (!strcmp(name, "loop_cap")) {
         if (value < 0) return SEXGPU_ERR_ARG;
         ctx->loop_cap = value;
@@ -1664,6 +2029,18 @@ int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value) {
     }
     ctx->err = std::string("unknown parameter ") + name;
     return SEXGPU_ERR_ARG;
+}
+
+int sexgpu_graph_stats(sexgpu_ctx *ctx, int *replayed, int *kernels, int *kinds) {
+    if (!ctx) return SEXGPU_ERR_ARG;
+    if (replayed) *replayed = ctx->last_graph;
+    if (kernels) *kernels = ctx->last_kernels;
+    if (kinds) {
+        int n = 0;
+        for (const GraphEntry &e : ctx->graphs) n += e.exec != nullptr;
+        *kinds = n;
+    }
+    return SEXGPU_OK;
 }
 
 int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max) {

@@ -125,7 +125,7 @@ EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extra
            "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times", "sexgpu_set_param",
            "sexgpu_read_nnw", "sexgpu_set_nnw", "sexgpu_extract_fits", "sexgpu_background_rms",
            "sexgpu_background_noalloc", "sexgpu_background_meshes", "sexgpu_background_map", "sexgpu_copy_apertures",
-           "sexgpu_extract_batch"]
+           "sexgpu_extract_batch", "sexgpu_graph_stats"]
 
 _lib = None
 
@@ -371,6 +371,12 @@ class Context:
     def set_param(self, name, value):
         """Execution parameter (results do not depend on it), e.g. kron_warp_max."""
         _check(lib().sexgpu_set_param(self.h, name.encode(), int(value)), self.h, "sexgpu_set_param")
+
+    def graph_stats(self):
+        """(replayed, kernels, kinds) of the last extraction (sexgpu_graph_stats)."""
+        r, k, n = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().sexgpu_graph_stats(self.h, C.byref(r), C.byref(k), C.byref(n)), self.h, "sexgpu_graph_stats")
+        return r.value, k.value, n.value
 
     def stage_times(self):
         st = (Stage * 32)()

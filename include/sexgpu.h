@@ -319,9 +319,23 @@ int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max);
  * every union-find walk, union retry and CLEAN chain walk of the following
  * extractions at n steps (a walk that runs out returns SEXGPU_ERR_LOOP and the
  * context stays usable); 0 (default) keeps the built-in caps, which no valid
- * frame reaches -- it exists to test the error path.  Returns SEXGPU_ERR_ARG
- * for an unknown name or value. */
+ * frame reaches -- it exists to test the error path.  "graph": 1 extracts
+ * through captured CUDA graphs (default 0).  The first frame of a kind (frame
+ * size, configuration, detection mask, input buffers and the parameters
+ * above) runs as without the parameter and sets capacities a quarter above its
+ * counts; the next one runs sized by those capacities, with every count kept
+ * on the device, and is captured; each later one is a single graph launch
+ * and one wait.  A frame whose counts exceed the capacities is extracted again
+ * without the graph and the capacities grow.  The catalogue is the same in
+ * every case; per-stage times are not kept for graph frames.  Returns
+ * SEXGPU_ERR_ARG for an unknown name or value. */
 int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value);
+
+/* How the last extraction of this context ran: *replayed 1 when it was a
+ * captured graph launch, *kernels the kernel launches of that graph (0
+ * otherwise), *kinds the frame kinds this context holds graphs for.  Any
+ * pointer may be NULL. */
+int sexgpu_graph_stats(sexgpu_ctx *ctx, int *replayed, int *kernels, int *kinds);
 
 #ifdef __cplusplus
 }
