@@ -377,7 +377,7 @@ def run_batch(ctx, frames, reps=5, workers=8, maxobj=400000):
             differing.append({"frame": i, "shape": list(frames[i][0].shape), "objects": [len(a), len(b)],
                               "columns": cols[:8]})
     nobj = sum(len(c) for c in ref)
-    t_plain = t_batch = float("inf")
+    t_plain = t_batch = t_graph = float("inf")
     for _ in range(reps):
         t0 = time.perf_counter()
         plain()
@@ -385,6 +385,17 @@ def run_batch(ctx, frames, reps=5, workers=8, maxobj=400000):
         t0 = time.perf_counter()
         batched()
         t_batch = min(t_batch, time.perf_counter() - t0)
+    # the batched form through captured graphs: each worker keeps the frame
+    # kinds it met (two warm-up batches learn the counts and capture)
+    ctx.set_param("graph", 1)
+    batched()
+    got_g = batched()
+    identical_g = len(ref) == len(got_g) and all(a.tobytes() == b.tobytes() for a, b in zip(ref, got_g))
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        batched()
+        t_graph = min(t_graph, time.perf_counter() - t0)
+    ctx.set_param("graph", 0)
     npx = sum(f.size for f, _ in frames)
     return {"workload": "c3: 64 frames (16x 4096x2048, 24x 1024^2, 16x 512^2, 8x 4096^2) cut from four "
                         "seeded 4096^2 fields of density 2e-4..1e-2 px^-2; BACK_SIZE 32/64/128 and "
@@ -396,6 +407,10 @@ def run_batch(ctx, frames, reps=5, workers=8, maxobj=400000):
                       "s": round(t_plain, 4)},
             "batched": {"frames_per_s": round(len(frames) / t_batch, 2),
                         "mobj_per_s": round(nobj / t_batch / 1e6, 4), "s": round(t_batch, 4)},
+            "batched_graph": {"frames_per_s": round(len(frames) / t_graph, 2),
+                              "mobj_per_s": round(nobj / t_graph / 1e6, 4), "s": round(t_graph, 4),
+                              "objects_ratio": round(t_plain / t_graph, 3),
+                              "identical_catalogues": bool(identical_g)},
             "objects_ratio": round(t_plain / t_batch, 3), "identical_catalogues": bool(identical),
             "host": host_state(frames),
             **({"differing": differing} if differing else {})}

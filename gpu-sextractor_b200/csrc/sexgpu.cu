@@ -17,6 +17,7 @@
 #include <atomic>
 #include <string>
 #include <thread>
+#include <mutex>
 #include <vector>
 
 #include "sexgpu.h"
@@ -154,6 +155,7 @@ struct sexgpu_ctx {
     std::vector<std::string> stage_names;
     std::vector<int> stage_launches;
     std::vector<sexgpu_ctx *> workers;  // contexts of sexgpu_extract_batch
+    std::vector<unsigned long long> batch_kinds;  // frame kinds a batch worker has extracted
     // buffers outgrown during a batch: freed when the batch ends, because
     // cudaFree waits for the whole device and would stall the other workers
     bool defer_free = false;
@@ -1831,6 +1833,7 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
         w->nnw_dev = ctx->nnw_dev;
         w->sync_block = ctx->batch_sync;
         w->defer_free = true;
+        w->graph_mode = ctx->graph_mode;
     }
     // largest frames first, so that the last frames to start are short
     std::vector<int> order(nframes);
@@ -1839,6 +1842,55 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
         return (long long)frames[a].w * frames[a].h > (long long)frames[b].w * frames[b].h;
     });
     std::atomic<int> next(0);
+    // With graphs, a worker takes the next frame of a kind it has met before
+    // (its graphs stay with it across batches), else the next frame: kinds
+    // are keyed by size, configuration and mask.
+    std::vector<unsigned long long> kind(nframes, 0);
+    std::vector<char> taken(nframes, 0);
+    std::mutex pick_mu;
+    if (ctx->graph_mode)
+        for (int i = 0; i < nframes; i++) {
+            const sexgpu_batch_frame &f = frames[i];
+            unsigned long long hsh = 1469598103934665603ull;
+            auto mix = [&](const void *p, size_t n) {
+                for (size_t k = 0; k < n; k++) hsh = (hsh ^ ((const unsigned char *)p)[k]) * 1099511628211ull;
+            };
+            if (f.cfg && f.w > 0 && f.h > 0) {
+                FrameParams Pm;
+                make_params(f.cfg, f.w, f.h, Pm);
+                mix(&Pm, sizeof(Pm));
+                if (f.cfg->filter_flag && f.cfg->conv)
+                    mix(f.cfg->conv, sizeof(float) * (size_t)std::max(f.cfg->conv_w, 0) * std::max(f.cfg->conv_h, 0));
+            }
+            const int hasw = f.wmap != nullptr;
+            mix(&hasw, sizeof(hasw));
+            kind[i] = hsh;
+        }
+    auto pick = [&](sexgpu_ctx *wc) -> int {
+        if (!ctx->graph_mode) {
+            const int k = next.fetch_add(1);
+            return k < nframes ? order[k] : -1;
+        }
+        std::lock_guard<std::mutex> lk(pick_mu);
+        int first = -1;
+        for (int k = 0; k < nframes; k++) {
+            const int i = order[k];
+            if (taken[i]) continue;
+            if (first < 0) first = i;
+            if (std::find(wc->batch_kinds.begin(), wc->batch_kinds.end(), kind[i]) != wc->batch_kinds.end()) {
+                first = i;
+                break;
+            }
+        }
+        if (first >= 0) {
+            taken[first] = 1;
+            if (std::find(wc->batch_kinds.begin(), wc->batch_kinds.end(), kind[first]) == wc->batch_kinds.end()) {
+                wc->batch_kinds.push_back(kind[first]);
+                if ((int)wc->batch_kinds.size() > 4 * GRAPH_CACHE) wc->batch_kinds.erase(wc->batch_kinds.begin());
+            }
+        }
+        return first;
+    };
     // Each worker copies its frame (and weight map) into its own pinned buffer
     // first and brings the catalogue rows back through another, so that the
     // transfers of different workers are DMA transfers that proceed in
@@ -1861,8 +1913,8 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
     auto run = [&](sexgpu_ctx *wc) {
         cudaSetDevice(wc->device);
         sx_grid_div = div;
-        for (int k; (k = next.fetch_add(1)) < nframes;) {
-            sexgpu_batch_frame &f = frames[order[k]];
+        for (int fi; (fi = pick(wc)) >= 0;) {
+            sexgpu_batch_frame &f = frames[fi];
             f.nobj = 0;
             if (!f.img || !f.cfg || f.w <= 0 || f.h <= 0 || f.max_objects < 0 || (f.max_objects > 0 && !f.objs)) {
                 f.status = SEXGPU_ERR_ARG;

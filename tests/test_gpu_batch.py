@@ -38,3 +38,24 @@ def test_batch_with_weight_map(gpu_ctx, masks):
     (cat, summ), = gpu_ctx.extract_batch([(img, kw, vm)], workers=1)
     ref, _, s = gpu_ctx.extract(img, weight=vm, **kw)
     assert cat.tobytes() == ref.tobytes() and summ.sigfac == s.sigfac
+
+
+def test_batch_through_graphs(masks):
+    """The batch with the "graph" parameter: frames of a few kinds (size,
+    settings) repeated; over three batches every worker learns, captures and
+    replays its kinds, and every frame's catalogue is the plain one."""
+    import sexgpu
+    kinds = [((1024, 512), dict(back_size=32, conv=masks["gauss_2.0_3x3"])),
+             ((512, 512), dict(back_size=64, conv=masks["gauss_3.0_7x7"])),
+             ((700, 300), dict(back_size=64, conv=masks["mexhat_2.5_7x7"], clean_flag=0))]
+    frames = []
+    for i in range(12):
+        (w, h), kw = kinds[i % 3]
+        frames.append((synth.frame_c1(seed=60 + i, w=w, h=h, density=4e-3 + 1e-3 * (i % 4)), kw))
+    with sexgpu.Context(0) as plain, sexgpu.Context(0) as ctx:
+        ref = [plain.extract(img, **kw)[0] for img, kw in frames]
+        ctx.set_param("graph", 1)
+        for _ in range(3):
+            got = ctx.extract_batch(frames, workers=3)
+            for r, (cat, _) in zip(ref, got):
+                assert cat.tobytes() == r.tobytes()
