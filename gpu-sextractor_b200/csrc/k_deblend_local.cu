@@ -149,6 +149,54 @@ __device__ __forceinline__ void dl_activate_union(const DebArgs &A, int off, int
     __syncthreads();
 }
 
+// deblending level of a filtered value: the highest L with c >= thr[L]
+__device__ __forceinline__ int dl_level_of(float c, const float *thr, int N) {
+    int lo = 0, hi = N - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (c >= thr[mid])
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// An object whose filtered values have a single local maximum (one pixel
+// with no 8-neighbour in the object strictly above it) cannot be split:
+// every superlevel set of it is connected, because each component of one
+// holds a pixel with no neighbour above it (its maximum: neighbours inside
+// the component are not above it, neighbours outside it are below the level
+// or, being adjacent, would belong to it).  The sweep's result for such an
+// object is the whole object, kept at level 0.  Neighbours in the object are
+// those with a root-list index (pixels of two roots are never adjacent).
+template <int NT>
+__device__ __forceinline__ bool dl_single_peak(const DebArgs &A, int P, const unsigned *pix, int *s_cnt) {
+    if (threadIdx.x == 0) *s_cnt = 0;
+    __syncthreads();
+    int n = 0;
+    for (int k = threadIdx.x; k < P; k += NT) {
+        const int p = (int)pix[k];
+        const int y = (int)fdiv((unsigned)p, A.wdiv), x = p - y * A.w;
+        const float c = A.cd[p];
+        bool top = true;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int ddx[8] = {-1, 0, 1, -1, 1, -1, 0, 1}, ddy[8] = {-1, -1, -1, 0, 0, 1, 1, 1};
+            const int nx = x + ddx[q], ny = y + ddy[q];
+            if (nx >= 0 && ny >= 0 && nx < A.w && ny < A.h) {
+                const size_t np = (size_t)ny * A.w + nx;
+                if (__ldg(A.pos2idx + np) >= 0 && __ldg(A.cd + np) > c) top = false;
+            }
+        }
+        n += top;
+    }
+    n = __reduce_add_sync(0xffffffffu, n);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(s_cnt, n);
+    __syncthreads();
+    return *s_cnt == 1;
+}
+
 // levels, level counts, level order (highest level first)
 template <int NT>
 __device__ __forceinline__ void dl_levels(const DebArgs &A, int P, const unsigned *pix, const float *thr,
@@ -160,15 +208,7 @@ __device__ __forceinline__ void dl_levels(const DebArgs &A, int P, const unsigne
     }
     __syncthreads();
     for (int k = threadIdx.x; k < P; k += NT) {
-        float c = A.cd[pix[k]];
-        int lo = 0, hi = A.N - 1;
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (c >= thr[mid])
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
+        const int lo = dl_level_of(A.cd[pix[k]], thr, A.N);
         lev[k] = (unsigned char)lo;
         atomicAdd(&lvcnt[lo], 1);
     }
@@ -201,7 +241,7 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
                                               int *glist, int *gcount, unsigned char *hyb) {
     __shared__ float thr[DB_MAXLEV];
     __shared__ int lvcnt[DB_MAXLEV + 1], lvstart[DB_MAXLEV + 1], lvcur[DB_MAXLEV];
-    __shared__ int s_nrl[2], s_nn[2], s_nkept;
+    __shared__ int s_nrl[2], s_nn[2], s_nkept, s_npeak;
     __shared__ unsigned s_peak;
     __shared__ XSum s_part[NT / 32];
     __shared__ float s_fdflux;
@@ -290,6 +330,18 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     const double value0 = (double)s_fdflux * A.mincont;
     block_thresholds(A, A.R.dthresh[r], fdpeak, thr);
     __syncthreads();
+    if (dl_single_peak<NT>(A, P, pix, &s_npeak)) {
+        // no split possible: the levels only count towards the summary
+        unsigned ls = 0;
+        for (int k = tid; k < P; k += NT) ls += (unsigned)dl_level_of(A.cd[pix[k]], thr, A.N);
+        ls = __reduce_add_sync(0xffffffffu, ls);
+        if ((tid & 31) == 0 && ls) atomicAdd(&A.sc->levpix, (unsigned long long)ls);
+        if (tid == 0) {
+            kept[0] = 0ull;
+            A.R.nkept[r] = 1;
+        }
+        return;
+    }
     dl_levels<NT>(A, P, pix, thr, lev, order, lvcnt, lvstart, lvcur, true);
     int cur = 0, lastL = -1;
     for (int L = A.N - 1; L >= 0; L--) {
