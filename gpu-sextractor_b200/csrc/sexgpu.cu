@@ -18,6 +18,7 @@
 #include <string>
 #include <thread>
 #include <mutex>
+#include <chrono>
 #include <vector>
 
 #include "sexgpu.h"
@@ -156,6 +157,7 @@ struct sexgpu_ctx {
     std::vector<int> stage_launches;
     std::vector<sexgpu_ctx *> workers;  // contexts of sexgpu_extract_batch
     std::vector<unsigned long long> batch_kinds;  // frame kinds a batch worker has extracted
+    int batch_workers = 8;  // workers of a batch called with workers = 0 (sexgpu_autotune_batch)
     // buffers outgrown during a batch: freed when the batch ends, because
     // cudaFree waits for the whole device and would stall the other workers
     bool defer_free = false;
@@ -1817,7 +1819,7 @@ int sexgpu_getconv(const char *path, float *mask, int maxn, int *mw, int *mh) {
 int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframes, int workers) {
     if (!ctx || nframes < 0 || (nframes > 0 && !frames) || workers < 0) return SEXGPU_ERR_ARG;
     if (nframes == 0) return SEXGPU_OK;
-    if (workers == 0) workers = 8;
+    if (workers == 0) workers = ctx->batch_workers;
     workers = std::min(workers, nframes);
     while ((int)ctx->workers.size() < workers) {
         sexgpu_ctx *w = nullptr;
@@ -2069,6 +2071,11 @@ int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value) {
         ctx->kron_warp_max = value;
         return SEXGPU_OK;
     }
+    if (!strcmp(name, "batch_workers")) {
+        if (value < 1 || value > 64) return SEXGPU_ERR_ARG;
+        ctx->batch_workers = value;
+        return SEXGPU_OK;
+    }
     if (!strcmp(name, "graph")) {
         if (value < 0 || value > 1) return SEXGPU_ERR_ARG;
         ctx->graph_mode = value;
@@ -2081,6 +2088,147 @@ int sexgpu_set_param(sexgpu_ctx *ctx, const char *name, int value) {
     }
     ctx->err = std::string("unknown parameter ") + name;
     return SEXGPU_ERR_ARG;
+}
+
+static void tune_entry(std::vector<sexgpu_tune_entry> &out, const char *name, int value, float ms) {
+    sexgpu_tune_entry e;
+    memset(&e, 0, sizeof(e));
+    strncpy(e.param, name, sizeof(e.param) - 1);
+    e.value = value;
+    e.ms = ms;
+    out.push_back(e);
+}
+
+static int tune_copy_out(const std::vector<sexgpu_tune_entry> &out, sexgpu_tune_entry *entries, int max_entries) {
+    if (entries)
+        for (int i = 0; i < (int)out.size() && i < max_entries; i++) entries[i] = out[i];
+    return (int)out.size();
+}
+
+int sexgpu_autotune(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, int h,
+                    const sexgpu_config *cfg, int reps, sexgpu_tune_entry *entries, int max_entries) {
+    if (!ctx || !d_img || !cfg || reps < 1 || max_entries < 0) return SEXGPU_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    std::vector<sexgpu_tune_entry> out;
+    std::vector<unsigned char> ref, got;
+    bool have_ref = false;
+    // one candidate: warm-up runs, then the best of reps timed runs; the rows
+    // of its last run against the first candidate's
+    auto trial = [&](const char *name, int value, float &best) -> int {
+        int rc = sexgpu_set_param(ctx, name, value);
+        for (int i = 0; !rc && i < 3; i++) rc = sexgpu_extract_device(ctx, d_img, d_wmap, w, h, cfg, nullptr);
+        best = 3.0e38f;
+        for (int i = 0; !rc && i < reps; i++) {
+            cudaEventRecord(e0, st);
+            rc = sexgpu_extract_device(ctx, d_img, d_wmap, w, h, cfg, nullptr);
+            cudaEventRecord(e1, st);
+            if (!rc && cudaEventSynchronize(e1) == cudaSuccess) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                best = std::min(best, ms);
+            }
+        }
+        if (rc) return rc;
+        got.resize((size_t)ctx->last_ns * sizeof(sexgpu_object));
+        if (!got.empty())
+            CK(cudaMemcpyAsync(got.data(), ctx->rows.p, got.size(), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (!have_ref) {
+            ref = got;
+            have_ref = true;
+        } else if (got != ref) {
+            ctx->err = std::string("rows differ under ") + name;
+            return SEXGPU_ERR_MISMATCH;
+        }
+        tune_entry(out, name, value, best);
+        return SEXGPU_OK;
+    };
+    int rc = SEXGPU_OK;
+    float best_ms = 3.0e38f, ms = 0.f;
+    int best_graph = ctx->graph_mode, best_kron = ctx->kron_warp_max;
+    for (int g = 0; g <= 1 && !rc; g++) {
+        rc = trial("graph", g, ms);
+        if (!rc && ms < best_ms) {
+            best_ms = ms;
+            best_graph = g;
+        }
+    }
+    if (!rc) rc = sexgpu_set_param(ctx, "graph", best_graph);
+    best_ms = 3.0e38f;
+    for (int v = 1024; v <= 32768 && !rc; v *= 2) {
+        rc = trial("kron_warp_max", v, ms);
+        if (!rc && ms < best_ms) {
+            best_ms = ms;
+            best_kron = v;
+        }
+    }
+    if (!rc) rc = sexgpu_set_param(ctx, "kron_warp_max", best_kron);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    return tune_copy_out(out, entries, max_entries);
+}
+
+int sexgpu_autotune_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframes, int reps,
+                          sexgpu_tune_entry *entries, int max_entries) {
+    if (!ctx || nframes <= 0 || !frames || reps < 1 || max_entries < 0) return SEXGPU_ERR_ARG;
+    std::vector<sexgpu_tune_entry> out;
+    std::vector<std::vector<unsigned char>> ref(nframes);
+    bool have_ref = false;
+    auto trial = [&](const char *name, int value, int workers, float &best) -> int {
+        int rc = SEXGPU_OK;
+        if (!strcmp(name, "batch_grid_div")) rc = sexgpu_set_param(ctx, name, value);
+        if (!rc) rc = sexgpu_extract_batch(ctx, frames, nframes, workers);  // warm-up
+        best = 3.0e38f;
+        for (int i = 0; !rc && i < reps; i++) {
+            auto t0 = std::chrono::steady_clock::now();
+            rc = sexgpu_extract_batch(ctx, frames, nframes, workers);
+            auto t1 = std::chrono::steady_clock::now();
+            best = std::min(best, (float)std::chrono::duration<double, std::milli>(t1 - t0).count());
+        }
+        if (rc) return rc;
+        for (int i = 0; i < nframes; i++) {
+            const sexgpu_batch_frame &f = frames[i];
+            const size_t n = f.objs ? (size_t)std::min(f.nobj, f.max_objects) * sizeof(sexgpu_object) : 0;
+            std::vector<unsigned char> cur(sizeof(int32_t) + n);
+            memcpy(cur.data(), &f.nobj, sizeof(int32_t));
+            if (n) memcpy(cur.data() + sizeof(int32_t), f.objs, n);
+            if (!have_ref)
+                ref[i].swap(cur);
+            else if (cur != ref[i]) {
+                ctx->err = std::string("catalogues differ under ") + name;
+                return SEXGPU_ERR_MISMATCH;
+            }
+        }
+        have_ref = true;
+        tune_entry(out, name, value, best);
+        return SEXGPU_OK;
+    };
+    int rc = SEXGPU_OK, best_w = ctx->batch_workers, best_div = ctx->batch_grid_div;
+    float best_ms = 3.0e38f, ms = 0.f;
+    for (int wk = 4; wk <= 16 && !rc; wk += 4) {
+        rc = trial("batch_workers", wk, wk, ms);
+        if (!rc && ms < best_ms) {
+            best_ms = ms;
+            best_w = wk;
+        }
+    }
+    if (!rc) ctx->batch_workers = best_w;
+    best_ms = 3.0e38f;
+    for (int d = 1; d <= 4 && !rc; d *= 2) {
+        rc = trial("batch_grid_div", d, best_w, ms);
+        if (!rc && ms < best_ms) {
+            best_ms = ms;
+            best_div = d;
+        }
+    }
+    if (!rc) rc = sexgpu_set_param(ctx, "batch_grid_div", best_div);
+    if (rc) return rc;
+    return tune_copy_out(out, entries, max_entries);
 }
 
 int sexgpu_graph_stats(sexgpu_ctx *ctx, int *replayed, int *kernels, int *kinds) {

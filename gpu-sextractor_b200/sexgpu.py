@@ -25,7 +25,7 @@ ERRORS = {-1: "bad argument", -2: "CUDA error", -3: "out of device memory",
           -4: "exact sum out of range", -5: "buffer too small", -6: "no CUDA device",
           -7: "zero or negative threshold", -8: "device loop cap reached",
           -9: "frame beyond the fixed scratch of the no-allocation entry point",
-          -10: "tile load timed out (destroy the context)"}
+          -10: "tile load timed out (destroy the context)", -11: "results differ between execution parameters"}
 
 
 class Config(C.Structure):
@@ -116,6 +116,10 @@ class FitsFormat(C.Structure):
                 ("bzero", C.c_double)]
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [("param", C.c_char * 24), ("value", C.c_int32), ("ms", C.c_float)]
+
+
 class Stage(C.Structure):
     _fields_ = [("name", C.c_char * 24), ("launches", C.c_int32), ("ms", C.c_float)]
 
@@ -125,7 +129,7 @@ EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extra
            "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times", "sexgpu_set_param",
            "sexgpu_read_nnw", "sexgpu_set_nnw", "sexgpu_extract_fits", "sexgpu_background_rms",
            "sexgpu_background_noalloc", "sexgpu_background_meshes", "sexgpu_background_map", "sexgpu_copy_apertures",
-           "sexgpu_extract_batch", "sexgpu_graph_stats"]
+           "sexgpu_extract_batch", "sexgpu_graph_stats", "sexgpu_autotune", "sexgpu_autotune_batch"]
 
 _lib = None
 
@@ -344,6 +348,33 @@ class Context:
     def extract_batch(self, frames, workers=0, max_objects=None):
         """frames: list of (img, settings dict[, weight map]).  All frames go to the library
         in one sexgpu_extract_batch call; returns [(catalogue, summary)]."""
+        arr, keep = self._batch_frames(frames, max_objects)
+        n = len(frames)
+        _check(lib().sexgpu_extract_batch(self.h, arr, n, workers), self.h, "sexgpu_extract_batch")
+        return [(keep[i][2][:arr[i].nobj], arr[i].summary) for i in range(n)]
+
+    def autotune(self, dev_ptr, w, h, wmap_ptr=None, reps=3, **kw):
+        """sexgpu_autotune on a device-resident frame: [(param, value, ms)];
+        the fastest values stay set on this context."""
+        cfg = make_config(**kw)
+        ent = (TuneEntry * 64)()
+        rc = lib().sexgpu_autotune(self.h, C.c_void_p(dev_ptr), C.c_void_p(wmap_ptr) if wmap_ptr else None, w, h,
+                                   C.byref(cfg), reps, ent, 64)
+        if rc < 0:
+            _check(rc, self.h, "sexgpu_autotune")
+        return [(ent[i].param.decode(), ent[i].value, ent[i].ms) for i in range(rc)]
+
+    def autotune_batch(self, frames, reps=2, max_objects=None):
+        """sexgpu_autotune_batch on these frames: [(param, value, ms)]; the
+        fastest worker count and grid divisor stay this context's defaults."""
+        arr, keep = self._batch_frames(frames, max_objects)
+        ent = (TuneEntry * 64)()
+        rc = lib().sexgpu_autotune_batch(self.h, arr, len(frames), reps, ent, 64)
+        if rc < 0:
+            _check(rc, self.h, "sexgpu_autotune_batch")
+        return [(ent[i].param.decode(), ent[i].value, ent[i].ms) for i in range(rc)]
+
+    def _batch_frames(self, frames, max_objects):
         n = len(frames)
         arr = (BatchFrame * max(n, 1))()
         keep = []
@@ -361,8 +392,7 @@ class Context:
             if wmap is not None:
                 f.wmap = _f(wmap)
             f.objs, f.max_objects = objs.ctypes.data_as(C.c_void_p), cap
-        _check(lib().sexgpu_extract_batch(self.h, arr, n, workers), self.h, "sexgpu_extract_batch")
-        return [(keep[i][2][:arr[i].nobj], arr[i].summary) for i in range(n)]
+        return arr, keep
 
     def set_nnw(self, net):
         """CLASS_STAR network of later extractions (NNW), or None to switch it off."""

@@ -42,6 +42,7 @@ extern "C" {
 #define SEXGPU_ERR_LOOP       -8   /* a bounded device loop hit its iteration cap */
 #define SEXGPU_ERR_NOALLOC_LIMIT -9 /* frame beyond the fixed scratch of sexgpu_background_noalloc */
 #define SEXGPU_ERR_LOAD      -10   /* a tile load did not complete in time: destroy the context */
+#define SEXGPU_ERR_MISMATCH  -11   /* results differed between execution parameters (a defect) */
 
 #define SEXGPU_NISO 8
 #define SEXGPU_MAXAPER 16   /* PHOT_APERTURES diameters per extraction */
@@ -279,13 +280,44 @@ typedef struct {
 /* Extraction of many frames of any sizes and settings (the batched form of
  * scanimage(); no counterpart in the reference, which handles one frame per
  * process).  The frames are taken largest first by `workers` device streams
- * of this context's device (0: 8), each with its own buffers, so that the
+ * of this context's device (0: 8, or what sexgpu_autotune_batch chose), each
+ * with its own buffers, so that the
  * stages of different frames overlap on the GPU.  Every frame's results are
  * exactly those of sexgpu_extract on that frame.  Returns SEXGPU_OK if every
  * frame succeeded, else the status of the first failed frame (each frame's
  * own status is in frames[i].status).  Not for use on the same context from
  * two threads at once. */
 int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframes, int workers);
+
+/* One timed candidate of the autotuners. */
+typedef struct {
+    char    param[24];          /* execution parameter (see sexgpu_set_param) */
+    int32_t value;
+    float   ms;                 /* best time of the timed runs: per frame, or per batch */
+} sexgpu_tune_entry;
+
+/* Autotuner of the execution parameters, which never change results.  Times
+ * the extraction of one device-resident frame (arguments as for
+ * sexgpu_extract_device) on this context with "graph" 0 and 1, then, with the
+ * faster, "kron_warp_max" 1024, 2048, ..., 32768: each candidate after its
+ * warm-up runs (a graph learns and captures), best of reps runs timed with
+ * CUDA events on the context's stream.  The fastest value of each parameter
+ * stays set on the context.  Every candidate's catalogue rows are compared
+ * with the first candidate's, byte for byte: SEXGPU_ERR_MISMATCH if they
+ * differ.  Up to max_entries candidates go to entries (may be NULL); returns
+ * the number of candidates timed, or an error code. */
+int sexgpu_autotune(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, int h,
+                    const sexgpu_config *cfg, int reps, sexgpu_tune_entry *entries, int max_entries);
+
+/* Autotuner of the batched form: times sexgpu_extract_batch on these frames
+ * (host wall clock, best of reps, after one warm-up batch per candidate) with
+ * 4, 8, 12 and 16 workers, then "batch_grid_div" 1, 2 and 4, and keeps the
+ * fastest as this context's defaults (the worker count of a batch called
+ * with workers = 0).  The frames' catalogues are compared with the first
+ * candidate's (SEXGPU_ERR_MISMATCH if they differ); they hold the last run's
+ * results on return.  Returns the number of candidates timed, or an error. */
+int sexgpu_autotune_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframes, int reps,
+                          sexgpu_tune_entry *entries, int max_entries);
 
 /* Aperture photometry of every aperture of the last extraction (FLUX_APER,
  * FLUXERR_APER, MAG_APER, MAGERR_APER as vectors), in catalogue order: out
@@ -319,7 +351,9 @@ int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max);
  * every union-find walk, union retry and CLEAN chain walk of the following
  * extractions at n steps (a walk that runs out returns SEXGPU_ERR_LOOP and the
  * context stays usable); 0 (default) keeps the built-in caps, which no valid
- * frame reaches -- it exists to test the error path.  "graph": 1 extracts
+ * frame reaches -- it exists to test the error path.  "batch_workers": the
+ * worker count of a batch called with workers = 0 (1..64, default 8).
+ * "graph": 1 extracts
  * through captured CUDA graphs (default 0).  The first frame of a kind (frame
  * size, configuration, detection mask, input buffers and the parameters
  * above) runs as without the parameter and sets capacities a quarter above its
