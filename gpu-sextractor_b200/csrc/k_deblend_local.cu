@@ -875,6 +875,18 @@ void launch_deblend_split(const int *size, int nroots, const int *nroots_dev, in
 
 int deblend_split_launches(int nroots) { return nroots > 0 ? 3 + radix_launches(16, nroots) : 0; }
 
+static void dl_fork(const DebStreams &S) {
+    cudaEventRecord(S.fork, S.main);
+    for (int i = 0; i < DL_SIDE; i++) cudaStreamWaitEvent(S.side[i], S.fork, 0);
+}
+
+static void dl_join(const DebStreams &S) {
+    for (int i = 0; i < DL_SIDE; i++) {
+        cudaEventRecord(S.join[i], S.side[i]);
+        cudaStreamWaitEvent(S.main, S.join[i], 0);
+    }
+}
+
 #define DL_SCUR(k) (counts + DL_NLISTS + (k))
 #define DL_ACUR(k) (counts + 2 * DL_NLISTS + (k))
 
@@ -898,9 +910,7 @@ void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int n
     const size_t m0 = DL_CAP0 * DL_SWEEP_BYTES, m1 = DL_CAP1 * DL_SWEEP_BYTES;
     const size_t h3 = (size_t)DL_HYB3 * DL_HYB_BYTES, h45 = (size_t)DL_HYB45 * DL_HYB_BYTES,
                  h12 = (size_t)DL_HYB12 * DL_HYB_BYTES;
-    cudaEventRecord(S.fork, S.main);
-    cudaStreamWaitEvent(S.side[0], S.fork, 0);
-    cudaStreamWaitEvent(S.side[1], S.fork, 0);
+    dl_fork(S);
     const int grid3 = min(nroots, dl_grid(k_deblend_sweep, DB_THREADS, 0, g3));
     k_deblend_sweep<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 6 * n, counts + 6, DL_SCUR(6));
     k_dl_sweep<256><<<min(nroots, dl_grid(k_dl_sweep<256>, 256, h45, g2)), 256, h45, S.side[0]>>>(
@@ -913,10 +923,7 @@ void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int n
         A, dl_lists(lists, counts, n, 0), DL_SCUR(0), DL_CAP0, glist, counts + 7, 0);
     k_dl_sweep<32><<<min(nroots, dl_grid(k_dl_sweep<32>, 32, m1, g4)), 32, m1, S.main>>>(
         A, dl_lists(lists, counts, n, 8), DL_SCUR(8), DL_CAP1, glist, counts + 7, 0);
-    cudaEventRecord(S.join[0], S.side[0]);
-    cudaEventRecord(S.join[1], S.side[1]);
-    cudaStreamWaitEvent(S.main, S.join[0], 0);
-    cudaStreamWaitEvent(S.main, S.join[1], 0);
+    dl_join(S);
     k_deblend_sweep<<<grid3, DB_THREADS, 0, S.main>>>(A, glist, counts + 7, DL_SCUR(7));
 }
 
@@ -932,9 +939,7 @@ void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int 
     const size_t n = (size_t)nroots;
     const size_t m0 = DL_CAP0 * DL_ASSIGN_BYTES, m1 = DL_CAP1 * DL_ASSIGN_BYTES;
     const size_t tb = (size_t)DL_GTAB_BIG * DL_GTAB_BYTES, tm = (size_t)DL_GTAB_MID * DL_GTAB_BYTES;
-    cudaEventRecord(S.fork, S.main);
-    cudaStreamWaitEvent(S.side[0], S.fork, 0);
-    cudaStreamWaitEvent(S.side[1], S.fork, 0);
+    dl_fork(S);
     const int grid3 = min(nroots, dl_grid(k_deblend_assign, DB_THREADS, 0, g3));
     k_deblend_assign<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 6 * n, counts + 6, DL_ACUR(6));
     k_deblend_assign<<<grid3, DB_THREADS, 0, S.side[0]>>>(A, lists + 7 * n, counts + 7, DL_ACUR(7));
@@ -948,10 +953,7 @@ void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int 
         A, dl_lists(lists, counts, n, 0), DL_ACUR(0), DL_CAP0, 0);
     k_dl_assign<32><<<min(nroots, dl_grid(k_dl_assign<32>, 32, m1, g4)), 32, m1, S.main>>>(
         A, dl_lists(lists, counts, n, 8), DL_ACUR(8), DL_CAP1, 0);
-    cudaEventRecord(S.join[0], S.side[0]);
-    cudaEventRecord(S.join[1], S.side[1]);
-    cudaStreamWaitEvent(S.main, S.join[0], 0);
-    cudaStreamWaitEvent(S.main, S.join[1], 0);
+    dl_join(S);
 }
 
 }  // namespace sx

@@ -152,10 +152,11 @@ struct DebArgs {
     int loop_cap;               // > 0: cap on union-find walks (failure tests); 0: the object's size
 };
 
-// the main stream, two side streams and the events that fork and join them
+// the main stream, the side streams and the events that fork and join them
+constexpr int DL_SIDE = 3;
 struct DebStreams {
-    cudaStream_t main, side[2];
-    cudaEvent_t fork, join[2];
+    cudaStream_t main, side[DL_SIDE];
+    cudaEvent_t fork, join[DL_SIDE];
 };
 
 void launch_deblend_split(const int *size, int nroots, const int *nroots_dev, int *lists, int *counts,

@@ -106,8 +106,8 @@ struct sexgpu_ctx {
     cudaEvent_t ev_block = nullptr;
     PipeState ps;
     cudaStream_t stream = nullptr;
-    cudaStream_t side[2] = {nullptr, nullptr};  // fork/join helpers of the deblending
-    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    cudaStream_t side[DL_SIDE] = {};  // fork/join helpers of the deblending
+    cudaEvent_t ev_fork = nullptr, ev_join[DL_SIDE] = {};
     bool own_stream = false;
     std::vector<DevBuf *> bufs;
     std::string err;
@@ -838,11 +838,11 @@ int pipe_deblend(sexgpu_ctx *ctx) {
     EN(rcounts, 5 * DL_NLISTS * 4);
     DebStreams S;
     S.main = st;
-    S.side[0] = ctx->side[0];
-    S.side[1] = ctx->side[1];
+    for (int i = 0; i < DL_SIDE; i++) {
+        S.side[i] = ctx->side[i];
+        S.join[i] = ctx->ev_join[i];
+    }
     S.fork = ctx->ev_fork;
-    S.join[0] = ctx->ev_join[0];
-    S.join[1] = ctx->ev_join[1];
     const int *nroots_dev = ps.capf ? &d_sc->nroots : nullptr;
     launch_deblend_split(R.size, nroots, nroots_dev, P<int>(ctx->rlists), P<int>(ctx->rcounts), P<unsigned>(ctx->keys),
                          P<unsigned>(ctx->vals), P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), tmp, st);
@@ -1377,11 +1377,11 @@ int sexgpu_create(sexgpu_ctx **out, int device) {
         return SEXGPU_ERR_CUDA;
     }
     ctx->own_stream = true;
-    if (cudaStreamCreateWithFlags(&ctx->side[0], cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->side[1], cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->ev_join[0], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->ev_join[1], cudaEventDisableTiming) != cudaSuccess) {
+    bool ok = true;
+    for (int i = 0; i < DL_SIDE; i++)
+        ok = ok && cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok || cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess) {
         sexgpu_destroy(ctx);
         return SEXGPU_ERR_CUDA;
     }
@@ -1438,7 +1438,7 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     free_buf(ctx->dmask);
     for (auto &s : ctx->stages) cudaEventDestroy(s.ev);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < DL_SIDE; i++) {
         if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
         if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
     }
