@@ -216,6 +216,89 @@ __device__ __forceinline__ XSum xs_warp_sum(XSum s) {
 __device__ __forceinline__ XSum xs_warp_reduce(XSum s) { return xs_warp_sum(s); }
 
 // ---------------------------------------------------------------------------
+// Exact sums of float terms, binned form: three double bins of 16 binary
+// orders each, the top one ending at the order `top` (a hint, for instance
+// the order of the largest term expected).  A term of order e = exponent
+// field - 127 goes to bin k = (top - e) >> 4 when 0 <= k <= 2: it is a
+// multiple of 2^(top-16k-38) below 2^(top-16k+1), so up to 2^14 such terms
+// (of one bin, over every lane that adds them up) sum below 2^53 units of
+// 2^(top-16k-38), and every double addition in the bin is exact.  A nonzero
+// term outside the bins is not added and makes bs_add return false; the
+// caller then takes the sum again with XSum.  Zero and subnormal terms add
+// nothing, as in xs_add, so a valid binned sum moved into an XSum has exactly
+// the value the XSum of the same terms has.  The hint only decides which
+// terms fit: a wrong one costs a second pass, never a different result.
+// ---------------------------------------------------------------------------
+constexpr int BS_MAX_TERMS = 1 << 14;  // terms per sum (all lanes together)
+
+struct BinSum {
+    double b0, b1, b2;
+};
+
+__device__ __forceinline__ void bs_init(BinSum &s) { s.b0 = s.b1 = s.b2 = 0.0; }
+
+__device__ __forceinline__ bool bs_add(BinSum &s, float f, int top) {
+    const unsigned u = __float_as_uint(f);
+    const int ef = (int)((u >> 23) & 0xff);
+    if (ef == 0) return true;
+    const int k = (top + 127 - ef) >> 4;
+    const double d = (double)f;
+    s.b0 += k == 0 ? d : 0.0;
+    s.b1 += k == 1 ? d : 0.0;
+    s.b2 += k == 2 ? d : 0.0;
+    return (unsigned)k < 3u;
+}
+
+// order of a float for the hint: exponent field - 127 (-127 for 0)
+__device__ __forceinline__ int bs_order(float f) { return (int)((__float_as_uint(f) >> 23) & 0xff) - 127; }
+
+// full-warp sum of the bins (exact: each bin's terms over the warp number
+// at most BS_MAX_TERMS); valid in every lane
+__device__ __forceinline__ BinSum bs_warp_sum(BinSum s) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s.b0 += __shfl_xor_sync(0xffffffffu, s.b0, o);
+        s.b1 += __shfl_xor_sync(0xffffffffu, s.b1, o);
+        s.b2 += __shfl_xor_sync(0xffffffffu, s.b2, o);
+    }
+    return s;
+}
+
+// s += d exactly, for a double d that is a multiple of a power of two no
+// smaller than 2^-1074 (every bin sum is)
+__device__ __forceinline__ void xs_add_double(XSum &s, double d) {
+    if (d == 0.0) return;
+    const unsigned long long u = (unsigned long long)__double_as_longlong(d);
+    const int ed = (int)((u >> 52) & 0x7ff);
+    unsigned long long m = u & 0xfffffffffffffull;
+    if (ed) m |= 1ull << 52;
+    const int tz = __ffsll((long long)m) - 1;
+    m >>= tz;
+    // d = m * 2^(te - 23) in the units of xs_add
+    const int te = (ed ? ed : 1) - 1075 + tz + 23;
+    if (te < s.e) xs_rescale(s, te);
+    const int sh = te - s.e;
+    if (sh + (64 - __clzll(m)) > 125) {
+        s.ovf = 1;
+        return;
+    }
+    const __int128 t = (__int128)((unsigned __int128)m << sh);
+    if (u >> 63)
+        s.v -= t;
+    else
+        s.v += t;
+}
+
+__device__ __forceinline__ XSum bs_to_xsum(const BinSum &b) {
+    XSum x;
+    xs_init(x);
+    xs_add_double(x, b.b2);
+    xs_add_double(x, b.b1);
+    xs_add_double(x, b.b0);
+    return x;
+}
+
+// ---------------------------------------------------------------------------
 // Fixed-scale exact accumulators usable with atomics: value =
 // sum_k (int64)w[k] * 2^(32k) in units of 2^(e0-23).  A float term of
 // exponent e >= e0 is split into 32-bit limbs; each limb word stays exact for

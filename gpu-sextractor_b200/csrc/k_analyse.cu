@@ -143,8 +143,13 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(AnaAr
     const float dthresh = A.O.dthr[o];
     int flags = A.O.flags[o];
 
-    XSum srv;
-    xs_init(srv);
+    // exact sums in double bins (hint: the object's filtered peak), or with
+    // XSum when a term falls outside them or the object is too large
+    const bool binned = n <= BS_MAX_TERMS;
+    BinSum brv;
+    bs_init(brv);
+    bool ok = binned;
+    const int top_c = bs_order(A.O.fdpeak[o]);
     unsigned pk = 0u, cpk = 0u;
     int xmin = 0x7fffffff, xmax = -1, ymin = 0x7fffffff, ymax = -1;
     for (int i = lane; i < n; i += 32) {
@@ -153,13 +158,20 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(AnaAr
         pk = max(pk, f2ord(__ldg(A.sub + p)));
         float c = __ldg(A.cd + p);
         cpk = max(cpk, f2ord(c));
-        xs_add(srv, c);
+        if (binned) ok &= bs_add(brv, c, top_c);
         xmin = min(xmin, x);
         xmax = max(xmax, x);
         ymin = min(ymin, y);
         ymax = max(ymax, y);
     }
-    srv = xs_warp_sum(srv);
+    XSum srv;
+    if (__all_sync(0xffffffffu, ok)) {
+        srv = bs_to_xsum(bs_warp_sum(brv));
+    } else {
+        xs_init(srv);
+        for (int i = lane; i < n; i += 32) xs_add(srv, __ldg(A.cd + __ldg(pix + i)));
+        srv = xs_warp_sum(srv);
+    }
     float peak = ord2f(warp_max_u(pk)), cpeak = ord2f(warp_max_u(cpk));
     xmin = warp_min_i(xmin);
     xmax = warp_max_i(xmax);
@@ -168,35 +180,68 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(AnaAr
     if (xmin == 0 || xmax == w - 1 || ymin == 0 || ymax == h - 1) flags |= SX_OBJ_TRUNC;
     float rv = xs_float(srv);
     double dth = dthresh, dthresh2 = (dth + peak) / 2.0;
-    XSum stv, smx, smy, smx2, smy2, smxy;
-    xs_init(stv);
-    xs_init(smx);
-    xs_init(smy);
-    xs_init(smx2);
-    xs_init(smy2);
-    xs_init(smxy);
+    // second pass: the moments' terms are below cpeak times the box sides
+    const int bx = 32 - __clz(xmax - xmin), by = 32 - __clz(ymax - ymin), tc = bs_order(cpeak) + 1;
+    BinSum bmx, bmy, bmx2, bmy2, bmxy, btv;
+    bs_init(bmx);
+    bs_init(bmy);
+    bs_init(bmx2);
+    bs_init(bmy2);
+    bs_init(bmxy);
+    bs_init(btv);
+    ok = binned;
+    const int tv_top = bs_order(peak);
     int dnpix = 0, area2 = 0;
     for (int i = lane; i < n; i += 32) {
         unsigned p = __ldg(pix + i);
         int yy = (int)fdiv(p, A.wdiv), x = (int)p - yy * w - xmin, y = yy - ymin;
         float cval = __ldg(A.cd + p), val = __ldg(A.sub + p);
-        xs_add(stv, val);
         dnpix += val > dth;
         area2 += val > dthresh2;
-        xs_add(smx, cval * x);
-        xs_add(smy, cval * y);
-        xs_add(smx2, cval * x * x);
-        xs_add(smy2, cval * y * y);
-        xs_add(smxy, cval * x * y);
+        if (binned) {
+            ok &= bs_add(btv, val, tv_top);
+            ok &= bs_add(bmx, cval * x, tc + bx);
+            ok &= bs_add(bmy, cval * y, tc + by);
+            ok &= bs_add(bmx2, cval * x * x, tc + 2 * bx);
+            ok &= bs_add(bmy2, cval * y * y, tc + 2 * by);
+            ok &= bs_add(bmxy, cval * x * y, tc + bx + by);
+        }
     }
-    stv = xs_warp_sum(stv);
-    smx = xs_warp_sum(smx);
-    smy = xs_warp_sum(smy);
-    smx2 = xs_warp_sum(smx2);
-    smy2 = xs_warp_sum(smy2);
-    smxy = xs_warp_sum(smxy);
     dnpix = warp_sum_i(dnpix);
     area2 = warp_sum_i(area2);
+    XSum stv, smx, smy, smx2, smy2, smxy;
+    if (__all_sync(0xffffffffu, ok)) {
+        stv = bs_to_xsum(bs_warp_sum(btv));
+        smx = bs_to_xsum(bs_warp_sum(bmx));
+        smy = bs_to_xsum(bs_warp_sum(bmy));
+        smx2 = bs_to_xsum(bs_warp_sum(bmx2));
+        smy2 = bs_to_xsum(bs_warp_sum(bmy2));
+        smxy = bs_to_xsum(bs_warp_sum(bmxy));
+    } else {
+        xs_init(stv);
+        xs_init(smx);
+        xs_init(smy);
+        xs_init(smx2);
+        xs_init(smy2);
+        xs_init(smxy);
+        for (int i = lane; i < n; i += 32) {
+            unsigned p = __ldg(pix + i);
+            int yy = (int)fdiv(p, A.wdiv), x = (int)p - yy * w - xmin, y = yy - ymin;
+            float cval = __ldg(A.cd + p), val = __ldg(A.sub + p);
+            xs_add(stv, val);
+            xs_add(smx, cval * x);
+            xs_add(smy, cval * y);
+            xs_add(smx2, cval * x * x);
+            xs_add(smy2, cval * y * y);
+            xs_add(smxy, cval * x * y);
+        }
+        stv = xs_warp_sum(stv);
+        smx = xs_warp_sum(smx);
+        smy = xs_warp_sum(smy);
+        smx2 = xs_warp_sum(smx2);
+        smy2 = xs_warp_sum(smy2);
+        smxy = xs_warp_sum(smxy);
+    }
     if (lane != 0) return;
     if (srv.ovf | stv.ovf | smx.ovf | smy.ovf | smx2.ovf | smy2.ovf | smxy.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
     RobustRaw R;
@@ -309,6 +354,12 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
     XSum stv, svar;
     xs_init(stv);
     xs_init(svar);
+    // the flux in double bins (hint: the object's peak), else with XSum
+    const bool binned = n <= BS_MAX_TERMS;
+    bool ok = binned;
+    BinSum btv;
+    bs_init(btv);
+    const int tv_top = bs_order(A.O.dpeak[o]);
     double esum = 0, emx2 = 0, emy2 = 0, emxy = 0;
     for (int i = lane; i < n; i += 32) {
         unsigned p = __ldg(pix + i);
@@ -321,7 +372,8 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
         // with a weight map: the pixel's own analysis threshold and variance
         const float pvar = A.wvar ? __ldg(A.wvar + p) : 0.0f;
         area += pv > sx_pix_thr(A.wthr, A.afac, pvar, gthresh);
-        xs_add(stv, pv);
+        if (binned)
+            ok &= bs_add(btv, pv, tv_top);
         if (A.wvar) xs_add(svar, pvar);
         double err = A.wvar ? (double)pvar : dbacknoise2;
         if (A.gain > 0.0 && cdpix > 0.0) err += cdpix / A.gain;
@@ -334,7 +386,12 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A
     float peak = ord2f(warp_max_u(pk));
     best = warp_max_ull(best);
     area = warp_sum_i(area);
-    stv = xs_warp_sum(stv);
+    if (__all_sync(0xffffffffu, ok)) {
+        stv = bs_to_xsum(bs_warp_sum(btv));
+    } else {
+        for (int i = lane; i < n; i += 32) xs_add(stv, __ldg(A.sub + __ldg(pix + i)));
+        stv = xs_warp_sum(stv);
+    }
     if (A.wvar) svar = xs_warp_sum(svar);
     esum = warp_sum_d(esum);
     emx2 = warp_sum_d(emx2);

@@ -540,8 +540,13 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
         const int o = ob + k, L = (int)(kept2[k] >> 32), nb = bcnt[k], bb = bstart[k];
         int xmin = 0x7fffffff, xmax = -1, ymin = 0x7fffffff, ymax = -1;
         unsigned pk = 0u, cpk = 0u;
-        XSum srv;
-        xs_init(srv);
+        // exact sums in double bins (hint: the raw object's filtered peak),
+        // or with XSum when a term falls outside them or the branch is large
+        const bool binned = nb <= BS_MAX_TERMS;
+        bool ok = binned;
+        BinSum brv;
+        bs_init(brv);
+        const int top_c = bs_order(fdpeak);
         for (int i = lane; i < nb; i += 32) {
             const unsigned p = pix[whole ? i : blist[bb + i]];
             const int y = (int)fdiv(p, A.wdiv), x = (int)p - y * A.w;
@@ -552,7 +557,7 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
             pk = max(pk, f2ord(A.sub[p]));
             const float c = A.cd[p];
             cpk = max(cpk, f2ord(c));
-            xs_add(srv, c);
+            if (binned) ok &= bs_add(brv, c, top_c);
         }
         for (int d = 16; d > 0; d >>= 1) {
             xmin = min(xmin, __shfl_xor_sync(0xffffffffu, xmin, d));
@@ -562,16 +567,28 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
             pk = max(pk, __shfl_xor_sync(0xffffffffu, pk, d));
             cpk = max(cpk, __shfl_xor_sync(0xffffffffu, cpk, d));
         }
-        srv = xs_warp_sum(srv);
+        XSum srv;
+        if (__all_sync(0xffffffffu, ok)) {
+            srv = bs_to_xsum(bs_warp_sum(brv));
+        } else {
+            xs_init(srv);
+            for (int i = lane; i < nb; i += 32) xs_add(srv, A.cd[pix[whole ? i : blist[bb + i]]]);
+            srv = xs_warp_sum(srv);
+        }
         const float peak = ord2f(pk);
         const double dthresh = thr[L], dthresh2 = (dthresh + peak) / 2.0;
-        XSum smx, smy, smx2, smy2, smxy, stv;
-        xs_init(smx);
-        xs_init(smy);
-        xs_init(smx2);
-        xs_init(smy2);
-        xs_init(smxy);
-        xs_init(stv);
+        // second pass: the moments' terms are below the filtered peak times
+        // the box sides
+        const int bx = 32 - __clz(xmax - xmin), by = 32 - __clz(ymax - ymin), tc = bs_order(ord2f(cpk)) + 1;
+        const int tv_top = bs_order(peak);
+        BinSum bmx, bmy, bmx2, bmy2, bmxy, btv;
+        bs_init(bmx);
+        bs_init(bmy);
+        bs_init(bmx2);
+        bs_init(bmy2);
+        bs_init(bmxy);
+        bs_init(btv);
+        ok = binned;
         int dnpix = 0, area2 = 0;
         for (int i = lane; i < nb; i += 32) {
             const unsigned p = pix[whole ? i : blist[bb + i]];
@@ -579,23 +596,52 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
             const float cval = A.cd[p], val = A.sub[p];
             dnpix += val > dthresh;
             area2 += val > dthresh2;
-            xs_add(smx, cval * x);
-            xs_add(smy, cval * y);
-            xs_add(smx2, cval * x * x);
-            xs_add(smy2, cval * y * y);
-            xs_add(smxy, cval * x * y);
-            xs_add(stv, val);
+            if (binned) {
+                ok &= bs_add(bmx, cval * x, tc + bx);
+                ok &= bs_add(bmy, cval * y, tc + by);
+                ok &= bs_add(bmx2, cval * x * x, tc + 2 * bx);
+                ok &= bs_add(bmy2, cval * y * y, tc + 2 * by);
+                ok &= bs_add(bmxy, cval * x * y, tc + bx + by);
+                ok &= bs_add(btv, val, tv_top);
+            }
         }
         for (int d = 16; d > 0; d >>= 1) {
             dnpix += __shfl_xor_sync(0xffffffffu, dnpix, d);
             area2 += __shfl_xor_sync(0xffffffffu, area2, d);
         }
-        smx = xs_warp_sum(smx);
-        smy = xs_warp_sum(smy);
-        smx2 = xs_warp_sum(smx2);
-        smy2 = xs_warp_sum(smy2);
-        smxy = xs_warp_sum(smxy);
-        stv = xs_warp_sum(stv);
+        XSum smx, smy, smx2, smy2, smxy, stv;
+        if (__all_sync(0xffffffffu, ok)) {
+            smx = bs_to_xsum(bs_warp_sum(bmx));
+            smy = bs_to_xsum(bs_warp_sum(bmy));
+            smx2 = bs_to_xsum(bs_warp_sum(bmx2));
+            smy2 = bs_to_xsum(bs_warp_sum(bmy2));
+            smxy = bs_to_xsum(bs_warp_sum(bmxy));
+            stv = bs_to_xsum(bs_warp_sum(btv));
+        } else {
+            xs_init(smx);
+            xs_init(smy);
+            xs_init(smx2);
+            xs_init(smy2);
+            xs_init(smxy);
+            xs_init(stv);
+            for (int i = lane; i < nb; i += 32) {
+                const unsigned p = pix[whole ? i : blist[bb + i]];
+                const int yy = (int)fdiv(p, A.wdiv), x = (int)p - yy * A.w - xmin, y = yy - ymin;
+                const float cval = A.cd[p], val = A.sub[p];
+                xs_add(smx, cval * x);
+                xs_add(smy, cval * y);
+                xs_add(smx2, cval * x * x);
+                xs_add(smy2, cval * y * y);
+                xs_add(smxy, cval * x * y);
+                xs_add(stv, val);
+            }
+            smx = xs_warp_sum(smx);
+            smy = xs_warp_sum(smy);
+            smx2 = xs_warp_sum(smx2);
+            smy2 = xs_warp_sum(smy2);
+            smxy = xs_warp_sum(smxy);
+            stv = xs_warp_sum(stv);
+        }
         if (lane != 0) continue;
         if (srv.ovf | smx.ovf | smy.ovf | smx2.ovf | smy2.ovf | smxy.ovf | stv.ovf) atomicOr(status, SX_ST_RANGE);
         int flag = 0;

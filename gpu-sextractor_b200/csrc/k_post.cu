@@ -531,6 +531,77 @@ __device__ __forceinline__ void kron_range(const EndArgs &A, int o, double mx, d
     }
 }
 
+// kron_range with the exact sums in double bins (see BinSum): the hints are
+// the object's peak (and, for pass 1's r*pix, the ellipse's largest r).
+// Returns false in every lane when any lane met a term outside the bins; the
+// caller then sums with kron_range.  Pass 2 with a variance map is not binned.
+template <int PASS>
+__device__ __forceinline__ bool kron_range_bin(const EndArgs &A, int o, double mx, double my, const KronGeo &g,
+                                               int i0, int i1, int step, KronAcc &out) {
+    const int w = A.w, h = A.h, bw = g.xmax - g.xmin;
+    const FastDiv bd = make_fastdiv_dev((unsigned)bw);
+    const int corrflag = (A.mask_type == 2);
+    const int top1 = bs_order(A.O.peak[o]), top0 = top1 + bs_order(sqrtf(g.klim2)) + 1;
+    BinSum b0, b1;
+    bs_init(b0);
+    bs_init(b1);
+    int area = 0, areab = 0;
+    bool ok = true;
+    for (int i = i0; i < i1; i += step) {
+        const int yo = (int)fdiv((unsigned)i, bd), x = g.xmin + (i - yo * bw), y = g.ymin + yo;
+        const float dx = x - mx, dy = y - my;
+        if (PASS == 1) {
+            float r2;
+            if ((r2 = g.cx2 * dx * dx + g.cy2 * dy * dy + g.cxy * dx * dy) <= g.klim2) {
+                const float pix = A.sub[(size_t)y * w + x];
+                const int t = A.alloc[(size_t)y * w + x];
+                if ((t == o || t == -1) & (pix > -SX_BIG)) {
+                    area++;
+                    ok &= bs_add(b0, sqrtf(r2) * pix, top0);
+                    ok &= bs_add(b1, pix, top1);
+                } else
+                    areab++;
+            }
+        } else if ((g.cx2 * dx * dx + g.cy2 * dy * dy + g.cxy * dx * dy) <= g.klim2) {
+            area++;
+            float pix = A.sub[(size_t)y * w + x];
+            int t = A.alloc[(size_t)y * w + x];
+            if ((t >= 0 && t != o) || pix <= -SX_BIG) {
+                areab++;
+                int x2, y2;
+                if (corrflag && (x2 = (int)(2 * mx + 0.49999 - x)) >= 0 && x2 < w &&
+                    (y2 = (int)(2 * my + 0.49999 - y)) >= 0 && y2 < h &&
+                    ((t = A.alloc[(size_t)y2 * w + x2]) == -1 || t == o) && A.sub[(size_t)y2 * w + x2] > -SX_BIG)
+                    pix = A.sub[(size_t)y2 * w + x2];
+                else
+                    pix = 0.0;
+            }
+            ok &= bs_add(b0, pix, top1);
+        }
+    }
+    if (!__all_sync(0xffffffffu, ok)) return false;
+    out.s0 = bs_to_xsum(bs_warp_sum(b0));
+    if (PASS == 1)
+        out.s1 = bs_to_xsum(bs_warp_sum(b1));
+    else
+        xs_init(out.s1);
+    out.area = wsum(area);
+    out.areab = wsum(areab);
+    return true;
+}
+
+// a warp's sums over box pixels i0, i0 + step, ... < i1 (every lane holds them)
+template <int PASS>
+__device__ __forceinline__ void kron_warp_sums(const EndArgs &A, int o, double mx, double my, const KronGeo &g,
+                                               int i0, int i1, int step, KronAcc &c) {
+    // at most BS_MAX_TERMS terms of the warp per bin
+    const bool binned = (PASS == 1 || !A.wvar) && (long long)(i1 - (i0 & ~31)) <= (long long)BS_MAX_TERMS * step / 32;
+    if (binned && kron_range_bin<PASS>(A, o, mx, my, g, i0, i1, step, c)) return;
+    kacc_init(c);
+    kron_range<PASS>(A, o, mx, my, g, i0, i1, step, c);
+    kacc_warp(c);
+}
+
 // Queue object o's pass-`pass` box (warp-collective).  False when the queue is
 // full; the warp then sums the box itself.
 __device__ bool kron_defer(const EndArgs &A, int pass, int o, int flags, float kron, const KronGeo &g, int nn) {
@@ -642,8 +713,7 @@ __device__ void kron_after1(const EndArgs &A, int o, double mx, double my, int f
     }
     const int nn = kron_npix(g);
     if (nn > defer_at && kron_defer(A, 1, o, flags, kron, g, nn)) return;
-    kron_range<2>(A, o, mx, my, g, threadIdx.x & 31, nn, 32, p2);
-    kacc_warp(p2);
+    kron_warp_sums<2>(A, o, mx, my, g, threadIdx.x & 31, nn, 32, p2);
     end_finish(A, o, flags, kron, true, p2);
 }
 
@@ -661,9 +731,7 @@ __global__ void __launch_bounds__(128, 8) k_endobject(EndArgs A) {
     const int nn = kron_npix(g);
     if (nn > A.K.warp_max && kron_defer(A, 0, o, flags, 0.0f, g, nn)) return;
     KronAcc p1;
-    kacc_init(p1);
-    kron_range<1>(A, o, mx, my, g, lane, nn, 32, p1);
-    kacc_warp(p1);
+    kron_warp_sums<1>(A, o, mx, my, g, lane, nn, 32, p1);
     kron_after1(A, o, mx, my, flags, p1, A.K.warp_max);
 }
 
@@ -679,9 +747,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_kron_chunks(EndArgs A) {
         const KronItem it = A.K.item[PASS - 1][k];
         const int i0 = (c - it.c0) * KR_CHUNK, i1 = min(kron_npix(it.g), i0 + KR_CHUNK);
         KronAcc acc;
-        kacc_init(acc);
-        kron_range<PASS>(A, it.o, A.O.mx[it.o], A.O.my[it.o], it.g, i0 + threadIdx.x, i1, KR_THREADS, acc);
-        kacc_warp(acc);
+        kron_warp_sums<PASS>(A, it.o, A.O.mx[it.o], A.O.my[it.o], it.g, i0 + threadIdx.x, i1, KR_THREADS, acc);
         if (lane == 0) red[wid] = acc;
         __syncthreads();
         if (wid == 0) {
