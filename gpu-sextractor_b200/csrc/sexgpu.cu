@@ -864,7 +864,7 @@ int pipe_deblend(sexgpu_ctx *ctx) {
     if (rc) return rc;
     A.O = ctx->O;
     launch_deblend_assign(A, P<int>(ctx->rlists), P<int>(ctx->rcounts), nroots, S);
-    stage_mark(ctx, "deblend", 12 + deblend_split_launches(nroots) + scan_launches(nroots));
+    stage_mark(ctx, "deblend", 14 + deblend_split_launches(nroots) + scan_launches(nroots));
     ps.stage = 3;
     return SEXGPU_OK;
 }
@@ -1086,7 +1086,7 @@ int pipe_end(sexgpu_ctx *ctx) {
     EN(rows, (size_t)(ns + 1) * sizeof(sexgpu_object));
     k_write_rows<<<grid1(ns + 1, 128), 128, 0, st>>>(O, P<unsigned>(ctx->svals), ns, ns_dev,
                                                      P<sexgpu_object>(ctx->rows));
-    stage_mark(ctx, "catalog", 5 + scan_launches(nobj) + radix_launches(cbits, ns));
+    stage_mark(ctx, "catalog", 4 + scan_launches(nobj) + radix_launches(cbits, ns));
     CK(cudaGetLastError());
     if (ps.capf) {
         // the scalars come back with the frame; the host reads them after the
