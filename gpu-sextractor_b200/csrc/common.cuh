@@ -384,6 +384,45 @@ __device__ __forceinline__ unsigned fdiv(unsigned p, const FastDiv &f) {
     return f.m ? (unsigned)__umul64hi((unsigned long long)p, f.m) : p;
 }
 
+// The six exact moment sums of a preanalysis with XSum (warp-collective):
+// sub values and cd x^a y^b terms over pixels pix[i] (or pix[list[base + i]]),
+// x, y relative to (x0, y0).  Not inlined: the rare path when binned sums do
+// not hold the terms, kept out of the callers' registers.
+struct Moments6 {
+    XSum tv, mx, my, mx2, my2, mxy;
+};
+
+__device__ __noinline__ void moments_xsum(const float *cd, const float *sub, const unsigned *pix,
+                                          const unsigned short *list, int base, int n, FastDiv wdiv, int w, int x0,
+                                          int y0, Moments6 *out) {
+    Moments6 m;
+    xs_init(m.tv);
+    xs_init(m.mx);
+    xs_init(m.my);
+    xs_init(m.mx2);
+    xs_init(m.my2);
+    xs_init(m.mxy);
+    for (int i = threadIdx.x & 31; i < n; i += 32) {
+        const unsigned p = pix[list ? list[base + i] : i];
+        const int yy = (int)fdiv(p, wdiv), x = (int)p - yy * w - x0, y = yy - y0;
+        const float cval = cd[p], val = sub[p];
+        xs_add(m.mx, cval * x);
+        xs_add(m.my, cval * y);
+        xs_add(m.mx2, cval * x * x);
+        xs_add(m.my2, cval * y * y);
+        xs_add(m.mxy, cval * x * y);
+        xs_add(m.tv, val);
+    }
+    m.tv = xs_warp_sum(m.tv);
+    m.mx = xs_warp_sum(m.mx);
+    m.my = xs_warp_sum(m.my);
+    m.mx2 = xs_warp_sum(m.mx2);
+    m.my2 = xs_warp_sum(m.my2);
+    m.mxy = xs_warp_sum(m.mxy);
+    *out = m;
+}
+
+
 __device__ __forceinline__ int fexpo(float v) { return (int)((__float_as_uint(v) >> 23) & 0xff) - 127; }
 
 // bilinear background at (x, y), src/back.c:685-731

@@ -218,29 +218,14 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(AnaAr
         smy2 = bs_to_xsum(bs_warp_sum(bmy2));
         smxy = bs_to_xsum(bs_warp_sum(bmxy));
     } else {
-        xs_init(stv);
-        xs_init(smx);
-        xs_init(smy);
-        xs_init(smx2);
-        xs_init(smy2);
-        xs_init(smxy);
-        for (int i = lane; i < n; i += 32) {
-            unsigned p = __ldg(pix + i);
-            int yy = (int)fdiv(p, A.wdiv), x = (int)p - yy * w - xmin, y = yy - ymin;
-            float cval = __ldg(A.cd + p), val = __ldg(A.sub + p);
-            xs_add(stv, val);
-            xs_add(smx, cval * x);
-            xs_add(smy, cval * y);
-            xs_add(smx2, cval * x * x);
-            xs_add(smy2, cval * y * y);
-            xs_add(smxy, cval * x * y);
-        }
-        stv = xs_warp_sum(stv);
-        smx = xs_warp_sum(smx);
-        smy = xs_warp_sum(smy);
-        smx2 = xs_warp_sum(smx2);
-        smy2 = xs_warp_sum(smy2);
-        smxy = xs_warp_sum(smxy);
+        Moments6 m;
+        moments_xsum(A.cd, A.sub, pix, nullptr, 0, n, A.wdiv, w, xmin, ymin, &m);
+        stv = m.tv;
+        smx = m.mx;
+        smy = m.my;
+        smx2 = m.mx2;
+        smy2 = m.my2;
+        smxy = m.mxy;
     }
     if (lane != 0) return;
     if (srv.ovf | stv.ovf | smx.ovf | smy.ovf | smx2.ovf | smy2.ovf | smxy.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);

@@ -45,7 +45,8 @@ namespace sx {
 #define SX_DL_ARENA_MAX 32767
 #endif
 constexpr int DL_CAP0 = 256;                   // shared-memory tier (one warp per object)
-constexpr int DL_CAP1 = 64;                    // its small-object half (more warps resident per SM)
+constexpr int DL_CAP1 = 64;                    // its small-object classes (more warps resident per SM)
+constexpr int DL_CAP2 = 128;
 constexpr int DL_MID = SX_DL_MID;              // arena tier with 64-thread CTAs up to here, 256 above
 constexpr int DL_ARENA_MAX = SX_DL_ARENA_MAX;  // at most 32767: element indices are 16-bit
 constexpr int DL_SWEEP_BYTES = 45;   // shared bytes per pixel, sweep
@@ -618,29 +619,14 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
             smxy = bs_to_xsum(bs_warp_sum(bmxy));
             stv = bs_to_xsum(bs_warp_sum(btv));
         } else {
-            xs_init(smx);
-            xs_init(smy);
-            xs_init(smx2);
-            xs_init(smy2);
-            xs_init(smxy);
-            xs_init(stv);
-            for (int i = lane; i < nb; i += 32) {
-                const unsigned p = pix[whole ? i : blist[bb + i]];
-                const int yy = (int)fdiv(p, A.wdiv), x = (int)p - yy * A.w - xmin, y = yy - ymin;
-                const float cval = A.cd[p], val = A.sub[p];
-                xs_add(smx, cval * x);
-                xs_add(smy, cval * y);
-                xs_add(smx2, cval * x * x);
-                xs_add(smy2, cval * y * y);
-                xs_add(smxy, cval * x * y);
-                xs_add(stv, val);
-            }
-            smx = xs_warp_sum(smx);
-            smy = xs_warp_sum(smy);
-            smx2 = xs_warp_sum(smx2);
-            smy2 = xs_warp_sum(smy2);
-            smxy = xs_warp_sum(smxy);
-            stv = xs_warp_sum(stv);
+            Moments6 m;
+            moments_xsum(A.cd, A.sub, pix, whole ? nullptr : blist, bb, nb, A.wdiv, A.w, xmin, ymin, &m);
+            smx = m.mx;
+            smy = m.my;
+            smx2 = m.mx2;
+            smy2 = m.my2;
+            smxy = m.mxy;
+            stv = m.tv;
         }
         if (lane != 0) continue;
         if (srv.ovf | smx.ovf | smy.ovf | smx2.ovf | smy2.ovf | smxy.ovf | stv.ovf) atomicOr(status, SX_ST_RANGE);
@@ -833,7 +819,8 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 32 : NT == 64 ? 16 : NT == 256 
 // Size classes (list k at lists + k * n, n the number of roots or the
 // capacity the launches were sized for; its length in counts[k]):
 //   8  <= 64 pixels              shared memory, one warp
-//   0  (64, 256]                 shared memory, one warp
+//   9  (64, 128]                 shared memory, one warp
+//   0  (128, 256]                shared memory, one warp
 //   1  (1024, 2048]   2 (256, 1024]       arena (hybrid), 64 threads
 //   4  (4096, 8192]   5 (2048, 4096]      arena (hybrid), 256 threads
 //   3  (8192, 32767]             arena (hybrid), 1024 threads
@@ -844,10 +831,11 @@ __global__ void __launch_bounds__(NT, NT == 32 ? 32 : NT == 64 ? 16 : NT == 256 
 // end on short ones.  counts[DL_NLISTS + k] and counts[2 * DL_NLISTS + k]
 // are the cursors of the sweep and the assignment kernel that takes list k
 // first; counts[3 * DL_NLISTS ...] hold the class boundaries in sorted order.
-constexpr int DL_NLISTS = 9;
+constexpr int DL_NLISTS = 10;
 
 __device__ __forceinline__ int dl_class(int s) {
     if (s <= DL_CAP1) return 8;
+    if (s <= DL_CAP2) return 9;
     if (s <= DL_CAP0) return 0;
     if (s <= DL_MID) return s > DL_MID / 2 ? 1 : 2;
     if (s <= DL_ARENA_MAX) return s > 4 * DL_MID ? 3 : s > 2 * DL_MID ? 4 : 5;
@@ -950,10 +938,10 @@ constexpr int DL_HYB_BYTES = 5;
 
 void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S) {
     if (nroots <= 0) return;
-    static DevCache g0, g1, g2, g3, g4, g5;
+    static DevCache g0, g1, g2, g3, g4, g5, g6;
     const size_t n = (size_t)nroots;
     int *glist = const_cast<int *>(lists) + 7 * n;
-    const size_t m0 = DL_CAP0 * DL_SWEEP_BYTES, m1 = DL_CAP1 * DL_SWEEP_BYTES;
+    const size_t m0 = DL_CAP0 * DL_SWEEP_BYTES, m1 = DL_CAP1 * DL_SWEEP_BYTES, m2 = DL_CAP2 * DL_SWEEP_BYTES;
     const size_t h3 = (size_t)DL_HYB3 * DL_HYB_BYTES, h45 = (size_t)DL_HYB45 * DL_HYB_BYTES,
                  h12 = (size_t)DL_HYB12 * DL_HYB_BYTES;
     dl_fork(S);
@@ -967,6 +955,8 @@ void launch_deblend_sweep(const DebArgs &A, const int *lists, int *counts, int n
         A, dl_lists(lists, counts, n, 1, 2), DL_SCUR(1), 0, glist, counts + 7, DL_HYB12);
     k_dl_sweep<32><<<min(nroots, dl_grid(k_dl_sweep<32>, 32, m0, g0)), 32, m0, S.main>>>(
         A, dl_lists(lists, counts, n, 0), DL_SCUR(0), DL_CAP0, glist, counts + 7, 0);
+    k_dl_sweep<32><<<min(nroots, dl_grid(k_dl_sweep<32>, 32, m2, g6)), 32, m2, S.main>>>(
+        A, dl_lists(lists, counts, n, 9), DL_SCUR(9), DL_CAP2, glist, counts + 7, 0);
     k_dl_sweep<32><<<min(nroots, dl_grid(k_dl_sweep<32>, 32, m1, g4)), 32, m1, S.main>>>(
         A, dl_lists(lists, counts, n, 8), DL_SCUR(8), DL_CAP1, glist, counts + 7, 0);
     dl_join(S);
@@ -981,9 +971,9 @@ constexpr int DL_GTAB_MID = 128;   // classes 1, 2: 4 KB
 
 void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int nroots, const DebStreams &S) {
     if (nroots <= 0) return;
-    static DevCache g0, g1, g2, g3, g4, g5;
+    static DevCache g0, g1, g2, g3, g4, g5, g6;
     const size_t n = (size_t)nroots;
-    const size_t m0 = DL_CAP0 * DL_ASSIGN_BYTES, m1 = DL_CAP1 * DL_ASSIGN_BYTES;
+    const size_t m0 = DL_CAP0 * DL_ASSIGN_BYTES, m1 = DL_CAP1 * DL_ASSIGN_BYTES, m2 = DL_CAP2 * DL_ASSIGN_BYTES;
     const size_t tb = (size_t)DL_GTAB_BIG * DL_GTAB_BYTES, tm = (size_t)DL_GTAB_MID * DL_GTAB_BYTES;
     dl_fork(S);
     const int grid3 = min(nroots, dl_grid(k_deblend_assign, DB_THREADS, 0, g3));
@@ -997,6 +987,8 @@ void launch_deblend_assign(const DebArgs &A, const int *lists, int *counts, int 
         A, dl_lists(lists, counts, n, 1, 2), DL_ACUR(1), 0, DL_GTAB_MID);
     k_dl_assign<32><<<min(nroots, dl_grid(k_dl_assign<32>, 32, m0, g0)), 32, m0, S.main>>>(
         A, dl_lists(lists, counts, n, 0), DL_ACUR(0), DL_CAP0, 0);
+    k_dl_assign<32><<<min(nroots, dl_grid(k_dl_assign<32>, 32, m2, g6)), 32, m2, S.main>>>(
+        A, dl_lists(lists, counts, n, 9), DL_ACUR(9), DL_CAP2, 0);
     k_dl_assign<32><<<min(nroots, dl_grid(k_dl_assign<32>, 32, m1, g4)), 32, m1, S.main>>>(
         A, dl_lists(lists, counts, n, 8), DL_ACUR(8), DL_CAP1, 0);
     dl_join(S);

@@ -864,7 +864,7 @@ int pipe_deblend(sexgpu_ctx *ctx) {
     if (rc) return rc;
     A.O = ctx->O;
     launch_deblend_assign(A, P<int>(ctx->rlists), P<int>(ctx->rcounts), nroots, S);
-    stage_mark(ctx, "deblend", 14 + deblend_split_launches(nroots) + scan_launches(nroots));
+    stage_mark(ctx, "deblend", 16 + deblend_split_launches(nroots) + scan_launches(nroots));
     ps.stage = 3;
     return SEXGPU_OK;
 }
