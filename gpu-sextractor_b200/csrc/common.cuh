@@ -501,6 +501,7 @@ struct FrameScalars {
     int e0sub;                      // smallest exponent of a non-zero |sub|
     int kitems[2], kchunks[2];      // queued Kron boxes and their work items (pass 1, 2)
     int nvbig;                      // CLEAN victims when too many for the one-block sort, else 0
+    int nbig;                       // raw objects of more than 256 objects (their list: k_obj_partition)
     unsigned long long levpix;      // sum of the deblending level of every raw-object pixel
 };
 

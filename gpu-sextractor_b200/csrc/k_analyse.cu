@@ -579,7 +579,8 @@ __global__ void __launch_bounds__(OP_WARPS * 32) k_obj_partition(const unsigned 
                                                                  const int *__restrict__ rnkept,
                                                                  const int *__restrict__ objbase,
                                                                  const int *__restrict__ ooff, int nroots,
-                                                                 const int *nroots_dev, unsigned *__restrict__ opix) {
+                                                                 const int *nroots_dev, unsigned *__restrict__ opix,
+                                                                 int *nbig, int *biglist) {
     __shared__ int cur[OP_WARPS][OP_KMAX];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int r = blockIdx.x * OP_WARPS + wid;
@@ -590,25 +591,28 @@ __global__ void __launch_bounds__(OP_WARPS * 32) k_obj_partition(const unsigned 
         for (int i = lane; i < P; i += 32) opix[off + i] = rpix[off + i];
         return;
     }
-    if (K > OP_KMAX) return;
+    if (K > OP_KMAX) {  // left to k_obj_partition_big
+        if (lane == 0) biglist[atomicAdd(nbig, 1)] = r;
+        return;
+    }
     obj_partition_walk(rpix, objkey, off, P, K, ob, ooff, opix, cur[wid]);
 }
 
-// raw objects of more than OP_KMAX objects: one warp each, cursors in dynamic
+// raw objects of more than OP_KMAX objects (the list k_obj_partition made, in
+// any order: each writes its own range): one warp each, cursors in dynamic
 // shared memory up to OP_BIG_KMAX objects, else in gcur (global)
 __global__ void __launch_bounds__(32) k_obj_partition_big(const unsigned *__restrict__ rpix,
                                                           const unsigned *__restrict__ objkey,
                                                           const int *__restrict__ roff, const int *__restrict__ rsize,
                                                           const int *__restrict__ rnkept,
                                                           const int *__restrict__ objbase,
-                                                          const int *__restrict__ ooff, int nroots,
-                                                          const int *nroots_dev, unsigned *__restrict__ opix,
-                                                          int *gcur) {
+                                                          const int *__restrict__ ooff, const int *nbig,
+                                                          const int *__restrict__ biglist,
+                                                          unsigned *__restrict__ opix, int *gcur) {
     extern __shared__ int bigcur[];
-    nroots = sx_count(nroots, nroots_dev);
-    for (int r = blockIdx.x; r < nroots; r += gridDim.x) {
-        const int K = rnkept[r];
-        if (K <= OP_KMAX) continue;
+    const int nb = *nbig;
+    for (int i = blockIdx.x; i < nb; i += gridDim.x) {
+        const int r = biglist[i], K = rnkept[r];
         const int ob = objbase[r];
         obj_partition_walk(rpix, objkey, roff[r], rsize[r], K, ob, ooff, opix,
                            K <= OP_BIG_KMAX ? bigcur : gcur + ob);
@@ -616,15 +620,18 @@ __global__ void __launch_bounds__(32) k_obj_partition_big(const unsigned *__rest
     }
 }
 
-// gcur: scratch of one int per object.  nroots_dev (device, or null): the
-// number of roots when only the device knows it; nroots is then the capacity.
+// gcur: scratch of one int per object; nbig (zero on entry) and biglist
+// (nroots ints): the raw objects k_obj_partition leaves to the big kernel.
+// nroots_dev (device, or null): the number of roots when only the device
+// knows it; nroots is then the capacity.
 void launch_obj_partition(const unsigned *rpix, const unsigned *objkey, const RootBufs &R, const int *ooff,
-                          int nroots, const int *nroots_dev, unsigned *opix, int *gcur, cudaStream_t st) {
+                          int nroots, const int *nroots_dev, unsigned *opix, int *gcur, int *nbig, int *biglist,
+                          cudaStream_t st) {
     if (nroots <= 0) return;
     k_obj_partition<<<(unsigned)((nroots + OP_WARPS - 1) / OP_WARPS), OP_WARPS * 32, 0, st>>>(
-        rpix, objkey, R.off, R.size, R.nkept, R.objbase, ooff, nroots, nroots_dev, opix);
+        rpix, objkey, R.off, R.size, R.nkept, R.objbase, ooff, nroots, nroots_dev, opix, nbig, biglist);
     k_obj_partition_big<<<(unsigned)std::min(nroots, OP_BIG_GRID), 32, OP_BIG_KMAX * sizeof(int), st>>>(
-        rpix, objkey, R.off, R.size, R.nkept, R.objbase, ooff, nroots, nroots_dev, opix, gcur);
+        rpix, objkey, R.off, R.size, R.nkept, R.objbase, ooff, nbig, biglist, opix, gcur);
 }
 
 void launch_analyse(const AnaArgs &A, cudaStream_t st) {

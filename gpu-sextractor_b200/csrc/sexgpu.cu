@@ -885,8 +885,10 @@ int pipe_analyse(sexgpu_ctx *ctx) {
     ObjBufs &O = ctx->O;
     const int *nobj_dev = ps.capf ? &d_sc->nobj : nullptr;
     exclusive_scan(O.n, O.off, nobj, nullptr, tmp, st, nobj_dev);
+    // the deblending's size-class lists are free now: the list of the raw
+    // objects too large for the one-warp partition goes there
     launch_obj_partition(rpix, A.objkey, ps.R, O.off, ps.nroots, ps.capf ? &d_sc->nroots : nullptr, vals,
-                         P<int>(ctx->kalt), st);
+                         P<int>(ctx->kalt), &d_sc->nbig, P<int>(ctx->rlists), st);
     AnaArgs AA;
     EN(o_raw, (size_t)(nobj + 1) * sizeof(RobustRaw));
     AA.raw = P<RobustRaw>(ctx->o_raw);
