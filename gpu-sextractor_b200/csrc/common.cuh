@@ -289,7 +289,9 @@ __device__ __forceinline__ void xs_add_double(XSum &s, double d) {
         s.v += t;
 }
 
-__device__ __forceinline__ XSum bs_to_xsum(const BinSum &b) {
+// (out of line: called once per sum and object, it keeps one copy of the
+// conversion in the instruction cache instead of one per sum)
+__device__ __noinline__ XSum bs_to_xsum(const BinSum &b) {
     XSum x;
     xs_init(x);
     xs_add_double(x, b.b2);
