@@ -134,7 +134,7 @@ struct AnaArgs {
 // moments, ellipse and area correction are finished by k_robust_finish, one
 // thread per object, so that the double-precision tail does not run on one
 // lane of a warp.
-__global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(const __grid_constant__ AnaArgs A) {
+__global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(AnaArgs A) {
     const int lane = threadIdx.x & 31;
     const int o = blockIdx.x * AN_WARPS + (threadIdx.x >> 5);
     if (o >= sx_count(A.nobj, A.nobj_dev) || A.O.level[o] == 0) return;
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_analyse_robust(const
     A.O.dflux[o] = xs_float(stv);
 }
 
-__global__ void k_robust_finish(const __grid_constant__ AnaArgs A) {
+__global__ void k_robust_finish(AnaArgs A) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= sx_count(A.nobj, A.nobj_dev) || A.O.level[o] == 0) return;
     const RobustRaw R = A.raw[o];
@@ -323,7 +323,7 @@ __global__ void k_robust_finish(const __grid_constant__ AnaArgs A) {
 
 // examineiso (src/cuda/cudaanalyse.cu:2176-2581) and the CLEAN threshold
 // mthresh of every object.
-__global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(const __grid_constant__ AnaArgs A) {
+__global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(AnaArgs A) {
     __shared__ __align__(16) unsigned hist[AN_WARPS][256];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int o = blockIdx.x * AN_WARPS + wid;
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(AN_WARPS * 32, AN_MINB) k_examineiso(const __g
 // examineiso, per object: position errors, fluxes, FWHM fit, background
 // (one thread per object, so that this double-precision tail does not run on
 // one lane of a warp)
-__global__ void k_examine_finish(const __grid_constant__ AnaArgs A) {
+__global__ void k_examine_finish(AnaArgs A) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= sx_count(A.nobj, A.nobj_dev)) return;
     const ExamRaw X = A.xraw[o];

@@ -442,84 +442,6 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
 // ---------------------------------------------------------------------------
 // assignment: ownership of the kept branches, their preanalysis, gatherup
 // ---------------------------------------------------------------------------
-// The exact sums of one kept branch's preanalysis (k_dl_assign)
-struct BranchSums {
-    XSum srv, smx, smy, smx2, smy2, smxy, stv;
-};
-
-// Moments, ellipse, area correction and the object's columns of kept branch
-// o (root r, level L of threshold thrL), from its sums: one thread.  Not
-// inlined and not a template, so the four assignment kernels share one copy.
-__device__ __noinline__ void dl_branch_finish(const DebArgs &A, int o, int r, int L, float thrL, const BranchSums *bs,
-                                              int xmin, int xmax, int ymin, int ymax, int dnpix, int area2,
-                                              float peak, float cpeak) {
-    const BranchSums &S = *bs;
-    const double dthresh = thrL, dthresh2 = (dthresh + peak) / 2.0;
-    if (S.srv.ovf | S.smx.ovf | S.smy.ovf | S.smx2.ovf | S.smy2.ovf | S.smxy.ovf | S.stv.ovf) atomicOr(&A.sc->status, SX_ST_RANGE);
-    int flag = 0;
-    if (L > 0) flag |= SX_OBJ_MERGED;
-    if (xmin == 0 || xmax == A.w - 1 || ymin == 0 || ymax == A.h - 1) flag |= SX_OBJ_TRUNC;
-    const float rv = xs_float(S.srv);
-    const double rvd = rv;
-    const double mx = xs_double(S.smx), my = xs_double(S.smy);
-    const double mx2 = xs_double(S.smx2), my2 = xs_double(S.smy2), mxy = xs_double(S.smxy);
-    const double xm = mx / rvd, ym = my / rvd;
-    double xm2 = mx2 / rvd - xm * xm, ym2 = my2 / rvd - ym * ym, xym = mxy / rvd - xm * ym;
-    double temp, temp2, theta, pmx2, pmy2, darea, t1t2;
-    int singu = 0;
-    if ((temp2 = xm2 * ym2 - xym * xym) < 0.00694) {
-        xm2 += 0.0833333;
-        ym2 += 0.0833333;
-        temp2 = xm2 * ym2 - xym * xym;
-        singu = 1;
-    }
-    if ((fabs(temp = xm2 - ym2)) > 0.0)
-        theta = atan2(2.0 * xym, temp) / 2.0;
-    else
-        theta = SX_PI / 4.0;
-    temp = sqrt(0.25 * temp * temp + xym * xym);
-    pmy2 = pmx2 = 0.5 * (xm2 + ym2);
-    pmx2 += temp;
-    pmy2 -= temp;
-    const float fa = (float)sqrt(pmx2), fb = (float)sqrt(pmy2);
-    float abcor;
-    darea = (double)area2 - dnpix;
-    t1t2 = dthresh / dthresh2;
-    if (t1t2 > 0.0) {
-        abcor = (darea < 0.0 ? darea : -1.0) / (2 * SX_PI * log(t1t2 < 1.0 ? t1t2 : 0.99) * fa * fb);
-        if (abcor > 1.0) abcor = 1.0;
-    } else
-        abcor = 1.0;
-    A.O.root[o] = r;
-    A.O.level[o] = L;
-    A.O.node_dthresh[o] = thrL;
-    A.O.dthr[o] = A.R.dthresh[r];
-    A.O.athr[o] = A.R.thresh[r];
-    A.O.xmin[o] = xmin;
-    A.O.xmax[o] = xmax;
-    A.O.ymin[o] = ymin;
-    A.O.ymax[o] = ymax;
-    A.O.flags[o] = flag;
-    A.O.singu[o] = singu;
-    A.O.dnpix[o] = dnpix;
-    A.O.fdflux[o] = rv;
-    A.O.dflux[o] = xs_float(S.stv);
-    A.O.fdpeak[o] = cpeak;
-    A.O.dpeak[o] = peak;
-    A.O.mx[o] = xm + xmin;
-    A.O.my[o] = ym + ymin;
-    A.O.mx2[o] = xm2;
-    A.O.my2[o] = ym2;
-    A.O.mxy[o] = xym;
-    A.O.a[o] = fa;
-    A.O.b[o] = fb;
-    A.O.theta[o] = theta * 180.0 / SX_PI;
-    A.O.cxx[o] = (float)(ym2 / temp2);
-    A.O.cyy[o] = (float)(xm2 / temp2);
-    A.O.cxy[o] = (float)(-2 * xym / temp2);
-    A.O.abcor[o] = abcor;
-}
-
 // gtab: shared memory for the centres and shapes of up to gcap kept
 // branches (32 B each), staged for the gatherup; null when the kernel has none
 template <int NT>
@@ -707,8 +629,69 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
             stv = m.tv;
         }
         if (lane != 0) continue;
-        BranchSums bsums = {srv, smx, smy, smx2, smy2, smxy, stv};
-        dl_branch_finish(A, o, r, L, thr[L], &bsums, xmin, xmax, ymin, ymax, dnpix, area2, peak, ord2f(cpk));
+        if (srv.ovf | smx.ovf | smy.ovf | smx2.ovf | smy2.ovf | smxy.ovf | stv.ovf) atomicOr(status, SX_ST_RANGE);
+        int flag = 0;
+        if (L > 0) flag |= SX_OBJ_MERGED;
+        if (xmin == 0 || xmax == A.w - 1 || ymin == 0 || ymax == A.h - 1) flag |= SX_OBJ_TRUNC;
+        const float rv = xs_float(srv);
+        const double rvd = rv;
+        const double mx = xs_double(smx), my = xs_double(smy);
+        const double mx2 = xs_double(smx2), my2 = xs_double(smy2), mxy = xs_double(smxy);
+        const double xm = mx / rvd, ym = my / rvd;
+        double xm2 = mx2 / rvd - xm * xm, ym2 = my2 / rvd - ym * ym, xym = mxy / rvd - xm * ym;
+        double temp, temp2, theta, pmx2, pmy2, darea, t1t2;
+        int singu = 0;
+        if ((temp2 = xm2 * ym2 - xym * xym) < 0.00694) {
+            xm2 += 0.0833333;
+            ym2 += 0.0833333;
+            temp2 = xm2 * ym2 - xym * xym;
+            singu = 1;
+        }
+        if ((fabs(temp = xm2 - ym2)) > 0.0)
+            theta = atan2(2.0 * xym, temp) / 2.0;
+        else
+            theta = SX_PI / 4.0;
+        temp = sqrt(0.25 * temp * temp + xym * xym);
+        pmy2 = pmx2 = 0.5 * (xm2 + ym2);
+        pmx2 += temp;
+        pmy2 -= temp;
+        const float fa = (float)sqrt(pmx2), fb = (float)sqrt(pmy2);
+        float abcor;
+        darea = (double)area2 - dnpix;
+        t1t2 = dthresh / dthresh2;
+        if (t1t2 > 0.0) {
+            abcor = (darea < 0.0 ? darea : -1.0) / (2 * SX_PI * log(t1t2 < 1.0 ? t1t2 : 0.99) * fa * fb);
+            if (abcor > 1.0) abcor = 1.0;
+        } else
+            abcor = 1.0;
+        A.O.root[o] = r;
+        A.O.level[o] = L;
+        A.O.node_dthresh[o] = thr[L];
+        A.O.dthr[o] = A.R.dthresh[r];
+        A.O.athr[o] = A.R.thresh[r];
+        A.O.xmin[o] = xmin;
+        A.O.xmax[o] = xmax;
+        A.O.ymin[o] = ymin;
+        A.O.ymax[o] = ymax;
+        A.O.flags[o] = flag;
+        A.O.singu[o] = singu;
+        A.O.dnpix[o] = dnpix;
+        A.O.fdflux[o] = rv;
+        A.O.dflux[o] = xs_float(stv);
+        A.O.fdpeak[o] = ord2f(cpk);
+        A.O.dpeak[o] = peak;
+        A.O.mx[o] = xm + xmin;
+        A.O.my[o] = ym + ymin;
+        A.O.mx2[o] = xm2;
+        A.O.my2[o] = ym2;
+        A.O.mxy[o] = xym;
+        A.O.a[o] = fa;
+        A.O.b[o] = fb;
+        A.O.theta[o] = theta * 180.0 / SX_PI;
+        A.O.cxx[o] = (float)(ym2 / temp2);
+        A.O.cyy[o] = (float)(xm2 / temp2);
+        A.O.cxy[o] = (float)(-2 * xym / temp2);
+        A.O.abcor[o] = abcor;
         A.O.n[o] = bcnt[k];
     }
     __syncthreads();

@@ -590,17 +590,6 @@ __device__ __forceinline__ bool kron_range_bin(const EndArgs &A, int o, double m
     return true;
 }
 
-// the XSum form of the same sums (out of line: the rare fallback)
-template <int PASS>
-__device__ __noinline__ void kron_sums_xsum(const EndArgs &A, int o, double mx, double my, const KronGeo &g, int i0,
-                                            int i1, int step, KronAcc *out) {
-    KronAcc c;
-    kacc_init(c);
-    kron_range<PASS>(A, o, mx, my, g, i0, i1, step, c);
-    kacc_warp(c);
-    *out = c;
-}
-
 // a warp's sums over box pixels i0, i0 + step, ... < i1 (every lane holds them)
 template <int PASS>
 __device__ __forceinline__ void kron_warp_sums(const EndArgs &A, int o, double mx, double my, const KronGeo &g,
@@ -608,7 +597,9 @@ __device__ __forceinline__ void kron_warp_sums(const EndArgs &A, int o, double m
     // at most BS_MAX_TERMS terms of the warp per bin
     const bool binned = (PASS == 1 || !A.wvar) && (long long)(i1 - (i0 & ~31)) <= (long long)BS_MAX_TERMS * step / 32;
     if (binned && kron_range_bin<PASS>(A, o, mx, my, g, i0, i1, step, c)) return;
-    kron_sums_xsum<PASS>(A, o, mx, my, g, i0, i1, step, &c);
+    kacc_init(c);
+    kron_range<PASS>(A, o, mx, my, g, i0, i1, step, c);
+    kacc_warp(c);
 }
 
 // Queue object o's pass-`pass` box (warp-collective).  False when the queue is
@@ -654,7 +645,7 @@ __device__ void end_finish(const EndArgs &A, int o, int flags, float kron, bool 
 // catalogue columns of a survivor from its photometry sums: AUTO, ISOCOR and
 // ISO fluxes, magnitudes and errors, FLAGS (one thread per object, so that
 // this double-precision tail does not run on one lane of a warp)
-__global__ void k_end_finish(const __grid_constant__ EndArgs A) {
+__global__ void k_end_finish(EndArgs A) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= sx_count(A.n, A.n_dev) || A.O.fmaster[o] >= 0) return;
     const EndRaw R = A.raw[o];
@@ -727,7 +718,7 @@ __device__ void kron_after1(const EndArgs &A, int o, double mx, double my, int f
 }
 
 // one warp per surviving object (eight CTAs of four warps per SM)
-__global__ void __launch_bounds__(128, 8) k_endobject(const __grid_constant__ EndArgs A) {
+__global__ void __launch_bounds__(128, 8) k_endobject(EndArgs A) {
     const int lane = threadIdx.x & 31;
     const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (o >= sx_count(A.n, A.n_dev)) return;
@@ -746,7 +737,7 @@ __global__ void __launch_bounds__(128, 8) k_endobject(const __grid_constant__ En
 
 // queued boxes: one CTA per KR_CHUNK-pixel work item, partial sums per item
 template <int PASS>
-__global__ void __launch_bounds__(KR_THREADS) k_kron_chunks(const __grid_constant__ EndArgs A) {
+__global__ void __launch_bounds__(KR_THREADS) k_kron_chunks(EndArgs A) {
     __shared__ KronAcc red[KR_THREADS / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nc = min(A.sc->kchunks[PASS - 1], A.K.ccap);
@@ -777,7 +768,7 @@ __global__ void __launch_bounds__(KR_THREADS) k_kron_chunks(const __grid_constan
 constexpr int KR_MERGE_MAX = 1024;
 
 template <int PASS>
-__global__ void k_kron_merge(const __grid_constant__ EndArgs A) {
+__global__ void k_kron_merge(EndArgs A) {
     const int lane = threadIdx.x & 31;
     const int n = min(A.sc->kitems[PASS - 1], A.K.icap);
     const int nw = (gridDim.x * blockDim.x) >> 5;
