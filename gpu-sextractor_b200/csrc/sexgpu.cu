@@ -89,6 +89,8 @@ struct GraphEntry {
     int kron_warp_max = 0, grid_div = 1;
     int cap_roots = 0, cap_rootpix = 0, cap_obj = 0;  // 0: not learned yet
     cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;   // the captured graph (child node of a batch graph)
+    unsigned long long id = 0;     // unique within the context
     unsigned char *pin = nullptr;  // pinned constants the graph uploads (PipeState::pin)
     PipeState ps;                  // host state of the captured frame, restored on replay
     ObjBufs O;
@@ -96,6 +98,28 @@ struct GraphEntry {
     bool no_graph = false;       // capture failed: the capacity form runs uncaptured
     int kernels = 0;             // kernel nodes of the graph
     unsigned long long used = 0;
+};
+
+// One-launch form of a batch (sexgpu_extract_batch with graphs): per worker
+// a chain of its frames, each the upload of the frame into the worker's
+// input buffer, the frame kind's captured graph as a child graph, and copies
+// of its catalogue rows and scalars into per-frame areas; the chains side by
+// side in one graph, ended by one copy of every frame's scalars to the host.
+struct BatchGraph {
+    std::vector<unsigned long long> sig;            // per frame: kind, size, weight map, worker
+    std::vector<unsigned long long> epochs, gens;   // per worker at build time
+    std::vector<std::vector<int>> lists;            // per worker: its frames in order
+    std::vector<size_t> in_off, row_off;            // per frame: pinned input offset, first row
+    std::vector<int> cap;                           // per frame: rows the area holds
+    std::vector<FrameParams> pm;                    // per frame
+    cudaGraphExec_t exec = nullptr;
+    unsigned char *in_host = nullptr;               // pinned frames and weight maps
+    size_t in_bytes = 0;
+    void *rows_dev = nullptr, *sc_dev = nullptr;
+    FrameScalars *sc_host = nullptr;                // pinned
+    unsigned char *rows_host = nullptr;             // pinned
+    size_t rows_total = 0;
+    int kernels = 0;
 };
 
 struct sexgpu_ctx {
@@ -141,6 +165,9 @@ struct sexgpu_ctx {
     unsigned long long gen = 0;          // bumped by every device allocation (graphs hold pointers)
     std::vector<GraphEntry> graphs;      // captured frames, least recently used evicted
     unsigned long long graph_clock = 0;
+    unsigned long long graph_epoch = 0;  // bumped whenever a graph is captured or dropped
+    unsigned long long last_entry = 0;   // id of the graph entry of the last extraction (0: none)
+    BatchGraph *bgraph = nullptr;        // one-launch form of the last batch (sexgpu_extract_batch)
     FrameScalars *hsc_pin = nullptr;     // pinned copy of the frame scalars (capacity form)
     int last_graph = 0;                  // the last extraction replayed a graph
     int last_kernels = 0;                // kernel launches of the last extraction
@@ -1133,6 +1160,48 @@ int run_pipeline(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w
 // ---------------------------------------------------------------------------
 constexpr int GRAPH_CACHE = 8;  // frame kinds kept per context
 
+void free_batch_graph(sexgpu_ctx *ctx) {
+    BatchGraph *b = ctx->bgraph;
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->in_host) cudaFreeHost(b->in_host);
+    if (b->rows_dev) cudaFree(b->rows_dev);
+    if (b->sc_dev) cudaFree(b->sc_dev);
+    if (b->sc_host) cudaFreeHost(b->sc_host);
+    if (b->rows_host) cudaFreeHost(b->rows_host);
+    delete b;
+    ctx->bgraph = nullptr;
+}
+
+// status of one frame from its scalars, as capacity_status: 1 when the frame
+// must be extracted again without its graph
+int scalars_status(const FrameScalars &sc) {
+    const int s = sc.status;
+    if (s & SX_ST_LOAD) return SEXGPU_ERR_LOAD;
+    if (s & SX_ST_CAPACITY) return 1;
+    if (s & SX_ST_LOOP) return SEXGPU_ERR_LOOP;
+    if (s & SX_ST_RANGE) return SEXGPU_ERR_RANGE;
+    if (s & SX_ST_THRESH) return SEXGPU_ERR_THRESH;
+    return SEXGPU_OK;
+}
+
+void summary_from_scalars(const FrameScalars &sc, const FrameParams &P, sexgpu_summary *s) {
+    memset(s, 0, sizeof(*s));
+    s->nbackx = P.nbx;
+    s->nbacky = P.nby;
+    s->backmean = sc.backmean;
+    s->backsig = sc.backsig;
+    s->dthresh = sc.dthresh;
+    s->thresh = sc.thresh;
+    s->npix_above = sc.npix_above;
+    s->nraw = sc.nroots;
+    s->nraw_pix = sc.nrootpix;
+    s->ndetected = sc.nobj;
+    s->nobj = sc.nsurv;
+    s->level_pix = (int64_t)sc.levpix;
+    s->sigfac = sc.sigfac;
+}
+
 int cap_of(long long count, long long bound) {
     const long long c = count + count / 4 + 256;
     return (int)std::max(0ll, std::min(c, bound));
@@ -1144,10 +1213,13 @@ void learn_caps(const sexgpu_ctx *ctx, GraphEntry &e, long long N, int minarea) 
     e.cap_obj = std::max(e.cap_obj, cap_of(ctx->hsc.nobj, N));
 }
 
-void drop_graph(GraphEntry &e) {
+void drop_graph(sexgpu_ctx *ctx, GraphEntry &e) {
+    if (e.exec || e.graph) ctx->graph_epoch++;
     if (e.exec) cudaGraphExecDestroy(e.exec);
+    if (e.graph) cudaGraphDestroy(e.graph);
     if (e.pin) cudaFreeHost(e.pin);
     e.exec = nullptr;
+    e.graph = nullptr;
     e.pin = nullptr;
 }
 
@@ -1220,12 +1292,14 @@ void capture_graph(sexgpu_ctx *ctx, GraphEntry &e, const float *d_img, const flo
         ce = cudaGraphInstantiate(&e.exec, g, 0);
         if (ce != cudaSuccess) e.exec = nullptr;
     }
-    if (g) cudaGraphDestroy(g);
     if (!e.exec) {
+        if (g) cudaGraphDestroy(g);
         cudaGetLastError();
         e.no_graph = true;
         return;
     }
+    e.graph = g;
+    ctx->graph_epoch++;
     e.gen = ctx->gen;
     e.ps = ps;
     e.O = ctx->O;
@@ -1248,6 +1322,7 @@ void finish_capacity(sexgpu_ctx *ctx, int w, int h) {
 int run_graph(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, int h, const sexgpu_config *cfg) {
     ctx->last_graph = 0;
     ctx->last_kernels = 0;
+    ctx->last_entry = 0;
     if (check_config(cfg, w, h) || (cfg->weight_type >= 1 && cfg->weight_type <= 3) != (d_wmap != nullptr))
         return run_pipeline(ctx, d_img, d_wmap, w, h, cfg);  // reports the error
     FrameParams Pm;
@@ -1266,7 +1341,7 @@ int run_graph(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, i
         if ((int)ctx->graphs.size() >= GRAPH_CACHE) {
             auto old = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
                                         [](const GraphEntry &a, const GraphEntry &b) { return a.used < b.used; });
-            drop_graph(*old);
+            drop_graph(ctx, *old);
             ctx->graphs.erase(old);
         }
         ctx->graphs.emplace_back();
@@ -1278,8 +1353,10 @@ int run_graph(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, i
         e->nnw = ctx->nnw_dev;
         e->kron_warp_max = ctx->kron_warp_max;
         e->grid_div = sx_grid_div;
+        e->id = ++ctx->graph_clock;
     }
     e->used = ++ctx->graph_clock;
+    ctx->last_entry = e->id;
     const long long N = (long long)w * h;
     if (!e->cap_obj) {  // a new frame kind: the plain form, and its counts
         int rc = run_pipeline(ctx, d_img, d_wmap, w, h, cfg);
@@ -1309,7 +1386,7 @@ int run_graph(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, i
         ctx->last_graph = 1;
         ctx->last_kernels = e->kernels;
     } else {
-        drop_graph(*e);
+        drop_graph(ctx, *e);
         ctx->ps.capf = true;
         set_caps(ctx->ps, *e);
         rc = run_pipeline(ctx, d_img, d_wmap, w, h, cfg);
@@ -1322,7 +1399,7 @@ int run_graph(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, i
     if (rc == 1) {  // counts beyond the capacities: plain form, larger capacities
         ctx->last_graph = 0;
         ctx->last_kernels = 0;
-        drop_graph(*e);
+        drop_graph(ctx, *e);
         e->no_graph = false;
         rc = run_pipeline(ctx, d_img, d_wmap, w, h, cfg);
         if (!rc) learn_caps(ctx, *e, N, Pm.minarea);
@@ -1446,7 +1523,8 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_block) cudaEventDestroy(ctx->ev_block);
-    for (GraphEntry &e : ctx->graphs) drop_graph(e);
+    free_batch_graph(ctx);
+    for (GraphEntry &e : ctx->graphs) drop_graph(ctx, e);
     ctx->graphs.clear();
     if (ctx->hsc_pin) cudaFreeHost(ctx->hsc_pin);
     for (sexgpu_ctx *w : ctx->workers) sexgpu_destroy(w);
@@ -1818,6 +1896,303 @@ int sexgpu_getconv(const char *path, float *mask, int maxn, int *mw, int *mh) {
     return n;
 }
 
+// pinned host buffers of a batch worker grow with headroom; outgrown ones
+// are freed after the batch
+static bool batch_grow(sexgpu_ctx *wc, void *&buf, size_t &have, size_t need) {
+    if (have >= need) return true;
+    if (buf) wc->host_graveyard.push_back(buf);
+    buf = nullptr;
+    have = 0;
+    const size_t want = need + need / 4;
+    if (cudaHostAlloc(&buf, want, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    have = want;
+    return true;
+}
+
+// One frame of a batch on worker wc.  The worker copies the frame (and
+// weight map) into its own pinned buffer first and brings the catalogue rows
+// back through another, so that the transfers of different workers are DMA
+// transfers that proceed in parallel instead of queueing on the driver's
+// pageable staging.
+static void batch_one_frame(sexgpu_ctx *wc, sexgpu_batch_frame &f) {
+    f.nobj = 0;
+    if (!f.img || !f.cfg || f.w <= 0 || f.h <= 0 || f.max_objects < 0 || (f.max_objects > 0 && !f.objs)) {
+        f.status = SEXGPU_ERR_ARG;
+        return;
+    }
+    const size_t bytes = (size_t)f.w * f.h * sizeof(float);
+    const float *src = f.img, *wsrc = f.wmap;
+    if (batch_grow(wc, wc->stage_host, wc->stage_bytes, f.wmap ? 2 * bytes : bytes)) {
+        memcpy(wc->stage_host, f.img, bytes);
+        src = (const float *)wc->stage_host;
+        if (f.wmap) {
+            memcpy((char *)wc->stage_host + bytes, f.wmap, bytes);
+            wsrc = (const float *)((char *)wc->stage_host + bytes);
+        }
+    }
+    const size_t rbytes = (size_t)f.max_objects * sizeof(sexgpu_object);
+    if (!batch_grow(wc, wc->rows_host, wc->rows_bytes, std::min(rbytes, (size_t)1 << 20))) {
+        f.status = sexgpu_extract(wc, src, wsrc, f.w, f.h, f.cfg, f.objs, f.max_objects, &f.nobj, nullptr, nullptr,
+                                  nullptr, &f.summary);
+        return;
+    }
+    f.status = sexgpu_extract(wc, src, wsrc, f.w, f.h, f.cfg, nullptr, 0, &f.nobj, nullptr, nullptr, nullptr,
+                              &f.summary);
+    if (f.status) return;
+    const int n = std::min(f.nobj, f.max_objects);
+    const size_t nb = (size_t)n * sizeof(sexgpu_object);
+    if (n > 0 && !batch_grow(wc, wc->rows_host, wc->rows_bytes, nb)) {
+        f.status = SEXGPU_ERR_NOMEM;
+        return;
+    }
+    if (n > 0) {
+        cudaError_t e = cudaMemcpyAsync(wc->rows_host, wc->rows.p, nb, cudaMemcpyDeviceToHost, wc->stream);
+        if (e == cudaSuccess) e = stream_wait(wc, wc->stream);
+        if (e != cudaSuccess) {
+            f.status = set_err(wc, e, "catalogue copy");
+            return;
+        }
+        memcpy(f.objs, wc->rows_host, nb);
+    }
+    if (f.nobj > f.max_objects) f.status = SEXGPU_ERR_CAPACITY;
+}
+
+// Frame kind of a batch frame (size, configuration, mask, weight map).
+static unsigned long long batch_kind(const sexgpu_batch_frame &f) {
+    unsigned long long hsh = 1469598103934665603ull;
+    auto mix = [&](const void *p, size_t n) {
+        for (size_t k = 0; k < n; k++) hsh = (hsh ^ ((const unsigned char *)p)[k]) * 1099511628211ull;
+    };
+    if (f.cfg && f.w > 0 && f.h > 0) {
+        FrameParams Pm;
+        make_params(f.cfg, f.w, f.h, Pm);
+        mix(&Pm, sizeof(Pm));
+        if (f.cfg->filter_flag && f.cfg->conv)
+            mix(f.cfg->conv, sizeof(float) * (size_t)std::max(f.cfg->conv_w, 0) * std::max(f.cfg->conv_h, 0));
+    }
+    const int hasw = f.wmap != nullptr;
+    mix(&hasw, sizeof(hasw));
+    return hsh;
+}
+
+// Frames of each worker with graphs: whole kinds to the least loaded worker
+// (largest kinds first, by pixels), a kind larger than a worker's share
+// frame by frame; each list largest frame first.  Deterministic, so that a
+// batch repeated keeps every kind on the worker that holds its graph.
+static std::vector<std::vector<int>> batch_lists(const sexgpu_batch_frame *frames, int n, int workers,
+                                                 const std::vector<int> &order,
+                                                 const std::vector<unsigned long long> &kind) {
+    std::vector<std::vector<int>> wl(workers);
+    std::vector<unsigned long long> kinds;
+    std::vector<long long> kpix;
+    std::vector<std::vector<int>> kfr;
+    long long total = 0;
+    for (int k = 0; k < n; k++) {
+        const int i = order[k];
+        const long long px = (long long)std::max(frames[i].w, 0) * std::max(frames[i].h, 0);
+        total += px;
+        size_t j = std::find(kinds.begin(), kinds.end(), kind[i]) - kinds.begin();
+        if (j == kinds.size()) {
+            kinds.push_back(kind[i]);
+            kpix.push_back(0);
+            kfr.emplace_back();
+        }
+        kpix[j] += px;
+        kfr[j].push_back(i);
+    }
+    std::vector<int> ko(kinds.size());
+    for (size_t j = 0; j < ko.size(); j++) ko[j] = (int)j;
+    std::stable_sort(ko.begin(), ko.end(), [&](int a, int b) { return kpix[a] > kpix[b]; });
+    std::vector<long long> load(workers, 0);
+    auto least = [&]() { return (int)(std::min_element(load.begin(), load.end()) - load.begin()); };
+    for (int j : ko) {
+        if (kpix[j] * workers <= total) {
+            const int w = least();
+            for (int i : kfr[j]) wl[w].push_back(i);
+            load[w] += kpix[j];
+        } else {
+            for (int i : kfr[j]) {
+                const int w = least();
+                wl[w].push_back(i);
+                load[w] += (long long)frames[i].w * frames[i].h;
+            }
+        }
+    }
+    std::vector<int> rank(n);
+    for (int k = 0; k < n; k++) rank[order[k]] = k;
+    for (auto &l : wl) std::stable_sort(l.begin(), l.end(), [&](int a, int b) { return rank[a] < rank[b]; });
+    return wl;
+}
+
+static bool batch_graph_valid(const sexgpu_ctx *ctx) {
+    const BatchGraph *b = ctx->bgraph;
+    if (!b || !b->exec || b->epochs.size() > ctx->workers.size()) return false;
+    for (size_t w = 0; w < b->epochs.size(); w++)
+        if (ctx->workers[w]->graph_epoch != b->epochs[w] || ctx->workers[w]->gen != b->gens[w]) return false;
+    return true;
+}
+
+// Builds the one-launch form of a batch whose every frame was just replayed
+// from its worker's graph (entry ids per frame).  Failure leaves no batch
+// graph: the next batch takes the per-frame path again.
+static void build_batch_graph(sexgpu_ctx *ctx, const sexgpu_batch_frame *frames, int n,
+                              const std::vector<std::vector<int>> &wl, const std::vector<unsigned long long> &sig,
+                              const std::vector<unsigned long long> &entry) {
+    free_batch_graph(ctx);
+    cudaSetDevice(ctx->device);
+    BatchGraph *b = new BatchGraph;
+    b->sig = sig;
+    b->lists = wl;
+    b->in_off.assign(n, 0);
+    b->row_off.assign(n, 0);
+    b->cap.assign(n, 0);
+    b->pm.resize(n);
+    std::vector<const GraphEntry *> ent(n, nullptr);
+    size_t in = 0, rows = 0;
+    const size_t S = sizeof(sexgpu_object);
+    bool ok = true;
+    for (size_t w = 0; w < wl.size() && ok; w++) {
+        const sexgpu_ctx *wc = ctx->workers[w];
+        b->epochs.push_back(wc->graph_epoch);
+        b->gens.push_back(wc->gen);
+        for (int i : wl[w]) {
+            for (const GraphEntry &e : wc->graphs)
+                if (e.id == entry[i] && e.graph && e.exec && e.gen == wc->gen) ent[i] = &e;
+            if (!ent[i]) {
+                ok = false;
+                break;
+            }
+            b->cap[i] = ent[i]->cap_obj;
+            b->pm[i] = ent[i]->Pm;
+            const size_t bytes = (size_t)frames[i].w * frames[i].h * sizeof(float) * (frames[i].wmap ? 2 : 1);
+            b->in_off[i] = in;
+            in += (bytes + 255) & ~(size_t)255;
+            b->row_off[i] = rows;
+            rows += (size_t)b->cap[i] + 1;
+        }
+    }
+    b->in_bytes = in;
+    b->rows_total = rows;
+    ok = ok && cudaHostAlloc((void **)&b->in_host, std::max(in, (size_t)256), cudaHostAllocPortable) == cudaSuccess &&
+         cudaMalloc(&b->rows_dev, rows * S) == cudaSuccess &&
+         cudaMalloc(&b->sc_dev, (size_t)n * sizeof(FrameScalars)) == cudaSuccess &&
+         cudaHostAlloc((void **)&b->sc_host, (size_t)n * sizeof(FrameScalars), cudaHostAllocPortable) == cudaSuccess &&
+         cudaHostAlloc((void **)&b->rows_host, rows * S, cudaHostAllocPortable) == cudaSuccess;
+    cudaGraph_t g = nullptr;
+    ok = ok && cudaGraphCreate(&g, 0) == cudaSuccess;
+    std::vector<cudaGraphNode_t> tails;
+    for (size_t w = 0; w < wl.size() && ok; w++) {
+        sexgpu_ctx *wc = ctx->workers[w];
+        cudaGraphNode_t prev = nullptr;
+        for (int i : wl[w]) {
+            const size_t bytes = (size_t)frames[i].w * frames[i].h * sizeof(float);
+            cudaGraphNode_t in1 = nullptr, in2 = nullptr, child = nullptr, r = nullptr, sc = nullptr, join = nullptr;
+            ok = ok && cudaGraphAddMemcpyNode1D(&in1, g, prev ? &prev : nullptr, prev ? 1 : 0, wc->img.p,
+                                                b->in_host + b->in_off[i], bytes, cudaMemcpyHostToDevice) ==
+                           cudaSuccess;
+            std::vector<cudaGraphNode_t> deps{in1};
+            if (ok && frames[i].wmap) {
+                ok = cudaGraphAddMemcpyNode1D(&in2, g, prev ? &prev : nullptr, prev ? 1 : 0, wc->var.p,
+                                              b->in_host + b->in_off[i] + bytes, bytes, cudaMemcpyHostToDevice) ==
+                     cudaSuccess;
+                deps.push_back(in2);
+            }
+            ok = ok && cudaGraphAddChildGraphNode(&child, g, deps.data(), deps.size(), ent[i]->graph) == cudaSuccess;
+            ok = ok && cudaGraphAddMemcpyNode1D(&r, g, &child, 1, (char *)b->rows_dev + b->row_off[i] * S,
+                                                wc->rows.p, ((size_t)b->cap[i] + 1) * S,
+                                                cudaMemcpyDeviceToDevice) == cudaSuccess;
+            ok = ok && cudaGraphAddMemcpyNode1D(&sc, g, &child, 1, (char *)b->sc_dev + (size_t)i * sizeof(FrameScalars),
+                                                wc->sc.p, sizeof(FrameScalars), cudaMemcpyDeviceToDevice) ==
+                           cudaSuccess;
+            cudaGraphNode_t two[2] = {r, sc};
+            ok = ok && cudaGraphAddEmptyNode(&join, g, two, 2) == cudaSuccess;
+            prev = join;
+            if (ok) b->kernels += ent[i]->kernels;
+        }
+        if (prev) tails.push_back(prev);
+    }
+    cudaGraphNode_t out = nullptr;
+    ok = ok && cudaGraphAddMemcpyNode1D(&out, g, tails.data(), tails.size(), b->sc_host, b->sc_dev,
+                                        (size_t)n * sizeof(FrameScalars), cudaMemcpyDeviceToHost) == cudaSuccess;
+    ok = ok && cudaGraphInstantiate(&b->exec, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    ctx->bgraph = b;
+    if (!ok) {
+        cudaGetLastError();
+        free_batch_graph(ctx);
+    }
+}
+
+// The batch as one graph launch.  Returns SEXGPU_OK or a frame's error;
+// frames whose counts exceeded their graph's capacities are extracted again
+// by their workers, and the batch graph is dropped (its capacities grew).
+static int batch_launch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int n) {
+    BatchGraph *b = ctx->bgraph;
+    cudaStream_t st = ctx->stream;
+    const size_t S = sizeof(sexgpu_object);
+    // frames into the pinned input, one host thread per worker list
+    {
+        auto stage = [&](size_t w) {
+            for (int i : b->lists[w]) {
+                const sexgpu_batch_frame &f = frames[i];
+                const size_t bytes = (size_t)f.w * f.h * sizeof(float);
+                memcpy(b->in_host + b->in_off[i], f.img, bytes);
+                if (f.wmap) memcpy(b->in_host + b->in_off[i] + bytes, f.wmap, bytes);
+            }
+        };
+        std::vector<std::thread> pool;
+        for (size_t w = 1; w < b->lists.size(); w++) pool.emplace_back(stage, w);
+        stage(0);
+        for (auto &t : pool) t.join();
+    }
+    CK(cudaGraphLaunch(b->exec, st));
+    CK(stream_wait(ctx, st));
+    std::vector<int> again;
+    for (int i = 0; i < n; i++) {
+        sexgpu_batch_frame &f = frames[i];
+        const FrameScalars &sc = b->sc_host[i];
+        const int rc = scalars_status(sc);
+        f.nobj = 0;
+        f.status = rc;
+        if (rc == 1) {
+            again.push_back(i);
+            continue;
+        }
+        if (rc) continue;
+        f.nobj = sc.nsurv;
+        summary_from_scalars(sc, b->pm[i], &f.summary);
+        const int k = std::min(f.nobj, f.max_objects);
+        if (k > 0 && f.objs)
+            CK(cudaMemcpyAsync(b->rows_host + b->row_off[i] * S, (char *)b->rows_dev + b->row_off[i] * S, (size_t)k * S,
+                               cudaMemcpyDeviceToHost, st));
+    }
+    CK(stream_wait(ctx, st));
+    for (int i = 0; i < n; i++) {
+        sexgpu_batch_frame &f = frames[i];
+        if (f.status) continue;
+        const int k = std::min(f.nobj, f.max_objects);
+        if (k > 0 && f.objs) memcpy(f.objs, b->rows_host + b->row_off[i] * S, (size_t)k * S);
+        if (f.nobj > f.max_objects) f.status = SEXGPU_ERR_CAPACITY;
+    }
+    ctx->last_graph = 1;
+    ctx->last_kernels = b->kernels;
+    if (!again.empty()) {
+        for (size_t w = 0; w < b->lists.size(); w++)
+            for (int i : b->lists[w])
+                if (std::find(again.begin(), again.end(), i) != again.end()) batch_one_frame(ctx->workers[w], frames[i]);
+        free_batch_graph(ctx);
+    }
+    for (int i = 0; i < n; i++)
+        if (frames[i].status != SEXGPU_OK) {
+            ctx->err = "frame " + std::to_string(i) + " failed";
+            return frames[i].status;
+        }
+    return SEXGPU_OK;
+}
+
 int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframes, int workers) {
     if (!ctx || nframes < 0 || (nframes > 0 && !frames) || workers < 0) return SEXGPU_ERR_ARG;
     if (nframes == 0) return SEXGPU_OK;
@@ -1839,131 +2214,64 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
         w->defer_free = true;
         w->graph_mode = ctx->graph_mode;
     }
+    ctx->last_graph = 0;
+    ctx->last_kernels = 0;
     // largest frames first, so that the last frames to start are short
     std::vector<int> order(nframes);
     for (int i = 0; i < nframes; i++) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
         return (long long)frames[a].w * frames[a].h > (long long)frames[b].w * frames[b].h;
     });
-    std::atomic<int> next(0);
-    // With graphs, a worker takes the next frame of a kind it has met before
-    // (its graphs stay with it across batches), else the next frame: kinds
-    // are keyed by size, configuration and mask.
-    std::vector<unsigned long long> kind(nframes, 0);
-    std::vector<char> taken(nframes, 0);
-    std::mutex pick_mu;
-    if (ctx->graph_mode)
+    const int div = ctx->batch_grid_div > 0 ? ctx->batch_grid_div : 1;
+    // With graphs: fixed lists per worker, so that each kind stays with the
+    // worker that holds its graph; a batch repeated after one whose every
+    // frame replayed a graph is a single launch of the batch graph.
+    std::vector<std::vector<int>> wl;
+    std::vector<unsigned long long> sig, kind(nframes, 0), entry(nframes, 0);
+    std::vector<char> replayed(nframes, 0);
+    if (ctx->graph_mode) {
+        bool args_ok = true;
         for (int i = 0; i < nframes; i++) {
             const sexgpu_batch_frame &f = frames[i];
-            unsigned long long hsh = 1469598103934665603ull;
-            auto mix = [&](const void *p, size_t n) {
-                for (size_t k = 0; k < n; k++) hsh = (hsh ^ ((const unsigned char *)p)[k]) * 1099511628211ull;
-            };
-            if (f.cfg && f.w > 0 && f.h > 0) {
-                FrameParams Pm;
-                make_params(f.cfg, f.w, f.h, Pm);
-                mix(&Pm, sizeof(Pm));
-                if (f.cfg->filter_flag && f.cfg->conv)
-                    mix(f.cfg->conv, sizeof(float) * (size_t)std::max(f.cfg->conv_w, 0) * std::max(f.cfg->conv_h, 0));
+            kind[i] = batch_kind(f);
+            args_ok = args_ok && f.img && f.cfg && f.w > 0 && f.h > 0 && f.max_objects >= 0 &&
+                      (f.max_objects == 0 || f.objs);
+        }
+        wl = batch_lists(frames, nframes, workers, order, kind);
+        for (int w = 0; w < workers; w++)
+            for (int i : wl[w]) {
+                sig.push_back(kind[i]);
+                sig.push_back(((unsigned long long)frames[i].w << 32) | (unsigned)frames[i].h);
+                sig.push_back(((unsigned long long)w << 32) | (unsigned)i | (frames[i].wmap ? 1ull << 31 : 0ull));
             }
-            const int hasw = f.wmap != nullptr;
-            mix(&hasw, sizeof(hasw));
-            kind[i] = hsh;
-        }
-    auto pick = [&](sexgpu_ctx *wc) -> int {
-        if (!ctx->graph_mode) {
-            const int k = next.fetch_add(1);
-            return k < nframes ? order[k] : -1;
-        }
-        std::lock_guard<std::mutex> lk(pick_mu);
-        int first = -1;
-        for (int k = 0; k < nframes; k++) {
-            const int i = order[k];
-            if (taken[i]) continue;
-            if (first < 0) first = i;
-            if (std::find(wc->batch_kinds.begin(), wc->batch_kinds.end(), kind[i]) != wc->batch_kinds.end()) {
-                first = i;
-                break;
-            }
-        }
-        if (first >= 0) {
-            taken[first] = 1;
-            if (std::find(wc->batch_kinds.begin(), wc->batch_kinds.end(), kind[first]) == wc->batch_kinds.end()) {
-                wc->batch_kinds.push_back(kind[first]);
-                if ((int)wc->batch_kinds.size() > 4 * GRAPH_CACHE) wc->batch_kinds.erase(wc->batch_kinds.begin());
-            }
-        }
-        return first;
-    };
-    // Each worker copies its frame (and weight map) into its own pinned buffer
-    // first and brings the catalogue rows back through another, so that the
-    // transfers of different workers are DMA transfers that proceed in
-    // parallel instead of queueing on the driver's pageable staging.
-    // pinned buffers grow with headroom; outgrown ones are freed after the batch
-    auto grow = [](sexgpu_ctx *wc, void *&buf, size_t &have, size_t need) {
-        if (have >= need) return true;
-        if (buf) wc->host_graveyard.push_back(buf);
-        buf = nullptr;
-        have = 0;
-        const size_t want = need + need / 4;
-        if (cudaHostAlloc(&buf, want, cudaHostAllocPortable) != cudaSuccess) {
-            cudaGetLastError();
-            return false;
-        }
-        have = want;
-        return true;
-    };
-    const int div = ctx->batch_grid_div > 0 ? ctx->batch_grid_div : 1;
-    auto run = [&](sexgpu_ctx *wc) {
+        sig.push_back((unsigned long long)div);
+        if (args_ok && ctx->bgraph && ctx->bgraph->sig == sig && batch_graph_valid(ctx))
+            return batch_launch(ctx, frames, nframes);
+    }
+    std::atomic<int> next(0);
+    std::vector<size_t> cursor(workers, 0);
+    auto run = [&](int wi) {
+        sexgpu_ctx *wc = ctx->workers[wi];
         cudaSetDevice(wc->device);
         sx_grid_div = div;
-        for (int fi; (fi = pick(wc)) >= 0;) {
-            sexgpu_batch_frame &f = frames[fi];
-            f.nobj = 0;
-            if (!f.img || !f.cfg || f.w <= 0 || f.h <= 0 || f.max_objects < 0 || (f.max_objects > 0 && !f.objs)) {
-                f.status = SEXGPU_ERR_ARG;
-                continue;
+        for (;;) {
+            int fi;
+            if (ctx->graph_mode) {
+                if (cursor[wi] >= wl[wi].size()) break;
+                fi = wl[wi][cursor[wi]++];
+            } else {
+                const int k = next.fetch_add(1);
+                if (k >= nframes) break;
+                fi = order[k];
             }
-            const size_t bytes = (size_t)f.w * f.h * sizeof(float);
-            const float *src = f.img, *wsrc = f.wmap;
-            if (grow(wc, wc->stage_host, wc->stage_bytes, f.wmap ? 2 * bytes : bytes)) {
-                memcpy(wc->stage_host, f.img, bytes);
-                src = (const float *)wc->stage_host;
-                if (f.wmap) {
-                    memcpy((char *)wc->stage_host + bytes, f.wmap, bytes);
-                    wsrc = (const float *)((char *)wc->stage_host + bytes);
-                }
-            }
-            const size_t rbytes = (size_t)f.max_objects * sizeof(sexgpu_object);
-            if (!grow(wc, wc->rows_host, wc->rows_bytes, std::min(rbytes, (size_t)1 << 20))) {
-                f.status = sexgpu_extract(wc, src, wsrc, f.w, f.h, f.cfg, f.objs, f.max_objects, &f.nobj, nullptr,
-                                          nullptr, nullptr, &f.summary);
-                continue;
-            }
-            f.status = sexgpu_extract(wc, src, wsrc, f.w, f.h, f.cfg, nullptr, 0, &f.nobj, nullptr, nullptr,
-                                      nullptr, &f.summary);
-            if (f.status) continue;
-            const int n = std::min(f.nobj, f.max_objects);
-            const size_t nb = (size_t)n * sizeof(sexgpu_object);
-            if (n > 0 && !grow(wc, wc->rows_host, wc->rows_bytes, nb)) {
-                f.status = SEXGPU_ERR_NOMEM;
-                continue;
-            }
-            if (n > 0) {
-                cudaError_t e = cudaMemcpyAsync(wc->rows_host, wc->rows.p, nb, cudaMemcpyDeviceToHost, wc->stream);
-                if (e == cudaSuccess) e = stream_wait(wc, wc->stream);
-                if (e != cudaSuccess) {
-                    f.status = set_err(wc, e, "catalogue copy");
-                    continue;
-                }
-                memcpy(f.objs, wc->rows_host, nb);
-            }
-            if (f.nobj > f.max_objects) f.status = SEXGPU_ERR_CAPACITY;
+            batch_one_frame(wc, frames[fi]);
+            replayed[fi] = (char)wc->last_graph;
+            entry[fi] = wc->last_entry;
         }
     };
     std::vector<std::thread> pool;
-    for (int i = 1; i < workers; i++) pool.emplace_back(run, ctx->workers[i]);
-    run(ctx->workers[0]);
+    for (int i = 1; i < workers; i++) pool.emplace_back(run, i);
+    run(0);
     for (auto &t : pool) t.join();
     sx_grid_div = 1;
     for (sexgpu_ctx *w : ctx->workers) {
@@ -1973,6 +2281,12 @@ int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframe
         w->graveyard.clear();
         w->host_graveyard.clear();
     }
+    bool all_ok = true, all_replayed = true;
+    for (int i = 0; i < nframes; i++) {
+        all_ok = all_ok && frames[i].status == SEXGPU_OK;
+        all_replayed = all_replayed && replayed[i];
+    }
+    if (ctx->graph_mode && all_ok && all_replayed) build_batch_graph(ctx, frames, nframes, wl, sig, entry);
     for (int i = 0; i < nframes; i++)
         if (frames[i].status != SEXGPU_OK) {
             ctx->err = "frame " + std::to_string(i) + " failed";

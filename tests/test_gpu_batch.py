@@ -42,8 +42,11 @@ def test_batch_with_weight_map(gpu_ctx, masks):
 
 def test_batch_through_graphs(masks):
     """The batch with the "graph" parameter: frames of a few kinds (size,
-    settings) repeated; over three batches every worker learns, captures and
-    replays its kinds, and every frame's catalogue is the plain one."""
+    settings) repeated.  Over the first batches every worker learns, captures
+    and replays its kinds; after a batch whose every frame replayed, the same
+    batch runs as one launch of the batch graph.  Every frame's catalogue is
+    the plain one each time, including the frames of a batch of new content
+    with the same kinds."""
     import sexgpu
     kinds = [((1024, 512), dict(back_size=32, conv=masks["gauss_2.0_3x3"])),
              ((512, 512), dict(back_size=64, conv=masks["gauss_3.0_7x7"])),
@@ -55,7 +58,18 @@ def test_batch_through_graphs(masks):
     with sexgpu.Context(0) as plain, sexgpu.Context(0) as ctx:
         ref = [plain.extract(img, **kw)[0] for img, kw in frames]
         ctx.set_param("graph", 1)
-        for _ in range(3):
+        launched = []
+        for _ in range(5):
             got = ctx.extract_batch(frames, workers=3)
+            launched.append(ctx.graph_stats()[0])
             for r, (cat, _) in zip(ref, got):
                 assert cat.tobytes() == r.tobytes()
+        assert launched[-1] == 1 and launched[0] == 0
+        # new frames of the same kinds: the batch graph again, new catalogues
+        frames2 = [(synth.frame_c1(seed=160 + i, w=img.shape[1], h=img.shape[0], density=5e-3), kw)
+                   for i, (img, kw) in enumerate(frames)]
+        ref2 = [plain.extract(img, **kw)[0] for img, kw in frames2]
+        got2 = ctx.extract_batch(frames2, workers=3)
+        assert ctx.graph_stats()[0] == 1
+        for r, (cat, _) in zip(ref2, got2):
+            assert cat.tobytes() == r.tobytes()
