@@ -281,7 +281,8 @@ typedef struct {
  * scanimage(); no counterpart in the reference, which handles one frame per
  * process).  The frames are taken largest first by `workers` device streams
  * of this context's device (0: 8, or what sexgpu_autotune_batch chose), each
- * with its own buffers, so that the
+ * with its own buffers (with "graph", each frame kind stays with one worker,
+ * which keeps its graph), so that the
  * stages of different frames overlap on the GPU.  Every frame's results are
  * exactly those of sexgpu_extract on that frame.  Returns SEXGPU_OK if every
  * frame succeeded, else the status of the first failed frame (each frame's
@@ -311,9 +312,9 @@ int sexgpu_autotune(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, in
 
 /* Autotuner of the batched form: times sexgpu_extract_batch on these frames
  * (host wall clock, best of reps, after one warm-up batch per candidate) with
- * 4, 8, 12 and 16 workers, then "batch_grid_div" 1, 2 and 4, and keeps the
- * fastest as this context's defaults (the worker count of a batch called
- * with workers = 0).  The frames' catalogues are compared with the first
+ * 4, 8, 12 and 16 workers, then "batch_grid_div" 1, 2 and 4, then (with
+ * "graph" set) "batch_one_launch" 0 and 1, and keeps the fastest as this
+ * context's defaults (the worker count of a batch called with workers = 0).  The frames' catalogues are compared with the first
  * candidate's (SEXGPU_ERR_MISMATCH if they differ); they hold the last run's
  * results on return.  Returns the number of candidates timed, or an error. */
 int sexgpu_autotune_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframes, int reps,
@@ -353,6 +354,12 @@ int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max);
  * context stays usable); 0 (default) keeps the built-in caps, which no valid
  * frame reaches -- it exists to test the error path.  "batch_workers": the
  * worker count of a batch called with workers = 0 (1..64, default 8).
+ * "batch_one_launch": with "graph", 1 (default) runs a batch repeated after
+ * one whose every frame replayed a graph (same frame sizes, settings and
+ * order; new pixel values allowed) as a single launch of a batch graph: the
+ * workers' chains of upload, frame graph and result copies side by side.
+ * Frames in page-locked host memory are uploaded from where they are, others
+ * through the batch's pinned buffer.  0 keeps one graph launch per frame.
  * "graph": 1 extracts
  * through captured CUDA graphs (default 0).  The first frame of a kind (frame
  * size, configuration, detection mask, input buffers and the parameters

@@ -73,3 +73,22 @@ def test_batch_through_graphs(masks):
         assert ctx.graph_stats()[0] == 1
         for r, (cat, _) in zip(ref2, got2):
             assert cat.tobytes() == r.tobytes()
+
+
+def test_batch_graph_from_pinned_frames(masks):
+    """Frames in page-locked host memory: the batch graph uploads them from
+    where they are (no staging copy); catalogues as the plain path's."""
+    import torch
+    import sexgpu
+    kw = dict(back_size=64, conv=masks["gauss_2.0_3x3"])
+    base = [synth.frame_c1(seed=170 + i, w=640, h=480, density=5e-3) for i in range(6)]
+    pinned = [torch.from_numpy(f).pin_memory() for f in base]
+    frames = [(p.numpy(), kw) for p in pinned]
+    with sexgpu.Context(0) as plain, sexgpu.Context(0) as ctx:
+        ref = [plain.extract(img, **kw)[0] for img in base]
+        ctx.set_param("graph", 1)
+        for k in range(5):
+            got = ctx.extract_batch(frames, workers=2)
+            for r, (cat, _) in zip(ref, got):
+                assert cat.tobytes() == r.tobytes()
+        assert ctx.graph_stats()[0] == 1
