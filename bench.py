@@ -416,7 +416,7 @@ def run_batch(ctx, frames, reps=5, workers=8, maxobj=400000):
 
     t_graph, identical_g, _ = graph_form(0)
     t_one, identical_one, one_stats = graph_form(1)
-    ctx.set_param("batch_one_launch", 1)
+    ctx.set_param("batch_one_launch", 0)
     ctx.set_param("graph", 0)
     npx = sum(f.size for f, _ in frames)
     return {"workload": "c3: 64 frames (16x 4096x2048, 24x 1024^2, 16x 512^2, 8x 4096^2) cut from four "

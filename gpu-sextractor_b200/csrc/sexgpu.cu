@@ -188,7 +188,7 @@ struct sexgpu_ctx {
     std::vector<sexgpu_ctx *> workers;  // contexts of sexgpu_extract_batch
     std::vector<unsigned long long> batch_kinds;  // frame kinds a batch worker has extracted
     int batch_workers = 8;  // workers of a batch called with workers = 0 (sexgpu_autotune_batch)
-    int batch_one_launch = 1;  // with graphs, a repeated batch is one launch of a batch graph
+    int batch_one_launch = 0;  // with graphs, a repeated batch is one launch of a batch graph
     // buffers outgrown during a batch: freed when the batch ends, because
     // cudaFree waits for the whole device and would stall the other workers
     bool defer_free = false;

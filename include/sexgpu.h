@@ -354,12 +354,14 @@ int sexgpu_stage_times(sexgpu_ctx *ctx, sexgpu_stage *stages, int max);
  * context stays usable); 0 (default) keeps the built-in caps, which no valid
  * frame reaches -- it exists to test the error path.  "batch_workers": the
  * worker count of a batch called with workers = 0 (1..64, default 8).
- * "batch_one_launch": with "graph", 1 (default) runs a batch repeated after
+ * "batch_one_launch": with "graph", 1 runs a batch repeated after
  * one whose every frame replayed a graph (same frame sizes, settings and
  * order; new pixel values allowed) as a single launch of a batch graph: the
  * workers' chains of upload, frame graph and result copies side by side.
  * Frames in page-locked host memory are uploaded from where they are, others
- * through the batch's pinned buffer.  0 keeps one graph launch per frame.
+ * through the batch's pinned buffer.  0 (default) keeps one graph launch per
+ * frame on the worker streams, which overlaps each frame's upload with the
+ * other workers' kernels.
  * "graph": 1 extracts
  * through captured CUDA graphs (default 0).  The first frame of a kind (frame
  * size, configuration, detection mask, input buffers and the parameters

@@ -58,6 +58,7 @@ def test_batch_through_graphs(masks):
     with sexgpu.Context(0) as plain, sexgpu.Context(0) as ctx:
         ref = [plain.extract(img, **kw)[0] for img, kw in frames]
         ctx.set_param("graph", 1)
+        ctx.set_param("batch_one_launch", 1)
         launched = []
         for _ in range(5):
             got = ctx.extract_batch(frames, workers=3)
@@ -87,8 +88,27 @@ def test_batch_graph_from_pinned_frames(masks):
     with sexgpu.Context(0) as plain, sexgpu.Context(0) as ctx:
         ref = [plain.extract(img, **kw)[0] for img in base]
         ctx.set_param("graph", 1)
+        ctx.set_param("batch_one_launch", 1)
         for k in range(5):
             got = ctx.extract_batch(frames, workers=2)
             for r, (cat, _) in zip(ref, got):
                 assert cat.tobytes() == r.tobytes()
         assert ctx.graph_stats()[0] == 1
+
+
+def test_batch_per_frame_graphs(masks):
+    """The default batch form with graphs: one graph launch per frame, each
+    kind on one worker; catalogues as the plain path's over repeated batches."""
+    import sexgpu
+    kinds = [((800, 600), dict(back_size=64, conv=masks["gauss_2.0_3x3"])),
+             ((512, 384), dict(back_size=32, conv=masks["gauss_3.0_7x7"]))]
+    frames = [(synth.frame_c1(seed=180 + i, w=kinds[i % 2][0][0], h=kinds[i % 2][0][1], density=6e-3),
+               kinds[i % 2][1]) for i in range(8)]
+    with sexgpu.Context(0) as plain, sexgpu.Context(0) as ctx:
+        ref = [plain.extract(img, **kw)[0] for img, kw in frames]
+        ctx.set_param("graph", 1)
+        for _ in range(4):
+            got = ctx.extract_batch(frames, workers=3)
+            assert ctx.graph_stats()[0] == 0
+            for r, (cat, _) in zip(ref, got):
+                assert cat.tobytes() == r.tobytes()
