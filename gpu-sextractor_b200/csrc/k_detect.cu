@@ -207,6 +207,45 @@ __device__ __forceinline__ bool sp_wait(unsigned bar, unsigned parity) {
     return done != 0;
 }
 
+// ---- union-find in shared memory (tile-local components)
+__device__ __forceinline__ int sfind(const int *L, int a) {
+    while (L[a] != a) a = L[a];
+    return a;
+}
+
+__device__ __forceinline__ void sunion(int *L, int a, int b) {
+    for (int it = 0; it < 4096; it++) {
+        a = sfind(L, a);
+        b = sfind(L, b);
+        if (a == b) return;
+        if (a < b) {
+            int t = a;
+            a = b;
+            b = t;
+        }
+        int old = atomicMin(&L[a], b);
+        if (old == a) return;
+        a = old;
+    }
+}
+
+// runs of foreground bits in a row mask
+__device__ __forceinline__ int run_start(unsigned starts, int b) {  // start bit of the run holding bit b
+    return 31 - __clz(starts & (0xffffffffu >> (31 - b)));
+}
+__device__ __forceinline__ int run_end(unsigned m, int b) {  // last bit of the run holding bit b
+    return b + __ffsll(~(unsigned long long)(m >> b)) - 2;     // 64-bit: a run may reach bit 31
+}
+
+// the same on 64-bit row masks (the subtract/filter kernel's 64-pixel tile rows)
+__device__ __forceinline__ int run_start64(unsigned long long starts, int b) {
+    return 63 - __clzll((long long)(starts & (~0ull >> (63 - b))));
+}
+__device__ __forceinline__ int run_end64(unsigned long long m, int b) {
+    const unsigned long long r = ~(m >> b);
+    return r ? b + __ffsll((long long)r) - 2 : 63;
+}
+
 template <int MW, int MH, bool WEIGHTED>
 __global__ void __launch_bounds__(ST_THREADS) k_sub_filter_pipe(const __grid_constant__ CUtensorMap tmap,
                                                                 const __grid_constant__ SpArgs A,
@@ -215,6 +254,8 @@ __global__ void __launch_bounds__(ST_THREADS) k_sub_filter_pipe(const __grid_con
     __shared__ __align__(8) unsigned long long bars[2];
     __shared__ float s_nd[ST_MAXBH][SP_NK], s_dnd[ST_MAXBH][SP_NK];
     __shared__ int s_kmin, s_nk;
+    __shared__ unsigned s_rowh[ST_TH][2];  // tile rows' foreground, two 32-bit halves
+    __shared__ int s_L[ST_TH * ST_TW];     // tile-local union-find
     const int mw = MW > 0 ? MW : A.mw, mh = MH > 0 ? MH : A.mh;
     const int rx = mw / 2, ry = mh / 2, rxa = A.rxa;
     const int bw = ST_TW + 2 * rxa, bh = ST_TH + 2 * ry;
@@ -335,23 +376,74 @@ __global__ void __launch_bounds__(ST_THREADS) k_sub_filter_pipe(const __grid_con
         else
             conv_rows_any(A.mask, tile, bw, cxo + rxa - rx, r0, mw, mh, acc);
         const int gx = x0 + cxo;
-        if (gx < w) {
+        unsigned fgb = 0u;  // bit k: pixel (cxo, r0 + k) above its threshold
 #pragma unroll
-            for (int k = 0; k < ST_RPT; k++) {
-                const int gy = y0 + r0 + k;
-                if (gy < h) {
-                    const int p = gy * w + gx;
-                    A.cd[p] = acc[k];
-                    bool fg;
-                    if (WEIGHTED) {
-                        const float v = __ldg(A.wvar + p);
-                        fg = (v < 1e30f) && acc[k] >= sx_pix_thr(A.wthr, A.dfac, v, dthresh);
-                    } else {
-                        fg = acc[k] >= dthresh;
-                    }
-                    A.lab[p] = fg ? p : -1;
-                    nabove += fg;
+        for (int k = 0; k < ST_RPT; k++) {
+            const int gy = y0 + r0 + k;
+            if (gx < w && gy < h) {
+                const int p = gy * w + gx;
+                A.cd[p] = acc[k];
+                bool fg;
+                if (WEIGHTED) {
+                    const float v = __ldg(A.wvar + p);
+                    fg = (v < 1e30f) && acc[k] >= sx_pix_thr(A.wthr, A.dfac, v, dthresh);
+                } else {
+                    fg = acc[k] >= dthresh;
                 }
+                fgb |= (unsigned)fg << k;
+                nabove += fg;
+            }
+        }
+        // Components within the tile (the first step of the CCL, done here
+        // while the tile's foreground is on chip): each tile row's foreground
+        // as 64 bits from two ballots; the pixels of a horizontal run join
+        // the run's first pixel; a run joins the runs of the row above that
+        // touch it or its diagonal ends.  Every link goes to a smaller tile
+        // index, so a tile component ends at its smallest pixel, which is
+        // written as the label of each of its pixels (global index).
+#pragma unroll
+        for (int k = 0; k < ST_RPT; k++) {
+            const unsigned m = __ballot_sync(0xffffffffu, (fgb >> k) & 1u);
+            if (lane == 0) s_rowh[r0 + k][cxo >> 5] = m;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < ST_RPT; k++) {
+            const int ty = r0 + k, t = ty * ST_TW + cxo;
+            const unsigned long long m = ((unsigned long long)s_rowh[ty][1] << 32) | s_rowh[ty][0];
+            s_L[t] = (fgb >> k) & 1u ? ty * ST_TW + run_start64(m & ~(m << 1), cxo) : -1;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < ST_RPT; k++) {
+            const int ty = r0 + k;
+            if (!((fgb >> k) & 1u) || ty == 0) continue;
+            const unsigned long long m = ((unsigned long long)s_rowh[ty][1] << 32) | s_rowh[ty][0];
+            if (!((m >> cxo) & 1ull) || (cxo > 0 && ((m >> (cxo - 1)) & 1ull))) continue;  // run starts only
+            const int e = run_end64(m, cxo);
+            const int s1 = cxo > 0 ? cxo - 1 : 0, e1 = e < 63 ? e + 1 : 63;
+            const unsigned long long dil = (e1 == 63 ? ~0ull : ((2ull << e1) - 1ull)) & ~((1ull << s1) - 1ull);
+            const unsigned long long mp = ((unsigned long long)s_rowh[ty - 1][1] << 32) | s_rowh[ty - 1][0];
+            const unsigned long long sp = mp & ~(mp << 1);
+            unsigned long long ov = mp & dil;
+            while (ov) {
+                const int b = __ffsll((long long)ov) - 1;
+                sunion(s_L, ty * ST_TW + cxo, (ty - 1) * ST_TW + run_start64(sp, b));
+                const int eb = run_end64(mp, b);
+                ov = eb >= 63 ? 0ull : ov & ~((2ull << eb) - 1ull);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < ST_RPT; k++) {
+            const int gy = y0 + r0 + k;
+            if (gx < w && gy < h) {
+                int l = -1;
+                if ((fgb >> k) & 1u) {
+                    const int r = sfind(s_L, (r0 + k) * ST_TW + cxo);
+                    l = (y0 + r / ST_TW) * w + x0 + r % ST_TW;
+                }
+                A.lab[gy * w + gx] = l;
             }
         }
         __syncthreads();
@@ -404,7 +496,10 @@ static bool make_frame_tmap(CUtensorMap *m, const float *img, int w, int h, int 
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const BackBufs &B, const FrameParams &P,
+// Returns true when the labels written are already tile-local components
+// (the subtract/filter pipeline's 64 x 32 tiles), false when they are seeds
+// (every foreground pixel its own label).
+bool launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const BackBufs &B, const FrameParams &P,
                        FrameScalars *d_sc, const float *d_var, const ConvMask &M, cudaStream_t st, int &launches) {
     const int mw = M.mw, mh = M.mh;
     const int rxa = ((mw / 2) + 3) & ~3;  // halo width rounded up to 16 bytes
@@ -483,7 +578,7 @@ void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const 
 #undef SP_MASK
 #undef SP_LAUNCH
         launches += 1;
-        return;
+        return true;
     }
     dim3 grid((P.w + SF_TW - 1) / SF_TW, (P.h + SF_TH - 1) / SF_TH);
     dim3 block(SF_TX, SF_TY);
@@ -491,6 +586,7 @@ void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const 
     k_sub_filter<<<grid, block, smem, st>>>(img, sub, cd, lab, B, P.w, P.h, P.nbx, P.back_type, M.dev, mw, mh, d_var,
                                             P.wthr, P.detect_thresh, d_sc);
     launches += 1;
+    return false;
 }
 
 // ---------------------------------------------------------------------------
@@ -498,40 +594,13 @@ void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const 
 // ---------------------------------------------------------------------------
 constexpr int CC_TW = 32, CC_TH = 16;
 
-__device__ __forceinline__ int sfind(const int *L, int a) {
-    while (L[a] != a) a = L[a];
-    return a;
-}
-
-__device__ __forceinline__ void sunion(int *L, int a, int b) {
-    for (int it = 0; it < 4096; it++) {
-        a = sfind(L, a);
-        b = sfind(L, b);
-        if (a == b) return;
-        if (a < b) {
-            int t = a;
-            a = b;
-            b = t;
-        }
-        int old = atomicMin(&L[a], b);
-        if (old == a) return;
-        a = old;
-    }
-}
-
-// Labels within one 32 x CC_TH tile, one warp per tile row.  A row's
-// foreground is one ballot; pixels of a horizontal run are connected
-// through the run's first pixel (bit arithmetic, no unions); a run joins the
-// runs of the row above that touch it or its two diagonal ends (8-connected)
-// with one union each, in shared memory.  Every link goes to a smaller tile
-// index, so each tile component ends at its smallest pixel.
-__device__ __forceinline__ int run_start(unsigned starts, int b) {  // start bit of the run holding bit b
-    return 31 - __clz(starts & (0xffffffffu >> (31 - b)));
-}
-__device__ __forceinline__ int run_end(unsigned m, int b) {  // last bit of the run holding bit b
-    return b + __ffsll(~(unsigned long long)(m >> b)) - 2;     // 64-bit: a run may reach bit 31
-}
-
+// Labels within one 32 x CC_TH tile, one warp per tile row (frames that the
+// subtract/filter kernel could not label itself).  A row's foreground is one
+// ballot; pixels of a horizontal run are connected through the run's first
+// pixel (bit arithmetic, no unions); a run joins the runs of the row above
+// that touch it or its two diagonal ends (8-connected) with one union each,
+// in shared memory.  Every link goes to a smaller tile index, so each tile
+// component ends at its smallest pixel.
 __global__ void __launch_bounds__(CC_TW *CC_TH) k_ccl_local(int *__restrict__ lab, int w, int h) {
     __shared__ int L[CC_TH * CC_TW];
     __shared__ unsigned rowm[CC_TH];
@@ -598,20 +667,21 @@ __device__ __forceinline__ void gunion(int *L, int a, int b, int *status, int lo
     atomicOr(status, SX_ST_LOOP);
 }
 
-// unions across tile borders: pixels on the first row or first/last column
-// of a tile look at their backward neighbours in other tiles
+// unions across tile borders (TW x TH tiles): pixels on the first row or
+// first/last column of a tile look at their backward neighbours in other tiles
+template <int TW, int TH>
 __global__ void k_ccl_border(int *__restrict__ lab, int w, int h, int *status, int loop_cap) {
-    int tilesx = (w + CC_TW - 1) / CC_TW;
-    int tile = blockIdx.x, k = threadIdx.x;           // k < CC_TW + CC_TH
-    int tx0 = (tile % tilesx) * CC_TW, ty0 = (tile / tilesx) * CC_TH;
+    int tilesx = (w + TW - 1) / TW;
+    int tile = blockIdx.x, k = threadIdx.x;           // k < TW + TH
+    int tx0 = (tile % tilesx) * TW, ty0 = (tile / tilesx) * TH;
     int x, y;
-    if (k < CC_TW) {
+    if (k < TW) {
         x = tx0 + k;
         y = ty0;
     } else {
         x = tx0;
-        y = ty0 + (k - CC_TW) + 1;
-        if (k - CC_TW + 1 >= CC_TH) return;
+        y = ty0 + (k - TW) + 1;
+        if (k - TW + 1 >= TH) return;
     }
     if (x >= w || y >= h) return;
     int p = y * w + x;
@@ -622,16 +692,17 @@ __global__ void k_ccl_border(int *__restrict__ lab, int w, int h, int *status, i
         // NW: other tile when x or y is on the tile's first column/row
         if (x > 0 && (x == tx0 || y == ty0) && lab[p - w - 1] >= 0) gunion(lab, p, p - w - 1, status, loop_cap);
         if (y == ty0 && lab[p - w] >= 0) gunion(lab, p, p - w, status, loop_cap);
-        if (x < w - 1 && (y == ty0 || x == tx0 + CC_TW - 1) && lab[p - w + 1] >= 0) gunion(lab, p, p - w + 1, status, loop_cap);
+        if (x < w - 1 && (y == ty0 || x == tx0 + TW - 1) && lab[p - w + 1] >= 0) gunion(lab, p, p - w + 1, status, loop_cap);
     }
 }
 
 // the last column of each tile also looks NE into the next tile (row y-1)
+template <int TW, int TH>
 __global__ void k_ccl_border_ne(int *__restrict__ lab, int w, int h, int *status, int loop_cap) {
-    int tilesx = (w + CC_TW - 1) / CC_TW;
-    int tile = blockIdx.x, k = threadIdx.x;  // k in [1, CC_TH)
-    if (k == 0 || k >= CC_TH) return;
-    int x = (tile % tilesx) * CC_TW + CC_TW - 1, y = (tile / tilesx) * CC_TH + k;
+    int tilesx = (w + TW - 1) / TW;
+    int tile = blockIdx.x, k = threadIdx.x;  // k in [1, TH)
+    if (k == 0 || k >= TH) return;
+    int x = (tile % tilesx) * TW + TW - 1, y = (tile / tilesx) * TH + k;
     if (x >= w - 1 || y >= h) return;
     int p = y * w + x;
     if (lab[p] >= 0 && lab[p - w + 1] >= 0) gunion(lab, p, p - w + 1, status, loop_cap);
@@ -654,16 +725,27 @@ __global__ void k_ccl_flatten(int *__restrict__ lab, long long n, int *__restric
 }
 
 // cnt: zeroed, w*h ints; receives the size of every component at its root
-void launch_ccl(int *lab, int *cnt, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st, int &launches) {
-    dim3 grid((P.w + CC_TW - 1) / CC_TW, (P.h + CC_TH - 1) / CC_TH);
-    k_ccl_local<<<grid, dim3(CC_TW, CC_TH), 0, st>>>(lab, P.w, P.h);
-    int ntiles = grid.x * grid.y;
+// tiled: the labels are already the tile-local components of the
+// subtract/filter pipeline's ST_TW x ST_TH tiles (else seeds, labelled here
+// in CC_TW x CC_TH tiles first)
+void launch_ccl(int *lab, int *cnt, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st, int &launches,
+                bool tiled) {
     int *status = &d_sc->status;
-    k_ccl_border<<<ntiles, CC_TW + CC_TH, 0, st>>>(lab, P.w, P.h, status, P.loop_cap);
-    k_ccl_border_ne<<<ntiles, CC_TH, 0, st>>>(lab, P.w, P.h, status, P.loop_cap);
+    if (tiled) {
+        const int ntiles = ((P.w + ST_TW - 1) / ST_TW) * ((P.h + ST_TH - 1) / ST_TH);
+        k_ccl_border<ST_TW, ST_TH><<<ntiles, ST_TW + ST_TH, 0, st>>>(lab, P.w, P.h, status, P.loop_cap);
+        k_ccl_border_ne<ST_TW, ST_TH><<<ntiles, ST_TH, 0, st>>>(lab, P.w, P.h, status, P.loop_cap);
+        launches += 3;
+    } else {
+        dim3 grid((P.w + CC_TW - 1) / CC_TW, (P.h + CC_TH - 1) / CC_TH);
+        k_ccl_local<<<grid, dim3(CC_TW, CC_TH), 0, st>>>(lab, P.w, P.h);
+        const int ntiles = grid.x * grid.y;
+        k_ccl_border<CC_TW, CC_TH><<<ntiles, CC_TW + CC_TH, 0, st>>>(lab, P.w, P.h, status, P.loop_cap);
+        k_ccl_border_ne<CC_TW, CC_TH><<<ntiles, CC_TH, 0, st>>>(lab, P.w, P.h, status, P.loop_cap);
+        launches += 4;
+    }
     long long n = (long long)P.w * P.h;
     k_ccl_flatten<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(lab, n, cnt, status, P.loop_cap);
-    launches += 4;
 }
 
 }  // namespace sx

@@ -130,11 +130,12 @@ struct ConvMask {
     int mw, mh;
 };
 
-void launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const BackBufs &B,
+bool launch_sub_filter(const float *img, float *sub, float *cd, int *lab, const BackBufs &B,
                        const FrameParams &P, FrameScalars *d_sc, const float *d_var, const ConvMask &M,
                        cudaStream_t st, int &launches);
 
-void launch_ccl(int *lab, int *cnt, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st, int &launches);
+void launch_ccl(int *lab, int *cnt, const FrameParams &P, FrameScalars *d_sc, cudaStream_t st, int &launches,
+                bool tiled);
 
 struct DebArgs {
     const float *cd, *sub;

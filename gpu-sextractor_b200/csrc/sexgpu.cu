@@ -686,14 +686,14 @@ int pipe_detect(sexgpu_ctx *ctx) {
     FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
     int *tmp = P<int>(ctx->scan_tmp);
     int rc = SEXGPU_OK, nl = 0;
-    launch_sub_filter(d_img, P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm, d_sc, ps.wvar,
+    const bool tiled = launch_sub_filter(d_img, P<float>(ctx->sub), P<float>(ctx->cd), P<int>(ctx->lab), B, Pm, d_sc, ps.wvar,
                       ctx->cmask, st, nl);
     stage_mark(ctx, "sub_filter", nl);
 
     nl = 0;
     int *lab = P<int>(ctx->lab), *cnt = P<int>(ctx->cnt), *flag = P<int>(ctx->flag), *pos = P<int>(ctx->pos);
     CK(cudaMemsetAsync(cnt, 0, N * 4, st));
-    launch_ccl(lab, cnt, Pm, d_sc, st, nl);  // labels to roots, component sizes at the roots
+    launch_ccl(lab, cnt, Pm, d_sc, st, nl, tiled);  // labels to roots, component sizes at the roots
     stage_mark(ctx, "ccl", nl);
 
     // ---- raw objects
