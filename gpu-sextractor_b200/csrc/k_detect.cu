@@ -247,7 +247,7 @@ __device__ __forceinline__ int run_end64(unsigned long long m, int b) {
 }
 
 template <int MW, int MH, bool WEIGHTED>
-__global__ void __launch_bounds__(ST_THREADS) k_sub_filter_pipe(const __grid_constant__ CUtensorMap tmap,
+__global__ void __launch_bounds__(ST_THREADS, 4) k_sub_filter_pipe(const __grid_constant__ CUtensorMap tmap,
                                                                 const __grid_constant__ SpArgs A,
                                                                 const __grid_constant__ ConvTaps taps) {
     extern __shared__ __align__(128) float sp_smem[];
