@@ -469,12 +469,14 @@ __device__ __forceinline__ void dl_assign_root(const DebArgs &A, const int r, un
     unsigned char *kl = reinterpret_cast<unsigned char *>(kidx + cap);
     int *status = &A.sc->status;
 
-    block_thresholds(A, A.R.dthresh[r], fdpeak, thr);
     // one kept branch that is the whole object at level 0 (nothing split
-    // off): every pixel is its own, in list order
+    // off): every pixel is its own, in list order; of the thresholds only
+    // the lowest (the object's own) is used
     const bool whole = K == 1 && (kept[0] >> 32) == 0;
+    if (!whole) block_thresholds(A, A.R.dthresh[r], fdpeak, thr);
     if (whole) {
         if (tid == 0) {
+            thr[0] = A.R.dthresh[r];
             kept2[0] = kept[0];
             bcnt[0] = P;
             bstart[0] = 0;

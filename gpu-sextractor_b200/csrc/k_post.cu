@@ -534,21 +534,14 @@ __device__ __forceinline__ void kron_range(const EndArgs &A, int o, double mx, d
 // kron_range with the exact sums in double bins (see BinSum): the hints are
 // the object's peak (and, for pass 1's r*pix, the ellipse's largest r).
 // Returns false in every lane when any lane met a term outside the bins; the
-// caller then sums with kron_range.
-template <int PASS, bool WV>
+// caller then sums with kron_range.  Pass 2 with a variance map is not binned.
+template <int PASS>
 __device__ __forceinline__ bool kron_range_bin(const EndArgs &A, int o, double mx, double my, const KronGeo &g,
                                                int i0, int i1, int step, KronAcc &out) {
     const int w = A.w, h = A.h, bw = g.xmax - g.xmin;
     const FastDiv bd = make_fastdiv_dev((unsigned)bw);
     const int corrflag = (A.mask_type == 2);
     const int top1 = bs_order(A.O.peak[o]), top0 = top1 + bs_order(sqrtf(g.klim2)) + 1;
-    // pass 2's variances: hint from the variance at the object's centre (the
-    // map varies smoothly)
-    int topv = 0;
-    if (PASS == 2 && WV) {
-        const int cx = min(max((int)(mx + 0.5), 0), w - 1), cy = min(max((int)(my + 0.5), 0), h - 1);
-        topv = bs_order(A.wvar[(size_t)cy * w + cx]) + 2;
-    }
     BinSum b0, b1;
     bs_init(b0);
     bs_init(b1);
@@ -573,27 +566,22 @@ __device__ __forceinline__ bool kron_range_bin(const EndArgs &A, int o, double m
             area++;
             float pix = A.sub[(size_t)y * w + x];
             int t = A.alloc[(size_t)y * w + x];
-            float pvar = WV ? A.wvar[(size_t)y * w + x] : 0.0f;
             if ((t >= 0 && t != o) || pix <= -SX_BIG) {
                 areab++;
                 int x2, y2;
                 if (corrflag && (x2 = (int)(2 * mx + 0.49999 - x)) >= 0 && x2 < w &&
                     (y2 = (int)(2 * my + 0.49999 - y)) >= 0 && y2 < h &&
-                    ((t = A.alloc[(size_t)y2 * w + x2]) == -1 || t == o) && A.sub[(size_t)y2 * w + x2] > -SX_BIG) {
+                    ((t = A.alloc[(size_t)y2 * w + x2]) == -1 || t == o) && A.sub[(size_t)y2 * w + x2] > -SX_BIG)
                     pix = A.sub[(size_t)y2 * w + x2];
-                    if (WV) pvar = A.wvar[(size_t)y2 * w + x2];
-                } else {
+                else
                     pix = 0.0;
-                    pvar = 0.0f;
-                }
             }
             ok &= bs_add(b0, pix, top1);
-            if (WV) ok &= bs_add(b1, pvar, topv);
         }
     }
     if (!__all_sync(0xffffffffu, ok)) return false;
     out.s0 = bs_to_xsum(bs_warp_sum(b0));
-    if (PASS == 1 || WV)
+    if (PASS == 1)
         out.s1 = bs_to_xsum(bs_warp_sum(b1));
     else
         xs_init(out.s1);
@@ -607,10 +595,8 @@ template <int PASS>
 __device__ __forceinline__ void kron_warp_sums(const EndArgs &A, int o, double mx, double my, const KronGeo &g,
                                                int i0, int i1, int step, KronAcc &c) {
     // at most BS_MAX_TERMS terms of the warp per bin
-    const bool binned = (long long)(i1 - (i0 & ~31)) <= (long long)BS_MAX_TERMS * step / 32;
-    if (binned && (PASS == 2 && A.wvar ? kron_range_bin<PASS, true>(A, o, mx, my, g, i0, i1, step, c)
-                                       : kron_range_bin<PASS, false>(A, o, mx, my, g, i0, i1, step, c)))
-        return;
+    const bool binned = (PASS == 1 || !A.wvar) && (long long)(i1 - (i0 & ~31)) <= (long long)BS_MAX_TERMS * step / 32;
+    if (binned && kron_range_bin<PASS>(A, o, mx, my, g, i0, i1, step, c)) return;
     kacc_init(c);
     kron_range<PASS>(A, o, mx, my, g, i0, i1, step, c);
     kacc_warp(c);
