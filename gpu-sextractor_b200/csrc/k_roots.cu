@@ -31,15 +31,31 @@ __global__ void k_root_thresholds(const int *__restrict__ lab, const int *__rest
                                   const int *__restrict__ rid, long long n, int minarea, const float *__restrict__ wvar,
                                   int wthr, double dfac, double afac, FrameScalars *sc, int *rdthr, int *rathr) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    const int l = lab[p];
-    if (l < 0 || cnt[l] < minarea) return;
-    const int r = rid[l];
-    const float v = wvar ? __ldg(wvar + p) : 0.0f;
-    const float dt = sx_pix_thr(wthr, dfac, v, sc->dthresh), at = sx_pix_thr(wthr, afac, v, sc->thresh);
-    atomicMin(rdthr + r, __float_as_int(dt));
-    atomicMin(rathr + r, __float_as_int(at));
-    atomicMin(&sc->e0cd, fexpo(dt));
+    int r = -1, idt = 0x7fffffff, iat = 0x7fffffff, e = 0x7fffffff;
+    if (p < n) {
+        const int l = lab[p];
+        if (l >= 0 && cnt[l] >= minarea) {
+            r = rid[l];
+            const float v = wvar ? __ldg(wvar + p) : 0.0f;
+            const float dt = sx_pix_thr(wthr, dfac, v, sc->dthresh), at = sx_pix_thr(wthr, afac, v, sc->thresh);
+            idt = __float_as_int(dt);
+            iat = __float_as_int(at);
+            e = fexpo(dt);
+        }
+    }
+    // the minima are taken in the warp first (neighbouring pixels mostly
+    // share their raw object), then one atomic per raw object and warp
+    e = __reduce_min_sync(0xffffffffu, e);
+    if ((threadIdx.x & 31) == 0 && e != 0x7fffffff) atomicMin(&sc->e0cd, e);
+    const unsigned grp = __match_any_sync(0xffffffffu, r);
+    if (r >= 0) {
+        idt = __reduce_min_sync(grp, idt);
+        iat = __reduce_min_sync(grp, iat);
+        if ((int)(threadIdx.x & 31) == __ffs(grp) - 1) {
+            atomicMin(rdthr + r, idt);
+            atomicMin(rathr + r, iat);
+        }
+    }
 }
 
 // without a weight map every raw object has the global thresholds
