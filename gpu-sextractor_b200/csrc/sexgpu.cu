@@ -140,6 +140,13 @@ struct sexgpu_ctx {
     std::string err;
     // frame-size buffers
     DevBuf img, sub, cd, lab, cnt, flag, pos, alloc, seg, pos2idx, var, imgm, wvar, wratio;
+    // frame streaming (sexgpu_stream_*): two input slots uploaded on a copy stream
+    DevBuf qimg[2], qvar[2];
+    int qw[2] = {0, 0}, qh[2] = {0, 0};
+    bool qhasvar[2] = {false, false};
+    int qhead = 0, qcount = 0;
+    cudaStream_t qstream = nullptr;
+    cudaEvent_t qev[2] = {nullptr, nullptr};
     // scan / sort scratch
     DevBuf scan_tmp, keys, vals, kalt, valt;
     // background
@@ -1530,6 +1537,12 @@ int sexgpu_destroy(sexgpu_ctx *ctx) {
     if (ctx->ev_block) cudaEventDestroy(ctx->ev_block);
     free_batch_graph(ctx);
     for (GraphEntry &e : ctx->graphs) drop_graph(ctx, e);
+    for (int i = 0; i < 2; i++) {
+        free_buf(ctx->qimg[i]);
+        free_buf(ctx->qvar[i]);
+        if (ctx->qev[i]) cudaEventDestroy(ctx->qev[i]);
+    }
+    if (ctx->qstream) cudaStreamDestroy(ctx->qstream);
     ctx->graphs.clear();
     if (ctx->hsc_pin) cudaFreeHost(ctx->hsc_pin);
     for (sexgpu_ctx *w : ctx->workers) sexgpu_destroy(w);
@@ -1642,6 +1655,52 @@ int sexgpu_extract(sexgpu_ctx *ctx, const float *img, const float *var, int w, i
     int rc = sexgpu_extract_device(ctx, P<float>(ctx->img), var ? P<float>(ctx->var) : nullptr, w, h, cfg, sum);
     if (rc) return rc;
     return sexgpu_copy_results(ctx, objs, max_objects, nobj, segmap, sub, cd);
+}
+
+int sexgpu_stream_submit(sexgpu_ctx *ctx, const float *img, const float *var, int w, int h) {
+    if (!ctx || !img || w <= 0 || h <= 0 || (long long)w * h >= (1ll << 31)) return SEXGPU_ERR_ARG;
+    if (ctx->qcount >= 2) {
+        ctx->err = "two frames are queued already";
+        return SEXGPU_ERR_CAPACITY;
+    }
+    cudaSetDevice(ctx->device);
+    if (!ctx->qstream) {
+        CK(cudaStreamCreateWithFlags(&ctx->qstream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; i++) CK(cudaEventCreateWithFlags(&ctx->qev[i], cudaEventDisableTiming));
+    }
+    const int slot = (ctx->qhead + ctx->qcount) & 1;
+    const long long N = (long long)w * h;
+    EN(qimg[slot], N * 4);
+    CK(cudaMemcpyAsync(ctx->qimg[slot].p, img, N * 4, cudaMemcpyHostToDevice, ctx->qstream));
+    if (var) {
+        EN(qvar[slot], N * 4);
+        CK(cudaMemcpyAsync(ctx->qvar[slot].p, var, N * 4, cudaMemcpyHostToDevice, ctx->qstream));
+    }
+    CK(cudaEventRecord(ctx->qev[slot], ctx->qstream));
+    ctx->qw[slot] = w;
+    ctx->qh[slot] = h;
+    ctx->qhasvar[slot] = var != nullptr;
+    ctx->qcount++;
+    return SEXGPU_OK;
+}
+
+int sexgpu_stream_next(sexgpu_ctx *ctx, const sexgpu_config *cfg, sexgpu_object *objs, int max_objects, int *nobj,
+                       sexgpu_summary *sum) {
+    if (!ctx || !cfg) return SEXGPU_ERR_ARG;
+    if (ctx->qcount == 0) {
+        ctx->err = "no frame is queued";
+        return SEXGPU_ERR_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    const int slot = ctx->qhead;
+    ctx->qhead ^= 1;
+    ctx->qcount--;
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->qev[slot], 0));
+    int rc = sexgpu_extract_device(ctx, P<float>(ctx->qimg[slot]),
+                                   ctx->qhasvar[slot] ? P<float>(ctx->qvar[slot]) : nullptr, ctx->qw[slot],
+                                   ctx->qh[slot], cfg, sum);
+    if (rc) return rc;
+    return sexgpu_copy_results(ctx, objs, max_objects, nobj, nullptr, nullptr, nullptr);
 }
 
 int sexgpu_extract_fits(sexgpu_ctx *ctx, const void *data, const sexgpu_fits_format *fmt, const float *var, int w,

@@ -129,7 +129,8 @@ EXPORTS = ["sexgpu_create", "sexgpu_destroy", "sexgpu_set_stream", "sexgpu_extra
            "sexgpu_getconv", "sexgpu_default_config", "sexgpu_last_error", "sexgpu_stage_times", "sexgpu_set_param",
            "sexgpu_read_nnw", "sexgpu_set_nnw", "sexgpu_extract_fits", "sexgpu_background_rms",
            "sexgpu_background_noalloc", "sexgpu_background_meshes", "sexgpu_background_map", "sexgpu_copy_apertures",
-           "sexgpu_extract_batch", "sexgpu_graph_stats", "sexgpu_autotune", "sexgpu_autotune_batch"]
+           "sexgpu_extract_batch", "sexgpu_graph_stats", "sexgpu_autotune", "sexgpu_autotune_batch",
+           "sexgpu_stream_submit", "sexgpu_stream_next"]
 
 _lib = None
 
@@ -401,6 +402,34 @@ class Context:
     def set_param(self, name, value):
         """Execution parameter (results do not depend on it), e.g. kron_warp_max."""
         _check(lib().sexgpu_set_param(self.h, name.encode(), int(value)), self.h, "sexgpu_set_param")
+
+    def stream_submit(self, img, weight=None):
+        """Queue a frame (sexgpu_stream_submit); its upload starts at once.  The
+        array is kept alive until its catalogue has been returned."""
+        img = np.ascontiguousarray(img, np.float32)
+        wmap = np.ascontiguousarray(weight, np.float32) if weight is not None else None
+        h, w = img.shape
+        _check(lib().sexgpu_stream_submit(self.h, _f(img), _f(wmap) if wmap is not None else None, w, h), self.h,
+               "sexgpu_stream_submit")
+        if not hasattr(self, "_queued"):
+            self._queued = []
+        self._queued.append((img, wmap))
+
+    def stream_next(self, max_objects=None, **kw):
+        """Extract the oldest queued frame (sexgpu_stream_next): (catalogue, summary)."""
+        cfg = make_config(**kw)
+        img = self._queued[0][0] if getattr(self, "_queued", None) else None
+        if max_objects is None:
+            max_objects = (img.size // max(1, cfg.detect_minarea) // 2 + 16) if img is not None else 16
+        objs = np.zeros(max_objects, OBJECT_DTYPE)
+        n = C.c_int()
+        s = Summary()
+        rc = lib().sexgpu_stream_next(self.h, C.byref(cfg), objs.ctypes.data_as(C.c_void_p), max_objects,
+                                      C.byref(n), C.byref(s))
+        if getattr(self, "_queued", None):
+            self._queued.pop(0)
+        _check(rc, self.h, "sexgpu_stream_next")
+        return objs[:n.value], s
 
     def graph_stats(self):
         """(replayed, kernels, kinds) of the last extraction (sexgpu_graph_stats)."""

@@ -290,6 +290,20 @@ typedef struct {
  * two threads at once. */
 int sexgpu_extract_batch(sexgpu_ctx *ctx, sexgpu_batch_frame *frames, int nframes, int workers);
 
+/* Frame streaming, for pipelines that extract frame after frame: the upload
+ * of the next frame overlaps the extraction of the current one.
+ * sexgpu_stream_submit queues a host frame (and weight map, or NULL) and
+ * starts its upload on a copy stream of the context; it returns without
+ * waiting.  sexgpu_stream_next extracts the oldest queued frame with cfg and
+ * returns its catalogue as sexgpu_extract does (no maps).  At most two frames
+ * are queued (SEXGPU_ERR_CAPACITY beyond).  A queued frame's host memory
+ * must stay unchanged until sexgpu_stream_next has returned its catalogue.
+ * The uploads overlap only from page-locked host memory; pageable frames are
+ * copied before sexgpu_stream_submit returns. */
+int sexgpu_stream_submit(sexgpu_ctx *ctx, const float *img, const float *var, int w, int h);
+int sexgpu_stream_next(sexgpu_ctx *ctx, const sexgpu_config *cfg, sexgpu_object *objs, int max_objects,
+                       int *nobj, sexgpu_summary *sum);
+
 /* One timed candidate of the autotuners. */
 typedef struct {
     char    param[24];          /* execution parameter (see sexgpu_set_param) */
