@@ -65,10 +65,11 @@ struct PipeState {
     // device only (k_gate stands in for the host checks between stages)
     bool capf = false;
     int cap_roots = 0, cap_rootpix = 0, cap_obj = 0;
-    // while the stages are captured: pinned host memory that the frame's
-    // constants (column tables, mask) are copied from, so that the graph holds
-    // its own uploads (8 w + 4 SX_MAXCONV^2 bytes)
-    unsigned char *pin = nullptr;
+    // while the stages are captured: device memory already holding the
+    // frame's constants (column tables, then the mask: 8 w + 4 SX_MAXCONV^2
+    // bytes), so that the graph has no host-to-device copies, which would
+    // queue behind a concurrent frame upload on the copy engine
+    unsigned char *cst = nullptr;
     BackBufs B;
     RootBufs R;
     DebArgs A;
@@ -91,7 +92,7 @@ struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;   // the captured graph (child node of a batch graph)
     unsigned long long id = 0;     // unique within the context
-    unsigned char *pin = nullptr;  // pinned constants the graph uploads (PipeState::pin)
+    unsigned char *cst = nullptr;  // device copy of the frame's constants (PipeState::cst)
     PipeState ps;                  // host state of the captured frame, restored on replay
     ObjBufs O;
     unsigned long long gen = 0;  // allocation generation the graph's pointers belong to
@@ -442,14 +443,13 @@ int load_mask(sexgpu_ctx *ctx, const float *mask, int mw, int mh) {
     }
     ctx->hmask.assign(mask, mask + (size_t)mw * mh);
     EN(dmask, sizeof(float) * SX_MAXCONV * SX_MAXCONV);
-    const float *src = ctx->hmask.data();
-    if (ctx->ps.pin) {  // being captured: upload from the graph's pinned copy
-        float *pm = reinterpret_cast<float *>(ctx->ps.pin + (size_t)8 * ctx->ps.w);
-        memcpy(pm, src, sizeof(float) * mw * mh);
-        src = pm;
+    if (ctx->ps.cst) {  // being captured: the graph's device copy
+        ctx->cmask.dev = reinterpret_cast<const float *>(ctx->ps.cst + (size_t)8 * ctx->ps.w);
+    } else {
+        CK(cudaMemcpyAsync(ctx->dmask.p, ctx->hmask.data(), sizeof(float) * mw * mh, cudaMemcpyHostToDevice,
+                           ctx->stream));
+        ctx->cmask.dev = P<float>(ctx->dmask);
     }
-    CK(cudaMemcpyAsync(ctx->dmask.p, src, sizeof(float) * mw * mh, cudaMemcpyHostToDevice, ctx->stream));
-    ctx->cmask.dev = P<float>(ctx->dmask);
     ctx->cmask.host = ctx->hmask.data();
     ctx->cmask.mw = mw;
     ctx->cmask.mh = mh;
@@ -625,16 +625,14 @@ int pipe_begin(sexgpu_ctx *ctx, const float *d_img, const float *d_wmap, int w, 
     FrameScalars *d_sc = P<FrameScalars>(ctx->sc);
     int *tmp = P<int>(ctx->scan_tmp);
 
-    column_table(w, Pm.nbx, Pm.bw, ctx->colk_h, ctx->coldx_h);
-    const void *src_k = ctx->colk_h.data(), *src_dx = ctx->coldx_h.data();
-    if (ps.pin) {  // being captured: upload from the graph's pinned copy
-        memcpy(ps.pin, src_k, (size_t)w * 4);
-        memcpy(ps.pin + (size_t)w * 4, src_dx, (size_t)w * 4);
-        src_k = ps.pin;
-        src_dx = ps.pin + (size_t)w * 4;
+    if (ps.cst) {  // being captured: the graph's device copy
+        B.colk = reinterpret_cast<int *>(ps.cst);
+        B.coldx = reinterpret_cast<float *>(ps.cst + (size_t)w * 4);
+    } else {
+        column_table(w, Pm.nbx, Pm.bw, ctx->colk_h, ctx->coldx_h);
+        CK(cudaMemcpyAsync(B.colk, ctx->colk_h.data(), w * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(B.coldx, ctx->coldx_h.data(), w * 4, cudaMemcpyHostToDevice, st));
     }
-    CK(cudaMemcpyAsync(B.colk, src_k, w * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(B.coldx, src_dx, w * 4, cudaMemcpyHostToDevice, st));
     rc = load_mask(ctx, cfg->filter_flag ? cfg->conv : nullptr, cfg->conv_w, cfg->conv_h);
     if (rc) return rc;
 
@@ -1229,10 +1227,10 @@ void drop_graph(sexgpu_ctx *ctx, GraphEntry &e) {
     if (e.exec || e.graph) ctx->graph_epoch++;
     if (e.exec) cudaGraphExecDestroy(e.exec);
     if (e.graph) cudaGraphDestroy(e.graph);
-    if (e.pin) cudaFreeHost(e.pin);
+    if (e.cst) cudaFree(e.cst);
     e.exec = nullptr;
     e.graph = nullptr;
-    e.pin = nullptr;
+    e.cst = nullptr;
 }
 
 // status of a capacity-form frame from its scalars: 1 when it must be
@@ -1271,16 +1269,32 @@ void capture_graph(sexgpu_ctx *ctx, GraphEntry &e, const float *d_img, const flo
                    const sexgpu_config *cfg) {
     PipeState &ps = ctx->ps;
     cudaStream_t st = ctx->stream;
-    if (!e.pin && cudaMallocHost((void **)&e.pin, (size_t)8 * w + 4 * SX_MAXCONV * SX_MAXCONV) != cudaSuccess) {
+    // the frame's constants into the entry's own device memory before the
+    // capture; the graph reads them there
+    if (!e.cst && cudaMalloc((void **)&e.cst, (size_t)8 * w + 4 * SX_MAXCONV * SX_MAXCONV) != cudaSuccess) {
         cudaGetLastError();
-        e.pin = nullptr;
+        e.cst = nullptr;
         e.no_graph = true;
         return;
+    }
+    {
+        std::vector<int> ck;
+        std::vector<float> cdx;
+        column_table(w, e.Pm.nbx, e.Pm.bw, ck, cdx);
+        const float *m = e.mask.data();
+        const size_t mbytes = sizeof(float) * e.mask.size();
+        if (cudaMemcpy(e.cst, ck.data(), (size_t)w * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(e.cst + (size_t)w * 4, cdx.data(), (size_t)w * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(e.cst + (size_t)8 * w, m, mbytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaGetLastError();
+            e.no_graph = true;
+            return;
+        }
     }
     const unsigned long long gen0 = ctx->gen;
     cudaGraph_t g = nullptr;
     ps.capf = true;
-    ps.pin = e.pin;
+    ps.cst = e.cst;
     set_caps(ps, e);
     int rc = SEXGPU_ERR_CUDA;
     cudaError_t ce = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
@@ -1289,7 +1303,7 @@ void capture_graph(sexgpu_ctx *ctx, GraphEntry &e, const float *d_img, const flo
         ce = cudaStreamEndCapture(st, &g);
     }
     ps.capf = false;
-    ps.pin = nullptr;
+    ps.cst = nullptr;
     if (ce == cudaSuccess && rc == SEXGPU_OK && g && ctx->gen == gen0) {
         size_t n = 0;
         if (cudaGraphGetNodes(g, nullptr, &n) == cudaSuccess) {
