@@ -105,34 +105,58 @@ __global__ void k_mesh_stat(const float *__restrict__ img, int w, int h, int bw,
 // copies and an odd stride.
 constexpr int BAND_STAGES = 4;
 
+// Copy c of a row (c = lane, lane + 32, ...; float4s when VEC, else floats)
+// is element r of mesh j, c = j q + r with q the copies per mesh row; (j0, r0)
+// is the lane's first and (dj, dr) the step of 32 copies, so no division is
+// needed per copy.
+struct BandCopy {
+    int q, j0, r0, dj, dr;
+};
+
 template <bool VEC>
-__device__ __forceinline__ void band_row_async(float *dst, const float *img, int w, int gy, int x0, int bw, int tw,
-                                               int stride) {
+__device__ __forceinline__ void band_row_async(float *dst, const float *img, int w, int gy, int x0, int tw,
+                                               int stride, const BandCopy &bc) {
     const int lane = threadIdx.x & 31;
     const float *src = img + (size_t)gy * w + x0;
+    int j = bc.j0, r = bc.r0;
     if (VEC) {
         for (int c = lane; 4 * c < tw; c += 32) {
-            const int j = (4 * c) / bw;
-            const unsigned d = (unsigned)__cvta_generic_to_shared(dst + j * stride + (4 * c - j * bw));
+            const unsigned d = (unsigned)__cvta_generic_to_shared(dst + j * stride + 4 * r);
             asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src + 4 * c) : "memory");
+            r += bc.dr;
+            j += bc.dj;
+            if (r >= bc.q) {
+                r -= bc.q;
+                j++;
+            }
         }
     } else {
         for (int c = lane; c < tw; c += 32) {
-            const int j = c / bw;
-            const unsigned d = (unsigned)__cvta_generic_to_shared(dst + j * stride + (c - j * bw));
+            const unsigned d = (unsigned)__cvta_generic_to_shared(dst + j * stride + r);
             asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src + c) : "memory");
+            r += bc.dr;
+            j += bc.dj;
+            if (r >= bc.q) {
+                r -= bc.q;
+                j++;
+            }
         }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 // the two accumulation loops of one row (pass 0: valid pixels; pass 1:
-// pixels inside [lcut, hcut])
+// pixels inside [lcut, hcut]).  The tests are made on the float: a float
+// compares with the float cuts as its double does, and f > (float)-BIG as
+// (double)f > -BIG (the float nearest -1e30 lies below it, the next one up
+// above it).  The square of a float is exact in double, so fma(p, p, s) is
+// s + p * p rounded once, as the reference adds it.
 template <int PASS>
-__device__ __forceinline__ void band_add(double pix, float lcut, float hcut, double &mean, double &sigma, int &npix) {
-    const bool in = PASS == 0 ? pix > -SX_BIG : (pix <= hcut && pix >= lcut);
-    mean += in ? pix : 0.0;
-    sigma += in ? pix * pix : 0.0;
+__device__ __forceinline__ void band_add(float f, float lcut, float hcut, double &mean, double &sigma, int &npix) {
+    const bool in = PASS == 0 ? f > (float)-SX_BIG : (f <= hcut && f >= lcut);
+    const double pix = (double)(in ? f : 0.0f);
+    mean += pix;
+    sigma = fma(pix, pix, sigma);
     npix += in;
 }
 
@@ -169,6 +193,12 @@ __global__ void __launch_bounds__(32) k_mesh_stat_band(const float *__restrict__
     const bool active = lane < nmesh;
     const int mw = lane == nmesh - 1 ? mw_last : bw;
     const int rowf = 32 * stride;  // floats per staged row
+    BandCopy bc;
+    bc.q = VEC ? bw >> 2 : bw;
+    bc.j0 = lane / bc.q;
+    bc.r0 = lane - bc.j0 * bc.q;
+    bc.dj = 32 / bc.q;
+    bc.dr = 32 - bc.dj * bc.q;
     double sig, mean = 0.0, sigma = 0.0;
     const double step = sqrt(2 / SX_PI) * SX_QUANTIF_NSIGMA / SX_QUANTIF_AMIN;
     int npix = 0;
@@ -177,14 +207,14 @@ __global__ void __launch_bounds__(32) k_mesh_stat_band(const float *__restrict__
     for (int pass = 0; pass < 2; pass++) {
         for (int y = 0; y < BAND_STAGES - 1; y++) {
             if (y < mh)
-                band_row_async<VEC>(band_smem + y * rowf, img, w, y0 + y, x0, bw, tw, stride);
+                band_row_async<VEC>(band_smem + y * rowf, img, w, y0 + y, x0, tw, stride, bc);
             else
                 asm volatile("cp.async.commit_group;" ::: "memory");
         }
         for (int y = 0; y < mh; y++) {
             const int ya = y + BAND_STAGES - 1;
             if (ya < mh)
-                band_row_async<VEC>(band_smem + (ya % BAND_STAGES) * rowf, img, w, y0 + ya, x0, bw, tw, stride);
+                band_row_async<VEC>(band_smem + (ya % BAND_STAGES) * rowf, img, w, y0 + ya, x0, tw, stride, bc);
             else
                 asm volatile("cp.async.commit_group;" ::: "memory");
             asm volatile("cp.async.wait_group %0;" ::"n"(BAND_STAGES - 1) : "memory");
@@ -378,6 +408,202 @@ __global__ void __launch_bounds__(GUESS_THREADS) k_mesh_guess(const float *__res
     }
     __syncthreads();
     guess_from_hist(hist, pfx, bm, back + m, sig + m);
+}
+
+// ---------------------------------------------------------------------------
+// backhisto + backguess with one warp per mesh, for meshes of fewer than
+// 65536 pixels (no bin count reaches 2^16).  The histogram is kept as 16-bit
+// counts, two per word, and summarised per chunk of 32 bins: the counts
+// below each chunk (cp) and each chunk's first and second moments (c1, c2).
+// A clipping iteration then reads the two partial chunks at the ends of its
+// cut range and the chunk sums between them, and finds the median split from
+// the chunk prefix and one chunk's scan, instead of walking the cut range.
+// The integer sums, the split and the double arithmetic are those of
+// guess_from_hist, so the mode and sigma are the same bits.
+constexpr int GW_WARPS = 4;                        // meshes (warps) per CTA
+constexpr int GW_CH = (SX_QUANTIF_NMAXLEVELS + 2 + 31) / 32;  // 32-bin chunks
+constexpr int GW_WORDS = GW_CH * 16;              // 16-bit counts of GW_CH * 32 bins
+
+struct GuessWarpSmem {
+    long long c2[GW_CH];    // sum over the chunk of bin^2 * count
+    int c1[GW_CH];          // sum over the chunk of bin * count (< 2^28)
+    int cp[GW_CH + 1];      // counts of the bins below chunk c
+    unsigned hw[GW_WORDS];  // bin b: bits 16 (b & 1) .. of word b >> 1
+};
+
+__device__ __forceinline__ int gw_hist(const GuessWarpSmem &S, int b) {
+    return (int)((S.hw[b >> 1] >> ((b & 1) << 4)) & 0xffffu);
+}
+
+// counts of the bins below bin i (0 <= i <= 32 GW_CH), whole warp
+__device__ __forceinline__ int gw_pfx(const GuessWarpSmem &S, int i, int lane) {
+    const int c = i >> 5, r = i & 31;
+    const int v = lane < r ? gw_hist(S, 32 * c + lane) : 0;
+    return S.cp[c] + (int)__reduce_add_sync(0xffffffffu, (unsigned)v);
+}
+
+__global__ void __launch_bounds__(32 * GW_WARPS) k_mesh_guess_warp(const float *__restrict__ img, int w, int h, int bw,
+                                                                    int bh, int nbx, int nby,
+                                                                    const MeshStat *__restrict__ ms,
+                                                                    float *__restrict__ back,
+                                                                    float *__restrict__ sig) {
+    __shared__ GuessWarpSmem smem[GW_WARPS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int m = blockIdx.x * GW_WARPS + wid;
+    if (m >= nbx * nby) return;  // whole warp
+    GuessWarpSmem &S = smem[wid];
+    const MeshStat bm = ms[m];
+    if (bm.mean <= -SX_BIG) {
+        if (lane == 0) back[m] = sig[m] = -SX_BIG;
+        return;
+    }
+    const int mx = m % nbx, my = m / nbx;
+    const int x0 = mx * bw, y0 = my * bh;
+    const int mw = (mx == nbx - 1 && w % bw) ? w % bw : bw;
+    const int mh = (my == nby - 1 && h % bh) ? h % bh : bh;
+    for (int i = lane; i < GW_WORDS; i += 32) S.hw[i] = 0u;
+    __syncwarp();
+    const int nlevels = bm.nlevels;
+    const float qscale = bm.qscale;
+    const float cste = 0.499999 - bm.qzero / qscale;
+    for (int r = 0; r < mh; r++) {
+        const float *row = img + (size_t)(y0 + r) * w + x0;
+#pragma unroll 2
+        for (int x = lane; x < mw; x += 32) {
+            const float b = __ldg(row + x) / qscale + cste;
+            if (b != b) continue;  // NaN: the host conversion yields INT_MIN
+            const int bin = (int)b;
+            if (bin >= 0 && bin < nlevels) atomicAdd(&S.hw[bin >> 1], 1u << ((bin & 1) << 4));
+        }
+    }
+    __syncwarp();
+    // chunk sums: lane owns chunks lane, lane + 32, ...; words read in an
+    // order rotated by the lane (at most two lanes on a bank)
+    int carry = 0;
+    for (int c0 = 0; c0 < GW_CH; c0 += 32) {
+        const int c = c0 + lane;
+        int s0 = 0, k1 = 0, k2 = 0;
+        if (c < GW_CH) {
+#pragma unroll 4
+            for (int t = 0; t < 16; t++) {
+                const int tw = (t + lane) & 15;
+                const unsigned wv = S.hw[16 * c + tw];
+                const int n0 = (int)(wv & 0xffffu), n1 = (int)(wv >> 16), k = 2 * tw;
+                s0 += n0 + n1;
+                k1 += k * n0 + (k + 1) * n1;
+                k2 += k * k * n0 + (k + 1) * (k + 1) * n1;
+            }
+            S.c1[c] = 32 * c * s0 + k1;
+            S.c2[c] = (long long)(32 * c) * (32 * c) * s0 + (long long)(64 * c) * k1 + k2;
+        }
+        int inc = s0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        if (c < GW_CH) S.cp[c] = carry + inc - s0;
+        carry += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (lane == 0) S.cp[GW_CH] = carry;
+    __syncwarp();
+
+    // src/back.c:347-432, every lane computing the same values
+    const int nlevelsm1 = nlevels - 1;
+    double sig_ = 10.0 * nlevelsm1, sig1 = 1.0, mea = bm.mean, med = bm.mean;
+    int lcut = 0, hcut = nlevelsm1;
+    for (int n = 100;;) {
+        if (!(n-- && (sig_ >= 0.1) && (fabs(sig_ / sig1 - 1.0) > SX_EPS))) break;
+        const int nn = hcut - lcut + 1;
+        // exact integer sums over [lcut, hcut]
+        long long sum = 0, t1 = 0, t2 = 0;
+        int il = lcut;
+        const int base = gw_pfx(S, lcut, lane);
+        if (nn > 0) {
+            const int cl = lcut >> 5, ch = hcut >> 5;
+            int p0 = 0, p1 = 0;
+            long long p2 = 0;
+            {
+                const int b = 32 * cl + lane;
+                if (b >= lcut && b <= hcut) {
+                    const int v = gw_hist(S, b);
+                    p0 += v;
+                    p1 += b * v;
+                    p2 += (long long)b * b * v;
+                }
+            }
+            if (ch != cl) {
+                const int b = 32 * ch + lane;
+                if (b <= hcut) {
+                    const int v = gw_hist(S, b);
+                    p0 += v;
+                    p1 += b * v;
+                    p2 += (long long)b * b * v;
+                }
+            }
+            for (int c = cl + 1 + lane; c < ch; c += 32) {
+                p0 += S.cp[c + 1] - S.cp[c];
+                p1 += S.c1[c];
+                p2 += S.c2[c];
+            }
+            sum = (int)__reduce_add_sync(0xffffffffu, (unsigned)p0);
+            t1 = (int)__reduce_add_sync(0xffffffffu, (unsigned)p1);
+            for (int o = 16; o > 0; o >>= 1) p2 += __shfl_xor_sync(0xffffffffu, p2, o);
+            t2 = p2;
+            // split of the two-pointer walk: the smallest bin i >= lcut with
+            // pfx(i) + pfx(i + 1) >= sum + 2 pfx(lcut) (bin hcut qualifies);
+            // first the chunk whose last bin qualifies, then the bin in it
+            const int T = (int)sum + 2 * base;
+            int cstar = ch;
+            for (int c0 = cl; c0 <= ch; c0 += 32) {
+                const int c = c0 + lane;
+                const bool ok = c <= ch && 2 * S.cp[c + 1] - gw_hist(S, 32 * c + 31) >= T;
+                const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                if (bal) {
+                    cstar = c0 + __ffs(bal) - 1;
+                    break;
+                }
+            }
+            const int hk = gw_hist(S, 32 * cstar + lane);
+            int inc = hk;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += v;
+            }
+            const int pk = S.cp[cstar] + inc - hk;  // pfx(32 cstar + lane)
+            const unsigned bal = __ballot_sync(0xffffffffu, 2 * pk + hk >= T);
+            il = max(32 * cstar + (bal ? __ffs(bal) - 1 : 31), lcut);
+        }
+        const int ih = il - 1;
+        const int pil = gw_pfx(S, il, lane), phc = gw_pfx(S, hcut + 1, lane);
+        const unsigned long lowsum = (unsigned long)(pil - base);
+        const unsigned long highsum = (unsigned long)(phc - pil);
+        sig1 = sig_;
+        sig_ = (double)t2;
+        mea = (double)t1;
+        const long hl = gw_hist(S, il), hh = ih >= 0 ? gw_hist(S, ih) : 0;
+        med = ih >= 0 ? ((double)ih + 0.5 + ((double)highsum - lowsum) / (2.0 * (hl > hh ? hl : hh))) : 0.0;
+        if (sum) {
+            mea /= (double)sum;
+            sig_ = sig_ / sum - mea * mea;
+        }
+        sig_ = sig_ > 0.0 ? sqrt(sig_) : 0.0;
+        double ftemp;
+        lcut = (ftemp = med - 3.0 * sig_) > 0.0 ? (int)(ftemp > 0.0 ? ftemp + 0.5 : ftemp - 0.5) : 0;
+        hcut = (ftemp = med + 3.0 * sig_) < nlevelsm1 ? (int)(ftemp > 0.0 ? ftemp + 0.5 : ftemp - 0.5) : nlevelsm1;
+    }
+    if (lane == 0) {
+        float mean;
+        // src/back.c:408: the C library abs(int) applied to the double sig
+        if (abs((int)sig_) > 0.0) {
+            if (fabs((mea - med) / sig_) < 0.3)
+                mean = bm.qzero + (2.5 * med - 1.5 * mea) * bm.qscale;
+            else
+                mean = bm.qzero + med * bm.qscale;
+        } else
+            mean = bm.qzero + mea * bm.qscale;
+        back[m] = mean;
+        sig[m] = sig_ * bm.qscale;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -930,7 +1156,11 @@ void launch_background(BackBufs &B, const float *img, const FrameParams &P, Fram
     } else {
         k_mesh_stat<<<(nb + 127) / 128, 128, 0, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, B.ms);
     }
-    k_mesh_guess<<<nb, GUESS_THREADS, 0, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, B.ms, B.back, B.sigma);
+    if ((long long)P.bw * P.bh < 65536)
+        k_mesh_guess_warp<<<(nb + GW_WARPS - 1) / GW_WARPS, 32 * GW_WARPS, 0, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx,
+                                                                                   P.nby, B.ms, B.back, B.sigma);
+    else
+        k_mesh_guess<<<nb, GUESS_THREADS, 0, st>>>(img, P.w, P.h, P.bw, P.bh, P.nbx, P.nby, B.ms, B.back, B.sigma);
     k_mesh_badfill<<<(nb + 127) / 128, 128, 0, st>>>(B.back, B.sigma, B.back2, P.nbx, P.nby);
     k_mesh_median<<<(nb + 127) / 128, 128, 0, st>>>(B.back2, B.sigma, B.back3, B.sigma3, P.nbx, P.nby, P.nfx / 2,
                                                    P.nfy / 2, P.fthresh);

@@ -58,6 +58,43 @@ def test_background_bitexact(gpu_ctx):
         assert np.array_equal(sub_g, sub_o)
 
 
+@pytest.mark.parametrize("kind", ["poisson", "constant_meshes", "bimodal", "blanks", "spikes", "mesh_255",
+                                  "mesh_256", "ragged"])
+def test_background_histogram_shapes(gpu_ctx, kind):
+    """Mesh histograms of unusual shapes: few distinct values (many pixels
+    per bin), meshes of zero spread, two modes, blank pixels, a spike on a
+    flat sky, meshes of 65025 pixels (the largest of the warp-per-mesh
+    histogram) and of 65536 (the CTA-per-mesh form), ragged last meshes.
+    Mesh modes and sigmas and the subtracted frame, bit for bit."""
+    rng = np.random.default_rng(21)
+    shape, bs = (384, 512), 64
+    if kind == "poisson":
+        img = rng.poisson(3.0, shape).astype(np.float32)
+    elif kind == "constant_meshes":
+        img = rng.normal(100, 5, shape).astype(np.float32)
+        img[:128, :192] = 42.0
+    elif kind == "bimodal":
+        img = np.where(rng.random(shape) < 0.3, rng.normal(50, 2, shape), rng.normal(80, 3, shape)).astype(np.float32)
+    elif kind == "blanks":
+        img = rng.normal(300, 12, shape).astype(np.float32)
+        img[rng.random(shape) < 0.2] = -1e30
+    elif kind == "spikes":
+        img = rng.normal(0, 1, shape).astype(np.float32)
+        img[rng.random(shape) < 0.05] = 5e3
+    elif kind in ("mesh_255", "mesh_256"):
+        shape, bs = (600, 700), int(kind[-3:])
+        img = rng.normal(200, 10, shape).astype(np.float32)
+    else:
+        shape, bs = (389, 517), 48
+        img = rng.gamma(2.0, 30.0, shape).astype(np.float32)
+    sub_g, back_g, sig_g, sg = gpu_ctx.background(img, back_size=bs)
+    sub_o, back_o, sig_o, so = O.background(img, back_size=bs)
+    assert np.array_equal(back_g, back_o)
+    assert np.array_equal(sig_g, sig_o)
+    assert sg.backmean == so.backmean and sg.backsig == so.backsig
+    assert np.array_equal(sub_g, sub_o)
+
+
 def test_filter_bitexact(gpu_ctx, masks):
     rng = np.random.default_rng(3)
     sub = rng.normal(0, 10, (300, 257)).astype(np.float32)
