@@ -466,14 +466,34 @@ __global__ void __launch_bounds__(32 * GW_WARPS) k_mesh_guess_warp(const float *
     const int nlevels = bm.nlevels;
     const float qscale = bm.qscale;
     const float cste = 0.499999 - bm.qzero / qscale;
-    for (int r = 0; r < mh; r++) {
-        const float *row = img + (size_t)(y0 + r) * w + x0;
-#pragma unroll 2
-        for (int x = lane; x < mw; x += 32) {
-            const float b = __ldg(row + x) / qscale + cste;
-            if (b != b) continue;  // NaN: the host conversion yields INT_MIN
-            const int bin = (int)b;
-            if (bin >= 0 && bin < nlevels) atomicAdd(&S.hw[bin >> 1], 1u << ((bin & 1) << 4));
+    // the mesh's pixels k = lane, lane + 32, ... in row-major order, GW_LOADS
+    // loads in flight per lane; (row, col) of k advance by (drow, dcol) per 32
+    {
+        constexpr int GW_LOADS = 16;
+        const int npx = mw * mh;
+        const int drow = 32 / mw, dcol = 32 - drow * mw;
+        int row = lane / mw, col = lane - row * mw;
+        for (int k0 = 0; k0 < npx; k0 += 32 * GW_LOADS) {
+            float v[GW_LOADS];
+#pragma unroll
+            for (int g = 0; g < GW_LOADS; g++) {
+                // beyond the mesh: NaN, which the histogram skips as it does a NaN pixel
+                v[g] = k0 + 32 * g + lane < npx ? __ldg(img + (size_t)(y0 + row) * w + x0 + col)
+                                                : __int_as_float(0x7fffffff);
+                row += drow;
+                col += dcol;
+                if (col >= mw) {
+                    col -= mw;
+                    row++;
+                }
+            }
+#pragma unroll
+            for (int g = 0; g < GW_LOADS; g++) {
+                const float b = v[g] / qscale + cste;
+                if (b != b) continue;  // NaN: the host conversion yields INT_MIN
+                const int bin = (int)b;
+                if (bin >= 0 && bin < nlevels) atomicAdd(&S.hw[bin >> 1], 1u << ((bin & 1) << 4));
+            }
         }
     }
     __syncwarp();
