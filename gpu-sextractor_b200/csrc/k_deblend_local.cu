@@ -198,19 +198,22 @@ __device__ __forceinline__ bool dl_single_peak(const DebArgs &A, int P, const un
     return *s_cnt == 1;
 }
 
-// levels, level counts, level order (highest level first)
+// levels, level counts, level order (highest level first); cdv holds the
+// filtered values of the elements, and every element's merge record starts
+// as "active from its level, not absorbed"
 template <int NT>
-__device__ __forceinline__ void dl_levels(const DebArgs &A, int P, const unsigned *pix, const float *thr,
+__device__ __forceinline__ void dl_levels(const DebArgs &A, int P, const float *cdv, const float *thr,
                                           unsigned char *lev, unsigned short *order, int *lvcnt, int *lvstart,
-                                          int *lvcur, bool count_levpix) {
+                                          int *lvcur, int *rec, bool count_levpix) {
     for (int i = threadIdx.x; i <= A.N; i += NT) {
         lvcnt[i] = 0;
         if (i < DB_MAXLEV) lvcur[i] = 0;
     }
     __syncthreads();
     for (int k = threadIdx.x; k < P; k += NT) {
-        const int lo = dl_level_of(A.cd[pix[k]], thr, A.N);
+        const int lo = dl_level_of(cdv[k], thr, A.N);
         lev[k] = (unsigned char)lo;
+        rec[k] = (lo << 24) | 0x00ffffff;
         atomicAdd(&lvcnt[lo], 1);
     }
     __syncthreads();
@@ -294,10 +297,17 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     XSum xs;
     xs_init(xs);
     unsigned pk = 0u;
+    // every element's size and flux term as the component it starts when it
+    // becomes active (nothing reads them before), and its filtered value for
+    // the levels, kept in the branch-count area until the sweep needs it
+    float *const cdv = reinterpret_cast<float *>(nds0);
     for (int k = tid; k < P; k += NT) {
         float c = A.cd[pix[k]];
         xs_add(xs, c);
         pk = max(pk, f2ord(c));
+        sz[k] = 1;
+        acc[k] = dl_term(c, e0);
+        cdv[k] = c;
     }
     xs = xs_warp_sum(xs);
     if ((tid & 31) == 0) s_part[tid >> 5] = xs;
@@ -334,7 +344,7 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     if (dl_single_peak<NT>(A, P, pix, &s_npeak)) {
         // no split possible: the levels only count towards the summary
         unsigned ls = 0;
-        for (int k = tid; k < P; k += NT) ls += (unsigned)dl_level_of(A.cd[pix[k]], thr, A.N);
+        for (int k = tid; k < P; k += NT) ls += (unsigned)dl_level_of(cdv[k], thr, A.N);
         ls = __reduce_add_sync(0xffffffffu, ls);
         if ((tid & 31) == 0 && ls) atomicAdd(&A.sc->levpix, (unsigned long long)ls);
         if (tid == 0) {
@@ -343,7 +353,7 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
         }
         return;
     }
-    dl_levels<NT>(A, P, pix, thr, lev, order, lvcnt, lvstart, lvcur, true);
+    dl_levels<NT>(A, P, cdv, thr, lev, order, lvcnt, lvstart, lvcur, rec, true);
     int cur = 0, lastL = -1;
     for (int L = A.N - 1; L >= 0; L--) {
         const int cnt = lvcnt[L];
@@ -352,14 +362,9 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
         const int b0 = lvstart[L], b1 = b0 + cnt;
         const int nold = lastL >= 0 ? s_nrl[prv] : 0;
         const int nprev = lastL >= 0 ? s_nn[prv] : 0;
-        // (a) sizes and fluxes of the new pixels; the children re-flagged at
-        // level L+1 when the levels since the last populated one were empty
-        for (int i = b0 + tid; i < b1; i += NT) {
-            const int e = order[i];
-            sz[e] = 1;
-            acc[e] = dl_term(A.cd[pix[e]], e0);
-            rec[e] = (L << 24) | 0x00ffffff;  // active from level L, not absorbed yet
-        }
+        // (a) the children re-flagged at level L+1 when the levels since the
+        // last populated one were empty (the new pixels' sizes, flux terms and
+        // records were set before the sweep)
         if (lastL > cl)
             for (int i = tid; i < nprev; i += NT) {
                 const int c = NDR(prv)[i];
