@@ -484,9 +484,9 @@ def run_batch(ctx, frames, reps=5, workers=8, maxobj=400000):
 # DRAM bytes (read + write) per c1 frame of each stage's launches, from one
 # ncu launch-list capture of bench.py --profile-case c1 (its summary is kept
 # under profiles/)
-NCU_TRAFFIC = {"background": 134_600_000, "sub_filter": 208_200_000, "ccl": 275_000_000, "roots": 668_900_000,
-               "deblend": 686_700_000, "analyse": 388_900_000, "clean": 14_900_000, "endobject": 211_500_000,
-               "catalog": 23_900_000}
+NCU_TRAFFIC = {"background": 134_700_000, "sub_filter": 207_900_000, "ccl": 168_700_000, "roots": 671_800_000,
+               "deblend": 715_500_000, "analyse": 406_900_000, "clean": 14_900_000, "endobject": 212_400_000,
+               "catalog": 24_000_000}
 
 
 def algorithmic_bytes(stage, N, s):
