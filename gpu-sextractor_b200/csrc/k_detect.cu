@@ -709,19 +709,45 @@ __global__ void k_ccl_border_ne(int *__restrict__ lab, int w, int h, int *status
 }
 
 // every pixel to its root, and the component sizes: lanes of a warp holding
-// the same root add once to cnt (zeroed before)
+// the same root add once to cnt (zeroed before).  Four consecutive pixels a
+// thread, their labels read and written as one 16-byte word where all four
+// are in the frame: each entry written is -1 (background, which nothing else
+// writes) or the pixel's root, so a concurrent walk through it still reads an
+// ancestor (the walks only read).
 __global__ void k_ccl_flatten(int *__restrict__ lab, long long n, int *__restrict__ cnt, int *status, int loop_cap) {
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int r = -1;
-    if (p < n) {
-        const int l = lab[p];
-        if (l >= 0) {
-            r = gfind(lab, (int)p, ccl_walk_cap(loop_cap), status);
-            if (r != l) lab[p] = r;
+    const long long base = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const bool vec = base + 3 < n && (reinterpret_cast<uintptr_t>(lab) & 15) == 0;
+    int l[4], r[4];
+    if (vec) {
+        const int4 v = *reinterpret_cast<const int4 *>(lab + base);
+        l[0] = v.x;
+        l[1] = v.y;
+        l[2] = v.z;
+        l[3] = v.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) l[k] = base + k < n ? lab[base + k] : -1;
+    }
+    bool changed = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        r[k] = l[k] >= 0 ? gfind(lab, (int)(base + k), ccl_walk_cap(loop_cap), status) : -1;
+        changed |= r[k] != l[k];
+    }
+    if (changed) {
+        if (vec) {
+            *reinterpret_cast<int4 *>(lab + base) = make_int4(r[0], r[1], r[2], r[3]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (r[k] != l[k]) lab[base + k] = r[k];
         }
     }
-    const unsigned same = __match_any_sync(0xffffffffu, r);
-    if (r >= 0 && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&cnt[r], __popc(same));
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const unsigned same = __match_any_sync(0xffffffffu, r[k]);
+        if (r[k] >= 0 && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&cnt[r[k]], __popc(same));
+    }
 }
 
 // cnt: zeroed, w*h ints; receives the size of every component at its root
@@ -745,7 +771,7 @@ void launch_ccl(int *lab, int *cnt, const FrameParams &P, FrameScalars *d_sc, cu
         launches += 4;
     }
     long long n = (long long)P.w * P.h;
-    k_ccl_flatten<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(lab, n, cnt, status, P.loop_cap);
+    k_ccl_flatten<<<(unsigned)((n + 1023) / 1024), 256, 0, st>>>(lab, n, cnt, status, P.loop_cap);
 }
 
 }  // namespace sx

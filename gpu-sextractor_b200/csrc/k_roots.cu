@@ -75,11 +75,28 @@ __global__ void k_root_thresholds_global(int nroots, const int *nroots_dev, cons
 // tiles of SCAN_TILE pixels are those of the scan primitive (1024 threads, 4
 // consecutive pixels each), so the per-tile counts of k_root_tile_counts and
 // the in-tile prefixes of k_root_number / k_root_compact line up.
-__device__ __forceinline__ void root_kept_flags(const int *__restrict__ lab, const int *__restrict__ cnt, long long p,
-                                                long long n, int minarea, int &isroot, int &kept, int &l) {
-    l = p < n ? lab[p] : -1;
-    kept = l >= 0 && cnt[l] >= minarea;
-    isroot = kept && l == (int)p;
+// The flags of a thread's SCAN_ITEMS (= 4) consecutive pixels from base (a
+// multiple of 4), with one 16-byte load of their labels where all four are
+// in the frame and the label array is 16-byte aligned.
+__device__ __forceinline__ void root_kept_flags4(const int *__restrict__ lab, const int *__restrict__ cnt,
+                                                 long long base, long long n, int minarea, int *isroot, int *kept,
+                                                 int *l) {
+    static_assert(SCAN_ITEMS == 4, "four pixels per thread");
+    if (base + 3 < n && ((reinterpret_cast<uintptr_t>(lab) & 15) == 0)) {
+        const int4 v = *reinterpret_cast<const int4 *>(lab + base);
+        l[0] = v.x;
+        l[1] = v.y;
+        l[2] = v.z;
+        l[3] = v.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) l[k] = base + k < n ? lab[base + k] : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        kept[k] = l[k] >= 0 && cnt[l[k]] >= minarea;
+        isroot[k] = kept[k] && l[k] == (int)(base + k);
+    }
 }
 
 // per tile: number of roots and of kept pixels
@@ -89,13 +106,12 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_root_tile_counts(const int *__
                                                                   int *__restrict__ tkept) {
     __shared__ int sh[32];
     const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
-    int cr = 0, ck = 0;
+    int cr = 0, ck = 0, r[SCAN_ITEMS], kp[SCAN_ITEMS], l[SCAN_ITEMS];
+    root_kept_flags4(lab, cnt, base, n, minarea, r, kp, l);
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS; k++) {
-        int r, kp, l;
-        root_kept_flags(lab, cnt, base + k, n, minarea, r, kp, l);
-        cr += r;
-        ck += kp;
+        cr += r[k];
+        ck += kp[k];
     }
     int tot;
     block_exclusive_scan(cr, sh, tot);
@@ -111,13 +127,10 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_root_number(const int *__restr
                                                              int *__restrict__ rfirst) {
     __shared__ int sh[32];
     const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
-    int fr[SCAN_ITEMS], c = 0;
+    int fr[SCAN_ITEMS], kp[SCAN_ITEMS], l[SCAN_ITEMS], c = 0;
+    root_kept_flags4(lab, cnt, base, n, minarea, fr, kp, l);
 #pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++) {
-        int kp, l;
-        root_kept_flags(lab, cnt, base + k, n, minarea, fr[k], kp, l);
-        c += fr[k];
-    }
+    for (int k = 0; k < SCAN_ITEMS; k++) c += fr[k];
     int tot;
     int id = block_exclusive_scan(c, sh, tot) + toff[blockIdx.x];
 #pragma unroll
@@ -141,21 +154,27 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_root_compact(const int *__rest
                                                               int *__restrict__ pos2idx) {
     __shared__ int sh[32];
     const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
-    int fk[SCAN_ITEMS], lb[SCAN_ITEMS], c = 0;
+    int fk[SCAN_ITEMS], lb[SCAN_ITEMS], fr[SCAN_ITEMS], c = 0;
+    root_kept_flags4(lab, cnt, base, n, minarea, fr, fk, lb);
 #pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++) {
-        int r;
-        root_kept_flags(lab, cnt, base + k, n, minarea, r, fk[k], lb[k]);
-        c += fk[k];
-    }
+    for (int k = 0; k < SCAN_ITEMS; k++) c += fk[k];
     int tot;
     int j = block_exclusive_scan(c, sh, tot) + toff[blockIdx.x];
+    const bool vec = base + 3 < n && ((reinterpret_cast<uintptr_t>(alloc) | reinterpret_cast<uintptr_t>(pos2idx)) & 15) == 0;
+    if (vec) {
+        *reinterpret_cast<int4 *>(alloc + base) =
+            make_int4(lb[0] >= 0 ? SX_ALLOC_OTHER : -1, lb[1] >= 0 ? SX_ALLOC_OTHER : -1,
+                      lb[2] >= 0 ? SX_ALLOC_OTHER : -1, lb[3] >= 0 ? SX_ALLOC_OTHER : -1);
+        *reinterpret_cast<int4 *>(pos2idx + base) = make_int4(-1, -1, -1, -1);
+    }
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS; k++) {
         const long long p = base + k;
         if (p >= n) break;
-        alloc[p] = lb[k] >= 0 ? SX_ALLOC_OTHER : -1;
-        pos2idx[p] = -1;
+        if (!vec) {
+            alloc[p] = lb[k] >= 0 ? SX_ALLOC_OTHER : -1;
+            pos2idx[p] = -1;
+        }
         if (fk[k]) {
             keys[j] = (unsigned)rid[lb[k]];
             vals[j] = (unsigned)p;
