@@ -11,17 +11,6 @@
 
 namespace sx {
 
-__global__ void k_pos2idx(const unsigned *__restrict__ vals, unsigned *__restrict__ rpix, int *__restrict__ pos2idx,
-                          int m, const int *m_dev) {
-    m = sx_count(m, m_dev);
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < m) {
-        const unsigned p = vals[j];
-        rpix[j] = p;
-        pos2idx[p] = j;
-    }
-}
-
 // Each raw object's thresholds: the smallest detection and analysis threshold
 // of its pixels (the global ones without a weight map); rdthr/rathr start at a
 // large positive float and are lowered through their bit patterns (positive

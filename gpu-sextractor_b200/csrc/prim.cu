@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const unsigned *__res
                                                              unsigned *__restrict__ kout,
                                                              unsigned *__restrict__ vout, int n, int shift,
                                                              int ntiles, const int *__restrict__ offs,
-                                                             const int *n_dev) {
+                                                             const int *n_dev, int *__restrict__ posmap) {
     __shared__ int cnt[RS_WARPS][RS_DIGITS];
     n = dev_count(n, n_dev);
     __shared__ int gbase[RS_DIGITS];
@@ -187,6 +187,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const unsigned *__res
             int pos = gbase[d] + cnt[wid][d] + rank[r];
             kout[pos] = key[r];
             vout[pos] = val[r];
+            if (posmap) posmap[val[r]] = pos;
         }
     }
 }
@@ -202,17 +203,32 @@ __global__ void k_copy_pairs(const unsigned *__restrict__ ka, const unsigned *__
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < dev_count(n, n_dev)) {
         kb[i] = ka[i];
-        vb[i] = va[i];
+        if (va) vb[i] = va[i];
     }
+}
+
+// a one-element sort with a final value array: the value and its position
+__global__ void k_copy_one(const unsigned *__restrict__ vals, unsigned *__restrict__ vfinal, int *__restrict__ posmap,
+                           const int *n_dev) {
+    if (dev_count(1, n_dev) < 1) return;
+    vfinal[0] = vals[0];
+    if (posmap) posmap[vals[0]] = 0;
 }
 
 // Stable sort by the low keybits bits of keys.  Result ends in (keys, vals);
 // (kalt, valt) are scratch of n elements each.  n_dev (device, may be NULL):
 // the count, at most n, when only the device knows it (elements beyond it
-// are left as they are).
+// are left as they are).  With vfinal (n elements), the last pass writes the
+// sorted values there instead, and with posmap also posmap[value] = its
+// sorted position (the values then index posmap); vals is left as scratch.
 void radix_sort_pairs(unsigned *keys, unsigned *vals, unsigned *kalt, unsigned *valt, long long n,
-                      int keybits, int *tmp, cudaStream_t st, const int *n_dev) {
-    if (n <= 1) return;
+                      int keybits, int *tmp, cudaStream_t st, const int *n_dev, unsigned *vfinal, int *posmap) {
+    if (n <= 1) {
+        // nothing to sort: the one value (if any) and its position
+        if (vfinal && n == 1)
+            k_copy_one<<<1, 1, 0, st>>>(vals, vfinal, posmap, n_dev);
+        return;
+    }
     int nt = (int)((n + RS_TILE - 1) / RS_TILE);
     long long h = (long long)nt * RS_DIGITS;
     int *hist = tmp, *offs = tmp + h, *stmp = tmp + 2 * h;
@@ -220,11 +236,24 @@ void radix_sort_pairs(unsigned *keys, unsigned *vals, unsigned *kalt, unsigned *
     int passes = (keybits + RS_BITS - 1) / RS_BITS;
     for (int p = 0; p < passes; p++) {
         int shift = p * RS_BITS;
+        const bool last = p == passes - 1;
+        unsigned *vo = last && vfinal ? vfinal : vb;
         k_rs_hist<<<nt, RS_THREADS, 0, st>>>(ka, (int)n, shift, nt, hist, n_dev);
         exclusive_scan(hist, offs, h, nullptr, stmp, st, nullptr);
-        k_rs_scatter<<<nt, RS_THREADS, 0, st>>>(ka, va, kb, vb, (int)n, shift, nt, offs, n_dev);
+        k_rs_scatter<<<nt, RS_THREADS, 0, st>>>(ka, va, kb, vo, (int)n, shift, nt, offs, n_dev,
+                                                last ? posmap : nullptr);
         unsigned *t = ka; ka = kb; kb = t;
         t = va; va = vb; vb = t;
+    }
+    if (vfinal) {
+        // the values are in vfinal; the keys go back if they ended in kalt
+        if (ka != keys) {
+            if (n_dev)
+                k_copy_pairs<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ka, nullptr, keys, nullptr, (int)n, n_dev);
+            else
+                cudaMemcpyAsync(keys, ka, n * sizeof(unsigned), cudaMemcpyDeviceToDevice, st);
+        }
+        return;
     }
     if (ka != keys) {
         if (n_dev) {

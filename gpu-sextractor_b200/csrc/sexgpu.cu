@@ -778,11 +778,13 @@ int pipe_detect(sexgpu_ctx *ctx) {
     }
     ps.nrootpix = nrootpix;
     const int *nrootpix_dev = ps.capf ? &d_sc->nrootpix : nullptr;
-    radix_sort_pairs(keys, vals, P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), nrootpix, bits_for(nroots), tmp, st,
-                     nrootpix_dev);
+    // the sort's last pass writes the pixel lists (rpix) and each root
+    // pixel's list index (pos2idx) directly
     unsigned *rpix = P<unsigned>(ctx->rpix);
-    k_pos2idx<<<grid1(nrootpix, 256), 256, 0, st>>>(vals, rpix, pos2idx, nrootpix, nrootpix_dev);
-    stage_mark(ctx, "roots", 5 + 2 * scan_launches(ntile) + scan_launches(nroots) + radix_launches(bits_for(nroots), nrootpix));
+    radix_sort_pairs(keys, vals, P<unsigned>(ctx->kalt), P<unsigned>(ctx->valt), nrootpix, bits_for(nroots), tmp, st,
+                     nrootpix_dev, rpix, pos2idx);
+    stage_mark(ctx, "roots", 4 + 2 * scan_launches(ntile) + scan_launches(nroots) +
+                                 radix_launches(bits_for(nroots), nrootpix) + (nrootpix == 1 ? 1 : 0));
     ps.stage = 2;
     return SEXGPU_OK;
 }
